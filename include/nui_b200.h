@@ -1,0 +1,222 @@
+/*
+ * nui_b200 -- C ABI of the B200 KinectFusion hot path.
+ *
+ * Replaces the device layer of hustztz/NatureUserInterfaceStudio for the per-frame path:
+ * src/OpenCLUtilities (context/queue singleton, kernel manager, buffer manager) and the
+ * OpenCL implementations of the tracker / frame / scene interfaces under
+ * src/SLAM/VisualOdometry/DeviceSpecific.  Plain C types only: host pointers for the
+ * session-level calls, device pointers (CUDA global memory of the context's device) for
+ * the kernel-level calls, sizes as integers, an int status for every call.
+ *
+ * Threading: one session must not be called concurrently from two threads; different
+ * sessions may be.  Every session-level call is synchronous with respect to the host
+ * buffers it is given (they may be reused when the call returns).
+ */
+#ifndef NUI_B200_H
+#define NUI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define NUI_API __attribute__((visibility("default")))
+#else
+#define NUI_API
+#endif
+
+/* ---------------------------------------------------------------- status codes
+ * The reference returns bool and prints OpenCL errors to stderr
+ * (src/OpenCLUtilities/NuiOpenCLUtil.h:10-13); here every call returns one of these. */
+typedef enum {
+  NUI_OK = 0,
+  NUI_ERR_INVALID_ARG = 1,
+  NUI_ERR_OOM = 2,
+  NUI_ERR_TRACKING_LOST = 3, /* singular ICP system (NuiKinfuOpenCLDepthTracker.cpp:465-472) */
+  NUI_ERR_HASH_FULL = 4,
+  NUI_ERR_MESH_OVERFLOW = 5,
+  NUI_ERR_TIMEOUT = 6,
+  NUI_ERR_DEVICE = 7,
+  NUI_ERR_UNSUPPORTED = 8
+} nui_status;
+
+/* TSDF storage formats of the dense volume.
+ * NUI_TSDF_I16 is the reference's short2 (tsdf * 32766 truncated, int16 weight;
+ * tsdfVolume.cl:31-190 with utils.cl:69-79).  The others store the same running average
+ * without the 16-bit quantisation. */
+typedef enum {
+  NUI_TSDF_I16 = 0,     /* 4 B/voxel: int16 tsdf, int16 weight                 */
+  NUI_TSDF_F32 = 1,     /* 8 B/voxel: float tsdf, float weight                 */
+  NUI_TSDF_F16_U8 = 2,  /* 3 B/voxel: half tsdf plane + uint8 weight plane     */
+  NUI_TSDF_F16_F16 = 3  /* 4 B/voxel: half tsdf, half weight                   */
+} nui_tsdf_format;
+
+typedef enum { NUI_VOLUME_DENSE = 0, NUI_VOLUME_HASH = 1 } nui_volume_kind;
+
+/* Session configuration.  Field meaning and defaults follow the reference configs:
+ * NuiTrackerConfig (NuiTrackerConfig.cpp:5-24), NuiKinfuVolumeConfig
+ * (NuiKinfuVolumeConfig.cpp:5-15), NuiCameraParams / NuiDepthFrame sensor range
+ * (src/Frame/NuiDepthFrame.h:12-16) and the engine's integration gate
+ * (NuiKinfuTrackingEngine.cpp:22). */
+typedef struct {
+  int width, height;
+  float fx, fy, cx, cy;
+  float depth_min, depth_max; /* metres; depth outside (min, max) is invalid */
+  /* dense volume */
+  int volume_kind;            /* nui_volume_kind */
+  int tsdf_format;            /* nui_tsdf_format */
+  int res[3];
+  float dim[3];               /* metres; volume spans x,y in [-dim/2, dim/2], z in [0, dim] */
+  float trunc_dist;           /* VolumeTrancDist; effective = max(trunc_dist, 2.1 * cell) */
+  int color_volume;           /* VolumeHadColor */
+  int max_color_weight;       /* MaxColorWeight */
+  /* tracker */
+  int levels;                 /* pyramid levels (<= 4) */
+  int iterations[4];          /* ICP iterations per level, finest first */
+  int filter_radius;          /* icp_filter_radius */
+  float sigma_space2_inv_half;/* icp_sigma_space2_inv_half */
+  float sigma_depth2_inv_half;/* icp_sigma_depth2_inv_half */
+  float depth_threshold;      /* icp_depth_threshold */
+  float dist_threshold;       /* icp_dist_threshold */
+  float integration_threshold;/* m_integration_metric_threshold */
+} nui_session_cfg;
+
+typedef struct nui_ctx nui_ctx;
+typedef struct nui_session nui_session;
+
+/* Fills the reference defaults (640x480, fx=fy=525, 256^3 over 3 m, 3 levels x 10 ICP
+ * iterations, bilateral radius 3, thresholds of NuiTrackerConfig). */
+NUI_API void nui_session_cfg_default(nui_session_cfg* cfg);
+
+/* Last error message of the calling thread ("" if none). */
+NUI_API const char* nui_last_error_string(void);
+
+/* ---------------------------------------------------------------- context
+ * Replaces NuiOpenCLGlobal::initializeOpenCL (NuiOpenCLGlobal.cpp:75-219): binds a CUDA
+ * device and a stream.  nui_ctx_set_stream lets the caller supply its own stream
+ * (cudaStream_t cast to void*); NULL restores the context's own stream. */
+NUI_API nui_status nui_ctx_create(int device, nui_ctx** out);
+NUI_API nui_status nui_ctx_destroy(nui_ctx* ctx);
+NUI_API nui_status nui_ctx_set_stream(nui_ctx* ctx, void* cuda_stream);
+NUI_API nui_status nui_ctx_synchronize(nui_ctx* ctx);
+
+/* ---------------------------------------------------------------- sessions
+ * A session holds one RGB-D stream's device state: frame pyramids, reference maps,
+ * pose, volume.  Construction replaces NuiKinfuTrackingFactory::BuildTrackingEngine
+ * (NuiKinfuTrackingFactory.h:23-50) + NuiSLAMController::setVolume
+ * (NuiSLAMController.cpp:33-69).  Bytes of device memory it needs: */
+NUI_API size_t nui_session_device_bytes(const nui_session_cfg* cfg);
+NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, nui_session** out);
+NUI_API nui_status nui_session_destroy(nui_session* s);
+/* NuiKinfuScene::reset + NuiKinfuTrackingEngine::reset: empty volume, identity pose. */
+NUI_API nui_status nui_reset(nui_session* s);
+
+/* One frame of NuiKinfuTrackingEngine::RunTracking (NuiKinfuTrackingEngine.cpp:68-142):
+ * upload + preprocess, then (frame 0) feedback maps + integrate, or (frame > 0) ICP,
+ * gated integration and raycast.  depth_mm: width*height uint16; bgra: width*height*4
+ * bytes or NULL.  pose_out (nullable): 12 floats, R row-major then t.
+ * Returns NUI_ERR_TRACKING_LOST when ICP hits a singular system (the frame then leaves
+ * the volume and pose untouched, as the reference's early `return false`). */
+NUI_API nui_status nui_process_frame(nui_session* s, const uint16_t* depth_mm, const uint8_t* bgra,
+                                     float* pose_out);
+/* Same with the frame already in device memory. */
+NUI_API nui_status nui_process_frame_device(nui_session* s, const uint16_t* d_depth_mm,
+                                            const uint8_t* d_bgra, float* pose_out);
+
+/* Step-wise calls mirroring the reference virtuals (for the C++ adaptor classes):
+ *  NuiKinfuFrame::UpdateVertexBuffers / UpdateColorBuffers  -> nui_frame_upload
+ *  NuiKinfuFeedbackFrame::UpdateBuffers                     -> nui_feedback_update
+ *  NuiKinfuTracker::EstimatePose                            -> nui_track
+ *  NuiKinfuScene::integrateVolume                           -> nui_integrate
+ *  NuiKinfuScene::raycastRender                             -> nui_raycast
+ *  NuiKinfuCameraState::UpdateCameraTransform / GetCameraPos-> nui_set_pose / nui_get_pose */
+NUI_API nui_status nui_frame_upload(nui_session* s, const uint16_t* depth_mm, const uint8_t* bgra);
+NUI_API nui_status nui_feedback_update(nui_session* s);
+NUI_API nui_status nui_track(nui_session* s, float* err_out, int* count_out);
+NUI_API nui_status nui_integrate(nui_session* s);
+NUI_API nui_status nui_raycast(nui_session* s);
+NUI_API nui_status nui_set_pose(nui_session* s, const float* pose12);
+NUI_API nui_status nui_get_pose(nui_session* s, float* pose12);
+
+/* Marching cubes over the dense volume (NuiKinfuScene::Volume2CLMesh,
+ * NuiKinfuOpenCLScene.cpp:617-786), compacted by prefix sums into the deterministic order
+ * of the reference's CPU extraction (y, then x, then z fastest).  pos: cap*3 floats,
+ * col: cap*4 floats (either may be NULL); *nverts receives the full vertex count, and
+ * NUI_ERR_MESH_OVERFLOW is returned (with the first cap vertices written) when it
+ * exceeds cap. */
+NUI_API nui_status nui_mesh(nui_session* s, float* pos, float* col, uint64_t cap, uint64_t* nverts);
+
+/* Debug / test readback of session buffers into host memory.  `what`:
+ *   0 filtered depth L0 (f32, W*H)      1 scaled depth for integration (f32, W*H)
+ *   2 vertex map level `level` (f32x4)  3 reference vertex map (f32x4, W*H, world)
+ *   4 reference normal map (f32x4)       5 volume in the reference layout, short2
+ *   6 raw volume storage of the session format   7 depth level `level` (f32)
+ *   8 reference colour map (u8x4)        9 colour volume, reference layout (u8x4)  */
+NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void* host, size_t bytes);
+/* Writes a reference-layout short2 volume into the session (any format). */
+NUI_API nui_status nui_debug_upload_volume(nui_session* s, const int16_t* ref_layout_short2);
+
+/* ---------------------------------------------------------------- batched ticks
+ * Advances n sessions by one frame each with one launch per stage for all of them
+ * (captured once in a CUDA graph and replayed).  depths[i] / bgras[i]: host frames
+ * (bgras may be NULL or have NULL entries).  per_session_status: n entries.
+ * poses_out (nullable): n*12 floats. */
+NUI_API nui_status nui_batch_tick(nui_ctx* ctx, nui_session* const* sessions, int n,
+                                  const uint16_t* const* depths, const uint8_t* const* bgras,
+                                  nui_status* per_session_status, float* poses_out);
+/* Same with device-resident frames (d_depths[i]: device pointers). */
+NUI_API nui_status nui_batch_tick_device(nui_ctx* ctx, nui_session* const* sessions, int n,
+                                         const uint16_t* const* d_depths, const uint8_t* const* d_bgras,
+                                         nui_status* per_session_status, float* poses_out);
+
+/* Per-stage device time of the last nui_batch_tick* / nui_process_frame* call of the
+ * context, when timing is enabled (CUDA events on the context stream).
+ * stage: 0 preprocess, 1 pyramid, 2 icp, 3 integrate, 4 raycast, 5 whole tick. */
+NUI_API nui_status nui_ctx_enable_timing(nui_ctx* ctx, int enable);
+NUI_API nui_status nui_ctx_stage_ms(nui_ctx* ctx, int stage, float* ms);
+/* Voxels read-modify-written by the last integration of a session. */
+NUI_API nui_status nui_session_touched_voxels(nui_session* s, uint64_t* n);
+
+/* ---------------------------------------------------------------- kernel-level calls
+ * One entry point per reference kernel launch on the hot path, on device pointers,
+ * launched on the context's stream (asynchronous).  Vertex/normal maps are float4 per
+ * pixel (xyz, w = 0); depth maps float; volumes in the session layout are reached
+ * through sessions only. */
+/* depth_passing_filter_kernel + bilateral_filter_depth_kernel + depth2vertex_kernel +
+ * scaleDepthsKernel (filters.cl:9-23, bilateralFilter.cl:68-119, transformMaps.cl:18-42,
+ * tsdfVolume.cl:8-29), fused: raw u16 -> filtered depth, vertex map (level 0) and the
+ * ray-length depth used by integration. */
+NUI_API nui_status nui_k_preprocess(nui_ctx* ctx, const uint16_t* d_raw, int W, int H, float fx, float fy,
+                                    float cx, float cy, float dmin, float dmax, int radius,
+                                    float sigma_space2_inv_half, float sigma_depth2_inv_half, float depth_thr,
+                                    float* d_filtered, float* d_vertex4, float* d_scaled);
+/* half_sample_kernel + depth2vertex_kernel for one pyramid level (transformMaps.cl:18-88). */
+NUI_API nui_status nui_k_pyramid_level(nui_ctx* ctx, const float* d_src, int dW, int dH, float fx, float fy,
+                                       float cx, float cy, int div, float depth_thr, float* d_dst,
+                                       float* d_vertex4);
+/* estimate_normals_simple_kernel + transform_maps_kernel (normalEstimation.cl:770-822,
+ * transformMaps.cl:91-127): camera vertices -> world vertex and normal maps.
+ * pose12: R row-major + t (host pointer). */
+NUI_API nui_status nui_k_feedback_maps(nui_ctx* ctx, const float* d_vertex4, int W, int H, float depth_thr,
+                                       const float* pose12, float* d_vref4, float* d_nref4);
+
+/* ---------------------------------------------------------------- synthetic input
+ * Seeded analytic scenes and trajectories standing in for recorded Kinect sessions. */
+typedef struct nui_synth_scene nui_synth_scene;
+enum { NUI_SYNTH_TABLETOP = 0, NUI_SYNTH_ROOM = 1 };
+NUI_API nui_synth_scene* nui_synth_scene_create(int kind, uint64_t seed, float extent);
+NUI_API void nui_synth_scene_destroy(nui_synth_scene* s);
+NUI_API float nui_synth_scene_sdf(const nui_synth_scene* s, float x, float y, float z);
+NUI_API void nui_synth_trajectory(int kind, uint64_t seed, int frame, float radius, float deg_per_frame,
+                                  float* R_out, float* t_out);
+NUI_API void nui_synth_render(const nui_synth_scene* s, const float* R, const float* t, int W, int H, float fx,
+                              float fy, float cx, float cy, uint64_t noise_seed, int frame, int add_noise,
+                              uint16_t* depth_mm, uint8_t* bgra);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NUI_B200_H */

@@ -1,0 +1,323 @@
+"""ctypes binding of libnui_b200.so (the C ABI declared in include/nui_b200.h).
+
+The library is the only implementation: if it is missing or cannot be loaded, every call
+raises -- there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnui_b200.so")
+
+NUI_OK = 0
+NUI_ERR_INVALID_ARG = 1
+NUI_ERR_OOM = 2
+NUI_ERR_TRACKING_LOST = 3
+NUI_ERR_HASH_FULL = 4
+NUI_ERR_MESH_OVERFLOW = 5
+NUI_ERR_TIMEOUT = 6
+NUI_ERR_DEVICE = 7
+NUI_ERR_UNSUPPORTED = 8
+
+TSDF_I16, TSDF_F32, TSDF_F16_U8, TSDF_F16_F16 = 0, 1, 2, 3
+SYNTH_TABLETOP, SYNTH_ROOM = 0, 1
+
+
+class SessionCfg(C.Structure):
+    _fields_ = [
+        ("width", C.c_int), ("height", C.c_int),
+        ("fx", C.c_float), ("fy", C.c_float), ("cx", C.c_float), ("cy", C.c_float),
+        ("depth_min", C.c_float), ("depth_max", C.c_float),
+        ("volume_kind", C.c_int), ("tsdf_format", C.c_int),
+        ("res", C.c_int * 3), ("dim", C.c_float * 3), ("trunc_dist", C.c_float),
+        ("color_volume", C.c_int), ("max_color_weight", C.c_int),
+        ("levels", C.c_int), ("iterations", C.c_int * 4), ("filter_radius", C.c_int),
+        ("sigma_space2_inv_half", C.c_float), ("sigma_depth2_inv_half", C.c_float),
+        ("depth_threshold", C.c_float), ("dist_threshold", C.c_float),
+        ("integration_threshold", C.c_float),
+    ]
+
+
+class NuiError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("nui status %d: %s" % (status, msg))
+        self.status = status
+
+
+_lib = None
+
+_P = C.c_void_p
+_SIGS = {
+    "nui_session_cfg_default": (None, [_P]),
+    "nui_last_error_string": (C.c_char_p, []),
+    "nui_ctx_create": (C.c_int, [C.c_int, _P]),
+    "nui_ctx_destroy": (C.c_int, [_P]),
+    "nui_ctx_set_stream": (C.c_int, [_P, _P]),
+    "nui_ctx_synchronize": (C.c_int, [_P]),
+    "nui_session_device_bytes": (C.c_size_t, [_P]),
+    "nui_session_create": (C.c_int, [_P, _P, _P]),
+    "nui_session_destroy": (C.c_int, [_P]),
+    "nui_reset": (C.c_int, [_P]),
+    "nui_process_frame": (C.c_int, [_P, _P, _P, _P]),
+    "nui_process_frame_device": (C.c_int, [_P, _P, _P, _P]),
+    "nui_frame_upload": (C.c_int, [_P, _P, _P]),
+    "nui_feedback_update": (C.c_int, [_P]),
+    "nui_track": (C.c_int, [_P, _P, _P]),
+    "nui_integrate": (C.c_int, [_P]),
+    "nui_raycast": (C.c_int, [_P]),
+    "nui_set_pose": (C.c_int, [_P, _P]),
+    "nui_get_pose": (C.c_int, [_P, _P]),
+    "nui_mesh": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
+    "nui_debug_download": (C.c_int, [_P, C.c_int, C.c_int, _P, C.c_size_t]),
+    "nui_debug_upload_volume": (C.c_int, [_P, _P]),
+    "nui_batch_tick": (C.c_int, [_P, _P, C.c_int, _P, _P, _P, _P]),
+    "nui_batch_tick_device": (C.c_int, [_P, _P, C.c_int, _P, _P, _P, _P]),
+    "nui_ctx_enable_timing": (C.c_int, [_P, C.c_int]),
+    "nui_ctx_stage_ms": (C.c_int, [_P, C.c_int, _P]),
+    "nui_session_touched_voxels": (C.c_int, [_P, _P]),
+    "nui_k_preprocess": (C.c_int, [_P, _P, C.c_int, C.c_int] + [C.c_float] * 6 + [C.c_int] + [C.c_float] * 3 + [_P, _P, _P]),
+    "nui_k_pyramid_level": (C.c_int, [_P, _P, C.c_int, C.c_int] + [C.c_float] * 4 + [C.c_int, C.c_float, _P, _P]),
+    "nui_k_feedback_maps": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_float, _P, _P, _P]),
+    "nui_synth_scene_create": (_P, [C.c_int, C.c_uint64, C.c_float]),
+    "nui_synth_scene_destroy": (None, [_P]),
+    "nui_synth_scene_sdf": (C.c_float, [_P, C.c_float, C.c_float, C.c_float]),
+    "nui_synth_trajectory": (None, [C.c_int, C.c_uint64, C.c_int, C.c_float, C.c_float, _P, _P]),
+    "nui_synth_render": (None, [_P, _P, _P, C.c_int, C.c_int] + [C.c_float] * 4 + [C.c_uint64, C.c_int, C.c_int, _P, _P]),
+}
+
+
+def lib():
+    """Load libnui_b200.so (raises if it is absent: the CUDA library is the only path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libnui_b200.so not built: run `python -m natureuserinterfacestudio_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != NUI_OK:
+        raise NuiError(status, lib().nui_last_error_string().decode())
+    return status
+
+
+def ptr(a):
+    """Host pointer of a C-contiguous numpy array (None passes NULL)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def default_cfg(**kw):
+    c = SessionCfg()
+    lib().nui_session_cfg_default(C.byref(c))
+    for k, v in kw.items():
+        if k in ("res", "dim", "iterations"):
+            arr = getattr(c, k)
+            for i, x in enumerate(v):
+                arr[i] = x
+        else:
+            setattr(c, k, v)
+    return c
+
+
+class Context:
+    def __init__(self, device=0):
+        h = C.c_void_p()
+        check(lib().nui_ctx_create(device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().nui_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle):
+        check(lib().nui_ctx_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None))
+
+    def sync(self):
+        check(lib().nui_ctx_synchronize(self.h))
+
+    def enable_timing(self, on=True):
+        check(lib().nui_ctx_enable_timing(self.h, 1 if on else 0))
+
+    def stage_ms(self, stage):
+        v = C.c_float()
+        check(lib().nui_ctx_stage_ms(self.h, stage, C.byref(v)))
+        return v.value
+
+    def batch_tick(self, sessions, depths, bgras=None, device=False):
+        """One frame for every session.  depths: list of uint16 arrays (host) or device
+        pointers (ints) when device=True.  Returns (statuses, poses[n,12])."""
+        n = len(sessions)
+        arr = (C.c_void_p * n)(*[s.h.value for s in sessions])
+        if device:
+            d = (C.c_void_p * n)(*depths)
+            b = (C.c_void_p * n)(*(bgras or [None] * n))
+        else:
+            d = (C.c_void_p * n)(*[x.ctypes.data for x in depths])
+            b = (C.c_void_p * n)(*[(x.ctypes.data if x is not None else None) for x in (bgras or [None] * n)])
+        st = np.zeros(n, np.int32)
+        poses = np.zeros((n, 12), np.float32)
+        fn = lib().nui_batch_tick_device if device else lib().nui_batch_tick
+        r = fn(self.h, arr, n, d, b, ptr(st), ptr(poses))
+        if r not in (NUI_OK, NUI_ERR_TRACKING_LOST):
+            check(r)
+        return st, poses
+
+
+class Session:
+    def __init__(self, ctx, cfg):
+        h = C.c_void_p()
+        check(lib().nui_session_create(ctx.h, C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.ctx = ctx
+        self.cfg = cfg
+        self.W, self.H = cfg.width, cfg.height
+        self.res = tuple(cfg.res)
+
+    def close(self):
+        if self.h:
+            lib().nui_session_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def process(self, depth, bgra=None):
+        pose = np.zeros(12, np.float32)
+        r = lib().nui_process_frame(self.h, ptr(depth), ptr(bgra), ptr(pose))
+        if r == NUI_ERR_TRACKING_LOST:
+            return False, pose
+        check(r)
+        return True, pose
+
+    def process_device(self, depth_ptr, bgra_ptr=None):
+        pose = np.zeros(12, np.float32)
+        r = lib().nui_process_frame_device(self.h, C.c_void_p(depth_ptr), C.c_void_p(bgra_ptr) if bgra_ptr else None,
+                                           ptr(pose))
+        if r == NUI_ERR_TRACKING_LOST:
+            return False, pose
+        check(r)
+        return True, pose
+
+    def reset(self):
+        check(lib().nui_reset(self.h))
+
+    def upload(self, depth, bgra=None):
+        check(lib().nui_frame_upload(self.h, ptr(depth), ptr(bgra)))
+
+    def feedback_update(self):
+        check(lib().nui_feedback_update(self.h))
+
+    def track(self):
+        err = C.c_float()
+        cnt = C.c_int()
+        r = lib().nui_track(self.h, C.byref(err), C.byref(cnt))
+        if r == NUI_ERR_TRACKING_LOST:
+            return False, err.value, cnt.value
+        check(r)
+        return True, err.value, cnt.value
+
+    def integrate(self):
+        check(lib().nui_integrate(self.h))
+
+    def raycast(self):
+        check(lib().nui_raycast(self.h))
+
+    def set_pose(self, R, t):
+        p = np.concatenate([np.asarray(R, np.float32).reshape(9), np.asarray(t, np.float32).reshape(3)])
+        check(lib().nui_set_pose(self.h, ptr(p)))
+
+    def get_pose(self):
+        p = np.zeros(12, np.float32)
+        check(lib().nui_get_pose(self.h, ptr(p)))
+        return p[:9].reshape(3, 3), p[9:]
+
+    def touched(self):
+        v = C.c_uint64()
+        check(lib().nui_session_touched_voxels(self.h, C.byref(v)))
+        return v.value
+
+    def download(self, what, level=0):
+        W, H = self.W >> level, self.H >> level
+        nv = self.res[0] * self.res[1] * self.res[2]
+        shapes = {0: ((H, W), np.float32), 1: ((H, W), np.float32), 2: ((H, W, 4), np.float32),
+                  3: ((self.H, self.W, 4), np.float32), 4: ((self.H, self.W, 4), np.float32),
+                  5: ((nv, 2), np.int16), 7: ((H, W), np.float32), 8: ((self.H, self.W, 4), np.uint8),
+                  9: ((nv, 4), np.uint8)}
+        shape, dt = shapes[what]
+        out = np.zeros(shape, dt)
+        check(lib().nui_debug_download(self.h, what, level, ptr(out), out.nbytes))
+        return out
+
+    def volume_ref_layout(self):
+        """Volume as the reference stores it: short2 at ((x + y*rx)*rz + z)."""
+        return self.download(5)
+
+    def upload_volume(self, ref_short2):
+        a = np.ascontiguousarray(ref_short2, np.int16)
+        check(lib().nui_debug_upload_volume(self.h, ptr(a)))
+
+    def mesh(self, cap):
+        pos = np.zeros((cap, 3), np.float32)
+        col = np.zeros((cap, 4), np.float32)
+        n = C.c_uint64()
+        r = lib().nui_mesh(self.h, ptr(pos), ptr(col), cap, C.byref(n))
+        if r not in (NUI_OK, NUI_ERR_MESH_OVERFLOW):
+            check(r)
+        k = min(n.value, cap)
+        return pos[:k], col[:k], n.value
+
+
+# ------------------------------------------------------------------ synthetic input
+class SynthScene:
+    def __init__(self, kind=SYNTH_TABLETOP, seed=1, extent=3.0):
+        self.h = lib().nui_synth_scene_create(kind, seed, extent)
+        self.kind = kind
+        self.seed = seed
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().nui_synth_scene_destroy(self.h)
+        except Exception:
+            pass
+
+    def sdf(self, x, y, z):
+        return lib().nui_synth_scene_sdf(self.h, x, y, z)
+
+    def pose(self, frame, radius=1.5, deg_per_frame=2.0, traj_seed=None):
+        R = np.zeros(9, np.float32)
+        t = np.zeros(3, np.float32)
+        lib().nui_synth_trajectory(self.kind, self.seed if traj_seed is None else traj_seed, frame, radius,
+                                   deg_per_frame, ptr(R), ptr(t))
+        return R.reshape(3, 3), t
+
+    def render(self, R, t, W=640, H=480, fx=525.0, fy=525.0, cx=319.5, cy=239.5, noise_seed=7, frame=0,
+               noise=True, color=False):
+        d = np.zeros((H, W), np.uint16)
+        c = np.zeros((H, W, 4), np.uint8) if color else None
+        Rf = np.ascontiguousarray(R, np.float32).reshape(9)
+        tf = np.ascontiguousarray(t, np.float32).reshape(3)
+        lib().nui_synth_render(self.h, ptr(Rf), ptr(tf), W, H, fx, fy, cx, cy, noise_seed, frame, 1 if noise else 0,
+                               ptr(d), ptr(c))
+        return d, c

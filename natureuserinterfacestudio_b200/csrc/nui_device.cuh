@@ -1,0 +1,206 @@
+// Device-side types and helpers of the B200 KinectFusion path.
+//
+// The whole library is compiled with --fmad=false: every a*b+c in these kernels is a
+// rounded multiply followed by a rounded add, in the order written, which is what makes
+// the float results bit-identical to the CPU restatement of the reference kernels.
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nui {
+
+constexpr int kMaxLevels = 4;
+constexpr int kMaxRadius = 7;
+constexpr int kIcpTerms = 29;  // 21 JtJ + 6 Jtr + r^2 + count  (icp.cl:122-160)
+
+// Camera intrinsics block (gpu_def.h:13-27).
+struct DevCam {
+  float fx, fy, fx_inv, fy_inv, cx, cy;
+  int W, H;
+  float dmin, dmax;
+};
+
+// Rigid transform block (gpu_def.h:29-34): camera -> world rotation (row-major), its
+// inverse, camera centre.
+struct DevXform {
+  float R[9], R_inv[9], t[3];
+};
+
+// Per-session tracking state, resident in device memory and updated by the kernels.
+struct TrackState {
+  DevXform xf;           // camera pose of the current frame (prev frame's during ICP)
+  float R[9], t[3];      // ICP running estimate (Rcurr, tcurr)
+  float Rg[9], tg[3];    // last accepted estimate of the level (Rgood, tgood)
+  double good[27];       // accepted J^T J / J^T r sums
+  float lambda, err_old; // Levenberg-Marquardt state of the level
+  float error, count;    // NuiKinfuTracker::getError / getCount
+  int level_done;        // the level's iteration loop has stopped early
+  int status;            // 0 ok, 3 tracking lost
+  int integrate;         // integration gate of this frame
+  int iterations_run;
+  float lastR[9], lastT[3];  // pose of the last integration
+  unsigned int block_counter;
+  unsigned int pad_;
+  unsigned long long touched;
+};
+
+// What one session does in the current tick (host-written, read by every kernel).
+enum FrameKind : int { kInactive = -1, kFirstFrame = 0, kTrackFrame = 1 };
+
+struct SessionDesc {
+  int kind;  // FrameKind
+  int W, H, levels;
+  DevCam cam;
+  // preprocessing (NuiTrackerConfig)
+  int radius;
+  float sigma_depth, depth_thr;
+  float gauss[2 * kMaxRadius + 1];
+  // tracking
+  float dist_thr;
+  int iters[kMaxLevels];
+  unsigned int icp_min_count[kMaxLevels];
+  float integ_thr;
+  // frame buffers
+  const uint16_t* raw;
+  const uint8_t* bgra;
+  float* dscaled;                 // pass-filtered depth * ray scale (integration input)
+  float* dlev[kMaxLevels];        // depth pyramid (level 0 = bilateral output)
+  float4* vlev[kMaxLevels];       // camera-space vertex pyramid
+  float4* vref;                   // world-space reference vertex map (W x H)
+  float4* nref;                   // world-space reference normal map
+  uchar4* cmap;                   // reference colour map (nullable)
+  // dense volume
+  int fmt;                        // nui_tsdf_format
+  int res[3];
+  float dim[3], cell[3], trunc;
+  void* vol;                      // format storage, x-fastest: x + rx*(y + ry*z)
+  uint8_t* wvol;                  // weight plane of NUI_TSDF_F16_U8
+  uchar4* cvol;                   // colour volume (nullable), same layout
+  int max_cw;
+  int zchunks;                    // integration: z chunks per column (one thread each)
+  // tracking state and ICP scratch
+  TrackState* ts;
+  float2* partials;               // per-block (hi, lo) sums, kIcpTerms per block
+};
+
+// ------------------------------------------------------------------ float helpers
+__device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 add3(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 mul3(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ bool isnan3(float3 v) { return isnan(v.x) || isnan(v.y) || isnan(v.z); }
+// OpenCL normalize()/fast_normalize(): v / |v|, a zero vector is returned unchanged
+__device__ __forceinline__ float3 normalize3(float3 v) {
+  if (v.x == 0.f && v.y == 0.f && v.z == 0.f) return v;
+  float l = sqrtf(dot3(v, v));
+  return f3(v.x / l, v.y / l, v.z / l);
+}
+__device__ __forceinline__ float3 xyz(float4 v) { return f3(v.x, v.y, v.z); }
+__device__ __forceinline__ float4 w0(float3 v) { return make_float4(v.x, v.y, v.z, 0.f); }
+__device__ __forceinline__ float3 rot_rows(const float* M, float3 v) {
+  return f3(dot3(f3(M[0], M[1], M[2]), v), dot3(f3(M[3], M[4], M[5]), v), dot3(f3(M[6], M[7], M[8]), v));
+}
+__device__ __forceinline__ float qnan() { return __int_as_float(0x7fc00000); }
+
+// exp() of the bilateral filter.  Method: x = k ln2 + r with a two-constant Cody-Waite
+// split of ln2, exp(r) by Horner evaluation of the degree-7 Taylor polynomial
+// (|r| <= ln2/2, truncation error < 1e-8 relative), scaled by 2^k in two exact steps.
+// The CPU oracle implements the same method, so both round identically.
+__device__ __forceinline__ float nui_expf(float x) {
+  if (isnan(x)) return x;
+  if (x > 88.5f) return __int_as_float(0x7f800000);
+  if (x < -103.5f) return 0.f;
+  float kf = rintf(x * 1.44269504088896341f);
+  float r = x - kf * 0.693145751953125f;
+  r = r - kf * 1.42860682030941723e-6f;
+  float p = 1.98412698412698413e-4f;
+  p = p * r + 1.38888888888888889e-3f;
+  p = p * r + 8.33333333333333333e-3f;
+  p = p * r + 4.16666666666666667e-2f;
+  p = p * r + 1.66666666666666667e-1f;
+  p = p * r + 0.5f;
+  p = p * r + 1.0f;
+  p = p * r + 1.0f;
+  int k = (int)kf;
+  int k1 = k / 2, k2 = k - k1;
+  float s1 = __int_as_float((k1 + 127) << 23), s2 = __int_as_float((k2 + 127) << 23);
+  return (p * s1) * s2;
+}
+
+// ------------------------------------------------------------------ voxel formats
+// Each format exposes read(idx, F, W) -> true if W > 0, and write(idx, F, W).
+template <int FMT>
+struct Voxel;
+
+template <>
+struct Voxel<0> {  // NUI_TSDF_I16: short2, F = tsdf * 32766 truncated (utils.cl:69-79)
+  static constexpr int kBytes = 4;
+  __device__ static __forceinline__ void load(const SessionDesc& s, size_t i, float& F, int& W) {
+    short2 v = reinterpret_cast<const short2*>(s.vol)[i];
+    F = (float)v.x / 32766.f;
+    W = v.y;
+  }
+  __device__ static __forceinline__ void store(const SessionDesc& s, size_t i, float F, int W) {
+    reinterpret_cast<short2*>(s.vol)[i] = make_short2((short)__float2int_rz(F * 32766.f), (short)W);
+  }
+  __device__ static __forceinline__ void init(const SessionDesc& s, size_t i) {
+    reinterpret_cast<short2*>(s.vol)[i] = make_short2(32767, 0);
+  }
+};
+template <>
+struct Voxel<1> {  // NUI_TSDF_F32: float2 (tsdf, weight)
+  static constexpr int kBytes = 8;
+  __device__ static __forceinline__ void load(const SessionDesc& s, size_t i, float& F, int& W) {
+    float2 v = reinterpret_cast<const float2*>(s.vol)[i];
+    F = v.x;
+    W = (int)v.y;
+  }
+  __device__ static __forceinline__ void store(const SessionDesc& s, size_t i, float F, int W) {
+    reinterpret_cast<float2*>(s.vol)[i] = make_float2(F, (float)W);
+  }
+  __device__ static __forceinline__ void init(const SessionDesc& s, size_t i) {
+    reinterpret_cast<float2*>(s.vol)[i] = make_float2(1.f, 0.f);
+  }
+};
+template <>
+struct Voxel<2> {  // NUI_TSDF_F16_U8: half tsdf plane + uint8 weight plane
+  static constexpr int kBytes = 3;
+  __device__ static __forceinline__ void load(const SessionDesc& s, size_t i, float& F, int& W) {
+    F = __half2float(reinterpret_cast<const __half*>(s.vol)[i]);
+    W = s.wvol[i];
+  }
+  __device__ static __forceinline__ void store(const SessionDesc& s, size_t i, float F, int W) {
+    reinterpret_cast<__half*>(s.vol)[i] = __float2half_rn(F);
+    s.wvol[i] = (uint8_t)W;
+  }
+  __device__ static __forceinline__ void init(const SessionDesc& s, size_t i) {
+    reinterpret_cast<__half*>(s.vol)[i] = __float2half_rn(1.f);
+    s.wvol[i] = 0;
+  }
+};
+template <>
+struct Voxel<3> {  // NUI_TSDF_F16_F16: half2 (tsdf, weight)
+  static constexpr int kBytes = 4;
+  __device__ static __forceinline__ void load(const SessionDesc& s, size_t i, float& F, int& W) {
+    __half2 v = reinterpret_cast<const __half2*>(s.vol)[i];
+    F = __low2float(v);
+    W = (int)__high2float(v);
+  }
+  __device__ static __forceinline__ void store(const SessionDesc& s, size_t i, float F, int W) {
+    reinterpret_cast<__half2*>(s.vol)[i] = __floats2half2_rn(F, (float)W);
+  }
+  __device__ static __forceinline__ void init(const SessionDesc& s, size_t i) {
+    reinterpret_cast<__half2*>(s.vol)[i] = __floats2half2_rn(1.f, 0.f);
+  }
+};
+
+__device__ __forceinline__ size_t vox_index(const SessionDesc& s, int x, int y, int z) {
+  return (size_t)x + (size_t)s.res[0] * ((size_t)y + (size_t)s.res[1] * (size_t)z);
+}
+
+}  // namespace nui

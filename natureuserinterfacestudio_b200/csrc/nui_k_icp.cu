@@ -1,0 +1,365 @@
+// Point-to-plane ICP, one launch per iteration, no host round trip.
+//
+// Per pixel (icp_block_kernel, icp.cl:222-292): transform the level's vertex by the running
+// estimate, project into the previous camera with full-resolution intrinsics, bilinearly
+// sample the world reference normal and vertex (icp.cl:192-220; a tap NaN -> no match), and
+// if |q - p| < distThres form the row [n x p, n | n.(q - p)].  Each thread accumulates the
+// 29 products of its pixels; blocks reduce them with warp shuffles and shared memory, all as
+// (hi, lo) two-sum pairs in FP32; the last block to finish (ticket on an atomic counter)
+// adds the per-block pairs in double in a fixed order and runs the host step of
+// NuiKinfuOpenCLDepthTracker::IterativeClosestPoint (NuiKinfuOpenCLDepthTracker.cpp:324-496):
+// Levenberg-Marquardt accept/reject, FP64 determinant check and Cholesky solve, ZYX Euler
+// increment composed in FP64.  The next launch reads the updated estimate.
+#include "nui_device.cuh"
+
+namespace nui {
+
+constexpr int kIcpThreads = 256;
+constexpr int kIcpPixPerThread = 4;
+
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+  s = a + b;
+  float bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+// (h1, l1) += (h2, l2)
+__device__ __forceinline__ void acc_pair(float& h1, float& l1, float h2, float l2) {
+  float s, e;
+  two_sum(h1, h2, s, e);
+  h1 = s;
+  l1 = (l1 + l2) + e;
+}
+
+// Bilinear sample with holes; taps whose linear index falls past the map read as holes.
+__device__ __forceinline__ float3 bilinear_holes(const float4* __restrict__ src, float px, float py, int W,
+                                                 int N) {
+  const int ix = (int)floorf(px), iy = (int)floorf(py);
+  const float dx = px - (float)ix, dy = py - (float)iy;
+  const int ia = ix + iy * W, ib = (ix + 1) + iy * W, ic = ix + (iy + 1) * W, id = (ix + 1) + (iy + 1) * W;
+  if (id >= N || ic >= N || ib >= N) return f3(qnan(), qnan(), qnan());
+  const float3 a = xyz(__ldg(src + ia)), b = xyz(__ldg(src + ib)), c = xyz(__ldg(src + ic)),
+               d = xyz(__ldg(src + id));
+  if (isnan3(a) || isnan3(b) || isnan3(c) || isnan3(d)) return f3(qnan(), qnan(), qnan());
+  const float ex = 1.0f - dx, ey = 1.0f - dy;
+  float3 r;
+  r.x = a.x * ex * ey + b.x * dx * ey + c.x * ex * dy + d.x * dx * dy;
+  r.y = a.y * ex * ey + b.y * dx * ey + c.y * ex * dy + d.y * dx * dy;
+  r.z = a.z * ex * ey + b.z * dx * ey + c.z * ex * dy + d.z * dx * dy;
+  return r;
+}
+
+// ---------------------------------------------------------------- FP64 host step
+__device__ double det6(double* A) {
+  double det = 1.0;
+  for (int c = 0; c < 6; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < 6; ++r)
+      if (fabs(A[r * 6 + c]) > fabs(A[piv * 6 + c])) piv = r;
+    if (A[piv * 6 + c] == 0.0) return 0.0;
+    if (piv != c) {
+      for (int k = 0; k < 6; ++k) {
+        double t = A[c * 6 + k];
+        A[c * 6 + k] = A[piv * 6 + k];
+        A[piv * 6 + k] = t;
+      }
+      det = -det;
+    }
+    det *= A[c * 6 + c];
+    for (int r = c + 1; r < 6; ++r) {
+      double f = A[r * 6 + c] / A[c * 6 + c];
+      for (int k = c; k < 6; ++k) A[r * 6 + k] -= f * A[c * 6 + k];
+    }
+  }
+  return det;
+}
+
+__device__ bool llt_solve6(const double* A, const double* b, double* x) {
+  double L[36];
+  for (int i = 0; i < 36; ++i) L[i] = 0.0;
+  for (int j = 0; j < 6; ++j) {
+    double s = A[j * 6 + j];
+    for (int k = 0; k < j; ++k) s -= L[j * 6 + k] * L[j * 6 + k];
+    if (!(s > 0.0)) return false;
+    L[j * 6 + j] = sqrt(s);
+    for (int i = j + 1; i < 6; ++i) {
+      double t = A[i * 6 + j];
+      for (int k = 0; k < j; ++k) t -= L[i * 6 + k] * L[j * 6 + k];
+      L[i * 6 + j] = t / L[j * 6 + j];
+    }
+  }
+  double y[6];
+  for (int i = 0; i < 6; ++i) {
+    double t = b[i];
+    for (int k = 0; k < i; ++k) t -= L[i * 6 + k] * y[k];
+    y[i] = t / L[i * 6 + i];
+  }
+  for (int i = 5; i >= 0; --i) {
+    double t = y[i];
+    for (int k = i + 1; k < 6; ++k) t -= L[k * 6 + i] * x[k];
+    x[i] = t / L[i * 6 + i];
+  }
+  return true;
+}
+
+// Rz(g) Ry(b) Rx(a) (AngleAxis composition at NuiKinfuOpenCLDepthTracker.cpp:486)
+__device__ void euler_zyx(double a, double b, double g, double* R) {
+  double ca = cos(a), sa = sin(a), cb = cos(b), sb = sin(b), cg = cos(g), sg = sin(g);
+  double Rz[9] = {cg, -sg, 0, sg, cg, 0, 0, 0, 1};
+  double Ry[9] = {cb, 0, sb, 0, 1, 0, -sb, 0, cb};
+  double Rx[9] = {1, 0, 0, 0, ca, -sa, 0, sa, ca};
+  double T[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += Rz[i * 3 + k] * Ry[k * 3 + j];
+      T[i * 3 + j] = s;
+    }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += T[i * 3 + k] * Rx[k * 3 + j];
+      R[i * 3 + j] = s;
+    }
+}
+
+// LM step on the reduced sums (runs on one thread of the last block).
+__device__ void icp_host_step(TrackState* ts, const double* sums, int iter, unsigned min_count) {
+  float err = (float)sums[27];
+  const float cnt = (float)sums[28];
+  err = (cnt > 0.f) ? sqrtf(err) / cnt : 3.402823466e+38f;
+  ts->error = err;
+  ts->count = cnt;
+  ts->iterations_run += 1;
+  if (iter == 0) {  // level start: lambda = 1, Rgood = Rcurr, errorOld = 1e20
+    ts->lambda = 1.0f;
+    for (int i = 0; i < 9; ++i) ts->Rg[i] = ts->R[i];
+    for (int i = 0; i < 3; ++i) ts->tg[i] = ts->t[i];
+    ts->err_old = 1e20f;
+    ts->level_done = 0;
+  }
+  if (cnt < (float)min_count || err > ts->err_old) {
+    ts->lambda *= 10.0f;
+    for (int i = 0; i < 9; ++i) ts->R[i] = ts->Rg[i];
+    for (int i = 0; i < 3; ++i) ts->t[i] = ts->tg[i];
+    if (iter == 0) {
+      ts->level_done = 1;
+      return;
+    }
+  } else {
+    ts->lambda /= 10.0f;
+    for (int i = 0; i < 9; ++i) ts->Rg[i] = ts->R[i];
+    for (int i = 0; i < 3; ++i) ts->tg[i] = ts->t[i];
+    ts->err_old = err;
+    for (int k = 0; k < 27; ++k) ts->good[k] = sums[k];
+  }
+  double A[36], b[6], Ac[36];
+  for (int i = 0, sh = 0; i < 6; ++i) {
+    for (int j = i; j < 7; ++j, ++sh) {
+      double v = ts->good[sh] / (double)cnt;
+      if (j == 6)
+        b[i] = v;
+      else
+        A[j * 6 + i] = A[i * 6 + j] = v;
+    }
+    A[i * 6 + i] *= (double)(1.0f + ts->lambda);
+  }
+  for (int i = 0; i < 36; ++i) Ac[i] = A[i];
+  const double det = det6(Ac);
+  double x[6];
+  if (fabs(det) < 1e-15 || isnan(det) || !llt_solve6(A, b, x)) {
+    ts->status = 3;
+    return;
+  }
+  const float al = (float)x[0], be = (float)x[1], ga = (float)x[2];
+  if (al * al + be * be + ga * ga < 1e-6f) {
+    ts->level_done = 1;
+    return;
+  }
+  double Ri[9];
+  euler_zyx(al, be, ga, Ri);
+  double tn[3], Rn[9];
+  for (int i = 0; i < 3; ++i) {
+    double s = 0;
+    for (int k = 0; k < 3; ++k) s += Ri[k * 3 + i] * (double)ts->t[k];
+    tn[i] = s + (double)(float)x[3 + i];
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += Ri[k * 3 + i] * (double)ts->R[k * 3 + j];
+      Rn[i * 3 + j] = s;
+    }
+  for (int i = 0; i < 3; ++i) ts->t[i] = (float)tn[i];
+  for (int i = 0; i < 9; ++i) ts->R[i] = (float)Rn[i];
+}
+
+__global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restrict__ descs, int level, int iter) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (s.kind != kTrackFrame || level >= s.levels || iter >= s.iters[level]) return;
+  TrackState* ts = s.ts;
+  if (ts->status != 0) return;
+  if (iter > 0 && ts->level_done) return;
+  const int w = s.W >> level, h = s.H >> level, n = w * h;
+  const int per_block = kIcpThreads * kIcpPixPerThread;
+  const int nblocks = (n + per_block - 1) / per_block;
+  if ((int)blockIdx.x >= nblocks) return;
+
+  __shared__ float sR[9], st[3];
+  __shared__ DevXform sp;
+  if (threadIdx.x < 9) sR[threadIdx.x] = ts->R[threadIdx.x];
+  if (threadIdx.x < 3) st[threadIdx.x] = ts->t[threadIdx.x];
+  if (threadIdx.x < 21) reinterpret_cast<float*>(&sp)[threadIdx.x] = reinterpret_cast<const float*>(&ts->xf)[threadIdx.x];
+  __syncthreads();
+
+  float hi[kIcpTerms], lo[kIcpTerms];
+#pragma unroll
+  for (int k = 0; k < kIcpTerms; ++k) hi[k] = lo[k] = 0.f;
+
+  const float4* __restrict__ V = s.vlev[level];
+  const float fx = s.cam.fx, fy = s.cam.fy, cx = s.cam.cx, cy = s.cam.cy;
+  const int RW = s.W, RN = s.W * s.H;
+  const float fW = (float)s.W, fH = (float)s.H;
+  const float3 tc = f3(st[0], st[1], st[2]), tp = f3(sp.t[0], sp.t[1], sp.t[2]);
+  const int base = blockIdx.x * per_block;
+#pragma unroll 1
+  for (int k = 0; k < kIcpPixPerThread; ++k) {
+    const int i = base + k * kIcpThreads + threadIdx.x;
+    if (i >= n) break;
+    const float3 v = xyz(__ldg(V + i));
+    if (isnan3(v)) continue;
+    const float3 pv = add3(rot_rows(sR, v), tc);
+    const float3 pp = rot_rows(sp.R_inv, sub3(pv, tp));
+    const float u = pp.x * fx / pp.z + cx;
+    const float vv = pp.y * fy / pp.z + cy;
+    if (!(u >= 0.0f && u < fW && vv >= 0.0f && vv < fH)) continue;
+    const float3 rn = bilinear_holes(s.nref, u, vv, RW, RN);
+    if (isnan3(rn)) continue;
+    const float3 rv = bilinear_holes(s.vref, u, vv, RW, RN);
+    if (isnan3(rv)) continue;
+    const float3 diff = sub3(rv, pv);
+    const float dist = sqrtf(dot3(diff, diff));
+    if (!(dist < s.dist_thr)) continue;
+    const float3 r0 = cross3(rn, pv);
+    const float c7[7] = {r0.x, r0.y, r0.z, rn.x, rn.y, rn.z, dot3(rn, diff)};
+    int sh = 0;
+#pragma unroll
+    for (int a = 0; a < 6; ++a)
+#pragma unroll
+      for (int b = a; b < 7; ++b, ++sh) {
+        float ss, e;
+        two_sum(hi[sh], c7[a] * c7[b], ss, e);
+        hi[sh] = ss;
+        lo[sh] += e;
+      }
+    {
+      float ss, e;
+      two_sum(hi[27], c7[6] * c7[6], ss, e);
+      hi[27] = ss;
+      lo[27] += e;
+    }
+    hi[28] += 1.0f;
+  }
+
+  // warp reduction of the (hi, lo) pairs
+#pragma unroll
+  for (int k = 0; k < kIcpTerms; ++k) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      float h2 = __shfl_down_sync(0xffffffffu, hi[k], off);
+      float l2 = __shfl_down_sync(0xffffffffu, lo[k], off);
+      acc_pair(hi[k], lo[k], h2, l2);
+    }
+  }
+  constexpr int kWarps = kIcpThreads / 32;
+  __shared__ float2 wsum[kWarps][kIcpTerms];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < kIcpTerms; ++k) wsum[warp][k] = make_float2(hi[k], lo[k]);
+  }
+  __syncthreads();
+  if (threadIdx.x < kIcpTerms) {
+    float H = 0.f, L = 0.f;
+    for (int wi = 0; wi < kWarps; ++wi) acc_pair(H, L, wsum[wi][threadIdx.x].x, wsum[wi][threadIdx.x].y);
+    s.partials[(size_t)blockIdx.x * kIcpTerms + threadIdx.x] = make_float2(H, L);
+  }
+  __threadfence();
+  __shared__ unsigned int ticket;
+  __syncthreads();
+  if (threadIdx.x == 0) ticket = atomicAdd(&ts->block_counter, 1u);
+  __syncthreads();
+  if (ticket != (unsigned)nblocks - 1) return;
+
+  // last block: fixed-order double reduction of the per-block pairs
+  __threadfence();
+  __shared__ double red[kWarps][32];
+  {
+    const int k = lane;  // term index handled by this lane
+    double acc = 0.0;
+    if (k < kIcpTerms)
+      for (int b = warp; b < nblocks; b += kWarps) {
+        float2 p = __ldcg(&s.partials[(size_t)b * kIcpTerms + k]);
+        acc += (double)p.x + (double)p.y;
+      }
+    red[warp][lane] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sums[kIcpTerms];
+    for (int k = 0; k < kIcpTerms; ++k) {
+      double a = 0.0;
+      for (int wi = 0; wi < kWarps; ++wi) a += red[wi][k];
+      sums[k] = a;
+    }
+    icp_host_step(ts, sums, iter, s.icp_min_count[level]);
+    ts->block_counter = 0;
+    __threadfence();
+  }
+}
+
+// After the last ICP launch (or on frame 0): publish the pose, decide the integration
+// gate (NuiKinfuTrackingEngine.cpp:115-127) and reset the estimate for the next frame.
+__global__ void k_track_finalize(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.x];
+  if (threadIdx.x != 0 || s.kind < 0) return;
+  TrackState* ts = s.ts;
+  ts->touched = 0ull;
+  if (s.kind == kFirstFrame) {
+    ts->integrate = ts->status == 0 ? 1 : 0;
+    return;
+  }
+  if (ts->status != 0) {  // tracking lost: keep the previous pose, skip the rest
+    for (int i = 0; i < 9; ++i) ts->R[i] = ts->xf.R[i];
+    for (int i = 0; i < 3; ++i) ts->t[i] = ts->xf.t[i];
+    ts->integrate = 0;
+    return;
+  }
+  double a[9];
+  for (int i = 0; i < 9; ++i) a[i] = ts->R[i];
+  const double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+  const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+  const double inv[9] = {c00, a[2] * a[7] - a[1] * a[8], a[1] * a[5] - a[2] * a[4],
+                         c01, a[0] * a[8] - a[2] * a[6], a[2] * a[3] - a[0] * a[5],
+                         c02, a[1] * a[6] - a[0] * a[7], a[0] * a[4] - a[1] * a[3]};
+  for (int i = 0; i < 9; ++i) {
+    ts->xf.R[i] = ts->R[i];
+    ts->xf.R_inv[i] = (float)(inv[i] / det);
+  }
+  for (int i = 0; i < 3; ++i) ts->xf.t[i] = ts->t[i];
+  // rotation angle of R^-1 * R_last and translation distance
+  double tr = 0;
+  for (int i = 0; i < 3; ++i)
+    for (int k = 0; k < 3; ++k) tr += (double)ts->R[k * 3 + i] * (double)ts->lastR[k * 3 + i];
+  const double cv = fmin(1.0, fmax(-1.0, (tr - 1.0) / 2.0));
+  const double rn = acos(cv);
+  double tn = 0;
+  for (int i = 0; i < 3; ++i) tn += ((double)ts->t[i] - ts->lastT[i]) * ((double)ts->t[i] - ts->lastT[i]);
+  tn = sqrt(tn);
+  ts->integrate = ((float)((rn + tn) / 2) >= s.integ_thr) ? 1 : 0;
+  if (ts->integrate) {
+    for (int i = 0; i < 9; ++i) ts->lastR[i] = ts->R[i];
+    for (int i = 0; i < 3; ++i) ts->lastT[i] = ts->t[i];
+  }
+}
+
+}  // namespace nui

@@ -1,0 +1,149 @@
+// Frame preprocessing kernels.
+//
+//  k_preprocess   depth_passing_filter_kernel (filters.cl:9-23) + bilateral_filter_depth_kernel
+//                 (bilateralFilter.cl:68-119) + depth2vertex_kernel at level 0
+//                 (transformMaps.cl:18-42) + scaleDepthsKernel (tsdfVolume.cl:8-29), fused.
+//                 One block per 32x8 output tile; the pass-filtered depth of the tile and
+//                 its radius-r halo is staged in shared memory once and read 49 times.
+//  k_pyramid      half_sample_kernel (transformMaps.cl:44-88) + depth2vertex_kernel for one
+//                 pyramid level.
+//  k_feedback     estimate_normals_simple_kernel (normalEstimation.cl:770-822) +
+//                 transform_maps_kernel (transformMaps.cl:91-127): frame-0 reference maps.
+//
+// Out-of-image taps are staged as NaN; the reference clamps its loops to the image
+// instead, and since NaN taps are skipped the accumulated sequence is the same.
+#include "nui_device.cuh"
+
+namespace nui {
+
+constexpr int kPreTX = 32, kPreTY = 8;
+
+__global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (s.kind < 0) return;
+  const int W = s.W, H = s.H, R = s.radius;
+  const int tilesX = (W + kPreTX - 1) / kPreTX;
+  const int tx0 = (blockIdx.x % tilesX) * kPreTX, ty0 = (blockIdx.x / tilesX) * kPreTY;
+  if (ty0 >= H) return;
+  constexpr int SW = kPreTX + 2 * kMaxRadius, SH = kPreTY + 2 * kMaxRadius;
+  __shared__ float tile[SH][SW];
+  __shared__ float gs[2 * kMaxRadius + 1];
+  const int tid = threadIdx.y * kPreTX + threadIdx.x;
+  if (tid < 2 * R + 1) gs[tid] = s.gauss[tid];
+  const float dmin = s.cam.dmin, dmax = s.cam.dmax;
+  const int sw = kPreTX + 2 * R, sh = kPreTY + 2 * R;
+  for (int i = tid; i < sw * sh; i += kPreTX * kPreTY) {
+    int ly = i / sw, lx = i - ly * sw;
+    int gx = tx0 - R + lx, gy = ty0 - R + ly;
+    float d = qnan();
+    if (gx >= 0 && gy >= 0 && gx < W && gy < H) {
+      float dp = (float)s.raw[(size_t)gy * W + gx] * 0.001f;
+      if (dp > dmin && dp < dmax) d = dp;
+    }
+    tile[ly][lx] = d;
+  }
+  __syncthreads();
+  const int x = tx0 + threadIdx.x, y = ty0 + threadIdx.y;
+  if (x >= W || y >= H) return;
+  const float c = tile[threadIdx.y + R][threadIdx.x + R];
+  float out = qnan();
+  if (!isnan(c)) {
+    float sd = 0.f, swt = 0.f;
+    const float thr = s.depth_thr, sig = s.sigma_depth;
+    for (int dy = 0; dy <= 2 * R; ++dy) {
+      const float gy = gs[dy];
+      for (int dx = 0; dx <= 2 * R; ++dx) {
+        float nr = tile[threadIdx.y + dy][threadIdx.x + dx];
+        if (isnan(nr)) continue;
+        float diff = fabsf(c - nr);
+        if (nr > 0.0f && diff < thr) {
+          float d2 = diff * diff;
+          float w = gs[dx] * gy * nui_expf(-(d2 * sig));
+          sd += nr * w;
+          swt += w;
+        }
+      }
+    }
+    out = sd / swt;
+  }
+  const size_t i = (size_t)y * W + x;
+  s.dlev[0][i] = out;
+  const float xl = ((float)x - s.cam.cx) * s.cam.fx_inv;
+  const float yl = ((float)y - s.cam.cy) * s.cam.fy_inv;
+  float4 v = make_float4(qnan(), qnan(), qnan(), 0.f);
+  if (!isnan(out)) v = make_float4(out * xl, out * yl, out * 1.0f, 0.f);
+  s.vlev[0][i] = v;
+  // ray-length depth for integration: the pass-filtered depth, not the bilateral output
+  // (NuiKinfuOpenCLScene.cpp:218 passes GetDepthBuffer())
+  float sc = c;
+  if (!isnan(c)) sc = c * sqrtf(xl * xl + yl * yl + 1.f);
+  s.dscaled[i] = sc;
+}
+
+// One pyramid level: dst(x,y) = mean of the 3x3 taps around src(2x,2y) within the depth
+// threshold of the centre (any valid tap if the centre is NaN); vertices with div = 2^l.
+__global__ void k_pyramid(const SessionDesc* __restrict__ descs, int level) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (s.kind != kTrackFrame || level >= s.levels) return;
+  const int dW = s.W >> level, dH = s.H >> level, sW = dW * 2, sH = dH * 2;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= dW * dH) return;
+  const int x = idx % dW, y = idx / dW;
+  const float* src = s.dlev[level - 1];
+  const int sx = 2 * x, sy = 2 * y;
+  const float c = src[(size_t)sy * sW + sx];
+  const float thr = s.depth_thr;
+  float sum = 0.f;
+  int n = 0;
+  for (int cy = max(sy - 1, 0); cy < min(sy + 2, sH); ++cy)
+    for (int cx = max(sx - 1, 0); cx < min(sx + 2, sW); ++cx) {
+      float nr = src[(size_t)cy * sW + cx];
+      if (!isnan(nr) && (isnan(c) || fabsf(c - nr) < thr)) {
+        sum += nr;
+        n += 1;
+      }
+    }
+  const float d = n > 0 ? sum / (float)n : qnan();
+  s.dlev[level][idx] = d;
+  const float div = (float)(1 << level);
+  const float fxi = div * s.cam.fx_inv, fyi = div * s.cam.fy_inv;
+  const float cxl = s.cam.cx / div, cyl = s.cam.cy / div;
+  float4 v = make_float4(qnan(), qnan(), qnan(), 0.f);
+  if (!isnan(d)) v = make_float4(d * (((float)x - cxl) * fxi), d * (((float)y - cyl) * fyi), d * 1.0f, 0.f);
+  s.vlev[level][idx] = v;
+}
+
+// Frame-0 reference maps: simple normals from the level-0 vertex map, then both maps to
+// world space with the current pose (NuiKinfuOpenCLFeedbackFrame::UpdateBuffers, :71-91).
+__global__ void k_feedback(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (s.kind != kFirstFrame) return;
+  const int W = s.W, H = s.H;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= W * H) return;
+  const int x = idx % W, y = idx / W;
+  const float4* V = s.vlev[0];
+  const float3 c = xyz(V[idx]);
+  const DevXform& m = s.ts->xf;
+  if (isnan3(c)) {
+    s.vref[idx] = make_float4(qnan(), qnan(), qnan(), 0.f);
+    s.nref[idx] = make_float4(qnan(), qnan(), qnan(), 0.f);
+    return;
+  }
+  const float thr = s.depth_thr;
+  auto pick = [&](bool ok, int j) {
+    if (!ok) return c;
+    float3 q = xyz(V[j]);
+    if (isnan3(q) || fabsf(c.z - q.z) > thr) return c;
+    return q;
+  };
+  const float3 l = pick(x > 0, idx - 1), r = pick(x < W - 1, idx + 1);
+  const float3 u = pick(y > 0, idx - W), d = pick(y < H - 1, idx + W);
+  const float3 n = normalize3(cross3(sub3(r, l), sub3(d, u)));
+  const float3 vw = add3(rot_rows(m.R, c), f3(m.t[0], m.t[1], m.t[2]));
+  s.vref[idx] = w0(vw);
+  s.nref[idx] = isnan3(n) ? make_float4(qnan(), qnan(), qnan(), 0.f) : w0(rot_rows(m.R, n));
+  if (s.cmap) s.cmap[idx] = s.bgra ? reinterpret_cast<const uchar4*>(s.bgra)[idx] : make_uchar4(0, 0, 0, 0);
+}
+
+}  // namespace nui

@@ -1,0 +1,157 @@
+// Dense TSDF integration (integrateTsdfVolumeKernel, tsdfVolume.cl:31-190) and volume reset
+// (initializeVolume, tsdfVolume.cl:192-211).
+//
+// Layout: voxel (x, y, z) at x + rx*(y + ry*z), so the 32 lanes of a warp (consecutive x)
+// touch one contiguous 128-256 B run of each z slice: every access is coalesced.  The
+// reference keeps z fastest and loops z inside a thread, which strides a warp by rz voxels.
+//
+// Arithmetic: the reference advances the camera-space coordinates of a column
+// incrementally along z (v_x += R_inv[2]*cell*fx, ...); rounding of that running sum
+// decides which pixel a voxel projects to, so each thread replays the same additions.
+// A thread owns one column and one chunk of z: it first replays the additions of the
+// z values below its chunk (4 float adds per slice, no memory traffic), then integrates
+// its chunk, evaluating the projections of kZUnroll slices before it issues their loads
+// so that several voxel reads are in flight per thread.
+#include "nui_device.cuh"
+
+namespace nui {
+
+constexpr int kTsdfThreads = 256;
+constexpr int kZUnroll = 4;
+
+template <int FMT>
+__global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (s.kind < 0 || s.fmt != FMT || !s.ts->integrate) return;
+  const int rx = s.res[0], ry = s.res[1], rz = s.res[2];
+  const int zchunks = s.zchunks;
+  const long ncol = (long)rx * ry;
+  const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= ncol * zchunks) return;
+  const int chunk = (int)(tid / ncol);
+  const long col = tid - (long)chunk * ncol;
+  const int vx = (int)(col % rx), vy = (int)(col / rx);
+  const int zlen = (rz + zchunks - 1) / zchunks;
+  const int z0 = chunk * zlen, z1 = min(rz, z0 + zlen);
+
+  const DevXform& m = s.ts->xf;
+  const float* Ri = m.R_inv;
+  const float c0 = s.cell[0], c1 = s.cell[1], c2 = s.cell[2];
+  const float vgx = ((float)(vx - rx / 2) + 0.5f) * c0 - m.t[0];
+  const float vgy = ((float)(vy - ry / 2) + 0.5f) * c1 - m.t[1];
+  float vgz = (0.5f) * c2 - m.t[2];
+  const float part = vgx * vgx + vgy * vgy;
+  const float fx = s.cam.fx, fy = s.cam.fy, ccx = s.cam.cx, ccy = s.cam.cy;
+  float v_x = (Ri[0] * vgx + Ri[1] * vgy + Ri[2] * vgz) * fx;
+  float v_y = (Ri[3] * vgx + Ri[4] * vgy + Ri[5] * vgz) * fy;
+  const float v_z = (Ri[6] * vgx + Ri[7] * vgy + Ri[8] * vgz);
+  float zs = 0.f;
+  const float trunc = s.trunc;
+  const float tinv = 1.f / trunc;
+  const float dx = Ri[2] * c2 * fx;
+  const float dy = Ri[5] * c2 * fy;
+  const float r8 = Ri[8];
+  for (int z = 0; z < z0; ++z) {
+    vgz += c2;
+    zs += c2;
+    v_x += dx;
+    v_y += dy;
+  }
+  const int W = s.W, H = s.H;
+  const float fW = (float)W, fH = (float)H;
+  const float* __restrict__ depth = s.dscaled;
+  const size_t slice = (size_t)rx * ry;
+  size_t idx = (size_t)vx + (size_t)rx * vy + slice * (size_t)z0;
+  unsigned int touched = 0;
+
+  for (int zb = z0; zb < z1; zb += kZUnroll) {
+    float sdf[kZUnroll];
+    int pix[kZUnroll];
+    bool ok[kZUnroll];
+#pragma unroll
+    for (int u = 0; u < kZUnroll; ++u) {
+      ok[u] = false;
+      pix[u] = 0;
+      sdf[u] = 0.f;
+      if (zb + u < z1) {
+        const float inv_z = 1.0f / (v_z + r8 * zs);
+        if (!(inv_z < 0.f)) {
+          const float px = roundf(v_x * inv_z + ccx);
+          const float py = roundf(v_y * inv_z + ccy);
+          if (px >= 0.f && py >= 0.f && px < fW && py < fH) {
+            const int p = (int)py * W + (int)px;
+            const float Dp = __ldg(depth + p);
+            const float sd = Dp - sqrtf(vgz * vgz + part);
+            if (!isnan(Dp) && sd >= -trunc) {
+              ok[u] = true;
+              sdf[u] = sd;
+              pix[u] = p;
+            }
+          }
+        }
+        vgz += c2;
+        zs += c2;
+        v_x += dx;
+        v_y += dy;
+      }
+    }
+    float F[kZUnroll];
+    int Wt[kZUnroll];
+#pragma unroll
+    for (int u = 0; u < kZUnroll; ++u)
+      if (ok[u]) Voxel<FMT>::load(s, idx + (size_t)u * slice, F[u], Wt[u]);
+#pragma unroll
+    for (int u = 0; u < kZUnroll; ++u) {
+      if (!ok[u]) continue;
+      const float tsdf = fminf(1.0f, sdf[u] * tinv);
+      const float tn = (F[u] * (float)Wt[u] + tsdf) / (float)(Wt[u] + 1);
+      const int wn = min(Wt[u] + 1, 128);
+      const size_t vi = idx + (size_t)u * slice;
+      Voxel<FMT>::store(s, vi, tn, wn);
+      ++touched;
+      if (s.cvol && s.bgra && fabsf(sdf[u]) < trunc) {
+        const uchar4 nc = reinterpret_cast<const uchar4*>(s.bgra)[pix[u]];
+        if (nc.w != 0) {
+          const uchar4 vc = s.cvol[vi];
+          const float wr = 1.f;
+          const float nx = ((float)(vc.x * vc.w) + wr * (float)nc.x) / ((float)vc.w + wr);
+          const float ny = ((float)(vc.y * vc.w) + wr * (float)nc.y) / ((float)vc.w + wr);
+          const float nz = ((float)(vc.z * vc.w) + wr * (float)nc.z) / ((float)vc.w + wr);
+          const unsigned char wnew = (unsigned char)(vc.w + 1);
+          uchar4 o;
+          o.x = (unsigned char)fminf(fmaxf(nx, 0.f), 255.f);
+          o.y = (unsigned char)fminf(fmaxf(ny, 0.f), 255.f);
+          o.z = (unsigned char)fminf(fmaxf(nz, 0.f), 255.f);
+          o.w = min((unsigned char)s.max_cw, wnew);
+          s.cvol[vi] = o;
+        }
+      }
+    }
+    idx += (size_t)kZUnroll * slice;
+  }
+  // warp-aggregated count of voxels read-modify-written
+  const unsigned int mask = __activemask();
+  const unsigned int t = __reduce_add_sync(mask, touched);
+  if ((int)(threadIdx.x & 31) == __ffs(mask) - 1 && t) atomicAdd(&s.ts->touched, (unsigned long long)t);
+}
+
+template <int FMT>
+__global__ void k_volume_init(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  const size_t n = (size_t)s.res[0] * s.res[1] * s.res[2];
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    Voxel<FMT>::init(s, i);
+    if (s.cvol) s.cvol[i] = make_uchar4(0, 0, 0, 0);
+  }
+}
+
+template __global__ void k_integrate<0>(const SessionDesc*);
+template __global__ void k_integrate<1>(const SessionDesc*);
+template __global__ void k_integrate<2>(const SessionDesc*);
+template __global__ void k_integrate<3>(const SessionDesc*);
+template __global__ void k_volume_init<0>(const SessionDesc*);
+template __global__ void k_volume_init<1>(const SessionDesc*);
+template __global__ void k_volume_init<2>(const SessionDesc*);
+template __global__ void k_volume_init<3>(const SessionDesc*);
+
+}  // namespace nui

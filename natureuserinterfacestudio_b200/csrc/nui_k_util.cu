@@ -1,0 +1,73 @@
+// Small utility kernels: per-session result publication and conversion between the
+// session volume layout and the reference layout ((x + y*rx)*rz + z, short2).
+#include "nui_device.cuh"
+
+namespace nui {
+
+// One thread per session: status, gate and pose of this tick into a packed array that
+// the host reads back with one copy.
+__global__ void k_publish(const SessionDesc* __restrict__ descs, int n, float* pose, int* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !pose || !status) return;
+  const SessionDesc& s = descs[i];
+  if (s.ts == nullptr) return;
+  const TrackState* ts = s.ts;
+  status[2 * i] = s.kind < 0 ? 0 : ts->status;
+  status[2 * i + 1] = ts->integrate;
+  for (int k = 0; k < 9; ++k) pose[14 * i + k] = ts->xf.R[k];
+  for (int k = 0; k < 3; ++k) pose[14 * i + 9 + k] = ts->xf.t[k];
+  pose[14 * i + 12] = ts->error;
+  pose[14 * i + 13] = ts->count;
+}
+
+template <int FMT>
+__global__ void k_export_ref(const SessionDesc* __restrict__ descs, short2* out, uchar4* cout) {
+  const SessionDesc& s = descs[0];
+  const int rx = s.res[0], ry = s.res[1], rz = s.res[2];
+  const size_t n = (size_t)rx * ry * rz;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % rx);
+    const int y = (int)((i / rx) % ry);
+    const int z = (int)(i / ((size_t)rx * ry));
+    const size_t o = ((size_t)x + (size_t)y * rx) * rz + z;
+    if (out) {
+      if (FMT == 0) {
+        out[o] = reinterpret_cast<const short2*>(s.vol)[i];
+      } else {
+        float F;
+        int W;
+        Voxel<FMT>::load(s, i, F, W);
+        out[o] = make_short2((short)__float2int_rz(F * 32766.f), (short)W);
+      }
+    }
+    if (cout && s.cvol) cout[o] = s.cvol[i];
+  }
+}
+
+template <int FMT>
+__global__ void k_import_ref(const SessionDesc* __restrict__ descs, const short2* in) {
+  const SessionDesc& s = descs[0];
+  const int rx = s.res[0], ry = s.res[1], rz = s.res[2];
+  const size_t n = (size_t)rx * ry * rz;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % rx);
+    const int y = (int)((i / rx) % ry);
+    const int z = (int)(i / ((size_t)rx * ry));
+    const short2 v = in[((size_t)x + (size_t)y * rx) * rz + z];
+    if (FMT == 0)
+      reinterpret_cast<short2*>(s.vol)[i] = v;
+    else
+      Voxel<FMT>::store(s, i, (float)v.x / 32766.f, v.y);
+  }
+}
+
+template __global__ void k_export_ref<0>(const SessionDesc*, short2*, uchar4*);
+template __global__ void k_export_ref<1>(const SessionDesc*, short2*, uchar4*);
+template __global__ void k_export_ref<2>(const SessionDesc*, short2*, uchar4*);
+template __global__ void k_export_ref<3>(const SessionDesc*, short2*, uchar4*);
+template __global__ void k_import_ref<0>(const SessionDesc*, const short2*);
+template __global__ void k_import_ref<1>(const SessionDesc*, const short2*);
+template __global__ void k_import_ref<2>(const SessionDesc*, const short2*);
+template __global__ void k_import_ref<3>(const SessionDesc*, const short2*);
+
+}  // namespace nui

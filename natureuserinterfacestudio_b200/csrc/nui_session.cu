@@ -1,0 +1,928 @@
+// Host runtime of the C ABI: context (device + stream), sessions (device-resident state),
+// the per-frame launch schedule, batched ticks under a CUDA graph, and the entry points
+// declared in include/nui_b200.h.
+//
+// One frame of a session (NuiKinfuTrackingEngine::RunTracking, NuiKinfuTrackingEngine.cpp:68-142)
+// is this fixed sequence of launches, each covering every session of the batch
+// (blockIdx.y = session):
+//   k_preprocess, k_pyramid x (levels-1), k_feedback, k_icp x sum(iterations),
+//   k_track_finalize, k_integrate<fmt>, k_raycast<fmt>
+// Which session does what in a tick (first frame / tracking / inactive) is data in the
+// session table, so the same sequence serves every tick and is captured once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/nui_b200.h"
+#include "nui_device.cuh"
+
+namespace nui {
+__global__ void k_preprocess(const SessionDesc*);
+__global__ void k_pyramid(const SessionDesc*, int);
+__global__ void k_feedback(const SessionDesc*);
+__global__ void k_icp(const SessionDesc*, int, int);
+__global__ void k_track_finalize(const SessionDesc*);
+template <int F>
+__global__ void k_integrate(const SessionDesc*);
+template <int F>
+__global__ void k_volume_init(const SessionDesc*);
+template <int F>
+__global__ void k_raycast(const SessionDesc*);
+__global__ void k_publish(const SessionDesc*, int, float*, int*);
+template <int F>
+__global__ void k_export_ref(const SessionDesc*, short2*, uchar4*);
+template <int F>
+__global__ void k_import_ref(const SessionDesc*, const short2*);
+}  // namespace nui
+
+using namespace nui;
+
+namespace {
+thread_local std::string g_err;
+nui_status fail(nui_status st, const std::string& msg) {
+  g_err = msg;
+  return st;
+}
+#define NUI_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) return fail(NUI_ERR_DEVICE, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr int kStages = 6;
+constexpr int kZChunkTargetThreads = 1 << 18;
+}  // namespace
+
+struct nui_session;
+
+struct BatchPlan {
+  int n = 0;
+  int maxW = 0, maxH = 0, maxLevels = 0;
+  int maxIters[kMaxLevels] = {0, 0, 0, 0};
+  long maxIntegThreads[4] = {0, 0, 0, 0};  // per format: columns * zchunks
+  int fmtMask = 0;
+  bool operator<(const BatchPlan& o) const { return std::memcmp(this, &o, sizeof(BatchPlan)) < 0; }
+};
+
+struct nui_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  bool timing = false;
+  cudaEvent_t ev[kStages + 1] = {};
+  float stage_ms[kStages] = {};
+  // batch table (device + pinned staging) and per-session outputs (status + pose)
+  int cap = 0;
+  SessionDesc* d_descs = nullptr;
+  SessionDesc* h_descs = nullptr;
+  float* d_pose = nullptr;  // cap * 14: R(9) t(3) err count
+  int* d_status = nullptr;  // cap * 2: status, integrate
+  float* h_pose = nullptr;
+  int* h_status = nullptr;
+  // scratch descriptor for kernel-level calls
+  SessionDesc* d_kdesc = nullptr;
+  TrackState* d_kts = nullptr;
+  std::map<BatchPlan, cudaGraphExec_t> graphs;
+};
+
+struct nui_session {
+  nui_ctx* ctx = nullptr;
+  nui_session_cfg cfg;
+  DevCam cam;
+  float cell[3], trunc;
+  int zchunks = 1;
+  unsigned icp_min_count[kMaxLevels] = {0, 0, 0, 0};
+  float gauss[2 * kMaxRadius + 1];
+  uint16_t* raw = nullptr;
+  uint8_t* bgra = nullptr;
+  float* dscaled = nullptr;
+  float* dlev[kMaxLevels] = {};
+  float4* vlev[kMaxLevels] = {};
+  float4 *vref = nullptr, *nref = nullptr;
+  uchar4* cmap = nullptr;
+  void* vol = nullptr;
+  uint8_t* wvol = nullptr;
+  uchar4* cvol = nullptr;
+  TrackState* ts = nullptr;
+  float2* partials = nullptr;
+  SessionDesc* d_desc1 = nullptr;  // one-entry table for the per-session path
+  long frames = 0;
+  bool color_frame = false;
+  std::vector<void*> allocs;
+};
+
+// ------------------------------------------------------------------ helpers
+namespace {
+
+size_t voxel_bytes(int fmt) { return fmt == NUI_TSDF_F32 ? 8 : (fmt == NUI_TSDF_F16_U8 ? 3 : 4); }
+
+bool cfg_valid(const nui_session_cfg* c, std::string& why) {
+  if (!c) return why = "null config", false;
+  if (c->width <= 0 || c->height <= 0 || c->width > 4096 || c->height > 4096) return why = "bad image size", false;
+  if (c->levels < 1 || c->levels > kMaxLevels) return why = "levels must be 1..4", false;
+  for (int l = 0; l < c->levels; ++l) {
+    if (c->iterations[l] < 0 || c->iterations[l] > 100) return why = "bad iteration count", false;
+    if ((c->width >> l) < 2 || (c->height >> l) < 2) return why = "too many levels for the image", false;
+    if (((c->width >> l) << l) != c->width || ((c->height >> l) << l) != c->height)
+      return why = "image size must be divisible by 2^(levels-1)", false;
+  }
+  if (c->volume_kind != NUI_VOLUME_DENSE) return why = "only dense volumes in this build", false;
+  if (c->tsdf_format < 0 || c->tsdf_format > 3) return why = "bad tsdf format", false;
+  for (int i = 0; i < 3; ++i) {
+    if (c->res[i] < 8 || c->res[i] > 1024) return why = "volume resolution must be 8..1024", false;
+    if (!(c->dim[i] > 0.f)) return why = "volume size must be positive", false;
+  }
+  if (c->filter_radius < 0 || c->filter_radius > kMaxRadius) return why = "filter radius must be 0..7", false;
+  if (!(c->fx > 0.f) || !(c->fy > 0.f)) return why = "focal lengths must be positive", false;
+  return true;
+}
+
+// ICP valid-count threshold per level.  The reference computes it from
+// kernelGlobalSize[0], which after the first level still holds the global size of the
+// last compute_sums launch (NuiKinfuOpenCLDepthTracker.cpp:309, 342, 368); reproduced.
+void icp_thresholds(const nui_session_cfg& c, unsigned* out) {
+  size_t g = (size_t)c.width * c.height;
+  for (int lv = c.levels - 1; lv >= 0; --lv) {
+    out[lv] = (unsigned)((double)(g >> (2 * lv)) * 0.1);
+    if (c.iterations[lv] > 0) {
+      size_t n = (size_t)(c.width >> lv) * (c.height >> lv);
+      unsigned size = (unsigned)std::ceil((float)n / 128.f);
+      unsigned nb = (unsigned)std::ceil((float)size / 128.f);
+      g = (size_t)nb * 128;
+    }
+  }
+}
+
+void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* raw, const uint8_t* bgra) {
+  std::memset(&d, 0, sizeof(d));
+  const nui_session_cfg& c = s->cfg;
+  d.kind = kind;
+  d.W = c.width;
+  d.H = c.height;
+  d.levels = c.levels;
+  d.cam = s->cam;
+  d.radius = c.filter_radius;
+  d.sigma_depth = c.sigma_depth2_inv_half;
+  d.depth_thr = c.depth_threshold;
+  std::memcpy(d.gauss, s->gauss, sizeof(d.gauss));
+  d.dist_thr = c.dist_threshold + c.dist_threshold / (float)c.levels;
+  for (int l = 0; l < kMaxLevels; ++l) {
+    d.iters[l] = l < c.levels ? c.iterations[l] : 0;
+    d.icp_min_count[l] = s->icp_min_count[l];
+    d.dlev[l] = s->dlev[l];
+    d.vlev[l] = s->vlev[l];
+  }
+  d.integ_thr = c.integration_threshold;
+  d.raw = raw;
+  d.bgra = bgra;
+  d.dscaled = s->dscaled;
+  d.vref = s->vref;
+  d.nref = s->nref;
+  d.cmap = s->cmap;
+  d.fmt = c.tsdf_format;
+  for (int i = 0; i < 3; ++i) {
+    d.res[i] = c.res[i];
+    d.dim[i] = c.dim[i];
+    d.cell[i] = s->cell[i];
+  }
+  d.trunc = s->trunc;
+  d.vol = s->vol;
+  d.wvol = s->wvol;
+  d.cvol = s->cvol;
+  d.max_cw = c.max_color_weight;
+  d.zchunks = s->zchunks;
+  d.ts = s->ts;
+  d.partials = s->partials;
+}
+
+void plan_add(BatchPlan& p, const nui_session* s) {
+  const nui_session_cfg& c = s->cfg;
+  p.maxW = std::max(p.maxW, c.width);
+  p.maxH = std::max(p.maxH, c.height);
+  p.maxLevels = std::max(p.maxLevels, c.levels);
+  for (int l = 0; l < c.levels; ++l) p.maxIters[l] = std::max(p.maxIters[l], c.iterations[l]);
+  long th = (long)c.res[0] * c.res[1] * s->zchunks;
+  p.maxIntegThreads[c.tsdf_format] = std::max(p.maxIntegThreads[c.tsdf_format], th);
+  p.fmtMask |= 1 << c.tsdf_format;
+}
+
+unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
+
+// zchunks per session: threads per launch >= 2^18, every chunk >= 16 slices
+int pick_zchunks(const nui_session_cfg& c) {
+  long ncol = (long)c.res[0] * c.res[1];
+  int z = (int)std::max(1L, (kZChunkTargetThreads + ncol - 1) / ncol);
+  z = std::min(z, std::max(1, c.res[2] / 16));
+  return z;
+}
+
+template <int F>
+void launch_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
+  if (!(p.fmtMask & (1 << F))) return;
+  k_integrate<F><<<dim3(cdiv(p.maxIntegThreads[F], 256), p.n), 256, 0, st>>>(d);
+}
+template <int F>
+void launch_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
+  if (!(p.fmtMask & (1 << F))) return;
+  k_raycast<F><<<dim3(cdiv((long)p.maxW * p.maxH, 128), p.n), 128, 0, st>>>(d);
+}
+
+// The launch schedule of one tick.  ev: optional stage events (timing only).
+void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float* d_pose, int* d_status, bool ev) {
+  cudaStream_t st = ctx->stream;
+  auto mark = [&](int i) {
+    if (ev) cudaEventRecord(ctx->ev[i], st);
+  };
+  mark(0);
+  const unsigned tiles = cdiv(p.maxW, 32) * cdiv(p.maxH, 8);
+  k_preprocess<<<dim3(tiles, p.n), dim3(32, 8), 0, st>>>(d);
+  mark(1);
+  for (int l = 1; l < p.maxLevels; ++l)
+    k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), p.n), 256, 0, st>>>(d, l);
+  k_feedback<<<dim3(cdiv((long)p.maxW * p.maxH, 256), p.n), 256, 0, st>>>(d);
+  mark(2);
+  for (int l = p.maxLevels - 1; l >= 0; --l) {
+    const unsigned nb = cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256 * 4);
+    for (int it = 0; it < p.maxIters[l]; ++it) k_icp<<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
+  }
+  k_track_finalize<<<p.n, 32, 0, st>>>(d);
+  k_publish<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n, d_pose, d_status);
+  mark(3);
+  launch_integrate<0>(p, d, st);
+  launch_integrate<1>(p, d, st);
+  launch_integrate<2>(p, d, st);
+  launch_integrate<3>(p, d, st);
+  mark(4);
+  launch_raycast<0>(p, d, st);
+  launch_raycast<1>(p, d, st);
+  launch_raycast<2>(p, d, st);
+  launch_raycast<3>(p, d, st);
+  mark(5);
+}
+
+nui_status ensure_cap(nui_ctx* ctx, int n) {
+  if (n <= ctx->cap) return NUI_OK;
+  int cap = std::max(n, std::max(64, ctx->cap * 2));
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  ctx->graphs.clear();
+  cudaFree(ctx->d_descs);
+  cudaFreeHost(ctx->h_descs);
+  cudaFree(ctx->d_pose);
+  cudaFree(ctx->d_status);
+  cudaFreeHost(ctx->h_pose);
+  cudaFreeHost(ctx->h_status);
+  NUI_CUDA(cudaMalloc(&ctx->d_descs, sizeof(SessionDesc) * cap));
+  NUI_CUDA(cudaMallocHost(&ctx->h_descs, sizeof(SessionDesc) * cap));
+  NUI_CUDA(cudaMalloc(&ctx->d_pose, sizeof(float) * 14 * cap));
+  NUI_CUDA(cudaMalloc(&ctx->d_status, sizeof(int) * 2 * cap));
+  NUI_CUDA(cudaMallocHost(&ctx->h_pose, sizeof(float) * 14 * cap));
+  NUI_CUDA(cudaMallocHost(&ctx->h_status, sizeof(int) * 2 * cap));
+  ctx->cap = cap;
+  return NUI_OK;
+}
+
+nui_status finish_timing(nui_ctx* ctx) {
+  if (!ctx->timing) return NUI_OK;
+  NUI_CUDA(cudaEventSynchronize(ctx->ev[5]));
+  for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ctx->stage_ms[i], ctx->ev[i], ctx->ev[i + 1]);
+  cudaEventElapsedTime(&ctx->stage_ms[5], ctx->ev[0], ctx->ev[5]);
+  return NUI_OK;
+}
+
+// Runs one tick over sessions[0..n) whose frames are already in device memory at
+// raws[i]/bgras[i].  use_graph: replay a captured graph for this batch shape.
+nui_status run_tick(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t* const* raws,
+                    const uint8_t* const* bgras, bool use_graph, nui_status* per, float* poses) {
+  nui_status st = ensure_cap(ctx, n);
+  if (st != NUI_OK) return st;
+  BatchPlan p;
+  p.n = n;
+  for (int i = 0; i < n; ++i) {
+    nui_session* s = ss[i];
+    plan_add(p, s);
+    int kind = s->frames == 0 ? kFirstFrame : kTrackFrame;
+    fill_desc(s, ctx->h_descs[i], kind, raws[i], bgras ? bgras[i] : nullptr);
+  }
+  NUI_CUDA(cudaMemcpyAsync(ctx->d_descs, ctx->h_descs, sizeof(SessionDesc) * n, cudaMemcpyHostToDevice, ctx->stream));
+  if (use_graph && !ctx->timing) {
+    auto it = ctx->graphs.find(p);
+    if (it == ctx->graphs.end()) {
+      cudaGraph_t g;
+      NUI_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      enqueue_tick(ctx, p, ctx->d_descs, ctx->d_pose, ctx->d_status, false);
+      NUI_CUDA(cudaStreamEndCapture(ctx->stream, &g));
+      cudaGraphExec_t ge;
+      NUI_CUDA(cudaGraphInstantiate(&ge, g, 0));
+      cudaGraphDestroy(g);
+      it = ctx->graphs.emplace(p, ge).first;
+    }
+    NUI_CUDA(cudaGraphLaunch(it->second, ctx->stream));
+  } else {
+    enqueue_tick(ctx, p, ctx->d_descs, ctx->d_pose, ctx->d_status, ctx->timing);
+    NUI_CUDA(cudaGetLastError());
+  }
+  NUI_CUDA(cudaMemcpyAsync(ctx->h_pose, ctx->d_pose, sizeof(float) * 14 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  NUI_CUDA(cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int) * 2 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  NUI_CUDA(cudaStreamSynchronize(ctx->stream));
+  st = finish_timing(ctx);
+  if (st != NUI_OK) return st;
+  nui_status agg = NUI_OK;
+  for (int i = 0; i < n; ++i) {
+    nui_session* s = ss[i];
+    int status = ctx->h_status[2 * i];
+    nui_status r = status == 0 ? NUI_OK : NUI_ERR_TRACKING_LOST;
+    if (per) per[i] = r;
+    if (r != NUI_OK) {
+      agg = NUI_ERR_TRACKING_LOST;
+      // the device state stays on the previous frame; clear the flag so that the next
+      // frame (after nui_reset or not) starts from a clean tracker
+      int zero = 0;
+      cudaMemcpy(&s->ts->status, &zero, sizeof(int), cudaMemcpyHostToDevice);
+    } else {
+      s->frames += 1;
+    }
+    if (poses) std::memcpy(poses + 12 * i, ctx->h_pose + 14 * i, 12 * sizeof(float));
+  }
+  return agg;
+}
+
+nui_status upload_frame(nui_session* s, const uint16_t* depth, const uint8_t* bgra) {
+  const size_t N = (size_t)s->cfg.width * s->cfg.height;
+  NUI_CUDA(cudaMemcpyAsync(s->raw, depth, N * 2, cudaMemcpyHostToDevice, s->ctx->stream));
+  s->color_frame = false;
+  if (bgra && s->bgra) {
+    NUI_CUDA(cudaMemcpyAsync(s->bgra, bgra, N * 4, cudaMemcpyHostToDevice, s->ctx->stream));
+    s->color_frame = true;
+  }
+  return NUI_OK;
+}
+
+template <int F>
+void launch_init(nui_session* s) {
+  k_volume_init<F><<<dim3(1184, 1), 256, 0, s->ctx->stream>>>(s->d_desc1);
+}
+
+nui_status reset_session(nui_session* s) {
+  SessionDesc d;
+  fill_desc(s, d, kInactive, nullptr, nullptr);
+  NUI_CUDA(cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, s->ctx->stream));
+  switch (s->cfg.tsdf_format) {
+    case 0: launch_init<0>(s); break;
+    case 1: launch_init<1>(s); break;
+    case 2: launch_init<2>(s); break;
+    case 3: launch_init<3>(s); break;
+  }
+  TrackState t;
+  std::memset(&t, 0, sizeof(t));
+  const float I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  std::memcpy(t.xf.R, I, sizeof(I));
+  std::memcpy(t.xf.R_inv, I, sizeof(I));
+  std::memcpy(t.R, I, sizeof(I));
+  std::memcpy(t.lastR, I, sizeof(I));
+  NUI_CUDA(cudaMemcpyAsync(s->ts, &t, sizeof(t), cudaMemcpyHostToDevice, s->ctx->stream));
+  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  NUI_CUDA(cudaGetLastError());
+  s->frames = 0;
+  return NUI_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+NUI_API const char* nui_last_error_string(void) { return g_err.c_str(); }
+
+NUI_API void nui_session_cfg_default(nui_session_cfg* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->width = 640;
+  c->height = 480;
+  c->fx = c->fy = 525.f;
+  c->cx = 319.5f;
+  c->cy = 239.5f;
+  c->depth_min = 0.5f;
+  c->depth_max = 4.5f;
+  c->volume_kind = NUI_VOLUME_DENSE;
+  c->tsdf_format = NUI_TSDF_I16;
+  c->res[0] = c->res[1] = c->res[2] = 256;
+  c->dim[0] = c->dim[1] = c->dim[2] = 3.f;
+  c->trunc_dist = 0.03f;
+  c->color_volume = 0;
+  c->max_color_weight = 128;
+  c->levels = 3;
+  c->iterations[0] = c->iterations[1] = c->iterations[2] = 10;
+  c->filter_radius = 3;
+  c->sigma_space2_inv_half = 0.08f;
+  c->sigma_depth2_inv_half = 50.0f;
+  c->depth_threshold = 0.3f;
+  c->dist_threshold = 0.1f;
+  c->integration_threshold = 0.15f;
+}
+
+NUI_API nui_status nui_ctx_create(int device, nui_ctx** out) {
+  if (!out) return fail(NUI_ERR_INVALID_ARG, "out is null");
+  int ndev = 0;
+  NUI_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(NUI_ERR_INVALID_ARG, "no such device");
+  NUI_CUDA(cudaSetDevice(device));
+  nui_ctx* c = new nui_ctx();
+  c->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(NUI_ERR_DEVICE, cudaGetErrorString(e));
+  }
+  c->stream = c->own;
+  for (int i = 0; i <= kStages; ++i) cudaEventCreate(&c->ev[i]);
+  if (cudaMalloc(&c->d_kdesc, sizeof(SessionDesc)) != cudaSuccess ||
+      cudaMalloc(&c->d_kts, sizeof(TrackState)) != cudaSuccess) {
+    delete c;
+    return fail(NUI_ERR_OOM, "context scratch");
+  }
+  *out = c;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_ctx_destroy(nui_ctx* c) {
+  if (!c) return NUI_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+  for (int i = 0; i <= kStages; ++i) cudaEventDestroy(c->ev[i]);
+  cudaFree(c->d_descs);
+  cudaFreeHost(c->h_descs);
+  cudaFree(c->d_pose);
+  cudaFree(c->d_status);
+  cudaFreeHost(c->h_pose);
+  cudaFreeHost(c->h_status);
+  cudaFree(c->d_kdesc);
+  cudaFree(c->d_kts);
+  cudaStreamDestroy(c->own);
+  delete c;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_ctx_set_stream(nui_ctx* c, void* stream) {
+  if (!c) return fail(NUI_ERR_INVALID_ARG, "null context");
+  NUI_CUDA(cudaStreamSynchronize(c->stream));
+  c->stream = stream ? (cudaStream_t)stream : c->own;
+  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+  c->graphs.clear();
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_ctx_synchronize(nui_ctx* c) {
+  if (!c) return fail(NUI_ERR_INVALID_ARG, "null context");
+  NUI_CUDA(cudaStreamSynchronize(c->stream));
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_ctx_enable_timing(nui_ctx* c, int enable) {
+  if (!c) return fail(NUI_ERR_INVALID_ARG, "null context");
+  c->timing = enable != 0;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_ctx_stage_ms(nui_ctx* c, int stage, float* ms) {
+  if (!c || !ms || stage < 0 || stage >= kStages) return fail(NUI_ERR_INVALID_ARG, "bad stage");
+  *ms = c->stage_ms[stage];
+  return NUI_OK;
+}
+
+NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
+  std::string why;
+  if (!cfg_valid(c, why)) return 0;
+  const size_t N = (size_t)c->width * c->height;
+  size_t b = N * 2 + N * 4 /*bgra*/ + N * 4 /*scaled*/ + N * 16 * 2 /*ref maps*/ + N * 4 /*cmap*/;
+  for (int l = 0; l < c->levels; ++l) b += (N >> (2 * l)) * (4 + 16);
+  const size_t nv = (size_t)c->res[0] * c->res[1] * c->res[2];
+  b += nv * voxel_bytes(c->tsdf_format);
+  if (c->color_volume) b += nv * 4;
+  b += sizeof(TrackState) + sizeof(SessionDesc) + ((N + 1023) / 1024) * kIcpTerms * sizeof(float2);
+  return b;
+}
+
+NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, nui_session** out) {
+  std::string why;
+  if (!ctx || !out) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  if (!cfg_valid(cfg, why)) return fail(NUI_ERR_INVALID_ARG, why);
+  NUI_CUDA(cudaSetDevice(ctx->device));
+  nui_session* s = new nui_session();
+  s->ctx = ctx;
+  s->cfg = *cfg;
+  const nui_session_cfg& c = s->cfg;
+  s->cam = DevCam{c.fx, c.fy, 1 / c.fx, 1 / c.fy, c.cx, c.cy, c.width, c.height, c.depth_min, c.depth_max};
+  for (int i = 0; i < 3; ++i) s->cell[i] = c.dim[i] / (float)c.res[i];
+  s->trunc = std::max(c.trunc_dist, 2.1f * std::max(s->cell[0], std::max(s->cell[1], s->cell[2])));
+  for (int i = 0; i < 2 * kMaxRadius + 1; ++i) s->gauss[i] = 0.f;
+  for (int i = 0; i < 2 * c.filter_radius + 1; ++i) {
+    int x = i - c.filter_radius;
+    s->gauss[i] = std::exp((float)(-(x * x)) * c.sigma_space2_inv_half);
+  }
+  icp_thresholds(c, s->icp_min_count);
+  s->zchunks = pick_zchunks(c);
+  const size_t N = (size_t)c.width * c.height;
+  const size_t nv = (size_t)c.res[0] * c.res[1] * c.res[2];
+  auto alloc = [&](void** p, size_t bytes) -> bool {
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    s->allocs.push_back(*p);
+    return true;
+  };
+  bool ok = alloc((void**)&s->raw, N * 2) && alloc((void**)&s->dscaled, N * 4) && alloc((void**)&s->vref, N * 16) &&
+            alloc((void**)&s->nref, N * 16) && alloc((void**)&s->ts, sizeof(TrackState)) &&
+            alloc((void**)&s->partials, ((N + 1023) / 1024) * kIcpTerms * sizeof(float2)) &&
+            alloc((void**)&s->d_desc1, sizeof(SessionDesc)) && alloc((void**)&s->vol, nv * (c.tsdf_format == 2 ? 2 : voxel_bytes(c.tsdf_format)));
+  for (int l = 0; ok && l < c.levels; ++l)
+    ok = alloc((void**)&s->dlev[l], (N >> (2 * l)) * 4) && alloc((void**)&s->vlev[l], (N >> (2 * l)) * 16);
+  if (ok && c.tsdf_format == NUI_TSDF_F16_U8) ok = alloc((void**)&s->wvol, nv);
+  if (ok && c.color_volume) ok = alloc((void**)&s->cvol, nv * 4) && alloc((void**)&s->bgra, N * 4) && alloc((void**)&s->cmap, N * 4);
+  if (!ok) {
+    for (void* p : s->allocs) cudaFree(p);
+    delete s;
+    return fail(NUI_ERR_OOM, "device allocation failed");
+  }
+  cudaMemsetAsync(s->ts, 0, sizeof(TrackState), ctx->stream);
+  nui_status st = reset_session(s);
+  if (st != NUI_OK) {
+    for (void* p : s->allocs) cudaFree(p);
+    delete s;
+    return st;
+  }
+  *out = s;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_session_destroy(nui_session* s) {
+  if (!s) return NUI_OK;
+  cudaStreamSynchronize(s->ctx->stream);
+  for (void* p : s->allocs) cudaFree(p);
+  delete s;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_reset(nui_session* s) {
+  if (!s) return fail(NUI_ERR_INVALID_ARG, "null session");
+  return reset_session(s);
+}
+
+NUI_API nui_status nui_process_frame(nui_session* s, const uint16_t* depth, const uint8_t* bgra, float* pose) {
+  if (!s || !depth) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  nui_status st = upload_frame(s, depth, bgra);
+  if (st != NUI_OK) return st;
+  const uint16_t* r = s->raw;
+  const uint8_t* b = s->color_frame ? s->bgra : nullptr;
+  nui_session* arr[1] = {s};
+  nui_status per;
+  return run_tick(s->ctx, arr, 1, &r, &b, false, &per, pose);
+}
+
+NUI_API nui_status nui_process_frame_device(nui_session* s, const uint16_t* d_depth, const uint8_t* d_bgra, float* pose) {
+  if (!s || !d_depth) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  nui_session* arr[1] = {s};
+  const uint8_t* b = (d_bgra && s->cvol) ? d_bgra : nullptr;
+  nui_status per;
+  return run_tick(s->ctx, arr, 1, &d_depth, &b, false, &per, pose);
+}
+
+NUI_API nui_status nui_batch_tick(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t* const* depths,
+                                  const uint8_t* const* bgras, nui_status* per, float* poses) {
+  if (!ctx || !ss || n <= 0 || !depths) return fail(NUI_ERR_INVALID_ARG, "bad batch");
+  std::vector<const uint16_t*> r(n);
+  std::vector<const uint8_t*> b(n);
+  for (int i = 0; i < n; ++i) {
+    if (!ss[i] || ss[i]->ctx != ctx || !depths[i]) return fail(NUI_ERR_INVALID_ARG, "bad session or frame");
+    nui_status st = upload_frame(ss[i], depths[i], bgras ? bgras[i] : nullptr);
+    if (st != NUI_OK) return st;
+    r[i] = ss[i]->raw;
+    b[i] = ss[i]->color_frame ? ss[i]->bgra : nullptr;
+  }
+  return run_tick(ctx, ss, n, r.data(), b.data(), true, per, poses);
+}
+
+NUI_API nui_status nui_batch_tick_device(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t* const* d_depths,
+                                         const uint8_t* const* d_bgras, nui_status* per, float* poses) {
+  if (!ctx || !ss || n <= 0 || !d_depths) return fail(NUI_ERR_INVALID_ARG, "bad batch");
+  std::vector<const uint8_t*> b(n, nullptr);
+  for (int i = 0; i < n; ++i) {
+    if (!ss[i] || ss[i]->ctx != ctx || !d_depths[i]) return fail(NUI_ERR_INVALID_ARG, "bad session or frame");
+    if (d_bgras && d_bgras[i] && ss[i]->cvol) b[i] = d_bgras[i];
+  }
+  return run_tick(ctx, ss, n, d_depths, b.data(), true, per, poses);
+}
+
+NUI_API nui_status nui_set_pose(nui_session* s, const float* pose12) {
+  if (!s || !pose12) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  TrackState t;
+  NUI_CUDA(cudaMemcpy(&t, s->ts, sizeof(t), cudaMemcpyDeviceToHost));
+  double a[9];
+  for (int i = 0; i < 9; ++i) a[i] = pose12[i];
+  const double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+  const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+  const double inv[9] = {c00, a[2] * a[7] - a[1] * a[8], a[1] * a[5] - a[2] * a[4],
+                         c01, a[0] * a[8] - a[2] * a[6], a[2] * a[3] - a[0] * a[5],
+                         c02, a[1] * a[6] - a[0] * a[7], a[0] * a[4] - a[1] * a[3]};
+  for (int i = 0; i < 9; ++i) {
+    t.xf.R[i] = t.R[i] = pose12[i];
+    t.xf.R_inv[i] = (float)(inv[i] / det);
+  }
+  for (int i = 0; i < 3; ++i) t.xf.t[i] = t.t[i] = pose12[9 + i];
+  NUI_CUDA(cudaMemcpy(s->ts, &t, sizeof(t), cudaMemcpyHostToDevice));
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_get_pose(nui_session* s, float* pose12) {
+  if (!s || !pose12) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  TrackState t;
+  NUI_CUDA(cudaMemcpy(&t, s->ts, sizeof(t), cudaMemcpyDeviceToHost));
+  std::memcpy(pose12, t.xf.R, 9 * sizeof(float));
+  std::memcpy(pose12 + 9, t.xf.t, 3 * sizeof(float));
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_session_touched_voxels(nui_session* s, uint64_t* n) {
+  if (!s || !n) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  TrackState t;
+  NUI_CUDA(cudaMemcpy(&t, s->ts, sizeof(t), cudaMemcpyDeviceToHost));
+  *n = t.touched;
+  return NUI_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ step-wise API, debug
+namespace {
+// Runs a subset of the tick on one session: `what` 0 = preprocess (+pyramid), 1 = track,
+// 2 = integrate, 3 = raycast, 4 = feedback maps (frame-0 path).
+nui_status run_stage(nui_session* s, int what) {
+  nui_ctx* ctx = s->ctx;
+  SessionDesc d;
+  int kind = (what == 4 || (what == 2 && s->frames == 0)) ? kFirstFrame : kTrackFrame;
+  fill_desc(s, d, kind, s->raw, s->color_frame ? s->bgra : nullptr);
+  NUI_CUDA(cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, ctx->stream));
+  BatchPlan p;
+  p.n = 1;
+  plan_add(p, s);
+  cudaStream_t st = ctx->stream;
+  const SessionDesc* dd = s->d_desc1;
+  if (what == 0) {
+    k_preprocess<<<dim3(cdiv(p.maxW, 32) * cdiv(p.maxH, 8), 1), dim3(32, 8), 0, st>>>(dd);
+    for (int l = 1; l < p.maxLevels; ++l)
+      k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), 1), 256, 0, st>>>(dd, l);
+  } else if (what == 1) {
+    for (int l = p.maxLevels - 1; l >= 0; --l) {
+      const unsigned nb = cdiv((long)(p.maxW >> l) * (p.maxH >> l), 1024);
+      for (int it = 0; it < p.maxIters[l]; ++it) k_icp<<<dim3(nb, 1), 256, 0, st>>>(dd, l, it);
+    }
+    k_track_finalize<<<1, 32, 0, st>>>(dd);
+    k_publish<<<1, 64, 0, st>>>(dd, 1, ctx->d_pose, ctx->d_status);
+  } else if (what == 2) {
+    launch_integrate<0>(p, dd, st);
+    launch_integrate<1>(p, dd, st);
+    launch_integrate<2>(p, dd, st);
+    launch_integrate<3>(p, dd, st);
+  } else if (what == 3) {
+    launch_raycast<0>(p, dd, st);
+    launch_raycast<1>(p, dd, st);
+    launch_raycast<2>(p, dd, st);
+    launch_raycast<3>(p, dd, st);
+  } else if (what == 4) {
+    k_feedback<<<dim3(cdiv((long)p.maxW * p.maxH, 256), 1), 256, 0, st>>>(dd);
+  }
+  NUI_CUDA(cudaGetLastError());
+  NUI_CUDA(cudaStreamSynchronize(st));
+  return NUI_OK;
+}
+
+template <int F>
+void launch_export(nui_session* s, short2* out, uchar4* cout) {
+  k_export_ref<F><<<1184, 256, 0, s->ctx->stream>>>(s->d_desc1, out, cout);
+}
+template <int F>
+void launch_import(nui_session* s, const short2* in) {
+  k_import_ref<F><<<1184, 256, 0, s->ctx->stream>>>(s->d_desc1, in);
+}
+}  // namespace
+
+extern "C" {
+
+NUI_API nui_status nui_frame_upload(nui_session* s, const uint16_t* depth, const uint8_t* bgra) {
+  if (!s || !depth) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  nui_status st = upload_frame(s, depth, bgra);
+  if (st != NUI_OK) return st;
+  return run_stage(s, 0);
+}
+
+NUI_API nui_status nui_feedback_update(nui_session* s) {
+  if (!s) return fail(NUI_ERR_INVALID_ARG, "null session");
+  return run_stage(s, 4);
+}
+
+NUI_API nui_status nui_track(nui_session* s, float* err, int* count) {
+  if (!s) return fail(NUI_ERR_INVALID_ARG, "null session");
+  nui_status st = ensure_cap(s->ctx, 1);
+  if (st != NUI_OK) return st;
+  // the track stage must run with the integration threshold of the session, and must
+  // not integrate: k_track_finalize only decides the gate
+  st = run_stage(s, 1);
+  if (st != NUI_OK) return st;
+  TrackState t;
+  NUI_CUDA(cudaMemcpy(&t, s->ts, sizeof(t), cudaMemcpyDeviceToHost));
+  if (err) *err = t.error;
+  if (count) *count = (int)t.count;
+  if (t.status != 0) {
+    int zero = 0;
+    cudaMemcpy(&s->ts->status, &zero, sizeof(int), cudaMemcpyHostToDevice);
+    return fail(NUI_ERR_TRACKING_LOST, "ICP system is singular");
+  }
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_integrate(nui_session* s) {
+  if (!s) return fail(NUI_ERR_INVALID_ARG, "null session");
+  int one = 1;
+  NUI_CUDA(cudaMemcpy(&s->ts->integrate, &one, sizeof(int), cudaMemcpyHostToDevice));
+  NUI_CUDA(cudaMemset(&s->ts->touched, 0, sizeof(unsigned long long)));
+  return run_stage(s, 2);
+}
+
+NUI_API nui_status nui_raycast(nui_session* s) {
+  if (!s) return fail(NUI_ERR_INVALID_ARG, "null session");
+  return run_stage(s, 3);
+}
+
+NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void* host, size_t bytes) {
+  if (!s || !host) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  const nui_session_cfg& c = s->cfg;
+  const size_t N = (size_t)c.width * c.height;
+  const size_t nv = (size_t)c.res[0] * c.res[1] * c.res[2];
+  if (level < 0 || level >= c.levels) return fail(NUI_ERR_INVALID_ARG, "bad level");
+  const size_t Nl = N >> (2 * level);
+  const void* src = nullptr;
+  size_t need = 0;
+  switch (what) {
+    case 0: src = s->dlev[0]; need = N * 4; break;
+    case 1: src = s->dscaled; need = N * 4; break;
+    case 2: src = s->vlev[level]; need = Nl * 16; break;
+    case 3: src = s->vref; need = N * 16; break;
+    case 4: src = s->nref; need = N * 16; break;
+    case 6: src = s->vol; need = nv * (c.tsdf_format == 2 ? 2 : voxel_bytes(c.tsdf_format)); break;
+    case 7: src = s->dlev[level]; need = Nl * 4; break;
+    case 8: src = s->cmap; need = N * 4; break;
+    case 5:
+    case 9: {
+      need = nv * 4;
+      if (bytes < need) return fail(NUI_ERR_INVALID_ARG, "buffer too small");
+      if (what == 9 && !s->cvol) return fail(NUI_ERR_INVALID_ARG, "no colour volume");
+      void* tmp = nullptr;
+      NUI_CUDA(cudaMalloc(&tmp, need));
+      SessionDesc d;
+      fill_desc(s, d, kInactive, nullptr, nullptr);
+      cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, s->ctx->stream);
+      short2* vo = what == 5 ? (short2*)tmp : nullptr;
+      uchar4* co = what == 9 ? (uchar4*)tmp : nullptr;
+      switch (c.tsdf_format) {
+        case 0: launch_export<0>(s, vo, co); break;
+        case 1: launch_export<1>(s, vo, co); break;
+        case 2: launch_export<2>(s, vo, co); break;
+        case 3: launch_export<3>(s, vo, co); break;
+      }
+      cudaError_t e = cudaMemcpyAsync(host, tmp, need, cudaMemcpyDeviceToHost, s->ctx->stream);
+      cudaStreamSynchronize(s->ctx->stream);
+      cudaFree(tmp);
+      if (e != cudaSuccess) return fail(NUI_ERR_DEVICE, cudaGetErrorString(e));
+      return NUI_OK;
+    }
+    default:
+      return fail(NUI_ERR_INVALID_ARG, "unknown buffer");
+  }
+  if (!src) return fail(NUI_ERR_INVALID_ARG, "buffer not present");
+  if (bytes < need) return fail(NUI_ERR_INVALID_ARG, "buffer too small");
+  NUI_CUDA(cudaMemcpy(host, src, need, cudaMemcpyDeviceToHost));
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_debug_upload_volume(nui_session* s, const int16_t* ref) {
+  if (!s || !ref) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  const size_t nv = (size_t)s->cfg.res[0] * s->cfg.res[1] * s->cfg.res[2];
+  void* tmp = nullptr;
+  NUI_CUDA(cudaMalloc(&tmp, nv * 4));
+  SessionDesc d;
+  fill_desc(s, d, kInactive, nullptr, nullptr);
+  cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, s->ctx->stream);
+  cudaMemcpyAsync(tmp, ref, nv * 4, cudaMemcpyHostToDevice, s->ctx->stream);
+  switch (s->cfg.tsdf_format) {
+    case 0: launch_import<0>(s, (const short2*)tmp); break;
+    case 1: launch_import<1>(s, (const short2*)tmp); break;
+    case 2: launch_import<2>(s, (const short2*)tmp); break;
+    case 3: launch_import<3>(s, (const short2*)tmp); break;
+  }
+  cudaError_t e = cudaStreamSynchronize(s->ctx->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(NUI_ERR_DEVICE, cudaGetErrorString(e));
+  return NUI_OK;
+}
+
+// ------------------------------------------------------------------ kernel-level calls
+NUI_API nui_status nui_k_preprocess(nui_ctx* ctx, const uint16_t* d_raw, int W, int H, float fx, float fy, float cx,
+                                    float cy, float dmin, float dmax, int radius, float ss2, float sd2, float thr,
+                                    float* d_filtered, float* d_vertex4, float* d_scaled) {
+  if (!ctx || !d_raw || !d_filtered || !d_vertex4 || !d_scaled || W <= 0 || H <= 0 || radius < 0 ||
+      radius > kMaxRadius)
+    return fail(NUI_ERR_INVALID_ARG, "bad argument");
+  SessionDesc d;
+  std::memset(&d, 0, sizeof(d));
+  d.kind = kTrackFrame;
+  d.W = W;
+  d.H = H;
+  d.levels = 1;
+  d.cam = DevCam{fx, fy, 1 / fx, 1 / fy, cx, cy, W, H, dmin, dmax};
+  d.radius = radius;
+  d.sigma_depth = sd2;
+  d.depth_thr = thr;
+  for (int i = 0; i < 2 * radius + 1; ++i) {
+    int x = i - radius;
+    d.gauss[i] = std::exp((float)(-(x * x)) * ss2);
+  }
+  d.raw = d_raw;
+  d.dlev[0] = d_filtered;
+  d.vlev[0] = (float4*)d_vertex4;
+  d.dscaled = d_scaled;
+  NUI_CUDA(cudaMemcpyAsync(ctx->d_kdesc, &d, sizeof(d), cudaMemcpyHostToDevice, ctx->stream));
+  k_preprocess<<<dim3(cdiv(W, 32) * cdiv(H, 8), 1), dim3(32, 8), 0, ctx->stream>>>(ctx->d_kdesc);
+  NUI_CUDA(cudaGetLastError());
+  NUI_CUDA(cudaStreamSynchronize(ctx->stream));
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_k_pyramid_level(nui_ctx* ctx, const float* d_src, int dW, int dH, float fx, float fy, float cx,
+                                       float cy, int div, float thr, float* d_dst, float* d_vertex4) {
+  if (!ctx || !d_src || !d_dst || !d_vertex4 || dW <= 0 || dH <= 0) return fail(NUI_ERR_INVALID_ARG, "bad argument");
+  int level = 0;
+  while ((1 << level) < div) ++level;
+  if ((1 << level) != div || level < 1 || level >= kMaxLevels) return fail(NUI_ERR_INVALID_ARG, "div must be 2, 4 or 8");
+  SessionDesc d;
+  std::memset(&d, 0, sizeof(d));
+  d.kind = kTrackFrame;
+  d.W = dW << level;
+  d.H = dH << level;
+  d.levels = level + 1;
+  d.cam = DevCam{fx, fy, 1 / fx, 1 / fy, cx, cy, d.W, d.H, 0, 0};
+  d.depth_thr = thr;
+  d.dlev[level - 1] = const_cast<float*>(d_src);
+  d.dlev[level] = d_dst;
+  d.vlev[level] = (float4*)d_vertex4;
+  NUI_CUDA(cudaMemcpyAsync(ctx->d_kdesc, &d, sizeof(d), cudaMemcpyHostToDevice, ctx->stream));
+  k_pyramid<<<dim3(cdiv((long)dW * dH, 256), 1), 256, 0, ctx->stream>>>(ctx->d_kdesc, level);
+  NUI_CUDA(cudaGetLastError());
+  NUI_CUDA(cudaStreamSynchronize(ctx->stream));
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_k_feedback_maps(nui_ctx* ctx, const float* d_vertex4, int W, int H, float thr,
+                                       const float* pose12, float* d_vref4, float* d_nref4) {
+  if (!ctx || !d_vertex4 || !pose12 || !d_vref4 || !d_nref4 || W <= 0 || H <= 0)
+    return fail(NUI_ERR_INVALID_ARG, "bad argument");
+  TrackState t;
+  std::memset(&t, 0, sizeof(t));
+  std::memcpy(t.xf.R, pose12, 9 * sizeof(float));
+  std::memcpy(t.xf.t, pose12 + 9, 3 * sizeof(float));
+  SessionDesc d;
+  std::memset(&d, 0, sizeof(d));
+  d.kind = kFirstFrame;
+  d.W = W;
+  d.H = H;
+  d.levels = 1;
+  d.depth_thr = thr;
+  d.vlev[0] = (float4*)const_cast<float*>(d_vertex4);
+  d.vref = (float4*)d_vref4;
+  d.nref = (float4*)d_nref4;
+  d.ts = ctx->d_kts;
+  NUI_CUDA(cudaMemcpyAsync(ctx->d_kts, &t, sizeof(t), cudaMemcpyHostToDevice, ctx->stream));
+  NUI_CUDA(cudaMemcpyAsync(ctx->d_kdesc, &d, sizeof(d), cudaMemcpyHostToDevice, ctx->stream));
+  k_feedback<<<dim3(cdiv((long)W * H, 256), 1), 256, 0, ctx->stream>>>(ctx->d_kdesc);
+  NUI_CUDA(cudaGetLastError());
+  NUI_CUDA(cudaStreamSynchronize(ctx->stream));
+  return NUI_OK;
+}
+
+}  // extern "C"
+
+extern "C" NUI_API nui_status nui_mesh(nui_session* s, float* pos, float* col, uint64_t cap, uint64_t* nverts) {
+  (void)pos;
+  (void)col;
+  (void)cap;
+  if (!s || !nverts) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  return fail(NUI_ERR_UNSUPPORTED, "marching cubes not built");
+}

@@ -1,0 +1,241 @@
+"""ctypes access to the CPU oracle (libnui_oracle.so) and to the reference's own kernels
+compiled for the host (oracle/_ref/libnui_ref.so).  Test infrastructure: imported only by
+tests/, __graft_entry__.smoke() and bench.py's CPU baseline / reference arm.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libnui_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libnui_ref.so")
+REFERENCE_TREE = "/root/reference"
+
+_P = C.c_void_p
+
+
+def build(reference=True):
+    """Compile the oracle (always) and, when the reference tree is present, oracle/_ref."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if reference and os.path.isdir(os.path.join(REFERENCE_TREE, "src", "Kernels")):
+        subprocess.run(["python", os.path.join(HERE, "build_ref.py"), "--reference", REFERENCE_TREE], check=True,
+                       stdout=subprocess.DEVNULL)
+
+
+def p(a):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return a.ctypes.data_as(_P)
+
+
+class OrcCam(C.Structure):
+    _fields_ = [("fx", C.c_float), ("fy", C.c_float), ("fx_inv", C.c_float), ("fy_inv", C.c_float),
+                ("cx", C.c_float), ("cy", C.c_float), ("W", C.c_uint32), ("H", C.c_uint32),
+                ("dmin", C.c_float), ("dmax", C.c_float)]
+
+    @staticmethod
+    def make(W, H, fx=525.0, fy=525.0, cx=319.5, cy=239.5, dmin=0.5, dmax=4.5):
+        f32 = np.float32
+        return OrcCam(f32(fx), f32(fy), f32(1) / f32(fx), f32(1) / f32(fy), f32(cx), f32(cy), W, H, f32(dmin), f32(dmax))
+
+    def flat(self):
+        return np.array([self.fx, self.fy, self.fx_inv, self.fy_inv, self.cx, self.cy, self.W, self.H, self.dmin,
+                         self.dmax], np.float32)
+
+
+class OrcXform(C.Structure):
+    _fields_ = [("R", C.c_float * 9), ("R_inv", C.c_float * 9), ("t", C.c_float * 3)]
+
+    def flat(self):
+        return np.array(list(self.R) + list(self.R_inv) + list(self.t), np.float32)
+
+
+class OrcTsdf(C.Structure):
+    _fields_ = [("res", C.c_float * 3), ("dim", C.c_float * 3), ("cell", C.c_float * 3), ("trunc", C.c_float)]
+
+    @staticmethod
+    def make(res, dim, trunc_cfg):
+        t = OrcTsdf()
+        cells = []
+        for i in range(3):
+            t.res[i] = float(res[i])
+            t.dim[i] = float(dim[i])
+            c = np.float32(dim[i]) / np.float32(res[i])
+            t.cell[i] = float(c)
+            cells.append(c)
+        t.trunc = float(max(np.float32(trunc_cfg), np.float32(2.1) * max(cells)))
+        return t
+
+    def flat(self):
+        return np.array(list(self.res) + list(self.dim) + list(self.cell) + [self.trunc], np.float32)
+
+
+class OrcIcpStats(C.Structure):
+    _fields_ = [("error", C.c_float), ("count", C.c_float), ("iterations", C.c_int), ("status", C.c_int)]
+
+
+class OrcEngineCfg(C.Structure):
+    _fields_ = [("W", C.c_int), ("H", C.c_int), ("fx", C.c_float), ("fy", C.c_float), ("cx", C.c_float),
+                ("cy", C.c_float), ("dmin", C.c_float), ("dmax", C.c_float), ("res", C.c_int * 3),
+                ("dim", C.c_float * 3), ("trunc_cfg", C.c_float), ("color", C.c_int), ("max_color_weight", C.c_int),
+                ("levels", C.c_int), ("iters", C.c_int * 4), ("filter_radius", C.c_int),
+                ("sigma_space2_inv_half", C.c_float), ("sigma_depth2_inv_half", C.c_float),
+                ("depth_threshold", C.c_float), ("dist_threshold", C.c_float), ("integration_threshold", C.c_float)]
+
+    @staticmethod
+    def from_session_cfg(c):
+        e = OrcEngineCfg()
+        e.W, e.H = c.width, c.height
+        e.fx, e.fy, e.cx, e.cy = c.fx, c.fy, c.cx, c.cy
+        e.dmin, e.dmax = c.depth_min, c.depth_max
+        for i in range(3):
+            e.res[i] = c.res[i]
+            e.dim[i] = c.dim[i]
+        e.trunc_cfg = c.trunc_dist
+        e.color = c.color_volume
+        e.max_color_weight = c.max_color_weight
+        e.levels = c.levels
+        for i in range(4):
+            e.iters[i] = c.iterations[i]
+        e.filter_radius = c.filter_radius
+        e.sigma_space2_inv_half = c.sigma_space2_inv_half
+        e.sigma_depth2_inv_half = c.sigma_depth2_inv_half
+        e.depth_threshold = c.depth_threshold
+        e.dist_threshold = c.dist_threshold
+        e.integration_threshold = c.integration_threshold
+        return e
+
+
+_orc = None
+_ref = None
+
+
+def oracle():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORACLE_SO):
+            build(reference=False)
+        L = C.CDLL(ORACLE_SO)
+        sig = {
+            "oracle_expf": (C.c_float, [C.c_float]),
+            "orc_pass_filter": (None, [_P, C.c_long, C.c_float, C.c_float, _P]),
+            "orc_gaussian_table": (None, [C.c_int, C.c_float, _P]),
+            "orc_bilateral": (None, [_P, C.c_int, C.c_int, _P, C.c_int, C.c_float, C.c_float, _P]),
+            "orc_half_sample": (None, [_P, C.c_int, C.c_int, C.c_int, C.c_float, _P]),
+            "orc_depth2vertex": (None, [_P, C.c_int, C.c_int, _P, C.c_int, _P]),
+            "orc_normals": (None, [_P, C.c_int, C.c_int, C.c_float, _P]),
+            "orc_transform_maps": (None, [_P, _P, C.c_int, C.c_int, _P, _P, _P]),
+            "orc_scale_depths": (None, [_P, C.c_int, C.c_int, _P]),
+            "orc_tsdf_init": (None, [_P, _P, C.c_long]),
+            "orc_tsdf_integrate": (None, [_P, _P, _P, _P, _P, _P, _P, C.c_int, _P]),
+            "orc_raycast": (None, [_P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P, _P]),
+            "orc_icp_rows": (None, [_P, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, C.c_float, _P, _P]),
+            "orc_inverse3": (None, [_P, _P]),
+            "orc_make_xform": (None, [_P, _P, _P]),
+            "orc_icp": (C.c_int, [_P, _P, C.c_int, _P, _P, _P, _P, C.c_float, _P, _P, _P]),
+            "orc_marching_cubes": (C.c_long, [_P, _P, _P, _P, _P, _P, C.c_long]),
+            "orc_scan_compact": (C.c_long, [_P, C.c_long, _P, _P]),
+            "orc_engine_create": (_P, [_P]),
+            "orc_engine_destroy": (None, [_P]),
+            "orc_engine_frame": (C.c_int, [_P, _P, _P]),
+            "orc_engine_pose": (None, [_P, _P, _P]),
+            "orc_engine_volume": (_P, [_P]),
+            "orc_engine_color_volume": (_P, [_P]),
+            "orc_engine_refmap": (_P, [_P, C.c_int]),
+            "orc_engine_tsdf_params": (None, [_P, _P]),
+            "orc_engine_icp_stats": (None, [_P, _P]),
+            "orc_engine_touched": (C.c_long, [_P]),
+        }
+        for k, (r, a) in sig.items():
+            f = getattr(L, k)
+            f.restype = r
+            f.argtypes = a
+        _orc = L
+    return _orc
+
+
+def ref_available():
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            raise RuntimeError("oracle/_ref/libnui_ref.so is not built (needs the reference tree)")
+        L = C.CDLL(REF_SO)
+        sig = {
+            "ref_pass_filter": (None, [_P, _P, C.c_long, C.c_float, C.c_float]),
+            "ref_bilateral": (None, [_P, _P, _P, C.c_int, C.c_int, C.c_uint, C.c_float, C.c_float]),
+            "ref_depth2vertex": (None, [_P, _P, _P, C.c_int, C.c_int, C.c_int]),
+            "ref_half_sample": (None, [_P, _P, C.c_int, C.c_int, C.c_uint, C.c_float]),
+            "ref_transform_maps": (None, [_P, _P, _P, _P, _P, C.c_int, C.c_int]),
+            "ref_normals_simple": (None, [_P, _P, C.c_int, C.c_int, C.c_float]),
+            "ref_scale_depths": (None, [_P, _P, C.c_int, C.c_int]),
+            "ref_integrate": (None, [_P, _P, _P, _P, _P, _P, _P, C.c_uint8]),
+            "ref_init_volume": (None, [_P, _P, _P]),
+            "ref_raycast": (None, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int]),
+            "ref_marching_cubes": (C.c_int, [_P, _P, _P, _P, _P]),
+            "ref_icp_iteration": (None, [_P, _P, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_float, _P]),
+        }
+        for k, (r, a) in sig.items():
+            f = getattr(L, k)
+            f.restype = r
+            f.argtypes = a
+        _ref = L
+    return _ref
+
+
+def make_xform(R, t):
+    x = OrcXform()
+    Rf = np.ascontiguousarray(R, np.float32).reshape(9)
+    tf = np.ascontiguousarray(t, np.float32).reshape(3)
+    oracle().orc_make_xform(p(Rf), p(tf), C.byref(x))
+    return x
+
+
+class Engine:
+    """The oracle's frame driver (RunTracking over the dense scene)."""
+
+    def __init__(self, session_cfg):
+        self.cfg = OrcEngineCfg.from_session_cfg(session_cfg)
+        self.h = oracle().orc_engine_create(C.byref(self.cfg))
+        t = OrcTsdf()
+        oracle().orc_engine_tsdf_params(self.h, C.byref(t))
+        self.tsdf = t
+        self.nvox = session_cfg.res[0] * session_cfg.res[1] * session_cfg.res[2]
+        self.W, self.H = session_cfg.width, session_cfg.height
+
+    def __del__(self):
+        try:
+            oracle().orc_engine_destroy(self.h)
+        except Exception:
+            pass
+
+    def frame(self, depth, bgra=None):
+        return oracle().orc_engine_frame(self.h, p(depth), p(bgra)) == 0
+
+    def pose(self):
+        R = np.zeros(9, np.float32)
+        t = np.zeros(3, np.float32)
+        oracle().orc_engine_pose(self.h, p(R), p(t))
+        return R.reshape(3, 3), t
+
+    def volume(self):
+        ptr_ = oracle().orc_engine_volume(self.h)
+        return np.ctypeslib.as_array(C.cast(ptr_, C.POINTER(C.c_int16)), shape=(self.nvox, 2)).copy()
+
+    def refmap(self, which):
+        ptr_ = oracle().orc_engine_refmap(self.h, which)
+        return np.ctypeslib.as_array(C.cast(ptr_, C.POINTER(C.c_float)), shape=(self.H, self.W, 3)).copy()
+
+    def icp_stats(self):
+        s = OrcIcpStats()
+        oracle().orc_engine_icp_stats(self.h, C.byref(s))
+        return s
+
+    def touched(self):
+        return oracle().orc_engine_touched(self.h)

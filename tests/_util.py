@@ -1,0 +1,77 @@
+"""Shared helpers of the tests: synthetic frames and the oracle pipeline pieces."""
+import ctypes as C
+
+import numpy as np
+
+from natureuserinterfacestudio_b200 import _lib as L
+from oracle import oracle as O
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint32 if a.dtype == np.float32 else np.uint16)
+
+
+def same_bits(a, b):
+    """Bit-exact float comparison (NaN == NaN when the bit patterns agree)."""
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    na, nb = np.isnan(a), np.isnan(b)
+    if not np.array_equal(na, nb):
+        return False
+    return np.array_equal(a[~na].view(np.uint32), b[~nb].view(np.uint32))
+
+
+def frames(n, W=640, H=480, seed=3, noise=True, color=False, deg=2.0, kind=L.SYNTH_TABLETOP, extent=3.0):
+    sc = L.SynthScene(kind, seed=seed, extent=extent)
+    out = []
+    f = 525.0 * W / 640.0
+    cx, cy = (W - 1) / 2.0, (H - 1) / 2.0
+    for i in range(n):
+        R, t = sc.pose(i, radius=extent / 2, deg_per_frame=deg)
+        d, c = sc.render(R, t, W, H, fx=f, fy=f, cx=cx, cy=cy, frame=i, noise=noise, color=color)
+        out.append((d, c, R, t))
+    return out
+
+
+def cfg_for(W=640, H=480, res=(256, 256, 256), dim=3.0, fmt=L.TSDF_I16, color=False, iters=(10, 5, 4),
+            trunc=0.046875, integ_thr=0.0):
+    f = 525.0 * W / 640.0
+    return L.default_cfg(width=W, height=H, fx=f, fy=f, cx=(W - 1) / 2.0, cy=(H - 1) / 2.0, res=res,
+                         dim=(dim, dim, dim), tsdf_format=fmt, color_volume=1 if color else 0,
+                         iterations=list(iters) + [0] * (4 - len(iters)), levels=len(iters), trunc_dist=trunc,
+                         integration_threshold=integ_thr)
+
+
+def oracle_preprocess(raw, cfg):
+    """Oracle pass filter + bilateral + vertex + pyramid + scaled depth of one frame."""
+    orc = O.oracle()
+    W, H = cfg.width, cfg.height
+    N = W * H
+    cam = O.OrcCam.make(W, H, cfg.fx, cfg.fy, cfg.cx, cfg.cy, cfg.depth_min, cfg.depth_max)
+    a = np.zeros(N, np.float32)
+    orc.orc_pass_filter(O.p(raw.reshape(-1)), N, cfg.depth_min, cfg.depth_max, O.p(a))
+    g = np.zeros(2 * cfg.filter_radius + 1, np.float32)
+    orc.orc_gaussian_table(cfg.filter_radius, cfg.sigma_space2_inv_half, O.p(g))
+    f = np.zeros(N, np.float32)
+    orc.orc_bilateral(O.p(a), W, H, O.p(g), cfg.filter_radius, cfg.sigma_depth2_inv_half, cfg.depth_threshold,
+                      O.p(f))
+    v = np.zeros(N * 3, np.float32)
+    orc.orc_depth2vertex(O.p(f), W, H, C.byref(cam), 1, O.p(v))
+    s = a.copy()
+    orc.orc_scale_depths(O.p(s), W, H, C.byref(cam))
+    levels = [(f.reshape(H, W), v.reshape(H, W, 3))]
+    src = f
+    for l in range(1, cfg.levels):
+        h = np.zeros((W >> l) * (H >> l), np.float32)
+        orc.orc_half_sample(O.p(src), W >> l, H >> l, 1, cfg.depth_threshold, O.p(h))
+        vv = np.zeros(h.size * 3, np.float32)
+        orc.orc_depth2vertex(O.p(h), W >> l, H >> l, C.byref(cam), 1 << l, O.p(vv))
+        levels.append((h.reshape(H >> l, W >> l), vv.reshape(H >> l, W >> l, 3)))
+        src = h
+    return dict(passd=a.reshape(H, W), scaled=s.reshape(H, W), levels=levels, cam=cam)
+
+
+def rot_angle(Ra, Rb):
+    M = np.asarray(Ra, np.float64).T @ np.asarray(Rb, np.float64)
+    c = np.clip((np.trace(M) - 1) / 2, -1, 1)
+    return float(np.arccos(c))
