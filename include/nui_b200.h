@@ -148,6 +148,9 @@ NUI_API nui_status nui_get_pose(nui_session* s, float* pose12);
  * NUI_ERR_MESH_OVERFLOW is returned (with the first cap vertices written) when it
  * exceeds cap. */
 NUI_API nui_status nui_mesh(nui_session* s, float* pos, float* col, uint64_t cap, uint64_t* nverts);
+/* Marching-cubes case index of every cube, (res[0]-1)*(res[1]-1)*(res[2]-1) bytes in the
+ * same (y, x, z) order; 0 for cubes skipped because a corner has no weight. */
+NUI_API nui_status nui_mesh_cases(nui_session* s, uint8_t* cases, size_t bytes, uint64_t* nverts);
 
 /* Debug / test readback of session buffers into host memory.  `what`:
  *   0 filtered depth L0 (f32, W*H)      1 scaled depth for integration (f32, W*H)

@@ -5,6 +5,7 @@ raises -- there is no CPU fallback.
 """
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -70,6 +71,7 @@ _SIGS = {
     "nui_set_pose": (C.c_int, [_P, _P]),
     "nui_get_pose": (C.c_int, [_P, _P]),
     "nui_mesh": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
+    "nui_mesh_cases": (C.c_int, [_P, _P, C.c_size_t, _P]),
     "nui_debug_download": (C.c_int, [_P, C.c_int, C.c_int, _P, C.c_size_t]),
     "nui_debug_upload_volume": (C.c_int, [_P, _P]),
     "nui_batch_tick": (C.c_int, [_P, _P, C.c_int, _P, _P, _P, _P]),
@@ -135,9 +137,14 @@ class Context:
         h = C.c_void_p()
         check(lib().nui_ctx_create(device, C.byref(h)))
         self.h = h
+        self._sessions = weakref.WeakSet()
 
     def close(self):
+        """Destroys the context; sessions still open on it are closed first (a session
+        must never outlive its context)."""
         if self.h:
+            for s in list(self._sessions):
+                s.close()
             lib().nui_ctx_destroy(self.h)
             self.h = None
 
@@ -187,14 +194,15 @@ class Session:
         check(lib().nui_session_create(ctx.h, C.byref(cfg), C.byref(h)))
         self.h = h
         self.ctx = ctx
+        ctx._sessions.add(self)
         self.cfg = cfg
         self.W, self.H = cfg.width, cfg.height
         self.res = tuple(cfg.res)
 
     def close(self):
-        if self.h:
+        if self.h and self.ctx.h:
             lib().nui_session_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -286,6 +294,13 @@ class Session:
             check(r)
         k = min(n.value, cap)
         return pos[:k], col[:k], n.value
+
+    def mesh_cases(self):
+        rx, ry, rz = self.res
+        out = np.zeros((ry - 1) * (rx - 1) * (rz - 1), np.uint8)
+        n = C.c_uint64()
+        check(lib().nui_mesh_cases(self.h, ptr(out), out.nbytes, C.byref(n)))
+        return out, n.value
 
 
 # ------------------------------------------------------------------ synthetic input

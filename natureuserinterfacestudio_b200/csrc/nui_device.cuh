@@ -41,7 +41,7 @@ struct TrackState {
   int iterations_run;
   float lastR[9], lastT[3];  // pose of the last integration
   unsigned int block_counter;
-  unsigned int pad_;
+  int dmax_bits;         // largest ray-length depth of the frame (float bits, >= 0)
   unsigned long long touched;
 };
 

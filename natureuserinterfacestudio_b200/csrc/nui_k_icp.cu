@@ -323,7 +323,6 @@ __global__ void k_track_finalize(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.x];
   if (threadIdx.x != 0 || s.kind < 0) return;
   TrackState* ts = s.ts;
-  ts->touched = 0ull;
   if (s.kind == kFirstFrame) {
     ts->integrate = ts->status == 0 ? 1 : 0;
     return;

@@ -44,7 +44,9 @@ __global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc
   }
   __syncthreads();
   const int x = tx0 + threadIdx.x, y = ty0 + threadIdx.y;
-  if (x >= W || y >= H) return;
+  const bool inside = x < W && y < H;
+  float sc = qnan();
+  if (inside) {
   const float c = tile[threadIdx.y + R][threadIdx.x + R];
   float out = qnan();
   if (!isnan(c)) {
@@ -75,9 +77,14 @@ __global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc
   s.vlev[0][i] = v;
   // ray-length depth for integration: the pass-filtered depth, not the bilateral output
   // (NuiKinfuOpenCLScene.cpp:218 passes GetDepthBuffer())
-  float sc = c;
+  sc = c;
   if (!isnan(c)) sc = c * sqrtf(xl * xl + yl * yl + 1.f);
   s.dscaled[i] = sc;
+  }
+  // frame maximum of the ray-length depth: bounds the voxels integration has to visit
+  float m = isnan(sc) ? 0.f : sc;
+  for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0 && m > 0.f && s.ts) atomicMax(&s.ts->dmax_bits, __float_as_int(m));
 }
 
 // One pyramid level: dst(x,y) = mean of the 3x3 taps around src(2x,2y) within the depth

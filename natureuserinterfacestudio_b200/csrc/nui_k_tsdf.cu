@@ -51,20 +51,59 @@ __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* _
   const float dx = Ri[2] * c2 * fx;
   const float dy = Ri[5] * c2 * fy;
   const float r8 = Ri[8];
-  for (int z = 0; z < z0; ++z) {
+  const int W = s.W, H = s.H;
+  // Conservative z interval of this column: only voxels whose exact projection can land
+  // inside the image (1.5 px margin) in front of the camera, and whose distance from the
+  // camera can be within the frame's largest ray length + trunc, can be updated.  The
+  // bounds come from the same affine recurrences the exact test uses, evaluated in
+  // double; one voxel of margin on each side absorbs the float rounding of the running
+  // sums, so every voxel outside the interval also fails the exact test below.
+  int kb = z0, ke = z1;
+  {
+    const double X0 = v_x, dX = dx, Y0 = v_y, dY = dy, Z0 = v_z, dZ = (double)r8 * (double)c2;
+    double lo = 0.0, hi = (double)(rz - 1);
+    bool empty = false;
+    auto ge = [&](double a, double b) {  // a + b k >= 0
+      if (b > 0) lo = fmax(lo, -a / b);
+      else if (b < 0) hi = fmin(hi, -a / b);
+      else if (a < 0) empty = true;
+    };
+    const double m = 1.5;
+    ge(X0 + ((double)ccx + m) * Z0, dX + ((double)ccx + m) * dZ);
+    ge(-(X0 + ((double)ccx - (double)W - m) * Z0), -(dX + ((double)ccx - (double)W - m) * dZ));
+    ge(Y0 + ((double)ccy + m) * Z0, dY + ((double)ccy + m) * dZ);
+    ge(-(Y0 + ((double)ccy - (double)H - m) * Z0), -(dY + ((double)ccy - (double)H - m) * dZ));
+    ge(Z0, dZ);
+    const double rmax = (double)__int_as_float(s.ts->dmax_bits) + (double)trunc + 2.0 * (double)c2;
+    const double s2 = rmax * rmax - (double)part;
+    if (s2 < 0) {
+      empty = true;
+    } else {
+      const double sr = sqrt(s2);
+      ge((double)vgz + sr, (double)c2);
+      ge(sr - (double)vgz, -(double)c2);
+    }
+    if (empty || lo > hi) {
+      kb = ke = z0;
+    } else {
+      kb = max(z0, (int)floor(lo) - 1);
+      ke = min(z1, (int)ceil(hi) + 2);
+      if (ke < kb) ke = kb;
+    }
+  }
+  for (int z = 0; z < kb; ++z) {
     vgz += c2;
     zs += c2;
     v_x += dx;
     v_y += dy;
   }
-  const int W = s.W, H = s.H;
   const float fW = (float)W, fH = (float)H;
   const float* __restrict__ depth = s.dscaled;
   const size_t slice = (size_t)rx * ry;
-  size_t idx = (size_t)vx + (size_t)rx * vy + slice * (size_t)z0;
+  size_t idx = (size_t)vx + (size_t)rx * vy + slice * (size_t)kb;
   unsigned int touched = 0;
 
-  for (int zb = z0; zb < z1; zb += kZUnroll) {
+  for (int zb = kb; zb < ke; zb += kZUnroll) {
     float sdf[kZUnroll];
     int pix[kZUnroll];
     bool ok[kZUnroll];
@@ -73,8 +112,8 @@ __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* _
       ok[u] = false;
       pix[u] = 0;
       sdf[u] = 0.f;
-      if (zb + u < z1) {
-        const float inv_z = 1.0f / (v_z + r8 * zs);
+      if (zb + u < ke) {
+        const float inv_z = __frcp_rn(v_z + r8 * zs);
         if (!(inv_z < 0.f)) {
           const float px = roundf(v_x * inv_z + ccx);
           const float py = roundf(v_y * inv_z + ccy);

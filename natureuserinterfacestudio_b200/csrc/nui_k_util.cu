@@ -20,6 +20,16 @@ __global__ void k_publish(const SessionDesc* __restrict__ descs, int n, float* p
   pose[14 * i + 13] = ts->count;
 }
 
+// Start of a tick: clear the per-frame counters of every active session.
+__global__ void k_tick_begin(const SessionDesc* __restrict__ descs, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const SessionDesc& s = descs[i];
+  if (s.kind < 0 || !s.ts) return;
+  s.ts->dmax_bits = 0;
+  s.ts->touched = 0ull;
+}
+
 template <int FMT>
 __global__ void k_export_ref(const SessionDesc* __restrict__ descs, short2* out, uchar4* cout) {
   const SessionDesc& s = descs[0];

@@ -35,6 +35,7 @@ __global__ void k_volume_init(const SessionDesc*);
 template <int F>
 __global__ void k_raycast(const SessionDesc*);
 __global__ void k_publish(const SessionDesc*, int, float*, int*);
+__global__ void k_tick_begin(const SessionDesc*, int);
 template <int F>
 __global__ void k_export_ref(const SessionDesc*, short2*, uchar4*);
 template <int F>
@@ -239,6 +240,7 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
     if (ev) cudaEventRecord(ctx->ev[i], st);
   };
   mark(0);
+  k_tick_begin<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n);
   const unsigned tiles = cdiv(p.maxW, 32) * cdiv(p.maxH, 8);
   k_preprocess<<<dim3(tiles, p.n), dim3(32, 8), 0, st>>>(d);
   mark(1);
@@ -676,6 +678,7 @@ nui_status run_stage(nui_session* s, int what) {
   cudaStream_t st = ctx->stream;
   const SessionDesc* dd = s->d_desc1;
   if (what == 0) {
+    k_tick_begin<<<1, 64, 0, st>>>(dd, 1);
     k_preprocess<<<dim3(cdiv(p.maxW, 32) * cdiv(p.maxH, 8), 1), dim3(32, 8), 0, st>>>(dd);
     for (int l = 1; l < p.maxLevels; ++l)
       k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), 1), 256, 0, st>>>(dd, l);
@@ -919,10 +922,99 @@ NUI_API nui_status nui_k_feedback_maps(nui_ctx* ctx, const float* d_vertex4, int
 
 }  // extern "C"
 
+// ------------------------------------------------------------------ marching cubes
+namespace nui {
+void mc_upload_tables(cudaStream_t st);
+template <int F>
+__global__ void k_mc_count(const SessionDesc*, unsigned int*, unsigned long long*, uint8_t*);
+__global__ void k_mc_scan(unsigned long long*, int);
+template <int F>
+__global__ void k_mc_emit(const SessionDesc*, const unsigned int*, const unsigned long long*, float*, float*,
+                          unsigned long long);
+}  // namespace nui
+
+namespace {
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+template <int F>
+void mc_count(nui_session* s, unsigned nb, unsigned* cc, unsigned long long* bt, uint8_t* cases) {
+  k_mc_count<F><<<nb, 128, 0, s->ctx->stream>>>(s->d_desc1, cc, bt, cases);
+}
+template <int F>
+void mc_emit(nui_session* s, unsigned nb, const unsigned* cc, const unsigned long long* bt, float* p, float* c,
+             unsigned long long cap) {
+  k_mc_emit<F><<<nb, 128, 0, s->ctx->stream>>>(s->d_desc1, cc, bt, p, c, cap);
+}
+// Count pass + block scan; returns the total vertex count.
+nui_status mc_prepare(nui_session* s, DevBuf& cc, DevBuf& bt, unsigned& nb, uint8_t* d_cases,
+                      unsigned long long& total) {
+  const nui_session_cfg& c = s->cfg;
+  cudaStream_t st = s->ctx->stream;
+  SessionDesc d;
+  fill_desc(s, d, kInactive, nullptr, nullptr);
+  NUI_CUDA(cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, st));
+  mc_upload_tables(st);
+  const unsigned tilesX = cdiv(c.res[0] - 1, 128);
+  nb = tilesX * (unsigned)(c.res[1] - 1);
+  NUI_CUDA(cudaMalloc(&cc.p, sizeof(unsigned) * (size_t)(c.res[0] - 1) * (c.res[1] - 1)));
+  NUI_CUDA(cudaMalloc(&bt.p, sizeof(unsigned long long) * (nb + 1)));
+  switch (c.tsdf_format) {
+    case 0: mc_count<0>(s, nb, (unsigned*)cc.p, (unsigned long long*)bt.p, d_cases); break;
+    case 1: mc_count<1>(s, nb, (unsigned*)cc.p, (unsigned long long*)bt.p, d_cases); break;
+    case 2: mc_count<2>(s, nb, (unsigned*)cc.p, (unsigned long long*)bt.p, d_cases); break;
+    case 3: mc_count<3>(s, nb, (unsigned*)cc.p, (unsigned long long*)bt.p, d_cases); break;
+  }
+  k_mc_scan<<<1, 1024, 0, st>>>((unsigned long long*)bt.p, (int)nb);
+  NUI_CUDA(cudaGetLastError());
+  NUI_CUDA(cudaMemcpyAsync(&total, (unsigned long long*)bt.p + nb, sizeof(total), cudaMemcpyDeviceToHost, st));
+  NUI_CUDA(cudaStreamSynchronize(st));
+  return NUI_OK;
+}
+}  // namespace
+
 extern "C" NUI_API nui_status nui_mesh(nui_session* s, float* pos, float* col, uint64_t cap, uint64_t* nverts) {
-  (void)pos;
-  (void)col;
-  (void)cap;
   if (!s || !nverts) return fail(NUI_ERR_INVALID_ARG, "null argument");
-  return fail(NUI_ERR_UNSUPPORTED, "marching cubes not built");
+  DevBuf cc, bt, dp, dc;
+  unsigned nb = 0;
+  unsigned long long total = 0;
+  nui_status st = mc_prepare(s, cc, bt, nb, nullptr, total);
+  if (st != NUI_OK) return st;
+  *nverts = total;
+  const unsigned long long k = total < cap ? total : cap;
+  if (k > 0 && (pos || col)) {
+    if (pos) NUI_CUDA(cudaMalloc(&dp.p, k * 3 * sizeof(float)));
+    if (col) NUI_CUDA(cudaMalloc(&dc.p, k * 4 * sizeof(float)));
+    switch (s->cfg.tsdf_format) {
+      case 0: mc_emit<0>(s, nb, (unsigned*)cc.p, (unsigned long long*)bt.p, (float*)dp.p, (float*)dc.p, k); break;
+      case 1: mc_emit<1>(s, nb, (unsigned*)cc.p, (unsigned long long*)bt.p, (float*)dp.p, (float*)dc.p, k); break;
+      case 2: mc_emit<2>(s, nb, (unsigned*)cc.p, (unsigned long long*)bt.p, (float*)dp.p, (float*)dc.p, k); break;
+      case 3: mc_emit<3>(s, nb, (unsigned*)cc.p, (unsigned long long*)bt.p, (float*)dp.p, (float*)dc.p, k); break;
+    }
+    NUI_CUDA(cudaGetLastError());
+    if (pos) NUI_CUDA(cudaMemcpyAsync(pos, dp.p, k * 3 * sizeof(float), cudaMemcpyDeviceToHost, s->ctx->stream));
+    if (col) NUI_CUDA(cudaMemcpyAsync(col, dc.p, k * 4 * sizeof(float), cudaMemcpyDeviceToHost, s->ctx->stream));
+    NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  }
+  if (total > cap) return fail(NUI_ERR_MESH_OVERFLOW, "mesh larger than the output capacity");
+  return NUI_OK;
+}
+
+extern "C" NUI_API nui_status nui_mesh_cases(nui_session* s, uint8_t* cases, size_t bytes, uint64_t* nverts) {
+  if (!s || !cases) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  const nui_session_cfg& c = s->cfg;
+  const size_t need = (size_t)(c.res[0] - 1) * (c.res[1] - 1) * (c.res[2] - 1);
+  if (bytes < need) return fail(NUI_ERR_INVALID_ARG, "buffer too small");
+  DevBuf cc, bt, dcase;
+  NUI_CUDA(cudaMalloc(&dcase.p, need));
+  unsigned nb = 0;
+  unsigned long long total = 0;
+  nui_status st = mc_prepare(s, cc, bt, nb, (uint8_t*)dcase.p, total);
+  if (st != NUI_OK) return st;
+  NUI_CUDA(cudaMemcpy(cases, dcase.p, need, cudaMemcpyDeviceToHost));
+  if (nverts) *nverts = total;
+  return NUI_OK;
 }

@@ -72,6 +72,8 @@ def oracle_preprocess(raw, cfg):
 
 
 def rot_angle(Ra, Rb):
+    """Angle of Ra^T Rb, robust near zero (atan2 of the skew and symmetric parts)."""
     M = np.asarray(Ra, np.float64).T @ np.asarray(Rb, np.float64)
-    c = np.clip((np.trace(M) - 1) / 2, -1, 1)
-    return float(np.arccos(c))
+    s = 0.5 * np.linalg.norm([M[2, 1] - M[1, 2], M[0, 2] - M[2, 0], M[1, 0] - M[0, 1]])
+    c = (np.trace(M) - 1) / 2
+    return float(np.arctan2(s, c))

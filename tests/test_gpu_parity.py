@@ -151,3 +151,37 @@ def test_batched_equals_alone(gpu_ctx):
             assert np.array_equal(poses[k], alone[k][0][i]), (i, k)
     for k in range(3):
         assert np.array_equal(ss[k].volume_ref_layout(), alone[k][1])
+
+
+def _volume_after(seq, cfg, n):
+    eng = O.Engine(cfg)
+    for d, _, _, _ in seq[:n]:
+        assert eng.frame(d)
+    return eng
+
+
+@pytest.mark.parametrize("res", [(96, 96, 96), (130, 97, 71)])
+def test_marching_cubes_bit_exact_and_ordered(gpu_ctx, seq, res):
+    cfg = cfg_for(res=res)
+    eng = _volume_after(seq, cfg, 3)
+    vol = eng.volume()
+    s = L.Session(gpu_ctx, cfg)
+    s.upload_volume(vol)
+    rx, ry, rz = res
+    ncube = (rx - 1) * (ry - 1) * (rz - 1)
+    cases_o = np.zeros(ncube, np.uint8)
+    cap = 3_000_000
+    pos_o = np.zeros((cap, 3), np.float32)
+    n_o = O.oracle().orc_marching_cubes(O.p(vol), None, C.byref(eng.tsdf), O.p(cases_o), O.p(pos_o), None, cap)
+    cases_g, n_g = s.mesh_cases()
+    assert n_g == n_o > 0
+    assert np.array_equal(cases_g, cases_o)
+    pos_g, col_g, n2 = s.mesh(cap)
+    assert n2 == n_o
+    assert same_bits(pos_g, pos_o[:n_o])
+    assert np.all(col_g[:, 3] == 1.0)
+    # overflow: the first `cap` vertices, and the status says so
+    small = n_o // 3
+    pos_s, _, n3 = s.mesh(small)
+    assert n3 == n_o and len(pos_s) == small
+    assert same_bits(pos_s, pos_o[:small])
