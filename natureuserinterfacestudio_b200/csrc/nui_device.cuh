@@ -13,6 +13,7 @@ namespace nui {
 constexpr int kMaxLevels = 4;
 constexpr int kMaxRadius = 7;
 constexpr int kIcpTerms = 29;  // 21 JtJ + 6 Jtr + r^2 + count  (icp.cl:122-160)
+constexpr int kTile = 16;      // pixel tile of the depth bound used by integration culling
 
 // Camera intrinsics block (gpu_def.h:13-27).
 struct DevCam {
@@ -70,6 +71,7 @@ struct SessionDesc {
   float4* vref;                   // world-space reference vertex map (W x H)
   float4* nref;                   // world-space reference normal map
   uchar4* cmap;                   // reference colour map (nullable)
+  float* tile_max;                // per 16x16 pixel tile: largest ray-length depth (0 = none)
   // dense volume
   int fmt;                        // nui_tsdf_format
   int res[3];
@@ -77,6 +79,7 @@ struct SessionDesc {
   void* vol;                      // format storage, x-fastest: x + rx*(y + ry*z)
   uint8_t* wvol;                  // weight plane of NUI_TSDF_F16_U8
   uchar4* cvol;                   // colour volume (nullable), same layout
+  uint8_t* occ;                   // per 8^3 brick: 1 once any voxel of it has weight > 0
   int max_cw;
   int zchunks;                    // integration: z chunks per column (one thread each)
   // tracking state and ICP scratch
@@ -201,6 +204,21 @@ struct Voxel<3> {  // NUI_TSDF_F16_F16: half2 (tsdf, weight)
 
 __device__ __forceinline__ size_t vox_index(const SessionDesc& s, int x, int y, int z) {
   return (size_t)x + (size_t)s.res[0] * ((size_t)y + (size_t)s.res[1] * (size_t)z);
+}
+// Occupancy bricks of 8^3 voxels.  Weights never decrease between resets, so a brick
+// whose byte is 0 holds only weight-0 voxels and readers may skip its loads.
+__device__ __forceinline__ size_t occ_index(const SessionDesc& s, int x, int y, int z) {
+  const size_t bx = (size_t)(s.res[0] + 7) >> 3, by = (size_t)(s.res[1] + 7) >> 3;
+  return (size_t)(x >> 3) + bx * ((size_t)(y >> 3) + by * (size_t)(z >> 3));
+}
+// round(p / c) for a voxel coordinate, exactly as the IEEE quotient would round: the
+// product with 1/c is within 2 ulp of the quotient, so unless it lies within 4 ulp of a
+// rounding boundary (n + 0.5) both round alike; otherwise divide.
+__device__ __forceinline__ int round_div(float p, float c, float inv) {
+  const float q = p * inv;
+  const float f = q - floorf(q);
+  if (fabsf(f - 0.5f) > fabsf(q) * 4.8e-7f + 1e-6f) return (int)roundf(q);
+  return (int)roundf(p / c);
 }
 
 }  // namespace nui

@@ -27,6 +27,7 @@ void mc_upload_tables(cudaStream_t st) {
 
 template <int FMT>
 __device__ __forceinline__ bool corner(const SessionDesc& s, int x, int y, int z, float& f) {
+  if (s.occ && __ldg(s.occ + occ_index(s, x, y, z)) == 0) return false;  // brick never weighted
   int w;
   Voxel<FMT>::load(s, vox_index(s, x, y, z), f, w);
   return w > 0;

@@ -3,8 +3,10 @@
 //  k_preprocess   depth_passing_filter_kernel (filters.cl:9-23) + bilateral_filter_depth_kernel
 //                 (bilateralFilter.cl:68-119) + depth2vertex_kernel at level 0
 //                 (transformMaps.cl:18-42) + scaleDepthsKernel (tsdfVolume.cl:8-29), fused.
-//                 One block per 32x8 output tile; the pass-filtered depth of the tile and
+//                 One block per 32x16 output tile; the pass-filtered depth of the tile and
 //                 its radius-r halo is staged in shared memory once and read 49 times.
+//                 Also writes the largest ray-length depth of each 16x16 tile (integration
+//                 uses it to skip voxels that are behind every surface they can project to).
 //  k_pyramid      half_sample_kernel (transformMaps.cl:44-88) + depth2vertex_kernel for one
 //                 pyramid level.
 //  k_feedback     estimate_normals_simple_kernel (normalEstimation.cl:770-822) +
@@ -16,7 +18,7 @@
 
 namespace nui {
 
-constexpr int kPreTX = 32, kPreTY = 8;
+constexpr int kPreTX = 32, kPreTY = 16;
 
 __global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
@@ -81,10 +83,21 @@ __global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc
   if (!isnan(c)) sc = c * sqrtf(xl * xl + yl * yl + 1.f);
   s.dscaled[i] = sc;
   }
-  // frame maximum of the ray-length depth: bounds the voxels integration has to visit
+  // largest ray-length depth of each 16x16 tile (lanes 0-15 / 16-31 of a row are two
+  // tiles) and of the frame: the bounds integration culls with
   float m = isnan(sc) ? 0.f : sc;
-  for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
-  if ((threadIdx.x & 31) == 0 && m > 0.f && s.ts) atomicMax(&s.ts->dmax_bits, __float_as_int(m));
+  for (int off = 8; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+  __shared__ float rowmax[kPreTY][2];
+  if ((threadIdx.x & 15) == 0) rowmax[threadIdx.y][threadIdx.x >> 4] = m;
+  __syncthreads();
+  if (threadIdx.y == 0 && threadIdx.x < 2) {
+    float t = 0.f;
+    for (int r = 0; r < kPreTY; ++r) t = fmaxf(t, rowmax[r][threadIdx.x]);
+    const int tcol = tx0 / kTile + threadIdx.x, trow = ty0 / kTile;
+    const int ntx = (W + kTile - 1) / kTile;
+    if (s.tile_max && tcol < ntx) s.tile_max[trow * ntx + tcol] = t;
+    if (t > 0.f && s.ts) atomicMax(&s.ts->dmax_bits, __float_as_int(t));
+  }
 }
 
 // One pyramid level: dst(x,y) = mean of the 3x3 taps around src(2x,2y) within the depth

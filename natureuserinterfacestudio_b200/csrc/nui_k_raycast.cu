@@ -16,15 +16,25 @@ struct RayVol {
   const SessionDesc& s;
   int rx, ry, rz;
   float c0, c1, c2;
+  float i0, i1, i2;  // 1 / cell
+  // tsdf of a voxel if its weight is > 0; bricks never touched are answered from the
+  // occupancy map without reading the voxel
   __device__ __forceinline__ bool tsdf_at(int x, int y, int z, float& f) const {
+    if (s.occ && __ldg(s.occ + occ_index(s, x, y, z)) == 0) return false;
+    const size_t i = vox_index(s, x, y, z);
+    if (FMT == 2) {  // weight plane first: the tsdf plane is read only for weighted voxels
+      if (__ldg(s.wvol + i) == 0) return false;
+      f = __half2float(reinterpret_cast<const __half*>(s.vol)[i]);
+      return true;
+    }
     int W;
-    Voxel<FMT>::load(s, vox_index(s, x, y, z), f, W);
+    Voxel<FMT>::load(s, i, f, W);
     return W > 0;
   }
   __device__ __forceinline__ void voxel_of(float3 p, int& gx, int& gy, int& gz) const {
-    gx = (int)roundf(p.x / c0);
-    gy = (int)roundf(p.y / c1);
-    gz = (int)roundf(p.z / c2);
+    gx = round_div(p.x, c0, i0);
+    gy = round_div(p.y, c1, i1);
+    gz = round_div(p.z, c2, i2);
   }
   __device__ float trilinear(float3 p) const {
     int gx, gy, gz;
@@ -65,7 +75,8 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
   const float4 nanv = make_float4(qnan(), qnan(), qnan(), 0.f);
   float4 vout = nanv, nout = nanv;
   uchar4 cout = make_uchar4(0, 0, 0, 0);
-  const RayVol<FMT> V{s, s.res[0], s.res[1], s.res[2], s.cell[0], s.cell[1], s.cell[2]};
+  const RayVol<FMT> V{s, s.res[0], s.res[1], s.res[2], s.cell[0], s.cell[1], s.cell[2],
+                       1.0f / s.cell[0], 1.0f / s.cell[1], 1.0f / s.cell[2]};
   const DevXform& m = s.ts->xf;
   const float D0 = s.dim[0], D1 = s.dim[1], D2 = s.dim[2];
   const float3 off = f3(D0 / 2.0f, D1 / 2.0f, 0.f);

@@ -18,6 +18,7 @@ namespace nui {
 
 constexpr int kTsdfThreads = 256;
 constexpr int kZUnroll = 4;
+constexpr int kChunk = 16;  // z slices per occlusion test
 
 template <int FMT>
 __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* __restrict__ descs) {
@@ -100,73 +101,116 @@ __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* _
   const float fW = (float)W, fH = (float)H;
   const float* __restrict__ depth = s.dscaled;
   const size_t slice = (size_t)rx * ry;
-  size_t idx = (size_t)vx + (size_t)rx * vy + slice * (size_t)kb;
+  const int ntx = (W + kTile - 1) / kTile, nty = (H + kTile - 1) / kTile;
   unsigned int touched = 0;
 
-  for (int zb = kb; zb < ke; zb += kZUnroll) {
-    float sdf[kZUnroll];
-    int pix[kZUnroll];
-    bool ok[kZUnroll];
-#pragma unroll
-    for (int u = 0; u < kZUnroll; ++u) {
-      ok[u] = false;
-      pix[u] = 0;
-      sdf[u] = 0.f;
-      if (zb + u < ke) {
-        const float inv_z = __frcp_rn(v_z + r8 * zs);
-        if (!(inv_z < 0.f)) {
-          const float px = roundf(v_x * inv_z + ccx);
-          const float py = roundf(v_y * inv_z + ccy);
-          if (px >= 0.f && py >= 0.f && px < fW && py < fH) {
-            const int p = (int)py * W + (int)px;
-            const float Dp = __ldg(depth + p);
-            const float sd = Dp - sqrtf(vgz * vgz + part);
-            if (!isnan(Dp) && sd >= -trunc) {
-              ok[u] = true;
-              sdf[u] = sd;
-              pix[u] = p;
-            }
+  for (int zc = kb; zc < ke; zc += kChunk) {
+    const int zend = min(zc + kChunk, ke);
+    // Occlusion test of the chunk: bound the pixels its voxels project to (the segment
+    // between the projections of its end voxels, 2 px margin) and the largest ray length
+    // over those pixels' tiles; if even the chunk's nearest voxel is farther than that
+    // plus trunc, no voxel of the chunk passes sdf >= -trunc.
+    bool skip = false;
+    {
+      const float k0 = (float)(zc - kb), k1 = (float)(zend - 1 - kb);
+      const float za = v_z + r8 * (zs + k0 * c2), zb2 = v_z + r8 * (zs + k1 * c2);
+      if (za > 1e-3f && zb2 > 1e-3f) {
+        const float ua = (v_x + k0 * dx) / za + ccx, ub = (v_x + k1 * dx) / zb2 + ccx;
+        const float va = (v_y + k0 * dy) / za + ccy, vb = (v_y + k1 * dy) / zb2 + ccy;
+        const float u0 = fmaxf(fminf(ua, ub) - 2.f, 0.f), u1 = fminf(fmaxf(ua, ub) + 2.f, fW - 1.f);
+        const float w0_ = fmaxf(fminf(va, vb) - 2.f, 0.f), w1 = fminf(fmaxf(va, vb) + 2.f, fH - 1.f);
+        if (u0 > u1 || w0_ > w1) {
+          skip = true;  // projects outside the image
+        } else {
+          const int tx0 = (int)u0 / kTile, tx1 = (int)u1 / kTile, ty0 = (int)w0_ / kTile, ty1 = (int)w1 / kTile;
+          if ((tx1 - tx0 + 1) * (ty1 - ty0 + 1) <= 16 && tx1 < ntx && ty1 < nty) {
+            float mx = 0.f;
+            for (int ty = ty0; ty <= ty1; ++ty)
+              for (int tx = tx0; tx <= tx1; ++tx) mx = fmaxf(mx, __ldg(s.tile_max + ty * ntx + tx));
+            const float g0 = vgz + k0 * c2, g1 = vgz + k1 * c2;
+            const float gz = (g0 <= 0.f && g1 >= 0.f) ? 0.f : fminf(fabsf(g0), fabsf(g1));
+            const float dmin = sqrtf(part + gz * gz);
+            skip = dmin > mx + trunc + 1e-3f * (1.f + dmin);
           }
         }
+      }
+    }
+    if (skip) {
+      for (int z = zc; z < zend; ++z) {
         vgz += c2;
         zs += c2;
         v_x += dx;
         v_y += dy;
       }
+      continue;
     }
-    float F[kZUnroll];
-    int Wt[kZUnroll];
+    size_t idx = (size_t)vx + (size_t)rx * vy + slice * (size_t)zc;
+    for (int zb = zc; zb < zend; zb += kZUnroll) {
+      float sdf[kZUnroll];
+      int pix[kZUnroll];
+      bool ok[kZUnroll];
 #pragma unroll
-    for (int u = 0; u < kZUnroll; ++u)
-      if (ok[u]) Voxel<FMT>::load(s, idx + (size_t)u * slice, F[u], Wt[u]);
-#pragma unroll
-    for (int u = 0; u < kZUnroll; ++u) {
-      if (!ok[u]) continue;
-      const float tsdf = fminf(1.0f, sdf[u] * tinv);
-      const float tn = (F[u] * (float)Wt[u] + tsdf) / (float)(Wt[u] + 1);
-      const int wn = min(Wt[u] + 1, 128);
-      const size_t vi = idx + (size_t)u * slice;
-      Voxel<FMT>::store(s, vi, tn, wn);
-      ++touched;
-      if (s.cvol && s.bgra && fabsf(sdf[u]) < trunc) {
-        const uchar4 nc = reinterpret_cast<const uchar4*>(s.bgra)[pix[u]];
-        if (nc.w != 0) {
-          const uchar4 vc = s.cvol[vi];
-          const float wr = 1.f;
-          const float nx = ((float)(vc.x * vc.w) + wr * (float)nc.x) / ((float)vc.w + wr);
-          const float ny = ((float)(vc.y * vc.w) + wr * (float)nc.y) / ((float)vc.w + wr);
-          const float nz = ((float)(vc.z * vc.w) + wr * (float)nc.z) / ((float)vc.w + wr);
-          const unsigned char wnew = (unsigned char)(vc.w + 1);
-          uchar4 o;
-          o.x = (unsigned char)fminf(fmaxf(nx, 0.f), 255.f);
-          o.y = (unsigned char)fminf(fmaxf(ny, 0.f), 255.f);
-          o.z = (unsigned char)fminf(fmaxf(nz, 0.f), 255.f);
-          o.w = min((unsigned char)s.max_cw, wnew);
-          s.cvol[vi] = o;
+      for (int u = 0; u < kZUnroll; ++u) {
+        ok[u] = false;
+        pix[u] = 0;
+        sdf[u] = 0.f;
+        if (zb + u < zend) {
+          const float inv_z = __frcp_rn(v_z + r8 * zs);
+          if (!(inv_z < 0.f)) {
+            const float px = roundf(v_x * inv_z + ccx);
+            const float py = roundf(v_y * inv_z + ccy);
+            if (px >= 0.f && py >= 0.f && px < fW && py < fH) {
+              const int p = (int)py * W + (int)px;
+              const float Dp = __ldg(depth + p);
+              const float sd = Dp - sqrtf(vgz * vgz + part);
+              if (!isnan(Dp) && sd >= -trunc) {
+                ok[u] = true;
+                sdf[u] = sd;
+                pix[u] = p;
+              }
+            }
+          }
+          vgz += c2;
+          zs += c2;
+          v_x += dx;
+          v_y += dy;
         }
       }
+      float F[kZUnroll];
+      int Wt[kZUnroll];
+#pragma unroll
+      for (int u = 0; u < kZUnroll; ++u)
+        if (ok[u]) Voxel<FMT>::load(s, idx + (size_t)u * slice, F[u], Wt[u]);
+#pragma unroll
+      for (int u = 0; u < kZUnroll; ++u) {
+        if (!ok[u]) continue;
+        const float tsdf = fminf(1.0f, sdf[u] * tinv);
+        const float tn = (F[u] * (float)Wt[u] + tsdf) / (float)(Wt[u] + 1);
+        const int wn = min(Wt[u] + 1, 128);
+        const size_t vi = idx + (size_t)u * slice;
+        Voxel<FMT>::store(s, vi, tn, wn);
+        ++touched;
+        if (s.occ) s.occ[occ_index(s, vx, vy, zb + u)] = 1;
+        if (s.cvol && s.bgra && fabsf(sdf[u]) < trunc) {
+          const uchar4 nc = reinterpret_cast<const uchar4*>(s.bgra)[pix[u]];
+          if (nc.w != 0) {
+            const uchar4 vc = s.cvol[vi];
+            const float wr = 1.f;
+            const float nx = ((float)(vc.x * vc.w) + wr * (float)nc.x) / ((float)vc.w + wr);
+            const float ny = ((float)(vc.y * vc.w) + wr * (float)nc.y) / ((float)vc.w + wr);
+            const float nz = ((float)(vc.z * vc.w) + wr * (float)nc.z) / ((float)vc.w + wr);
+            const unsigned char wnew = (unsigned char)(vc.w + 1);
+            uchar4 o;
+            o.x = (unsigned char)fminf(fmaxf(nx, 0.f), 255.f);
+            o.y = (unsigned char)fminf(fmaxf(ny, 0.f), 255.f);
+            o.z = (unsigned char)fminf(fmaxf(nz, 0.f), 255.f);
+            o.w = min((unsigned char)s.max_cw, wnew);
+            s.cvol[vi] = o;
+          }
+        }
+      }
+      idx += (size_t)kZUnroll * slice;
     }
-    idx += (size_t)kZUnroll * slice;
   }
   // warp-aggregated count of voxels read-modify-written
   const unsigned int mask = __activemask();
@@ -182,6 +226,10 @@ __global__ void k_volume_init(const SessionDesc* __restrict__ descs) {
     Voxel<FMT>::init(s, i);
     if (s.cvol) s.cvol[i] = make_uchar4(0, 0, 0, 0);
   }
+  const size_t nb = (size_t)((s.res[0] + 7) >> 3) * ((s.res[1] + 7) >> 3) * ((s.res[2] + 7) >> 3);
+  if (s.occ)
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (size_t)gridDim.x * blockDim.x)
+      s.occ[i] = 0;
 }
 
 template __global__ void k_integrate<0>(const SessionDesc*);

@@ -54,6 +54,15 @@ __global__ void k_export_ref(const SessionDesc* __restrict__ descs, short2* out,
   }
 }
 
+// Clears the occupancy bytes of a session (before an import or at reset).
+__global__ void k_occ_clear(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[0];
+  if (!s.occ) return;
+  const size_t n = (size_t)((s.res[0] + 7) >> 3) * ((s.res[1] + 7) >> 3) * ((s.res[2] + 7) >> 3);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    s.occ[i] = 0;
+}
+
 template <int FMT>
 __global__ void k_import_ref(const SessionDesc* __restrict__ descs, const short2* in) {
   const SessionDesc& s = descs[0];
@@ -68,6 +77,7 @@ __global__ void k_import_ref(const SessionDesc* __restrict__ descs, const short2
       reinterpret_cast<short2*>(s.vol)[i] = v;
     else
       Voxel<FMT>::store(s, i, (float)v.x / 32766.f, v.y);
+    if (s.occ && v.y > 0) s.occ[occ_index(s, x, y, z)] = 1;
   }
 }
 

@@ -36,6 +36,7 @@ template <int F>
 __global__ void k_raycast(const SessionDesc*);
 __global__ void k_publish(const SessionDesc*, int, float*, int*);
 __global__ void k_tick_begin(const SessionDesc*, int);
+__global__ void k_occ_clear(const SessionDesc*);
 template <int F>
 __global__ void k_export_ref(const SessionDesc*, short2*, uchar4*);
 template <int F>
@@ -109,6 +110,8 @@ struct nui_session {
   void* vol = nullptr;
   uint8_t* wvol = nullptr;
   uchar4* cvol = nullptr;
+  uint8_t* occ = nullptr;
+  float* tile_max = nullptr;
   TrackState* ts = nullptr;
   float2* partials = nullptr;
   SessionDesc* d_desc1 = nullptr;  // one-entry table for the per-session path
@@ -185,6 +188,7 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
   d.vref = s->vref;
   d.nref = s->nref;
   d.cmap = s->cmap;
+  d.tile_max = s->tile_max;
   d.fmt = c.tsdf_format;
   for (int i = 0; i < 3; ++i) {
     d.res[i] = c.res[i];
@@ -195,6 +199,7 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
   d.vol = s->vol;
   d.wvol = s->wvol;
   d.cvol = s->cvol;
+  d.occ = s->occ;
   d.max_cw = c.max_color_weight;
   d.zchunks = s->zchunks;
   d.ts = s->ts;
@@ -241,8 +246,8 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
   };
   mark(0);
   k_tick_begin<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n);
-  const unsigned tiles = cdiv(p.maxW, 32) * cdiv(p.maxH, 8);
-  k_preprocess<<<dim3(tiles, p.n), dim3(32, 8), 0, st>>>(d);
+  const unsigned tiles = cdiv(p.maxW, 32) * cdiv(p.maxH, 16);
+  k_preprocess<<<dim3(tiles, p.n), dim3(32, 16), 0, st>>>(d);
   mark(1);
   for (int l = 1; l < p.maxLevels; ++l)
     k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), p.n), 256, 0, st>>>(d, l);
@@ -507,6 +512,7 @@ NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
   b += nv * voxel_bytes(c->tsdf_format);
   if (c->color_volume) b += nv * 4;
   b += sizeof(TrackState) + sizeof(SessionDesc) + ((N + 1023) / 1024) * kIcpTerms * sizeof(float2);
+  b += (size_t)((c->res[0] + 7) / 8) * ((c->res[1] + 7) / 8) * ((c->res[2] + 7) / 8) + (N / (kTile * kTile) + 64) * 4;
   return b;
 }
 
@@ -546,6 +552,9 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
   for (int l = 0; ok && l < c.levels; ++l)
     ok = alloc((void**)&s->dlev[l], (N >> (2 * l)) * 4) && alloc((void**)&s->vlev[l], (N >> (2 * l)) * 16);
   if (ok && c.tsdf_format == NUI_TSDF_F16_U8) ok = alloc((void**)&s->wvol, nv);
+  const size_t nbricks = (size_t)((c.res[0] + 7) / 8) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8);
+  const size_t ntiles = (size_t)((c.width + kTile - 1) / kTile) * ((c.height + kTile - 1) / kTile);
+  if (ok) ok = alloc((void**)&s->occ, nbricks) && alloc((void**)&s->tile_max, ntiles * sizeof(float));
   if (ok && c.color_volume) ok = alloc((void**)&s->cvol, nv * 4) && alloc((void**)&s->bgra, N * 4) && alloc((void**)&s->cmap, N * 4);
   if (!ok) {
     for (void* p : s->allocs) cudaFree(p);
@@ -679,7 +688,7 @@ nui_status run_stage(nui_session* s, int what) {
   const SessionDesc* dd = s->d_desc1;
   if (what == 0) {
     k_tick_begin<<<1, 64, 0, st>>>(dd, 1);
-    k_preprocess<<<dim3(cdiv(p.maxW, 32) * cdiv(p.maxH, 8), 1), dim3(32, 8), 0, st>>>(dd);
+    k_preprocess<<<dim3(cdiv(p.maxW, 32) * cdiv(p.maxH, 16), 1), dim3(32, 16), 0, st>>>(dd);
     for (int l = 1; l < p.maxLevels; ++l)
       k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), 1), 256, 0, st>>>(dd, l);
   } else if (what == 1) {
@@ -825,6 +834,7 @@ NUI_API nui_status nui_debug_upload_volume(nui_session* s, const int16_t* ref) {
   fill_desc(s, d, kInactive, nullptr, nullptr);
   cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, s->ctx->stream);
   cudaMemcpyAsync(tmp, ref, nv * 4, cudaMemcpyHostToDevice, s->ctx->stream);
+  k_occ_clear<<<256, 256, 0, s->ctx->stream>>>(s->d_desc1);
   switch (s->cfg.tsdf_format) {
     case 0: launch_import<0>(s, (const short2*)tmp); break;
     case 1: launch_import<1>(s, (const short2*)tmp); break;
@@ -863,7 +873,7 @@ NUI_API nui_status nui_k_preprocess(nui_ctx* ctx, const uint16_t* d_raw, int W, 
   d.vlev[0] = (float4*)d_vertex4;
   d.dscaled = d_scaled;
   NUI_CUDA(cudaMemcpyAsync(ctx->d_kdesc, &d, sizeof(d), cudaMemcpyHostToDevice, ctx->stream));
-  k_preprocess<<<dim3(cdiv(W, 32) * cdiv(H, 8), 1), dim3(32, 8), 0, ctx->stream>>>(ctx->d_kdesc);
+  k_preprocess<<<dim3(cdiv(W, 32) * cdiv(H, 16), 1), dim3(32, 16), 0, ctx->stream>>>(ctx->d_kdesc);
   NUI_CUDA(cudaGetLastError());
   NUI_CUDA(cudaStreamSynchronize(ctx->stream));
   return NUI_OK;
