@@ -273,8 +273,9 @@ def run_ours(args, rank, world):
 
 
 def tick_launch_count(sessions):
-    # preprocess + 2 pyramid + feedback + 19 icp + finalize + publish + integrate + raycast
-    return 1 + 2 + 1 + 19 + 1 + 1 + 1 + 1
+    # tick_begin + preprocess + 2 pyramid + feedback + 19 icp + finalize + publish + integrate
+    # + brick summary + raycast
+    return 1 + 1 + 2 + 1 + 19 + 1 + 1 + 1 + 1 + 1
 
 
 def profile_traffic(kernel):

@@ -79,7 +79,7 @@ struct SessionDesc {
   void* vol;                      // format storage, x-fastest: x + rx*(y + ry*z)
   uint8_t* wvol;                  // weight plane of NUI_TSDF_F16_U8
   uchar4* cvol;                   // colour volume (nullable), same layout
-  uint8_t* occ;                   // per 8^3 brick: 1 once any voxel of it has weight > 0
+  uint8_t* occ;                   // per 8^3 brick state (kBrick*)
   int max_cw;
   int zchunks;                    // integration: z chunks per column (one thread each)
   // tracking state and ICP scratch
@@ -205,8 +205,10 @@ struct Voxel<3> {  // NUI_TSDF_F16_F16: half2 (tsdf, weight)
 __device__ __forceinline__ size_t vox_index(const SessionDesc& s, int x, int y, int z) {
   return (size_t)x + (size_t)s.res[0] * ((size_t)y + (size_t)s.res[1] * (size_t)z);
 }
-// Occupancy bricks of 8^3 voxels.  Weights never decrease between resets, so a brick
-// whose byte is 0 holds only weight-0 voxels and readers may skip its loads.
+// Brick states of 8^3 voxels.  Weights never decrease between resets, so an empty brick
+// holds only weight-0 voxels; a positive brick has every voxel weighted with tsdf > 0.
+// Integration marks the bricks it touches dirty and k_brick_summary re-classifies them.
+enum BrickState : uint8_t { kBrickEmpty = 0, kBrickMixed = 1, kBrickPositive = 2, kBrickDirty = 3 };
 __device__ __forceinline__ size_t occ_index(const SessionDesc& s, int x, int y, int z) {
   const size_t bx = (size_t)(s.res[0] + 7) >> 3, by = (size_t)(s.res[1] + 7) >> 3;
   return (size_t)(x >> 3) + bx * ((size_t)(y >> 3) + by * (size_t)(z >> 3));

@@ -3,33 +3,58 @@
 // reference vertex / normal maps (and colour) that the next frame's ICP reads.
 //
 // Semantics kept from the reference: nearest-voxel sampling by round(p / cell) with voxel
-// centres at (g + 0.5) cell, march step 0.8 * trunc, zero crossing refined by the two
-// trilinear samples around it, central-difference normal; the trilinear weights pair the
-// x-neighbour voxel with the y fraction and the y-neighbour with the x fraction, as the
-// reference's index walk does (raycast.cl:66-119).
+// centres at (g + 0.5) cell, march step 0.8 * trunc accumulated in float, zero crossing
+// refined by the two trilinear samples around it, central-difference normal; the
+// trilinear weights pair the x-neighbour voxel with the y fraction and the y-neighbour
+// with the x fraction, as the reference's index walk does (raycast.cl:66-119).
+//
+// Brick skipping (exact): when a sample lands in an 8^3 brick whose voxels are all
+// unweighted (every sample there reads NaN) or all weighted with tsdf > 0 (every sample
+// there is positive, so after the first one no transition can happen), the following
+// samples that stay inside the brick -- by a margin of 1% of a voxel -- change nothing but
+// the march parameter; they are skipped by advancing the parameter with the same float
+// additions.
 #include "nui_device.cuh"
 
 namespace nui {
 
 template <int FMT>
 struct RayVol {
-  const SessionDesc& s;
-  int rx, ry, rz;
+  const void* vol;
+  const uint8_t* wvol;
+  const uint8_t* occ;
+  int rx, ry, rz, bx, by;
   float c0, c1, c2;
   float i0, i1, i2;  // 1 / cell
-  // tsdf of a voxel if its weight is > 0; bricks never touched are answered from the
-  // occupancy map without reading the voxel
-  __device__ __forceinline__ bool tsdf_at(int x, int y, int z, float& f) const {
-    if (s.occ && __ldg(s.occ + occ_index(s, x, y, z)) == 0) return false;
-    const size_t i = vox_index(s, x, y, z);
-    if (FMT == 2) {  // weight plane first: the tsdf plane is read only for weighted voxels
-      if (__ldg(s.wvol + i) == 0) return false;
-      f = __half2float(reinterpret_cast<const __half*>(s.vol)[i]);
+  __device__ __forceinline__ unsigned vidx(int x, int y, int z) const {
+    return (unsigned)x + (unsigned)rx * ((unsigned)y + (unsigned)ry * (unsigned)z);
+  }
+  __device__ __forceinline__ unsigned bidx(int x, int y, int z) const {
+    return (unsigned)(x >> 3) + (unsigned)bx * ((unsigned)(y >> 3) + (unsigned)by * (unsigned)(z >> 3));
+  }
+  __device__ __forceinline__ bool load(unsigned i, float& f) const {
+    if (FMT == 0) {
+      const short2 v = __ldg(reinterpret_cast<const short2*>(vol) + i);
+      f = (float)v.x / 32766.f;
+      return v.y > 0;
+    } else if (FMT == 1) {
+      const float2 v = __ldg(reinterpret_cast<const float2*>(vol) + i);
+      f = v.x;
+      return (int)v.y > 0;
+    } else if (FMT == 2) {
+      if (__ldg(wvol + i) == 0) return false;
+      f = __half2float(reinterpret_cast<const __half*>(vol)[i]);
       return true;
+    } else {
+      const __half2 v = reinterpret_cast<const __half2*>(vol)[i];
+      f = __low2float(v);
+      return (int)__high2float(v) > 0;
     }
-    int W;
-    Voxel<FMT>::load(s, i, f, W);
-    return W > 0;
+  }
+  // tsdf of a voxel if its weight is > 0
+  __device__ __forceinline__ bool tsdf_at(int x, int y, int z, float& f) const {
+    if (occ && __ldg(occ + bidx(x, y, z)) == kBrickEmpty) return false;
+    return load(vidx(x, y, z), f);
   }
   __device__ __forceinline__ void voxel_of(float3 p, int& gx, int& gy, int& gz) const {
     gx = round_div(p.x, c0, i0);
@@ -62,6 +87,25 @@ struct RayVol {
            t011 * (1 - a) * b * c + t100 * a * (1 - b) * (1 - c) + t101 * a * (1 - b) * c +
            t110 * a * b * (1 - c) + t111 * a * b * c;
   }
+  // Largest ray parameter up to which a sample stays (by 1% of a voxel) inside the
+  // p-box of brick (x>>3, y>>3, z>>3) clipped to the volume; samples with parameter below
+  // it map to voxels of that brick.
+  __device__ __forceinline__ float brick_exit(int gx, int gy, int gz, float3 start, float3 dir) const {
+    const int b[3] = {gx & ~7, gy & ~7, gz & ~7};
+    const int r[3] = {rx, ry, rz};
+    const float c[3] = {c0, c1, c2};
+    const float o[3] = {start.x, start.y, start.z};
+    const float d[3] = {dir.x, dir.y, dir.z};
+    float te = 3.4e38f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float lo = ((float)b[a] - 0.5f + 0.01f) * c[a];
+      const float hi = ((float)min(b[a] + 8, r[a]) - 0.5f - 0.01f) * c[a];
+      if (d[a] > 0.f) te = fminf(te, (hi - o[a]) / d[a]);
+      else if (d[a] < 0.f) te = fminf(te, (lo - o[a]) / d[a]);
+    }
+    return te;
+  }
 };
 
 template <int FMT>
@@ -75,8 +119,8 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
   const float4 nanv = make_float4(qnan(), qnan(), qnan(), 0.f);
   float4 vout = nanv, nout = nanv;
   uchar4 cout = make_uchar4(0, 0, 0, 0);
-  const RayVol<FMT> V{s, s.res[0], s.res[1], s.res[2], s.cell[0], s.cell[1], s.cell[2],
-                       1.0f / s.cell[0], 1.0f / s.cell[1], 1.0f / s.cell[2]};
+  const RayVol<FMT> V{s.vol, s.wvol, s.occ, s.res[0], s.res[1], s.res[2], (s.res[0] + 7) >> 3, (s.res[1] + 7) >> 3,
+                      s.cell[0], s.cell[1], s.cell[2], 1.0f / s.cell[0], 1.0f / s.cell[1], 1.0f / s.cell[2]};
   const DevXform& m = s.ts->xf;
   const float D0 = s.dim[0], D1 = s.dim[1], D2 = s.dim[2];
   const float3 off = f3(D0 / 2.0f, D1 / 2.0f, 0.f);
@@ -109,7 +153,22 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
       const float prev = tsdf;
       V.voxel_of(add3(start, mul3(dir, tc + step)), gx, gy, gz);
       if (!(gx >= 0 && gy >= 0 && gz >= 0 && gx < V.rx && gy < V.ry && gz < V.rz)) break;
-      tsdf = V.tsdf_at(gx, gy, gz, f) ? f : qnan();
+      const uint8_t st = V.occ ? __ldg(V.occ + V.bidx(gx, gy, gz)) : (uint8_t)kBrickMixed;
+      if (st == kBrickEmpty) {
+        tsdf = qnan();
+      } else {
+        tsdf = V.load(V.vidx(gx, gy, gz), f) ? f : qnan();
+      }
+      if (st == kBrickEmpty || (st == kBrickPositive && !(prev < 0.f))) {
+        // every further sample inside this brick reads the same kind of value: skip them
+        const float te = V.brick_exit(gx, gy, gz, start, dir);
+        for (;;) {
+          const float tn = tc + step;
+          if (!(tn < max_time) || !(tn + step < te)) break;
+          tc = tn;
+        }
+        continue;
+      }
       if (isnan(tsdf) || isnan(prev)) continue;
       if (prev < 0.f && tsdf > 0.f) break;
       if (prev >= 0.f && tsdf <= 0.f) {
@@ -120,7 +179,7 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
         const float Ts = tc - step * Ft / (Ftdt - Ft);
         const float3 vf = add3(start, mul3(dir, Ts));
         vout = w0(sub3(vf, off));
-        if (s.cvol) cout = s.cvol[vox_index(s, gx, gy, gz)];
+        if (s.cvol) cout = s.cvol[V.vidx(gx, gy, gz)];
         int hx, hy, hz;
         V.voxel_of(add3(start, mul3(dir, tc)), hx, hy, hz);
         if (hx > 1 && hy > 1 && hz > 1 && hx < V.rx - 2 && hy < V.ry - 2 && hz < V.rz - 2) {

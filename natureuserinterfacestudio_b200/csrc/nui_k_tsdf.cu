@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* _
         const size_t vi = idx + (size_t)u * slice;
         Voxel<FMT>::store(s, vi, tn, wn);
         ++touched;
-        if (s.occ) s.occ[occ_index(s, vx, vy, zb + u)] = 1;
+        if (s.occ) s.occ[occ_index(s, vx, vy, zb + u)] = kBrickDirty;
         if (s.cvol && s.bgra && fabsf(sdf[u]) < trunc) {
           const uchar4 nc = reinterpret_cast<const uchar4*>(s.bgra)[pix[u]];
           if (nc.w != 0) {
@@ -218,6 +218,36 @@ __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* _
   if ((int)(threadIdx.x & 31) == __ffs(mask) - 1 && t) atomicAdd(&s.ts->touched, (unsigned long long)t);
 }
 
+// Re-classifies the bricks integration touched: one warp per brick, each lane reads 16 of
+// its 512 voxels (8 consecutive x per row, so every row is one contiguous run).
+template <int FMT>
+__global__ void __launch_bounds__(256) k_brick_summary(const SessionDesc* __restrict__ descs, int force) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (s.fmt != FMT || !s.occ) return;
+  if (!force && (s.kind < 0 || !s.ts->integrate)) return;
+  const int bx = (s.res[0] + 7) >> 3, by = (s.res[1] + 7) >> 3, bz = (s.res[2] + 7) >> 3;
+  const long nb = (long)bx * by * bz;
+  const long b = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (b >= nb) return;
+  if (s.occ[b] != kBrickDirty) return;
+  const int lane = threadIdx.x & 31;
+  const int x0 = (int)(b % bx) * 8, y0 = (int)((b / bx) % by) * 8, z0 = (int)(b / ((long)bx * by)) * 8;
+  bool all_pos = true;
+  for (int r = lane >> 3; r < 64; r += 4) {  // 64 rows (y, z) of 8 voxels; lane & 7 = x
+    const int x = x0 + (lane & 7), y = y0 + (r & 7), z = z0 + (r >> 3);
+    if (x >= s.res[0] || y >= s.res[1] || z >= s.res[2]) {
+      all_pos = false;  // partial bricks at the volume edge stay mixed
+      continue;
+    }
+    float F;
+    int W;
+    Voxel<FMT>::load(s, vox_index(s, x, y, z), F, W);
+    if (!(W > 0 && F > 0.f)) all_pos = false;
+  }
+  const unsigned pos = __all_sync(0xffffffffu, all_pos);
+  if (lane == 0) s.occ[b] = pos ? kBrickPositive : kBrickMixed;
+}
+
 template <int FMT>
 __global__ void k_volume_init(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
@@ -236,6 +266,10 @@ template __global__ void k_integrate<0>(const SessionDesc*);
 template __global__ void k_integrate<1>(const SessionDesc*);
 template __global__ void k_integrate<2>(const SessionDesc*);
 template __global__ void k_integrate<3>(const SessionDesc*);
+template __global__ void k_brick_summary<0>(const SessionDesc*, int);
+template __global__ void k_brick_summary<1>(const SessionDesc*, int);
+template __global__ void k_brick_summary<2>(const SessionDesc*, int);
+template __global__ void k_brick_summary<3>(const SessionDesc*, int);
 template __global__ void k_volume_init<0>(const SessionDesc*);
 template __global__ void k_volume_init<1>(const SessionDesc*);
 template __global__ void k_volume_init<2>(const SessionDesc*);

@@ -77,7 +77,7 @@ __global__ void k_import_ref(const SessionDesc* __restrict__ descs, const short2
       reinterpret_cast<short2*>(s.vol)[i] = v;
     else
       Voxel<FMT>::store(s, i, (float)v.x / 32766.f, v.y);
-    if (s.occ && v.y > 0) s.occ[occ_index(s, x, y, z)] = 1;
+    if (s.occ && v.y > 0) s.occ[occ_index(s, x, y, z)] = kBrickDirty;
   }
 }
 

@@ -33,6 +33,8 @@ __global__ void k_integrate(const SessionDesc*);
 template <int F>
 __global__ void k_volume_init(const SessionDesc*);
 template <int F>
+__global__ void k_brick_summary(const SessionDesc*, int);
+template <int F>
 __global__ void k_raycast(const SessionDesc*);
 __global__ void k_publish(const SessionDesc*, int, float*, int*);
 __global__ void k_tick_begin(const SessionDesc*, int);
@@ -68,6 +70,7 @@ struct BatchPlan {
   int maxW = 0, maxH = 0, maxLevels = 0;
   int maxIters[kMaxLevels] = {0, 0, 0, 0};
   long maxIntegThreads[4] = {0, 0, 0, 0};  // per format: columns * zchunks
+  long maxBricks[4] = {0, 0, 0, 0};        // per format: 8^3 bricks
   int fmtMask = 0;
   bool operator<(const BatchPlan& o) const { return std::memcmp(this, &o, sizeof(BatchPlan)) < 0; }
 };
@@ -215,6 +218,8 @@ void plan_add(BatchPlan& p, const nui_session* s) {
   long th = (long)c.res[0] * c.res[1] * s->zchunks;
   p.maxIntegThreads[c.tsdf_format] = std::max(p.maxIntegThreads[c.tsdf_format], th);
   p.fmtMask |= 1 << c.tsdf_format;
+  const long nb = (long)((c.res[0] + 7) / 8) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8);
+  p.maxBricks[c.tsdf_format] = std::max(p.maxBricks[c.tsdf_format], nb);
 }
 
 unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
@@ -231,6 +236,11 @@ template <int F>
 void launch_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   if (!(p.fmtMask & (1 << F))) return;
   k_integrate<F><<<dim3(cdiv(p.maxIntegThreads[F], 256), p.n), 256, 0, st>>>(d);
+}
+template <int F>
+void launch_summary(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, int force) {
+  if (!(p.fmtMask & (1 << F))) return;
+  k_brick_summary<F><<<dim3(cdiv(p.maxBricks[F], 8), p.n), 256, 0, st>>>(d, force);
 }
 template <int F>
 void launch_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
@@ -264,6 +274,10 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
   launch_integrate<1>(p, d, st);
   launch_integrate<2>(p, d, st);
   launch_integrate<3>(p, d, st);
+  launch_summary<0>(p, d, st, 0);
+  launch_summary<1>(p, d, st, 0);
+  launch_summary<2>(p, d, st, 0);
+  launch_summary<3>(p, d, st, 0);
   mark(4);
   launch_raycast<0>(p, d, st);
   launch_raycast<1>(p, d, st);
@@ -703,6 +717,10 @@ nui_status run_stage(nui_session* s, int what) {
     launch_integrate<1>(p, dd, st);
     launch_integrate<2>(p, dd, st);
     launch_integrate<3>(p, dd, st);
+    launch_summary<0>(p, dd, st, 0);
+    launch_summary<1>(p, dd, st, 0);
+    launch_summary<2>(p, dd, st, 0);
+    launch_summary<3>(p, dd, st, 0);
   } else if (what == 3) {
     launch_raycast<0>(p, dd, st);
     launch_raycast<1>(p, dd, st);
@@ -841,6 +859,13 @@ NUI_API nui_status nui_debug_upload_volume(nui_session* s, const int16_t* ref) {
     case 2: launch_import<2>(s, (const short2*)tmp); break;
     case 3: launch_import<3>(s, (const short2*)tmp); break;
   }
+  BatchPlan p;
+  p.n = 1;
+  plan_add(p, s);
+  launch_summary<0>(p, s->d_desc1, s->ctx->stream, 1);
+  launch_summary<1>(p, s->d_desc1, s->ctx->stream, 1);
+  launch_summary<2>(p, s->d_desc1, s->ctx->stream, 1);
+  launch_summary<3>(p, s->d_desc1, s->ctx->stream, 1);
   cudaError_t e = cudaStreamSynchronize(s->ctx->stream);
   cudaFree(tmp);
   if (e != cudaSuccess) return fail(NUI_ERR_DEVICE, cudaGetErrorString(e));
