@@ -89,7 +89,7 @@ def session_cfgs(L, n, fmt):
     for i in range(n):
         r = VOLUMES[i % len(VOLUMES)]
         dim = 3.0 if r == 256 else 4.0
-        cfgs.append(L.default_cfg(res=(r, r, r), dim=(dim, dim, dim), tsdf_format=fmt, trunc_dist=0.0,
+        cfgs.append(L.default_cfg(res=(r, r, r), dim=(dim, dim, dim), tsdf_format=fmt, trunc_dist=0.03,
                                   iterations=[10, 5, 4, 0], integration_threshold=0.0))
     return cfgs
 

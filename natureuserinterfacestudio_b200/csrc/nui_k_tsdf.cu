@@ -218,8 +218,10 @@ __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* _
   if ((int)(threadIdx.x & 31) == __ffs(mask) - 1 && t) atomicAdd(&s.ts->touched, (unsigned long long)t);
 }
 
-// Re-classifies the bricks integration touched: one warp per brick, each lane reads 16 of
-// its 512 voxels (8 consecutive x per row, so every row is one contiguous run).
+// Re-classifies the bricks integration touched.  A block looks at 1024 bricks: it first
+// compacts the dirty ones into a shared list, then each warp classifies listed bricks,
+// every lane reading 16 of a brick's 512 voxels (8 consecutive x per row, so each row is
+// one contiguous run).
 template <int FMT>
 __global__ void __launch_bounds__(256) k_brick_summary(const SessionDesc* __restrict__ descs, int force) {
   const SessionDesc& s = descs[blockIdx.y];
@@ -227,25 +229,36 @@ __global__ void __launch_bounds__(256) k_brick_summary(const SessionDesc* __rest
   if (!force && (s.kind < 0 || !s.ts->integrate)) return;
   const int bx = (s.res[0] + 7) >> 3, by = (s.res[1] + 7) >> 3, bz = (s.res[2] + 7) >> 3;
   const long nb = (long)bx * by * bz;
-  const long b = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (b >= nb) return;
-  if (s.occ[b] != kBrickDirty) return;
-  const int lane = threadIdx.x & 31;
-  const int x0 = (int)(b % bx) * 8, y0 = (int)((b / bx) % by) * 8, z0 = (int)(b / ((long)bx * by)) * 8;
-  bool all_pos = true;
-  for (int r = lane >> 3; r < 64; r += 4) {  // 64 rows (y, z) of 8 voxels; lane & 7 = x
-    const int x = x0 + (lane & 7), y = y0 + (r & 7), z = z0 + (r >> 3);
-    if (x >= s.res[0] || y >= s.res[1] || z >= s.res[2]) {
-      all_pos = false;  // partial bricks at the volume edge stay mixed
-      continue;
-    }
-    float F;
-    int W;
-    Voxel<FMT>::load(s, vox_index(s, x, y, z), F, W);
-    if (!(W > 0 && F > 0.f)) all_pos = false;
+  const long b0 = (long)blockIdx.x * 1024;
+  if (b0 >= nb) return;
+  __shared__ int list[1024];
+  __shared__ int count;
+  if (threadIdx.x == 0) count = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < 1024; i += blockDim.x) {
+    const long b = b0 + i;
+    if (b < nb && s.occ[b] == kBrickDirty) list[atomicAdd(&count, 1)] = i;
   }
-  const unsigned pos = __all_sync(0xffffffffu, all_pos);
-  if (lane == 0) s.occ[b] = pos ? kBrickPositive : kBrickMixed;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int k = threadIdx.x >> 5; k < count; k += blockDim.x >> 5) {
+    const long b = b0 + list[k];
+    const int x0 = (int)(b % bx) * 8, y0 = (int)((b / bx) % by) * 8, z0 = (int)(b / ((long)bx * by)) * 8;
+    bool all_pos = true;
+    for (int r = lane >> 3; r < 64; r += 4) {  // 64 rows (y, z) of 8 voxels; lane & 7 = x
+      const int x = x0 + (lane & 7), y = y0 + (r & 7), z = z0 + (r >> 3);
+      if (x >= s.res[0] || y >= s.res[1] || z >= s.res[2]) {
+        all_pos = false;  // partial bricks at the volume edge stay mixed
+        continue;
+      }
+      float F;
+      int W;
+      Voxel<FMT>::load(s, vox_index(s, x, y, z), F, W);
+      if (!(W > 0 && F > 0.f)) all_pos = false;
+    }
+    const unsigned pos = __all_sync(0xffffffffu, all_pos);
+    if (lane == 0) s.occ[b] = pos ? kBrickPositive : kBrickMixed;
+  }
 }
 
 template <int FMT>

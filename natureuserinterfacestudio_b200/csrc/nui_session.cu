@@ -240,7 +240,7 @@ void launch_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st)
 template <int F>
 void launch_summary(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, int force) {
   if (!(p.fmtMask & (1 << F))) return;
-  k_brick_summary<F><<<dim3(cdiv(p.maxBricks[F], 8), p.n), 256, 0, st>>>(d, force);
+  k_brick_summary<F><<<dim3(cdiv(p.maxBricks[F], 1024), p.n), 256, 0, st>>>(d, force);
 }
 template <int F>
 void launch_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
