@@ -40,7 +40,16 @@ UNITS = {
     "raycast.cl": "launch_raycast.inc",
     "marchingCube.cl": "launch_mc.inc",
     "icp.cl": "launch_icp.inc",
+    "KinfuHashScene.cl": "launch_hash_scene.inc",
+    "KinfuHashRaycast.cl": "launch_hash_raycast.inc",
+    "KinfuHashVisualization.cl": "launch_hash_mesh.inc",
 }
+# The reference fixes its hash table sizes at compile time (hashing_gpu_def.h:9-20:
+# 0x150000 buckets, 0x30000 excess entries, 2^20 voxel blocks = 3.2 GB of voxels).  The
+# host build uses small tables of the same structure so that tests can run it; only
+# these constants change.
+HASH_TEST_SIZES = {"SDF_BUCKET_NUM": "0x10000", "SDF_HASH_MASK": "0xffff", "SDF_EXCESS_LIST_SIZE": "0x4000",
+                   "SDF_LOCAL_BLOCK_NUM": "0x8000"}
 # every file the units include
 INCLUDED = ["utils.cl", "gpu_def.h", "cameraUtils.cl", "hashing_gpu_def.h", "KinfuHashUtils.cl",
             "prefixSum.cl"]
@@ -114,6 +123,9 @@ def main():
             spec = UNITS.get(f)
             if isinstance(spec, tuple):
                 text = extract(text, spec[1])
+            if f == "hashing_gpu_def.h":
+                for k, v in HASH_TEST_SIZES.items():
+                    text = re.sub(r"(#define\s+%s\s+)\S+" % k, r"\g<1>" + v, text)
             with open(os.path.join(tmp, f), "w") as fh:
                 fh.write(rewrite(text))
         objs = []

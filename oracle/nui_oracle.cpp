@@ -970,3 +970,526 @@ ORC_API const float* orc_engine_refmap(const OrcEngine* e, int which) {
 ORC_API void orc_engine_tsdf_params(const OrcEngine* e, OrcTsdf* out) { *out = e->tp; }
 ORC_API void orc_engine_icp_stats(const OrcEngine* e, OrcIcpStats* out) { *out = e->last; }
 ORC_API long orc_engine_touched(const OrcEngine* e) { return e->touched; }
+
+// =================================================================================
+// Voxel-block hashing (KinfuHashScene.cl, KinfuHashRaycast.cl, KinfuHashVisualization.cl,
+// host NuiKinfuOpenCLHashScene.cpp / NuiKinfuVoxelBlockHash.cpp), with runtime table sizes.
+// Races of the reference are given deterministic intended semantics:
+//  * new blocks colliding in one bucket (or chain end) in one frame: the block coordinate
+//    written last in pixel-raster / ray-step order wins (what the kernel gives when its
+//    work-items run one after another, KinfuHashScene.cl:127-130);
+//  * free blocks and excess slots are popped in increasing entry index
+//    (KinfuHashScene.cl:138-194 run sequentially);
+//  * the visible list is the increasing list of entries with visible type > 0
+//    (intended meaning of compactifyValidPrefixSum_kernel, prefixSum.cl:222-232) over all
+//    entries (the reference's scan covers only the first 2^20, NuiOpenCLPrefixSum.cpp:16-41);
+//  * every voxel of the pool starts at (sdf 0, weight 0, colour 0) (reset_voxel_block_kernel,
+//    KinfuHashScene.cl:5-20, clears only the first 2^20+511 voxels);
+//  * the expected-range image is updated with atomic min / max
+//    (project_minmax_depths_kernel, KinfuHashRaycast.cl:67-75, is a plain read-modify-write);
+//    its `zRange.y = fmax(zRange.x, z)` (:49) is kept as written;
+//  * castRay reads the voxel before checking the block index (KinfuHashRaycast.cl:193-195):
+//    a missing block reads as sdf 1.
+namespace {
+struct HEntry {
+  int16_t pos[3];
+  int16_t pad;
+  int32_t ptr;
+  uint32_t offset;
+};
+}  // namespace
+
+struct OrcHashCfg {
+  int buckets, excess, pool;  // bucket count, excess list length, voxel blocks in the pool
+  uint32_t mask;              // hash mask (buckets - 1 for power-of-two tables)
+  float voxel, mu;            // virtualVoxelSize, truncScale
+  int max_w;                  // integrationWeightMax
+};
+
+struct OrcHash {
+  OrcHashCfg c;
+  std::vector<HEntry> e;
+  std::vector<int16_t> sdf;
+  std::vector<uint8_t> w, rgb;
+  std::vector<int> alloc_list, excess_list;
+  int last_block, last_excess;
+  std::vector<uint8_t> alloc_type, vis;
+  std::vector<int16_t> coords;
+  std::vector<int> vis_ids;
+  std::vector<float> range;  // expected range image (2 floats per pixel)
+  long failed_allocs = 0;
+};
+
+ORC_API void orc_hash_reset(OrcHash* h) {
+  const long ne = (long)h->c.buckets + h->c.excess;
+  for (long i = 0; i < ne; ++i) h->e[i] = HEntry{{0, 0, 0}, 0, -2, 0};
+  std::fill(h->sdf.begin(), h->sdf.end(), 0);
+  std::fill(h->w.begin(), h->w.end(), 0);
+  std::fill(h->rgb.begin(), h->rgb.end(), 0);
+  for (int i = 0; i < h->c.pool; ++i) h->alloc_list[i] = i;
+  for (int i = 0; i < h->c.excess; ++i) h->excess_list[i] = i;
+  h->last_block = h->c.pool - 1;
+  h->last_excess = h->c.excess - 1;
+  std::fill(h->alloc_type.begin(), h->alloc_type.end(), 0);
+  std::fill(h->vis.begin(), h->vis.end(), 0);
+  h->vis_ids.clear();
+  h->failed_allocs = 0;
+}
+
+ORC_API OrcHash* orc_hash_create(const OrcHashCfg* cfg) {
+  OrcHash* h = new OrcHash();
+  h->c = *cfg;
+  const long ne = (long)cfg->buckets + cfg->excess;
+  h->e.resize(ne);
+  h->sdf.resize((size_t)cfg->pool * 512);
+  h->w.resize((size_t)cfg->pool * 512);
+  h->rgb.resize((size_t)cfg->pool * 512 * 3);
+  h->alloc_list.resize(cfg->pool);
+  h->excess_list.resize(cfg->excess);
+  h->alloc_type.resize(ne);
+  h->vis.resize(ne);
+  h->coords.resize(3 * ne);
+  orc_hash_reset(h);
+  return h;
+}
+ORC_API void orc_hash_destroy(OrcHash* h) { delete h; }
+
+static inline uint32_t hash_index(const OrcHashCfg& c, int x, int y, int z) {
+  return (((uint32_t)x * 73856093u) ^ ((uint32_t)y * 19349669u) ^ ((uint32_t)z * 83492791u)) & c.mask;
+}
+
+// Block-pool voxel index of virtual voxel v (findVoxelBlockIndex, KinfuHashRaycast.cl:78-111);
+// -1 when its block is not allocated.
+static long hash_find(const OrcHash* h, int vx, int vy, int vz) {
+  int bx = vx < 0 ? vx - 7 : vx, by = vy < 0 ? vy - 7 : vy, bz = vz < 0 ? vz - 7 : vz;
+  bx /= 8;
+  by /= 8;
+  bz /= 8;
+  const int lin = (vx - 8 * bx) + 8 * (vy - 8 * by) + 64 * (vz - 8 * bz);
+  const int16_t sx = (int16_t)bx, sy = (int16_t)by, sz = (int16_t)bz;
+  uint32_t hi = hash_index(h->c, sx, sy, sz);
+  for (;;) {
+    const HEntry& en = h->e[hi];
+    if (en.pos[0] == sx && en.pos[1] == sy && en.pos[2] == sz && en.ptr >= 0) return (long)en.ptr * 512 + lin;
+    if (en.offset < 1) break;
+    hi = (uint32_t)h->c.buckets + en.offset - 1;
+  }
+  return -1;
+}
+
+static inline f3 xf_apply(const OrcXform* m, f3 v) {
+  return mk(dot3(mk(m->R[0], m->R[1], m->R[2]), v), dot3(mk(m->R[3], m->R[4], m->R[5]), v),
+            dot3(mk(m->R[6], m->R[7], m->R[8]), v)) + mk(m->t[0], m->t[1], m->t[2]);
+}
+static inline f3 xf_inverse(const OrcXform* m, f3 v) {
+  v = v - mk(m->t[0], m->t[1], m->t[2]);
+  return mk(dot3(mk(m->R_inv[0], m->R_inv[1], m->R_inv[2]), v), dot3(mk(m->R_inv[3], m->R_inv[4], m->R_inv[5]), v),
+            dot3(mk(m->R_inv[6], m->R_inv[7], m->R_inv[8]), v));
+}
+// kinectDepthToSkeleton (cameraUtils.cl:46-53)
+static inline f3 depth_to_point(const OrcCam* cam, int ux, int uy, float d) {
+  const float x = ((float)ux - cam->cx) / cam->fx, y = ((float)uy - cam->cy) / cam->fy;
+  return mk(d * x, d * y, d);
+}
+
+// A16: ResetVisibleEntrys + ResetAllocType + buildHashAllocAndVisibleType +
+// allocateVoxelBlocksList + buildVisibleList + compaction (AllocateSceneFromDepth,
+// NuiKinfuOpenCLHashScene.cpp:404-424).  depth: pass-filtered z-depth (NaN invalid).
+ORC_API long orc_hash_allocate(OrcHash* h, const float* depth, const OrcCam* cam, const OrcXform* m) {
+  const OrcHashCfg& c = h->c;
+  const long ne = (long)c.buckets + c.excess;
+  for (int id : h->vis_ids) h->vis[id] = 3;
+  std::fill(h->alloc_type.begin(), h->alloc_type.end(), 0);
+  const float obs = 1.0f / (c.voxel * 8);
+  const int W = (int)cam->W, H = (int)cam->H;
+  for (int py = 0; py < H; ++py)
+    for (int px = 0; px < W; ++px) {
+      const float Dp = depth[(long)py * W + px];
+      if (std::isnan(Dp)) continue;
+      const f3 pc = depth_to_point(cam, px, py, Dp);
+      const float norm = c.mu / length3(pc);
+      f3 rmin = xf_apply(m, pc * (1.0f - norm)) * obs;
+      const f3 rmax = xf_apply(m, pc * (1.0f + norm)) * obs;
+      f3 rdir = rmax - rmin;
+      const float rn = length3(rdir);
+      const int steps = (int)std::ceil(2.0f * rn);
+      const float dv = (float)(steps - 1);
+      rdir = mk(rdir.x / dv, rdir.y / dv, rdir.z / dv);
+      for (int i = 0; i < steps; ++i) {
+        const int16_t bx = (int16_t)std::floor(rmin.x), by = (int16_t)std::floor(rmin.y), bz = (int16_t)std::floor(rmin.z);
+        uint32_t hi = hash_index(c, bx, by, bz);
+        HEntry en = h->e[hi];
+        bool found = false;
+        if (en.pos[0] == bx && en.pos[1] == by && en.pos[2] == bz && en.ptr >= -1) {
+          h->vis[hi] = (en.ptr == -1) ? 2 : 1;
+          found = true;
+        }
+        if (!found) {
+          bool excess = false;
+          if (en.ptr >= -1) {
+            while (en.offset >= 1) {
+              hi = (uint32_t)c.buckets + en.offset - 1;
+              en = h->e[hi];
+              if (en.pos[0] == bx && en.pos[1] == by && en.pos[2] == bz && en.ptr >= -1) {
+                h->vis[hi] = (en.ptr == -1) ? 2 : 1;
+                found = true;
+                break;
+              }
+            }
+            excess = true;
+          }
+          if (!found) {
+            h->alloc_type[hi] = excess ? 2 : 1;
+            h->vis[hi] = 1;
+            h->coords[3 * hi] = bx;
+            h->coords[3 * hi + 1] = by;
+            h->coords[3 * hi + 2] = bz;
+          }
+        }
+        rmin = rmin + rdir;
+      }
+    }
+  for (long i = 0; i < ne; ++i) {
+    const int t = h->alloc_type[i];
+    if (t == 1) {
+      const int vba = h->last_block--;
+      if (vba >= 0) {
+        HEntry en{{h->coords[3 * i], h->coords[3 * i + 1], h->coords[3 * i + 2]}, 0, h->alloc_list[vba], 0};
+        h->e[i] = en;
+      } else {
+        ++h->failed_allocs;
+      }
+    } else if (t == 2) {
+      const int vba = h->last_block--;
+      const int exl = h->last_excess--;
+      if (vba >= 0 && exl >= 0) {
+        HEntry en{{h->coords[3 * i], h->coords[3 * i + 1], h->coords[3 * i + 2]}, 0, h->alloc_list[vba], 0};
+        const int off = h->excess_list[exl];
+        h->e[i].offset = (uint32_t)off + 1;
+        h->e[(long)c.buckets + off] = en;
+        h->vis[(long)c.buckets + off] = 1;
+      } else {
+        ++h->failed_allocs;
+      }
+    }
+  }
+  // buildVisibleList_kernel (KinfuHashScene.cl:262-285) with checkBlockVisibility (:196-260)
+  const float factor = 8.0f * c.voxel;
+  auto point_visible = [&](f3 p) {
+    const f3 q = xf_inverse(m, p);
+    if (isnan3(q)) return false;
+    const int sx = (int)(q.x * cam->fx / q.z + cam->cx + 0.5f), sy = (int)(q.y * cam->fy / q.z + cam->cy + 0.5f);
+    return sx >= 0 && sx < (int)cam->W && sy >= 0 && sy < (int)cam->H;
+  };
+  for (long i = 0; i < ne; ++i) {
+    if (h->vis[i] != 3) continue;
+    const HEntry& en = h->e[i];
+    f3 p = mk((float)en.pos[0] * factor, (float)en.pos[1] * factor, (float)en.pos[2] * factor);
+    bool v = point_visible(p);
+    if (!v) { p.z += factor; v = point_visible(p); }
+    if (!v) { p.y += factor; v = point_visible(p); }
+    if (!v) { p.x += factor; v = point_visible(p); }
+    if (!v) { p.z -= factor; v = point_visible(p); }
+    if (!v) { p.y -= factor; v = point_visible(p); }
+    if (!v) { p.x -= factor; p.y += factor; v = point_visible(p); }
+    if (!v) { p.x += factor; p.y -= factor; p.z += factor; v = point_visible(p); }
+    if (!v) h->vis[i] = 0;
+  }
+  h->vis_ids.clear();
+  for (long i = 0; i < ne; ++i)
+    if (h->vis[i] > 0) h->vis_ids.push_back((int)i);
+  return (long)h->vis_ids.size();
+}
+
+// A17: integrateIntoScene_kernel (KinfuHashScene.cl:387-470) over the visible list.
+ORC_API void orc_hash_integrate(OrcHash* h, const float* depth, const uint8_t* bgra, const OrcCam* cam,
+                                const OrcXform* m, long* touched) {
+  const OrcHashCfg& c = h->c;
+  long cnt = 0;
+  const long nvis = (long)h->vis_ids.size();
+#pragma omp parallel for schedule(dynamic, 8) reduction(+ : cnt)
+  for (long k = 0; k < nvis; ++k) {
+    const HEntry en = h->e[h->vis_ids[k]];
+    if (en.ptr < 0) continue;
+    for (int lid = 0; lid < 512; ++lid) {
+      const long bid = (long)en.ptr * 512 + lid;
+      if (c.max_w == h->w[bid]) continue;
+      const int lx = (lid % 64) % 8, ly = (lid % 64) / 8, lz = lid / 64;
+      const f3 pm = mk((float)(en.pos[0] * 8 + lx), (float)(en.pos[1] * 8 + ly), (float)(en.pos[2] * 8 + lz)) * c.voxel;
+      const f3 pc = xf_inverse(m, pm);
+      if (pc.z <= 0) continue;
+      const int ix = (int)(pc.x * cam->fx / pc.z + cam->cx + 0.5f), iy = (int)(pc.y * cam->fy / pc.z + cam->cy + 0.5f);
+      if (ix < 0 || ix >= (int)cam->W || iy < 0 || iy >= (int)cam->H) continue;
+      const long sid = (long)iy * cam->W + ix;
+      const float d = depth[sid];
+      if (std::isnan(d)) continue;
+      const float eta = d - pc.z;
+      const float sdf = eta / c.mu;
+      if (eta < -c.mu) continue;
+      const float oldF = (float)h->sdf[bid] / 32767.0f, oldW = (float)h->w[bid];
+      float newF = std::min(1.0f, sdf);
+      const float newW = 1.0f, cw = oldW + newW;
+      if (bgra && eta < c.mu && std::fabs(sdf) < 0.25f) {
+        const uint8_t* col = bgra + 4 * sid;
+        if (col[3] == 255) {
+          uint8_t* vc = &h->rgb[3 * bid];
+          const float r = (oldW * (float)vc[0] + newW * (float)col[2]) / cw;
+          const float g = (oldW * (float)vc[1] + newW * (float)col[1]) / cw;
+          const float b = (oldW * (float)vc[2] + newW * (float)col[0]) / cw;
+          vc[0] = (uint8_t)std::min(std::max(r, 0.f), 255.f);
+          vc[1] = (uint8_t)std::min(std::max(g, 0.f), 255.f);
+          vc[2] = (uint8_t)std::min(std::max(b, 0.f), 255.f);
+        }
+      }
+      newF = oldW * oldF + newW * newF;
+      newF /= cw;
+      h->sdf[bid] = (int16_t)(newF * 32767.0f);
+      h->w[bid] = (uint8_t)std::min((int)(uint8_t)cw, c.max_w);
+      ++cnt;
+    }
+  }
+  if (touched) *touched = cnt;
+}
+
+// A18: CreateExpectedDepths (project_minmax_depths_kernel) + castRay, the plain raycast
+// path of NuiKinfuOpenCLHashScene::raycastRender (forward rendering off).  Outputs world
+// vertex / normal maps (3 floats per pixel), colour (4 bytes, nullable) and the range image.
+static float hash_read_sdf(const OrcHash* h, int x, int y, int z) {
+  const long bi = hash_find(h, x, y, z);
+  return bi < 0 ? 1.0f : (float)h->sdf[bi] / 32767.0f;
+}
+
+ORC_API void orc_hash_raycast(OrcHash* h, const OrcCam* cam, const OrcXform* m, float* vmap, float* nmap,
+                              uint8_t* cmap, float* range_out) {
+  const OrcHashCfg& c = h->c;
+  const int W = (int)cam->W, H = (int)cam->H;
+  const long N = (long)W * H;
+  std::vector<float> rg(2 * N);
+  for (long i = 0; i < N; ++i) {
+    rg[2 * i] = 999999.9f;
+    rg[2 * i + 1] = 0.05f;
+  }
+  for (int id : h->vis_ids) {
+    const HEntry& en = h->e[id];
+    if (en.ptr < 0) continue;
+    int ulx = W, uly = H, lrx = 0, lry = 0;
+    float zx = 999999.9f, zy = 0.05f;
+    for (int corner = 0; corner < 8; ++corner) {
+      const int cx = en.pos[0] + ((corner & 1) ? 1 : 0), cy = en.pos[1] + ((corner & 2) ? 1 : 0),
+                cz = en.pos[2] + ((corner & 4) ? 1 : 0);
+      f3 p = mk((float)(int16_t)cx, (float)(int16_t)cy, (float)(int16_t)cz) * 8.0f * c.voxel;
+      p = xf_inverse(m, p);
+      if (isnan3(p) || p.z < 1e-6) continue;
+      const float u = p.x * cam->fx / p.z + cam->cx, v = p.y * cam->fy / p.z + cam->cy;
+      ulx = std::min(ulx, (int)std::floor(u));
+      lrx = std::max(lrx, (int)std::ceil(u));
+      uly = std::min(uly, (int)std::floor(v));
+      lry = std::max(lry, (int)std::ceil(v));
+      zx = std::fmin(zx, p.z);
+      zy = std::fmax(zx, p.z);
+    }
+    if (ulx < 0) ulx = 0;
+    if (uly < 0) uly = 0;
+    if (lrx >= W) lrx = W - 1;
+    if (lry >= H) lry = H - 1;
+    if (zx < 0.05f) zx = 0.05f;
+    for (int by = uly; by <= lry; ++by)
+      for (int bx = ulx; bx <= lrx; ++bx) {
+        const long li = (long)by * W + bx;
+        rg[2 * li] = std::fmin(rg[2 * li], zx);
+        rg[2 * li + 1] = std::fmax(rg[2 * li + 1], zy);
+      }
+  }
+  if (range_out) std::memcpy(range_out, rg.data(), sizeof(float) * 2 * N);
+  const float oov = 1.0f / c.voxel;
+  const float stepScale = c.mu * oov * 0.6f;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int py = 0; py < H; ++py)
+    for (int px = 0; px < W; ++px) {
+      const long pid = (long)py * W + px;
+      f3 ps = depth_to_point(cam, px, py, rg[2 * pid]);
+      float total = length3(ps) * oov;
+      ps = xf_apply(m, ps) * oov;
+      f3 pe = depth_to_point(cam, px, py, rg[2 * pid + 1]);
+      const float totalMax = length3(pe) * oov;
+      pe = xf_apply(m, pe) * oov;
+      float sdfv = 1.0f, stepLen;
+      const f3 dir = normalize3(pe - ps);
+      f3 pr = ps;
+      while (total < totalMax) {
+        const int vx = (int)std::round(pr.x), vy = (int)std::round(pr.y), vz = (int)std::round(pr.z);
+        const long bi = hash_find(h, vx, vy, vz);
+        if (bi < 0) {
+          sdfv = 1.0f;
+          stepLen = 8.0f;
+        } else {
+          sdfv = (float)h->sdf[bi] / 32767.0f;
+          if (sdfv <= 0.1f && sdfv >= -0.5f) {
+            // readInterpolatedVoxelSDF (KinfuHashRaycast.cl:124-153)
+            const int ix = (int)std::floor(pr.x), iy = (int)std::floor(pr.y), iz = (int)std::floor(pr.z);
+            const f3 cf = mk(pr.x - (float)ix, pr.y - (float)iy, pr.z - (float)iz);
+            float v1 = hash_read_sdf(h, ix, iy, iz), v2 = hash_read_sdf(h, ix + 1, iy, iz);
+            float r1 = (1.0f - cf.x) * v1 + cf.x * v2;
+            v1 = hash_read_sdf(h, ix, iy + 1, iz);
+            v2 = hash_read_sdf(h, ix + 1, iy + 1, iz);
+            r1 = (1.0f - cf.y) * r1 + cf.y * ((1.0f - cf.x) * v1 + cf.x * v2);
+            v1 = hash_read_sdf(h, ix, iy, iz + 1);
+            v2 = hash_read_sdf(h, ix + 1, iy, iz + 1);
+            float r2 = (1.0f - cf.x) * v1 + cf.x * v2;
+            v1 = hash_read_sdf(h, ix, iy + 1, iz + 1);
+            v2 = hash_read_sdf(h, ix + 1, iy + 1, iz + 1);
+            r2 = (1.0f - cf.y) * r2 + cf.y * ((1.0f - cf.x) * v1 + cf.x * v2);
+            sdfv = (1.0f - cf.z) * r1 + cf.z * r2;
+          }
+          if (sdfv <= 0.0f) break;
+          stepLen = std::max(sdfv * stepScale, 1.0f);
+        }
+        pr = pr + dir * stepLen;
+        total += stepLen;
+      }
+      f3 vout = mk(QNAN, QNAN, QNAN), nout = mk(QNAN, QNAN, QNAN);
+      uint8_t col[4] = {0, 0, 0, 0};
+      if (sdfv <= 0.0f) {
+        stepLen = sdfv * stepScale;
+        pr = pr + dir * stepLen;
+        const int ix = (int)std::floor(pr.x), iy = (int)std::floor(pr.y), iz = (int)std::floor(pr.z);
+        const f3 cf = mk(pr.x - (float)ix, pr.y - (float)iy, pr.z - (float)iz);
+        const f3 nc = mk(1.0f - cf.x, 1.0f - cf.y, 1.0f - cf.z);
+        static const int O[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0}, {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+        float fb[8];
+        float nearest = 1.0e20f;
+        for (int k = 0; k < 8; ++k) {
+          const long bi = hash_find(h, ix + O[k][0], iy + O[k][1], iz + O[k][2]);
+          fb[k] = bi < 0 ? 1.0f : (float)h->sdf[bi] / 32767.0f;
+          const f3 dd = mk(O[k][0] ? nc.x : cf.x, O[k][1] ? nc.y : cf.y, O[k][2] ? nc.z : cf.z);
+          const float cd = length3(dd);
+          if (cmap && bi >= 0 && (k == 0 || nearest > cd)) {
+            nearest = cd;
+            col[0] = h->rgb[3 * bi];
+            col[1] = h->rgb[3 * bi + 1];
+            col[2] = h->rgb[3 * bi + 2];
+            col[3] = 255;
+          }
+        }
+        // front = k 0..3 (x, y), back = k 4..7
+        sdfv = fb[0] * nc.x * nc.y * nc.z + fb[1] * cf.x * nc.y * nc.z + fb[2] * nc.x * cf.y * nc.z +
+               fb[3] * cf.x * cf.y * nc.z + fb[4] * nc.x * nc.y * cf.z + fb[5] * cf.x * nc.y * cf.z +
+               fb[6] * nc.x * cf.y * cf.z + fb[7] * cf.x * cf.y * cf.z;
+        stepLen = sdfv * stepScale;
+        pr = pr + dir * stepLen;
+        vout = pr * c.voxel;
+        if (nmap) {
+          auto rs = [&](int a, int b, int cc) { return hash_read_sdf(h, ix + a, iy + b, iz + cc); };
+          float p1, p2, v1;
+          f3 g;
+          p1 = fb[0] * nc.y * nc.z + fb[2] * cf.y * nc.z + fb[4] * nc.y * cf.z + fb[6] * cf.y * cf.z;
+          p2 = rs(-1, 0, 0) * nc.y * nc.z + rs(-1, 1, 0) * cf.y * nc.z + rs(-1, 0, 1) * nc.y * cf.z +
+               rs(-1, 1, 1) * cf.y * cf.z;
+          v1 = p1 * cf.x + p2 * nc.x;
+          p1 = fb[1] * nc.y * nc.z + fb[3] * cf.y * nc.z + fb[5] * nc.y * cf.z + fb[7] * cf.y * cf.z;
+          p2 = rs(2, 0, 0) * nc.y * nc.z + rs(2, 1, 0) * cf.y * nc.z + rs(2, 0, 1) * nc.y * cf.z +
+               rs(2, 1, 1) * cf.y * cf.z;
+          g.x = p1 * nc.x + p2 * cf.x - v1;
+          p1 = fb[0] * nc.x * nc.z + fb[1] * cf.x * nc.z + fb[4] * nc.x * cf.z + fb[5] * cf.x * cf.z;
+          p2 = rs(0, -1, 0) * nc.x * nc.z + rs(1, -1, 0) * cf.x * nc.z + rs(0, -1, 1) * nc.x * cf.z +
+               rs(1, -1, 1) * cf.x * cf.z;
+          v1 = p1 * cf.y + p2 * nc.y;
+          p1 = fb[2] * nc.x * nc.z + fb[3] * cf.x * nc.z + fb[6] * nc.x * cf.z + fb[7] * cf.x * cf.z;
+          p2 = rs(0, 2, 0) * nc.x * nc.z + rs(1, 2, 0) * cf.x * nc.z + rs(0, 2, 1) * nc.x * cf.z +
+               rs(1, 2, 1) * cf.x * cf.z;
+          g.y = p1 * nc.y + p2 * cf.y - v1;
+          p1 = fb[0] * nc.x * nc.y + fb[1] * cf.x * nc.y + fb[2] * nc.x * cf.y + fb[3] * cf.x * cf.y;
+          p2 = rs(0, 0, -1) * nc.x * nc.y + rs(1, 0, -1) * cf.x * nc.y + rs(0, 1, -1) * nc.x * cf.y +
+               rs(1, 1, -1) * cf.x * cf.y;
+          v1 = p1 * cf.z + p2 * nc.z;
+          p1 = fb[4] * nc.x * nc.y + fb[5] * cf.x * nc.y + fb[6] * nc.x * cf.y + fb[7] * cf.x * cf.y;
+          p2 = rs(0, 0, 2) * nc.x * nc.y + rs(1, 0, 2) * cf.x * nc.y + rs(0, 1, 2) * nc.x * cf.y +
+               rs(1, 1, 2) * cf.x * cf.y;
+          g.z = p1 * nc.z + p2 * cf.z - v1;
+          nout = normalize3(g);
+        }
+      }
+      st3(vmap, pid, vout);
+      if (nmap) st3(nmap, pid, nout);
+      if (cmap) std::memcpy(cmap + 4 * pid, col, 4);
+    }
+}
+
+// A19: meshHashScene_kernel (KinfuHashVisualization.cl:88-271) over the visible list, in
+// visible-list order, voxels z-y-x within a block, triangles in table order.  Returns the
+// vertex count (uncapped); positions / colours written up to cap vertices.
+static inline f3 sdf_interp(f3 p1, f3 p2, float v1, float v2) {
+  if (std::fabs(0.0f - v1) < 0.00001f) return p1;
+  if (std::fabs(0.0f - v2) < 0.00001f) return p2;
+  if (std::fabs(v1 - v2) < 0.00001f) return p1;
+  return p1 + (p2 - p1) * ((0.0f - v1) / (v2 - v1));
+}
+
+ORC_API long orc_hash_mesh(const OrcHash* h, float* pos, float* col, long cap) {
+  static const int CO[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+  static const int E[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  long out = 0;
+  for (int id : h->vis_ids) {
+    const HEntry& en = h->e[id];
+    if (en.ptr < 0) continue;
+    const int gx = en.pos[0] * 8, gy = en.pos[1] * 8, gz = en.pos[2] * 8;
+    for (int z = 0; z < 8; ++z)
+      for (int y = 0; y < 8; ++y)
+        for (int x = 0; x < 8; ++x) {
+          float sv[8];
+          f3 pt[8], cl[8];
+          bool ok = true;
+          for (int k = 0; k < 8 && ok; ++k) {
+            const int vx = gx + x + CO[k][0], vy = gy + y + CO[k][1], vz = gz + z + CO[k][2];
+            const long bi = hash_find(h, vx, vy, vz);
+            if (bi < 0) {
+              ok = false;
+              break;
+            }
+            sv[k] = (float)h->sdf[bi] / 32767.0f;
+            pt[k] = mk((float)vx, (float)vy, (float)vz);
+            cl[k] = mk((float)h->rgb[3 * bi], (float)h->rgb[3 * bi + 1], (float)h->rgb[3 * bi + 2]);
+            cl[k] = mk(cl[k].x / 255.f, cl[k].y / 255.f, cl[k].z / 255.f);
+          }
+          if (!ok) continue;
+          int cube = 0;
+          for (int k = 0; k < 8; ++k)
+            if (sv[k] < 0) cube |= 1 << k;
+          const uint64_t word = NUI_MC_TRI_PACKED[cube];
+          const int ntri = (int)(word >> 60);
+          if (ntri == 0) continue;
+          for (int t = 0; t < ntri; ++t)
+            for (int q = 0; q < 3; ++q, ++out) {
+              const int e = (int)((word >> (4 * (3 * t + q))) & 0xF);
+              if (out < cap) {
+                const f3 p = sdf_interp(pt[E[e][0]], pt[E[e][1]], sv[E[e][0]], sv[E[e][1]]) * h->c.voxel;
+                if (pos) st3(pos, out, p);
+                if (col) {
+                  const f3 cc = sdf_interp(cl[E[e][0]], cl[E[e][1]], sv[E[e][0]], sv[E[e][1]]);
+                  col[4 * out] = cc.x;
+                  col[4 * out + 1] = cc.y;
+                  col[4 * out + 2] = cc.z;
+                  col[4 * out + 3] = 1.0f;
+                }
+              }
+            }
+        }
+  }
+  return out;
+}
+
+// accessors for tests
+ORC_API long orc_hash_visible(const OrcHash* h, int* ids, long cap) {
+  const long n = (long)h->vis_ids.size();
+  for (long i = 0; i < n && i < cap; ++i) ids[i] = h->vis_ids[i];
+  return n;
+}
+ORC_API const void* orc_hash_entries(const OrcHash* h) { return h->e.data(); }
+ORC_API const int16_t* orc_hash_sdf(const OrcHash* h) { return h->sdf.data(); }
+ORC_API const uint8_t* orc_hash_weight(const OrcHash* h) { return h->w.data(); }
+ORC_API const uint8_t* orc_hash_rgb(const OrcHash* h) { return h->rgb.data(); }
+ORC_API void orc_hash_counters(const OrcHash* h, int* last_block, int* last_excess, long* failed) {
+  *last_block = h->last_block;
+  *last_excess = h->last_excess;
+  *failed = h->failed_allocs;
+}

@@ -239,3 +239,163 @@ class Engine:
 
     def touched(self):
         return oracle().orc_engine_touched(self.h)
+
+
+# ------------------------------------------------------------------ voxel-block hashing
+class OrcHashCfg(C.Structure):
+    _fields_ = [("buckets", C.c_int), ("excess", C.c_int), ("pool", C.c_int), ("mask", C.c_uint32),
+                ("voxel", C.c_float), ("mu", C.c_float), ("max_w", C.c_int)]
+
+
+HASH_ENTRY = np.dtype([("pos", np.int16, 3), ("pad", np.int16), ("ptr", np.int32), ("offset", np.uint32)])
+REF_VOXEL = np.dtype([("sdf", np.int16), ("rgb", np.uint8, 3), ("w", np.uint8)])
+
+_hash_sigs = {
+    "orc_hash_create": (_P, [_P]),
+    "orc_hash_destroy": (None, [_P]),
+    "orc_hash_reset": (None, [_P]),
+    "orc_hash_allocate": (C.c_long, [_P, _P, _P, _P]),
+    "orc_hash_integrate": (None, [_P, _P, _P, _P, _P, _P]),
+    "orc_hash_raycast": (None, [_P, _P, _P, _P, _P, _P, _P]),
+    "orc_hash_mesh": (C.c_long, [_P, _P, _P, C.c_long]),
+    "orc_hash_visible": (C.c_long, [_P, _P, C.c_long]),
+    "orc_hash_entries": (_P, [_P]),
+    "orc_hash_sdf": (_P, [_P]),
+    "orc_hash_weight": (_P, [_P]),
+    "orc_hash_rgb": (_P, [_P]),
+    "orc_hash_counters": (None, [_P, _P, _P, _P]),
+}
+_ref_hash_sigs = {
+    "ref_hash_sizes": (None, [_P, _P, _P]),
+    "ref_hash_reset": (None, [_P, _P, _P, _P, _P, _P]),
+    "ref_hash_frame": (None, [_P] * 15 + [C.c_float, C.c_float, C.c_int, C.c_int]),
+    "ref_hash_raycast": (None, [_P, _P, _P, C.c_int, _P, _P, C.c_float, C.c_float, _P, _P, _P, _P]),
+    "ref_hash_mesh": (C.c_int, [_P, _P, _P, C.c_int, C.c_float, _P, _P]),
+}
+
+
+def _bind(L, sigs):
+    for k, (r, a) in sigs.items():
+        f = getattr(L, k)
+        f.restype = r
+        f.argtypes = a
+
+
+class OracleHash:
+    """The oracle's voxel-block hash scene."""
+
+    def __init__(self, buckets, excess, pool, voxel=0.005, mu=0.02, max_w=255, mask=None):
+        L = oracle()
+        _bind(L, _hash_sigs)
+        self.cfg = OrcHashCfg(buckets, excess, pool, (buckets - 1) if mask is None else mask, voxel, mu, max_w)
+        self.h = L.orc_hash_create(C.byref(self.cfg))
+        self.n_entries = buckets + excess
+
+    def __del__(self):
+        try:
+            oracle().orc_hash_destroy(self.h)
+        except Exception:
+            pass
+
+    def allocate(self, depth, cam, xform):
+        return oracle().orc_hash_allocate(self.h, p(depth), C.byref(cam), C.byref(xform))
+
+    def integrate(self, depth, bgra, cam, xform):
+        t = C.c_long()
+        oracle().orc_hash_integrate(self.h, p(depth), p(bgra), C.byref(cam), C.byref(xform), C.byref(t))
+        return t.value
+
+    def raycast(self, cam, xform, color=False):
+        N = cam.W * cam.H
+        vm = np.zeros(N * 3, np.float32)
+        nm = np.zeros(N * 3, np.float32)
+        cm = np.zeros(N * 4, np.uint8) if color else None
+        rg = np.zeros(N * 2, np.float32)
+        oracle().orc_hash_raycast(self.h, C.byref(cam), C.byref(xform), p(vm), p(nm), p(cm), p(rg))
+        return vm, nm, cm, rg
+
+    def mesh(self, cap):
+        pos = np.zeros((cap, 3), np.float32)
+        col = np.zeros((cap, 4), np.float32)
+        n = oracle().orc_hash_mesh(self.h, p(pos), p(col), cap)
+        return pos[:min(n, cap)], col[:min(n, cap)], n
+
+    def visible(self):
+        ids = np.zeros(self.n_entries, np.int32)
+        n = oracle().orc_hash_visible(self.h, p(ids), ids.size)
+        return ids[:n].copy()
+
+    def entries(self):
+        ptr_ = oracle().orc_hash_entries(self.h)
+        raw = np.ctypeslib.as_array(C.cast(ptr_, C.POINTER(C.c_uint8)), shape=(self.n_entries * 16,))
+        return raw.copy().view(HASH_ENTRY)
+
+    def voxels(self):
+        n = self.cfg.pool * 512
+        L = oracle()
+        sdf = np.ctypeslib.as_array(C.cast(L.orc_hash_sdf(self.h), C.POINTER(C.c_int16)), shape=(n,)).copy()
+        w = np.ctypeslib.as_array(C.cast(L.orc_hash_weight(self.h), C.POINTER(C.c_uint8)), shape=(n,)).copy()
+        rgb = np.ctypeslib.as_array(C.cast(L.orc_hash_rgb(self.h), C.POINTER(C.c_uint8)), shape=(n, 3)).copy()
+        return sdf, w, rgb
+
+    def counters(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_long()
+        oracle().orc_hash_counters(self.h, C.byref(a), C.byref(b), C.byref(c))
+        return a.value, b.value, c.value
+
+
+class RefHash:
+    """The reference's own hash kernels (host build, test table sizes), run sequentially."""
+
+    def __init__(self, voxel=0.005, mu=0.02, max_w=255):
+        L = ref()
+        _bind(L, _ref_hash_sigs)
+        b, e, pl = C.c_int(), C.c_int(), C.c_int()
+        L.ref_hash_sizes(C.byref(b), C.byref(e), C.byref(pl))
+        self.buckets, self.excess, self.pool = b.value, e.value, pl.value
+        ne = self.buckets + self.excess
+        self.entries = np.zeros(ne, HASH_ENTRY)
+        self.voxels = np.zeros(self.pool * 512, REF_VOXEL)
+        self.alloc_list = np.zeros(self.pool, np.int32)
+        self.excess_list = np.zeros(self.excess, np.int32)
+        self.last = np.zeros(2, np.int32)
+        self.alloc_type = np.zeros(ne, np.uint8)
+        self.vis_type = np.zeros(ne, np.uint8)
+        self.coords = np.zeros(ne * 4, np.int16)
+        self.vis_ids = np.zeros(ne, np.int32)
+        self.nvis = C.c_int(0)
+        self.voxel, self.mu, self.max_w = voxel, mu, max_w
+        last_b, last_e = C.c_int(), C.c_int()
+        L.ref_hash_reset(p(self.entries), p(self.voxels), p(self.alloc_list), p(self.excess_list), C.byref(last_b),
+                         C.byref(last_e))
+        self.last[:] = [last_b.value, last_e.value]
+
+    def frame(self, depth, bgra, cam, xform, integrate=True):
+        lb = self.last[0:1]
+        le = self.last[1:2]
+        ref().ref_hash_frame(p(self.entries), p(self.voxels), p(self.alloc_list), p(self.excess_list), p(lb), p(le),
+                             p(self.alloc_type), p(self.vis_type), p(self.coords), p(self.vis_ids),
+                             C.byref(self.nvis), p(depth), p(bgra), p(cam.flat()), p(xform.flat()), self.voxel,
+                             self.mu, self.max_w, 1 if integrate else 0)
+        return self.nvis.value
+
+    def visible(self):
+        return self.vis_ids[:self.nvis.value].copy()
+
+    def raycast(self, cam, xform, color=False):
+        N = cam.W * cam.H
+        vm = np.zeros(N * 3, np.float32)
+        nm = np.zeros(N * 3, np.float32)
+        cm = np.zeros(N * 4, np.uint8) if color else None
+        rg = np.zeros(N * 2, np.float32)
+        ref().ref_hash_raycast(p(self.entries), p(self.voxels), p(self.vis_ids), self.nvis.value, p(cam.flat()),
+                               p(xform.flat()), self.voxel, self.mu, p(rg), p(vm), p(nm), p(cm))
+        return vm, nm, cm, rg
+
+    def mesh(self):
+        cap = 5_000_000 + 3  # the kernel stops at MAX_OUTPUT_VERTEX_SIZE (+2, its `>` check)
+        pos = np.zeros((cap, 3), np.float32)
+        col = np.zeros((cap, 4), np.float32)
+        n = ref().ref_hash_mesh(p(self.entries), p(self.voxels), p(self.vis_ids), self.nvis.value, self.voxel, p(pos),
+                                p(col))
+        return pos[:n], col[:n], n
