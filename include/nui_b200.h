@@ -82,6 +82,17 @@ typedef struct {
   float depth_threshold;      /* icp_depth_threshold */
   float dist_threshold;       /* icp_dist_threshold */
   float integration_threshold;/* m_integration_metric_threshold */
+  /* voxel-block hash (volume_kind == NUI_VOLUME_HASH); NuiHashingSDFConfig
+   * (NuiHashingSDFConfig.cpp:3-15).  Table sizes are runtime parameters here; the
+   * reference fixes them at compile time (hashing_gpu_def.h:9-20).  tsdf_format selects
+   * the voxel sdf storage: NUI_TSDF_I16 = the reference's int16 (sdf * 32767), anything
+   * else = half; weights are uint8 (cap hash_max_weight) and colours RGB8. */
+  float voxel_size;           /* m_virtualVoxelSize */
+  float trunc_scale;          /* m_truncScale */
+  int hash_buckets;           /* power of two; hash mask = buckets - 1 */
+  int hash_excess;            /* excess (collision) list length */
+  int hash_pool_blocks;       /* 8^3 voxel blocks in the pool */
+  int hash_max_weight;        /* m_integrationWeightMax */
 } nui_session_cfg;
 
 typedef struct nui_ctx nui_ctx;
@@ -159,6 +170,12 @@ NUI_API nui_status nui_mesh_cases(nui_session* s, uint8_t* cases, size_t bytes, 
  *   6 raw volume storage of the session format   7 depth level `level` (f32)
  *   8 reference colour map (u8x4)        9 colour volume, reference layout (u8x4)  */
 NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void* host, size_t bytes);
+/* Voxel-hash sessions: what = 20 entries (16 B each: short pos[3], pad, int ptr, uint
+ * offset), 21 visible list (int, count = nui_hash_stats visible), 22 pool voxels in the
+ * reference voxel layout (short sdf, uchar rgb[3], uchar weight; 6 B each), 23 expected
+ * range image (float2 per pixel). */
+NUI_API nui_status nui_hash_stats(nui_session* s, int* visible, int* last_free_block, int* last_free_excess,
+                                  int* failed_allocs);
 /* Writes a reference-layout short2 volume into the session (any format). */
 NUI_API nui_status nui_debug_upload_volume(nui_session* s, const int16_t* ref_layout_short2);
 

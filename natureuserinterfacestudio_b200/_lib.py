@@ -23,6 +23,7 @@ NUI_ERR_DEVICE = 7
 NUI_ERR_UNSUPPORTED = 8
 
 TSDF_I16, TSDF_F32, TSDF_F16_U8, TSDF_F16_F16 = 0, 1, 2, 3
+VOLUME_DENSE, VOLUME_HASH = 0, 1
 SYNTH_TABLETOP, SYNTH_ROOM = 0, 1
 
 
@@ -38,6 +39,8 @@ class SessionCfg(C.Structure):
         ("sigma_space2_inv_half", C.c_float), ("sigma_depth2_inv_half", C.c_float),
         ("depth_threshold", C.c_float), ("dist_threshold", C.c_float),
         ("integration_threshold", C.c_float),
+        ("voxel_size", C.c_float), ("trunc_scale", C.c_float), ("hash_buckets", C.c_int),
+        ("hash_excess", C.c_int), ("hash_pool_blocks", C.c_int), ("hash_max_weight", C.c_int),
     ]
 
 
@@ -74,6 +77,7 @@ _SIGS = {
     "nui_mesh_cases": (C.c_int, [_P, _P, C.c_size_t, _P]),
     "nui_debug_download": (C.c_int, [_P, C.c_int, C.c_int, _P, C.c_size_t]),
     "nui_debug_upload_volume": (C.c_int, [_P, _P]),
+    "nui_hash_stats": (C.c_int, [_P, _P, _P, _P, _P]),
     "nui_batch_tick": (C.c_int, [_P, _P, C.c_int, _P, _P, _P, _P]),
     "nui_batch_tick_device": (C.c_int, [_P, _P, C.c_int, _P, _P, _P, _P]),
     "nui_ctx_enable_timing": (C.c_int, [_P, C.c_int]),
@@ -275,6 +279,27 @@ class Session:
         shape, dt = shapes[what]
         out = np.zeros(shape, dt)
         check(lib().nui_debug_download(self.h, what, level, ptr(out), out.nbytes))
+        return out
+
+    def hash_stats(self):
+        v, b, e, f = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib().nui_hash_stats(self.h, C.byref(v), C.byref(b), C.byref(e), C.byref(f)))
+        return v.value, b.value, e.value, f.value
+
+    def hash_download(self, what):
+        """20 entries, 21 visible list, 22 voxels (reference layout), 23 range image."""
+        c = self.cfg
+        ne = c.hash_buckets + c.hash_excess
+        if what == 20:
+            out = np.zeros(ne * 16, np.uint8)
+        elif what == 21:
+            out = np.zeros(self.hash_stats()[0], np.int32)
+        elif what == 22:
+            out = np.zeros(c.hash_pool_blocks * 512 * 6, np.uint8)
+        else:
+            out = np.zeros(self.W * self.H * 2, np.float32)
+        if out.size:
+            check(lib().nui_debug_download(self.h, what, 0, ptr(out), out.nbytes))
         return out
 
     def volume_ref_layout(self):

@@ -85,6 +85,35 @@ struct SessionDesc {
   // tracking state and ICP scratch
   TrackState* ts;
   float2* partials;               // per-block (hi, lo) sums, kIcpTerms per block
+  // voxel-block hash (volume_kind == hash; fmt is then -1 so the dense kernels skip)
+  int hash;                       // 1 for a hash session
+  int hfmt;                       // 0: int16 sdf (reference), 1: half sdf
+  struct HEntry* entries;         // buckets + excess entries
+  int nb, ne, np;                 // buckets, excess list length, pool blocks
+  unsigned int hmask;
+  float voxel, mu;                // virtualVoxelSize, truncScale
+  int max_w;                      // integrationWeightMax
+  void* hsdf;                     // np * 512 sdf (int16 or half)
+  uint8_t* hw;                    // np * 512 weights
+  uchar4* hrgb;                   // np * 512 colours (nullable)
+  int* alloc_list;                // free-block stack
+  int* excess_list;               // free excess-slot stack
+  int* hcount;                    // [0] last free block, [1] last free excess, [2] visible count, [3] failed allocations
+  uint8_t* alloc_type;            // per entry
+  uint8_t* vis;                   // per entry visible type
+  short4* coords;                 // per entry block coordinates of a pending allocation
+  unsigned long long* keys;       // per entry: last writer key of a pending allocation
+  int* vis_ids;                   // visible list
+  unsigned int* blk;              // scan scratch: per 1024 entries, 2 counts + 2 offsets
+  float2* range;                  // expected range image
+};
+
+// Hash entry (NuiKinfuHashEntry, hashing_gpu_def.h:49-63): 16 bytes.
+struct __align__(16) HEntry {
+  short pos[3];
+  short pad;
+  int ptr;
+  unsigned int offset;
 };
 
 // ------------------------------------------------------------------ float helpers

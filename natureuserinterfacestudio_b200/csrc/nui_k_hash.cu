@@ -1,0 +1,860 @@
+// Voxel-block hashing on the GPU (KinfuHashScene.cl, KinfuHashRaycast.cl; host
+// NuiKinfuOpenCLHashScene.cpp AllocateSceneFromDepth / IntegrateIntoScene / raycastRender).
+//
+// Per frame, for every hash session of the batch:
+//   k_hash_prepare      visible types of the last frame's list -> 3, allocation types -> 0
+//   k_hash_walk(0)      per pixel: walk [d - mu, d + mu] along the ray in block units; mark
+//                       found blocks visible, mark missing ones for allocation and keep, per
+//                       entry slot, the largest (pixel, step) key that wanted it
+//   k_hash_walk(1)      the walk again: the key owner writes its block coordinates (the
+//                       block the last writer in raster order would have left)
+//   k_hash_count(0) + k_hash_scan + k_hash_alloc
+//                       entries needing allocation, ranked in index order, pop blocks from
+//                       the free stack (and excess slots for chain appends) in that order
+//   k_hash_visible      previously visible entries (type 3): 8-corner frustum test
+//   k_hash_count(1) + k_hash_scan + k_hash_compact
+//                       visible list = entries with visible type > 0 in index order
+//   k_hash_integrate    one 512-thread block per visible entry, one voxel per thread
+//   k_hash_range + k_hash_project + k_hash_raycast
+//                       expected range image by atomic min/max of projected block boxes,
+//                       then castRay per pixel
+// Arithmetic follows the reference kernels operation by operation (the library is built
+// without contraction), so all outputs match the CPU restatement bit for bit.
+#include "nui_device.cuh"
+
+namespace nui {
+
+constexpr int kHashScanBlock = 1024;
+
+__device__ __forceinline__ unsigned hash_index(unsigned mask, int x, int y, int z) {
+  return (((unsigned)x * 73856093u) ^ ((unsigned)y * 19349669u) ^ ((unsigned)z * 83492791u)) & mask;
+}
+__device__ __forceinline__ HEntry load_entry(const HEntry* e, unsigned i) {
+  const int4 v = __ldcg(reinterpret_cast<const int4*>(e) + i);
+  HEntry r;
+  r.pos[0] = (short)(v.x & 0xffff);
+  r.pos[1] = (short)((unsigned)v.x >> 16);
+  r.pos[2] = (short)(v.y & 0xffff);
+  r.pad = (short)((unsigned)v.y >> 16);
+  r.ptr = v.z;
+  r.offset = (unsigned)v.w;
+  return r;
+}
+__device__ __forceinline__ void store_entry(HEntry* e, unsigned i, const HEntry& r) {
+  int4 v;
+  v.x = (int)((unsigned short)r.pos[0] | ((unsigned)(unsigned short)r.pos[1] << 16));
+  v.y = (int)((unsigned short)r.pos[2] | ((unsigned)(unsigned short)r.pad << 16));
+  v.z = r.ptr;
+  v.w = (int)r.offset;
+  reinterpret_cast<int4*>(e)[i] = v;
+}
+__device__ __forceinline__ float3 xf_apply(const DevXform& m, float3 v) {
+  return add3(rot_rows(m.R, v), f3(m.t[0], m.t[1], m.t[2]));
+}
+__device__ __forceinline__ float3 xf_inverse(const DevXform& m, float3 v) {
+  return rot_rows(m.R_inv, sub3(v, f3(m.t[0], m.t[1], m.t[2])));
+}
+// pass-filtered z-depth of a pixel (depth_passing_filter_kernel, filters.cl:9-23)
+__device__ __forceinline__ float pass_depth(const SessionDesc& s, int i) {
+  const float dp = (float)s.raw[i] * 0.001f;
+  return (dp > s.cam.dmin && dp < s.cam.dmax) ? dp : qnan();
+}
+// kinectDepthToSkeleton (cameraUtils.cl:46-53)
+__device__ __forceinline__ float3 depth_to_point(const DevCam& c, int ux, int uy, float d) {
+  const float x = ((float)ux - c.cx) / c.fx, y = ((float)uy - c.cy) / c.fy;
+  return f3(d * x, d * y, d);
+}
+__device__ __forceinline__ bool hash_active(const SessionDesc& s) { return s.hash && s.kind >= 0 && s.ts->integrate; }
+
+// ------------------------------------------------------------------ allocation
+__global__ void k_hash_prepare(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!hash_active(s)) return;
+  const unsigned n = (unsigned)(s.nb + s.ne);
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    s.alloc_type[i] = 0;
+    s.vis[i] = s.vis[i] ? 3 : 0;
+  }
+}
+
+// buildHashAllocAndVisibleType_kernel (KinfuHashScene.cl:52-136); pass 1 writes the
+// coordinates of the last writer of each pending slot.
+__global__ void __launch_bounds__(256) k_hash_walk(const SessionDesc* __restrict__ descs, int pass) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!hash_active(s)) return;
+  const int W = s.W, H = s.H;
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= W * H) return;
+  const float Dp = pass_depth(s, id);
+  if (isnan(Dp)) return;
+  const int px = id % W, py = id / W;
+  const DevXform& m = s.ts->xf;
+  const float3 pc = depth_to_point(s.cam, px, py, Dp);
+  const float norm = s.mu / sqrtf(dot3(pc, pc));
+  const float obs = 1.0f / (s.voxel * 8);
+  float3 rmin = mul3(xf_apply(m, mul3(pc, 1.0f - norm)), obs);
+  const float3 rmax = mul3(xf_apply(m, mul3(pc, 1.0f + norm)), obs);
+  float3 rdir = sub3(rmax, rmin);
+  const float rn = sqrtf(dot3(rdir, rdir));
+  const int steps = (int)ceilf(2.0f * rn);
+  const float dv = (float)(steps - 1);
+  rdir = f3(rdir.x / dv, rdir.y / dv, rdir.z / dv);
+  for (int i = 0; i < steps; ++i) {
+    const short bx = (short)floorf(rmin.x), by = (short)floorf(rmin.y), bz = (short)floorf(rmin.z);
+    unsigned hi = hash_index(s.hmask, bx, by, bz);
+    HEntry en = load_entry(s.entries, hi);
+    bool found = false;
+    if (en.pos[0] == bx && en.pos[1] == by && en.pos[2] == bz && en.ptr >= -1) {
+      if (pass == 0) s.vis[hi] = (en.ptr == -1) ? 2 : 1;
+      found = true;
+    }
+    if (!found) {
+      bool excess = false;
+      if (en.ptr >= -1) {
+        while (en.offset >= 1) {
+          hi = (unsigned)s.nb + en.offset - 1;
+          en = load_entry(s.entries, hi);
+          if (en.pos[0] == bx && en.pos[1] == by && en.pos[2] == bz && en.ptr >= -1) {
+            if (pass == 0) s.vis[hi] = (en.ptr == -1) ? 2 : 1;
+            found = true;
+            break;
+          }
+        }
+        excess = true;
+      }
+      if (!found) {
+        const unsigned long long key = ((unsigned long long)(id + 1) << 16) | (unsigned long long)(i & 0xffff);
+        if (pass == 0) {
+          s.alloc_type[hi] = excess ? 2 : 1;
+          s.vis[hi] = 1;
+          atomicMax(&s.keys[hi], key);
+        } else if (__ldcg(&s.keys[hi]) == key) {
+          s.coords[hi] = make_short4(bx, by, bz, 0);
+        }
+      }
+    }
+    rmin = add3(rmin, rdir);
+  }
+}
+
+// Per 1024 entries: number of entries needing a block (type >= 1) and an excess slot
+// (type 2) (which == 0), or of visible entries (which == 1).
+__global__ void __launch_bounds__(256) k_hash_count(const SessionDesc* __restrict__ descs, int which) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!hash_active(s)) return;
+  const unsigned n = (unsigned)(s.nb + s.ne);
+  const unsigned b0 = blockIdx.x * kHashScanBlock;
+  if (b0 >= n) return;
+  unsigned a = 0, e = 0;
+  for (unsigned i = b0 + threadIdx.x; i < min(n, b0 + kHashScanBlock); i += blockDim.x) {
+    if (which == 0) {
+      const uint8_t t = s.alloc_type[i];
+      a += t != 0;
+      e += t == 2;
+    } else {
+      a += s.vis[i] > 0;
+    }
+  }
+  a = __reduce_add_sync(0xffffffffu, a);
+  e = __reduce_add_sync(0xffffffffu, e);
+  __shared__ unsigned sa[8], se[8];
+  if ((threadIdx.x & 31) == 0) {
+    sa[threadIdx.x >> 5] = a;
+    se[threadIdx.x >> 5] = e;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned ta = 0, te = 0;
+    for (int w = 0; w < 8; ++w) {
+      ta += sa[w];
+      te += se[w];
+    }
+    s.blk[4 * blockIdx.x] = ta;
+    s.blk[4 * blockIdx.x + 1] = te;
+  }
+}
+
+// Exclusive scan of the per-block counts of one session (one 1024-thread block per
+// session); offsets go to blk[4b + 2], blk[4b + 3].  Totals: allocation -> updates the free
+// stacks; visible -> visible count.
+__global__ void __launch_bounds__(1024) k_hash_scan(const SessionDesc* __restrict__ descs, int which) {
+  const SessionDesc& s = descs[blockIdx.x];
+  if (!hash_active(s)) return;
+  const int nblk = (s.nb + s.ne + kHashScanBlock - 1) / kHashScanBlock;
+  __shared__ unsigned wa[32], we[32];
+  __shared__ unsigned carry_a, carry_e;
+  if (threadIdx.x == 0) carry_a = carry_e = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int base = 0; base < nblk; base += 1024) {
+    const int i = base + threadIdx.x;
+    const unsigned va = i < nblk ? s.blk[4 * i] : 0u, ve = i < nblk ? s.blk[4 * i + 1] : 0u;
+    unsigned ia = va, ie = ve;
+    for (int off = 1; off < 32; off <<= 1) {
+      const unsigned oa = __shfl_up_sync(0xffffffffu, ia, off), oe = __shfl_up_sync(0xffffffffu, ie, off);
+      if (lane >= off) {
+        ia += oa;
+        ie += oe;
+      }
+    }
+    if (lane == 31) {
+      wa[warp] = ia;
+      we[warp] = ie;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      const unsigned a = wa[lane], e = we[lane];
+      unsigned xa = a, xe = e;
+      for (int off = 1; off < 32; off <<= 1) {
+        const unsigned oa = __shfl_up_sync(0xffffffffu, xa, off), oe = __shfl_up_sync(0xffffffffu, xe, off);
+        if (lane >= off) {
+          xa += oa;
+          xe += oe;
+        }
+      }
+      wa[lane] = xa - a;
+      we[lane] = xe - e;
+    }
+    __syncthreads();
+    const unsigned ea = carry_a + wa[warp] + ia - va, ee = carry_e + we[warp] + ie - ve;
+    __syncthreads();
+    if (i < nblk) {
+      s.blk[4 * i + 2] = ea;
+      s.blk[4 * i + 3] = ee;
+    }
+    if (threadIdx.x == 1023) {
+      carry_a = ea + va;
+      carry_e = ee + ve;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (which == 1) s.hcount[2] = (int)carry_a;
+  }
+}
+
+// Rank of entry i among the entries of its 1024-block satisfying `pred` (block-wide scan in
+// index order).  All threads of the block must call it.
+template <class Pred>
+__device__ __forceinline__ unsigned block_rank(unsigned i, unsigned n, Pred pred, bool& flag, unsigned& total) {
+  __shared__ unsigned wsum[kHashScanBlock / 32];
+  flag = i < n && pred(i);
+  const unsigned ballot = __ballot_sync(0xffffffffu, flag);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) wsum[warp] = __popc(ballot);
+  __syncthreads();
+  unsigned before = 0;
+  for (int w = 0; w < warp; ++w) before += wsum[w];
+  total = 0;
+  for (int w = 0; w < kHashScanBlock / 32; ++w) total += wsum[w];
+  __syncthreads();
+  return before + __popc(ballot & ((1u << lane) - 1u));
+}
+
+// allocateVoxelBlocksList_kernel (KinfuHashScene.cl:138-194) with the pops in index order.
+__global__ void __launch_bounds__(kHashScanBlock) k_hash_alloc(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!hash_active(s)) return;
+  const unsigned n = (unsigned)(s.nb + s.ne);
+  const unsigned b = blockIdx.x;
+  if (b * kHashScanBlock >= n) return;
+  const unsigned i = b * kHashScanBlock + threadIdx.x;
+  bool fa, fe;
+  unsigned ta, te;
+  const unsigned ra = block_rank(i, n, [&](unsigned k) { return s.alloc_type[k] != 0; }, fa, ta);
+  const unsigned re = block_rank(i, n, [&](unsigned k) { return s.alloc_type[k] == 2; }, fe, te);
+  if (!fa) return;
+  const int last_block = s.hcount[0], last_excess = s.hcount[1];
+  const int vba = last_block - (int)(s.blk[4 * b + 2] + ra);
+  const uint8_t t = s.alloc_type[i];
+  const short4 c = s.coords[i];
+  s.keys[i] = 0ull;
+  if (t == 1) {
+    if (vba >= 0) {
+      HEntry en;
+      en.pos[0] = c.x;
+      en.pos[1] = c.y;
+      en.pos[2] = c.z;
+      en.pad = 0;
+      en.ptr = s.alloc_list[vba];
+      en.offset = 0;
+      store_entry(s.entries, i, en);
+    } else {
+      atomicAdd(&s.hcount[3], 1);
+    }
+  } else {
+    const int exl = last_excess - (int)(s.blk[4 * b + 3] + re);
+    if (vba >= 0 && exl >= 0) {
+      HEntry en;
+      en.pos[0] = c.x;
+      en.pos[1] = c.y;
+      en.pos[2] = c.z;
+      en.pad = 0;
+      en.ptr = s.alloc_list[vba];
+      en.offset = 0;
+      const int off = s.excess_list[exl];
+      HEntry parent = load_entry(s.entries, i);
+      parent.offset = (unsigned)off + 1;
+      store_entry(s.entries, i, parent);
+      store_entry(s.entries, (unsigned)s.nb + off, en);
+      s.vis[s.nb + off] = 1;
+    } else {
+      atomicAdd(&s.hcount[3], 1);
+    }
+  }
+}
+
+// After k_hash_alloc: pop the free stacks by the number of requests (as the reference's
+// atomic_dec calls do, successful or not).
+__global__ void k_hash_alloc_done(const SessionDesc* __restrict__ descs, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const SessionDesc& s = descs[k];
+  if (!hash_active(s)) return;
+  const int nblk = (s.nb + s.ne + kHashScanBlock - 1) / kHashScanBlock;
+  const unsigned ta = s.blk[4 * (nblk - 1) + 2] + s.blk[4 * (nblk - 1)];
+  const unsigned te = s.blk[4 * (nblk - 1) + 3] + s.blk[4 * (nblk - 1) + 1];
+  s.hcount[0] -= (int)ta;
+  s.hcount[1] -= (int)te;
+}
+
+// buildVisibleList_kernel + checkBlockVisibility (KinfuHashScene.cl:196-285)
+__device__ __forceinline__ bool point_visible(const SessionDesc& s, const DevXform& m, float3 p) {
+  const float3 q = xf_inverse(m, p);
+  if (isnan3(q)) return false;
+  const int sx = (int)(q.x * s.cam.fx / q.z + s.cam.cx + 0.5f), sy = (int)(q.y * s.cam.fy / q.z + s.cam.cy + 0.5f);
+  return sx >= 0 && sx < s.W && sy >= 0 && sy < s.H;
+}
+__global__ void k_hash_visible(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!hash_active(s)) return;
+  const unsigned n = (unsigned)(s.nb + s.ne);
+  const DevXform& m = s.ts->xf;
+  const float factor = 8.0f * s.voxel;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (s.vis[i] != 3) continue;
+    const HEntry en = load_entry(s.entries, i);
+    float3 p = f3((float)en.pos[0] * factor, (float)en.pos[1] * factor, (float)en.pos[2] * factor);
+    bool v = point_visible(s, m, p);
+    if (!v) { p.z += factor; v = point_visible(s, m, p); }
+    if (!v) { p.y += factor; v = point_visible(s, m, p); }
+    if (!v) { p.x += factor; v = point_visible(s, m, p); }
+    if (!v) { p.z -= factor; v = point_visible(s, m, p); }
+    if (!v) { p.y -= factor; v = point_visible(s, m, p); }
+    if (!v) { p.x -= factor; p.y += factor; v = point_visible(s, m, p); }
+    if (!v) { p.x += factor; p.y -= factor; p.z += factor; v = point_visible(s, m, p); }
+    if (!v) s.vis[i] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kHashScanBlock) k_hash_compact(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!hash_active(s)) return;
+  const unsigned n = (unsigned)(s.nb + s.ne);
+  const unsigned b = blockIdx.x;
+  if (b * kHashScanBlock >= n) return;
+  const unsigned i = b * kHashScanBlock + threadIdx.x;
+  bool f;
+  unsigned t;
+  const unsigned r = block_rank(i, n, [&](unsigned k) { return s.vis[k] > 0; }, f, t);
+  if (f) s.vis_ids[s.blk[4 * b + 2] + r] = (int)i;
+}
+
+// ------------------------------------------------------------------ integration
+template <int HF>
+struct HVox;
+template <>
+struct HVox<0> {  // reference int16 sdf (KinfuHashScene.cl:438, 468)
+  __device__ static __forceinline__ float load(const void* p, unsigned i) {
+    return (float)reinterpret_cast<const short*>(p)[i] / 32767.0f;
+  }
+  __device__ static __forceinline__ void store(void* p, unsigned i, float f) {
+    reinterpret_cast<short*>(p)[i] = (short)__float2int_rz(f * 32767.0f);
+  }
+};
+template <>
+struct HVox<1> {  // half sdf
+  __device__ static __forceinline__ float load(const void* p, unsigned i) {
+    return __half2float(reinterpret_cast<const __half*>(p)[i]);
+  }
+  __device__ static __forceinline__ void store(void* p, unsigned i, float f) {
+    reinterpret_cast<__half*>(p)[i] = __float2half_rn(f);
+  }
+};
+
+// integrateIntoScene_kernel (KinfuHashScene.cl:387-470); blocks stride over the list.
+template <int HF>
+__global__ void __launch_bounds__(512) k_hash_integrate(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!hash_active(s) || s.hfmt != HF) return;
+  const int nvis = s.hcount[2];
+  const DevXform& m = s.ts->xf;
+  const int lid = threadIdx.x;
+  const int lx = (lid % 64) % 8, ly = (lid % 64) / 8, lz = lid / 64;
+  unsigned touched = 0;
+  for (int k = blockIdx.x; k < nvis; k += gridDim.x) {
+    const HEntry en = load_entry(s.entries, (unsigned)s.vis_ids[k]);
+    if (en.ptr < 0) continue;
+    const unsigned bid = (unsigned)en.ptr * 512u + (unsigned)lid;
+    const int w = s.hw[bid];
+    if (s.max_w == w) continue;
+    const float3 pm = mul3(f3((float)(en.pos[0] * 8 + lx), (float)(en.pos[1] * 8 + ly), (float)(en.pos[2] * 8 + lz)),
+                           s.voxel);
+    const float3 pc = xf_inverse(m, pm);
+    if (pc.z <= 0) continue;
+    const int ix = (int)(pc.x * s.cam.fx / pc.z + s.cam.cx + 0.5f), iy = (int)(pc.y * s.cam.fy / pc.z + s.cam.cy + 0.5f);
+    if (ix < 0 || ix >= s.W || iy < 0 || iy >= s.H) continue;
+    const int sid = iy * s.W + ix;
+    const float d = pass_depth(s, sid);
+    if (isnan(d)) continue;
+    const float eta = d - pc.z;
+    const float sdf = eta / s.mu;
+    if (eta < -s.mu) continue;
+    const float oldF = HVox<HF>::load(s.hsdf, bid), oldW = (float)w;
+    float newF = fminf(1.0f, sdf);
+    const float newW = 1.0f, cw = oldW + newW;
+    if (s.bgra && s.hrgb && eta < s.mu && fabsf(sdf) < 0.25f) {
+      const uchar4 col = reinterpret_cast<const uchar4*>(s.bgra)[sid];
+      if (col.w == 255) {
+        const uchar4 vc = s.hrgb[bid];
+        const float r = (oldW * (float)vc.x + newW * (float)col.z) / cw;
+        const float g = (oldW * (float)vc.y + newW * (float)col.y) / cw;
+        const float bl = (oldW * (float)vc.z + newW * (float)col.x) / cw;
+        s.hrgb[bid] = make_uchar4((unsigned char)fminf(fmaxf(r, 0.f), 255.f), (unsigned char)fminf(fmaxf(g, 0.f), 255.f),
+                                  (unsigned char)fminf(fmaxf(bl, 0.f), 255.f), 0);
+      }
+    }
+    newF = oldW * oldF + newW * newF;
+    newF /= cw;
+    HVox<HF>::store(s.hsdf, bid, newF);
+    s.hw[bid] = (uint8_t)min((int)(uint8_t)cw, s.max_w);
+    ++touched;
+  }
+  const unsigned t = __reduce_add_sync(0xffffffffu, touched);
+  if ((threadIdx.x & 31) == 0 && t) atomicAdd(&s.ts->touched, (unsigned long long)t);
+}
+
+// ------------------------------------------------------------------ raycast
+__global__ void k_hash_range(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!s.hash || s.kind != kTrackFrame || s.ts->status != 0) return;
+  const int n = s.W * s.H;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    s.range[i] = make_float2(999999.9f, 0.05f);
+}
+
+// project_minmax_depths_kernel (KinfuHashRaycast.cl:4-76) with atomic min / max per pixel
+// (positive floats order like their bit patterns).
+__global__ void k_hash_project(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!s.hash || s.kind != kTrackFrame || s.ts->status != 0) return;
+  const int nvis = s.hcount[2];
+  const DevXform& m = s.ts->xf;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nvis; k += gridDim.x * blockDim.x) {
+    const HEntry en = load_entry(s.entries, (unsigned)s.vis_ids[k]);
+    if (en.ptr < 0) continue;
+    int ulx = s.W, uly = s.H, lrx = 0, lry = 0;
+    float zx = 999999.9f, zy = 0.05f;
+    for (int corner = 0; corner < 8; ++corner) {
+      const short cx = (short)(en.pos[0] + ((corner & 1) ? 1 : 0)), cy = (short)(en.pos[1] + ((corner & 2) ? 1 : 0)),
+                  cz = (short)(en.pos[2] + ((corner & 4) ? 1 : 0));
+      float3 p = mul3(mul3(f3((float)cx, (float)cy, (float)cz), 8.0f), s.voxel);
+      p = xf_inverse(m, p);
+      if (isnan3(p) || p.z < 1e-6) continue;
+      const float u = p.x * s.cam.fx / p.z + s.cam.cx, v = p.y * s.cam.fy / p.z + s.cam.cy;
+      ulx = min(ulx, (int)floorf(u));
+      lrx = max(lrx, (int)ceilf(u));
+      uly = min(uly, (int)floorf(v));
+      lry = max(lry, (int)ceilf(v));
+      zx = fminf(zx, p.z);
+      zy = fmaxf(zx, p.z);
+    }
+    if (ulx < 0) ulx = 0;
+    if (uly < 0) uly = 0;
+    if (lrx >= s.W) lrx = s.W - 1;
+    if (lry >= s.H) lry = s.H - 1;
+    if (zx < 0.05f) zx = 0.05f;
+    for (int by = uly; by <= lry; ++by)
+      for (int bx = ulx; bx <= lrx; ++bx) {
+        float2* r = s.range + by * s.W + bx;
+        atomicMin(reinterpret_cast<int*>(&r->x), __float_as_int(zx));
+        atomicMax(reinterpret_cast<int*>(&r->y), __float_as_int(zy));
+      }
+  }
+}
+
+template <int HF>
+struct HashRead {
+  const SessionDesc& s;
+  short cbx, cby, cbz;
+  int cptr;  // cached block (findVoxelBlockIndex's cache; transparent to results)
+  __device__ __forceinline__ int find(int vx, int vy, int vz) {
+    int bx = vx < 0 ? vx - 7 : vx, by = vy < 0 ? vy - 7 : vy, bz = vz < 0 ? vz - 7 : vz;
+    bx /= 8;
+    by /= 8;
+    bz /= 8;
+    const int lin = (vx - 8 * bx) + 8 * (vy - 8 * by) + 64 * (vz - 8 * bz);
+    const short sx = (short)bx, sy = (short)by, sz = (short)bz;
+    if (cptr >= 0 && sx == cbx && sy == cby && sz == cbz) return cptr + lin;
+    unsigned hi = hash_index(s.hmask, sx, sy, sz);
+    for (;;) {
+      const HEntry en = load_entry(s.entries, hi);
+      if (en.pos[0] == sx && en.pos[1] == sy && en.pos[2] == sz && en.ptr >= 0) {
+        cbx = sx;
+        cby = sy;
+        cbz = sz;
+        cptr = en.ptr * 512;
+        return cptr + lin;
+      }
+      if (en.offset < 1) break;
+      hi = (unsigned)s.nb + en.offset - 1;
+    }
+    return -1;
+  }
+  __device__ __forceinline__ float sdf_at(int vx, int vy, int vz) {
+    const int bi = find(vx, vy, vz);
+    return bi < 0 ? 1.0f : HVox<HF>::load(s.hsdf, (unsigned)bi);
+  }
+};
+
+// castRay + raycast_kernel (KinfuHashRaycast.cl:155-471)
+template <int HF>
+__global__ void __launch_bounds__(128) k_hash_raycast(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!s.hash || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
+  const int W = s.W, H = s.H;
+  const int pid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pid >= W * H) return;
+  const int px = pid % W, py = pid / W;
+  const DevXform& m = s.ts->xf;
+  HashRead<HF> R{s, 0, 0, 0, -1};
+  const float2 mm = s.range[pid];
+  const float oov = 1.0f / s.voxel;
+  const float stepScale = s.mu * oov * 0.6f;
+  float3 ps = depth_to_point(s.cam, px, py, mm.x);
+  float total = sqrtf(dot3(ps, ps)) * oov;
+  ps = mul3(xf_apply(m, ps), oov);
+  float3 pe = depth_to_point(s.cam, px, py, mm.y);
+  const float totalMax = sqrtf(dot3(pe, pe)) * oov;
+  pe = mul3(xf_apply(m, pe), oov);
+  float sdfv = 1.0f, stepLen;
+  const float3 dir = normalize3(sub3(pe, ps));
+  float3 pr = ps;
+  while (total < totalMax) {
+    const int vx = (int)roundf(pr.x), vy = (int)roundf(pr.y), vz = (int)roundf(pr.z);
+    const int bi = R.find(vx, vy, vz);
+    if (bi < 0) {
+      sdfv = 1.0f;
+      stepLen = 8.0f;
+    } else {
+      sdfv = HVox<HF>::load(s.hsdf, (unsigned)bi);
+      if (sdfv <= 0.1f && sdfv >= -0.5f) {
+        const int ix = (int)floorf(pr.x), iy = (int)floorf(pr.y), iz = (int)floorf(pr.z);
+        const float3 cf = f3(pr.x - (float)ix, pr.y - (float)iy, pr.z - (float)iz);
+        float v1 = R.sdf_at(ix, iy, iz), v2 = R.sdf_at(ix + 1, iy, iz);
+        float r1 = (1.0f - cf.x) * v1 + cf.x * v2;
+        v1 = R.sdf_at(ix, iy + 1, iz);
+        v2 = R.sdf_at(ix + 1, iy + 1, iz);
+        r1 = (1.0f - cf.y) * r1 + cf.y * ((1.0f - cf.x) * v1 + cf.x * v2);
+        v1 = R.sdf_at(ix, iy, iz + 1);
+        v2 = R.sdf_at(ix + 1, iy, iz + 1);
+        float r2 = (1.0f - cf.x) * v1 + cf.x * v2;
+        v1 = R.sdf_at(ix, iy + 1, iz + 1);
+        v2 = R.sdf_at(ix + 1, iy + 1, iz + 1);
+        r2 = (1.0f - cf.y) * r2 + cf.y * ((1.0f - cf.x) * v1 + cf.x * v2);
+        sdfv = (1.0f - cf.z) * r1 + cf.z * r2;
+      }
+      if (sdfv <= 0.0f) break;
+      stepLen = fmaxf(sdfv * stepScale, 1.0f);
+    }
+    pr = add3(pr, mul3(dir, stepLen));
+    total += stepLen;
+  }
+  const float4 nanv = make_float4(qnan(), qnan(), qnan(), 0.f);
+  float4 vout = nanv, nout = nanv;
+  uchar4 col = make_uchar4(0, 0, 0, 0);
+  if (sdfv <= 0.0f) {
+    stepLen = sdfv * stepScale;
+    pr = add3(pr, mul3(dir, stepLen));
+    const int ix = (int)floorf(pr.x), iy = (int)floorf(pr.y), iz = (int)floorf(pr.z);
+    const float3 cf = f3(pr.x - (float)ix, pr.y - (float)iy, pr.z - (float)iz);
+    const float3 nc = f3(1.0f - cf.x, 1.0f - cf.y, 1.0f - cf.z);
+    float fb[8];
+    float nearest = 1.0e20f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
+      const int bi = R.find(ix + ox, iy + oy, iz + oz);
+      fb[k] = bi < 0 ? 1.0f : HVox<HF>::load(s.hsdf, (unsigned)bi);
+      const float3 dd = f3(ox ? nc.x : cf.x, oy ? nc.y : cf.y, oz ? nc.z : cf.z);
+      const float cd = sqrtf(dot3(dd, dd));
+      if (s.cmap && s.hrgb && bi >= 0 && (k == 0 || nearest > cd)) {
+        nearest = cd;
+        const uchar4 v = s.hrgb[bi];
+        col = make_uchar4(v.x, v.y, v.z, 255);
+      }
+    }
+    sdfv = fb[0] * nc.x * nc.y * nc.z + fb[1] * cf.x * nc.y * nc.z + fb[2] * nc.x * cf.y * nc.z +
+           fb[3] * cf.x * cf.y * nc.z + fb[4] * nc.x * nc.y * cf.z + fb[5] * cf.x * nc.y * cf.z +
+           fb[6] * nc.x * cf.y * cf.z + fb[7] * cf.x * cf.y * cf.z;
+    stepLen = sdfv * stepScale;
+    pr = add3(pr, mul3(dir, stepLen));
+    vout = w0(mul3(pr, s.voxel));
+    float p1, p2, v1;
+    float3 g;
+    p1 = fb[0] * nc.y * nc.z + fb[2] * cf.y * nc.z + fb[4] * nc.y * cf.z + fb[6] * cf.y * cf.z;
+    p2 = R.sdf_at(ix - 1, iy, iz) * nc.y * nc.z + R.sdf_at(ix - 1, iy + 1, iz) * cf.y * nc.z +
+         R.sdf_at(ix - 1, iy, iz + 1) * nc.y * cf.z + R.sdf_at(ix - 1, iy + 1, iz + 1) * cf.y * cf.z;
+    v1 = p1 * cf.x + p2 * nc.x;
+    p1 = fb[1] * nc.y * nc.z + fb[3] * cf.y * nc.z + fb[5] * nc.y * cf.z + fb[7] * cf.y * cf.z;
+    p2 = R.sdf_at(ix + 2, iy, iz) * nc.y * nc.z + R.sdf_at(ix + 2, iy + 1, iz) * cf.y * nc.z +
+         R.sdf_at(ix + 2, iy, iz + 1) * nc.y * cf.z + R.sdf_at(ix + 2, iy + 1, iz + 1) * cf.y * cf.z;
+    g.x = p1 * nc.x + p2 * cf.x - v1;
+    p1 = fb[0] * nc.x * nc.z + fb[1] * cf.x * nc.z + fb[4] * nc.x * cf.z + fb[5] * cf.x * cf.z;
+    p2 = R.sdf_at(ix, iy - 1, iz) * nc.x * nc.z + R.sdf_at(ix + 1, iy - 1, iz) * cf.x * nc.z +
+         R.sdf_at(ix, iy - 1, iz + 1) * nc.x * cf.z + R.sdf_at(ix + 1, iy - 1, iz + 1) * cf.x * cf.z;
+    v1 = p1 * cf.y + p2 * nc.y;
+    p1 = fb[2] * nc.x * nc.z + fb[3] * cf.x * nc.z + fb[6] * nc.x * cf.z + fb[7] * cf.x * cf.z;
+    p2 = R.sdf_at(ix, iy + 2, iz) * nc.x * nc.z + R.sdf_at(ix + 1, iy + 2, iz) * cf.x * nc.z +
+         R.sdf_at(ix, iy + 2, iz + 1) * nc.x * cf.z + R.sdf_at(ix + 1, iy + 2, iz + 1) * cf.x * cf.z;
+    g.y = p1 * nc.y + p2 * cf.y - v1;
+    p1 = fb[0] * nc.x * nc.y + fb[1] * cf.x * nc.y + fb[2] * nc.x * cf.y + fb[3] * cf.x * cf.y;
+    p2 = R.sdf_at(ix, iy, iz - 1) * nc.x * nc.y + R.sdf_at(ix + 1, iy, iz - 1) * cf.x * nc.y +
+         R.sdf_at(ix, iy + 1, iz - 1) * nc.x * cf.y + R.sdf_at(ix + 1, iy + 1, iz - 1) * cf.x * cf.y;
+    v1 = p1 * cf.z + p2 * nc.z;
+    p1 = fb[4] * nc.x * nc.y + fb[5] * cf.x * nc.y + fb[6] * nc.x * cf.y + fb[7] * cf.x * cf.y;
+    p2 = R.sdf_at(ix, iy, iz + 2) * nc.x * nc.y + R.sdf_at(ix + 1, iy, iz + 2) * cf.x * nc.y +
+         R.sdf_at(ix, iy + 1, iz + 2) * nc.x * cf.y + R.sdf_at(ix + 1, iy + 1, iz + 2) * cf.x * cf.y;
+    g.z = p1 * nc.z + p2 * cf.z - v1;
+    nout = w0(normalize3(g));
+  }
+  s.vref[pid] = vout;
+  s.nref[pid] = nout;
+  if (s.cmap) s.cmap[pid] = col;
+}
+
+template __global__ void k_hash_integrate<0>(const SessionDesc*);
+template __global__ void k_hash_integrate<1>(const SessionDesc*);
+template __global__ void k_hash_raycast<0>(const SessionDesc*);
+template __global__ void k_hash_raycast<1>(const SessionDesc*);
+
+}  // namespace nui
+
+namespace nui {
+// NuiKinfuVoxelBlockHash::reset (NuiKinfuVoxelBlockHash.cpp:78-213): every entry free,
+// identity free lists, every voxel (sdf 0, weight 0, colour 0).
+__global__ void k_hash_reset(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[0];
+  const size_t ne = (size_t)s.nb + s.ne, nv = (size_t)s.np * 512;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (size_t i = t0; i < ne; i += stride) {
+    HEntry e;
+    e.pos[0] = e.pos[1] = e.pos[2] = 0;
+    e.pad = 0;
+    e.ptr = -2;
+    e.offset = 0;
+    store_entry(s.entries, (unsigned)i, e);
+    s.alloc_type[i] = 0;
+    s.vis[i] = 0;
+    s.keys[i] = 0ull;
+  }
+  for (size_t i = t0; i < (size_t)s.np; i += stride) s.alloc_list[i] = (int)i;
+  for (size_t i = t0; i < (size_t)s.ne; i += stride) s.excess_list[i] = (int)i;
+  for (size_t i = t0; i < nv; i += stride) {
+    if (s.hfmt == 0)
+      reinterpret_cast<short*>(s.hsdf)[i] = 0;
+    else
+      reinterpret_cast<__half*>(s.hsdf)[i] = __float2half_rn(0.f);
+    s.hw[i] = 0;
+    if (s.hrgb) s.hrgb[i] = make_uchar4(0, 0, 0, 0);
+  }
+  if (t0 == 0) {
+    s.hcount[0] = s.np - 1;
+    s.hcount[1] = s.ne - 1;
+    s.hcount[2] = 0;
+    s.hcount[3] = 0;
+  }
+}
+
+// Pool voxels in the reference's AoS layout (short sdf, uchar rgb[3], uchar weight).
+__global__ void k_hash_export_voxels(const SessionDesc* __restrict__ descs, uint8_t* out) {
+  const SessionDesc& s = descs[0];
+  const size_t nv = (size_t)s.np * 512;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (size_t)gridDim.x * blockDim.x) {
+    short v;
+    if (s.hfmt == 0)
+      v = reinterpret_cast<const short*>(s.hsdf)[i];
+    else
+      v = (short)__float2int_rz(__half2float(reinterpret_cast<const __half*>(s.hsdf)[i]) * 32767.0f);
+    uint8_t* o = out + 6 * i;
+    o[0] = (uint8_t)(v & 0xff);
+    o[1] = (uint8_t)((unsigned short)v >> 8);
+    const uchar4 c = s.hrgb ? s.hrgb[i] : make_uchar4(0, 0, 0, 0);
+    o[2] = c.x;
+    o[3] = c.y;
+    o[4] = c.z;
+    o[5] = s.hw[i];
+  }
+}
+}  // namespace nui
+
+// ------------------------------------------------------------------ marching cubes
+// meshHashScene_kernel (KinfuHashVisualization.cl:88-271): the cubes of every visible
+// block, emitted in visible-list order, voxels z-y-x inside a block (thread id = x + 8y +
+// 64z), triangles in table order.  No weight test: the reference reads sdf alone.
+namespace nui {
+__constant__ uint64_t c_htri[256];
+void hash_mc_upload_tables(cudaStream_t st, const uint64_t* table) {
+  cudaMemcpyToSymbolAsync(c_htri, table, 256 * sizeof(uint64_t), 0, cudaMemcpyHostToDevice, st);
+}
+
+template <int HF>
+__device__ __forceinline__ int hash_cube(HashRead<HF>& R, int vx, int vy, int vz, float* sv) {
+  const int CX[8] = {0, 1, 1, 0, 0, 1, 1, 0}, CY[8] = {0, 0, 1, 1, 0, 0, 1, 1}, CZ[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+  int cube = 0;
+  for (int k = 0; k < 8; ++k) {
+    const int bi = R.find(vx + CX[k], vy + CY[k], vz + CZ[k]);
+    if (bi < 0) return -1;
+    sv[k] = HVox<HF>::load(R.s.hsdf, (unsigned)bi);
+    if (sv[k] < 0) cube |= 1 << k;
+  }
+  return cube;
+}
+
+template <int HF>
+__global__ void __launch_bounds__(512) k_hash_mesh_count(const SessionDesc* __restrict__ descs, unsigned* cnt) {
+  const SessionDesc& s = descs[0];
+  const int nvis = s.hcount[2];
+  __shared__ unsigned wsum[16];
+  HashRead<HF> R{s, 0, 0, 0, -1};
+  for (int k = blockIdx.x; k < nvis; k += gridDim.x) {
+    const HEntry en = load_entry(s.entries, (unsigned)s.vis_ids[k]);
+    unsigned n = 0;
+    if (en.ptr >= 0) {
+      const int lid = threadIdx.x;
+      float sv[8];
+      const int c = hash_cube<HF>(R, en.pos[0] * 8 + (lid & 7), en.pos[1] * 8 + ((lid >> 3) & 7),
+                                  en.pos[2] * 8 + (lid >> 6), sv);
+      if (c >= 0) n = 3u * (unsigned)(c_htri[c] >> 60);
+    }
+    n = __reduce_add_sync(0xffffffffu, n);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = n;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned t = 0;
+      for (int w = 0; w < 16; ++w) t += wsum[w];
+      cnt[k] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// In-place exclusive scan of n counts (u32 -> u64 offsets), total at off[n].
+__global__ void __launch_bounds__(1024) k_hash_mesh_scan(const unsigned* cnt, unsigned long long* off, int n) {
+  __shared__ unsigned long long wt[32];
+  __shared__ unsigned long long carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int base = 0; base < n; base += 1024) {
+    const int i = base + threadIdx.x;
+    const unsigned long long v = i < n ? cnt[i] : 0ull;
+    unsigned long long inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    if (lane == 31) wt[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+      const unsigned long long w = wt[lane];
+      unsigned long long wi = w;
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long t = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += t;
+      }
+      wt[lane] = wi - w;
+    }
+    __syncthreads();
+    const unsigned long long ex = carry + wt[warp] + inc - v;
+    __syncthreads();
+    if (i < n) off[i] = ex;
+    if (threadIdx.x == 1023) carry = ex + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) off[n] = carry;
+}
+
+__device__ __forceinline__ float3 sdf_interp3(float3 p1, float3 p2, float v1, float v2) {
+  if (fabsf(0.0f - v1) < 0.00001f) return p1;
+  if (fabsf(0.0f - v2) < 0.00001f) return p2;
+  if (fabsf(v1 - v2) < 0.00001f) return p1;
+  return add3(p1, mul3(sub3(p2, p1), (0.0f - v1) / (v2 - v1)));
+}
+
+template <int HF>
+__global__ void __launch_bounds__(512) k_hash_mesh_emit(const SessionDesc* __restrict__ descs,
+                                                        const unsigned long long* off, float* pos, float* col,
+                                                        unsigned long long cap) {
+  const SessionDesc& s = descs[0];
+  const int nvis = s.hcount[2];
+  __shared__ unsigned wsum[16];
+  HashRead<HF> R{s, 0, 0, 0, -1};
+  const int lid = threadIdx.x, lane = lid & 31, warp = lid >> 5;
+  const int CX[8] = {0, 1, 1, 0, 0, 1, 1, 0}, CY[8] = {0, 0, 1, 1, 0, 0, 1, 1}, CZ[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+  const int E0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3}, E1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
+  for (int k = blockIdx.x; k < nvis; k += gridDim.x) {
+    const HEntry en = load_entry(s.entries, (unsigned)s.vis_ids[k]);
+    float sv[8];
+    int c = -1;
+    const int vx = en.pos[0] * 8 + (lid & 7), vy = en.pos[1] * 8 + ((lid >> 3) & 7), vz = en.pos[2] * 8 + (lid >> 6);
+    if (en.ptr >= 0) c = hash_cube<HF>(R, vx, vy, vz, sv);
+    const unsigned n = c >= 0 ? 3u * (unsigned)(c_htri[c] >> 60) : 0u;
+    unsigned inc = n;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    unsigned before = 0;
+    for (int w = 0; w < warp; ++w) before += wsum[w];
+    __syncthreads();
+    unsigned long long out = off[k] + before + inc - n;
+    if (n == 0) continue;
+    const uint64_t word = c_htri[c];
+    float3 pt[8], cl[8];
+    for (int q = 0; q < 8; ++q) {
+      pt[q] = f3((float)(vx + CX[q]), (float)(vy + CY[q]), (float)(vz + CZ[q]));
+      cl[q] = f3(0.f, 0.f, 0.f);
+      if (col && s.hrgb) {
+        const int bi = R.find(vx + CX[q], vy + CY[q], vz + CZ[q]);
+        const uchar4 v = s.hrgb[bi];
+        cl[q] = f3((float)v.x / 255.f, (float)v.y / 255.f, (float)v.z / 255.f);
+      }
+    }
+    for (unsigned j = 0; j < n && out < cap; ++j, ++out) {
+      const int e = (int)((word >> (4 * j)) & 0xF);
+      const int a = E0[e], b = E1[e];
+      if (pos) {
+        const float3 p = mul3(sdf_interp3(pt[a], pt[b], sv[a], sv[b]), s.voxel);
+        pos[3 * out] = p.x;
+        pos[3 * out + 1] = p.y;
+        pos[3 * out + 2] = p.z;
+      }
+      if (col) {
+        const float3 cc = sdf_interp3(cl[a], cl[b], sv[a], sv[b]);
+        reinterpret_cast<float4*>(col)[out] = make_float4(cc.x, cc.y, cc.z, 1.0f);
+      }
+    }
+  }
+}
+
+template __global__ void k_hash_mesh_count<0>(const SessionDesc*, unsigned*);
+template __global__ void k_hash_mesh_count<1>(const SessionDesc*, unsigned*);
+template __global__ void k_hash_mesh_emit<0>(const SessionDesc*, const unsigned long long*, float*, float*,
+                                             unsigned long long);
+template __global__ void k_hash_mesh_emit<1>(const SessionDesc*, const unsigned long long*, float*, float*,
+                                             unsigned long long);
+}  // namespace nui

@@ -39,6 +39,22 @@ __global__ void k_raycast(const SessionDesc*);
 __global__ void k_publish(const SessionDesc*, int, float*, int*);
 __global__ void k_tick_begin(const SessionDesc*, int);
 __global__ void k_occ_clear(const SessionDesc*);
+__global__ void k_hash_prepare(const SessionDesc*);
+__global__ void k_hash_walk(const SessionDesc*, int);
+__global__ void k_hash_count(const SessionDesc*, int);
+__global__ void k_hash_scan(const SessionDesc*, int);
+__global__ void k_hash_alloc(const SessionDesc*);
+__global__ void k_hash_alloc_done(const SessionDesc*, int);
+__global__ void k_hash_visible(const SessionDesc*);
+__global__ void k_hash_compact(const SessionDesc*);
+template <int F>
+__global__ void k_hash_integrate(const SessionDesc*);
+__global__ void k_hash_range(const SessionDesc*);
+__global__ void k_hash_project(const SessionDesc*);
+template <int F>
+__global__ void k_hash_raycast(const SessionDesc*);
+__global__ void k_hash_reset(const SessionDesc*);
+__global__ void k_hash_export_voxels(const SessionDesc*, uint8_t*);
 template <int F>
 __global__ void k_export_ref(const SessionDesc*, short2*, uchar4*);
 template <int F>
@@ -71,6 +87,8 @@ struct BatchPlan {
   int maxIters[kMaxLevels] = {0, 0, 0, 0};
   long maxIntegThreads[4] = {0, 0, 0, 0};  // per format: columns * zchunks
   long maxBricks[4] = {0, 0, 0, 0};        // per format: 8^3 bricks
+  int hashMask = 0;                        // bit per hash sdf format
+  long maxHashBlk = 0;                     // scan blocks of 1024 entries
   int fmtMask = 0;
   bool operator<(const BatchPlan& o) const { return std::memcmp(this, &o, sizeof(BatchPlan)) < 0; }
 };
@@ -117,7 +135,19 @@ struct nui_session {
   float* tile_max = nullptr;
   TrackState* ts = nullptr;
   float2* partials = nullptr;
-  SessionDesc* d_desc1 = nullptr;  // one-entry table for the per-session path
+  SessionDesc* d_desc1 = nullptr;
+  // voxel-block hash
+  bool hash = false;
+  HEntry* entries = nullptr;
+  void* hsdf = nullptr;
+  uint8_t* hw = nullptr;
+  uchar4* hrgb = nullptr;
+  int *alloc_list = nullptr, *excess_list = nullptr, *hcount = nullptr, *vis_ids = nullptr;
+  uint8_t *alloc_type = nullptr, *vis = nullptr;
+  short4* coords = nullptr;
+  unsigned long long* keys = nullptr;
+  unsigned* blk = nullptr;
+  float2* range = nullptr;  // one-entry table for the per-session path
   long frames = 0;
   bool color_frame = false;
   std::vector<void*> allocs;
@@ -138,9 +168,17 @@ bool cfg_valid(const nui_session_cfg* c, std::string& why) {
     if (((c->width >> l) << l) != c->width || ((c->height >> l) << l) != c->height)
       return why = "image size must be divisible by 2^(levels-1)", false;
   }
-  if (c->volume_kind != NUI_VOLUME_DENSE) return why = "only dense volumes in this build", false;
+  if (c->volume_kind != NUI_VOLUME_DENSE && c->volume_kind != NUI_VOLUME_HASH) return why = "bad volume kind", false;
   if (c->tsdf_format < 0 || c->tsdf_format > 3) return why = "bad tsdf format", false;
-  for (int i = 0; i < 3; ++i) {
+  if (c->volume_kind == NUI_VOLUME_HASH) {
+    if (c->hash_buckets < 16 || (c->hash_buckets & (c->hash_buckets - 1))) return why = "hash buckets must be a power of two >= 16", false;
+    if (c->hash_excess < 1 || c->hash_pool_blocks < 1 || (long)c->hash_buckets + c->hash_excess > (1L << 28))
+      return why = "bad hash table sizes", false;
+    if ((long)c->hash_pool_blocks > (1L << 22)) return why = "hash pool larger than 2^22 blocks", false;
+    if (!(c->voxel_size > 0.f) || !(c->trunc_scale > 0.f)) return why = "voxel size / truncation must be positive", false;
+    if (c->hash_max_weight < 1 || c->hash_max_weight > 255) return why = "hash max weight must be 1..255", false;
+  }
+  for (int i = 0; i < 3 && c->volume_kind == NUI_VOLUME_DENSE; ++i) {
     if (c->res[i] < 8 || c->res[i] > 1024) return why = "volume resolution must be 8..1024", false;
     if (!(c->dim[i] > 0.f)) return why = "volume size must be positive", false;
   }
@@ -207,6 +245,32 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
   d.zchunks = s->zchunks;
   d.ts = s->ts;
   d.partials = s->partials;
+  if (s->hash) {
+    d.fmt = -1;  // dense kernels skip hash sessions
+    d.hash = 1;
+    d.hfmt = c.tsdf_format == NUI_TSDF_I16 ? 0 : 1;
+    d.entries = s->entries;
+    d.nb = c.hash_buckets;
+    d.ne = c.hash_excess;
+    d.np = c.hash_pool_blocks;
+    d.hmask = (unsigned)(c.hash_buckets - 1);
+    d.voxel = c.voxel_size;
+    d.mu = c.trunc_scale;
+    d.max_w = c.hash_max_weight;
+    d.hsdf = s->hsdf;
+    d.hw = s->hw;
+    d.hrgb = s->hrgb;
+    d.alloc_list = s->alloc_list;
+    d.excess_list = s->excess_list;
+    d.hcount = s->hcount;
+    d.alloc_type = s->alloc_type;
+    d.vis = s->vis;
+    d.coords = s->coords;
+    d.keys = s->keys;
+    d.vis_ids = s->vis_ids;
+    d.blk = s->blk;
+    d.range = s->range;
+  }
 }
 
 void plan_add(BatchPlan& p, const nui_session* s) {
@@ -215,6 +279,11 @@ void plan_add(BatchPlan& p, const nui_session* s) {
   p.maxH = std::max(p.maxH, c.height);
   p.maxLevels = std::max(p.maxLevels, c.levels);
   for (int l = 0; l < c.levels; ++l) p.maxIters[l] = std::max(p.maxIters[l], c.iterations[l]);
+  if (s->hash) {
+    p.hashMask |= 1 << (c.tsdf_format == NUI_TSDF_I16 ? 0 : 1);
+    p.maxHashBlk = std::max(p.maxHashBlk, ((long)c.hash_buckets + c.hash_excess + 1023) / 1024);
+    return;
+  }
   long th = (long)c.res[0] * c.res[1] * s->zchunks;
   p.maxIntegThreads[c.tsdf_format] = std::max(p.maxIntegThreads[c.tsdf_format], th);
   p.fmtMask |= 1 << c.tsdf_format;
@@ -248,6 +317,33 @@ void launch_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   k_raycast<F><<<dim3(cdiv((long)p.maxW * p.maxH, 128), p.n), 128, 0, st>>>(d);
 }
 
+void launch_hash_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
+  if (!p.hashMask) return;
+  const unsigned nb = (unsigned)p.maxHashBlk;
+  k_hash_prepare<<<dim3(592, p.n), 256, 0, st>>>(d);
+  const unsigned pix = cdiv((long)p.maxW * p.maxH, 256);
+  k_hash_walk<<<dim3(pix, p.n), 256, 0, st>>>(d, 0);
+  k_hash_walk<<<dim3(pix, p.n), 256, 0, st>>>(d, 1);
+  k_hash_count<<<dim3(nb, p.n), 256, 0, st>>>(d, 0);
+  k_hash_scan<<<p.n, 1024, 0, st>>>(d, 0);
+  k_hash_alloc<<<dim3(nb, p.n), 1024, 0, st>>>(d);
+  k_hash_alloc_done<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n);
+  k_hash_visible<<<dim3(592, p.n), 256, 0, st>>>(d);
+  k_hash_count<<<dim3(nb, p.n), 256, 0, st>>>(d, 1);
+  k_hash_scan<<<p.n, 1024, 0, st>>>(d, 1);
+  k_hash_compact<<<dim3(nb, p.n), 1024, 0, st>>>(d);
+  if (p.hashMask & 1) k_hash_integrate<0><<<dim3(1184, p.n), 512, 0, st>>>(d);
+  if (p.hashMask & 2) k_hash_integrate<1><<<dim3(1184, p.n), 512, 0, st>>>(d);
+}
+void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
+  if (!p.hashMask) return;
+  k_hash_range<<<dim3(296, p.n), 256, 0, st>>>(d);
+  k_hash_project<<<dim3(296, p.n), 128, 0, st>>>(d);
+  const unsigned pix = cdiv((long)p.maxW * p.maxH, 128);
+  if (p.hashMask & 1) k_hash_raycast<0><<<dim3(pix, p.n), 128, 0, st>>>(d);
+  if (p.hashMask & 2) k_hash_raycast<1><<<dim3(pix, p.n), 128, 0, st>>>(d);
+}
+
 // The launch schedule of one tick.  ev: optional stage events (timing only).
 void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float* d_pose, int* d_status, bool ev) {
   cudaStream_t st = ctx->stream;
@@ -278,11 +374,13 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
   launch_summary<1>(p, d, st, 0);
   launch_summary<2>(p, d, st, 0);
   launch_summary<3>(p, d, st, 0);
+  launch_hash_integrate(p, d, st);
   mark(4);
   launch_raycast<0>(p, d, st);
   launch_raycast<1>(p, d, st);
   launch_raycast<2>(p, d, st);
   launch_raycast<3>(p, d, st);
+  launch_hash_raycast(p, d, st);
   mark(5);
 }
 
@@ -393,11 +491,15 @@ nui_status reset_session(nui_session* s) {
   SessionDesc d;
   fill_desc(s, d, kInactive, nullptr, nullptr);
   NUI_CUDA(cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, s->ctx->stream));
-  switch (s->cfg.tsdf_format) {
-    case 0: launch_init<0>(s); break;
-    case 1: launch_init<1>(s); break;
-    case 2: launch_init<2>(s); break;
-    case 3: launch_init<3>(s); break;
+  if (s->hash) {
+    k_hash_reset<<<1184, 256, 0, s->ctx->stream>>>(s->d_desc1);
+  } else {
+    switch (s->cfg.tsdf_format) {
+      case 0: launch_init<0>(s); break;
+      case 1: launch_init<1>(s); break;
+      case 2: launch_init<2>(s); break;
+      case 3: launch_init<3>(s); break;
+    }
   }
   TrackState t;
   std::memset(&t, 0, sizeof(t));
@@ -444,6 +546,12 @@ NUI_API void nui_session_cfg_default(nui_session_cfg* c) {
   c->depth_threshold = 0.3f;
   c->dist_threshold = 0.1f;
   c->integration_threshold = 0.15f;
+  c->voxel_size = 0.005f;
+  c->trunc_scale = 0.02f;
+  c->hash_buckets = 1 << 20;
+  c->hash_excess = 0x30000;
+  c->hash_pool_blocks = 1 << 20;
+  c->hash_max_weight = 255;
 }
 
 NUI_API nui_status nui_ctx_create(int device, nui_ctx** out) {
@@ -522,11 +630,19 @@ NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
   const size_t N = (size_t)c->width * c->height;
   size_t b = N * 2 + N * 4 /*bgra*/ + N * 4 /*scaled*/ + N * 16 * 2 /*ref maps*/ + N * 4 /*cmap*/;
   for (int l = 0; l < c->levels; ++l) b += (N >> (2 * l)) * (4 + 16);
+  b += sizeof(TrackState) + sizeof(SessionDesc) + ((N + 1023) / 1024) * kIcpTerms * sizeof(float2);
+  b += (N / (kTile * kTile) + 64) * 4;
+  if (c->volume_kind == NUI_VOLUME_HASH) {
+    const size_t ne = (size_t)c->hash_buckets + c->hash_excess, nv = (size_t)c->hash_pool_blocks * 512;
+    b += ne * (16 + 1 + 1 + 8 + 8 + 4) + ((ne + 1023) / 1024) * 16 + (size_t)c->hash_pool_blocks * 4 +
+         (size_t)c->hash_excess * 4 + N * 8;
+    b += nv * ((c->tsdf_format == NUI_TSDF_I16 ? 2 : 2) + 1 + (c->color_volume ? 4 : 0));
+    return b;
+  }
   const size_t nv = (size_t)c->res[0] * c->res[1] * c->res[2];
   b += nv * voxel_bytes(c->tsdf_format);
   if (c->color_volume) b += nv * 4;
-  b += sizeof(TrackState) + sizeof(SessionDesc) + ((N + 1023) / 1024) * kIcpTerms * sizeof(float2);
-  b += (size_t)((c->res[0] + 7) / 8) * ((c->res[1] + 7) / 8) * ((c->res[2] + 7) / 8) + (N / (kTile * kTile) + 64) * 4;
+  b += (size_t)((c->res[0] + 7) / 8) * ((c->res[1] + 7) / 8) * ((c->res[2] + 7) / 8);
   return b;
 }
 
@@ -559,17 +675,31 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
     s->allocs.push_back(*p);
     return true;
   };
+  s->hash = c.volume_kind == NUI_VOLUME_HASH;
   bool ok = alloc((void**)&s->raw, N * 2) && alloc((void**)&s->dscaled, N * 4) && alloc((void**)&s->vref, N * 16) &&
             alloc((void**)&s->nref, N * 16) && alloc((void**)&s->ts, sizeof(TrackState)) &&
             alloc((void**)&s->partials, ((N + 1023) / 1024) * kIcpTerms * sizeof(float2)) &&
-            alloc((void**)&s->d_desc1, sizeof(SessionDesc)) && alloc((void**)&s->vol, nv * (c.tsdf_format == 2 ? 2 : voxel_bytes(c.tsdf_format)));
+            alloc((void**)&s->d_desc1, sizeof(SessionDesc));
   for (int l = 0; ok && l < c.levels; ++l)
     ok = alloc((void**)&s->dlev[l], (N >> (2 * l)) * 4) && alloc((void**)&s->vlev[l], (N >> (2 * l)) * 16);
-  if (ok && c.tsdf_format == NUI_TSDF_F16_U8) ok = alloc((void**)&s->wvol, nv);
-  const size_t nbricks = (size_t)((c.res[0] + 7) / 8) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8);
   const size_t ntiles = (size_t)((c.width + kTile - 1) / kTile) * ((c.height + kTile - 1) / kTile);
-  if (ok) ok = alloc((void**)&s->occ, nbricks) && alloc((void**)&s->tile_max, ntiles * sizeof(float));
-  if (ok && c.color_volume) ok = alloc((void**)&s->cvol, nv * 4) && alloc((void**)&s->bgra, N * 4) && alloc((void**)&s->cmap, N * 4);
+  if (ok) ok = alloc((void**)&s->tile_max, ntiles * sizeof(float));
+  if (s->hash) {
+    const size_t ne = (size_t)c.hash_buckets + c.hash_excess, hv = (size_t)c.hash_pool_blocks * 512;
+    ok = ok && alloc((void**)&s->entries, ne * sizeof(HEntry)) && alloc((void**)&s->hsdf, hv * 2) &&
+         alloc((void**)&s->hw, hv) && alloc((void**)&s->alloc_list, (size_t)c.hash_pool_blocks * 4) &&
+         alloc((void**)&s->excess_list, (size_t)c.hash_excess * 4) && alloc((void**)&s->hcount, 16) &&
+         alloc((void**)&s->alloc_type, ne) && alloc((void**)&s->vis, ne) && alloc((void**)&s->coords, ne * 8) &&
+         alloc((void**)&s->keys, ne * 8) && alloc((void**)&s->vis_ids, ne * 4) &&
+         alloc((void**)&s->blk, ((ne + 1023) / 1024) * 16) && alloc((void**)&s->range, N * 8);
+    if (ok && c.color_volume) ok = alloc((void**)&s->hrgb, hv * 4) && alloc((void**)&s->bgra, N * 4) && alloc((void**)&s->cmap, N * 4);
+  } else {
+    ok = ok && alloc((void**)&s->vol, nv * (c.tsdf_format == 2 ? 2 : voxel_bytes(c.tsdf_format)));
+    if (ok && c.tsdf_format == NUI_TSDF_F16_U8) ok = alloc((void**)&s->wvol, nv);
+    const size_t nbricks = (size_t)((c.res[0] + 7) / 8) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8);
+    if (ok) ok = alloc((void**)&s->occ, nbricks);
+    if (ok && c.color_volume) ok = alloc((void**)&s->cvol, nv * 4) && alloc((void**)&s->bgra, N * 4) && alloc((void**)&s->cmap, N * 4);
+  }
   if (!ok) {
     for (void* p : s->allocs) cudaFree(p);
     delete s;
@@ -721,11 +851,13 @@ nui_status run_stage(nui_session* s, int what) {
     launch_summary<1>(p, dd, st, 0);
     launch_summary<2>(p, dd, st, 0);
     launch_summary<3>(p, dd, st, 0);
+    launch_hash_integrate(p, dd, st);
   } else if (what == 3) {
     launch_raycast<0>(p, dd, st);
     launch_raycast<1>(p, dd, st);
     launch_raycast<2>(p, dd, st);
     launch_raycast<3>(p, dd, st);
+    launch_hash_raycast(p, dd, st);
   } else if (what == 4) {
     k_feedback<<<dim3(cdiv((long)p.maxW * p.maxH, 256), 1), 256, 0, st>>>(dd);
   }
@@ -798,6 +930,8 @@ NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void*
   const size_t N = (size_t)c.width * c.height;
   const size_t nv = (size_t)c.res[0] * c.res[1] * c.res[2];
   if (level < 0 || level >= c.levels) return fail(NUI_ERR_INVALID_ARG, "bad level");
+  if ((what == 5 || what == 6 || what == 9) && s->hash) return fail(NUI_ERR_INVALID_ARG, "not a dense session");
+  if (what >= 20 && !s->hash) return fail(NUI_ERR_INVALID_ARG, "not a hash session");
   const size_t Nl = N >> (2 * level);
   const void* src = nullptr;
   size_t need = 0;
@@ -810,6 +944,31 @@ NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void*
     case 6: src = s->vol; need = nv * (c.tsdf_format == 2 ? 2 : voxel_bytes(c.tsdf_format)); break;
     case 7: src = s->dlev[level]; need = Nl * 4; break;
     case 8: src = s->cmap; need = N * 4; break;
+    case 20: src = s->entries; need = ((size_t)c.hash_buckets + c.hash_excess) * 16; break;
+    case 21: {
+      int cnt[4];
+      NUI_CUDA(cudaMemcpy(cnt, s->hcount, 16, cudaMemcpyDeviceToHost));
+      src = s->vis_ids;
+      need = (size_t)cnt[2] * 4;
+      break;
+    }
+    case 23: src = s->range; need = N * 8; break;
+    case 22: {
+      if (!s->hash) return fail(NUI_ERR_INVALID_ARG, "not a hash session");
+      need = (size_t)c.hash_pool_blocks * 512 * 6;
+      if (bytes < need) return fail(NUI_ERR_INVALID_ARG, "buffer too small");
+      void* tmp = nullptr;
+      NUI_CUDA(cudaMalloc(&tmp, need));
+      SessionDesc d;
+      fill_desc(s, d, kInactive, nullptr, nullptr);
+      cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, s->ctx->stream);
+      k_hash_export_voxels<<<1184, 256, 0, s->ctx->stream>>>(s->d_desc1, (uint8_t*)tmp);
+      cudaError_t e = cudaMemcpyAsync(host, tmp, need, cudaMemcpyDeviceToHost, s->ctx->stream);
+      cudaStreamSynchronize(s->ctx->stream);
+      cudaFree(tmp);
+      if (e != cudaSuccess) return fail(NUI_ERR_DEVICE, cudaGetErrorString(e));
+      return NUI_OK;
+    }
     case 5:
     case 9: {
       need = nv * 4;
@@ -843,7 +1002,20 @@ NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void*
   return NUI_OK;
 }
 
+NUI_API nui_status nui_hash_stats(nui_session* s, int* visible, int* last_block, int* last_excess, int* failed) {
+  if (!s || !s->hash) return fail(NUI_ERR_INVALID_ARG, "not a hash session");
+  int cnt[4];
+  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  NUI_CUDA(cudaMemcpy(cnt, s->hcount, 16, cudaMemcpyDeviceToHost));
+  if (visible) *visible = cnt[2];
+  if (last_block) *last_block = cnt[0];
+  if (last_excess) *last_excess = cnt[1];
+  if (failed) *failed = cnt[3];
+  return NUI_OK;
+}
+
 NUI_API nui_status nui_debug_upload_volume(nui_session* s, const int16_t* ref) {
+  if (s && s->hash) return fail(NUI_ERR_UNSUPPORTED, "dense volumes only");
   if (!s || !ref) return fail(NUI_ERR_INVALID_ARG, "null argument");
   const size_t nv = (size_t)s->cfg.res[0] * s->cfg.res[1] * s->cfg.res[2];
   void* tmp = nullptr;
@@ -958,6 +1130,67 @@ NUI_API nui_status nui_k_feedback_maps(nui_ctx* ctx, const float* d_vertex4, int
 }  // extern "C"
 
 // ------------------------------------------------------------------ marching cubes
+namespace {
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+}  // namespace
+namespace nui {
+void hash_mc_upload_tables(cudaStream_t st, const uint64_t* table);
+template <int F>
+__global__ void k_hash_mesh_count(const SessionDesc*, unsigned*);
+__global__ void k_hash_mesh_scan(const unsigned*, unsigned long long*, int);
+template <int F>
+__global__ void k_hash_mesh_emit(const SessionDesc*, const unsigned long long*, float*, float*, unsigned long long);
+}  // namespace nui
+#include "nui_mc_tables.h"
+namespace {
+// Volume2CLMesh of the hash scene: the visible blocks of the last integration.
+nui_status nui_hash_mesh_impl(nui_session* s, float* pos, float* col, uint64_t cap, uint64_t* nverts) {
+  cudaStream_t st = s->ctx->stream;
+  int cnt4[4];
+  NUI_CUDA(cudaStreamSynchronize(st));
+  NUI_CUDA(cudaMemcpy(cnt4, s->hcount, 16, cudaMemcpyDeviceToHost));
+  const int nvis = cnt4[2];
+  *nverts = 0;
+  if (nvis == 0) return NUI_OK;
+  SessionDesc d;
+  fill_desc(s, d, kInactive, nullptr, nullptr);
+  NUI_CUDA(cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, st));
+  hash_mc_upload_tables(st, NUI_MC_TRI_PACKED);
+  DevBuf cnt, off, dp, dc;
+  NUI_CUDA(cudaMalloc(&cnt.p, (size_t)nvis * 4));
+  NUI_CUDA(cudaMalloc(&off.p, ((size_t)nvis + 1) * 8));
+  const int hf = d.hfmt;
+  if (hf == 0)
+    k_hash_mesh_count<0><<<1184, 512, 0, st>>>(s->d_desc1, (unsigned*)cnt.p);
+  else
+    k_hash_mesh_count<1><<<1184, 512, 0, st>>>(s->d_desc1, (unsigned*)cnt.p);
+  k_hash_mesh_scan<<<1, 1024, 0, st>>>((const unsigned*)cnt.p, (unsigned long long*)off.p, nvis);
+  unsigned long long total = 0;
+  NUI_CUDA(cudaMemcpyAsync(&total, (unsigned long long*)off.p + nvis, 8, cudaMemcpyDeviceToHost, st));
+  NUI_CUDA(cudaStreamSynchronize(st));
+  *nverts = total;
+  const unsigned long long k = total < cap ? total : cap;
+  if (k > 0 && (pos || col)) {
+    if (pos) NUI_CUDA(cudaMalloc(&dp.p, k * 12));
+    if (col) NUI_CUDA(cudaMalloc(&dc.p, k * 16));
+    if (hf == 0)
+      k_hash_mesh_emit<0><<<1184, 512, 0, st>>>(s->d_desc1, (const unsigned long long*)off.p, (float*)dp.p, (float*)dc.p, k);
+    else
+      k_hash_mesh_emit<1><<<1184, 512, 0, st>>>(s->d_desc1, (const unsigned long long*)off.p, (float*)dp.p, (float*)dc.p, k);
+    NUI_CUDA(cudaGetLastError());
+    if (pos) NUI_CUDA(cudaMemcpyAsync(pos, dp.p, k * 12, cudaMemcpyDeviceToHost, st));
+    if (col) NUI_CUDA(cudaMemcpyAsync(col, dc.p, k * 16, cudaMemcpyDeviceToHost, st));
+    NUI_CUDA(cudaStreamSynchronize(st));
+  }
+  if (total > cap) return fail(NUI_ERR_MESH_OVERFLOW, "mesh larger than the output capacity");
+  return NUI_OK;
+}
+}  // namespace
 namespace nui {
 void mc_upload_tables(cudaStream_t st);
 template <int F>
@@ -969,12 +1202,6 @@ __global__ void k_mc_emit(const SessionDesc*, const unsigned int*, const unsigne
 }  // namespace nui
 
 namespace {
-struct DevBuf {
-  void* p = nullptr;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
-};
 template <int F>
 void mc_count(nui_session* s, unsigned nb, unsigned* cc, unsigned long long* bt, uint8_t* cases) {
   k_mc_count<F><<<nb, 128, 0, s->ctx->stream>>>(s->d_desc1, cc, bt, cases);
@@ -1013,6 +1240,7 @@ nui_status mc_prepare(nui_session* s, DevBuf& cc, DevBuf& bt, unsigned& nb, uint
 
 extern "C" NUI_API nui_status nui_mesh(nui_session* s, float* pos, float* col, uint64_t cap, uint64_t* nverts) {
   if (!s || !nverts) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  if (s->hash) return nui_hash_mesh_impl(s, pos, col, cap, nverts);
   DevBuf cc, bt, dp, dc;
   unsigned nb = 0;
   unsigned long long total = 0;
@@ -1040,6 +1268,7 @@ extern "C" NUI_API nui_status nui_mesh(nui_session* s, float* pos, float* col, u
 
 extern "C" NUI_API nui_status nui_mesh_cases(nui_session* s, uint8_t* cases, size_t bytes, uint64_t* nverts) {
   if (!s || !cases) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  if (s->hash) return fail(NUI_ERR_UNSUPPORTED, "case indices of dense volumes only");
   const nui_session_cfg& c = s->cfg;
   const size_t need = (size_t)(c.res[0] - 1) * (c.res[1] - 1) * (c.res[2] - 1);
   if (bytes < need) return fail(NUI_ERR_INVALID_ARG, "buffer too small");

@@ -841,7 +841,17 @@ struct OrcEngineCfg {
   int filter_radius;
   float sigma_space2_inv_half, sigma_depth2_inv_half, depth_threshold, dist_threshold;
   float integration_threshold;
+  int hash;  // 1: voxel-block hash scene (NuiKinfuOpenCLHashScene) instead of the dense volume
+  float voxel, mu;
+  int buckets, excess, pool, max_w;
 };
+
+struct OrcHash;
+OrcHash* orc_hash_create_internal(int buckets, int excess, int pool, float voxel, float mu, int max_w);
+void orc_hash_destroy_internal(OrcHash* h);
+void orc_hash_scene_integrate(OrcHash* h, const float* depth, const uint8_t* bgra, const OrcCam* cam,
+                              const OrcXform* m, long* touched);
+void orc_hash_scene_raycast(OrcHash* h, const OrcCam* cam, const OrcXform* m, float* vmap, float* nmap);
 
 struct OrcEngine {
   OrcEngineCfg c;
@@ -856,6 +866,7 @@ struct OrcEngine {
   std::vector<std::vector<float>> dl, vl;  // per-level depth / vertices
   OrcIcpStats last{};
   long touched = 0;
+  OrcHash* hs = nullptr;
 };
 
 ORC_API OrcEngine* orc_engine_create(const OrcEngineCfg* cfg) {
@@ -869,10 +880,14 @@ ORC_API OrcEngine* orc_engine_create(const OrcEngineCfg* cfg) {
     e->tp.cell[i] = c.dim[i] / (float)c.res[i];
   }
   e->tp.trunc = std::max(c.trunc_cfg, 2.1f * std::max(e->tp.cell[0], std::max(e->tp.cell[1], e->tp.cell[2])));
-  long nvox = (long)c.res[0] * c.res[1] * c.res[2];
-  e->vol.resize(2 * nvox);
-  if (c.color) e->cvol.resize(4 * nvox);
-  orc_tsdf_init(e->vol.data(), c.color ? e->cvol.data() : nullptr, nvox);
+  if (c.hash) {
+    e->hs = orc_hash_create_internal(c.buckets, c.excess, c.pool, c.voxel, c.mu, c.max_w);
+  } else {
+    long nvox = (long)c.res[0] * c.res[1] * c.res[2];
+    e->vol.resize(2 * nvox);
+    if (c.color) e->cvol.resize(4 * nvox);
+    orc_tsdf_init(e->vol.data(), c.color ? e->cvol.data() : nullptr, nvox);
+  }
   e->gauss.resize(2 * c.filter_radius + 1);
   orc_gaussian_table(c.filter_radius, c.sigma_space2_inv_half, e->gauss.data());
   long N = (long)c.W * c.H;
@@ -895,7 +910,10 @@ ORC_API OrcEngine* orc_engine_create(const OrcEngineCfg* cfg) {
   return e;
 }
 
-ORC_API void orc_engine_destroy(OrcEngine* e) { delete e; }
+ORC_API void orc_engine_destroy(OrcEngine* e) {
+  if (e->hs) orc_hash_destroy_internal(e->hs);
+  delete e;
+}
 
 static double rel_angle(const float* Ra, const float* Rb) {
   // angle of Ra^-1 Rb (rodrigues2 norm, NuiMatrixUtilities.cpp:7-52)
@@ -916,12 +934,20 @@ ORC_API int orc_engine_frame(OrcEngine* e, const uint16_t* raw, const uint8_t* b
                 c.depth_threshold, e->dl[0].data());
   orc_depth2vertex(e->dl[0].data(), W, H, &e->cam, 1, e->vl[0].data());
   const uint8_t* col = c.color ? bgra : nullptr;
+  // NuiKinfuScene::integrateVolume / raycastRender of the configured scene
+  auto integrate = [&]() {
+    if (e->hs) {
+      orc_hash_scene_integrate(e->hs, e->depth.data(), col, &e->cam, &e->xf, &e->touched);
+    } else {
+      orc_scale_depths(e->depth.data(), W, H, &e->cam);
+      orc_tsdf_integrate(e->depth.data(), col, &e->cam, &e->xf, &e->tp, e->vol.data(),
+                         c.color ? e->cvol.data() : nullptr, c.max_color_weight, &e->touched);
+    }
+  };
   if (e->frames == 0) {
     orc_normals(e->vl[0].data(), W, H, c.depth_threshold, e->normals.data());
     orc_transform_maps(e->vl[0].data(), e->normals.data(), W, H, &e->xf, e->vref.data(), e->nref.data());
-    orc_scale_depths(e->depth.data(), W, H, &e->cam);
-    orc_tsdf_integrate(e->depth.data(), col, &e->cam, &e->xf, &e->tp, e->vol.data(),
-                       c.color ? e->cvol.data() : nullptr, c.max_color_weight, &e->touched);
+    integrate();
   } else {
     for (int l = 1; l < c.levels; ++l) {
       orc_half_sample(e->dl[l - 1].data(), W >> l, H >> l, 1, c.depth_threshold, e->dl[l].data());
@@ -943,14 +969,15 @@ ORC_API int orc_engine_frame(OrcEngine* e, const uint16_t* raw, const uint8_t* b
                           (double)(e->xf.t[1] - e->lastT[1]) * (e->xf.t[1] - e->lastT[1]) +
                           (double)(e->xf.t[2] - e->lastT[2]) * (e->xf.t[2] - e->lastT[2]));
     if ((float)((rn + tn) / 2) >= c.integration_threshold) {
-      orc_scale_depths(e->depth.data(), W, H, &e->cam);
-      orc_tsdf_integrate(e->depth.data(), col, &e->cam, &e->xf, &e->tp, e->vol.data(),
-                         c.color ? e->cvol.data() : nullptr, c.max_color_weight, &e->touched);
+      integrate();
       std::memcpy(e->lastR, e->xf.R, sizeof(e->lastR));
       std::memcpy(e->lastT, e->xf.t, sizeof(e->lastT));
     }
-    orc_raycast(e->vol.data(), c.color ? e->cvol.data() : nullptr, &e->tp, &e->cam, &e->xf, W, H,
-                e->vref.data(), e->nref.data(), nullptr, nullptr);
+    if (e->hs)
+      orc_hash_scene_raycast(e->hs, &e->cam, &e->xf, e->vref.data(), e->nref.data());
+    else
+      orc_raycast(e->vol.data(), c.color ? e->cvol.data() : nullptr, &e->tp, &e->cam, &e->xf, W, H,
+                  e->vref.data(), e->nref.data(), nullptr, nullptr);
   }
   e->frames += 1;
   return 0;
@@ -961,6 +988,7 @@ ORC_API void orc_engine_pose(const OrcEngine* e, float* R, float* t) {
   std::memcpy(t, e->xf.t, 3 * sizeof(float));
 }
 ORC_API const int16_t* orc_engine_volume(const OrcEngine* e) { return e->vol.data(); }
+ORC_API OrcHash* orc_engine_hash(const OrcEngine* e) { return e->hs; }
 ORC_API const uint8_t* orc_engine_color_volume(const OrcEngine* e) {
   return e->cvol.empty() ? nullptr : e->cvol.data();
 }
@@ -1492,4 +1520,20 @@ ORC_API void orc_hash_counters(const OrcHash* h, int* last_block, int* last_exce
   *last_block = h->last_block;
   *last_excess = h->last_excess;
   *failed = h->failed_allocs;
+}
+
+// Engine glue for the hash scene (NuiKinfuOpenCLHashScene::integrateVolume, :533-583, and
+// raycastRender with forward rendering off, :1014-1064).
+OrcHash* orc_hash_create_internal(int buckets, int excess, int pool, float voxel, float mu, int max_w) {
+  OrcHashCfg c{buckets, excess, pool, (uint32_t)(buckets - 1), voxel, mu, max_w};
+  return orc_hash_create(&c);
+}
+void orc_hash_destroy_internal(OrcHash* h) { orc_hash_destroy(h); }
+void orc_hash_scene_integrate(OrcHash* h, const float* depth, const uint8_t* bgra, const OrcCam* cam,
+                              const OrcXform* m, long* touched) {
+  orc_hash_allocate(h, depth, cam, m);
+  orc_hash_integrate(h, depth, bgra, cam, m, touched);
+}
+void orc_hash_scene_raycast(OrcHash* h, const OrcCam* cam, const OrcXform* m, float* vmap, float* nmap) {
+  orc_hash_raycast(h, cam, m, vmap, nmap, nullptr, nullptr);
 }

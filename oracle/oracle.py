@@ -83,7 +83,9 @@ class OrcEngineCfg(C.Structure):
                 ("dim", C.c_float * 3), ("trunc_cfg", C.c_float), ("color", C.c_int), ("max_color_weight", C.c_int),
                 ("levels", C.c_int), ("iters", C.c_int * 4), ("filter_radius", C.c_int),
                 ("sigma_space2_inv_half", C.c_float), ("sigma_depth2_inv_half", C.c_float),
-                ("depth_threshold", C.c_float), ("dist_threshold", C.c_float), ("integration_threshold", C.c_float)]
+                ("depth_threshold", C.c_float), ("dist_threshold", C.c_float), ("integration_threshold", C.c_float),
+                ("hash", C.c_int), ("voxel", C.c_float), ("mu", C.c_float), ("buckets", C.c_int), ("excess", C.c_int),
+                ("pool", C.c_int), ("max_w", C.c_int)]
 
     @staticmethod
     def from_session_cfg(c):
@@ -106,6 +108,9 @@ class OrcEngineCfg(C.Structure):
         e.depth_threshold = c.depth_threshold
         e.dist_threshold = c.dist_threshold
         e.integration_threshold = c.integration_threshold
+        e.hash = 1 if c.volume_kind == 1 else 0
+        e.voxel, e.mu = c.voxel_size, c.trunc_scale
+        e.buckets, e.excess, e.pool, e.max_w = c.hash_buckets, c.hash_excess, c.hash_pool_blocks, c.hash_max_weight
         return e
 
 
@@ -148,6 +153,7 @@ def oracle():
             "orc_engine_tsdf_params": (None, [_P, _P]),
             "orc_engine_icp_stats": (None, [_P, _P]),
             "orc_engine_touched": (C.c_long, [_P]),
+            "orc_engine_hash": (_P, [_P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(L, k)
@@ -240,6 +246,17 @@ class Engine:
     def touched(self):
         return oracle().orc_engine_touched(self.h)
 
+    def hash_scene(self):
+        """The engine's OracleHash view (hash sessions only)."""
+        h = OracleHash.__new__(OracleHash)
+        _bind(oracle(), _hash_sigs)
+        c = self.cfg
+        h.cfg = OrcHashCfg(c.buckets, c.excess, c.pool, c.buckets - 1, c.voxel, c.mu, c.max_w)
+        h.h = oracle().orc_engine_hash(self.h)
+        h.n_entries = c.buckets + c.excess
+        h._borrowed = True
+        return h
+
 
 # ------------------------------------------------------------------ voxel-block hashing
 class OrcHashCfg(C.Structure):
@@ -293,7 +310,8 @@ class OracleHash:
 
     def __del__(self):
         try:
-            oracle().orc_hash_destroy(self.h)
+            if not getattr(self, "_borrowed", False):
+                oracle().orc_hash_destroy(self.h)
         except Exception:
             pass
 

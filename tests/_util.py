@@ -77,3 +77,13 @@ def rot_angle(Ra, Rb):
     s = 0.5 * np.linalg.norm([M[2, 1] - M[1, 2], M[0, 2] - M[2, 0], M[1, 0] - M[0, 1]])
     c = (np.trace(M) - 1) / 2
     return float(np.arctan2(s, c))
+
+
+def cfg_hash(W=320, H=240, buckets=1 << 16, excess=1 << 14, pool=1 << 16, voxel=0.005, mu=0.02, fmt=L.TSDF_I16,
+             color=False, iters=(10, 5, 4), integ_thr=0.0):
+    f = 525.0 * W / 640.0
+    return L.default_cfg(width=W, height=H, fx=f, fy=f, cx=(W - 1) / 2.0, cy=(H - 1) / 2.0, volume_kind=L.VOLUME_HASH,
+                         tsdf_format=fmt, color_volume=1 if color else 0, hash_buckets=buckets, hash_excess=excess,
+                         hash_pool_blocks=pool, voxel_size=voxel, trunc_scale=mu,
+                         iterations=list(iters) + [0] * (4 - len(iters)), levels=len(iters),
+                         integration_threshold=integ_thr, depth_min=0.4)

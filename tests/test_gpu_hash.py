@@ -1,0 +1,85 @@
+"""GPU parity of the voxel-block hash path against the oracle (itself pinned bit for bit
+to the reference hash kernels): allocation, visible list, integration, raycast, mesh."""
+import numpy as np
+import pytest
+
+from natureuserinterfacestudio_b200 import _lib as L
+from oracle import oracle as O
+
+from _util import cfg_hash, frames, rot_angle, same_bits
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def room():
+    return frames(5, W=320, H=240, seed=5, kind=L.SYNTH_ROOM, deg=0.0, color=True)
+
+
+def _state(s):
+    return s.hash_download(20), s.hash_download(21), s.hash_download(22)
+
+
+def _oracle_state(eng):
+    h = eng.hash_scene()
+    sdf, w, rgb = h.voxels()
+    vox = np.zeros(sdf.size, O.REF_VOXEL)
+    vox["sdf"], vox["w"], vox["rgb"] = sdf, w, rgb
+    return h.entries().view(np.uint8), h.visible(), vox.view(np.uint8), h
+
+
+@pytest.mark.parametrize("color", [False, True])
+def test_hash_first_frame_bit_exact(gpu_ctx, room, color):
+    cfg = cfg_hash(color=color)
+    s = L.Session(gpu_ctx, cfg)
+    eng = O.Engine(cfg)
+    d, c, _, _ = room[0]
+    ok, _ = s.process(d, c if color else None)
+    assert ok and eng.frame(d, np.ascontiguousarray(c) if color else None)
+    e_g, v_g, x_g = _state(s)
+    e_o, v_o, x_o, _ = _oracle_state(eng)
+    assert v_g.size > 1000
+    assert np.array_equal(v_g, v_o)
+    assert np.array_equal(e_g, e_o)
+    assert np.array_equal(x_g, x_o)
+    vis, lb, le, failed = s.hash_stats()
+    assert failed == 0 and vis == v_o.size
+
+
+def test_hash_tracking_sequence(gpu_ctx, room):
+    cfg = cfg_hash()
+    s = L.Session(gpu_ctx, cfg)
+    eng = O.Engine(cfg)
+    exact = True
+    for i, (d, _, Rt, tt) in enumerate(room):
+        ok, pose = s.process(d)
+        assert ok and eng.frame(d), i
+        Ro, to = eng.pose()
+        Rg, tg = pose[:9].reshape(3, 3), pose[9:]
+        assert rot_angle(Rg, Ro) < 1e-4 and np.max(np.abs(tg - to)) < 1e-4, i
+        exact = exact and np.array_equal(Rg, Ro) and np.array_equal(tg, to)
+        assert rot_angle(Rg, Rt) < 0.03 and np.max(np.abs(tg - tt)) < 0.03, i
+    e_g, v_g, x_g = _state(s)
+    e_o, v_o, x_o, h = _oracle_state(eng)
+    if exact:  # identical poses: identical scenes
+        assert np.array_equal(v_g, v_o) and np.array_equal(e_g, e_o) and np.array_equal(x_g, x_o)
+        assert same_bits(s.download(3)[..., :3].reshape(-1), eng.refmap(0).reshape(-1))
+        assert same_bits(s.download(4)[..., :3].reshape(-1), eng.refmap(1).reshape(-1))
+        cap = 4_000_000
+        pg, cg, ng = s.mesh(cap)
+        po, co, no = h.mesh(cap)
+        assert ng == no > 0 and same_bits(pg, po) and same_bits(cg, co)
+    else:
+        inter = np.intersect1d(v_g, v_o).size
+        assert inter > 0.99 * max(v_g.size, v_o.size)
+
+
+def test_hash_half_format_tracks_like_int16(gpu_ctx, room):
+    a = L.Session(gpu_ctx, cfg_hash(fmt=L.TSDF_I16))
+    b = L.Session(gpu_ctx, cfg_hash(fmt=L.TSDF_F16_U8))
+    for d, _, _, _ in room:
+        ok1, p1 = a.process(d)
+        ok2, p2 = b.process(d)
+        assert ok1 and ok2
+        assert rot_angle(p1[:9].reshape(3, 3), p2[:9].reshape(3, 3)) < 2e-3
+        assert np.max(np.abs(p1[9:] - p2[9:])) < 2e-3
