@@ -242,13 +242,21 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
     const float3 r0 = cross3(rn, pv);
     const float c7[7] = {r0.x, r0.y, r0.z, rn.x, rn.y, rn.z, dot3(rn, diff)};
     int sh = 0;
-    // a thread sums at most kIcpPixPerThread rows: plain float here, compensated from the
-    // warp reduction on
 #pragma unroll
     for (int a = 0; a < 6; ++a)
 #pragma unroll
-      for (int b = a; b < 7; ++b, ++sh) hi[sh] += c7[a] * c7[b];
-    hi[27] += c7[6] * c7[6];
+      for (int b = a; b < 7; ++b, ++sh) {
+        float ss, e;
+        two_sum(hi[sh], c7[a] * c7[b], ss, e);
+        hi[sh] = ss;
+        lo[sh] += e;
+      }
+    {
+      float ss, e;
+      two_sum(hi[27], c7[6] * c7[6], ss, e);
+      hi[27] = ss;
+      lo[27] += e;
+    }
     hi[28] += 1.0f;
   }
 

@@ -87,3 +87,12 @@ def cfg_hash(W=320, H=240, buckets=1 << 16, excess=1 << 14, pool=1 << 16, voxel=
                          hash_pool_blocks=pool, voxel_size=voxel, trunc_scale=mu,
                          iterations=list(iters) + [0] * (4 - len(iters)), levels=len(iters),
                          integration_threshold=integ_thr, depth_min=0.4)
+
+
+def relative_gt(seq):
+    """Ground-truth poses expressed in the first camera's frame (the tracker starts at I)."""
+    R0, t0 = np.asarray(seq[0][2], np.float64), np.asarray(seq[0][3], np.float64)
+    out = []
+    for _, _, R, t in seq:
+        out.append((R0.T @ np.asarray(R, np.float64), R0.T @ (np.asarray(t, np.float64) - t0)))
+    return out
