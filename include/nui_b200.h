@@ -159,6 +159,21 @@ NUI_API nui_status nui_get_pose(nui_session* s, float* pose12);
  * NUI_ERR_MESH_OVERFLOW is returned (with the first cap vertices written) when it
  * exceeds cap. */
 NUI_API nui_status nui_mesh(nui_session* s, float* pos, float* col, uint64_t cap, uint64_t* nverts);
+/* Marching cubes of a dense session into caller-provided DEVICE buffers, without any
+ * device allocation.  No counterpart in the reference: it exists for callers that cannot
+ * call cudaMalloc while meshing, e.g. a host application that owns all device memory
+ * through its own pool, or code running where allocation is forbidden or would stall the
+ * GPU.  The per-column counts and block offsets the kernels need live in one file-scope
+ * __device__ array of 1 MiB + 32 KiB (held by every GPU that loads the library until the
+ * process exits), which bounds the volume to (res[0]-1)*(res[1]-1) <= 262144 columns and
+ * (res[1]-1)*ceil((res[0]-1)/128) <= 4095 count blocks; larger volumes are rejected with
+ * NUI_ERR_INVALID_ARG.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call outside any
+ * stream capture.  All calls share the array: two calls that overlap on the GPU (other
+ * threads, other streams) race on it.  Same order, capacity and overflow rules as
+ * nui_mesh; d_pos: cap*3 floats, d_col: cap*4 floats, either may be NULL. */
+NUI_API nui_status nui_mesh_device_noalloc(nui_session* s, float* d_pos, float* d_col, uint64_t cap,
+                                           uint64_t* nverts);
 /* Marching-cubes case index of every cube, (res[0]-1)*(res[1]-1)*(res[2]-1) bytes in the
  * same (y, x, z) order; 0 for cubes skipped because a corner has no weight. */
 NUI_API nui_status nui_mesh_cases(nui_session* s, uint8_t* cases, size_t bytes, uint64_t* nverts);

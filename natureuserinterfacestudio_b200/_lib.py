@@ -75,6 +75,7 @@ _SIGS = {
     "nui_get_pose": (C.c_int, [_P, _P]),
     "nui_mesh": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
     "nui_mesh_cases": (C.c_int, [_P, _P, C.c_size_t, _P]),
+    "nui_mesh_device_noalloc": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
     "nui_debug_download": (C.c_int, [_P, C.c_int, C.c_int, _P, C.c_size_t]),
     "nui_debug_upload_volume": (C.c_int, [_P, _P]),
     "nui_hash_stats": (C.c_int, [_P, _P, _P, _P, _P]),

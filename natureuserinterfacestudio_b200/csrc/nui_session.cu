@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1280,5 +1281,90 @@ extern "C" NUI_API nui_status nui_mesh_cases(nui_session* s, uint8_t* cases, siz
   if (st != NUI_OK) return st;
   NUI_CUDA(cudaMemcpy(cases, dcase.p, need, cudaMemcpyDeviceToHost));
   if (nverts) *nverts = total;
+  return NUI_OK;
+}
+
+// ------------------------------------------------------------------ meshing without allocation
+// Scratch of nui_mesh_device_noalloc: per-column vertex counts (u32) and per-block offsets
+// (u64).  A file-scope device array: host code reaches it only through the address that
+// cudaGetSymbolAddress returns for the current device.
+namespace {
+constexpr size_t kNoAllocCols = 262144;   // (res[0]-1)*(res[1]-1) bound
+constexpr size_t kNoAllocBlocks = 4096;   // count blocks + 1 bound
+static __device__ __align__(256) unsigned char g_mesh_scratch[kNoAllocCols * 4 + kNoAllocBlocks * 8];
+constexpr int kMaxDevices = 64;
+unsigned char* g_mesh_scratch_addr[kMaxDevices] = {};
+std::mutex g_mesh_scratch_mu;
+
+// Device address of the scratch array on `device` (current); looked up on the first call.
+// Nothing in the array needs to start at zero: the count pass writes every column count and
+// every block total before the scan and the emit pass read them.
+nui_status noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= kMaxDevices) return fail(NUI_ERR_INVALID_ARG, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_mesh_scratch_mu);
+  if (!g_mesh_scratch_addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_mesh_scratch);
+    if (e != cudaSuccess) return fail(NUI_ERR_DEVICE, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_mesh_scratch_addr[device] = (unsigned char*)p;
+  }
+  *out = g_mesh_scratch_addr[device];
+  return NUI_OK;
+}
+}  // namespace
+
+extern "C" NUI_API nui_status nui_mesh_device_noalloc(nui_session* s, float* d_pos, float* d_col, uint64_t cap,
+                                                      uint64_t* nverts) {
+  if (!s || !nverts) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  if (s->hash) return fail(NUI_ERR_UNSUPPORTED, "dense sessions only");
+  const nui_session_cfg& c = s->cfg;
+  const size_t ncols = (size_t)(c.res[0] - 1) * (c.res[1] - 1);
+  const unsigned nb = cdiv(c.res[0] - 1, 128) * (unsigned)(c.res[1] - 1);
+  if (ncols > kNoAllocCols || (size_t)nb + 1 > kNoAllocBlocks)
+    return fail(NUI_ERR_INVALID_ARG, "volume too large for the no-allocation mesh scratch");
+  NUI_CUDA(cudaSetDevice(s->ctx->device));
+  for (const float* q : {(const float*)d_pos, (const float*)d_col}) {
+    if (!q) continue;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, q) != cudaSuccess ||
+        (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)) {
+      cudaGetLastError();
+      return fail(NUI_ERR_INVALID_ARG, "output buffers must be device memory");
+    }
+  }
+  unsigned char* base = nullptr;
+  nui_status st0 = noalloc_scratch(s->ctx->device, &base);
+  if (st0 != NUI_OK) return st0;
+  unsigned* cc = (unsigned*)base;
+  unsigned long long* bt = (unsigned long long*)(base + kNoAllocCols * 4);
+  cudaStream_t st = s->ctx->stream;
+  SessionDesc d;
+  fill_desc(s, d, kInactive, nullptr, nullptr);
+  NUI_CUDA(cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, st));
+  mc_upload_tables(st);
+  switch (c.tsdf_format) {
+    case 0: mc_count<0>(s, nb, cc, bt, nullptr); break;
+    case 1: mc_count<1>(s, nb, cc, bt, nullptr); break;
+    case 2: mc_count<2>(s, nb, cc, bt, nullptr); break;
+    case 3: mc_count<3>(s, nb, cc, bt, nullptr); break;
+  }
+  k_mc_scan<<<1, 1024, 0, st>>>(bt, (int)nb);
+  NUI_CUDA(cudaGetLastError());
+  unsigned long long total = 0;
+  NUI_CUDA(cudaMemcpyAsync(&total, bt + nb, sizeof(total), cudaMemcpyDeviceToHost, st));
+  NUI_CUDA(cudaStreamSynchronize(st));
+  *nverts = total;
+  const unsigned long long k = total < cap ? total : cap;
+  if (k > 0 && (d_pos || d_col)) {
+    switch (c.tsdf_format) {
+      case 0: mc_emit<0>(s, nb, cc, bt, d_pos, d_col, k); break;
+      case 1: mc_emit<1>(s, nb, cc, bt, d_pos, d_col, k); break;
+      case 2: mc_emit<2>(s, nb, cc, bt, d_pos, d_col, k); break;
+      case 3: mc_emit<3>(s, nb, cc, bt, d_pos, d_col, k); break;
+    }
+    NUI_CUDA(cudaGetLastError());
+    NUI_CUDA(cudaStreamSynchronize(st));
+  }
+  if (total > cap) return fail(NUI_ERR_MESH_OVERFLOW, "mesh larger than the output capacity");
   return NUI_OK;
 }
