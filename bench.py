@@ -205,7 +205,11 @@ def run_ours(args, rank, world):
     stage /= reps
     touched /= reps
     bytes_per_voxel = 3  # FP16 tsdf + u8 weight
-    integ_bytes = touched * 2 * bytes_per_voxel + n * W_IMG * H_IMG * 4
+    # algorithmic bytes of one integration launch: every voxel's state read and written once
+    # plus each session's depth image read once (N_vox * 2 * S + W * H * 4 per session)
+    n_vox = sum(int(np.prod(c.res)) for c in session_cfgs(L, n, L.TSDF_F16_U8))
+    integ_bytes = n_vox * 2 * bytes_per_voxel + n * W_IMG * H_IMG * 4
+    touched_bytes = touched * 2 * bytes_per_voxel + n * W_IMG * H_IMG * 4
     integ_ms = stage[3]
     peak, peak_kind = peaks()
     achieved = integ_bytes / (integ_ms / 1e3) / 1e9
@@ -263,7 +267,9 @@ def run_ours(args, rank, world):
             "roofline": {"kernel": "k_integrate<F16_U8>", "bound": "hbm", "achieved": round(achieved, 1),
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": profile_traffic("k_integrate"),
-                         "algorithmic_bytes_per_launch": int(integ_bytes), "launch_ms": round(float(integ_ms), 4)},
+                         "algorithmic_bytes_per_launch": int(integ_bytes), "launch_ms": round(float(integ_ms), 4),
+                         "touched_voxel_bytes_per_launch": int(touched_bytes),
+                         "touched_voxel_gbs": round(touched_bytes / (integ_ms / 1e3) / 1e9, 1)},
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "tracking_lost": lost,
