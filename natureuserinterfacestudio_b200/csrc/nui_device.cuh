@@ -80,6 +80,8 @@ struct SessionDesc {
   uint8_t* wvol;                  // weight plane of NUI_TSDF_F16_U8
   uchar4* cvol;                   // colour volume (nullable), same layout
   uint8_t* occ;                   // per 8^3 brick state (kBrick*)
+  uint8_t* occ2;                  // per 32^3 super-brick state (kSuper*)
+  uint8_t* occ3;                  // per 128^3 region state (kSuper*, over its super-bricks)
   int max_cw;
   int zchunks;                    // integration: z chunks per column (one thread each)
   // tracking state and ICP scratch
@@ -234,13 +236,30 @@ struct Voxel<3> {  // NUI_TSDF_F16_F16: half2 (tsdf, weight)
 __device__ __forceinline__ size_t vox_index(const SessionDesc& s, int x, int y, int z) {
   return (size_t)x + (size_t)s.res[0] * ((size_t)y + (size_t)s.res[1] * (size_t)z);
 }
-// Brick states of 8^3 voxels.  Weights never decrease between resets, so an empty brick
-// holds only weight-0 voxels; a positive brick has every voxel weighted with tsdf > 0.
+// Brick states of 8^3 voxels (the voxels of a brick inside the volume).  Weights never
+// decrease between resets, so an empty brick holds only weight-0 voxels; a positive brick
+// has every voxel weighted with tsdf > 0; a no-negative brick mixes weight-0 voxels with
+// weighted ones of tsdf > 0; a mixed brick has a weighted voxel with tsdf <= 0.
 // Integration marks the bricks it touches dirty and k_brick_summary re-classifies them.
-enum BrickState : uint8_t { kBrickEmpty = 0, kBrickMixed = 1, kBrickPositive = 2, kBrickDirty = 3 };
+enum BrickState : uint8_t {
+  kBrickEmpty = 0,
+  kBrickMixed = 1,
+  kBrickPositive = 2,
+  kBrickDirty = 3,
+  kBrickNoNeg = 4
+};
+// States of 32^3-voxel super-bricks (4^3 bricks): all bricks empty; some brick mixed or
+// dirty; every brick empty, positive or no-negative (a march can cross it without a sign
+// change); or awaiting re-classification.  128^3-voxel regions (4^3 super-bricks) use the
+// same states over their super-bricks.
+enum SuperState : uint8_t { kSuperEmpty = 0, kSuperMixed = 1, kSuperSkip = 2, kSuperDirty = 3 };
 __device__ __forceinline__ size_t occ_index(const SessionDesc& s, int x, int y, int z) {
   const size_t bx = (size_t)(s.res[0] + 7) >> 3, by = (size_t)(s.res[1] + 7) >> 3;
   return (size_t)(x >> 3) + bx * ((size_t)(y >> 3) + by * (size_t)(z >> 3));
+}
+__device__ __forceinline__ size_t occ2_index(const SessionDesc& s, int x, int y, int z) {
+  const size_t sx = (size_t)(s.res[0] + 31) >> 5, sy = (size_t)(s.res[1] + 31) >> 5;
+  return (size_t)(x >> 5) + sx * ((size_t)(y >> 5) + sy * (size_t)(z >> 5));
 }
 // round(p / c) for a voxel coordinate, exactly as the IEEE quotient would round: the
 // product with 1/c is within 2 ulp of the quotient, so unless it lies within 4 ulp of a

@@ -8,15 +8,74 @@
 // trilinear weights pair the x-neighbour voxel with the y fraction and the y-neighbour
 // with the x fraction, as the reference's index walk does (raycast.cl:66-119).
 //
-// Brick skipping (exact): when a sample lands in an 8^3 brick whose voxels are all
-// unweighted (every sample there reads NaN) or all weighted with tsdf > 0 (every sample
-// there is positive, so after the first one no transition can happen), the following
-// samples that stay inside the brick -- by a margin of 1% of a voxel -- change nothing but
-// the march parameter; they are skipped by advancing the parameter with the same float
-// additions.
+// Region skipping (exact): when a sample lands in an 8^3 brick, or a 32^3 super-brick,
+// that holds no weighted voxel with tsdf <= 0, no two consecutive samples inside it can
+// form a transition (each reads NaN or a positive value).  The samples that stay inside
+// the region -- by a margin of 1% of a voxel -- are skipped: the march parameter jumps to
+// the last of them along the exact float sequence t <- t + step (march_advance), and only
+// that sample is read (its value, NaN or positive, is the next "previous" sample).  In an
+// all-empty region, or a brick whose voxels are all weighted and positive, it is known
+// without the read.
 #include "nui_device.cuh"
 
 namespace nui {
+
+// t <- fl(t + step) repeated while fl(t + step) < Y (for Y <= cap this is also the
+// plain loop's "while t < cap and fl(t + step) < Y"); returns the final t, the same value
+// as the plain loop.  Inside one binade [2^e, 2^(e+1)) every element is a multiple of
+// u = 2^(e-23), and as long as the sum stays in the binade fl(t + step) = t + M u with M
+// the integer nearest step / u (on an exact tie, round to even: once t / u is even the
+// increment is the even one of the two neighbours).  Runs of additions inside a binade
+// are therefore counted in 32-bit integers (t / u < 2^24); the addition that leaves a
+// binade is done plainly.
+__device__ __forceinline__ float march_advance(float t, float step, float Y) {
+  for (;;) {
+    const float n = t + step;
+    if (!(n < Y) || !(n > t)) return t;
+    const int ex = ((__float_as_int(t) >> 23) & 0xff) - 127;  // t in [2^ex, 2^(ex+1))
+    if (ex < -100 || ex > 100) {
+      t = n;
+      continue;
+    }
+    const float inv_u = __int_as_float((127 + 23 - ex) << 23);
+    const float u = __int_as_float((127 - 23 + ex) << 23);
+    const float q = step * inv_u;  // exact: scaling by a power of two
+    if (!(q < 8388608.f)) {        // the step spans the binade
+      t = n;
+      continue;
+    }
+    const float fq = floorf(q), fr = q - fq;
+    unsigned M = (unsigned)fq;
+    const unsigned T = (unsigned)(t * inv_u);
+    if (fr == 0.5f) {
+      if (T & 1u) {  // the first tie may round up; afterwards t / u stays even
+        t = n;
+        continue;
+      }
+      M += (M & 1u);
+    } else if (fr > 0.5f) {
+      M += 1u;
+    }
+    const float ys = Y * inv_u;
+    const unsigned L = ys < 16777216.f ? (unsigned)ceilf(ys) - 1u : 16777215u;  // results must stay <= L
+    if (L < T + M) {  // the next addition leaves the binade
+      t = n;
+      continue;
+    }
+    const unsigned k = (L - T) / M;
+    t = (float)(T + k * M) * u;
+  }
+}
+
+// The plain loop, for the rare call whose cap lies below its bound.
+__device__ __noinline__ float march_advance_capped(float t, float step, float Y, float cap) {
+  for (;;) {
+    if (!(t < cap)) return t;
+    const float n = t + step;
+    if (!(n < Y) || !(n > t)) return t;
+    t = n;
+  }
+}
 
 template <int FMT>
 struct RayVol {
@@ -88,21 +147,24 @@ struct RayVol {
            t110 * a * b * (1 - c) + t111 * a * b * c;
   }
   // Largest ray parameter up to which a sample stays (by 1% of a voxel) inside the
-  // p-box of brick (x>>3, y>>3, z>>3) clipped to the volume; samples with parameter below
-  // it map to voxels of that brick.
-  __device__ __forceinline__ float brick_exit(int gx, int gy, int gz, float3 start, float3 dir) const {
-    const int b[3] = {gx & ~7, gy & ~7, gz & ~7};
+  // p-box of the aligned region of S^3 voxels (S a power of two) holding (gx, gy, gz),
+  // clipped to the volume; samples with parameter below it map to voxels of that region.
+  // The margin also absorbs the rounding of the reciprocal direction used here.
+  __device__ __forceinline__ float region_exit(int S, int gx, int gy, int gz, float3 start, float3 dir,
+                                               float3 idir) const {
+    const int b[3] = {gx & ~(S - 1), gy & ~(S - 1), gz & ~(S - 1)};
     const int r[3] = {rx, ry, rz};
     const float c[3] = {c0, c1, c2};
     const float o[3] = {start.x, start.y, start.z};
     const float d[3] = {dir.x, dir.y, dir.z};
+    const float id[3] = {idir.x, idir.y, idir.z};
     float te = 3.4e38f;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const float lo = ((float)b[a] - 0.5f + 0.01f) * c[a];
-      const float hi = ((float)min(b[a] + 8, r[a]) - 0.5f - 0.01f) * c[a];
-      if (d[a] > 0.f) te = fminf(te, (hi - o[a]) / d[a]);
-      else if (d[a] < 0.f) te = fminf(te, (lo - o[a]) / d[a]);
+      const float hi = ((float)min(b[a] + S, r[a]) - 0.5f - 0.01f) * c[a];
+      if (d[a] > 0.f) te = fminf(te, (hi - o[a]) * id[a]);
+      else if (d[a] < 0.f) te = fminf(te, (lo - o[a]) * id[a]);
     }
     return te;
   }
@@ -112,10 +174,15 @@ template <int FMT>
 __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (s.kind != kTrackFrame || s.fmt != FMT || s.ts->status != 0) return;
+  // a block shades 16 x 8 pixels, each warp an 8 x 4 tile (neighbouring rays march alike)
   const int W = s.W, H = s.H;
-  const int id = blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= W * H) return;
-  const int px = id % W, py = id / W;
+  const int tiles_x = (W + 15) >> 4;
+  if ((int)blockIdx.x >= tiles_x * ((H + 7) >> 3)) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int px = ((int)blockIdx.x % tiles_x) * 16 + (warp & 1) * 8 + (lane & 7);
+  const int py = ((int)blockIdx.x / tiles_x) * 8 + (warp >> 1) * 4 + (lane >> 3);
+  if (px >= W || py >= H) return;
+  const int id = py * W + px;
   const float4 nanv = make_float4(qnan(), qnan(), qnan(), 0.f);
   float4 vout = nanv, nout = nanv;
   uchar4 cout = make_uchar4(0, 0, 0, 0);
@@ -149,30 +216,66 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
     if (V.tsdf_at(gx, gy, gz, f)) tsdf = f;
     const float max_time = 3 * (D0 + D1 + D2);
     const float step = s.trunc * 0.8f;
-    for (; tc < max_time; tc += step) {
-      const float prev = tsdf;
-      V.voxel_of(add3(start, mul3(dir, tc + step)), gx, gy, gz);
+    const int sx = (V.rx + 31) >> 5, sy = (V.ry + 31) >> 5;
+    const int hx = (V.rx + 127) >> 7, hy = (V.ry + 127) >> 7;
+    const float3 idir = f3(1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z);
+    bool pend = false;  // tsdf stands for a skipped sample at tc whose class (NaN or > 0) is unread
+    while (tc < max_time) {
+      float prev = tsdf;
+      const float tn = tc + step;
+      V.voxel_of(add3(start, mul3(dir, tn)), gx, gy, gz);
       if (!(gx >= 0 && gy >= 0 && gz >= 0 && gx < V.rx && gy < V.ry && gz < V.rz)) break;
       const uint8_t st = V.occ ? __ldg(V.occ + V.bidx(gx, gy, gz)) : (uint8_t)kBrickMixed;
+      // only the class of a sample (NaN, < 0, 0, > 0) enters the march decisions
       if (st == kBrickEmpty) {
         tsdf = qnan();
+      } else if (st == kBrickPositive) {
+        tsdf = 1.0f;
       } else {
         tsdf = V.load(V.vidx(gx, gy, gz), f) ? f : qnan();
       }
-      if (st == kBrickEmpty || (st == kBrickPositive && !(prev < 0.f))) {
-        // every further sample inside this brick reads the same kind of value: skip them
-        const float te = V.brick_exit(gx, gy, gz, start, dir);
-        for (;;) {
-          const float tn = tc + step;
-          if (!(tn < max_time) || !(tn + step < te)) break;
-          tc = tn;
+      if ((st == kBrickEmpty || st == kBrickPositive || st == kBrickNoNeg) && (!(prev < 0.f) || isnan(tsdf))) {
+        // no transition at this sample (its value is NaN or > 0 and prev is not negative,
+        // or it is NaN), nor between any two samples of the region: skip to the last one
+        int S = 128;
+        bool uniform;
+        const uint8_t s3 = __ldg(s.occ3 + (gx >> 7) + hx * ((gy >> 7) + hy * (gz >> 7)));
+        if (s3 == kSuperEmpty || s3 == kSuperSkip) {
+          uniform = s3 == kSuperEmpty;
+        } else {
+          const uint8_t s2 = __ldg(s.occ2 + (gx >> 5) + sx * ((gy >> 5) + sy * (gz >> 5)));
+          if (s2 == kSuperEmpty || s2 == kSuperSkip) {
+            S = 32;
+            uniform = s2 == kSuperEmpty;
+          } else {
+            S = 8;
+            uniform = st != kBrickNoNeg;
+          }
         }
+        const float te = V.region_exit(S, gx, gy, gz, start, dir, idir);
+        const float tl = te <= max_time ? march_advance(tn, step, te) : march_advance_capped(tn, step, te, max_time);
+        if (tl == tn || uniform) {
+          pend = false;  // tsdf is the class of the sample at tl
+        } else {
+          pend = true;
+          tsdf = 1.0f;
+        }
+        tc = tl;
         continue;
       }
-      if (isnan(tsdf) || isnan(prev)) continue;
+      if (pend) {  // the previous sample was skipped: read its class now
+        int lx, ly, lz;
+        V.voxel_of(add3(start, mul3(dir, tc)), lx, ly, lz);
+        prev = V.tsdf_at(lx, ly, lz, f) ? f : qnan();
+        pend = false;
+      }
+      if (isnan(tsdf) || isnan(prev)) {
+        tc = tn;
+        continue;
+      }
       if (prev < 0.f && tsdf > 0.f) break;
       if (prev >= 0.f && tsdf <= 0.f) {
-        const float Ftdt = V.trilinear(add3(start, mul3(dir, tc + step)));
+        const float Ftdt = V.trilinear(add3(start, mul3(dir, tn)));
         if (isnan(Ftdt)) break;
         const float Ft = V.trilinear(add3(start, mul3(dir, tc)));
         if (isnan(Ft)) break;
@@ -197,6 +300,7 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
         }
         break;
       }
+      tc = tn;
     }
   }
   s.vref[id] = vout;

@@ -241,24 +241,71 @@ __global__ void __launch_bounds__(256) k_brick_summary(const SessionDesc* __rest
   }
   __syncthreads();
   const int lane = threadIdx.x & 31;
+  const int sx = (s.res[0] + 31) >> 5, sy = (s.res[1] + 31) >> 5;
   for (int k = threadIdx.x >> 5; k < count; k += blockDim.x >> 5) {
     const long b = b0 + list[k];
     const int x0 = (int)(b % bx) * 8, y0 = (int)((b / bx) % by) * 8, z0 = (int)(b / ((long)bx * by)) * 8;
-    bool all_pos = true;
+    bool weighted = false, unweighted = false, nonpos = false;
     for (int r = lane >> 3; r < 64; r += 4) {  // 64 rows (y, z) of 8 voxels; lane & 7 = x
       const int x = x0 + (lane & 7), y = y0 + (r & 7), z = z0 + (r >> 3);
-      if (x >= s.res[0] || y >= s.res[1] || z >= s.res[2]) {
-        all_pos = false;  // partial bricks at the volume edge stay mixed
-        continue;
-      }
+      if (x >= s.res[0] || y >= s.res[1] || z >= s.res[2]) continue;
       float F;
       int W;
       Voxel<FMT>::load(s, vox_index(s, x, y, z), F, W);
-      if (!(W > 0 && F > 0.f)) all_pos = false;
+      if (W > 0) {
+        weighted = true;
+        if (!(F > 0.f)) nonpos = true;
+      } else {
+        unweighted = true;
+      }
     }
-    const unsigned pos = __all_sync(0xffffffffu, all_pos);
-    if (lane == 0) s.occ[b] = pos ? kBrickPositive : kBrickMixed;
+    const bool any_w = __any_sync(0xffffffffu, weighted), any_u = __any_sync(0xffffffffu, unweighted);
+    const bool any_np = __any_sync(0xffffffffu, nonpos);
+    if (lane == 0) {
+      s.occ[b] = any_np ? kBrickMixed : !any_w ? kBrickEmpty : any_u ? kBrickNoNeg : kBrickPositive;
+      if (s.occ2) s.occ2[(x0 >> 5) + (size_t)sx * ((y0 >> 5) + (size_t)sy * (z0 >> 5))] = kSuperDirty;
+    }
   }
+}
+
+// Re-classifies the super-bricks whose bricks k_brick_summary changed, then the 128^3
+// regions holding them: one block of 64 threads per region, one thread per super-brick.
+__global__ void __launch_bounds__(64) k_super_summary(const SessionDesc* __restrict__ descs, int force) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (s.fmt < 0 || !s.occ2) return;
+  if (!force && (s.kind < 0 || !s.ts->integrate)) return;
+  const int sx = (s.res[0] + 31) >> 5, sy = (s.res[1] + 31) >> 5, sz = (s.res[2] + 31) >> 5;
+  const int hx = (sx + 3) >> 2, hy = (sy + 3) >> 2, hz = (sz + 3) >> 2;
+  const int h = blockIdx.x;
+  if (h >= hx * hy * hz) return;
+  const int HX = h % hx, HY = (h / hx) % hy, HZ = h / (hx * hy);
+  const int X = 4 * HX + (threadIdx.x & 3), Y = 4 * HY + ((threadIdx.x >> 2) & 3), Z = 4 * HZ + (threadIdx.x >> 4);
+  const bool live = X < sx && Y < sy && Z < sz;
+  const size_t i = (size_t)X + (size_t)sx * (Y + (size_t)sy * Z);
+  uint8_t st = kSuperEmpty;
+  bool changed = false;
+  if (live) {
+    st = s.occ2[i];
+    if (st == kSuperDirty) {
+      changed = true;
+      const int bx = (s.res[0] + 7) >> 3, by = (s.res[1] + 7) >> 3, bz = (s.res[2] + 7) >> 3;
+      bool all_empty = true, mixed = false;
+      for (int c = 4 * Z; c < min(4 * Z + 4, bz); ++c)
+        for (int b = 4 * Y; b < min(4 * Y + 4, by); ++b)
+          for (int a = 4 * X; a < min(4 * X + 4, bx); ++a) {
+            const uint8_t bs = s.occ[a + (size_t)bx * (b + (size_t)by * c)];
+            if (bs != kBrickEmpty) all_empty = false;
+            if (bs == kBrickMixed || bs == kBrickDirty) mixed = true;
+          }
+      st = mixed ? kSuperMixed : all_empty ? kSuperEmpty : kSuperSkip;
+      s.occ2[i] = st;
+    }
+  }
+  const bool any_changed = __syncthreads_or(changed);
+  if (!any_changed) return;
+  const bool any_mixed = __syncthreads_or(st == kSuperMixed || st == kSuperDirty);
+  const bool any_nonempty = __syncthreads_or(st != kSuperEmpty);
+  if (threadIdx.x == 0) s.occ3[h] = any_mixed ? kSuperMixed : any_nonempty ? kSuperSkip : kSuperEmpty;
 }
 
 template <int FMT>
@@ -272,7 +319,15 @@ __global__ void k_volume_init(const SessionDesc* __restrict__ descs) {
   const size_t nb = (size_t)((s.res[0] + 7) >> 3) * ((s.res[1] + 7) >> 3) * ((s.res[2] + 7) >> 3);
   if (s.occ)
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (size_t)gridDim.x * blockDim.x)
-      s.occ[i] = 0;
+      s.occ[i] = kBrickEmpty;
+  const size_t ns = (size_t)((s.res[0] + 31) >> 5) * ((s.res[1] + 31) >> 5) * ((s.res[2] + 31) >> 5);
+  if (s.occ2)
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (size_t)gridDim.x * blockDim.x)
+      s.occ2[i] = kSuperEmpty;
+  const size_t nh = (size_t)((s.res[0] + 127) >> 7) * ((s.res[1] + 127) >> 7) * ((s.res[2] + 127) >> 7);
+  if (s.occ3)
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nh; i += (size_t)gridDim.x * blockDim.x)
+      s.occ3[i] = kSuperEmpty;
 }
 
 template __global__ void k_integrate<0>(const SessionDesc*);

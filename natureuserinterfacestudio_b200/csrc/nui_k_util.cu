@@ -60,7 +60,15 @@ __global__ void k_occ_clear(const SessionDesc* __restrict__ descs) {
   if (!s.occ) return;
   const size_t n = (size_t)((s.res[0] + 7) >> 3) * ((s.res[1] + 7) >> 3) * ((s.res[2] + 7) >> 3);
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    s.occ[i] = 0;
+    s.occ[i] = kBrickEmpty;
+  const size_t ns = (size_t)((s.res[0] + 31) >> 5) * ((s.res[1] + 31) >> 5) * ((s.res[2] + 31) >> 5);
+  if (s.occ2)
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (size_t)gridDim.x * blockDim.x)
+      s.occ2[i] = kSuperEmpty;
+  const size_t nh = (size_t)((s.res[0] + 127) >> 7) * ((s.res[1] + 127) >> 7) * ((s.res[2] + 127) >> 7);
+  if (s.occ3)
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nh; i += (size_t)gridDim.x * blockDim.x)
+      s.occ3[i] = kSuperEmpty;
 }
 
 template <int FMT>

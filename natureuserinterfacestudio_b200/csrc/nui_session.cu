@@ -35,6 +35,7 @@ template <int F>
 __global__ void k_volume_init(const SessionDesc*);
 template <int F>
 __global__ void k_brick_summary(const SessionDesc*, int);
+__global__ void k_super_summary(const SessionDesc*, int);
 template <int F>
 __global__ void k_raycast(const SessionDesc*);
 __global__ void k_publish(const SessionDesc*, int, float*, int*);
@@ -82,15 +83,19 @@ constexpr int kZChunkTargetThreads = 1 << 18;
 
 struct nui_session;
 
+// Launch shape of a batch; the key of the graph cache (compared bytewise, so the
+// constructor zeroes every byte, padding included).
 struct BatchPlan {
-  int n = 0;
-  int maxW = 0, maxH = 0, maxLevels = 0;
-  int maxIters[kMaxLevels] = {0, 0, 0, 0};
-  long maxIntegThreads[4] = {0, 0, 0, 0};  // per format: columns * zchunks
-  long maxBricks[4] = {0, 0, 0, 0};        // per format: 8^3 bricks
-  int hashMask = 0;                        // bit per hash sdf format
-  long maxHashBlk = 0;                     // scan blocks of 1024 entries
-  int fmtMask = 0;
+  int n;
+  int maxW, maxH, maxLevels;
+  int maxIters[kMaxLevels];
+  long maxIntegThreads[4];  // per format: columns * zchunks
+  long maxBricks[4];        // per format: 8^3 bricks
+  long maxHyper;            // 128^3 regions, all dense formats
+  long maxHashBlk;          // scan blocks of 1024 entries
+  int hashMask;             // bit per hash sdf format
+  int fmtMask;
+  BatchPlan() { std::memset(this, 0, sizeof(*this)); }
   bool operator<(const BatchPlan& o) const { return std::memcmp(this, &o, sizeof(BatchPlan)) < 0; }
 };
 
@@ -133,6 +138,8 @@ struct nui_session {
   uint8_t* wvol = nullptr;
   uchar4* cvol = nullptr;
   uint8_t* occ = nullptr;
+  uint8_t* occ2 = nullptr;
+  uint8_t* occ3 = nullptr;
   float* tile_max = nullptr;
   TrackState* ts = nullptr;
   float2* partials = nullptr;
@@ -242,6 +249,8 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
   d.wvol = s->wvol;
   d.cvol = s->cvol;
   d.occ = s->occ;
+  d.occ2 = s->occ2;
+  d.occ3 = s->occ3;
   d.max_cw = c.max_color_weight;
   d.zchunks = s->zchunks;
   d.ts = s->ts;
@@ -290,6 +299,8 @@ void plan_add(BatchPlan& p, const nui_session* s) {
   p.fmtMask |= 1 << c.tsdf_format;
   const long nb = (long)((c.res[0] + 7) / 8) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8);
   p.maxBricks[c.tsdf_format] = std::max(p.maxBricks[c.tsdf_format], nb);
+  const long nh = (long)((c.res[0] + 127) / 128) * ((c.res[1] + 127) / 128) * ((c.res[2] + 127) / 128);
+  p.maxHyper = std::max(p.maxHyper, nh);
 }
 
 unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
@@ -312,10 +323,18 @@ void launch_summary(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, i
   if (!(p.fmtMask & (1 << F))) return;
   k_brick_summary<F><<<dim3(cdiv(p.maxBricks[F], 1024), p.n), 256, 0, st>>>(d, force);
 }
+// Brick re-classification after integration, then the super-bricks it touched.
+void launch_summaries(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, int force) {
+  launch_summary<0>(p, d, st, force);
+  launch_summary<1>(p, d, st, force);
+  launch_summary<2>(p, d, st, force);
+  launch_summary<3>(p, d, st, force);
+  if (p.fmtMask) k_super_summary<<<dim3((unsigned)p.maxHyper, p.n), 64, 0, st>>>(d, force);
+}
 template <int F>
 void launch_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   if (!(p.fmtMask & (1 << F))) return;
-  k_raycast<F><<<dim3(cdiv((long)p.maxW * p.maxH, 128), p.n), 128, 0, st>>>(d);
+  k_raycast<F><<<dim3(cdiv(p.maxW, 16) * cdiv(p.maxH, 8), p.n), 128, 0, st>>>(d);
 }
 
 void launch_hash_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
@@ -371,10 +390,7 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
   launch_integrate<1>(p, d, st);
   launch_integrate<2>(p, d, st);
   launch_integrate<3>(p, d, st);
-  launch_summary<0>(p, d, st, 0);
-  launch_summary<1>(p, d, st, 0);
-  launch_summary<2>(p, d, st, 0);
-  launch_summary<3>(p, d, st, 0);
+  launch_summaries(p, d, st, 0);
   launch_hash_integrate(p, d, st);
   mark(4);
   launch_raycast<0>(p, d, st);
@@ -644,6 +660,8 @@ NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
   b += nv * voxel_bytes(c->tsdf_format);
   if (c->color_volume) b += nv * 4;
   b += (size_t)((c->res[0] + 7) / 8) * ((c->res[1] + 7) / 8) * ((c->res[2] + 7) / 8);
+  b += (size_t)((c->res[0] + 31) / 32) * ((c->res[1] + 31) / 32) * ((c->res[2] + 31) / 32);
+  b += (size_t)((c->res[0] + 127) / 128) * ((c->res[1] + 127) / 128) * ((c->res[2] + 127) / 128);
   return b;
 }
 
@@ -698,7 +716,9 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
     ok = ok && alloc((void**)&s->vol, nv * (c.tsdf_format == 2 ? 2 : voxel_bytes(c.tsdf_format)));
     if (ok && c.tsdf_format == NUI_TSDF_F16_U8) ok = alloc((void**)&s->wvol, nv);
     const size_t nbricks = (size_t)((c.res[0] + 7) / 8) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8);
-    if (ok) ok = alloc((void**)&s->occ, nbricks);
+    const size_t nsuper = (size_t)((c.res[0] + 31) / 32) * ((c.res[1] + 31) / 32) * ((c.res[2] + 31) / 32);
+    const size_t nhyper = (size_t)((c.res[0] + 127) / 128) * ((c.res[1] + 127) / 128) * ((c.res[2] + 127) / 128);
+    if (ok) ok = alloc((void**)&s->occ, nbricks) && alloc((void**)&s->occ2, nsuper) && alloc((void**)&s->occ3, nhyper);
     if (ok && c.color_volume) ok = alloc((void**)&s->cvol, nv * 4) && alloc((void**)&s->bgra, N * 4) && alloc((void**)&s->cmap, N * 4);
   }
   if (!ok) {
@@ -848,10 +868,7 @@ nui_status run_stage(nui_session* s, int what) {
     launch_integrate<1>(p, dd, st);
     launch_integrate<2>(p, dd, st);
     launch_integrate<3>(p, dd, st);
-    launch_summary<0>(p, dd, st, 0);
-    launch_summary<1>(p, dd, st, 0);
-    launch_summary<2>(p, dd, st, 0);
-    launch_summary<3>(p, dd, st, 0);
+    launch_summaries(p, dd, st, 0);
     launch_hash_integrate(p, dd, st);
   } else if (what == 3) {
     launch_raycast<0>(p, dd, st);
@@ -1035,10 +1052,7 @@ NUI_API nui_status nui_debug_upload_volume(nui_session* s, const int16_t* ref) {
   BatchPlan p;
   p.n = 1;
   plan_add(p, s);
-  launch_summary<0>(p, s->d_desc1, s->ctx->stream, 1);
-  launch_summary<1>(p, s->d_desc1, s->ctx->stream, 1);
-  launch_summary<2>(p, s->d_desc1, s->ctx->stream, 1);
-  launch_summary<3>(p, s->d_desc1, s->ctx->stream, 1);
+  launch_summaries(p, s->d_desc1, s->ctx->stream, 1);
   cudaError_t e = cudaStreamSynchronize(s->ctx->stream);
   cudaFree(tmp);
   if (e != cudaSuccess) return fail(NUI_ERR_DEVICE, cudaGetErrorString(e));
