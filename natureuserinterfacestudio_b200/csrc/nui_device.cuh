@@ -84,6 +84,7 @@ struct SessionDesc {
   uint8_t* occ3;                  // per 128^3 region state (kSuper*, over its super-bricks)
   int max_cw;
   int zchunks;                    // integration: z chunks per column (one thread each)
+  float* ztab;                    // integration: running sums shared by all columns, 2 (rz + 1)
   // tracking state and ICP scratch
   TrackState* ts;
   float2* partials;               // per-block (hi, lo) sums, kIcpTerms per block

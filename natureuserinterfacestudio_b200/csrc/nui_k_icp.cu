@@ -319,12 +319,35 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
 
 // After the last ICP launch (or on frame 0): publish the pose, decide the integration
 // gate (NuiKinfuTrackingEngine.cpp:115-127) and reset the estimate for the next frame.
+// Running sums of integrateTsdfVolumeKernel that do not depend on the voxel column
+// (tsdfVolume.cl:74-79: v_g_z and z_scaled, both advanced by cell_z per slice), for the
+// pose integration will use: ztab[z] and ztab[rz + 1 + z] after z additions.
+__device__ void fill_ztab(const SessionDesc& s, const TrackState* ts) {
+  if (!s.ztab) return;
+  const int rz = s.res[2];
+  const float c2 = s.cell[2];
+  float vgz = 0.5f * c2 - ts->xf.t[2], zs = 0.f;
+  for (int z = 0; z <= rz; ++z) {
+    s.ztab[z] = vgz;
+    s.ztab[rz + 1 + z] = zs;
+    vgz += c2;
+    zs += c2;
+  }
+}
+
+// The table for an integration the host requests directly (step-wise calls).
+__global__ void k_ztab(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.x];
+  if (threadIdx.x == 0 && s.kind >= 0) fill_ztab(s, s.ts);
+}
+
 __global__ void k_track_finalize(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.x];
   if (threadIdx.x != 0 || s.kind < 0) return;
   TrackState* ts = s.ts;
   if (s.kind == kFirstFrame) {
     ts->integrate = ts->status == 0 ? 1 : 0;
+    if (ts->integrate) fill_ztab(s, ts);
     return;
   }
   if (ts->status != 0) {  // tracking lost: keep the previous pose, skip the rest
@@ -356,6 +379,7 @@ __global__ void k_track_finalize(const SessionDesc* __restrict__ descs) {
   tn = sqrt(tn);
   ts->integrate = ((float)((rn + tn) / 2) >= s.integ_thr) ? 1 : 0;
   if (ts->integrate) {
+    fill_ztab(s, ts);
     for (int i = 0; i < 9; ++i) ts->lastR[i] = ts->R[i];
     for (int i = 0; i < 3; ++i) ts->lastT[i] = ts->t[i];
   }

@@ -40,13 +40,14 @@ __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* _
   const float c0 = s.cell[0], c1 = s.cell[1], c2 = s.cell[2];
   const float vgx = ((float)(vx - rx / 2) + 0.5f) * c0 - m.t[0];
   const float vgy = ((float)(vy - ry / 2) + 0.5f) * c1 - m.t[1];
-  float vgz = (0.5f) * c2 - m.t[2];
+  const float vgz0 = (0.5f) * c2 - m.t[2];
+  const float* __restrict__ zt_vgz = s.ztab;            // v_g_z after z additions
+  const float* __restrict__ zt_zs = s.ztab + rz + 1;    // z_scaled after z additions
   const float part = vgx * vgx + vgy * vgy;
   const float fx = s.cam.fx, fy = s.cam.fy, ccx = s.cam.cx, ccy = s.cam.cy;
-  float v_x = (Ri[0] * vgx + Ri[1] * vgy + Ri[2] * vgz) * fx;
-  float v_y = (Ri[3] * vgx + Ri[4] * vgy + Ri[5] * vgz) * fy;
-  const float v_z = (Ri[6] * vgx + Ri[7] * vgy + Ri[8] * vgz);
-  float zs = 0.f;
+  float v_x = (Ri[0] * vgx + Ri[1] * vgy + Ri[2] * vgz0) * fx;
+  float v_y = (Ri[3] * vgx + Ri[4] * vgy + Ri[5] * vgz0) * fy;
+  const float v_z = (Ri[6] * vgx + Ri[7] * vgy + Ri[8] * vgz0);
   const float trunc = s.trunc;
   const float tinv = 1.f / trunc;
   const float dx = Ri[2] * c2 * fx;
@@ -81,8 +82,8 @@ __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* _
       empty = true;
     } else {
       const double sr = sqrt(s2);
-      ge((double)vgz + sr, (double)c2);
-      ge(sr - (double)vgz, -(double)c2);
+      ge((double)vgz0 + sr, (double)c2);
+      ge(sr - (double)vgz0, -(double)c2);
     }
     if (empty || lo > hi) {
       kb = ke = z0;
@@ -92,9 +93,10 @@ __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* _
       if (ke < kb) ke = kb;
     }
   }
+  if (kb >= ke) return;  // nothing to update in this column chunk
+  // v_x and v_y depend on the column: replay their additions below the interval
+#pragma unroll 4
   for (int z = 0; z < kb; ++z) {
-    vgz += c2;
-    zs += c2;
     v_x += dx;
     v_y += dy;
   }
@@ -112,7 +114,9 @@ __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* _
     // plus trunc, no voxel of the chunk passes sdf >= -trunc.
     bool skip = false;
     {
-      const float k0 = (float)(zc - kb), k1 = (float)(zend - 1 - kb);
+      // v_x, v_y and the table entries all stand at slice zc here
+      const float k0 = 0.f, k1 = (float)(zend - 1 - zc);
+      const float zs = zt_zs[zc], vgz = zt_vgz[zc];
       const float za = v_z + r8 * (zs + k0 * c2), zb2 = v_z + r8 * (zs + k1 * c2);
       if (za > 1e-3f && zb2 > 1e-3f) {
         const float ua = (v_x + k0 * dx) / za + ccx, ub = (v_x + k1 * dx) / zb2 + ccx;
@@ -136,9 +140,8 @@ __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* _
       }
     }
     if (skip) {
+#pragma unroll 4
       for (int z = zc; z < zend; ++z) {
-        vgz += c2;
-        zs += c2;
         v_x += dx;
         v_y += dy;
       }
@@ -155,6 +158,7 @@ __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* _
         pix[u] = 0;
         sdf[u] = 0.f;
         if (zb + u < zend) {
+          const float zs = zt_zs[zb + u], vgz = zt_vgz[zb + u];
           const float inv_z = __frcp_rn(v_z + r8 * zs);
           if (!(inv_z < 0.f)) {
             const float px = roundf(v_x * inv_z + ccx);
@@ -170,8 +174,6 @@ __global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* _
               }
             }
           }
-          vgz += c2;
-          zs += c2;
           v_x += dx;
           v_y += dy;
         }

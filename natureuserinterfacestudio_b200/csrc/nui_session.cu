@@ -29,6 +29,7 @@ __global__ void k_pyramid(const SessionDesc*, int);
 __global__ void k_feedback(const SessionDesc*);
 __global__ void k_icp(const SessionDesc*, int, int);
 __global__ void k_track_finalize(const SessionDesc*);
+__global__ void k_ztab(const SessionDesc*);
 template <int F>
 __global__ void k_integrate(const SessionDesc*);
 template <int F>
@@ -139,6 +140,7 @@ struct nui_session {
   uchar4* cvol = nullptr;
   uint8_t* occ = nullptr;
   uint8_t* occ2 = nullptr;
+  float* ztab = nullptr;
   uint8_t* occ3 = nullptr;
   float* tile_max = nullptr;
   TrackState* ts = nullptr;
@@ -250,6 +252,7 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
   d.cvol = s->cvol;
   d.occ = s->occ;
   d.occ2 = s->occ2;
+  d.ztab = s->ztab;
   d.occ3 = s->occ3;
   d.max_cw = c.max_color_weight;
   d.zchunks = s->zchunks;
@@ -662,6 +665,7 @@ NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
   b += (size_t)((c->res[0] + 7) / 8) * ((c->res[1] + 7) / 8) * ((c->res[2] + 7) / 8);
   b += (size_t)((c->res[0] + 31) / 32) * ((c->res[1] + 31) / 32) * ((c->res[2] + 31) / 32);
   b += (size_t)((c->res[0] + 127) / 128) * ((c->res[1] + 127) / 128) * ((c->res[2] + 127) / 128);
+  b += 2 * ((size_t)c->res[2] + 1) * sizeof(float);
   return b;
 }
 
@@ -718,7 +722,8 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
     const size_t nbricks = (size_t)((c.res[0] + 7) / 8) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8);
     const size_t nsuper = (size_t)((c.res[0] + 31) / 32) * ((c.res[1] + 31) / 32) * ((c.res[2] + 31) / 32);
     const size_t nhyper = (size_t)((c.res[0] + 127) / 128) * ((c.res[1] + 127) / 128) * ((c.res[2] + 127) / 128);
-    if (ok) ok = alloc((void**)&s->occ, nbricks) && alloc((void**)&s->occ2, nsuper) && alloc((void**)&s->occ3, nhyper);
+    if (ok) ok = alloc((void**)&s->occ, nbricks) && alloc((void**)&s->occ2, nsuper) && alloc((void**)&s->occ3, nhyper) &&
+                 alloc((void**)&s->ztab, 2 * ((size_t)c.res[2] + 1) * sizeof(float));
     if (ok && c.color_volume) ok = alloc((void**)&s->cvol, nv * 4) && alloc((void**)&s->bgra, N * 4) && alloc((void**)&s->cmap, N * 4);
   }
   if (!ok) {
@@ -864,6 +869,7 @@ nui_status run_stage(nui_session* s, int what) {
     k_track_finalize<<<1, 32, 0, st>>>(dd);
     k_publish<<<1, 64, 0, st>>>(dd, 1, ctx->d_pose, ctx->d_status);
   } else if (what == 2) {
+    k_ztab<<<1, 32, 0, st>>>(dd);
     launch_integrate<0>(p, dd, st);
     launch_integrate<1>(p, dd, st);
     launch_integrate<2>(p, dd, st);
