@@ -93,6 +93,12 @@ typedef struct {
   int hash_excess;            /* excess (collision) list length */
   int hash_pool_blocks;       /* 8^3 voxel blocks in the pool */
   int hash_max_weight;        /* m_integrationWeightMax */
+  /* colour tracking: weight of the photometric normal equations (the rows of
+   * color_icp_block_kernel, colorIcp.cl:91-183, against the previous frame's colours at
+   * the previous raycast's points) added to the point-to-plane ones in every ICP iteration
+   * of the finest level; 0 = depth only.  Needs color_volume = 1 and BGRA frames whose
+   * valid pixels have alpha 255.  Colours and gradients enter in units of 1/255. */
+  float photometric_weight;
 } nui_session_cfg;
 
 typedef struct nui_ctx nui_ctx;
@@ -183,7 +189,9 @@ NUI_API nui_status nui_mesh_cases(nui_session* s, uint8_t* cases, size_t bytes, 
  *   2 vertex map level `level` (f32x4)  3 reference vertex map (f32x4, W*H, world)
  *   4 reference normal map (f32x4)       5 volume in the reference layout, short2
  *   6 raw volume storage of the session format   7 depth level `level` (f32)
- *   8 reference colour map (u8x4)        9 colour volume, reference layout (u8x4)  */
+ *   8 reference colour map (u8x4)        9 colour volume, reference layout (u8x4)
+ *  10 model colours of colour tracking: the previous frame's (u8x4)
+ *  11 / 12 x / y colour gradients of the current frame (u8x4, signed bytes; level 0) */
 NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void* host, size_t bytes);
 /* Voxel-hash sessions: what = 20 entries (16 B each: short pos[3], pad, int ptr, uint
  * offset), 21 visible list (int, count = nui_hash_stats visible), 22 pool voxels in the

@@ -41,6 +41,7 @@ class SessionCfg(C.Structure):
         ("integration_threshold", C.c_float),
         ("voxel_size", C.c_float), ("trunc_scale", C.c_float), ("hash_buckets", C.c_int),
         ("hash_excess", C.c_int), ("hash_pool_blocks", C.c_int), ("hash_max_weight", C.c_int),
+                ("photometric_weight", C.c_float),
     ]
 
 
@@ -276,7 +277,8 @@ class Session:
         shapes = {0: ((H, W), np.float32), 1: ((H, W), np.float32), 2: ((H, W, 4), np.float32),
                   3: ((self.H, self.W, 4), np.float32), 4: ((self.H, self.W, 4), np.float32),
                   5: ((nv, 2), np.int16), 7: ((H, W), np.float32), 8: ((self.H, self.W, 4), np.uint8),
-                  9: ((nv, 4), np.uint8)}
+                  9: ((nv, 4), np.uint8), 10: ((self.H, self.W, 4), np.uint8), 11: ((H, W, 4), np.uint8),
+                  12: ((H, W, 4), np.uint8)}
         shape, dt = shapes[what]
         out = np.zeros(shape, dt)
         check(lib().nui_debug_download(self.h, what, level, ptr(out), out.nbytes))

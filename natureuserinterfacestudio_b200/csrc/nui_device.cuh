@@ -85,6 +85,14 @@ struct SessionDesc {
   int max_cw;
   int zchunks;                    // integration: z chunks per column (one thread each)
   float* ztab;                    // integration: running sums shared by all columns, 2 (rz + 1)
+  // colour tracking: weight of the photometric term (0: depth only); the previous frame's
+  // colours (the model colours of the reference maps); the frame's colour pyramid (level 0
+  // is bgra) and its x / y gradients per level (signed bytes)
+  float photo_w;
+  uchar4* cprev;
+  uchar4* cpyr[kMaxLevels];
+  uchar4* cgx[kMaxLevels];
+  uchar4* cgy[kMaxLevels];
   // tracking state and ICP scratch
   TrackState* ts;
   float2* partials;               // per-block (hi, lo) sums, kIcpTerms per block

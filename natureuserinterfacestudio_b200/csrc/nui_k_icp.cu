@@ -48,6 +48,65 @@ __device__ __forceinline__ float3 bilinear_holes(const float4* __restrict__ src,
   return r;
 }
 
+// ---------------------------------------------------------------- photometric rows
+// One model point of the colour tracker's term (color_icp_block_kernel, colorIcp.cl:
+// 119-178, in the tracker's convention), at the finest level: the world point m of the
+// previous raycast, whose colour is the previous frame's at the same pixel (the raycast
+// is rendered from the previous pose), is taken to the current camera by the running
+// estimate, p = R^T (m - t), projected and rounded to a pixel of the current colour
+// image; the residual is the colour difference (units of 1/255) and its derivative in
+// each ICP parameter x_k is  grad(I) . d(proj)/dp . dp/dx_k  with dp/dx_k = R^T (e_k x m)
+// for the rotations and -R^T e_k for the translations (the depth ICP's update
+// R <- Rinc^-1 R, t <- Rinc^-1 t + tinc).  Colours count with alpha 255.  c receives the
+// upper triangle of [D | -diff]^T [D | -diff] by rows (21 + 6), |diff|^2 and 1.
+__device__ __forceinline__ bool color_row(const SessionDesc& s, int i, const float* R, const float3 t, float* c) {
+  const float3 m = xyz(__ldg(s.vref + i));
+  if (isnan3(m)) return false;
+  const uchar4 mc = __ldg(s.cprev + i);
+  if (mc.w != 255) return false;
+  const float3 d = sub3(m, t);
+  const float3 c0 = f3(R[0], R[3], R[6]), c1 = f3(R[1], R[4], R[7]), c2 = f3(R[2], R[5], R[8]);
+  const float3 p = f3(dot3(c0, d), dot3(c1, d), dot3(c2, d));
+  const float fx = s.cam.fx, fy = s.cam.fy, cx = s.cam.cx, cy = s.cam.cy;
+  const int lw = s.W, lh = s.H;
+  const int u = (int)roundf(p.x * fx / p.z + cx), v = (int)roundf(p.y * fy / p.z + cy);
+  if (!(u >= 0 && u < lw && v >= 0 && v < lh)) return false;
+  const int li = v * lw + u;
+  const uchar4 co = __ldg(reinterpret_cast<const uchar4*>(s.bgra) + li);
+  const uchar4 gx = __ldg(s.cgx[0] + li), gy = __ldg(s.cgy[0] + li);
+  if (co.w != 255 || gx.w != 255 || gy.w != 255) return false;
+  const float k255 = 1.0f / 255.0f;
+  const float3 diff = mul3(f3((float)co.x - (float)mc.x, (float)co.y - (float)mc.y, (float)co.z - (float)mc.z), k255);
+  const float3 g1 = mul3(f3((float)(signed char)gx.x, (float)(signed char)gx.y, (float)(signed char)gx.z), k255);
+  const float3 g2 = mul3(f3((float)(signed char)gy.x, (float)(signed char)gy.y, (float)(signed char)gy.z), k255);
+  float3 D[6];
+  const float zz = p.z * p.z;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const float3 w = k == 0 ? f3(0.f, -m.z, m.y)
+                   : k == 1 ? f3(m.z, 0.f, -m.x)
+                   : k == 2 ? f3(-m.y, m.x, 0.f)
+                   : k == 3 ? f3(-1.f, 0.f, 0.f)
+                   : k == 4 ? f3(0.f, -1.f, 0.f)
+                            : f3(0.f, 0.f, -1.f);
+    const float3 dp = f3(dot3(c0, w), dot3(c1, w), dot3(c2, w));
+    const float jx = fx * ((p.z * dp.x - dp.z * p.x) / zz);
+    const float jy = fy * ((p.z * dp.y - dp.z * p.y) / zz);
+    D[k] = f3(jx * g1.x + jy * g2.x, jx * g1.y + jy * g2.y, jx * g1.z + jy * g2.z);
+  }
+  const float3 nd = f3(-diff.x, -diff.y, -diff.z);
+  int sh = 0;
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
+#pragma unroll
+    for (int b = a; b < 6; ++b) c[sh++] = dot3(D[a], D[b]);
+    c[sh++] = dot3(D[a], nd);
+  }
+  c[27] = dot3(diff, diff);
+  c[28] = 1.0f;
+  return true;
+}
+
 // ---------------------------------------------------------------- FP64 host step
 __device__ double det6(double* A) {
   double det = 1.0;
@@ -202,7 +261,11 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
   const int w = s.W >> level, h = s.H >> level, n = w * h;
   const int per_block = kIcpThreads * kIcpPixPerThread;
   const int nblocks = (n + per_block - 1) / per_block;
-  if ((int)blockIdx.x >= nblocks) return;
+  // colour tracking: at the finest level, blocks past the depth ones take the photometric
+  // term over the full-size model maps
+  const bool photo = s.photo_w > 0.f && level == 0;
+  const int ncb = photo ? (s.W * s.H + per_block - 1) / per_block : 0;
+  if ((int)blockIdx.x >= nblocks + ncb) return;
 
   __shared__ float sR[9], st[3];
   __shared__ DevXform sp;
@@ -220,9 +283,27 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
   const int RW = s.W, RN = s.W * s.H;
   const float fW = (float)s.W, fH = (float)s.H;
   const float3 tc = f3(st[0], st[1], st[2]), tp = f3(sp.t[0], sp.t[1], sp.t[2]);
+  if ((int)blockIdx.x >= nblocks) {
+    const int cbase = ((int)blockIdx.x - nblocks) * per_block, NM = s.W * s.H;
+#pragma unroll 1
+    for (int k = 0; k < kIcpPixPerThread; ++k) {
+      const int i = cbase + k * kIcpThreads + threadIdx.x;
+      if (i >= NM) break;
+      float c[kIcpTerms];
+      if (!color_row(s, i, sR, tc, c)) continue;
+#pragma unroll
+      for (int q = 0; q < kIcpTerms - 1; ++q) {
+        float ss, e;
+        two_sum(hi[q], c[q], ss, e);
+        hi[q] = ss;
+        lo[q] += e;
+      }
+      hi[28] += 1.0f;
+    }
+  }
   const int base = blockIdx.x * per_block;
 #pragma unroll 1
-  for (int k = 0; k < kIcpPixPerThread; ++k) {
+  for (int k = 0; k < kIcpPixPerThread && (int)blockIdx.x < nblocks; ++k) {
     const int i = base + k * kIcpThreads + threadIdx.x;
     if (i >= n) break;
     const float3 v = xyz(__ldg(V + i));
@@ -288,29 +369,37 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
   __syncthreads();
   if (threadIdx.x == 0) ticket = atomicAdd(&ts->block_counter, 1u);
   __syncthreads();
-  if (ticket != (unsigned)nblocks - 1) return;
+  if (ticket != (unsigned)(nblocks + ncb) - 1) return;
 
-  // last block: fixed-order double reduction of the per-block pairs
+  // last block: fixed-order double reduction of the per-block pairs, the depth blocks
+  // and the photometric blocks separately
   __threadfence();
   __shared__ double red[kWarps][32];
-  {
-    const int k = lane;  // term index handled by this lane
-    double acc = 0.0;
-    if (k < kIcpTerms)
-      for (int b = warp; b < nblocks; b += kWarps) {
-        float2 p = __ldcg(&s.partials[(size_t)b * kIcpTerms + k]);
-        acc += (double)p.x + (double)p.y;
-      }
-    red[warp][lane] = acc;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double sums[kIcpTerms];
-    for (int k = 0; k < kIcpTerms; ++k) {
-      double a = 0.0;
-      for (int wi = 0; wi < kWarps; ++wi) a += red[wi][k];
-      sums[k] = a;
+  __shared__ double sums[kIcpTerms];
+  for (int part = 0; part < (photo ? 2 : 1); ++part) {
+    const int b0 = part == 0 ? 0 : nblocks, b1 = part == 0 ? nblocks : nblocks + ncb;
+    {
+      const int k = lane;  // term index handled by this lane
+      double acc = 0.0;
+      if (k < kIcpTerms)
+        for (int b = b0 + warp; b < b1; b += kWarps) {
+          float2 p = __ldcg(&s.partials[(size_t)b * kIcpTerms + k]);
+          acc += (double)p.x + (double)p.y;
+        }
+      red[warp][lane] = acc;
     }
+    __syncthreads();
+    if (threadIdx.x < kIcpTerms) {
+      double a = 0.0;
+      for (int wi = 0; wi < kWarps; ++wi) a += red[wi][threadIdx.x];
+      // the photometric normal equations and residual enter weighted; the count stays
+      // the depth count
+      if (part == 0) sums[threadIdx.x] = a;
+      else if (threadIdx.x < kIcpTerms - 1) sums[threadIdx.x] += (double)s.photo_w * a;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
     icp_host_step(ts, sums, iter, s.icp_min_count[level]);
     ts->block_counter = 0;
     __threadfence();

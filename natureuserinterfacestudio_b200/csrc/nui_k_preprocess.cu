@@ -163,7 +163,11 @@ __global__ void k_feedback(const SessionDesc* __restrict__ descs) {
   const float3 vw = add3(rot_rows(m.R, c), f3(m.t[0], m.t[1], m.t[2]));
   s.vref[idx] = w0(vw);
   s.nref[idx] = isnan3(n) ? make_float4(qnan(), qnan(), qnan(), 0.f) : w0(rot_rows(m.R, n));
-  if (s.cmap) s.cmap[idx] = s.bgra ? reinterpret_cast<const uchar4*>(s.bgra)[idx] : make_uchar4(0, 0, 0, 0);
+  if (s.cmap) {  // model colours of the first frame: the frame's (R, G, B order in hash scenes)
+    uchar4 cc = s.bgra ? reinterpret_cast<const uchar4*>(s.bgra)[idx] : make_uchar4(0, 0, 0, 0);
+    if (s.hash) cc = make_uchar4(cc.z, cc.y, cc.x, cc.w);
+    s.cmap[idx] = cc;
+  }
 }
 
 }  // namespace nui

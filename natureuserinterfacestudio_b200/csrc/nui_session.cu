@@ -30,6 +30,9 @@ __global__ void k_feedback(const SessionDesc*);
 __global__ void k_icp(const SessionDesc*, int, int);
 __global__ void k_track_finalize(const SessionDesc*);
 __global__ void k_ztab(const SessionDesc*);
+__global__ void k_color_level(const SessionDesc*, int);
+__global__ void k_color_grad(const SessionDesc*);
+__global__ void k_color_keep(const SessionDesc*);
 template <int F>
 __global__ void k_integrate(const SessionDesc*);
 template <int F>
@@ -96,6 +99,7 @@ struct BatchPlan {
   long maxHashBlk;          // scan blocks of 1024 entries
   int hashMask;             // bit per hash sdf format
   int fmtMask;
+  int colorIcp;             // some session tracks with the photometric term
   BatchPlan() { std::memset(this, 0, sizeof(*this)); }
   bool operator<(const BatchPlan& o) const { return std::memcmp(this, &o, sizeof(BatchPlan)) < 0; }
 };
@@ -145,6 +149,9 @@ struct nui_session {
   float* tile_max = nullptr;
   TrackState* ts = nullptr;
   float2* partials = nullptr;
+  uchar4* cprev = nullptr;        // colour tracking: the previous frame's colours and the
+  uchar4* cgx[kMaxLevels] = {};   // current frame's gradients (level 0)
+  uchar4* cgy[kMaxLevels] = {};
   SessionDesc* d_desc1 = nullptr;
   // voxel-block hash
   bool hash = false;
@@ -194,6 +201,9 @@ bool cfg_valid(const nui_session_cfg* c, std::string& why) {
   }
   if (c->filter_radius < 0 || c->filter_radius > kMaxRadius) return why = "filter radius must be 0..7", false;
   if (!(c->fx > 0.f) || !(c->fy > 0.f)) return why = "focal lengths must be positive", false;
+  if (!(c->photometric_weight >= 0.f) || !(c->photometric_weight < 1e30f))
+    return why = "photometric weight must be finite and >= 0", false;
+  if (c->photometric_weight > 0.f && !c->color_volume) return why = "colour tracking needs color_volume = 1", false;
   return true;
 }
 
@@ -258,6 +268,14 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
   d.zchunks = s->zchunks;
   d.ts = s->ts;
   d.partials = s->partials;
+  // colour tracking runs on frames that carry colour, once its buffers exist
+  d.photo_w = (bgra && s->cgx[0] && s->cprev) ? s->cfg.photometric_weight : 0.f;
+  d.cprev = s->cprev;
+  for (int l = 0; l < kMaxLevels; ++l) {
+    d.cpyr[l] = nullptr;
+    d.cgx[l] = s->cgx[l];
+    d.cgy[l] = s->cgy[l];
+  }
   if (s->hash) {
     d.fmt = -1;  // dense kernels skip hash sessions
     d.hash = 1;
@@ -291,6 +309,7 @@ void plan_add(BatchPlan& p, const nui_session* s) {
   p.maxW = std::max(p.maxW, c.width);
   p.maxH = std::max(p.maxH, c.height);
   p.maxLevels = std::max(p.maxLevels, c.levels);
+  if (c.photometric_weight > 0.f) p.colorIcp = 1;
   for (int l = 0; l < c.levels; ++l) p.maxIters[l] = std::max(p.maxIters[l], c.iterations[l]);
   if (s->hash) {
     p.hashMask |= 1 << (c.tsdf_format == NUI_TSDF_I16 ? 0 : 1);
@@ -367,6 +386,20 @@ void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t 
   if (p.hashMask & 2) k_hash_raycast<1><<<dim3(pix, p.n), 128, 0, st>>>(d);
 }
 
+// Colour pyramid (if any session tracks with colour), the ICP iterations of every level,
+// the integration gate and the published pose.
+void launch_track(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, float* d_pose, int* d_status) {
+  const unsigned npix = cdiv((long)p.maxW * p.maxH, 256);
+  if (p.colorIcp) k_color_grad<<<dim3(npix, p.n, 1), 256, 0, st>>>(d);  // finest level
+  for (int l = p.maxLevels - 1; l >= 0; --l) {
+    const unsigned nb = cdiv((long)(p.maxW >> l) * (p.maxH >> l), 1024) + (l == 0 && p.colorIcp ? npix / 4 + 1 : 0);
+    for (int it = 0; it < p.maxIters[l]; ++it) k_icp<<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
+  }
+  k_track_finalize<<<p.n, 32, 0, st>>>(d);
+  k_publish<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n, d_pose, d_status);
+  if (p.colorIcp) k_color_keep<<<dim3(npix, p.n), 256, 0, st>>>(d);
+}
+
 // The launch schedule of one tick.  ev: optional stage events (timing only).
 void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float* d_pose, int* d_status, bool ev) {
   cudaStream_t st = ctx->stream;
@@ -382,12 +415,7 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
     k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), p.n), 256, 0, st>>>(d, l);
   k_feedback<<<dim3(cdiv((long)p.maxW * p.maxH, 256), p.n), 256, 0, st>>>(d);
   mark(2);
-  for (int l = p.maxLevels - 1; l >= 0; --l) {
-    const unsigned nb = cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256 * 4);
-    for (int it = 0; it < p.maxIters[l]; ++it) k_icp<<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
-  }
-  k_track_finalize<<<p.n, 32, 0, st>>>(d);
-  k_publish<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n, d_pose, d_status);
+  launch_track(p, d, st, d_pose, d_status);
   mark(3);
   launch_integrate<0>(p, d, st);
   launch_integrate<1>(p, d, st);
@@ -521,6 +549,8 @@ nui_status reset_session(nui_session* s) {
       case 3: launch_init<3>(s); break;
     }
   }
+  if (s->cprev)
+    NUI_CUDA(cudaMemsetAsync(s->cprev, 0, (size_t)s->cfg.width * s->cfg.height * 4, s->ctx->stream));
   TrackState t;
   std::memset(&t, 0, sizeof(t));
   const float I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
@@ -701,7 +731,7 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
   s->hash = c.volume_kind == NUI_VOLUME_HASH;
   bool ok = alloc((void**)&s->raw, N * 2) && alloc((void**)&s->dscaled, N * 4) && alloc((void**)&s->vref, N * 16) &&
             alloc((void**)&s->nref, N * 16) && alloc((void**)&s->ts, sizeof(TrackState)) &&
-            alloc((void**)&s->partials, ((N + 1023) / 1024) * kIcpTerms * sizeof(float2)) &&
+            alloc((void**)&s->partials, ((N + 1023) / 1024) * kIcpTerms * sizeof(float2) * (c.photometric_weight > 0.f ? 2 : 1)) &&
             alloc((void**)&s->d_desc1, sizeof(SessionDesc));
   for (int l = 0; ok && l < c.levels; ++l)
     ok = alloc((void**)&s->dlev[l], (N >> (2 * l)) * 4) && alloc((void**)&s->vlev[l], (N >> (2 * l)) * 16);
@@ -726,6 +756,8 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
                  alloc((void**)&s->ztab, 2 * ((size_t)c.res[2] + 1) * sizeof(float));
     if (ok && c.color_volume) ok = alloc((void**)&s->cvol, nv * 4) && alloc((void**)&s->bgra, N * 4) && alloc((void**)&s->cmap, N * 4);
   }
+  if (ok && c.photometric_weight > 0.f)
+    ok = alloc((void**)&s->cprev, N * 4) && alloc((void**)&s->cgx[0], N * 4) && alloc((void**)&s->cgy[0], N * 4);
   if (!ok) {
     for (void* p : s->allocs) cudaFree(p);
     delete s;
@@ -769,7 +801,7 @@ NUI_API nui_status nui_process_frame(nui_session* s, const uint16_t* depth, cons
 NUI_API nui_status nui_process_frame_device(nui_session* s, const uint16_t* d_depth, const uint8_t* d_bgra, float* pose) {
   if (!s || !d_depth) return fail(NUI_ERR_INVALID_ARG, "null argument");
   nui_session* arr[1] = {s};
-  const uint8_t* b = (d_bgra && s->cvol) ? d_bgra : nullptr;
+  const uint8_t* b = (d_bgra && s->cmap) ? d_bgra : nullptr;
   nui_status per;
   return run_tick(s->ctx, arr, 1, &d_depth, &b, false, &per, pose);
 }
@@ -795,7 +827,7 @@ NUI_API nui_status nui_batch_tick_device(nui_ctx* ctx, nui_session* const* ss, i
   std::vector<const uint8_t*> b(n, nullptr);
   for (int i = 0; i < n; ++i) {
     if (!ss[i] || ss[i]->ctx != ctx || !d_depths[i]) return fail(NUI_ERR_INVALID_ARG, "bad session or frame");
-    if (d_bgras && d_bgras[i] && ss[i]->cvol) b[i] = d_bgras[i];
+    if (d_bgras && d_bgras[i] && ss[i]->cmap) b[i] = d_bgras[i];
   }
   return run_tick(ctx, ss, n, d_depths, b.data(), true, per, poses);
 }
@@ -862,12 +894,7 @@ nui_status run_stage(nui_session* s, int what) {
     for (int l = 1; l < p.maxLevels; ++l)
       k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), 1), 256, 0, st>>>(dd, l);
   } else if (what == 1) {
-    for (int l = p.maxLevels - 1; l >= 0; --l) {
-      const unsigned nb = cdiv((long)(p.maxW >> l) * (p.maxH >> l), 1024);
-      for (int it = 0; it < p.maxIters[l]; ++it) k_icp<<<dim3(nb, 1), 256, 0, st>>>(dd, l, it);
-    }
-    k_track_finalize<<<1, 32, 0, st>>>(dd);
-    k_publish<<<1, 64, 0, st>>>(dd, 1, ctx->d_pose, ctx->d_status);
+    launch_track(p, dd, st, ctx->d_pose, ctx->d_status);
   } else if (what == 2) {
     k_ztab<<<1, 32, 0, st>>>(dd);
     launch_integrate<0>(p, dd, st);
@@ -884,6 +911,7 @@ nui_status run_stage(nui_session* s, int what) {
     launch_hash_raycast(p, dd, st);
   } else if (what == 4) {
     k_feedback<<<dim3(cdiv((long)p.maxW * p.maxH, 256), 1), 256, 0, st>>>(dd);
+    if (p.colorIcp) k_color_keep<<<dim3(cdiv((long)p.maxW * p.maxH, 256), 1), 256, 0, st>>>(dd);
   }
   NUI_CUDA(cudaGetLastError());
   NUI_CUDA(cudaStreamSynchronize(st));
@@ -968,6 +996,9 @@ NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void*
     case 6: src = s->vol; need = nv * (c.tsdf_format == 2 ? 2 : voxel_bytes(c.tsdf_format)); break;
     case 7: src = s->dlev[level]; need = Nl * 4; break;
     case 8: src = s->cmap; need = N * 4; break;
+    case 10: src = s->cprev; need = N * 4; break;
+    case 11: src = s->cgx[level]; need = Nl * 4; break;
+    case 12: src = s->cgy[level]; need = Nl * 4; break;
     case 20: src = s->entries; need = ((size_t)c.hash_buckets + c.hash_excess) * 16; break;
     case 21: {
       int cnt[4];

@@ -40,6 +40,7 @@ UNITS = {
     "raycast.cl": "launch_raycast.inc",
     "marchingCube.cl": "launch_mc.inc",
     "icp.cl": "launch_icp.inc",
+    "colorIcp.cl": "launch_color_icp.inc",
     "KinfuHashScene.cl": "launch_hash_scene.inc",
     "KinfuHashRaycast.cl": "launch_hash_raycast.inc",
     "KinfuHashVisualization.cl": "launch_hash_mesh.inc",

@@ -548,6 +548,187 @@ ORC_API void orc_icp_rows(const float* vcur, int w, int h, const float* vref, co
 }
 
 // ---------------------------------------------------------------------------------
+// A8  colour ICP.
+//
+// Colour pyramid   half_sample_bgra_kernel  transformMaps.cl:106-146, radius 1 from the host
+// (NuiKinfuOpenCLColorTracker.cpp:159-191): pixel (x, y) of the dW x dH level is the integer
+// mean (truncated) of every channel over the taps of the (2r+1)^2 window around (2x, 2y) of
+// the level below, clamped to that image; alpha 255.
+ORC_API void orc_color_half_sample(const uint8_t* src, int dW, int dH, int radius, uint8_t* dst) {
+  const int sW = dW * 2, sH = dH * 2;
+#pragma omp parallel for schedule(static)
+  for (int y = 0; y < dH; ++y)
+    for (int x = 0; x < dW; ++x) {
+      const int sx = 2 * x, sy = 2 * y;
+      const int x0 = std::max(sx - radius, 0), x1 = std::min(sx + radius + 1, sW);
+      const int y0 = std::max(sy - radius, 0), y1 = std::min(sy + radius + 1, sH);
+      int sum[4] = {0, 0, 0, 0}, n = 0;
+      for (int cy = y0; cy < y1; ++cy)
+        for (int cx = x0; cx < x1; ++cx) {
+          for (int k = 0; k < 4; ++k) sum[k] += src[4 * ((long)cy * sW + cx) + k];
+          ++n;
+        }
+      uint8_t* o = dst + 4 * ((long)y * dW + x);
+      for (int k = 0; k < 3; ++k) o[k] = (uint8_t)(n > 0 ? sum[k] / n : 0);
+      o[3] = 255;
+    }
+}
+
+// BGRA gradients   bgra_gradient_kernel  transformMaps.cl:514-560: Sobel / 8 of each colour
+// channel in float, stored as convert_uchar (the low byte of the truncation toward zero:
+// a negative gradient wraps, and since |Sobel / 8| <= 127.5 reading the byte as a signed
+// char gives the truncated gradient back); alpha 255; border pixels (0, 0, 0, 0).
+// The reference steps to the rows above and below by the image height and stores one row
+// and one pixel past the centre, which agree with the centre-stored Sobel only on square
+// images and off by (1, 1); here rows are stepped by the width and stored at the centre.
+ORC_API void orc_color_gradient(const uint8_t* c, int W, int H, uint8_t* gx, uint8_t* gy) {
+#pragma omp parallel for schedule(static)
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      const long i = (long)y * W + x;
+      if (!(x > 0 && x < W - 1 && y > 0 && y < H - 1)) {
+        for (int k = 0; k < 4; ++k) gx[4 * i + k] = gy[4 * i + k] = 0;
+        continue;
+      }
+      auto px = [&](int dx, int dy, int k) { return (float)c[4 * (i + dx + (long)dy * W) + k]; };
+      for (int k = 0; k < 3; ++k) {
+        float tx = (px(1, -1, k) - px(-1, -1, k)) + 2 * (px(1, 0, k) - px(-1, 0, k)) + (px(1, 1, k) - px(-1, 1, k));
+        float ty = (px(-1, 1, k) - px(-1, -1, k)) + 2 * (px(0, 1, k) - px(0, -1, k)) + (px(1, 1, k) - px(1, -1, k));
+        tx /= 8.0f;
+        ty /= 8.0f;
+        gx[4 * i + k] = (uint8_t)(int)tx;
+        gy[4 * i + k] = (uint8_t)(int)ty;
+      }
+      gx[4 * i + 3] = gy[4 * i + 3] = 255;
+    }
+}
+
+// Photometric rows   color_icp_block_kernel  colorIcp.cl:91-183, per model point i of the
+// full-size model maps (world vertices mv, colours mc: the previous raycast), against the
+// level-`level` colour image of the current frame and its gradients.
+//
+// ref_mode = 1 evaluates the kernel as written, for pinning: the point is moved by (R, t)
+// as given, parameters are ordered (tx, ty, tz, rx, ry, rz) with rotations about the
+// camera axes, gradients are read as unsigned bytes, colours unscaled, both colours must
+// have alpha 255, and the 29 outputs are packed as the kernel packs them (per parameter
+// p: d_p.d_q for q <= p, then d_p.diff; then |diff|, 1).
+//
+// ref_mode = 0 is the tracker's form: (R, t) is the camera-to-world estimate, so the
+// point's camera coordinates are R^T (m - t); the parameters are those of the depth ICP
+// step ((alpha, beta, gamma, tx, ty, tz) of R <- Rinc^-1 R, t <- Rinc^-1 t + tinc), whose
+// derivatives of the camera point are R^T (e_k x m) and -R^T e_k; gradients are signed
+// bytes; colours and gradients are scaled by 1/255; outputs are packed like the depth
+// rows: the upper triangle of [D | -diff]^T [D | -diff] by rows (21 + 6), then |diff|^2
+// and 1.  In both modes a model colour counts when its alpha is 255.
+ORC_API void orc_color_rows(const float* mv, const uint8_t* mc, const OrcCam* cam, int level,
+                            const uint8_t* pc, const uint8_t* pgx, const uint8_t* pgy, const float* R,
+                            const float* t, int ref_mode, float* rows, double* sums) {
+  const int W = (int)cam->W, H = (int)cam->H;
+  const long n = (long)W * H;
+  const int div = 1 << level;
+  const float fx = cam->fx / (float)div, fy = cam->fy / (float)div;
+  const float cx = cam->cx / (float)div, cy = cam->cy / (float)div;
+  const int lw = W / div, lh = H / div;
+  const long CH = 4096;
+  const long nch = (n + CH - 1) / CH;
+  std::vector<double> part((size_t)std::max(nch, 1L) * 29, 0.0);
+  const float k255 = 1.0f / 255.0f;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long ch = 0; ch < nch; ++ch) {
+    double* acc = part.data() + 29 * (size_t)ch;
+    for (long i = ch * CH; i < std::min(n, (ch + 1) * CH); ++i) {
+      float cr[29];
+      for (int k = 0; k < 29; ++k) cr[k] = 0.f;
+      bool ok = false;
+      const f3 m = ld3(mv, i);
+      const uint8_t* kc = mc + 4 * i;
+      if (!isnan3(m) && kc[3] == 255) {
+        f3 p;
+        if (ref_mode) {
+          p = mk(dot3(mk(R[0], R[1], R[2]), m), dot3(mk(R[3], R[4], R[5]), m), dot3(mk(R[6], R[7], R[8]), m)) +
+              mk(t[0], t[1], t[2]);
+        } else {
+          const f3 d = m - mk(t[0], t[1], t[2]);
+          p = mk(dot3(mk(R[0], R[3], R[6]), d), dot3(mk(R[1], R[4], R[7]), d), dot3(mk(R[2], R[5], R[8]), d));
+        }
+        const int u = (int)std::round(p.x * fx / p.z + cx), v = (int)std::round(p.y * fy / p.z + cy);
+        if (u >= 0 && u < lw && v >= 0 && v < lh) {
+          const long li = (long)v * lw + u;
+          const uint8_t *co = pc + 4 * li, *gx = pgx + 4 * li, *gy = pgy + 4 * li;
+          if (co[3] == 255 && gx[3] == 255 && gy[3] == 255) {
+            f3 diff = mk((float)co[0] - (float)kc[0], (float)co[1] - (float)kc[1], (float)co[2] - (float)kc[2]);
+            f3 g1, g2;
+            if (ref_mode) {
+              g1 = mk((float)gx[0], (float)gx[1], (float)gx[2]);
+              g2 = mk((float)gy[0], (float)gy[1], (float)gy[2]);
+            } else {
+              diff = diff * k255;
+              g1 = mk((float)(int8_t)gx[0], (float)(int8_t)gx[1], (float)(int8_t)gx[2]) * k255;
+              g2 = mk((float)(int8_t)gy[0], (float)(int8_t)gy[1], (float)(int8_t)gy[2]) * k255;
+            }
+            f3 d[6];
+            for (int k = 0; k < 6; ++k) {
+              f3 dp;
+              if (ref_mode) {
+                switch (k) {
+                  case 0: dp = mk(1.f, 0.f, 0.f); break;
+                  case 1: dp = mk(0.f, 1.f, 0.f); break;
+                  case 2: dp = mk(0.f, 0.f, 1.f); break;
+                  case 3: dp = mk(0.f, -p.z, p.y); break;
+                  case 4: dp = mk(p.z, 0.f, -p.x); break;
+                  default: dp = mk(-p.y, p.x, 0.f); break;
+                }
+              } else {
+                f3 w;  // e_k x m (rotations) or -e_k (translations), then R^T
+                switch (k) {
+                  case 0: w = mk(0.f, -m.z, m.y); break;
+                  case 1: w = mk(m.z, 0.f, -m.x); break;
+                  case 2: w = mk(-m.y, m.x, 0.f); break;
+                  case 3: w = mk(-1.f, 0.f, 0.f); break;
+                  case 4: w = mk(0.f, -1.f, 0.f); break;
+                  default: w = mk(0.f, 0.f, -1.f); break;
+                }
+                dp = mk(dot3(mk(R[0], R[3], R[6]), w), dot3(mk(R[1], R[4], R[7]), w), dot3(mk(R[2], R[5], R[8]), w));
+              }
+              const float zz = p.z * p.z;
+              const float jx = fx * ((p.z * dp.x - dp.z * p.x) / zz);
+              const float jy = fy * ((p.z * dp.y - dp.z * p.y) / zz);
+              d[k] = mk(jx * g1.x + jy * g2.x, jx * g1.y + jy * g2.y, jx * g1.z + jy * g2.z);
+            }
+            int s = 0;
+            if (ref_mode) {
+              for (int a = 0; a < 6; ++a) {
+                for (int b = 0; b <= a; ++b) cr[s++] = dot3(d[a], d[b]);
+                cr[s++] = dot3(d[a], diff);
+              }
+              cr[s++] = length3(diff);
+            } else {
+              const f3 nd = mk(-diff.x, -diff.y, -diff.z);
+              for (int a = 0; a < 6; ++a) {
+                for (int b = a; b < 6; ++b) cr[s++] = dot3(d[a], d[b]);
+                cr[s++] = dot3(d[a], nd);
+              }
+              cr[s++] = dot3(diff, diff);
+            }
+            cr[s++] = 1.0f;
+            ok = true;
+          }
+        }
+      }
+      if (rows)
+        for (int k = 0; k < 29; ++k) rows[29 * i + k] = cr[k];
+      if (ok)
+        for (int k = 0; k < 29; ++k) acc[k] += (double)cr[k];
+    }
+  }
+  for (int k = 0; k < 29; ++k) {
+    double s = 0.0;
+    for (long c = 0; c < nch; ++c) s += part[29 * (size_t)c + k];
+    sums[k] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------------
 // Small dense linear algebra for the ICP host step (Eigen in the reference; Eigen is not
 // vendored, so these are textbook restatements: partial-pivot LU determinant and
 // Cholesky LL^T solve, both in double).
@@ -646,12 +827,29 @@ struct OrcIcpStats {
   int status;  // 0 ok, 1 singular (tracking lost)
 };
 
+// Photometric term of the colour tracker (A8), used at the finest level: the world
+// vertices of the previous raycast with the previous frame's colours (the raycast is
+// rendered from the previous pose, so pixel i of both holds the same surface point), and
+// the current frame's colour image and gradients; weight on its normal equations.
+struct OrcColorIcp {
+  const float* mv;      // model world vertices (W x H float3)
+  const uint8_t* mc;    // model colours: the previous frame (W x H BGRA)
+  const uint8_t* pyr;   // current frame (W x H BGRA)
+  const uint8_t* gx;    // its x / y gradients (signed bytes)
+  const uint8_t* gy;
+  float weight;
+};
+
 // A7 host loop   NuiKinfuOpenCLDepthTracker.cpp:240-504.
 // vlevels[l] is the level-l vertex map ((W>>l) x (H>>l)); iters[l] its iteration count.
 // R/t: in = initial estimate, out = estimate.  Returns 0 on success, 1 on singular system.
+// With `col` (nullable, weight > 0) every iteration of the finest level adds the
+// photometric normal equations of orc_color_rows times the weight to the point-to-plane
+// ones, and the weighted |diff|^2 sum to the residual sum; the accept/reject count stays
+// the depth count.
 ORC_API int orc_icp(const float* const* vlevels, const int* iters, int levels, const float* vref,
                     const float* nref, const OrcCam* cam, const OrcXform* prev, float dist_thr,
-                    float* R, float* t, OrcIcpStats* stats) {
+                    float* R, float* t, OrcIcpStats* stats, const OrcColorIcp* col) {
   size_t gsize = (size_t)cam->W * cam->H;  // kernelGlobalSize[0]; stale across levels
   float Rc[9], tc[3];
   std::memcpy(Rc, R, sizeof(Rc));
@@ -670,6 +868,11 @@ ORC_API int orc_icp(const float* const* vlevels, const int* iters, int levels, c
     for (int it = 0; it < iters[lv]; ++it) {
       double sums[29];
       orc_icp_rows(vlevels[lv], w, h, vref, nref, cam, Rc, tc, prev, dist_thr, nullptr, sums);
+      if (col && col->weight > 0.f && lv == 0) {
+        double sc[29];
+        orc_color_rows(col->mv, col->mc, cam, 0, col->pyr, col->gx, col->gy, Rc, tc, 0, nullptr, sc);
+        for (int k = 0; k < 28; ++k) sums[k] += (double)col->weight * sc[k];
+      }
       ++total_iters;
       gsize = (size_t)w * h;
       unsigned size = (unsigned)std::ceil((float)gsize / 128.f);
@@ -844,6 +1047,7 @@ struct OrcEngineCfg {
   int hash;  // 1: voxel-block hash scene (NuiKinfuOpenCLHashScene) instead of the dense volume
   float voxel, mu;
   int buckets, excess, pool, max_w;
+  float photometric_weight;  // > 0 (with colour): the colour tracker's term joins ICP
 };
 
 struct OrcHash;
@@ -851,7 +1055,8 @@ OrcHash* orc_hash_create_internal(int buckets, int excess, int pool, float voxel
 void orc_hash_destroy_internal(OrcHash* h);
 void orc_hash_scene_integrate(OrcHash* h, const float* depth, const uint8_t* bgra, const OrcCam* cam,
                               const OrcXform* m, long* touched);
-void orc_hash_scene_raycast(OrcHash* h, const OrcCam* cam, const OrcXform* m, float* vmap, float* nmap);
+void orc_hash_scene_raycast(OrcHash* h, const OrcCam* cam, const OrcXform* m, float* vmap, float* nmap,
+                            uint8_t* cmap);
 
 struct OrcEngine {
   OrcEngineCfg c;
@@ -867,6 +1072,8 @@ struct OrcEngine {
   OrcIcpStats last{};
   long touched = 0;
   OrcHash* hs = nullptr;
+  // colour tracking: the previous frame's colours, the current frame's gradients
+  std::vector<uint8_t> cprev, cgx, cgy;
 };
 
 ORC_API OrcEngine* orc_engine_create(const OrcEngineCfg* cfg) {
@@ -898,6 +1105,11 @@ ORC_API OrcEngine* orc_engine_create(const OrcEngineCfg* cfg) {
   e->normals.resize(3 * N);
   e->dl.resize(c.levels);
   e->vl.resize(c.levels);
+  if (c.color && c.photometric_weight > 0.f) {
+    e->cprev.assign(4 * N, 0);
+    e->cgx.assign(4 * N, 0);
+    e->cgy.assign(4 * N, 0);
+  }
   for (int l = 0; l < c.levels; ++l) {
     long n = (long)(c.W >> l) * (c.H >> l);
     e->dl[l].resize(n);
@@ -944,6 +1156,7 @@ ORC_API int orc_engine_frame(OrcEngine* e, const uint16_t* raw, const uint8_t* b
                          c.color ? e->cvol.data() : nullptr, c.max_color_weight, &e->touched);
     }
   };
+  const bool photometric = col && !e->cprev.empty();
   if (e->frames == 0) {
     orc_normals(e->vl[0].data(), W, H, c.depth_threshold, e->normals.data());
     orc_transform_maps(e->vl[0].data(), e->normals.data(), W, H, &e->xf, e->vref.data(), e->nref.data());
@@ -960,8 +1173,13 @@ ORC_API int orc_engine_frame(OrcEngine* e, const uint16_t* raw, const uint8_t* b
     std::memcpy(t, e->xf.t, sizeof(t));
     const float step = c.dist_threshold / (float)c.levels;
     const float dthr = c.dist_threshold + step;
+    OrcColorIcp ci{};
+    if (photometric) {  // NuiKinfuOpenCLColorTracker::GradientBuffers (:194-242), finest level
+      orc_color_gradient(col, W, H, e->cgx.data(), e->cgy.data());
+      ci = OrcColorIcp{e->vref.data(), e->cprev.data(), col, e->cgx.data(), e->cgy.data(), c.photometric_weight};
+    }
     int st = orc_icp(lv.data(), c.iters, c.levels, e->vref.data(), e->nref.data(), &e->cam, &e->xf, dthr,
-                     R, t, &e->last);
+                     R, t, &e->last, photometric ? &ci : nullptr);
     if (st != 0) return 1;
     orc_make_xform(R, t, &e->xf);
     double rn = rel_angle(e->xf.R, e->lastR);
@@ -974,11 +1192,12 @@ ORC_API int orc_engine_frame(OrcEngine* e, const uint16_t* raw, const uint8_t* b
       std::memcpy(e->lastT, e->xf.t, sizeof(e->lastT));
     }
     if (e->hs)
-      orc_hash_scene_raycast(e->hs, &e->cam, &e->xf, e->vref.data(), e->nref.data());
+      orc_hash_scene_raycast(e->hs, &e->cam, &e->xf, e->vref.data(), e->nref.data(), nullptr);
     else
       orc_raycast(e->vol.data(), c.color ? e->cvol.data() : nullptr, &e->tp, &e->cam, &e->xf, W, H,
                   e->vref.data(), e->nref.data(), nullptr, nullptr);
   }
+  if (photometric) std::memcpy(e->cprev.data(), col, 4 * N);  // the next frame's model colours
   e->frames += 1;
   return 0;
 }
@@ -1534,6 +1753,7 @@ void orc_hash_scene_integrate(OrcHash* h, const float* depth, const uint8_t* bgr
   orc_hash_allocate(h, depth, cam, m);
   orc_hash_integrate(h, depth, bgra, cam, m, touched);
 }
-void orc_hash_scene_raycast(OrcHash* h, const OrcCam* cam, const OrcXform* m, float* vmap, float* nmap) {
-  orc_hash_raycast(h, cam, m, vmap, nmap, nullptr, nullptr);
+void orc_hash_scene_raycast(OrcHash* h, const OrcCam* cam, const OrcXform* m, float* vmap, float* nmap,
+                            uint8_t* cmap) {
+  orc_hash_raycast(h, cam, m, vmap, nmap, cmap, nullptr);
 }

@@ -85,7 +85,7 @@ class OrcEngineCfg(C.Structure):
                 ("sigma_space2_inv_half", C.c_float), ("sigma_depth2_inv_half", C.c_float),
                 ("depth_threshold", C.c_float), ("dist_threshold", C.c_float), ("integration_threshold", C.c_float),
                 ("hash", C.c_int), ("voxel", C.c_float), ("mu", C.c_float), ("buckets", C.c_int), ("excess", C.c_int),
-                ("pool", C.c_int), ("max_w", C.c_int)]
+                ("pool", C.c_int), ("max_w", C.c_int), ("photometric_weight", C.c_float)]
 
     @staticmethod
     def from_session_cfg(c):
@@ -111,6 +111,7 @@ class OrcEngineCfg(C.Structure):
         e.hash = 1 if c.volume_kind == 1 else 0
         e.voxel, e.mu = c.voxel_size, c.trunc_scale
         e.buckets, e.excess, e.pool, e.max_w = c.hash_buckets, c.hash_excess, c.hash_pool_blocks, c.hash_max_weight
+        e.photometric_weight = getattr(c, "photometric_weight", 0.0)
         return e
 
 
@@ -140,7 +141,10 @@ def oracle():
             "orc_icp_rows": (None, [_P, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, C.c_float, _P, _P]),
             "orc_inverse3": (None, [_P, _P]),
             "orc_make_xform": (None, [_P, _P, _P]),
-            "orc_icp": (C.c_int, [_P, _P, C.c_int, _P, _P, _P, _P, C.c_float, _P, _P, _P]),
+            "orc_icp": (C.c_int, [_P, _P, C.c_int, _P, _P, _P, _P, C.c_float, _P, _P, _P, _P]),
+            "orc_color_half_sample": (None, [_P, C.c_int, C.c_int, C.c_int, _P]),
+            "orc_color_gradient": (None, [_P, C.c_int, C.c_int, _P, _P]),
+            "orc_color_rows": (None, [_P, _P, _P, C.c_int, _P, _P, _P, _P, _P, C.c_int, _P, _P]),
             "orc_marching_cubes": (C.c_long, [_P, _P, _P, _P, _P, _P, C.c_long]),
             "orc_scan_compact": (C.c_long, [_P, C.c_long, _P, _P]),
             "orc_engine_create": (_P, [_P]),
@@ -186,6 +190,9 @@ def ref():
             "ref_raycast": (None, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int]),
             "ref_marching_cubes": (C.c_int, [_P, _P, _P, _P, _P]),
             "ref_icp_iteration": (None, [_P, _P, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_float, _P]),
+            "ref_half_sample_bgra": (None, [_P, _P, C.c_int, C.c_int, C.c_uint]),
+            "ref_bgra_gradient": (None, [_P, _P, _P, C.c_int, C.c_int]),
+            "ref_color_icp_blocks": (None, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_int, _P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(L, k)

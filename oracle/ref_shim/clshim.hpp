@@ -298,6 +298,9 @@ CLSHIM_CONV(uint, uint)
 CLSHIM_CONV(short, short)
 CLSHIM_CONV(ushort, ushort)
 CLSHIM_CONV(uchar, uchar)
+// float -> uchar: OpenCL leaves out-of-range values to the implementation; this shim keeps
+// the low byte of the truncation toward zero (negative values wrap), as x86 hosts do.
+inline uchar convert_uchar(float s) { return (uchar)(int)s; }
 CLSHIM_CONV(char, signed char)
 
 // ------------------------------------------------------------------ loads / stores
