@@ -215,7 +215,48 @@ NUI_API nui_status nui_batch_tick_device(nui_ctx* ctx, nui_session* const* sessi
                                          const uint16_t* const* d_depths, const uint8_t* const* d_bgras,
                                          nui_status* per_session_status, float* poses_out);
 
-/* Per-stage device time of the last nui_batch_tick* / nui_process_frame* call of the
+/* ---------------------------------------------------------------- serving loop
+ * Continuous batching of many RGB-D streams on one GPU.  No counterpart in the reference,
+ * which runs one stream (NuiKinfuTrackingEngine on its tracking thread).
+ *   admit    creates a session for a stream if its device bytes (nui_session_device_bytes)
+ *            fit in what is left of the HBM budget and a slot is free (else NUI_ERR_OOM:
+ *            the caller keeps the stream waiting and tries again after a release);
+ *   submit   queues one frame of a stream (host pointers, read at the step that takes the
+ *            frame; they must stay valid until its result is polled; pinned memory lets
+ *            the upload overlap the previous batch);
+ *   step     launches the next batch -- the oldest queued frame of every stream that has
+ *            one, all streams in one batched tick -- after starting its uploads on a second
+ *            stream, then collects the batch launched by the previous step;
+ *   poll     returns the finished frames with their submit and completion times on the
+ *            server clock (seconds; completion from CUDA events on the compute stream);
+ *   release  ends a stream and frees its budget (a frame of it in flight is completed first).
+ * Streams join and leave between steps; the batch keeps every live stream (streams without
+ * a queued frame sit the tick out), so its captured graph changes only when streams join
+ * or leave.  One server per context; not thread-safe. */
+typedef struct nui_server nui_server;
+typedef struct {
+  int slot;
+  int status;         /* nui_status of the frame */
+  uint64_t tag;       /* as submitted */
+  double t_submit;    /* server clock, seconds */
+  double t_done;
+  float pose[12];     /* R row-major, t */
+} nui_server_result;
+NUI_API nui_status nui_server_create(nui_ctx* ctx, size_t hbm_budget_bytes, int max_streams, nui_server** out);
+NUI_API nui_status nui_server_destroy(nui_server* srv);
+NUI_API double nui_server_clock(const nui_server* srv);
+NUI_API nui_status nui_server_admit(nui_server* srv, const nui_session_cfg* cfg, int* slot);
+NUI_API nui_status nui_server_release(nui_server* srv, int slot);
+/* t_submit < 0: now on the server clock (else the caller's arrival time on that clock) */
+NUI_API nui_status nui_server_submit(nui_server* srv, int slot, const uint16_t* depth_mm, const uint8_t* bgra,
+                                     uint64_t tag, double t_submit);
+NUI_API nui_status nui_server_step(nui_server* srv, int* frames_launched);
+NUI_API nui_status nui_server_drain(nui_server* srv);
+NUI_API nui_status nui_server_poll(nui_server* srv, nui_server_result* out, int cap, int* n);
+NUI_API nui_status nui_server_stats(const nui_server* srv, size_t* bytes_used, int* streams, int* queued);
+NUI_API nui_session* nui_server_session(nui_server* srv, int slot);
+
+/* Per-stage device time of the last nui_batch_tick* / nui_process_frame* call of the/* Per-stage device time of the last nui_batch_tick* / nui_process_frame* call of the
  * context, when timing is enabled (CUDA events on the context stream).
  * stage: 0 preprocess, 1 pyramid, 2 icp, 3 integrate, 4 raycast, 5 whole tick. */
 NUI_API nui_status nui_ctx_enable_timing(nui_ctx* ctx, int enable);
@@ -246,7 +287,17 @@ NUI_API nui_status nui_k_pyramid_level(nui_ctx* ctx, const float* d_src, int dW,
 NUI_API nui_status nui_k_feedback_maps(nui_ctx* ctx, const float* d_vertex4, int W, int H, float depth_thr,
                                        const float* pose12, float* d_vref4, float* d_nref4);
 
-/* ---------------------------------------------------------------- synthetic input
+/* half_sample_bgra_kernel + bgra_gradient_kernel over a whole colour pyramid
+ * (transformMaps.cl:106-146, 514-560; NuiKinfuOpenCLColorTracker::SubSampleColors /
+ * GradientBuffers, NuiKinfuOpenCLColorTracker.cpp:125-242): d_bgra (W x H BGRA) is level 0;
+ * d_levels[l] (l >= 1) receives level l ((W >> l) x (H >> l) BGRA, radius-1 box mean,
+ * alpha 255); d_gx[l] / d_gy[l] receive the Sobel / 8 gradients of level l as signed
+ * bytes (alpha 255, border 0).  Host arrays of `levels` device pointers (d_levels[0] is
+ * not used). */
+NUI_API nui_status nui_k_color_pyramid(nui_ctx* ctx, const uint8_t* d_bgra, int W, int H, int levels,
+                                       uint8_t* const* d_levels, uint8_t* const* d_gx, uint8_t* const* d_gy);
+
+/* ---------------------------------------------------------------- synthetic input/* ---------------------------------------------------------------- synthetic input
  * Seeded analytic scenes and trajectories standing in for recorded Kinect sessions. */
 typedef struct nui_synth_scene nui_synth_scene;
 enum { NUI_SYNTH_TABLETOP = 0, NUI_SYNTH_ROOM = 1 };

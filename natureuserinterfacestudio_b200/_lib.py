@@ -77,6 +77,18 @@ _SIGS = {
     "nui_mesh": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
     "nui_mesh_cases": (C.c_int, [_P, _P, C.c_size_t, _P]),
     "nui_mesh_device_noalloc": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
+    "nui_k_color_pyramid": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, _P, _P]),
+    "nui_server_create": (C.c_int, [_P, C.c_size_t, C.c_int, _P]),
+    "nui_server_destroy": (C.c_int, [_P]),
+    "nui_server_clock": (C.c_double, [_P]),
+    "nui_server_admit": (C.c_int, [_P, _P, _P]),
+    "nui_server_release": (C.c_int, [_P, C.c_int]),
+    "nui_server_submit": (C.c_int, [_P, C.c_int, _P, _P, C.c_uint64, C.c_double]),
+    "nui_server_step": (C.c_int, [_P, _P]),
+    "nui_server_drain": (C.c_int, [_P]),
+    "nui_server_poll": (C.c_int, [_P, _P, C.c_int, _P]),
+    "nui_server_stats": (C.c_int, [_P, _P, _P, _P]),
+    "nui_server_session": (_P, [_P, C.c_int]),
     "nui_debug_download": (C.c_int, [_P, C.c_int, C.c_int, _P, C.c_size_t]),
     "nui_debug_upload_volume": (C.c_int, [_P, _P]),
     "nui_hash_stats": (C.c_int, [_P, _P, _P, _P, _P]),
@@ -364,3 +376,76 @@ class SynthScene:
         lib().nui_synth_render(self.h, ptr(Rf), ptr(tf), W, H, fx, fy, cx, cy, noise_seed, frame, 1 if noise else 0,
                                ptr(d), ptr(c))
         return d, c
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("slot", C.c_int), ("status", C.c_int), ("tag", C.c_uint64), ("t_submit", C.c_double),
+                ("t_done", C.c_double), ("pose", C.c_float * 12)]
+
+
+class Server:
+    """Continuous batching of many streams on one context (nui_server_*).
+
+    Frames passed to submit() must stay alive until their result is polled; pinned
+    (page-locked) host arrays let the upload overlap the previous batch."""
+
+    def __init__(self, ctx, hbm_budget_bytes, max_streams=64):
+        h = C.c_void_p()
+        check(lib().nui_server_create(ctx.h, int(hbm_budget_bytes), int(max_streams), C.byref(h)))
+        self.h = h
+        self.ctx = ctx
+        self._keep = {}
+
+    def close(self):
+        if self.h:
+            lib().nui_server_destroy(self.h)
+            self.h = None
+            self._keep = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def clock(self):
+        return lib().nui_server_clock(self.h)
+
+    def admit(self, cfg):
+        """Slot of the new stream, or None when it does not fit (budget or slots)."""
+        k = C.c_int()
+        r = lib().nui_server_admit(self.h, C.byref(cfg), C.byref(k))
+        if r == NUI_ERR_OOM:
+            return None
+        check(r)
+        return k.value
+
+    def release(self, slot):
+        check(lib().nui_server_release(self.h, slot))
+        self._keep = {k: v for k, v in self._keep.items() if k[0] != slot}
+
+    def submit(self, slot, depth, bgra=None, tag=0, t_submit=-1.0):
+        self._keep[(slot, tag)] = (depth, bgra)
+        check(lib().nui_server_submit(self.h, slot, ptr(depth), ptr(bgra), int(tag), float(t_submit)))
+
+    def step(self):
+        n = C.c_int()
+        check(lib().nui_server_step(self.h, C.byref(n)))
+        return n.value
+
+    def drain(self):
+        check(lib().nui_server_drain(self.h))
+
+    def poll(self, cap=4096):
+        out = (ServerResult * cap)()
+        n = C.c_int()
+        check(lib().nui_server_poll(self.h, out, cap, C.byref(n)))
+        res = [out[i] for i in range(n.value)]
+        for r in res:
+            self._keep.pop((r.slot, r.tag), None)
+        return res
+
+    def stats(self):
+        used, ns, nq = C.c_size_t(), C.c_int(), C.c_int()
+        check(lib().nui_server_stats(self.h, C.byref(used), C.byref(ns), C.byref(nq)))
+        return used.value, ns.value, nq.value

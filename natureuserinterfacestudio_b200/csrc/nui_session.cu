@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <deque>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -83,6 +85,7 @@ nui_status fail(nui_status st, const std::string& msg) {
 
 constexpr int kStages = 6;
 constexpr int kZChunkTargetThreads = 1 << 18;
+constexpr size_t kMaxGraphs = 64;  // captured tick graphs kept per context
 }  // namespace
 
 struct nui_session;
@@ -464,8 +467,11 @@ nui_status finish_timing(nui_ctx* ctx) {
 
 // Runs one tick over sessions[0..n) whose frames are already in device memory at
 // raws[i]/bgras[i].  use_graph: replay a captured graph for this batch shape.
-nui_status run_tick(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t* const* raws,
-                    const uint8_t* const* bgras, bool use_graph, nui_status* per, float* poses) {
+// Launches one batched tick on the context stream (asynchronous).  raws[i] == nullptr
+// leaves session i out of this tick (inactive: every kernel skips it), so that a batch
+// keeps its shape -- and its captured graph -- while some sessions have no frame.
+nui_status tick_launch(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t* const* raws,
+                       const uint8_t* const* bgras, bool use_graph) {
   nui_status st = ensure_cap(ctx, n);
   if (st != NUI_OK) return st;
   BatchPlan p;
@@ -473,13 +479,17 @@ nui_status run_tick(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t*
   for (int i = 0; i < n; ++i) {
     nui_session* s = ss[i];
     plan_add(p, s);
-    int kind = s->frames == 0 ? kFirstFrame : kTrackFrame;
+    int kind = !raws[i] ? kInactive : s->frames == 0 ? kFirstFrame : kTrackFrame;
     fill_desc(s, ctx->h_descs[i], kind, raws[i], bgras ? bgras[i] : nullptr);
   }
   NUI_CUDA(cudaMemcpyAsync(ctx->d_descs, ctx->h_descs, sizeof(SessionDesc) * n, cudaMemcpyHostToDevice, ctx->stream));
   if (use_graph && !ctx->timing) {
     auto it = ctx->graphs.find(p);
     if (it == ctx->graphs.end()) {
+      if (ctx->graphs.size() >= kMaxGraphs) {  // bounded cache: start over
+        for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+        ctx->graphs.clear();
+      }
       cudaGraph_t g;
       NUI_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
       enqueue_tick(ctx, p, ctx->d_descs, ctx->d_pose, ctx->d_status, false);
@@ -496,12 +506,22 @@ nui_status run_tick(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t*
   }
   NUI_CUDA(cudaMemcpyAsync(ctx->h_pose, ctx->d_pose, sizeof(float) * 14 * n, cudaMemcpyDeviceToHost, ctx->stream));
   NUI_CUDA(cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int) * 2 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  return NUI_OK;
+}
+
+// Waits for the launched tick and takes its per-session results.
+nui_status tick_finish(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t* const* raws, nui_status* per,
+                       float* poses) {
   NUI_CUDA(cudaStreamSynchronize(ctx->stream));
-  st = finish_timing(ctx);
+  nui_status st = finish_timing(ctx);
   if (st != NUI_OK) return st;
   nui_status agg = NUI_OK;
   for (int i = 0; i < n; ++i) {
     nui_session* s = ss[i];
+    if (!raws[i]) {
+      if (per) per[i] = NUI_OK;
+      continue;
+    }
     int status = ctx->h_status[2 * i];
     nui_status r = status == 0 ? NUI_OK : NUI_ERR_TRACKING_LOST;
     if (per) per[i] = r;
@@ -517,6 +537,13 @@ nui_status run_tick(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t*
     if (poses) std::memcpy(poses + 12 * i, ctx->h_pose + 14 * i, 12 * sizeof(float));
   }
   return agg;
+}
+
+nui_status run_tick(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t* const* raws,
+                    const uint8_t* const* bgras, bool use_graph, nui_status* per, float* poses) {
+  nui_status st = tick_launch(ctx, ss, n, raws, bgras, use_graph);
+  if (st != NUI_OK) return st;
+  return tick_finish(ctx, ss, n, raws, per, poses);
 }
 
 nui_status upload_frame(nui_session* s, const uint16_t* depth, const uint8_t* bgra) {
@@ -1152,6 +1179,35 @@ NUI_API nui_status nui_k_pyramid_level(nui_ctx* ctx, const float* d_src, int dW,
   return NUI_OK;
 }
 
+NUI_API nui_status nui_k_color_pyramid(nui_ctx* ctx, const uint8_t* d_bgra, int W, int H, int levels,
+                                       uint8_t* const* d_levels, uint8_t* const* d_gx, uint8_t* const* d_gy) {
+  if (!ctx || !d_bgra || !d_levels || !d_gx || !d_gy || W <= 0 || H <= 0 || levels < 1 || levels > kMaxLevels)
+    return fail(NUI_ERR_INVALID_ARG, "bad argument");
+  if (((W >> (levels - 1)) << (levels - 1)) != W || ((H >> (levels - 1)) << (levels - 1)) != H)
+    return fail(NUI_ERR_INVALID_ARG, "image size must be divisible by 2^(levels-1)");
+  SessionDesc d;
+  std::memset(&d, 0, sizeof(d));
+  d.kind = kTrackFrame;
+  d.W = W;
+  d.H = H;
+  d.levels = levels;
+  d.photo_w = 1.f;
+  d.bgra = d_bgra;
+  for (int l = 0; l < levels; ++l) {
+    if ((l > 0 && !d_levels[l]) || !d_gx[l] || !d_gy[l]) return fail(NUI_ERR_INVALID_ARG, "null level buffer");
+    d.cpyr[l] = l > 0 ? (uchar4*)d_levels[l] : nullptr;
+    d.cgx[l] = (uchar4*)d_gx[l];
+    d.cgy[l] = (uchar4*)d_gy[l];
+  }
+  NUI_CUDA(cudaMemcpyAsync(ctx->d_kdesc, &d, sizeof(d), cudaMemcpyHostToDevice, ctx->stream));
+  for (int l = 1; l < levels; ++l)
+    k_color_level<<<dim3(cdiv((long)(W >> l) * (H >> l), 256), 1), 256, 0, ctx->stream>>>(ctx->d_kdesc, l);
+  k_color_grad<<<dim3(cdiv((long)W * H, 256), 1, levels), 256, 0, ctx->stream>>>(ctx->d_kdesc);
+  NUI_CUDA(cudaGetLastError());
+  NUI_CUDA(cudaStreamSynchronize(ctx->stream));
+  return NUI_OK;
+}
+
 NUI_API nui_status nui_k_feedback_maps(nui_ctx* ctx, const float* d_vertex4, int W, int H, float thr,
                                        const float* pose12, float* d_vref4, float* d_nref4) {
   if (!ctx || !d_vertex4 || !pose12 || !d_vref4 || !d_nref4 || W <= 0 || H <= 0)
@@ -1419,3 +1475,265 @@ extern "C" NUI_API nui_status nui_mesh_device_noalloc(nui_session* s, float* d_p
   if (total > cap) return fail(NUI_ERR_MESH_OVERFLOW, "mesh larger than the output capacity");
   return NUI_OK;
 }
+
+// ------------------------------------------------------------------ serving loop
+struct nui_server {
+  struct Frame {
+    const uint16_t* depth;
+    const uint8_t* bgra;
+    uint64_t tag;
+    double t_submit;
+  };
+  struct Slot {
+    nui_session* s = nullptr;
+    size_t bytes = 0;
+    std::deque<Frame> q;
+    uint16_t* draw[2] = {nullptr, nullptr};  // device frame double buffer
+    uint8_t* dbgra[2] = {nullptr, nullptr};
+    int buf = 0;
+  };
+  nui_ctx* ctx = nullptr;
+  size_t budget = 0, used = 0;
+  cudaStream_t up = nullptr;
+  cudaEvent_t ev_t0 = nullptr, ev_up = nullptr, ev_done = nullptr;
+  std::chrono::steady_clock::time_point t0;
+  std::vector<Slot> slots;
+  // the batch in flight: every live slot, with the frame it got (or none)
+  bool inflight = false;
+  std::vector<int> bslot;
+  std::vector<nui_session*> bsess;
+  std::vector<const uint16_t*> braw;
+  std::vector<const uint8_t*> bbgra;
+  std::vector<Frame> bframe;
+  std::vector<nui_server_result> done;
+  double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+};
+
+namespace {
+nui_status server_collect(nui_server* v) {
+  if (!v->inflight) return NUI_OK;
+  v->inflight = false;
+  NUI_CUDA(cudaEventSynchronize(v->ev_done));
+  float ms = 0.f;
+  NUI_CUDA(cudaEventElapsedTime(&ms, v->ev_t0, v->ev_done));
+  const double t_done = ms * 1e-3;
+  const int n = (int)v->bsess.size();
+  std::vector<nui_status> per(n);
+  std::vector<float> poses(12 * (size_t)n);
+  nui_status st = tick_finish(v->ctx, v->bsess.data(), n, v->braw.data(), per.data(), poses.data());
+  if (st != NUI_OK && st != NUI_ERR_TRACKING_LOST) return st;
+  for (int i = 0; i < n; ++i) {
+    if (!v->braw[i]) continue;
+    nui_server_result r;
+    r.slot = v->bslot[i];
+    r.status = per[i];
+    r.tag = v->bframe[i].tag;
+    r.t_submit = v->bframe[i].t_submit;
+    r.t_done = t_done;
+    std::memcpy(r.pose, poses.data() + 12 * i, sizeof(r.pose));
+    v->done.push_back(r);
+  }
+  return NUI_OK;
+}
+}  // namespace
+
+extern "C" {
+
+NUI_API nui_status nui_server_create(nui_ctx* ctx, size_t budget, int max_streams, nui_server** out) {
+  if (!ctx || !out || max_streams <= 0) return fail(NUI_ERR_INVALID_ARG, "bad argument");
+  NUI_CUDA(cudaSetDevice(ctx->device));
+  nui_server* v = new nui_server();
+  v->ctx = ctx;
+  v->budget = budget;
+  v->slots.resize(max_streams);
+  if (cudaStreamCreateWithFlags(&v->up, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&v->ev_t0) != cudaSuccess || cudaEventCreateWithFlags(&v->ev_up, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreate(&v->ev_done) != cudaSuccess) {
+    delete v;
+    return fail(NUI_ERR_DEVICE, "stream / event creation failed");
+  }
+  // the server clock: host time of a recorded event, so device completion times map onto it
+  NUI_CUDA(cudaStreamSynchronize(ctx->stream));
+  NUI_CUDA(cudaEventRecord(v->ev_t0, ctx->stream));
+  NUI_CUDA(cudaEventSynchronize(v->ev_t0));
+  v->t0 = std::chrono::steady_clock::now();
+  *out = v;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_server_destroy(nui_server* v) {
+  if (!v) return NUI_OK;
+  server_collect(v);
+  for (int i = 0; i < (int)v->slots.size(); ++i)
+    if (v->slots[i].s) nui_server_release(v, i);
+  cudaStreamDestroy(v->up);
+  cudaEventDestroy(v->ev_t0);
+  cudaEventDestroy(v->ev_up);
+  cudaEventDestroy(v->ev_done);
+  delete v;
+  return NUI_OK;
+}
+
+NUI_API double nui_server_clock(const nui_server* v) { return v ? v->now() : 0.0; }
+
+NUI_API nui_status nui_server_admit(nui_server* v, const nui_session_cfg* cfg, int* slot) {
+  if (!v || !cfg || !slot) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  const size_t need = nui_session_device_bytes(cfg) + (size_t)cfg->width * cfg->height * 12;
+  if (need == (size_t)cfg->width * cfg->height * 12) {
+    std::string why;
+    cfg_valid(cfg, why);
+    return fail(NUI_ERR_INVALID_ARG, why);
+  }
+  if (v->used + need > v->budget) return fail(NUI_ERR_OOM, "stream does not fit in the HBM budget");
+  int k = -1;
+  for (int i = 0; i < (int)v->slots.size() && k < 0; ++i)
+    if (!v->slots[i].s) k = i;
+  if (k < 0) return fail(NUI_ERR_OOM, "no free stream slot");
+  nui_session* s = nullptr;
+  nui_status st = nui_session_create(v->ctx, cfg, &s);
+  if (st != NUI_OK) return st;
+  nui_server::Slot& sl = v->slots[k];
+  const size_t N = (size_t)cfg->width * cfg->height;
+  bool ok = true;
+  for (int b = 0; b < 2 && ok; ++b) {
+    ok = cudaMalloc(&sl.draw[b], N * 2) == cudaSuccess;
+    if (ok && s->cmap) ok = cudaMalloc(&sl.dbgra[b], N * 4) == cudaSuccess;
+  }
+  if (!ok) {
+    for (int b = 0; b < 2; ++b) {
+      cudaFree(sl.draw[b]);
+      cudaFree(sl.dbgra[b]);
+      sl.draw[b] = nullptr;
+      sl.dbgra[b] = nullptr;
+    }
+    nui_session_destroy(s);
+    return fail(NUI_ERR_OOM, "device allocation failed");
+  }
+  sl.s = s;
+  sl.bytes = need;
+  sl.buf = 0;
+  sl.q.clear();
+  v->used += need;
+  *slot = k;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_server_release(nui_server* v, int slot) {
+  if (!v || slot < 0 || slot >= (int)v->slots.size() || !v->slots[slot].s) return fail(NUI_ERR_INVALID_ARG, "bad slot");
+  if (v->inflight && std::find(v->bslot.begin(), v->bslot.end(), slot) != v->bslot.end()) {
+    nui_status st = server_collect(v);
+    if (st != NUI_OK) return st;
+  }
+  NUI_CUDA(cudaStreamSynchronize(v->up));
+  nui_server::Slot& sl = v->slots[slot];
+  for (int b = 0; b < 2; ++b) {
+    cudaFree(sl.draw[b]);
+    cudaFree(sl.dbgra[b]);
+    sl.draw[b] = nullptr;
+    sl.dbgra[b] = nullptr;
+  }
+  nui_session_destroy(sl.s);
+  sl.s = nullptr;
+  sl.q.clear();
+  v->used -= sl.bytes;
+  sl.bytes = 0;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_server_submit(nui_server* v, int slot, const uint16_t* depth, const uint8_t* bgra, uint64_t tag,
+                                     double t_submit) {
+  if (!v || !depth || slot < 0 || slot >= (int)v->slots.size() || !v->slots[slot].s)
+    return fail(NUI_ERR_INVALID_ARG, "bad slot or frame");
+  v->slots[slot].q.push_back(nui_server::Frame{depth, bgra, tag, t_submit < 0 ? v->now() : t_submit});
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_server_step(nui_server* v, int* launched) {
+  if (!v) return fail(NUI_ERR_INVALID_ARG, "null server");
+  // the next batch: every live stream, with its oldest queued frame if it has one
+  std::vector<int> nslot;
+  std::vector<nui_session*> nsess;
+  std::vector<const uint16_t*> nraw;
+  std::vector<const uint8_t*> nbgra;
+  std::vector<nui_server::Frame> nframe;
+  int count = 0;
+  for (int i = 0; i < (int)v->slots.size(); ++i) {
+    nui_server::Slot& sl = v->slots[i];
+    if (!sl.s) continue;
+    nslot.push_back(i);
+    nsess.push_back(sl.s);
+    if (sl.q.empty()) {
+      nraw.push_back(nullptr);
+      nbgra.push_back(nullptr);
+      nframe.push_back(nui_server::Frame{nullptr, nullptr, 0, 0.0});
+      continue;
+    }
+    nui_server::Frame f = sl.q.front();
+    sl.q.pop_front();
+    const int b = sl.buf ^ 1;  // the buffer the batch in flight does not read
+    sl.buf = b;
+    const size_t N = (size_t)sl.s->cfg.width * sl.s->cfg.height;
+    NUI_CUDA(cudaMemcpyAsync(sl.draw[b], f.depth, N * 2, cudaMemcpyHostToDevice, v->up));
+    const uint8_t* db = nullptr;
+    if (f.bgra && sl.dbgra[b]) {
+      NUI_CUDA(cudaMemcpyAsync(sl.dbgra[b], f.bgra, N * 4, cudaMemcpyHostToDevice, v->up));
+      db = sl.dbgra[b];
+    }
+    nraw.push_back(sl.draw[b]);
+    nbgra.push_back(db);
+    nframe.push_back(f);
+    ++count;
+  }
+  NUI_CUDA(cudaEventRecord(v->ev_up, v->up));
+  // collect the batch in flight while these uploads run
+  nui_status st = server_collect(v);
+  if (st != NUI_OK) return st;
+  if (launched) *launched = count;
+  if (count == 0) return NUI_OK;
+  NUI_CUDA(cudaStreamWaitEvent(v->ctx->stream, v->ev_up, 0));
+  st = tick_launch(v->ctx, nsess.data(), (int)nsess.size(), nraw.data(), nbgra.data(), true);
+  if (st != NUI_OK) return st;
+  NUI_CUDA(cudaEventRecord(v->ev_done, v->ctx->stream));
+  v->bslot.swap(nslot);
+  v->bsess.swap(nsess);
+  v->braw.swap(nraw);
+  v->bbgra.swap(nbgra);
+  v->bframe.swap(nframe);
+  v->inflight = true;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_server_drain(nui_server* v) {
+  if (!v) return fail(NUI_ERR_INVALID_ARG, "null server");
+  return server_collect(v);
+}
+
+NUI_API nui_status nui_server_poll(nui_server* v, nui_server_result* out, int cap, int* n) {
+  if (!v || !n || (cap > 0 && !out)) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  const int k = std::min(cap, (int)v->done.size());
+  for (int i = 0; i < k; ++i) out[i] = v->done[i];
+  v->done.erase(v->done.begin(), v->done.begin() + k);
+  *n = k;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_server_stats(const nui_server* v, size_t* used, int* streams, int* queued) {
+  if (!v) return fail(NUI_ERR_INVALID_ARG, "null server");
+  int ns = 0, nq = 0;
+  for (const auto& sl : v->slots)
+    if (sl.s) {
+      ++ns;
+      nq += (int)sl.q.size();
+    }
+  if (used) *used = v->used;
+  if (streams) *streams = ns;
+  if (queued) *queued = nq;
+  return NUI_OK;
+}
+
+NUI_API nui_session* nui_server_session(nui_server* v, int slot) {
+  if (!v || slot < 0 || slot >= (int)v->slots.size()) return nullptr;
+  return v->slots[slot].s;
+}
+
+}  // extern "C"

@@ -93,3 +93,31 @@ def test_color_tracking_fp16_ate_within_1mm_of_fp32(gpu_ctx):
         ate[fmt] = float(np.sqrt(np.mean(err)))
         s.close()
     assert abs(ate[L.TSDF_F16_U8] - ate[L.TSDF_F32]) <= 1e-3, ate
+
+
+def test_kernel_level_color_pyramid_bit_exact(gpu_ctx):
+    torch = pytest.importorskip("torch")
+    import ctypes as C
+    bgra = np.ascontiguousarray(frames(1, W=640, H=480, seed=9, color=True)[0][1])
+    H, W, levels = 480, 640, 3
+    d_in = torch.from_numpy(bgra).cuda()
+    lv = [None] + [torch.zeros((H >> l, W >> l, 4), dtype=torch.uint8, device="cuda") for l in range(1, levels)]
+    gx = [torch.zeros((H >> l, W >> l, 4), dtype=torch.uint8, device="cuda") for l in range(levels)]
+    gy = [torch.zeros((H >> l, W >> l, 4), dtype=torch.uint8, device="cuda") for l in range(levels)]
+    arr = C.c_void_p * levels
+    pl = arr(*[None] + [t.data_ptr() for t in lv[1:]])
+    pgx = arr(*[t.data_ptr() for t in gx])
+    pgy = arr(*[t.data_ptr() for t in gy])
+    L.check(L.lib().nui_k_color_pyramid(gpu_ctx.h, C.c_void_p(d_in.data_ptr()), W, H, levels, pl, pgx, pgy))
+    src = bgra
+    for l in range(levels):
+        if l > 0:
+            want = np.zeros((H >> l, W >> l, 4), np.uint8)
+            O.oracle().orc_color_half_sample(O.p(src), W >> l, H >> l, 1, O.p(want))
+            assert np.array_equal(lv[l].cpu().numpy(), want), l
+            src = want
+        ox = np.zeros_like(src)
+        oy = np.zeros_like(src)
+        O.oracle().orc_color_gradient(O.p(src), W >> l, H >> l, O.p(ox), O.p(oy))
+        assert np.array_equal(gx[l].cpu().numpy(), ox), l
+        assert np.array_equal(gy[l].cpu().numpy(), oy), l
