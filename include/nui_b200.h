@@ -229,7 +229,9 @@ NUI_API nui_status nui_batch_tick_device(nui_ctx* ctx, nui_session* const* sessi
  *            stream, then collects the batch launched by the previous step;
  *   poll     returns the finished frames with their submit and completion times on the
  *            server clock (seconds; completion from CUDA events on the compute stream);
- *   release  ends a stream and frees its budget (a frame of it in flight is completed first).
+ *   release  ends a stream (a frame of it in flight is completed first); its session is
+ *            kept for the next stream of the same configuration and freed when another
+ *            stream needs its budget.
  * Streams join and leave between steps; the batch keeps every live stream (streams without
  * a queued frame sit the tick out), so its captured graph changes only when streams join
  * or leave.  One server per context; not thread-safe. */
@@ -247,6 +249,10 @@ NUI_API nui_status nui_server_destroy(nui_server* srv);
 NUI_API double nui_server_clock(const nui_server* srv);
 NUI_API nui_status nui_server_admit(nui_server* srv, const nui_session_cfg* cfg, int* slot);
 NUI_API nui_status nui_server_release(nui_server* srv, int slot);
+/* Creates `count` idle sessions of `cfg` (counted in the budget) that later admissions of
+ * that configuration take without allocating; a released stream's session is kept the
+ * same way until a new stream needs its memory. */
+NUI_API nui_status nui_server_reserve(nui_server* srv, const nui_session_cfg* cfg, int count);
 /* t_submit < 0: now on the server clock (else the caller's arrival time on that clock) */
 NUI_API nui_status nui_server_submit(nui_server* srv, int slot, const uint16_t* depth_mm, const uint8_t* bgra,
                                      uint64_t tag, double t_submit);
@@ -258,9 +264,13 @@ NUI_API nui_session* nui_server_session(nui_server* srv, int slot);
 
 /* Per-stage device time of the last nui_batch_tick* / nui_process_frame* call of the/* Per-stage device time of the last nui_batch_tick* / nui_process_frame* call of the
  * context, when timing is enabled (CUDA events on the context stream).
- * stage: 0 preprocess, 1 pyramid, 2 icp, 3 integrate, 4 raycast, 5 whole tick. */
+ * stage: 0 preprocess, 1 pyramid + feedback maps, 2 tracking (colour gradients, ICP, gate),
+ * 3 dense integration kernel, 4 brick summaries + voxel-hash allocation / integration,
+ * 5 raycast (dense and hash), 6 whole tick. */
 NUI_API nui_status nui_ctx_enable_timing(nui_ctx* ctx, int enable);
 NUI_API nui_status nui_ctx_stage_ms(nui_ctx* ctx, int stage, float* ms);
+/* Kernel launches in the captured graph of the context's last graphed batch tick. */
+NUI_API nui_status nui_ctx_last_tick_kernels(nui_ctx* ctx, int* n);
 /* Voxels read-modify-written by the last integration of a session. */
 NUI_API nui_status nui_session_touched_voxels(nui_session* s, uint64_t* n);
 

@@ -41,7 +41,7 @@ class SessionCfg(C.Structure):
         ("integration_threshold", C.c_float),
         ("voxel_size", C.c_float), ("trunc_scale", C.c_float), ("hash_buckets", C.c_int),
         ("hash_excess", C.c_int), ("hash_pool_blocks", C.c_int), ("hash_max_weight", C.c_int),
-                ("photometric_weight", C.c_float),
+        ("photometric_weight", C.c_float),
     ]
 
 
@@ -83,6 +83,7 @@ _SIGS = {
     "nui_server_clock": (C.c_double, [_P]),
     "nui_server_admit": (C.c_int, [_P, _P, _P]),
     "nui_server_release": (C.c_int, [_P, C.c_int]),
+    "nui_server_reserve": (C.c_int, [_P, _P, C.c_int]),
     "nui_server_submit": (C.c_int, [_P, C.c_int, _P, _P, C.c_uint64, C.c_double]),
     "nui_server_step": (C.c_int, [_P, _P]),
     "nui_server_drain": (C.c_int, [_P]),
@@ -96,6 +97,7 @@ _SIGS = {
     "nui_batch_tick_device": (C.c_int, [_P, _P, C.c_int, _P, _P, _P, _P]),
     "nui_ctx_enable_timing": (C.c_int, [_P, C.c_int]),
     "nui_ctx_stage_ms": (C.c_int, [_P, C.c_int, _P]),
+    "nui_ctx_last_tick_kernels": (C.c_int, [_P, _P]),
     "nui_session_touched_voxels": (C.c_int, [_P, _P]),
     "nui_k_preprocess": (C.c_int, [_P, _P, C.c_int, C.c_int] + [C.c_float] * 6 + [C.c_int] + [C.c_float] * 3 + [_P, _P, _P]),
     "nui_k_pyramid_level": (C.c_int, [_P, _P, C.c_int, C.c_int] + [C.c_float] * 4 + [C.c_int, C.c_float, _P, _P]),
@@ -180,6 +182,11 @@ class Context:
 
     def enable_timing(self, on=True):
         check(lib().nui_ctx_enable_timing(self.h, 1 if on else 0))
+
+    def last_tick_kernels(self):
+        v = C.c_int()
+        check(lib().nui_ctx_last_tick_kernels(self.h, C.byref(v)))
+        return v.value
 
     def stage_ms(self, stage):
         v = C.c_float()
@@ -395,6 +402,7 @@ class Server:
         self.h = h
         self.ctx = ctx
         self._keep = {}
+        ctx._sessions.add(self)  # closed before its context
 
     def close(self):
         if self.h:
@@ -420,6 +428,14 @@ class Server:
         check(r)
         return k.value
 
+    def reserve(self, cfg, count):
+        """Idle sessions of cfg for later admissions (None when the budget is short)."""
+        r = lib().nui_server_reserve(self.h, C.byref(cfg), int(count))
+        if r == NUI_ERR_OOM:
+            return None
+        check(r)
+        return count
+
     def release(self, slot):
         check(lib().nui_server_release(self.h, slot))
         self._keep = {k: v for k, v in self._keep.items() if k[0] != slot}
@@ -436,11 +452,17 @@ class Server:
     def drain(self):
         check(lib().nui_server_drain(self.h))
 
-    def poll(self, cap=4096):
-        out = (ServerResult * cap)()
-        n = C.c_int()
-        check(lib().nui_server_poll(self.h, out, cap, C.byref(n)))
-        res = [out[i] for i in range(n.value)]
+    def poll(self, cap=1024):
+        if getattr(self, "_pollbuf", None) is None or len(self._pollbuf) < cap:
+            self._pollbuf = (ServerResult * cap)()
+        out = self._pollbuf
+        res = []
+        while True:
+            n = C.c_int()
+            check(lib().nui_server_poll(self.h, out, cap, C.byref(n)))
+            res += [ServerResult.from_buffer_copy(out[i]) for i in range(n.value)]
+            if n.value < cap:
+                break
         for r in res:
             self._keep.pop((r.slot, r.tag), None)
         return res

@@ -483,63 +483,76 @@ __global__ void k_hash_project(const SessionDesc* __restrict__ descs) {
   }
 }
 
+// Pool offset (block index * 512) of block (sx, sy, sz) or -1: the bucket, then its excess
+// chain (findVoxelBlockIndex, KinfuHashRaycast.cl:78-111).
+__device__ __noinline__ int hash_block_lookup(const SessionDesc& s, short sx, short sy, short sz) {
+  unsigned hi = hash_index(s.hmask, sx, sy, sz);
+  for (;;) {
+    const HEntry en = load_entry(s.entries, hi);
+    if (en.pos[0] == sx && en.pos[1] == sy && en.pos[2] == sz && en.ptr >= 0) return en.ptr * 512;
+    if (en.offset < 1) return -1;
+    hi = (unsigned)s.nb + en.offset - 1;
+  }
+}
+
 template <int HF>
 struct HashRead {
   const SessionDesc& s;
   short cbx, cby, cbz;
   int cptr;  // cached block (findVoxelBlockIndex's cache; transparent to results)
-  __device__ __forceinline__ int find(int vx, int vy, int vz) {
-    int bx = vx < 0 ? vx - 7 : vx, by = vy < 0 ? vy - 7 : vy, bz = vz < 0 ? vz - 7 : vz;
-    bx /= 8;
-    by /= 8;
-    bz /= 8;
-    const int lin = (vx - 8 * bx) + 8 * (vy - 8 * by) + 64 * (vz - 8 * bz);
+  // Pool offset (block index * 512) of block (bx, by, bz), or -1 if it is not allocated.
+  // The lookup itself is out of line: it is called from many places of the raycast, and
+  // inlined copies of its chain walk overflow the instruction cache.
+  __device__ __forceinline__ int block(int bx, int by, int bz) {
     const short sx = (short)bx, sy = (short)by, sz = (short)bz;
-    if (cptr >= 0 && sx == cbx && sy == cby && sz == cbz) return cptr + lin;
-    unsigned hi = hash_index(s.hmask, sx, sy, sz);
-    for (;;) {
-      const HEntry en = load_entry(s.entries, hi);
-      if (en.pos[0] == sx && en.pos[1] == sy && en.pos[2] == sz && en.ptr >= 0) {
-        cbx = sx;
-        cby = sy;
-        cbz = sz;
-        cptr = en.ptr * 512;
-        return cptr + lin;
-      }
-      if (en.offset < 1) break;
-      hi = (unsigned)s.nb + en.offset - 1;
+    if (cptr >= 0 && sx == cbx && sy == cby && sz == cbz) return cptr;
+    const int p = hash_block_lookup(s, sx, sy, sz);
+    if (p >= 0) {
+      cbx = sx;
+      cby = sy;
+      cbz = sz;
+      cptr = p;
     }
-    return -1;
+    return p;
+  }
+  // virtualVoxelPosToSDFBlock + the voxel's linear index (x + 8y + 64z); the reference's
+  // rounding of negative coordinates toward -infinity is an arithmetic shift
+  __device__ __forceinline__ int find(int vx, int vy, int vz) {
+    const int b = block(vx >> 3, vy >> 3, vz >> 3);
+    return b < 0 ? -1 : b + ((vx & 7) + 8 * (vy & 7) + 64 * (vz & 7));
   }
   __device__ __forceinline__ float sdf_at(int vx, int vy, int vz) {
     const int bi = find(vx, vy, vz);
     return bi < 0 ? 1.0f : HVox<HF>::load(s.hsdf, (unsigned)bi);
   }
+  __device__ __noinline__ float sdf_slow(int vx, int vy, int vz) { return sdf_at(vx, vy, vz); }
+  // The sdf of voxel (ix + dx, iy + dy, iz + dz): one block lookup for the whole
+  // neighbourhood when it lies inside the block of (ix, iy, iz) (base >= 0 then holds that
+  // voxel's pool index, or -2 if the block is not allocated), else a lookup per voxel.
+  __device__ __forceinline__ float near(int base, int ix, int iy, int iz, int dx, int dy, int dz) {
+    if (base == -1) return sdf_slow(ix + dx, iy + dy, iz + dz);
+    if (base == -2) return 1.0f;
+    return HVox<HF>::load(s.hsdf, (unsigned)(base + dx + 8 * dy + 64 * dz));
+  }
+  // base for near(): neighbours with offsets in [lo, hi] on every axis
+  __device__ __forceinline__ int near_base(int ix, int iy, int iz, int lo, int hi) {
+    const int x = ix & 7, y = iy & 7, z = iz & 7;
+    if (x + lo < 0 || x + hi > 7 || y + lo < 0 || y + hi > 7 || z + lo < 0 || z + hi > 7) return -1;
+    const int b = block(ix >> 3, iy >> 3, iz >> 3);
+    return b < 0 ? -2 : b + x + 8 * y + 64 * z;
+  }
 };
 
-// castRay + raycast_kernel (KinfuHashRaycast.cl:155-471)
+// castRay + raycast_kernel (KinfuHashRaycast.cl:155-471): one thread per pixel.  The
+// block cache of HashRead and the one-lookup neighbourhoods only save hash lookups; the
+// values read are those of the reference's per-voxel findVoxelBlockIndex.
+
+// The march of castRay (KinfuHashRaycast.cl:170-232) from (pr, total) until a surface
+// (sdf <= 0) or the end of the range.
 template <int HF>
-__global__ void __launch_bounds__(128) k_hash_raycast(const SessionDesc* __restrict__ descs) {
-  const SessionDesc& s = descs[blockIdx.y];
-  if (!s.hash || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
-  const int W = s.W, H = s.H;
-  const int pid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pid >= W * H) return;
-  const int px = pid % W, py = pid / W;
-  const DevXform& m = s.ts->xf;
-  HashRead<HF> R{s, 0, 0, 0, -1};
-  const float2 mm = s.range[pid];
-  const float oov = 1.0f / s.voxel;
-  const float stepScale = s.mu * oov * 0.6f;
-  float3 ps = depth_to_point(s.cam, px, py, mm.x);
-  float total = sqrtf(dot3(ps, ps)) * oov;
-  ps = mul3(xf_apply(m, ps), oov);
-  float3 pe = depth_to_point(s.cam, px, py, mm.y);
-  const float totalMax = sqrtf(dot3(pe, pe)) * oov;
-  pe = mul3(xf_apply(m, pe), oov);
-  float sdfv = 1.0f, stepLen;
-  const float3 dir = normalize3(sub3(pe, ps));
-  float3 pr = ps;
+__device__ __forceinline__ void hash_march(HashRead<HF>& R, const SessionDesc& s, float3& pr, float& total,
+                                           const float totalMax, const float3 dir, const float stepScale, float& sdfv) {
+  float stepLen;
   while (total < totalMax) {
     const int vx = (int)roundf(pr.x), vy = (int)roundf(pr.y), vz = (int)roundf(pr.z);
     const int bi = R.find(vx, vy, vz);
@@ -551,25 +564,51 @@ __global__ void __launch_bounds__(128) k_hash_raycast(const SessionDesc* __restr
       if (sdfv <= 0.1f && sdfv >= -0.5f) {
         const int ix = (int)floorf(pr.x), iy = (int)floorf(pr.y), iz = (int)floorf(pr.z);
         const float3 cf = f3(pr.x - (float)ix, pr.y - (float)iy, pr.z - (float)iz);
-        float v1 = R.sdf_at(ix, iy, iz), v2 = R.sdf_at(ix + 1, iy, iz);
+        const int nb = R.near_base(ix, iy, iz, 0, 1);
+        float v1 = R.near(nb, ix, iy, iz, 0, 0, 0), v2 = R.near(nb, ix, iy, iz, 1, 0, 0);
         float r1 = (1.0f - cf.x) * v1 + cf.x * v2;
-        v1 = R.sdf_at(ix, iy + 1, iz);
-        v2 = R.sdf_at(ix + 1, iy + 1, iz);
+        v1 = R.near(nb, ix, iy, iz, 0, 1, 0);
+        v2 = R.near(nb, ix, iy, iz, 1, 1, 0);
         r1 = (1.0f - cf.y) * r1 + cf.y * ((1.0f - cf.x) * v1 + cf.x * v2);
-        v1 = R.sdf_at(ix, iy, iz + 1);
-        v2 = R.sdf_at(ix + 1, iy, iz + 1);
+        v1 = R.near(nb, ix, iy, iz, 0, 0, 1);
+        v2 = R.near(nb, ix, iy, iz, 1, 0, 1);
         float r2 = (1.0f - cf.x) * v1 + cf.x * v2;
-        v1 = R.sdf_at(ix, iy + 1, iz + 1);
-        v2 = R.sdf_at(ix + 1, iy + 1, iz + 1);
+        v1 = R.near(nb, ix, iy, iz, 0, 1, 1);
+        v2 = R.near(nb, ix, iy, iz, 1, 1, 1);
         r2 = (1.0f - cf.y) * r2 + cf.y * ((1.0f - cf.x) * v1 + cf.x * v2);
         sdfv = (1.0f - cf.z) * r1 + cf.z * r2;
       }
-      if (sdfv <= 0.0f) break;
+      if (sdfv <= 0.0f) return;
       stepLen = fmaxf(sdfv * stepScale, 1.0f);
     }
     pr = add3(pr, mul3(dir, stepLen));
     total += stepLen;
   }
+}
+
+// Ray of pixel pid: start and end of the expected range in voxel units, and direction.
+template <int HF>
+__device__ __forceinline__ void hash_ray(const SessionDesc& s, int pid, float3& ps, float& total, float& totalMax,
+                                         float3& dir) {
+  const int px = pid % s.W, py = pid / s.W;
+  const DevXform& m = s.ts->xf;
+  const float2 mm = s.range[pid];
+  const float oov = 1.0f / s.voxel;
+  ps = depth_to_point(s.cam, px, py, mm.x);
+  total = sqrtf(dot3(ps, ps)) * oov;
+  ps = mul3(xf_apply(m, ps), oov);
+  float3 pe = depth_to_point(s.cam, px, py, mm.y);
+  totalMax = sqrtf(dot3(pe, pe)) * oov;
+  pe = mul3(xf_apply(m, pe), oov);
+  dir = normalize3(sub3(pe, ps));
+}
+
+// The surface refinement, normal and colour of castRay / raycast_kernel
+// (KinfuHashRaycast.cl:233-471) and the map writes of pixel pid.
+template <int HF>
+__device__ __forceinline__ void hash_finish(HashRead<HF>& R, const SessionDesc& s, int pid, float3 pr,
+                                            const float3 dir, const float stepScale, float sdfv) {
+  float stepLen;
   const float4 nanv = make_float4(qnan(), qnan(), qnan(), 0.f);
   float4 vout = nanv, nout = nanv;
   uchar4 col = make_uchar4(0, 0, 0, 0);
@@ -581,10 +620,11 @@ __global__ void __launch_bounds__(128) k_hash_raycast(const SessionDesc* __restr
     const float3 nc = f3(1.0f - cf.x, 1.0f - cf.y, 1.0f - cf.z);
     float fb[8];
     float nearest = 1.0e20f;
+    const int nb = R.near_base(ix, iy, iz, 0, 1);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-      const int bi = R.find(ix + ox, iy + oy, iz + oz);
+      const int bi = nb >= 0 ? nb + ox + 8 * oy + 64 * oz : nb == -2 ? -1 : R.find(ix + ox, iy + oy, iz + oz);
       fb[k] = bi < 0 ? 1.0f : HVox<HF>::load(s.hsdf, (unsigned)bi);
       const float3 dd = f3(ox ? nc.x : cf.x, oy ? nc.y : cf.y, oz ? nc.z : cf.z);
       const float cd = sqrtf(dot3(dd, dd));
@@ -601,36 +641,58 @@ __global__ void __launch_bounds__(128) k_hash_raycast(const SessionDesc* __restr
     pr = add3(pr, mul3(dir, stepLen));
     vout = w0(mul3(pr, s.voxel));
     float p1, p2, v1;
+    const int n2 = R.near_base(ix, iy, iz, -1, 2);
     float3 g;
     p1 = fb[0] * nc.y * nc.z + fb[2] * cf.y * nc.z + fb[4] * nc.y * cf.z + fb[6] * cf.y * cf.z;
-    p2 = R.sdf_at(ix - 1, iy, iz) * nc.y * nc.z + R.sdf_at(ix - 1, iy + 1, iz) * cf.y * nc.z +
-         R.sdf_at(ix - 1, iy, iz + 1) * nc.y * cf.z + R.sdf_at(ix - 1, iy + 1, iz + 1) * cf.y * cf.z;
+    p2 = R.near(n2, ix, iy, iz, -1, 0, 0) * nc.y * nc.z + R.near(n2, ix, iy, iz, -1, +1, 0) * cf.y * nc.z +
+         R.near(n2, ix, iy, iz, -1, 0, +1) * nc.y * cf.z + R.near(n2, ix, iy, iz, -1, +1, +1) * cf.y * cf.z;
     v1 = p1 * cf.x + p2 * nc.x;
     p1 = fb[1] * nc.y * nc.z + fb[3] * cf.y * nc.z + fb[5] * nc.y * cf.z + fb[7] * cf.y * cf.z;
-    p2 = R.sdf_at(ix + 2, iy, iz) * nc.y * nc.z + R.sdf_at(ix + 2, iy + 1, iz) * cf.y * nc.z +
-         R.sdf_at(ix + 2, iy, iz + 1) * nc.y * cf.z + R.sdf_at(ix + 2, iy + 1, iz + 1) * cf.y * cf.z;
+    p2 = R.near(n2, ix, iy, iz, +2, 0, 0) * nc.y * nc.z + R.near(n2, ix, iy, iz, +2, +1, 0) * cf.y * nc.z +
+         R.near(n2, ix, iy, iz, +2, 0, +1) * nc.y * cf.z + R.near(n2, ix, iy, iz, +2, +1, +1) * cf.y * cf.z;
     g.x = p1 * nc.x + p2 * cf.x - v1;
     p1 = fb[0] * nc.x * nc.z + fb[1] * cf.x * nc.z + fb[4] * nc.x * cf.z + fb[5] * cf.x * cf.z;
-    p2 = R.sdf_at(ix, iy - 1, iz) * nc.x * nc.z + R.sdf_at(ix + 1, iy - 1, iz) * cf.x * nc.z +
-         R.sdf_at(ix, iy - 1, iz + 1) * nc.x * cf.z + R.sdf_at(ix + 1, iy - 1, iz + 1) * cf.x * cf.z;
+    p2 = R.near(n2, ix, iy, iz, 0, -1, 0) * nc.x * nc.z + R.near(n2, ix, iy, iz, +1, -1, 0) * cf.x * nc.z +
+         R.near(n2, ix, iy, iz, 0, -1, +1) * nc.x * cf.z + R.near(n2, ix, iy, iz, +1, -1, +1) * cf.x * cf.z;
     v1 = p1 * cf.y + p2 * nc.y;
     p1 = fb[2] * nc.x * nc.z + fb[3] * cf.x * nc.z + fb[6] * nc.x * cf.z + fb[7] * cf.x * cf.z;
-    p2 = R.sdf_at(ix, iy + 2, iz) * nc.x * nc.z + R.sdf_at(ix + 1, iy + 2, iz) * cf.x * nc.z +
-         R.sdf_at(ix, iy + 2, iz + 1) * nc.x * cf.z + R.sdf_at(ix + 1, iy + 2, iz + 1) * cf.x * cf.z;
+    p2 = R.near(n2, ix, iy, iz, 0, +2, 0) * nc.x * nc.z + R.near(n2, ix, iy, iz, +1, +2, 0) * cf.x * nc.z +
+         R.near(n2, ix, iy, iz, 0, +2, +1) * nc.x * cf.z + R.near(n2, ix, iy, iz, +1, +2, +1) * cf.x * cf.z;
     g.y = p1 * nc.y + p2 * cf.y - v1;
     p1 = fb[0] * nc.x * nc.y + fb[1] * cf.x * nc.y + fb[2] * nc.x * cf.y + fb[3] * cf.x * cf.y;
-    p2 = R.sdf_at(ix, iy, iz - 1) * nc.x * nc.y + R.sdf_at(ix + 1, iy, iz - 1) * cf.x * nc.y +
-         R.sdf_at(ix, iy + 1, iz - 1) * nc.x * cf.y + R.sdf_at(ix + 1, iy + 1, iz - 1) * cf.x * cf.y;
+    p2 = R.near(n2, ix, iy, iz, 0, 0, -1) * nc.x * nc.y + R.near(n2, ix, iy, iz, +1, 0, -1) * cf.x * nc.y +
+         R.near(n2, ix, iy, iz, 0, +1, -1) * nc.x * cf.y + R.near(n2, ix, iy, iz, +1, +1, -1) * cf.x * cf.y;
     v1 = p1 * cf.z + p2 * nc.z;
     p1 = fb[4] * nc.x * nc.y + fb[5] * cf.x * nc.y + fb[6] * nc.x * cf.y + fb[7] * cf.x * cf.y;
-    p2 = R.sdf_at(ix, iy, iz + 2) * nc.x * nc.y + R.sdf_at(ix + 1, iy, iz + 2) * cf.x * nc.y +
-         R.sdf_at(ix, iy + 1, iz + 2) * nc.x * cf.y + R.sdf_at(ix + 1, iy + 1, iz + 2) * cf.x * cf.y;
+    p2 = R.near(n2, ix, iy, iz, 0, 0, +2) * nc.x * nc.y + R.near(n2, ix, iy, iz, +1, 0, +2) * cf.x * nc.y +
+         R.near(n2, ix, iy, iz, 0, +1, +2) * nc.x * cf.y + R.near(n2, ix, iy, iz, +1, +1, +2) * cf.x * cf.y;
     g.z = p1 * nc.z + p2 * cf.z - v1;
     nout = w0(normalize3(g));
   }
   s.vref[pid] = vout;
   s.nref[pid] = nout;
   if (s.cmap) s.cmap[pid] = col;
+}
+
+template <int HF>
+__global__ void __launch_bounds__(128) k_hash_raycast(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!s.hash || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
+  // a block shades 16 x 8 pixels, each warp an 8 x 4 tile (neighbouring rays march alike)
+  const int tiles_x = (s.W + 15) >> 4;
+  if ((int)blockIdx.x >= tiles_x * ((s.H + 7) >> 3)) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int px = ((int)blockIdx.x % tiles_x) * 16 + (warp & 1) * 8 + (lane & 7);
+  const int py = ((int)blockIdx.x / tiles_x) * 8 + (warp >> 1) * 4 + (lane >> 3);
+  if (px >= s.W || py >= s.H) return;
+  const int pid = py * s.W + px;
+  HashRead<HF> R{s, 0, 0, 0, -1};
+  const float stepScale = s.mu * (1.0f / s.voxel) * 0.6f;
+  float3 pr, dir;
+  float total, totalMax, sdfv = 1.0f;
+  hash_ray<HF>(s, pid, pr, total, totalMax, dir);
+  hash_march<HF>(R, s, pr, total, totalMax, dir, stepScale, sdfv);
+  hash_finish<HF>(R, s, pid, pr, dir, stepScale, sdfv);
 }
 
 template __global__ void k_hash_integrate<0>(const SessionDesc*);

@@ -83,7 +83,7 @@ nui_status fail(nui_status st, const std::string& msg) {
     if (e_ != cudaSuccess) return fail(NUI_ERR_DEVICE, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
-constexpr int kStages = 6;
+constexpr int kStages = 7;  // 6 stage intervals and the whole tick
 constexpr int kZChunkTargetThreads = 1 << 18;
 constexpr size_t kMaxGraphs = 64;  // captured tick graphs kept per context
 }  // namespace
@@ -111,7 +111,7 @@ struct nui_ctx {
   int device = 0;
   cudaStream_t own = nullptr, stream = nullptr;
   bool timing = false;
-  cudaEvent_t ev[kStages + 1] = {};
+  cudaEvent_t ev[kStages] = {};
   float stage_ms[kStages] = {};
   // batch table (device + pinned staging) and per-session outputs (status + pose)
   int cap = 0;
@@ -124,7 +124,12 @@ struct nui_ctx {
   // scratch descriptor for kernel-level calls
   SessionDesc* d_kdesc = nullptr;
   TrackState* d_kts = nullptr;
-  std::map<BatchPlan, cudaGraphExec_t> graphs;
+  struct Graph {
+    cudaGraphExec_t exec;
+    int kernels;  // kernel launches per replay
+  };
+  std::map<BatchPlan, Graph> graphs;
+  int last_kernels = 0;  // kernels of the last graphed tick
 };
 
 struct nui_session {
@@ -168,6 +173,7 @@ struct nui_session {
   unsigned long long* keys = nullptr;
   unsigned* blk = nullptr;
   float2* range = nullptr;  // one-entry table for the per-session path
+
   long frames = 0;
   bool color_frame = false;
   std::vector<void*> allocs;
@@ -328,6 +334,23 @@ void plan_add(BatchPlan& p, const nui_session* s) {
   p.maxHyper = std::max(p.maxHyper, nh);
 }
 
+// Elementwise maximum of two launch shapes (n stays a's).
+void plan_merge(BatchPlan& a, const BatchPlan& b) {
+  a.maxW = std::max(a.maxW, b.maxW);
+  a.maxH = std::max(a.maxH, b.maxH);
+  a.maxLevels = std::max(a.maxLevels, b.maxLevels);
+  for (int l = 0; l < kMaxLevels; ++l) a.maxIters[l] = std::max(a.maxIters[l], b.maxIters[l]);
+  for (int f = 0; f < 4; ++f) {
+    a.maxIntegThreads[f] = std::max(a.maxIntegThreads[f], b.maxIntegThreads[f]);
+    a.maxBricks[f] = std::max(a.maxBricks[f], b.maxBricks[f]);
+  }
+  a.maxHyper = std::max(a.maxHyper, b.maxHyper);
+  a.maxHashBlk = std::max(a.maxHashBlk, b.maxHashBlk);
+  a.hashMask |= b.hashMask;
+  a.fmtMask |= b.fmtMask;
+  a.colorIcp |= b.colorIcp;
+}
+
 unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
 
 // zchunks per session: threads per launch >= 2^18, every chunk >= 16 slices
@@ -384,9 +407,9 @@ void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t 
   if (!p.hashMask) return;
   k_hash_range<<<dim3(296, p.n), 256, 0, st>>>(d);
   k_hash_project<<<dim3(296, p.n), 128, 0, st>>>(d);
-  const unsigned pix = cdiv((long)p.maxW * p.maxH, 128);
-  if (p.hashMask & 1) k_hash_raycast<0><<<dim3(pix, p.n), 128, 0, st>>>(d);
-  if (p.hashMask & 2) k_hash_raycast<1><<<dim3(pix, p.n), 128, 0, st>>>(d);
+  const unsigned tiles = cdiv(p.maxW, 16) * cdiv(p.maxH, 8);
+  if (p.hashMask & 1) k_hash_raycast<0><<<dim3(tiles, p.n), 128, 0, st>>>(d);
+  if (p.hashMask & 2) k_hash_raycast<1><<<dim3(tiles, p.n), 128, 0, st>>>(d);
 }
 
 // Colour pyramid (if any session tracks with colour), the ICP iterations of every level,
@@ -424,22 +447,23 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
   launch_integrate<1>(p, d, st);
   launch_integrate<2>(p, d, st);
   launch_integrate<3>(p, d, st);
+  mark(4);
   launch_summaries(p, d, st, 0);
   launch_hash_integrate(p, d, st);
-  mark(4);
+  mark(5);
   launch_raycast<0>(p, d, st);
   launch_raycast<1>(p, d, st);
   launch_raycast<2>(p, d, st);
   launch_raycast<3>(p, d, st);
   launch_hash_raycast(p, d, st);
-  mark(5);
+  mark(6);
 }
 
 nui_status ensure_cap(nui_ctx* ctx, int n) {
   if (n <= ctx->cap) return NUI_OK;
   int cap = std::max(n, std::max(64, ctx->cap * 2));
   cudaStreamSynchronize(ctx->stream);
-  for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second.exec);
   ctx->graphs.clear();
   cudaFree(ctx->d_descs);
   cudaFreeHost(ctx->h_descs);
@@ -459,47 +483,65 @@ nui_status ensure_cap(nui_ctx* ctx, int n) {
 
 nui_status finish_timing(nui_ctx* ctx) {
   if (!ctx->timing) return NUI_OK;
-  NUI_CUDA(cudaEventSynchronize(ctx->ev[5]));
-  for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ctx->stage_ms[i], ctx->ev[i], ctx->ev[i + 1]);
-  cudaEventElapsedTime(&ctx->stage_ms[5], ctx->ev[0], ctx->ev[5]);
+  NUI_CUDA(cudaEventSynchronize(ctx->ev[kStages - 1]));
+  for (int i = 0; i < kStages - 1; ++i) cudaEventElapsedTime(&ctx->stage_ms[i], ctx->ev[i], ctx->ev[i + 1]);
+  cudaEventElapsedTime(&ctx->stage_ms[kStages - 1], ctx->ev[0], ctx->ev[kStages - 1]);
   return NUI_OK;
 }
 
-// Runs one tick over sessions[0..n) whose frames are already in device memory at
-// raws[i]/bgras[i].  use_graph: replay a captured graph for this batch shape.
 // Launches one batched tick on the context stream (asynchronous).  raws[i] == nullptr
 // leaves session i out of this tick (inactive: every kernel skips it), so that a batch
 // keeps its shape -- and its captured graph -- while some sessions have no frame.
+// A null session is an empty slot: an inactive descriptor without buffers.  `floor`
+// (nullable) is merged into the launch shape, so that a caller can keep one shape -- and
+// its graph -- while sessions come and go.
 nui_status tick_launch(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t* const* raws,
-                       const uint8_t* const* bgras, bool use_graph) {
+                       const uint8_t* const* bgras, bool use_graph, const BatchPlan* floor) {
   nui_status st = ensure_cap(ctx, n);
   if (st != NUI_OK) return st;
   BatchPlan p;
   p.n = n;
   for (int i = 0; i < n; ++i) {
     nui_session* s = ss[i];
+    if (!s) {
+      std::memset(&ctx->h_descs[i], 0, sizeof(SessionDesc));
+      ctx->h_descs[i].kind = kInactive;
+      ctx->h_descs[i].fmt = -1;
+      continue;
+    }
     plan_add(p, s);
     int kind = !raws[i] ? kInactive : s->frames == 0 ? kFirstFrame : kTrackFrame;
     fill_desc(s, ctx->h_descs[i], kind, raws[i], bgras ? bgras[i] : nullptr);
   }
+  if (floor) plan_merge(p, *floor);
   NUI_CUDA(cudaMemcpyAsync(ctx->d_descs, ctx->h_descs, sizeof(SessionDesc) * n, cudaMemcpyHostToDevice, ctx->stream));
   if (use_graph && !ctx->timing) {
     auto it = ctx->graphs.find(p);
     if (it == ctx->graphs.end()) {
       if (ctx->graphs.size() >= kMaxGraphs) {  // bounded cache: start over
-        for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+        for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second.exec);
         ctx->graphs.clear();
       }
       cudaGraph_t g;
       NUI_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
       enqueue_tick(ctx, p, ctx->d_descs, ctx->d_pose, ctx->d_status, false);
       NUI_CUDA(cudaStreamEndCapture(ctx->stream, &g));
+      size_t nn = 0;
+      NUI_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+      std::vector<cudaGraphNode_t> nodes(nn);
+      NUI_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+      int kernels = 0;
+      for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType ty;
+        if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++kernels;
+      }
       cudaGraphExec_t ge;
       NUI_CUDA(cudaGraphInstantiate(&ge, g, 0));
       cudaGraphDestroy(g);
-      it = ctx->graphs.emplace(p, ge).first;
+      it = ctx->graphs.emplace(p, nui_ctx::Graph{ge, kernels}).first;
     }
-    NUI_CUDA(cudaGraphLaunch(it->second, ctx->stream));
+    ctx->last_kernels = it->second.kernels;
+    NUI_CUDA(cudaGraphLaunch(it->second.exec, ctx->stream));
   } else {
     enqueue_tick(ctx, p, ctx->d_descs, ctx->d_pose, ctx->d_status, ctx->timing);
     NUI_CUDA(cudaGetLastError());
@@ -518,7 +560,7 @@ nui_status tick_finish(nui_ctx* ctx, nui_session* const* ss, int n, const uint16
   nui_status agg = NUI_OK;
   for (int i = 0; i < n; ++i) {
     nui_session* s = ss[i];
-    if (!raws[i]) {
+    if (!s || !raws[i]) {
       if (per) per[i] = NUI_OK;
       continue;
     }
@@ -541,7 +583,7 @@ nui_status tick_finish(nui_ctx* ctx, nui_session* const* ss, int n, const uint16
 
 nui_status run_tick(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t* const* raws,
                     const uint8_t* const* bgras, bool use_graph, nui_status* per, float* poses) {
-  nui_status st = tick_launch(ctx, ss, n, raws, bgras, use_graph);
+  nui_status st = tick_launch(ctx, ss, n, raws, bgras, use_graph, nullptr);
   if (st != NUI_OK) return st;
   return tick_finish(ctx, ss, n, raws, per, poses);
 }
@@ -562,7 +604,9 @@ void launch_init(nui_session* s) {
   k_volume_init<F><<<dim3(1184, 1), 256, 0, s->ctx->stream>>>(s->d_desc1);
 }
 
-nui_status reset_session(nui_session* s) {
+// sync = false leaves the reset queued on the context stream (the host copies are staged
+// by the runtime before the calls return).
+nui_status reset_session(nui_session* s, bool sync = true) {
   SessionDesc d;
   fill_desc(s, d, kInactive, nullptr, nullptr);
   NUI_CUDA(cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, s->ctx->stream));
@@ -586,7 +630,7 @@ nui_status reset_session(nui_session* s) {
   std::memcpy(t.R, I, sizeof(I));
   std::memcpy(t.lastR, I, sizeof(I));
   NUI_CUDA(cudaMemcpyAsync(s->ts, &t, sizeof(t), cudaMemcpyHostToDevice, s->ctx->stream));
-  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  if (sync) NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
   NUI_CUDA(cudaGetLastError());
   s->frames = 0;
   return NUI_OK;
@@ -645,7 +689,7 @@ NUI_API nui_status nui_ctx_create(int device, nui_ctx** out) {
     return fail(NUI_ERR_DEVICE, cudaGetErrorString(e));
   }
   c->stream = c->own;
-  for (int i = 0; i <= kStages; ++i) cudaEventCreate(&c->ev[i]);
+  for (int i = 0; i < kStages; ++i) cudaEventCreate(&c->ev[i]);
   if (cudaMalloc(&c->d_kdesc, sizeof(SessionDesc)) != cudaSuccess ||
       cudaMalloc(&c->d_kts, sizeof(TrackState)) != cudaSuccess) {
     delete c;
@@ -659,8 +703,8 @@ NUI_API nui_status nui_ctx_destroy(nui_ctx* c) {
   if (!c) return NUI_OK;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
-  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
-  for (int i = 0; i <= kStages; ++i) cudaEventDestroy(c->ev[i]);
+  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
+  for (int i = 0; i < kStages; ++i) cudaEventDestroy(c->ev[i]);
   cudaFree(c->d_descs);
   cudaFreeHost(c->h_descs);
   cudaFree(c->d_pose);
@@ -678,7 +722,7 @@ NUI_API nui_status nui_ctx_set_stream(nui_ctx* c, void* stream) {
   if (!c) return fail(NUI_ERR_INVALID_ARG, "null context");
   NUI_CUDA(cudaStreamSynchronize(c->stream));
   c->stream = stream ? (cudaStream_t)stream : c->own;
-  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
   c->graphs.clear();
   return NUI_OK;
 }
@@ -692,6 +736,12 @@ NUI_API nui_status nui_ctx_synchronize(nui_ctx* c) {
 NUI_API nui_status nui_ctx_enable_timing(nui_ctx* c, int enable) {
   if (!c) return fail(NUI_ERR_INVALID_ARG, "null context");
   c->timing = enable != 0;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_ctx_last_tick_kernels(nui_ctx* c, int* n) {
+  if (!c || !n) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  *n = c->last_kernels;
   return NUI_OK;
 }
 
@@ -1477,6 +1527,12 @@ extern "C" NUI_API nui_status nui_mesh_device_noalloc(nui_session* s, float* d_p
 }
 
 // ------------------------------------------------------------------ serving loop
+// Every tick of the server covers all its slots (empty or idle ones sit out), with a
+// launch shape that only grows as streams of new kinds are admitted: the captured graph
+// of a tick is therefore reused while streams come and go.  Released sessions are kept
+// for the next stream of the same configuration (a reset instead of a free and an
+// allocation, which would synchronise the device); they are freed when a new stream
+// needs their memory.
 struct nui_server {
   struct Frame {
     const uint16_t* depth;
@@ -1490,17 +1546,24 @@ struct nui_server {
     std::deque<Frame> q;
     uint16_t* draw[2] = {nullptr, nullptr};  // device frame double buffer
     uint8_t* dbgra[2] = {nullptr, nullptr};
+    size_t cap_px = 0;                       // pixels the buffers hold
+    bool cap_bgra = false;
     int buf = 0;
   };
+  struct Pooled {
+    nui_session* s;
+    size_t bytes;
+  };
   nui_ctx* ctx = nullptr;
-  size_t budget = 0, used = 0;
+  size_t budget = 0, used = 0;  // live and pooled sessions
   cudaStream_t up = nullptr;
   cudaEvent_t ev_t0 = nullptr, ev_up = nullptr, ev_done = nullptr;
   std::chrono::steady_clock::time_point t0;
   std::vector<Slot> slots;
-  // the batch in flight: every live slot, with the frame it got (or none)
+  std::vector<Pooled> pool;
+  BatchPlan floor;
+  // the batch in flight: every slot, with its session and frame (or none)
   bool inflight = false;
-  std::vector<int> bslot;
   std::vector<nui_session*> bsess;
   std::vector<const uint16_t*> braw;
   std::vector<const uint8_t*> bbgra;
@@ -1523,9 +1586,9 @@ nui_status server_collect(nui_server* v) {
   nui_status st = tick_finish(v->ctx, v->bsess.data(), n, v->braw.data(), per.data(), poses.data());
   if (st != NUI_OK && st != NUI_ERR_TRACKING_LOST) return st;
   for (int i = 0; i < n; ++i) {
-    if (!v->braw[i]) continue;
+    if (!v->bsess[i] || !v->braw[i]) continue;
     nui_server_result r;
-    r.slot = v->bslot[i];
+    r.slot = i;
     r.status = per[i];
     r.tag = v->bframe[i].tag;
     r.t_submit = v->bframe[i].t_submit;
@@ -1535,17 +1598,29 @@ nui_status server_collect(nui_server* v) {
   }
   return NUI_OK;
 }
+
+void server_free_slot_buffers(nui_server::Slot& sl) {
+  for (int b = 0; b < 2; ++b) {
+    cudaFree(sl.draw[b]);
+    cudaFree(sl.dbgra[b]);
+    sl.draw[b] = nullptr;
+    sl.dbgra[b] = nullptr;
+  }
+  sl.cap_px = 0;
+  sl.cap_bgra = false;
+}
 }  // namespace
 
 extern "C" {
 
 NUI_API nui_status nui_server_create(nui_ctx* ctx, size_t budget, int max_streams, nui_server** out) {
-  if (!ctx || !out || max_streams <= 0) return fail(NUI_ERR_INVALID_ARG, "bad argument");
+  if (!ctx || !out || max_streams <= 0 || max_streams > 4096) return fail(NUI_ERR_INVALID_ARG, "bad argument");
   NUI_CUDA(cudaSetDevice(ctx->device));
   nui_server* v = new nui_server();
   v->ctx = ctx;
   v->budget = budget;
   v->slots.resize(max_streams);
+  v->floor.n = max_streams;
   if (cudaStreamCreateWithFlags(&v->up, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&v->ev_t0) != cudaSuccess || cudaEventCreateWithFlags(&v->ev_up, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&v->ev_done) != cudaSuccess) {
@@ -1564,8 +1639,12 @@ NUI_API nui_status nui_server_create(nui_ctx* ctx, size_t budget, int max_stream
 NUI_API nui_status nui_server_destroy(nui_server* v) {
   if (!v) return NUI_OK;
   server_collect(v);
-  for (int i = 0; i < (int)v->slots.size(); ++i)
-    if (v->slots[i].s) nui_server_release(v, i);
+  cudaStreamSynchronize(v->up);
+  for (auto& sl : v->slots) {
+    if (sl.s) nui_session_destroy(sl.s);
+    server_free_slot_buffers(sl);
+  }
+  for (auto& p : v->pool) nui_session_destroy(p.s);
   cudaStreamDestroy(v->up);
   cudaEventDestroy(v->ev_t0);
   cudaEventDestroy(v->ev_up);
@@ -1578,64 +1657,89 @@ NUI_API double nui_server_clock(const nui_server* v) { return v ? v->now() : 0.0
 
 NUI_API nui_status nui_server_admit(nui_server* v, const nui_session_cfg* cfg, int* slot) {
   if (!v || !cfg || !slot) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  std::string why;
+  if (!cfg_valid(cfg, why)) return fail(NUI_ERR_INVALID_ARG, why);
   const size_t need = nui_session_device_bytes(cfg) + (size_t)cfg->width * cfg->height * 12;
-  if (need == (size_t)cfg->width * cfg->height * 12) {
-    std::string why;
-    cfg_valid(cfg, why);
-    return fail(NUI_ERR_INVALID_ARG, why);
-  }
-  if (v->used + need > v->budget) return fail(NUI_ERR_OOM, "stream does not fit in the HBM budget");
   int k = -1;
   for (int i = 0; i < (int)v->slots.size() && k < 0; ++i)
     if (!v->slots[i].s) k = i;
   if (k < 0) return fail(NUI_ERR_OOM, "no free stream slot");
+  // a pooled session of the same configuration, else room for a new one
   nui_session* s = nullptr;
-  nui_status st = nui_session_create(v->ctx, cfg, &s);
-  if (st != NUI_OK) return st;
+  size_t bytes = need;
+  for (size_t i = 0; i < v->pool.size() && !s; ++i)
+    if (std::memcmp(&v->pool[i].s->cfg, cfg, sizeof(nui_session_cfg)) == 0) {
+      s = v->pool[i].s;
+      bytes = v->pool[i].bytes;
+      v->pool.erase(v->pool.begin() + i);
+      nui_status st = reset_session(s, false);  // queued behind the batch in flight
+      if (st != NUI_OK) return st;
+    }
+  if (!s) {
+    while (v->used + need > v->budget && !v->pool.empty()) {
+      nui_session_destroy(v->pool.front().s);
+      v->used -= v->pool.front().bytes;
+      v->pool.erase(v->pool.begin());
+    }
+    if (v->used + need > v->budget) return fail(NUI_ERR_OOM, "stream does not fit in the HBM budget");
+    nui_status st = nui_session_create(v->ctx, cfg, &s);
+    if (st != NUI_OK) return st;
+    v->used += need;
+  }
   nui_server::Slot& sl = v->slots[k];
   const size_t N = (size_t)cfg->width * cfg->height;
-  bool ok = true;
-  for (int b = 0; b < 2 && ok; ++b) {
-    ok = cudaMalloc(&sl.draw[b], N * 2) == cudaSuccess;
-    if (ok && s->cmap) ok = cudaMalloc(&sl.dbgra[b], N * 4) == cudaSuccess;
-  }
-  if (!ok) {
-    for (int b = 0; b < 2; ++b) {
-      cudaFree(sl.draw[b]);
-      cudaFree(sl.dbgra[b]);
-      sl.draw[b] = nullptr;
-      sl.dbgra[b] = nullptr;
+  const bool col = s->cmap != nullptr;
+  if (sl.cap_px < N || (col && !sl.cap_bgra)) {
+    cudaStreamSynchronize(v->up);
+    server_free_slot_buffers(sl);
+    bool ok = true;
+    for (int b = 0; b < 2 && ok; ++b) {
+      ok = cudaMalloc(&sl.draw[b], N * 2) == cudaSuccess;
+      if (ok && col) ok = cudaMalloc(&sl.dbgra[b], N * 4) == cudaSuccess;
     }
-    nui_session_destroy(s);
-    return fail(NUI_ERR_OOM, "device allocation failed");
+    if (!ok) {
+      server_free_slot_buffers(sl);
+      v->pool.push_back(nui_server::Pooled{s, bytes});
+      return fail(NUI_ERR_OOM, "device allocation failed");
+    }
+    sl.cap_px = N;
+    sl.cap_bgra = col;
   }
   sl.s = s;
-  sl.bytes = need;
+  sl.bytes = bytes;
   sl.buf = 0;
   sl.q.clear();
-  v->used += need;
+  plan_add(v->floor, s);
   *slot = k;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_server_reserve(nui_server* v, const nui_session_cfg* cfg, int count) {
+  if (!v || !cfg || count < 0) return fail(NUI_ERR_INVALID_ARG, "bad argument");
+  std::string why;
+  if (!cfg_valid(cfg, why)) return fail(NUI_ERR_INVALID_ARG, why);
+  const size_t need = nui_session_device_bytes(cfg) + (size_t)cfg->width * cfg->height * 12;
+  for (int i = 0; i < count; ++i) {
+    if (v->used + need > v->budget) return fail(NUI_ERR_OOM, "reservation does not fit in the HBM budget");
+    nui_session* s = nullptr;
+    nui_status st = nui_session_create(v->ctx, cfg, &s);
+    if (st != NUI_OK) return st;
+    v->used += need;
+    v->pool.push_back(nui_server::Pooled{s, need});
+  }
   return NUI_OK;
 }
 
 NUI_API nui_status nui_server_release(nui_server* v, int slot) {
   if (!v || slot < 0 || slot >= (int)v->slots.size() || !v->slots[slot].s) return fail(NUI_ERR_INVALID_ARG, "bad slot");
-  if (v->inflight && std::find(v->bslot.begin(), v->bslot.end(), slot) != v->bslot.end()) {
+  if (v->inflight && v->bsess[slot]) {
     nui_status st = server_collect(v);
     if (st != NUI_OK) return st;
   }
-  NUI_CUDA(cudaStreamSynchronize(v->up));
   nui_server::Slot& sl = v->slots[slot];
-  for (int b = 0; b < 2; ++b) {
-    cudaFree(sl.draw[b]);
-    cudaFree(sl.dbgra[b]);
-    sl.draw[b] = nullptr;
-    sl.dbgra[b] = nullptr;
-  }
-  nui_session_destroy(sl.s);
+  v->pool.push_back(nui_server::Pooled{sl.s, sl.bytes});  // kept for the next stream like it
   sl.s = nullptr;
   sl.q.clear();
-  v->used -= sl.bytes;
   sl.bytes = 0;
   return NUI_OK;
 }
@@ -1650,38 +1754,30 @@ NUI_API nui_status nui_server_submit(nui_server* v, int slot, const uint16_t* de
 
 NUI_API nui_status nui_server_step(nui_server* v, int* launched) {
   if (!v) return fail(NUI_ERR_INVALID_ARG, "null server");
-  // the next batch: every live stream, with its oldest queued frame if it has one
-  std::vector<int> nslot;
-  std::vector<nui_session*> nsess;
-  std::vector<const uint16_t*> nraw;
-  std::vector<const uint8_t*> nbgra;
-  std::vector<nui_server::Frame> nframe;
+  const int ns = (int)v->slots.size();
+  // the next batch: every slot, with the oldest queued frame of its stream if it has one
+  std::vector<nui_session*> nsess(ns, nullptr);
+  std::vector<const uint16_t*> nraw(ns, nullptr);
+  std::vector<const uint8_t*> nbgra(ns, nullptr);
+  std::vector<nui_server::Frame> nframe(ns, nui_server::Frame{nullptr, nullptr, 0, 0.0});
   int count = 0;
-  for (int i = 0; i < (int)v->slots.size(); ++i) {
+  for (int i = 0; i < ns; ++i) {
     nui_server::Slot& sl = v->slots[i];
     if (!sl.s) continue;
-    nslot.push_back(i);
-    nsess.push_back(sl.s);
-    if (sl.q.empty()) {
-      nraw.push_back(nullptr);
-      nbgra.push_back(nullptr);
-      nframe.push_back(nui_server::Frame{nullptr, nullptr, 0, 0.0});
-      continue;
-    }
+    nsess[i] = sl.s;
+    if (sl.q.empty()) continue;
     nui_server::Frame f = sl.q.front();
     sl.q.pop_front();
     const int b = sl.buf ^ 1;  // the buffer the batch in flight does not read
     sl.buf = b;
     const size_t N = (size_t)sl.s->cfg.width * sl.s->cfg.height;
     NUI_CUDA(cudaMemcpyAsync(sl.draw[b], f.depth, N * 2, cudaMemcpyHostToDevice, v->up));
-    const uint8_t* db = nullptr;
     if (f.bgra && sl.dbgra[b]) {
       NUI_CUDA(cudaMemcpyAsync(sl.dbgra[b], f.bgra, N * 4, cudaMemcpyHostToDevice, v->up));
-      db = sl.dbgra[b];
+      nbgra[i] = sl.dbgra[b];
     }
-    nraw.push_back(sl.draw[b]);
-    nbgra.push_back(db);
-    nframe.push_back(f);
+    nraw[i] = sl.draw[b];
+    nframe[i] = f;
     ++count;
   }
   NUI_CUDA(cudaEventRecord(v->ev_up, v->up));
@@ -1691,10 +1787,9 @@ NUI_API nui_status nui_server_step(nui_server* v, int* launched) {
   if (launched) *launched = count;
   if (count == 0) return NUI_OK;
   NUI_CUDA(cudaStreamWaitEvent(v->ctx->stream, v->ev_up, 0));
-  st = tick_launch(v->ctx, nsess.data(), (int)nsess.size(), nraw.data(), nbgra.data(), true);
+  st = tick_launch(v->ctx, nsess.data(), ns, nraw.data(), nbgra.data(), true, &v->floor);
   if (st != NUI_OK) return st;
   NUI_CUDA(cudaEventRecord(v->ev_done, v->ctx->stream));
-  v->bslot.swap(nslot);
   v->bsess.swap(nsess);
   v->braw.swap(nraw);
   v->bbgra.swap(nbgra);
