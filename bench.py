@@ -347,8 +347,12 @@ def serving_sim(L, ctx, host_frames, seconds, n_target, warm=2.0, seed=11):
 
     waits = []
 
+    admit_ms = []
+
     def try_admit(st, now):
+        a0 = time.perf_counter()
         sl = srv.admit(st["cfg"])
+        admit_ms.append((time.perf_counter() - a0) * 1e3)
         if sl is None:
             return False
         st["slot"] = sl
@@ -357,19 +361,23 @@ def serving_sim(L, ctx, host_frames, seconds, n_target, warm=2.0, seed=11):
         live[sl] = st
         return True
 
+    start = srv.clock()
+    for _ in range(n_target):
+        try_admit(new_stream(start), start)
     # warm pool: idle sessions of every stream configuration for the arrivals to come
     kinds = {}
     for i in range(15):
         c = stream_cfg(L, i, L.TSDF_F16_U8, L.TSDF_F16_U8)
         kinds[bytes(c)] = c
     for c in kinds.values():
-        srv.reserve(c, 4)
+        srv.reserve(c, 8)
     start = srv.clock()
-    for _ in range(n_target):
-        try_admit(new_stream(start), start)
+    for st in live.values():
+        st["next"] = start + rng.uniform(0, 1 / 30.0)
     t_end = start + warm + seconds
     next_arrival = start + rng.exponential(1 / lam)
     conc = []
+    step_ms = []
     steps = 0
     while True:
         now = srv.clock()
@@ -386,7 +394,9 @@ def serving_sim(L, ctx, host_frames, seconds, n_target, warm=2.0, seed=11):
                 srv.submit(st["slot"], fr, tag=st["sent"], t_submit=st["next"])
                 st["sent"] += 1
                 st["next"] += 1 / 30.0 + rng.uniform(-0.003, 0.003)
+        s0 = time.perf_counter()
         launched = srv.step()
+        step_ms.append((time.perf_counter() - s0) * 1e3)
         steps += 1
         for r in srv.poll():
             st = live[r.slot]
@@ -409,7 +419,10 @@ def serving_sim(L, ctx, host_frames, seconds, n_target, warm=2.0, seed=11):
             "latency_p50_ms": round(float(np.percentile(lat, 50)), 3) if lat.size else None,
             "latency_p99_ms": round(float(np.percentile(lat, 99)), 3) if lat.size else None,
             "admission_wait_p99_ms": round(float(np.percentile(np.array(waits) * 1e3, 99)), 1) if waits else None,
-            "loop_steps": steps}
+            "loop_steps": steps, "step_ms_p99": round(float(np.percentile(step_ms, 99)), 2),
+            "step_ms_max": round(float(np.max(step_ms)), 2),
+            "admit_ms_max": round(float(np.max(admit_ms)), 2) if admit_ms else None,
+            "admissions_over_5ms": int(sum(a > 5 for a in admit_ms))}
 
 
 def profile_traffic(kernel):
@@ -429,7 +442,8 @@ def max_over_ranks(ms, world):
         return ms
     import torch
     import torch.distributed as dist
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

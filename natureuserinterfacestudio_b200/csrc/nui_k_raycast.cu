@@ -120,7 +120,9 @@ struct RayVol {
     gy = round_div(p.y, c1, i1);
     gz = round_div(p.z, c2, i2);
   }
-  __device__ float trilinear(float3 p) const {
+  // Out of line: called at eight places of the hit refinement, whose inlined copies
+  // overflow the instruction cache.
+  __device__ __noinline__ float trilinear(float3 p) const {
     int gx, gy, gz;
     voxel_of(p, gx, gy, gz);
     if (gx <= 0 || gx >= rx - 1) return qnan();
