@@ -675,7 +675,7 @@ __device__ __forceinline__ void hash_finish(HashRead<HF>& R, const SessionDesc& 
 }
 
 template <int HF>
-__global__ void __launch_bounds__(128) k_hash_raycast(const SessionDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(128, 8) k_hash_raycast(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (!s.hash || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
   // a block shades 16 x 8 pixels, each warp an 8 x 4 tile (neighbouring rays march alike)
