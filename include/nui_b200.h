@@ -307,7 +307,26 @@ NUI_API nui_status nui_k_feedback_maps(nui_ctx* ctx, const float* d_vertex4, int
 NUI_API nui_status nui_k_color_pyramid(nui_ctx* ctx, const uint8_t* d_bgra, int W, int H, int levels,
                                        uint8_t* const* d_levels, uint8_t* const* d_gx, uint8_t* const* d_gy);
 
-/* ---------------------------------------------------------------- synthetic input/* ---------------------------------------------------------------- synthetic input
+/* ---------------------------------------------------------------- recorded frames
+ * The reference's frame file format (NuiFileIOUtilities.cpp:13-161): int64 timestamp,
+ * uint32 width, uint32 height, uint32 stored size, then the raw pixels or -- when the
+ * stored size differs from width * height * pixel bytes -- their zlib stream
+ * (compress2 at Z_BEST_SPEED).  Camera files (.camIntri) hold fx, fy, cx, cy as floats.
+ * A recording is a directory of <n>.depth (uint16 mm), <n>.color (BGRA), <n>.camIntri,
+ * n = 0, 1, ... (NuiFrameLoader.cpp:26-92). */
+NUI_API nui_status nui_frame_file_write(const char* path, int compressed, int64_t timestamp, uint32_t width,
+                                        uint32_t height, const void* pixels, uint32_t pixel_bytes);
+NUI_API nui_status nui_frame_file_header(const char* path, int64_t* timestamp, uint32_t* width, uint32_t* height);
+NUI_API nui_status nui_frame_file_read(const char* path, void* pixels, uint32_t bytes);
+NUI_API nui_status nui_camera_file_write(const char* path, const float* fx_fy_cx_cy);
+NUI_API nui_status nui_camera_file_read(const char* path, float* fx_fy_cx_cy);
+/* Frame `index` of a recording: whichever of depth / colour / intrinsics the directory has
+ * and the caller asks for (null pointers skip); NUI_ERR_INVALID_ARG past the last frame or
+ * when the stored size is not width x height. */
+NUI_API nui_status nui_recording_frame(const char* dir, int index, uint16_t* depth_mm, uint8_t* bgra,
+                                       float* fx_fy_cx_cy, int64_t* timestamp, uint32_t width, uint32_t height);
+
+/* ---------------------------------------------------------------- synthetic input
  * Seeded analytic scenes and trajectories standing in for recorded Kinect sessions. */
 typedef struct nui_synth_scene nui_synth_scene;
 enum { NUI_SYNTH_TABLETOP = 0, NUI_SYNTH_ROOM = 1 };

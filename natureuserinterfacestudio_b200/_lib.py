@@ -102,6 +102,12 @@ _SIGS = {
     "nui_k_preprocess": (C.c_int, [_P, _P, C.c_int, C.c_int] + [C.c_float] * 6 + [C.c_int] + [C.c_float] * 3 + [_P, _P, _P]),
     "nui_k_pyramid_level": (C.c_int, [_P, _P, C.c_int, C.c_int] + [C.c_float] * 4 + [C.c_int, C.c_float, _P, _P]),
     "nui_k_feedback_maps": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_float, _P, _P, _P]),
+    "nui_frame_file_write": (C.c_int, [C.c_char_p, C.c_int, C.c_int64, C.c_uint32, C.c_uint32, _P, C.c_uint32]),
+    "nui_frame_file_header": (C.c_int, [C.c_char_p, _P, _P, _P]),
+    "nui_frame_file_read": (C.c_int, [C.c_char_p, _P, C.c_uint32]),
+    "nui_camera_file_write": (C.c_int, [C.c_char_p, _P]),
+    "nui_camera_file_read": (C.c_int, [C.c_char_p, _P]),
+    "nui_recording_frame": (C.c_int, [C.c_char_p, C.c_int, _P, _P, _P, _P, C.c_uint32, C.c_uint32]),
     "nui_synth_scene_create": (_P, [C.c_int, C.c_uint64, C.c_float]),
     "nui_synth_scene_destroy": (None, [_P]),
     "nui_synth_scene_sdf": (C.c_float, [_P, C.c_float, C.c_float, C.c_float]),
@@ -471,3 +477,38 @@ class Server:
         used, ns, nq = C.c_size_t(), C.c_int(), C.c_int()
         check(lib().nui_server_stats(self.h, C.byref(used), C.byref(ns), C.byref(nq)))
         return used.value, ns.value, nq.value
+
+
+# ---------------------------------------------------------------- recorded frames
+def write_recording(directory, frames, intrinsics, compressed=True, t0=0, dt=33333):
+    """Writes frames [(depth uint16 HxW, bgra uint8 HxWx4 or None), ...] as a recording:
+    <n>.depth, <n>.color, <n>.camIntri (the reference's layout and file format)."""
+    os.makedirs(directory, exist_ok=True)
+    cam = np.asarray(intrinsics, np.float32)
+    for n, (d, c) in enumerate(frames):
+        base = os.path.join(directory, str(n)).encode()
+        d = np.ascontiguousarray(d, np.uint16)
+        H, W = d.shape
+        check(lib().nui_frame_file_write(base + b".depth", int(compressed), t0 + n * dt, W, H, ptr(d), 2))
+        if c is not None:
+            c = np.ascontiguousarray(c, np.uint8)
+            check(lib().nui_frame_file_write(base + b".color", int(compressed), t0 + n * dt, W, H, ptr(c), 4))
+        check(lib().nui_camera_file_write(base + b".camIntri", ptr(cam)))
+
+
+def read_recording(directory, width, height, color=True):
+    """Frames of a recording: [(depth, bgra or None, intrinsics[4], timestamp), ...]."""
+    out = []
+    n = 0
+    while True:
+        d = np.zeros((height, width), np.uint16)
+        c = np.zeros((height, width, 4), np.uint8) if color else None
+        cam = np.zeros(4, np.float32)
+        ts = C.c_int64()
+        r = lib().nui_recording_frame(directory.encode(), n, ptr(d), ptr(c), ptr(cam), C.byref(ts), width, height)
+        if r != NUI_OK:
+            break
+        has_c = color and os.path.exists(os.path.join(directory, "%d.color" % n))
+        out.append((d, c if has_c else None, cam, ts.value))
+        n += 1
+    return out
