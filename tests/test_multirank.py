@@ -32,7 +32,7 @@ def _rank(rank, world, port, out):
 
 def test_max_over_ranks_gloo_world2():
     world = 2
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.start_processes(_rank, args=(world, _free_port(), out), nprocs=world, start_method="spawn")
     assert out[0][0] == out[1][0] == pytest.approx(15.0)
