@@ -333,6 +333,8 @@ enum { NUI_SYNTH_TABLETOP = 0, NUI_SYNTH_ROOM = 1 };
 NUI_API nui_synth_scene* nui_synth_scene_create(int kind, uint64_t seed, float extent);
 NUI_API void nui_synth_scene_destroy(nui_synth_scene* s);
 NUI_API float nui_synth_scene_sdf(const nui_synth_scene* s, float x, float y, float z);
+/* The analytic signed distance at n points (xyz: 3n floats). */
+NUI_API void nui_synth_scene_sdf_many(const nui_synth_scene* s, const float* xyz, long n, float* out);
 NUI_API void nui_synth_trajectory(int kind, uint64_t seed, int frame, float radius, float deg_per_frame,
                                   float* R_out, float* t_out);
 NUI_API void nui_synth_render(const nui_synth_scene* s, const float* R, const float* t, int W, int H, float fx,

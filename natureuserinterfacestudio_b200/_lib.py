@@ -111,6 +111,7 @@ _SIGS = {
     "nui_synth_scene_create": (_P, [C.c_int, C.c_uint64, C.c_float]),
     "nui_synth_scene_destroy": (None, [_P]),
     "nui_synth_scene_sdf": (C.c_float, [_P, C.c_float, C.c_float, C.c_float]),
+    "nui_synth_scene_sdf_many": (None, [_P, _P, C.c_long, _P]),
     "nui_synth_trajectory": (None, [C.c_int, C.c_uint64, C.c_int, C.c_float, C.c_float, _P, _P]),
     "nui_synth_render": (None, [_P, _P, _P, C.c_int, C.c_int] + [C.c_float] * 4 + [C.c_uint64, C.c_int, C.c_int, _P, _P]),
 }
@@ -372,6 +373,12 @@ class SynthScene:
 
     def sdf(self, x, y, z):
         return lib().nui_synth_scene_sdf(self.h, x, y, z)
+
+    def sdf_many(self, xyz):
+        p = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+        out = np.zeros(len(p), np.float32)
+        lib().nui_synth_scene_sdf_many(self.h, ptr(p), len(p), ptr(out))
+        return out
 
     def pose(self, frame, radius=1.5, deg_per_frame=2.0, traj_seed=None):
         R = np.zeros(9, np.float32)

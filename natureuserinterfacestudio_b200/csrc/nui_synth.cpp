@@ -204,6 +204,11 @@ NUI_API float nui_synth_scene_sdf(const nui_synth_scene* s, float x, float y, fl
   return (float)scene_sdf(*s, v3(x, y, z));
 }
 
+NUI_API void nui_synth_scene_sdf_many(const nui_synth_scene* s, const float* xyz, long n, float* out) {
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; ++i) out[i] = (float)scene_sdf(*s, v3(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
+}
+
 // Camera-to-world pose (R row-major, t = camera centre) of `frame` on the scene's path.
 //  tabletop: orbit of radius `radius` around (0, 0, radius) starting at the origin looking
 //            down +z, deg_per_frame per frame, seeded jitter (1 mm, 0.2 deg, 1 sigma).
