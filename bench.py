@@ -169,6 +169,15 @@ def run_ours(args, rank, world):
     def hframe(i, step):
         return host_frames[i % nseq][pingpong(offs[i] + step)].numpy()
 
+    # ---------------------------------------------------------------- launch shapes
+    tuning, tune_s = None, 0.0
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        t, _ = ctx.autotune(cfgs, [[hframe(i, k) for k in range(4)] for i in range(n)], repeats=5)
+        tune_s = time.perf_counter() - t0
+        tuning = t.as_dict()
+        torch.cuda.empty_cache()
+
     # ---------------------------------------------------------------- value: device frames
     sessions = [L.Session(ctx, c) for c in cfgs]
     with ClockSampler(dev) as clk:
@@ -296,7 +305,8 @@ def run_ours(args, rank, world):
                        "dense": "FP16 TSDF + u8 weight, %s^3 round robin" % "/".join(map(str, VOLUMES)),
                        "hash": "5 mm voxels, 2^20 buckets, pools 2^19/2^20/2^21 blocks, half sdf + u8 weight",
                        "icp_iterations": [10, 5, 4], "l2": "inputs larger than L2 (volumes ~60 GB per GPU)",
-                       "graph": "one CUDA graph per tick"},
+                       "graph": "one CUDA graph per tick",
+                       "tuning": tuning, "autotune_s": round(tune_s, 2)},
             "latency_ms": {"tick_p50": round(float(np.percentile(lat_t, 50)), 3),
                            "tick_p99": round(float(np.percentile(lat_t, 99)), 3),
                            "e2e_p50": round(float(np.percentile(e2e_lat, 50)), 3),
@@ -496,6 +506,8 @@ def main():
     ap.add_argument("--serve-seconds", dest="serve_seconds", type=float, default=12.0)
     ap.add_argument("--no-plain", dest="plain", action="store_false")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", dest="no_autotune", action="store_true",
+                    help="keep the default launch shapes instead of timing the candidates first")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))

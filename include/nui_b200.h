@@ -262,7 +262,7 @@ NUI_API nui_status nui_server_poll(nui_server* srv, nui_server_result* out, int 
 NUI_API nui_status nui_server_stats(const nui_server* srv, size_t* bytes_used, int* streams, int* queued);
 NUI_API nui_session* nui_server_session(nui_server* srv, int slot);
 
-/* Per-stage device time of the last nui_batch_tick* / nui_process_frame* call of the/* Per-stage device time of the last nui_batch_tick* / nui_process_frame* call of the
+/* Per-stage device time of the last nui_batch_tick* / nui_process_frame* call of the
  * context, when timing is enabled (CUDA events on the context stream).
  * stage: 0 preprocess, 1 pyramid + feedback maps, 2 tracking (colour gradients, ICP, gate),
  * 3 dense integration kernel, 4 brick summaries + voxel-hash allocation / integration,
@@ -271,6 +271,36 @@ NUI_API nui_status nui_ctx_enable_timing(nui_ctx* ctx, int enable);
 NUI_API nui_status nui_ctx_stage_ms(nui_ctx* ctx, int stage, float* ms);
 /* Kernel launches in the captured graph of the context's last graphed batch tick. */
 NUI_API nui_status nui_ctx_last_tick_kernels(nui_ctx* ctx, int* n);
+/* Launch shapes of a context's tick, chosen by nui_ctx_autotune (or set by hand).  No
+ * choice changes a result bit except the ICP pixels per thread, which regroups the float
+ * partial sums of the normal equations (poses agree to the rounding of those sums).
+ *   integrate_threads_log2   dense integration: each volume column is split into z chunks,
+ *                            one thread each, until a session's launch has >= 2^this
+ *                            threads (chunks of >= 16 slices); 14..22, default 18
+ *   icp_pixels_per_thread    ICP block: 256 threads x this many pixels; 2, 4 or 8 (4)
+ *   raycast_tile_width       dense raycast: a warp shades a tile this wide and 32 / this
+ *                            high, a block 2 x 2 such tiles; 4, 8, 16 or 32 (8)
+ *   hash_raycast_tile_width  the same for the voxel-hash raycast (8)
+ * The reference fixes its work-group sizes per kernel in its OpenCL sources. */
+typedef struct nui_tuning {
+  int integrate_threads_log2;
+  int icp_pixels_per_thread;
+  int raycast_tile_width;
+  int hash_raycast_tile_width;
+} nui_tuning;
+NUI_API nui_status nui_ctx_get_tuning(nui_ctx* ctx, nui_tuning* out);
+NUI_API nui_status nui_ctx_set_tuning(nui_ctx* ctx, const nui_tuning* t);
+/* Autotuner: creates n scratch sessions of cfgs (device memory for all n at once), runs
+ * `frames` frames of each through batch ticks (frame f of session i: depth_mm[i * frames
+ * + f], host u16; bgra likewise or NULL), then times every candidate of each parameter in
+ * turn (coordinate descent: integration, ICP, dense raycast, hash raycast; parameters no
+ * session uses are skipped) as the median device time of its stage over `repeats` ticks,
+ * keeps the fastest in the context, frees the scratch sessions and reports the choice
+ * (out) and the whole-tick median with it (out_tick_ms, nullable).  Takes the context's
+ * stream for the whole call. */
+NUI_API nui_status nui_ctx_autotune(nui_ctx* ctx, const nui_session_cfg* cfgs, int n,
+                                    const uint16_t* const* depth_mm, const uint8_t* const* bgra, int frames,
+                                    int repeats, nui_tuning* out, float* out_tick_ms);
 /* Voxels read-modify-written by the last integration of a session. */
 NUI_API nui_status nui_session_touched_voxels(nui_session* s, uint64_t* n);
 

@@ -45,6 +45,17 @@ class SessionCfg(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    """Launch shapes of a context's tick (nui_tuning)."""
+    _fields_ = [
+        ("integrate_threads_log2", C.c_int), ("icp_pixels_per_thread", C.c_int),
+        ("raycast_tile_width", C.c_int), ("hash_raycast_tile_width", C.c_int),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class NuiError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__("nui status %d: %s" % (status, msg))
@@ -98,6 +109,9 @@ _SIGS = {
     "nui_ctx_enable_timing": (C.c_int, [_P, C.c_int]),
     "nui_ctx_stage_ms": (C.c_int, [_P, C.c_int, _P]),
     "nui_ctx_last_tick_kernels": (C.c_int, [_P, _P]),
+    "nui_ctx_get_tuning": (C.c_int, [_P, _P]),
+    "nui_ctx_set_tuning": (C.c_int, [_P, _P]),
+    "nui_ctx_autotune": (C.c_int, [_P, _P, C.c_int, _P, _P, C.c_int, C.c_int, _P, _P]),
     "nui_session_touched_voxels": (C.c_int, [_P, _P]),
     "nui_k_preprocess": (C.c_int, [_P, _P, C.c_int, C.c_int] + [C.c_float] * 6 + [C.c_int] + [C.c_float] * 3 + [_P, _P, _P]),
     "nui_k_pyramid_level": (C.c_int, [_P, _P, C.c_int, C.c_int] + [C.c_float] * 4 + [C.c_int, C.c_float, _P, _P]),
@@ -199,6 +213,36 @@ class Context:
         v = C.c_float()
         check(lib().nui_ctx_stage_ms(self.h, stage, C.byref(v)))
         return v.value
+
+    def tuning(self):
+        t = Tuning()
+        check(lib().nui_ctx_get_tuning(self.h, C.byref(t)))
+        return t
+
+    def set_tuning(self, t=None, **kw):
+        """Sets the launch shapes: a Tuning, or fields by keyword over the current ones."""
+        t = t or self.tuning()
+        for k, v in kw.items():
+            setattr(t, k, v)
+        check(lib().nui_ctx_set_tuning(self.h, C.byref(t)))
+
+    def autotune(self, cfgs, seqs, bgras=None, repeats=5):
+        """Times the launch-shape candidates on scratch sessions of cfgs fed seqs[i] (a
+        list of >= 2 uint16 depth frames per session, bgras likewise or None) and keeps
+        the fastest in the context.  Returns (Tuning, whole-tick median ms)."""
+        n, frames = len(cfgs), len(seqs[0])
+        assert all(len(q) == frames for q in seqs)
+        cf = (SessionCfg * n)(*cfgs)
+        keep = [np.ascontiguousarray(x) for q in seqs for x in q]
+        d = (C.c_void_p * (n * frames))(*[x.ctypes.data for x in keep])
+        b = None
+        if bgras is not None:
+            keepc = [np.ascontiguousarray(x) for q in bgras for x in q]
+            keep += keepc
+            b = (C.c_void_p * (n * frames))(*[x.ctypes.data for x in keepc])
+        t, ms = Tuning(), C.c_float()
+        check(lib().nui_ctx_autotune(self.h, cf, n, d, b, frames, repeats, C.byref(t), C.byref(ms)))
+        return t, ms.value
 
     def batch_tick(self, sessions, depths, bgras=None, device=False):
         """One frame for every session.  depths: list of uint16 arrays (host) or device

@@ -675,15 +675,17 @@ __device__ __forceinline__ void hash_finish(HashRead<HF>& R, const SessionDesc& 
 }
 
 template <int HF>
-__global__ void __launch_bounds__(128, 8) k_hash_raycast(const SessionDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(128, 8) k_hash_raycast(const SessionDesc* __restrict__ descs, int tw) {
   const SessionDesc& s = descs[blockIdx.y];
   if (!s.hash || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
-  // a block shades 16 x 8 pixels, each warp an 8 x 4 tile (neighbouring rays march alike)
-  const int tiles_x = (s.W + 15) >> 4;
-  if ((int)blockIdx.x >= tiles_x * ((s.H + 7) >> 3)) return;
+  // each warp shades a tw x (32 / tw) pixel tile, a block 2 x 2 of them (neighbouring rays
+  // march alike; tw is tuned)
+  const int th = 32 / tw, bw = 2 * tw, bh = 2 * th;
+  const int tiles_x = (s.W + bw - 1) / bw;
+  if ((int)blockIdx.x >= tiles_x * ((s.H + bh - 1) / bh)) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int px = ((int)blockIdx.x % tiles_x) * 16 + (warp & 1) * 8 + (lane & 7);
-  const int py = ((int)blockIdx.x / tiles_x) * 8 + (warp >> 1) * 4 + (lane >> 3);
+  const int px = ((int)blockIdx.x % tiles_x) * bw + (warp & 1) * tw + lane % tw;
+  const int py = ((int)blockIdx.x / tiles_x) * bh + (warp >> 1) * th + lane / tw;
   if (px >= s.W || py >= s.H) return;
   const int pid = py * s.W + px;
   HashRead<HF> R{s, 0, 0, 0, -1};
@@ -697,8 +699,8 @@ __global__ void __launch_bounds__(128, 8) k_hash_raycast(const SessionDesc* __re
 
 template __global__ void k_hash_integrate<0>(const SessionDesc*);
 template __global__ void k_hash_integrate<1>(const SessionDesc*);
-template __global__ void k_hash_raycast<0>(const SessionDesc*);
-template __global__ void k_hash_raycast<1>(const SessionDesc*);
+template __global__ void k_hash_raycast<0>(const SessionDesc*, int);
+template __global__ void k_hash_raycast<1>(const SessionDesc*, int);
 
 }  // namespace nui
 

@@ -14,8 +14,7 @@
 
 namespace nui {
 
-constexpr int kIcpThreads = 256;
-constexpr int kIcpPixPerThread = 4;
+constexpr int kIcpThreads = 256;  // pixels per thread: the template parameter PPT (tuned)
 
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
   s = a + b;
@@ -252,6 +251,7 @@ __device__ void icp_host_step(TrackState* ts, const double* sums, int iter, unsi
   for (int i = 0; i < 9; ++i) ts->R[i] = (float)Rn[i];
 }
 
+template <int PPT>
 __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restrict__ descs, int level, int iter) {
   const SessionDesc& s = descs[blockIdx.y];
   if (s.kind != kTrackFrame || level >= s.levels || iter >= s.iters[level]) return;
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
   if (ts->status != 0) return;
   if (iter > 0 && ts->level_done) return;
   const int w = s.W >> level, h = s.H >> level, n = w * h;
-  const int per_block = kIcpThreads * kIcpPixPerThread;
+  const int per_block = kIcpThreads * PPT;
   const int nblocks = (n + per_block - 1) / per_block;
   // colour tracking: at the finest level, blocks past the depth ones take the photometric
   // term over the full-size model maps
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
   if ((int)blockIdx.x >= nblocks) {
     const int cbase = ((int)blockIdx.x - nblocks) * per_block, NM = s.W * s.H;
 #pragma unroll 1
-    for (int k = 0; k < kIcpPixPerThread; ++k) {
+    for (int k = 0; k < PPT; ++k) {
       const int i = cbase + k * kIcpThreads + threadIdx.x;
       if (i >= NM) break;
       float c[kIcpTerms];
@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
   }
   const int base = blockIdx.x * per_block;
 #pragma unroll 1
-  for (int k = 0; k < kIcpPixPerThread && (int)blockIdx.x < nblocks; ++k) {
+  for (int k = 0; k < PPT && (int)blockIdx.x < nblocks; ++k) {
     const int i = base + k * kIcpThreads + threadIdx.x;
     if (i >= n) break;
     const float3 v = xyz(__ldg(V + i));
@@ -405,6 +405,10 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
     __threadfence();
   }
 }
+
+template __global__ void k_icp<2>(const SessionDesc*, int, int);
+template __global__ void k_icp<4>(const SessionDesc*, int, int);
+template __global__ void k_icp<8>(const SessionDesc*, int, int);
 
 // After the last ICP launch (or on frame 0): publish the pose, decide the integration
 // gate (NuiKinfuTrackingEngine.cpp:115-127) and reset the estimate for the next frame.

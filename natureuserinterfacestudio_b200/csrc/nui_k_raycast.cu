@@ -173,16 +173,18 @@ struct RayVol {
 };
 
 template <int FMT>
-__global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__ descs, int tw) {
   const SessionDesc& s = descs[blockIdx.y];
   if (s.kind != kTrackFrame || s.fmt != FMT || s.ts->status != 0) return;
-  // a block shades 16 x 8 pixels, each warp an 8 x 4 tile (neighbouring rays march alike)
+  // each warp shades a tw x (32 / tw) pixel tile, a block 2 x 2 of them (neighbouring rays
+  // march alike; tw is tuned)
   const int W = s.W, H = s.H;
-  const int tiles_x = (W + 15) >> 4;
-  if ((int)blockIdx.x >= tiles_x * ((H + 7) >> 3)) return;
+  const int th = 32 / tw, bw = 2 * tw, bh = 2 * th;
+  const int tiles_x = (W + bw - 1) / bw;
+  if ((int)blockIdx.x >= tiles_x * ((H + bh - 1) / bh)) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int px = ((int)blockIdx.x % tiles_x) * 16 + (warp & 1) * 8 + (lane & 7);
-  const int py = ((int)blockIdx.x / tiles_x) * 8 + (warp >> 1) * 4 + (lane >> 3);
+  const int px = ((int)blockIdx.x % tiles_x) * bw + (warp & 1) * tw + lane % tw;
+  const int py = ((int)blockIdx.x / tiles_x) * bh + (warp >> 1) * th + lane / tw;
   if (px >= W || py >= H) return;
   const int id = py * W + px;
   const float4 nanv = make_float4(qnan(), qnan(), qnan(), 0.f);
@@ -310,9 +312,9 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
   if (s.cmap) s.cmap[id] = cout;
 }
 
-template __global__ void k_raycast<0>(const SessionDesc*);
-template __global__ void k_raycast<1>(const SessionDesc*);
-template __global__ void k_raycast<2>(const SessionDesc*);
-template __global__ void k_raycast<3>(const SessionDesc*);
+template __global__ void k_raycast<0>(const SessionDesc*, int);
+template __global__ void k_raycast<1>(const SessionDesc*, int);
+template __global__ void k_raycast<2>(const SessionDesc*, int);
+template __global__ void k_raycast<3>(const SessionDesc*, int);
 
 }  // namespace nui

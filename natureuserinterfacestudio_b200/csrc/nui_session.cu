@@ -29,6 +29,7 @@ namespace nui {
 __global__ void k_preprocess(const SessionDesc*);
 __global__ void k_pyramid(const SessionDesc*, int);
 __global__ void k_feedback(const SessionDesc*);
+template <int PPT>
 __global__ void k_icp(const SessionDesc*, int, int);
 __global__ void k_track_finalize(const SessionDesc*);
 __global__ void k_ztab(const SessionDesc*);
@@ -43,7 +44,7 @@ template <int F>
 __global__ void k_brick_summary(const SessionDesc*, int);
 __global__ void k_super_summary(const SessionDesc*, int);
 template <int F>
-__global__ void k_raycast(const SessionDesc*);
+__global__ void k_raycast(const SessionDesc*, int);
 __global__ void k_publish(const SessionDesc*, int, float*, int*);
 __global__ void k_tick_begin(const SessionDesc*, int);
 __global__ void k_occ_clear(const SessionDesc*);
@@ -60,7 +61,7 @@ __global__ void k_hash_integrate(const SessionDesc*);
 __global__ void k_hash_range(const SessionDesc*);
 __global__ void k_hash_project(const SessionDesc*);
 template <int F>
-__global__ void k_hash_raycast(const SessionDesc*);
+__global__ void k_hash_raycast(const SessionDesc*, int);
 __global__ void k_hash_reset(const SessionDesc*);
 __global__ void k_hash_export_voxels(const SessionDesc*, uint8_t*);
 template <int F>
@@ -84,7 +85,7 @@ nui_status fail(nui_status st, const std::string& msg) {
   } while (0)
 
 constexpr int kStages = 7;  // 6 stage intervals and the whole tick
-constexpr int kZChunkTargetThreads = 1 << 18;
+constexpr int kMinIcpPpt = 2;  // smallest ICP pixels per thread: sizes the partial sums
 constexpr size_t kMaxGraphs = 64;  // captured tick graphs kept per context
 }  // namespace
 
@@ -103,6 +104,7 @@ struct BatchPlan {
   int hashMask;             // bit per hash sdf format
   int fmtMask;
   int colorIcp;             // some session tracks with the photometric term
+  nui_tuning tune;          // the context's launch shapes
   BatchPlan() { std::memset(this, 0, sizeof(*this)); }
   bool operator<(const BatchPlan& o) const { return std::memcmp(this, &o, sizeof(BatchPlan)) < 0; }
 };
@@ -130,6 +132,7 @@ struct nui_ctx {
   };
   std::map<BatchPlan, Graph> graphs;
   int last_kernels = 0;  // kernels of the last graphed tick
+  nui_tuning tune = {18, 4, 8, 8};
 };
 
 struct nui_session {
@@ -137,7 +140,6 @@ struct nui_session {
   nui_session_cfg cfg;
   DevCam cam;
   float cell[3], trunc;
-  int zchunks = 1;
   unsigned icp_min_count[kMaxLevels] = {0, 0, 0, 0};
   float gauss[2 * kMaxRadius + 1];
   uint16_t* raw = nullptr;
@@ -232,6 +234,14 @@ void icp_thresholds(const nui_session_cfg& c, unsigned* out) {
   }
 }
 
+// Integration z chunks of a volume: threads per launch >= 2^log2_threads, every chunk
+// >= 16 slices.  The chunking changes no result (every chunk replays its column's sums).
+int pick_zchunks(const nui_session_cfg& c, int log2_threads) {
+  const long ncol = (long)c.res[0] * c.res[1], target = 1L << log2_threads;
+  int z = (int)std::max(1L, (target + ncol - 1) / ncol);
+  return std::min(z, std::max(1, c.res[2] / 16));
+}
+
 void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* raw, const uint8_t* bgra) {
   std::memset(&d, 0, sizeof(d));
   const nui_session_cfg& c = s->cfg;
@@ -274,7 +284,7 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
   d.ztab = s->ztab;
   d.occ3 = s->occ3;
   d.max_cw = c.max_color_weight;
-  d.zchunks = s->zchunks;
+  d.zchunks = pick_zchunks(s->cfg, s->ctx->tune.integrate_threads_log2);
   d.ts = s->ts;
   d.partials = s->partials;
   // colour tracking runs on frames that carry colour, once its buffers exist
@@ -315,6 +325,7 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
 
 void plan_add(BatchPlan& p, const nui_session* s) {
   const nui_session_cfg& c = s->cfg;
+  p.tune = s->ctx->tune;
   p.maxW = std::max(p.maxW, c.width);
   p.maxH = std::max(p.maxH, c.height);
   p.maxLevels = std::max(p.maxLevels, c.levels);
@@ -325,7 +336,7 @@ void plan_add(BatchPlan& p, const nui_session* s) {
     p.maxHashBlk = std::max(p.maxHashBlk, ((long)c.hash_buckets + c.hash_excess + 1023) / 1024);
     return;
   }
-  long th = (long)c.res[0] * c.res[1] * s->zchunks;
+  long th = (long)c.res[0] * c.res[1] * pick_zchunks(c, p.tune.integrate_threads_log2);
   p.maxIntegThreads[c.tsdf_format] = std::max(p.maxIntegThreads[c.tsdf_format], th);
   p.fmtMask |= 1 << c.tsdf_format;
   const long nb = (long)((c.res[0] + 7) / 8) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8);
@@ -353,13 +364,13 @@ void plan_merge(BatchPlan& a, const BatchPlan& b) {
 
 unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
 
-// zchunks per session: threads per launch >= 2^18, every chunk >= 16 slices
-int pick_zchunks(const nui_session_cfg& c) {
-  long ncol = (long)c.res[0] * c.res[1];
-  int z = (int)std::max(1L, (kZChunkTargetThreads + ncol - 1) / ncol);
-  z = std::min(z, std::max(1, c.res[2] / 16));
-  return z;
+// ICP partial-sum slots of a session (the block count at the smallest pixels per thread,
+// twice with the photometric blocks)
+size_t icp_partial_bytes(const nui_session_cfg& c) {
+  const size_t N = (size_t)c.width * c.height, per = 256 * kMinIcpPpt;
+  return ((N + per - 1) / per) * kIcpTerms * sizeof(float2) * (c.photometric_weight > 0.f ? 2 : 1);
 }
+
 
 template <int F>
 void launch_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
@@ -379,10 +390,13 @@ void launch_summaries(const BatchPlan& p, const SessionDesc* d, cudaStream_t st,
   launch_summary<3>(p, d, st, force);
   if (p.fmtMask) k_super_summary<<<dim3((unsigned)p.maxHyper, p.n), 64, 0, st>>>(d, force);
 }
+// Blocks of the raycasts: 2 x 2 warps, each a tw x (32 / tw) pixel tile.
+unsigned ray_blocks(const BatchPlan& p, int tw) { return cdiv(p.maxW, 2 * tw) * cdiv(p.maxH, 2 * (32 / tw)); }
 template <int F>
 void launch_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   if (!(p.fmtMask & (1 << F))) return;
-  k_raycast<F><<<dim3(cdiv(p.maxW, 16) * cdiv(p.maxH, 8), p.n), 128, 0, st>>>(d);
+  const int tw = p.tune.raycast_tile_width;
+  k_raycast<F><<<dim3(ray_blocks(p, tw), p.n), 128, 0, st>>>(d, tw);
 }
 
 void launch_hash_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
@@ -407,9 +421,10 @@ void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t 
   if (!p.hashMask) return;
   k_hash_range<<<dim3(296, p.n), 256, 0, st>>>(d);
   k_hash_project<<<dim3(296, p.n), 128, 0, st>>>(d);
-  const unsigned tiles = cdiv(p.maxW, 16) * cdiv(p.maxH, 8);
-  if (p.hashMask & 1) k_hash_raycast<0><<<dim3(tiles, p.n), 128, 0, st>>>(d);
-  if (p.hashMask & 2) k_hash_raycast<1><<<dim3(tiles, p.n), 128, 0, st>>>(d);
+  const int tw = p.tune.hash_raycast_tile_width;
+  const unsigned tiles = ray_blocks(p, tw);
+  if (p.hashMask & 1) k_hash_raycast<0><<<dim3(tiles, p.n), 128, 0, st>>>(d, tw);
+  if (p.hashMask & 2) k_hash_raycast<1><<<dim3(tiles, p.n), 128, 0, st>>>(d, tw);
 }
 
 // Colour pyramid (if any session tracks with colour), the ICP iterations of every level,
@@ -417,9 +432,15 @@ void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t 
 void launch_track(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, float* d_pose, int* d_status) {
   const unsigned npix = cdiv((long)p.maxW * p.maxH, 256);
   if (p.colorIcp) k_color_grad<<<dim3(npix, p.n, 1), 256, 0, st>>>(d);  // finest level
+  const int ppt = p.tune.icp_pixels_per_thread, per = 256 * ppt;
   for (int l = p.maxLevels - 1; l >= 0; --l) {
-    const unsigned nb = cdiv((long)(p.maxW >> l) * (p.maxH >> l), 1024) + (l == 0 && p.colorIcp ? npix / 4 + 1 : 0);
-    for (int it = 0; it < p.maxIters[l]; ++it) k_icp<<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
+    const unsigned nb = cdiv((long)(p.maxW >> l) * (p.maxH >> l), per) +
+                        (l == 0 && p.colorIcp ? cdiv((long)p.maxW * p.maxH, per) : 0);
+    for (int it = 0; it < p.maxIters[l]; ++it) {
+      if (ppt == 2) k_icp<2><<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
+      else if (ppt == 8) k_icp<8><<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
+      else k_icp<4><<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
+    }
   }
   k_track_finalize<<<p.n, 32, 0, st>>>(d);
   k_publish<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n, d_pose, d_status);
@@ -514,6 +535,7 @@ nui_status tick_launch(nui_ctx* ctx, nui_session* const* ss, int n, const uint16
     fill_desc(s, ctx->h_descs[i], kind, raws[i], bgras ? bgras[i] : nullptr);
   }
   if (floor) plan_merge(p, *floor);
+  p.tune = ctx->tune;
   NUI_CUDA(cudaMemcpyAsync(ctx->d_descs, ctx->h_descs, sizeof(SessionDesc) * n, cudaMemcpyHostToDevice, ctx->stream));
   if (use_graph && !ctx->timing) {
     auto it = ctx->graphs.find(p);
@@ -745,6 +767,117 @@ NUI_API nui_status nui_ctx_last_tick_kernels(nui_ctx* c, int* n) {
   return NUI_OK;
 }
 
+bool tuning_valid(const nui_tuning& t) {
+  auto tw_ok = [](int w) { return w == 4 || w == 8 || w == 16 || w == 32; };
+  return t.integrate_threads_log2 >= 14 && t.integrate_threads_log2 <= 22 &&
+         (t.icp_pixels_per_thread == 2 || t.icp_pixels_per_thread == 4 || t.icp_pixels_per_thread == 8) &&
+         tw_ok(t.raycast_tile_width) && tw_ok(t.hash_raycast_tile_width);
+}
+
+NUI_API nui_status nui_ctx_get_tuning(nui_ctx* c, nui_tuning* out) {
+  if (!c || !out) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  *out = c->tune;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_ctx_set_tuning(nui_ctx* c, const nui_tuning* t) {
+  if (!c || !t) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  if (!tuning_valid(*t)) return fail(NUI_ERR_INVALID_ARG, "tuning out of range");
+  c->tune = *t;  // the graph cache is keyed by the launch shape, tuning included
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_ctx_autotune(nui_ctx* c, const nui_session_cfg* cfgs, int n, const uint16_t* const* depth,
+                                    const uint8_t* const* bgra, int frames, int repeats, nui_tuning* out,
+                                    float* out_tick_ms) {
+  if (!c || !cfgs || n <= 0 || !depth || frames < 2 || repeats < 1 || repeats > 101)
+    return fail(NUI_ERR_INVALID_ARG, "autotune: bad argument (frames >= 2, 1 <= repeats <= 101)");
+  for (int i = 0; i < n * frames; ++i)
+    if (!depth[i]) return fail(NUI_ERR_INVALID_ARG, "autotune: null depth frame");
+  std::vector<nui_session*> ss(n, nullptr);
+  auto drop = [&]() {
+    for (nui_session* s : ss)
+      if (s) nui_session_destroy(s);
+  };
+  for (int i = 0; i < n; ++i) {
+    nui_status st = nui_session_create(c, &cfgs[i], &ss[i]);
+    if (st != NUI_OK) {
+      const std::string why = g_err;
+      drop();
+      return fail(st, "autotune: scratch session: " + why);
+    }
+  }
+  bool dense = false, hash = false;
+  for (int i = 0; i < n; ++i) (ss[i]->hash ? hash : dense) = true;
+  const bool timing = c->timing;
+  c->timing = true;
+  std::vector<const uint16_t*> raws(n);
+  std::vector<const uint8_t*> cols(n);
+  std::vector<nui_status> per(n);
+  std::vector<float> poses(n * 12);
+  // frame f of every session; past the sequence the last two frames alternate
+  auto tick = [&](int f) -> nui_status {
+    if (f >= frames) f = frames - 2 + ((f - frames) & 1);
+    for (int i = 0; i < n; ++i) {
+      raws[i] = depth[(size_t)i * frames + f];
+      cols[i] = bgra ? bgra[(size_t)i * frames + f] : nullptr;
+    }
+    // a lost frame still ran the whole tick: it times like any other
+    const nui_status r =
+        nui_batch_tick(c, ss.data(), n, raws.data(), bgra ? cols.data() : nullptr, per.data(), poses.data());
+    return r == NUI_ERR_TRACKING_LOST ? NUI_OK : r;
+  };
+  nui_status st = NUI_OK;
+  int f = 0;
+  for (; f < frames && st == NUI_OK; ++f) st = tick(f);
+  auto measure = [&](int stage, float* tick_ms) -> float {
+    std::vector<float> t, w;
+    for (int r = 0; r < repeats && st == NUI_OK; ++r) {
+      st = tick(f++);
+      t.push_back(c->stage_ms[stage]);
+      w.push_back(c->stage_ms[kStages - 1]);
+    }
+    if (st != NUI_OK) return 0.f;
+    std::sort(t.begin(), t.end());
+    std::sort(w.begin(), w.end());
+    if (tick_ms) *tick_ms = w[w.size() / 2];
+    return t[t.size() / 2];
+  };
+  nui_tuning best = c->tune;
+  // one parameter at a time: its stage's median over `repeats` ticks
+  auto tune_one = [&](int nui_tuning::*field, std::initializer_list<int> cands, int stage) {
+    float best_ms = 0.f;
+    int pick = best.*field;
+    for (int v : cands) {
+      if (st != NUI_OK) return;
+      c->tune = best;
+      c->tune.*field = v;
+      const float ms = measure(stage, nullptr);
+      if (st == NUI_OK && (best_ms == 0.f || ms < best_ms)) best_ms = ms, pick = v;
+    }
+    best.*field = pick;
+  };
+  if (dense) tune_one(&nui_tuning::integrate_threads_log2, {16, 17, 18, 19, 20}, 3);
+  tune_one(&nui_tuning::icp_pixels_per_thread, {2, 4, 8}, 2);
+  if (dense) tune_one(&nui_tuning::raycast_tile_width, {4, 8, 16, 32}, 5);
+  if (hash) tune_one(&nui_tuning::hash_raycast_tile_width, {4, 8, 16, 32}, 5);
+  float tick_ms = 0.f;
+  if (st == NUI_OK) {
+    c->tune = best;
+    measure(kStages - 1, &tick_ms);
+  }
+  const std::string why = g_err;
+  c->timing = timing;
+  drop();
+  if (st != NUI_OK) {
+    c->tune = best;
+    return fail(st, "autotune: " + why);
+  }
+  if (out) *out = best;
+  if (out_tick_ms) *out_tick_ms = tick_ms;
+  return NUI_OK;
+}
+
 NUI_API nui_status nui_ctx_stage_ms(nui_ctx* c, int stage, float* ms) {
   if (!c || !ms || stage < 0 || stage >= kStages) return fail(NUI_ERR_INVALID_ARG, "bad stage");
   *ms = c->stage_ms[stage];
@@ -757,7 +890,7 @@ NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
   const size_t N = (size_t)c->width * c->height;
   size_t b = N * 2 + N * 4 /*bgra*/ + N * 4 /*scaled*/ + N * 16 * 2 /*ref maps*/ + N * 4 /*cmap*/;
   for (int l = 0; l < c->levels; ++l) b += (N >> (2 * l)) * (4 + 16);
-  b += sizeof(TrackState) + sizeof(SessionDesc) + ((N + 1023) / 1024) * kIcpTerms * sizeof(float2);
+  b += sizeof(TrackState) + sizeof(SessionDesc) + icp_partial_bytes(*c);
   b += (N / (kTile * kTile) + 64) * 4;
   if (c->volume_kind == NUI_VOLUME_HASH) {
     const size_t ne = (size_t)c->hash_buckets + c->hash_excess, nv = (size_t)c->hash_pool_blocks * 512;
@@ -794,7 +927,6 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
     s->gauss[i] = std::exp((float)(-(x * x)) * c.sigma_space2_inv_half);
   }
   icp_thresholds(c, s->icp_min_count);
-  s->zchunks = pick_zchunks(c);
   const size_t N = (size_t)c.width * c.height;
   const size_t nv = (size_t)c.res[0] * c.res[1] * c.res[2];
   auto alloc = [&](void** p, size_t bytes) -> bool {
@@ -808,7 +940,7 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
   s->hash = c.volume_kind == NUI_VOLUME_HASH;
   bool ok = alloc((void**)&s->raw, N * 2) && alloc((void**)&s->dscaled, N * 4) && alloc((void**)&s->vref, N * 16) &&
             alloc((void**)&s->nref, N * 16) && alloc((void**)&s->ts, sizeof(TrackState)) &&
-            alloc((void**)&s->partials, ((N + 1023) / 1024) * kIcpTerms * sizeof(float2) * (c.photometric_weight > 0.f ? 2 : 1)) &&
+            alloc((void**)&s->partials, icp_partial_bytes(c)) &&
             alloc((void**)&s->d_desc1, sizeof(SessionDesc));
   for (int l = 0; ok && l < c.levels; ++l)
     ok = alloc((void**)&s->dlev[l], (N >> (2 * l)) * 4) && alloc((void**)&s->vlev[l], (N >> (2 * l)) * 16);
