@@ -171,7 +171,10 @@ def run_ours(args, rank, world):
 
     # ---------------------------------------------------------------- launch shapes
     tuning, tune_s = None, 0.0
-    if not args.no_autotune:
+    if args.tuning:
+        ctx.set_tuning(L.Tuning(*[int(x) for x in args.tuning.split(",")]))
+        tuning = ctx.tuning().as_dict()
+    elif not args.no_autotune:
         t0 = time.perf_counter()
         t, _ = ctx.autotune(cfgs, [[hframe(i, k) for k in range(4)] for i in range(n)], repeats=5)
         tune_s = time.perf_counter() - t0
@@ -508,6 +511,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", dest="no_autotune", action="store_true",
                     help="keep the default launch shapes instead of timing the candidates first")
+    ap.add_argument("--tuning", default="",
+                    help="launch shapes to use instead of autotuning: integration threads log2, ICP pixels "
+                         "per thread, dense and hash ray tile widths (e.g. 16,8,8,4)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))
