@@ -521,25 +521,38 @@ struct HashRead {
     const int b = block(vx >> 3, vy >> 3, vz >> 3);
     return b < 0 ? -1 : b + ((vx & 7) + 8 * (vy & 7) + 64 * (vz & 7));
   }
-  __device__ __forceinline__ float sdf_at(int vx, int vy, int vz) {
-    const int bi = find(vx, vy, vz);
+  // Neighbourhood reads.  Voxels (i + LO .. i + HI) on each axis span at most two blocks
+  // per axis, so at most eight: each is looked up once, by every lane at the same call
+  // site, and a voxel read then selects its block among them.  (Reading each neighbour
+  // through its own lookup sent the lanes of a warp into two dozen separate divergent
+  // calls.)
+  struct Hood {
+    int b0x, b0y, b0z;  // first block on each axis
+    int P[8];           // pool offsets, index (bx - b0x) + 2 (by - b0y) + 4 (bz - b0z); -1: none
+  };
+  template <int LO, int HI>
+  __device__ __forceinline__ void hood(Hood& h, int ix, int iy, int iz) {
+    h.b0x = (ix + LO) >> 3;
+    h.b0y = (iy + LO) >> 3;
+    h.b0z = (iz + LO) >> 3;
+    const int sx = ((ix + HI) >> 3) - h.b0x, sy = ((iy + HI) >> 3) - h.b0y, sz = ((iz + HI) >> 3) - h.b0z;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int ox = k & 1, oy = (k >> 1) & 1, oz = k >> 2;
+      h.P[k] = (ox <= sx && oy <= sy && oz <= sz) ? block(h.b0x + ox, h.b0y + oy, h.b0z + oz) : -1;
+    }
+  }
+  // pool index of voxel (x, y, z) of the neighbourhood, or -1 if its block is not allocated
+  __device__ __forceinline__ int hood_index(const Hood& h, int x, int y, int z) const {
+    const int sel = ((x >> 3) - h.b0x) + 2 * ((y >> 3) - h.b0y) + 4 * ((z >> 3) - h.b0z);
+    int b = h.P[0];
+#pragma unroll
+    for (int k = 1; k < 8; ++k) b = sel == k ? h.P[k] : b;
+    return b < 0 ? -1 : b + (x & 7) + 8 * (y & 7) + 64 * (z & 7);
+  }
+  __device__ __forceinline__ float hood_sdf(const Hood& h, int x, int y, int z) const {
+    const int bi = hood_index(h, x, y, z);
     return bi < 0 ? 1.0f : HVox<HF>::load(s.hsdf, (unsigned)bi);
-  }
-  __device__ __noinline__ float sdf_slow(int vx, int vy, int vz) { return sdf_at(vx, vy, vz); }
-  // The sdf of voxel (ix + dx, iy + dy, iz + dz): one block lookup for the whole
-  // neighbourhood when it lies inside the block of (ix, iy, iz) (base >= 0 then holds that
-  // voxel's pool index, or -2 if the block is not allocated), else a lookup per voxel.
-  __device__ __forceinline__ float near(int base, int ix, int iy, int iz, int dx, int dy, int dz) {
-    if (base == -1) return sdf_slow(ix + dx, iy + dy, iz + dz);
-    if (base == -2) return 1.0f;
-    return HVox<HF>::load(s.hsdf, (unsigned)(base + dx + 8 * dy + 64 * dz));
-  }
-  // base for near(): neighbours with offsets in [lo, hi] on every axis
-  __device__ __forceinline__ int near_base(int ix, int iy, int iz, int lo, int hi) {
-    const int x = ix & 7, y = iy & 7, z = iz & 7;
-    if (x + lo < 0 || x + hi > 7 || y + lo < 0 || y + hi > 7 || z + lo < 0 || z + hi > 7) return -1;
-    const int b = block(ix >> 3, iy >> 3, iz >> 3);
-    return b < 0 ? -2 : b + x + 8 * y + 64 * z;
   }
 };
 
@@ -564,17 +577,18 @@ __device__ __forceinline__ void hash_march(HashRead<HF>& R, const SessionDesc& s
       if (sdfv <= 0.1f && sdfv >= -0.5f) {
         const int ix = (int)floorf(pr.x), iy = (int)floorf(pr.y), iz = (int)floorf(pr.z);
         const float3 cf = f3(pr.x - (float)ix, pr.y - (float)iy, pr.z - (float)iz);
-        const int nb = R.near_base(ix, iy, iz, 0, 1);
-        float v1 = R.near(nb, ix, iy, iz, 0, 0, 0), v2 = R.near(nb, ix, iy, iz, 1, 0, 0);
+        typename HashRead<HF>::Hood h;
+        R.template hood<0, 1>(h, ix, iy, iz);
+        float v1 = R.hood_sdf(h, ix, iy, iz), v2 = R.hood_sdf(h, ix + 1, iy, iz);
         float r1 = (1.0f - cf.x) * v1 + cf.x * v2;
-        v1 = R.near(nb, ix, iy, iz, 0, 1, 0);
-        v2 = R.near(nb, ix, iy, iz, 1, 1, 0);
+        v1 = R.hood_sdf(h, ix, iy + 1, iz);
+        v2 = R.hood_sdf(h, ix + 1, iy + 1, iz);
         r1 = (1.0f - cf.y) * r1 + cf.y * ((1.0f - cf.x) * v1 + cf.x * v2);
-        v1 = R.near(nb, ix, iy, iz, 0, 0, 1);
-        v2 = R.near(nb, ix, iy, iz, 1, 0, 1);
+        v1 = R.hood_sdf(h, ix, iy, iz + 1);
+        v2 = R.hood_sdf(h, ix + 1, iy, iz + 1);
         float r2 = (1.0f - cf.x) * v1 + cf.x * v2;
-        v1 = R.near(nb, ix, iy, iz, 0, 1, 1);
-        v2 = R.near(nb, ix, iy, iz, 1, 1, 1);
+        v1 = R.hood_sdf(h, ix, iy + 1, iz + 1);
+        v2 = R.hood_sdf(h, ix + 1, iy + 1, iz + 1);
         r2 = (1.0f - cf.y) * r2 + cf.y * ((1.0f - cf.x) * v1 + cf.x * v2);
         sdfv = (1.0f - cf.z) * r1 + cf.z * r2;
       }
@@ -620,11 +634,13 @@ __device__ __forceinline__ void hash_finish(HashRead<HF>& R, const SessionDesc& 
     const float3 nc = f3(1.0f - cf.x, 1.0f - cf.y, 1.0f - cf.z);
     float fb[8];
     float nearest = 1.0e20f;
-    const int nb = R.near_base(ix, iy, iz, 0, 1);
+    // one neighbourhood for the corners and the gradient's outer samples
+    typename HashRead<HF>::Hood h;
+    R.template hood<-1, 2>(h, ix, iy, iz);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-      const int bi = nb >= 0 ? nb + ox + 8 * oy + 64 * oz : nb == -2 ? -1 : R.find(ix + ox, iy + oy, iz + oz);
+      const int bi = R.hood_index(h, ix + ox, iy + oy, iz + oz);
       fb[k] = bi < 0 ? 1.0f : HVox<HF>::load(s.hsdf, (unsigned)bi);
       const float3 dd = f3(ox ? nc.x : cf.x, oy ? nc.y : cf.y, oz ? nc.z : cf.z);
       const float cd = sqrtf(dot3(dd, dd));
@@ -641,31 +657,31 @@ __device__ __forceinline__ void hash_finish(HashRead<HF>& R, const SessionDesc& 
     pr = add3(pr, mul3(dir, stepLen));
     vout = w0(mul3(pr, s.voxel));
     float p1, p2, v1;
-    const int n2 = R.near_base(ix, iy, iz, -1, 2);
+    auto nr = [&](int dx, int dy, int dz) { return R.hood_sdf(h, ix + dx, iy + dy, iz + dz); };
     float3 g;
     p1 = fb[0] * nc.y * nc.z + fb[2] * cf.y * nc.z + fb[4] * nc.y * cf.z + fb[6] * cf.y * cf.z;
-    p2 = R.near(n2, ix, iy, iz, -1, 0, 0) * nc.y * nc.z + R.near(n2, ix, iy, iz, -1, +1, 0) * cf.y * nc.z +
-         R.near(n2, ix, iy, iz, -1, 0, +1) * nc.y * cf.z + R.near(n2, ix, iy, iz, -1, +1, +1) * cf.y * cf.z;
+    p2 = nr(-1, 0, 0) * nc.y * nc.z + nr(-1, +1, 0) * cf.y * nc.z +
+         nr(-1, 0, +1) * nc.y * cf.z + nr(-1, +1, +1) * cf.y * cf.z;
     v1 = p1 * cf.x + p2 * nc.x;
     p1 = fb[1] * nc.y * nc.z + fb[3] * cf.y * nc.z + fb[5] * nc.y * cf.z + fb[7] * cf.y * cf.z;
-    p2 = R.near(n2, ix, iy, iz, +2, 0, 0) * nc.y * nc.z + R.near(n2, ix, iy, iz, +2, +1, 0) * cf.y * nc.z +
-         R.near(n2, ix, iy, iz, +2, 0, +1) * nc.y * cf.z + R.near(n2, ix, iy, iz, +2, +1, +1) * cf.y * cf.z;
+    p2 = nr(+2, 0, 0) * nc.y * nc.z + nr(+2, +1, 0) * cf.y * nc.z +
+         nr(+2, 0, +1) * nc.y * cf.z + nr(+2, +1, +1) * cf.y * cf.z;
     g.x = p1 * nc.x + p2 * cf.x - v1;
     p1 = fb[0] * nc.x * nc.z + fb[1] * cf.x * nc.z + fb[4] * nc.x * cf.z + fb[5] * cf.x * cf.z;
-    p2 = R.near(n2, ix, iy, iz, 0, -1, 0) * nc.x * nc.z + R.near(n2, ix, iy, iz, +1, -1, 0) * cf.x * nc.z +
-         R.near(n2, ix, iy, iz, 0, -1, +1) * nc.x * cf.z + R.near(n2, ix, iy, iz, +1, -1, +1) * cf.x * cf.z;
+    p2 = nr(0, -1, 0) * nc.x * nc.z + nr(+1, -1, 0) * cf.x * nc.z +
+         nr(0, -1, +1) * nc.x * cf.z + nr(+1, -1, +1) * cf.x * cf.z;
     v1 = p1 * cf.y + p2 * nc.y;
     p1 = fb[2] * nc.x * nc.z + fb[3] * cf.x * nc.z + fb[6] * nc.x * cf.z + fb[7] * cf.x * cf.z;
-    p2 = R.near(n2, ix, iy, iz, 0, +2, 0) * nc.x * nc.z + R.near(n2, ix, iy, iz, +1, +2, 0) * cf.x * nc.z +
-         R.near(n2, ix, iy, iz, 0, +2, +1) * nc.x * cf.z + R.near(n2, ix, iy, iz, +1, +2, +1) * cf.x * cf.z;
+    p2 = nr(0, +2, 0) * nc.x * nc.z + nr(+1, +2, 0) * cf.x * nc.z +
+         nr(0, +2, +1) * nc.x * cf.z + nr(+1, +2, +1) * cf.x * cf.z;
     g.y = p1 * nc.y + p2 * cf.y - v1;
     p1 = fb[0] * nc.x * nc.y + fb[1] * cf.x * nc.y + fb[2] * nc.x * cf.y + fb[3] * cf.x * cf.y;
-    p2 = R.near(n2, ix, iy, iz, 0, 0, -1) * nc.x * nc.y + R.near(n2, ix, iy, iz, +1, 0, -1) * cf.x * nc.y +
-         R.near(n2, ix, iy, iz, 0, +1, -1) * nc.x * cf.y + R.near(n2, ix, iy, iz, +1, +1, -1) * cf.x * cf.y;
+    p2 = nr(0, 0, -1) * nc.x * nc.y + nr(+1, 0, -1) * cf.x * nc.y +
+         nr(0, +1, -1) * nc.x * cf.y + nr(+1, +1, -1) * cf.x * cf.y;
     v1 = p1 * cf.z + p2 * nc.z;
     p1 = fb[4] * nc.x * nc.y + fb[5] * cf.x * nc.y + fb[6] * nc.x * cf.y + fb[7] * cf.x * cf.y;
-    p2 = R.near(n2, ix, iy, iz, 0, 0, +2) * nc.x * nc.y + R.near(n2, ix, iy, iz, +1, 0, +2) * cf.x * nc.y +
-         R.near(n2, ix, iy, iz, 0, +1, +2) * nc.x * cf.y + R.near(n2, ix, iy, iz, +1, +1, +2) * cf.x * cf.y;
+    p2 = nr(0, 0, +2) * nc.x * nc.y + nr(+1, 0, +2) * cf.x * nc.y +
+         nr(0, +1, +2) * nc.x * cf.y + nr(+1, +1, +2) * cf.x * cf.y;
     g.z = p1 * nc.z + p2 * cf.z - v1;
     nout = w0(normalize3(g));
   }
