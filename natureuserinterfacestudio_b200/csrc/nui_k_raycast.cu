@@ -224,9 +224,11 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
     const int hx = (V.rx + 127) >> 7, hy = (V.ry + 127) >> 7;
     const float3 idir = f3(1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z);
     bool pend = false;  // tsdf stands for a skipped sample at tc whose class (NaN or > 0) is unread
+    bool hit = false;   // a zero crossing between the samples at tc and tn = tc + step
+    float tn = tc;
     while (tc < max_time) {
       float prev = tsdf;
-      const float tn = tc + step;
+      tn = tc + step;
       V.voxel_of(add3(start, mul3(dir, tn)), gx, gy, gz);
       if (!(gx >= 0 && gy >= 0 && gz >= 0 && gx < V.rx && gy < V.ry && gz < V.rz)) break;
       const uint8_t st = V.occ ? __ldg(V.occ + V.bidx(gx, gy, gz)) : (uint8_t)kBrickMixed;
@@ -279,10 +281,17 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
       }
       if (prev < 0.f && tsdf > 0.f) break;
       if (prev >= 0.f && tsdf <= 0.f) {
-        const float Ftdt = V.trilinear(add3(start, mul3(dir, tn)));
-        if (isnan(Ftdt)) break;
-        const float Ft = V.trilinear(add3(start, mul3(dir, tc)));
-        if (isnan(Ft)) break;
+        hit = true;
+        break;
+      }
+      tc = tn;
+    }
+    // The refinement runs after the march, so that the lanes of a warp whose rays end at
+    // different samples still refine together.
+    if (hit) {
+      const float Ftdt = V.trilinear(add3(start, mul3(dir, tn)));
+      const float Ft = isnan(Ftdt) ? Ftdt : V.trilinear(add3(start, mul3(dir, tc)));
+      if (!isnan(Ft)) {
         const float Ts = tc - step * Ft / (Ftdt - Ft);
         const float3 vf = add3(start, mul3(dir, Ts));
         vout = w0(sub3(vf, off));
@@ -302,9 +311,7 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
           n.z = fz1 - fz2;
           nout = w0(normalize3(n));
         }
-        break;
       }
-      tc = tn;
     }
   }
   s.vref[id] = vout;
