@@ -13,6 +13,7 @@ Rewrites (each purely syntactic):
   * multi-component swizzles `.xy`, `.s012`  -> `.swz<0,1>()`, `.swz<0,1,2>()`
   * `__local T name[N];` inside a kernel      -> `static thread_local T name[N];`
   * `__attribute__((reqd_work_group_size(..)))` and `#pragma OPENCL` lines removed
+  * implicit-int declarations `const idx =` (extract.cl) -> `const int idx =`
 
 Usage:  python oracle/build_ref.py [--reference /root/reference]
 """
@@ -44,6 +45,7 @@ UNITS = {
     "KinfuHashScene.cl": "launch_hash_scene.inc",
     "KinfuHashRaycast.cl": "launch_hash_raycast.inc",
     "KinfuHashVisualization.cl": "launch_hash_mesh.inc",
+    "extract.cl": "launch_extract.inc",
 }
 # The reference fixes its hash table sizes at compile time (hashing_gpu_def.h:9-20:
 # 0x150000 buckets, 0x30000 excess entries, 2^20 voxel blocks = 3.2 GB of voxels).  The
@@ -71,6 +73,7 @@ def rewrite(src):
     src = re.sub(r"^\s*#pragma\s+OPENCL.*$", "", src, flags=re.M)
     src = re.sub(r"__attribute__\s*\(\(\s*reqd_work_group_size\s*\([^)]*\)\s*\)\)", "", src)
     src = re.sub(r"\(\s*(%s)\s*\)\s*\(" % VEC_T, r"\1(", src)
+    src = re.sub(r"\bconst\s+idx\s*=", "const int idx =", src)
 
     def swz(m):
         idx = swizzle_indices(m.group(1))

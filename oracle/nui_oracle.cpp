@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <vector>
 
@@ -264,13 +265,15 @@ ORC_API void orc_tsdf_init(int16_t* vol, uint8_t* cvol, long nvox) {
   if (cvol) std::memset(cvol, 0, (size_t)nvox * 4);
 }
 
-// A10  integrateTsdfVolumeKernel   tsdfVolume.cl:31-190 (voxelWrap = 0, normals = NULL as
-// passed by NuiKinfuOpenCLScene.cpp:278).  `touched` receives the number of voxels
-// read-modify-written.
-ORC_API void orc_tsdf_integrate(const float* depth, const uint8_t* bgra, const OrcCam* cam,
-                                const OrcXform* m, const OrcTsdf* p, int16_t* vol, uint8_t* cvol,
-                                int max_color_weight, long* touched) {
+// A10  integrateTsdfVolumeKernel   tsdfVolume.cl:31-190 (normals = NULL as passed by
+// NuiKinfuOpenCLScene.cpp:278).  `touched` receives the number of voxels
+// read-modify-written.  wrap: the shifting volume's voxelWrap (tsdfVolume.cl:71,104; voxel
+// (x, y, z) lives at ((x + wx) % rx, (y + wy) % ry, (z + wz) % rz)), NULL for none.
+ORC_API void orc_tsdf_integrate_wrap(const float* depth, const uint8_t* bgra, const OrcCam* cam,
+                                     const OrcXform* m, const OrcTsdf* p, int16_t* vol, uint8_t* cvol,
+                                     int max_color_weight, long* touched, const int* wrap) {
   const int rx = (int)p->res[0], ry = (int)p->res[1], rz = (int)p->res[2];
+  const int wx = wrap ? wrap[0] : 0, wy = wrap ? wrap[1] : 0, wz = wrap ? wrap[2] : 0;
   const int W = (int)cam->W, H = (int)cam->H;
   long cnt = 0;
 #pragma omp parallel for schedule(dynamic, 4) reduction(+ : cnt)
@@ -288,7 +291,7 @@ ORC_API void orc_tsdf_integrate(const float* depth, const uint8_t* bgra, const O
       const float tinv = 1.f / p->trunc;
       const float dx = Ri[2] * p->cell[2] * cam->fx;
       const float dy = Ri[5] * p->cell[2] * cam->fy;
-      const long base = ((long)vx + (long)vy * rx) * rz;
+      const long base = ((long)((vx + wx) % rx) + (long)((vy + wy) % ry) * rx) * rz;
       for (int vz = 0; vz < rz; ++vz, vgz += p->cell[2], zs += p->cell[2], v_x += dx, v_y += dy) {
         float inv_z = 1.0f / (v_z + Ri[8] * zs);
         if (inv_z < 0.f) continue;
@@ -300,7 +303,7 @@ ORC_API void orc_tsdf_integrate(const float* depth, const uint8_t* bgra, const O
         float sdf = Dp - std::sqrt(vgz * vgz + part);
         if (std::isnan(Dp) || !(sdf >= -p->trunc)) continue;
         float tsdf = std::min(1.0f, sdf * tinv);
-        long idx = base + vz;
+        long idx = base + (vz + wz) % rz;
         int16_t* vp = vol + 2 * idx;
         float F = (float)vp[0] / 32766.f;
         int Wt = vp[1];
@@ -329,6 +332,12 @@ ORC_API void orc_tsdf_integrate(const float* depth, const uint8_t* bgra, const O
   if (touched) *touched = cnt;
 }
 
+ORC_API void orc_tsdf_integrate(const float* depth, const uint8_t* bgra, const OrcCam* cam,
+                                const OrcXform* m, const OrcTsdf* p, int16_t* vol, uint8_t* cvol,
+                                int max_color_weight, long* touched) {
+  orc_tsdf_integrate_wrap(depth, bgra, cam, m, p, vol, cvol, max_color_weight, touched, nullptr);
+}
+
 // ---------------------------------------------------------------------------------
 // A12  raycastKernel   raycast.cl:128-277 with interpolateTrilineary raycast.cl:36-120.
 // The trilinear weights are reproduced as written: the x-neighbour voxel is weighted
@@ -338,7 +347,18 @@ struct RcVol {
   const int16_t* v;
   int rx, ry, rz;
   float cell[3];
-  long idx(int x, int y, int z) const { return ((long)y * rx + x) * rz + z; }
+  int w[3];  // voxelWrap (raycast.cl:62,184,201)
+  // the reference's trilinear neighbour addressing (buffer strides from the wrapped first
+  // voxel), for pinning only; false: each neighbour wrapped on its own
+  bool strides = false;
+  long idx(int x, int y, int z) const {
+    return ((long)((y + w[1]) % ry) * rx + (x + w[0]) % rx) * rz + (z + w[2]) % rz;
+  }
+  // neighbour (dx, dy, dz) in {0, 1}^3 of voxel (x, y, z)
+  long nidx(int x, int y, int z, int dx, int dy, int dz) const {
+    if (!strides) return idx(x + dx, y + dy, z + dz);
+    return idx(x, y, z) + dz + (long)dx * rz + (long)dy * rx * rz;
+  }
 };
 inline void voxel_of(f3 p, const float* cell, int& gx, int& gy, int& gz) {
   gx = (int)std::round(p.x / cell[0]);
@@ -346,6 +366,7 @@ inline void voxel_of(f3 p, const float* cell, int& gx, int& gy, int& gz) {
   gz = (int)std::round(p.z / cell[2]);
 }
 inline bool tsdf_at(const RcVol& V, long idx, float& f) {
+  if (idx < 0 || idx >= (long)V.rx * V.ry * V.rz) return false;  // strides past the buffer
   int16_t a = V.v[2 * idx], w = V.v[2 * idx + 1];
   f = (float)a / 32766.f;
   return w > 0;
@@ -368,23 +389,28 @@ float trilinear(f3 p, const RcVol& V) {
   // names follow the reference: t_abc with a = y step, b = x step, c = z step
   float t000, t001, t011, t010, t110, t111, t101, t100;
   if (!tsdf_at(V, V.idx(gx, gy, gz), t000)) return QNAN;
-  if (!tsdf_at(V, V.idx(gx, gy, gz + 1), t001)) return QNAN;
-  if (!tsdf_at(V, V.idx(gx + 1, gy, gz + 1), t011)) return QNAN;
-  if (!tsdf_at(V, V.idx(gx + 1, gy, gz), t010)) return QNAN;
-  if (!tsdf_at(V, V.idx(gx + 1, gy + 1, gz), t110)) return QNAN;
-  if (!tsdf_at(V, V.idx(gx + 1, gy + 1, gz + 1), t111)) return QNAN;
-  if (!tsdf_at(V, V.idx(gx, gy + 1, gz + 1), t101)) return QNAN;
-  if (!tsdf_at(V, V.idx(gx, gy + 1, gz), t100)) return QNAN;
+  if (!tsdf_at(V, V.nidx(gx, gy, gz, 0, 0, 1), t001)) return QNAN;
+  if (!tsdf_at(V, V.nidx(gx, gy, gz, 1, 0, 1), t011)) return QNAN;
+  if (!tsdf_at(V, V.nidx(gx, gy, gz, 1, 0, 0), t010)) return QNAN;
+  if (!tsdf_at(V, V.nidx(gx, gy, gz, 1, 1, 0), t110)) return QNAN;
+  if (!tsdf_at(V, V.nidx(gx, gy, gz, 1, 1, 1), t111)) return QNAN;
+  if (!tsdf_at(V, V.nidx(gx, gy, gz, 0, 1, 1), t101)) return QNAN;
+  if (!tsdf_at(V, V.nidx(gx, gy, gz, 0, 1, 0), t100)) return QNAN;
   return t000 * (1 - a) * (1 - b) * (1 - c) + t001 * (1 - a) * (1 - b) * c +
          t010 * (1 - a) * b * (1 - c) + t011 * (1 - a) * b * c + t100 * a * (1 - b) * (1 - c) +
          t101 * a * (1 - b) * c + t110 * a * b * (1 - c) + t111 * a * b * c;
 }
 }  // namespace
 
-ORC_API void orc_raycast(const int16_t* vol, const uint8_t* cvol, const OrcTsdf* p,
-                         const OrcCam* cam, const OrcXform* m, int W, int H, float* vmap,
-                         float* nmap, uint8_t* cmap, long* steps_out) {
-  RcVol V{vol, (int)p->res[0], (int)p->res[1], (int)p->res[2], {p->cell[0], p->cell[1], p->cell[2]}};
+// ref_strides: the trilinear reads reach their neighbours by the reference's buffer strides
+// from the wrapped first voxel (raycast.cl:62-108), so that a read straddling the wrap seam
+// takes voxels of the next buffer row as the reference does; used to pin the rest of this
+// function against the reference.  0: each neighbour is the voxel's true neighbour.
+ORC_API void orc_raycast_wrap_mode(const int16_t* vol, const uint8_t* cvol, const OrcTsdf* p, const OrcCam* cam,
+                                   const OrcXform* m, int W, int H, float* vmap, float* nmap, uint8_t* cmap,
+                                   long* steps_out, const int* wrap, int ref_strides) {
+  RcVol V{vol, (int)p->res[0], (int)p->res[1], (int)p->res[2], {p->cell[0], p->cell[1], p->cell[2]},
+          {wrap ? wrap[0] : 0, wrap ? wrap[1] : 0, wrap ? wrap[2] : 0}, ref_strides != 0};
   const f3 off = mk(p->dim[0] / 2.0f, p->dim[1] / 2.0f, 0.f);
   const f3 r0 = mk(m->R[0], m->R[1], m->R[2]), r1 = mk(m->R[3], m->R[4], m->R[5]),
            r2 = mk(m->R[6], m->R[7], m->R[8]), t = mk(m->t[0], m->t[1], m->t[2]);
@@ -460,6 +486,116 @@ ORC_API void orc_raycast(const int16_t* vol, const uint8_t* cvol, const OrcTsdf*
       }
     }
   if (steps_out) *steps_out = steps_total;
+}
+
+ORC_API void orc_raycast_wrap(const int16_t* vol, const uint8_t* cvol, const OrcTsdf* p, const OrcCam* cam,
+                              const OrcXform* m, int W, int H, float* vmap, float* nmap, uint8_t* cmap,
+                              long* steps_out, const int* wrap) {
+  orc_raycast_wrap_mode(vol, cvol, p, cam, m, W, H, vmap, nmap, cmap, steps_out, wrap, 0);
+}
+
+ORC_API void orc_raycast(const int16_t* vol, const uint8_t* cvol, const OrcTsdf* p,
+                         const OrcCam* cam, const OrcXform* m, int W, int H, float* vmap,
+                         float* nmap, uint8_t* cmap, long* steps_out) {
+  orc_raycast_wrap(vol, cvol, p, cam, m, W, H, vmap, nmap, cmap, steps_out, nullptr);
+}
+
+// ---------------------------------------------------------------------------------
+// Shifting dense volume (NuiKinfuOpenCLShiftScene, the eScene_ShiftingVolume scene of
+// NuiSLAMController.cpp:55-62): a cyclic volume addressed through voxelWrap.
+
+// initializeVolume over a slab (tsdfVolume.cl:192-211 as launched by clearSlice,
+// NuiKinfuOpenCLShiftScene.cpp:76-115): voxels (x + off) of x in [0, range) per axis.
+ORC_API void orc_tsdf_clear_slice(int16_t* vol, uint8_t* cvol, const OrcTsdf* p, const int* off,
+                                  const int* range) {
+  const int rx = (int)p->res[0], ry = (int)p->res[1], rz = (int)p->res[2];
+  for (int y = 0; y < range[1]; ++y)
+    for (int x = 0; x < range[0]; ++x)
+      for (int z = 0; z < range[2]; ++z) {
+        const long idx = ((long)((y + off[1]) % ry) * rx + (x + off[0]) % rx) * rz + (z + off[2]) % rz;
+        vol[2 * idx] = 32767;
+        vol[2 * idx + 1] = 0;
+        if (cvol) std::memset(cvol + 4 * idx, 0, 4);
+      }
+}
+
+// fetchShiftVolumeKernel (extract.cl:82-179): surface points of a slab, from each voxel
+// whose tsdf is exactly 0 and between z-neighbours of opposite sign, with the kernel's
+// own index arithmetic (its z loop adds voxelWrap.z twice, and its offsets step by whole
+// volumes as written).  fetchVolumeKernel (extract.cl:4-79) is the case wrap = offset = 0.
+// Points go to xyz (3 floats) / rgba (4 floats) up to cap; returns how many were found.
+ORC_API long orc_fetch_points(const int16_t* vol, const uint8_t* cvol, const OrcTsdf* p, const int* range,
+                              const int* wrap, const int* voff, float* xyz, float* rgba, long cap) {
+  const int rx = (int)p->res[0], ry = (int)p->res[1], rz = (int)p->res[2];
+  const float half_x = (float)(rx >> 1), half_y = (float)(ry >> 1);
+  const float* cs = p->cell;
+  long n = 0;
+  auto emit = [&](float x, float y, float z, const float c[4]) {
+    if (n < cap) {
+      xyz[3 * n] = x;
+      xyz[3 * n + 1] = y;
+      xyz[3 * n + 2] = z;
+      std::memcpy(rgba + 4 * n, c, 4 * sizeof(float));
+    }
+    ++n;
+  };
+  for (int vx = 0; vx < range[0]; ++vx)
+    for (int vy = 0; vy < range[1]; ++vy) {
+      const long vid = ((long)((vy + wrap[1]) % ry) * rx + (vx + wrap[0]) % rx) * rz;
+      int ob[3] = {(voff[0] / rx) * rx, (voff[1] / ry) * ry, (voff[2] / rz) * rz};
+      if (voff[0] > 0) {
+        if (vx < voff[0] % rx) ob[0] += rx;
+      } else if (vx > rx + voff[0] % rx) {
+        ob[0] -= rx;
+      }
+      if (voff[1] > 0) {
+        if (vy < voff[1] % ry) ob[1] += ry;
+      } else if (vy > ry + voff[1] % ry) {
+        ob[1] -= ry;
+      }
+      float tsdf = QNAN;
+      const int zend = range[2] + wrap[2];
+      for (int vz = wrap[2]; vz < zend; ++vz) {
+        const float prev = tsdf;
+        const long idx = vid + (vz + wrap[2]) % rz;
+        const int16_t* v = vol + 2 * idx;
+        if (v[1] <= 0) {
+          tsdf = QNAN;
+          continue;
+        }
+        int oz = ob[2];
+        if (voff[2] > 0) {
+          if (vz < voff[2] % rz) oz += rz;
+        } else if (vz > rz + voff[2] % rz) {
+          oz -= rz;
+        }
+        tsdf = (float)v[0] / 32766.f;
+        if (tsdf == 0.f) {
+          float c[4] = {0.f, 0.f, 0.f, 1.f};
+          if (cvol) {
+            const uint8_t* g = cvol + 4 * idx;
+            c[0] = (float)g[0] / 255.f;
+            c[1] = (float)g[1] / 255.f;
+            c[2] = (float)g[2] / 255.f;
+          }
+          emit(((float)(vx + ob[0]) + 0.5f - half_x) * cs[0], (-(float)(vy + ob[1]) - 0.5f + half_y) * cs[1],
+               ((float)(vz + oz) + 0.5f) * cs[2], c);
+        } else if ((prev < 0.f && tsdf > 0.f) || (prev > 0.f && tsdf < 0.f)) {
+          const float ti = 1.f / std::fabs(tsdf), tpi = 1.f / std::fabs(prev);
+          const float dp = (ti * (float)(vz + oz) + tpi * (float)(vz + oz - 1)) / (ti + tpi);
+          float c[4] = {0.f, 0.f, 0.f, 1.f};
+          if (cvol) {  // the crossing case reads the colour bytes in reverse order
+            const uint8_t* g = cvol + 4 * idx;
+            c[0] = (float)g[2] / 255.f;
+            c[1] = (float)g[1] / 255.f;
+            c[2] = (float)g[0] / 255.f;
+          }
+          emit(((float)(vx + ob[0]) + 0.5f - half_x) * cs[0], (-(float)(vy + ob[1]) - 0.5f + half_y) * cs[1],
+               (dp + 0.5f) * cs[2], c);
+        }
+      }
+    }
+  return n;
 }
 
 // ---------------------------------------------------------------------------------
@@ -1048,6 +1184,9 @@ struct OrcEngineCfg {
   float voxel, mu;
   int buckets, excess, pool, max_w;
   float photometric_weight;  // > 0 (with colour): the colour tracker's term joins ICP
+  int voxel_shift;           // > 0: the shifting dense volume (NuiKinfuVolumeConfig::voxel_shift)
+  float shift_basis[3];      // NuiKinfuVolumeConfig::translateBasis
+  long point_cap;            // points kept of the slabs that leave the shifting volume
 };
 
 struct OrcHash;
@@ -1074,6 +1213,10 @@ struct OrcEngine {
   OrcHash* hs = nullptr;
   // colour tracking: the previous frame's colours, the current frame's gradients
   std::vector<uint8_t> cprev, cgx, cgy;
+  // shifting volume: m_voxel_offset and the point cache (NuiKinfuVertexCache)
+  int voff[3] = {0, 0, 0};
+  std::vector<float> pts_xyz, pts_rgba;
+  long pts_n = 0;
 };
 
 ORC_API OrcEngine* orc_engine_create(const OrcEngineCfg* cfg) {
@@ -1136,6 +1279,92 @@ static double rel_angle(const float* Ra, const float* Rb) {
   return std::acos(cv);
 }
 
+// NuiKinfuOpenCLShiftScene::getVoxelWrap (NuiKinfuOpenCLShiftScene.cpp:44-56)
+static void engine_voxel_wrap(const OrcEngine* e, int* w) {
+  for (int a = 0; a < 3; ++a) w[a] = e->voff[a] >= 0 ? e->voff[a] : e->c.res[a] - ((-e->voff[a]) % e->c.res[a]);
+}
+
+// The camera's global translation: local + getVoxelOffsetSize (:58-66); a fixed volume
+// (offset 0) keeps the local translation.
+static void engine_global_t(const OrcEngine* e, float* g) {
+  for (int a = 0; a < 3; ++a) g[a] = e->voff[a] ? e->xf.t[a] + (float)e->voff[a] * e->tp.cell[a] : e->xf.t[a];
+}
+
+// fetchAndClearX/Y/Z (:235-286): the slab of |tr| voxels that leaves the volume goes to the
+// point cache (fetchSlice, :117-233), is cleared (clearSlice, :76-115), and the offset moves.
+static void engine_fetch_and_clear(OrcEngine* e, int a, int tr) {
+  const OrcEngineCfg& c = e->c;
+  int off = e->voff[a];
+  if (tr < 0) off += tr;
+  off = off >= 0 ? off % c.res[a] : c.res[a] - (-off) % c.res[a];
+  int wrap[3] = {0, 0, 0}, range[3] = {c.res[0], c.res[1], c.res[2]};
+  wrap[a] = off;
+  range[a] = std::abs(tr);
+  if (c.point_cap > 0) {
+    const long room = std::max(0L, c.point_cap - e->pts_n);
+    std::vector<float> xyz(3 * (size_t)room + 3), rgba(4 * (size_t)room + 4);
+    const long n = orc_fetch_points(e->vol.data(), c.color ? e->cvol.data() : nullptr, &e->tp, range, wrap, e->voff,
+                                    xyz.data(), rgba.data(), room);
+    const long keep = std::min(n, room);
+    e->pts_xyz.insert(e->pts_xyz.end(), xyz.begin(), xyz.begin() + 3 * keep);
+    e->pts_rgba.insert(e->pts_rgba.end(), rgba.begin(), rgba.begin() + 4 * keep);
+    e->pts_n += n;
+  }
+  orc_tsdf_clear_slice(e->vol.data(), c.color ? e->cvol.data() : nullptr, &e->tp, wrap, range);
+  e->voff[a] += tr;
+}
+
+// shiftVolume (:288-351) on the camera's local translation, before the integration.
+static void engine_shift_volume(OrcEngine* e) {
+  const OrcEngineCfg& c = e->c;
+  float st[3];
+  int tr[3];
+  for (int a = 0; a < 3; ++a) {
+    st[a] = e->xf.t[a] - c.shift_basis[a];
+    const int f = (int)std::floor(st[a] / e->tp.cell[a]);
+    tr[a] = st[a] < 0 ? std::max(-c.voxel_shift, f) : std::min(c.voxel_shift, f);
+  }
+  for (int a = 0; a < 3; ++a)
+    if (std::abs(tr[a]) >= c.voxel_shift) {
+      engine_fetch_and_clear(e, a, tr[a]);
+      st[a] -= (float)tr[a] * e->tp.cell[a];
+    }
+  float R[9], t[3];
+  std::memcpy(R, e->xf.R, sizeof(R));
+  for (int a = 0; a < 3; ++a) t[a] = st[a] + c.shift_basis[a];
+  orc_make_xform(R, t, &e->xf);
+}
+
+// NuiKinfuScene::integrateVolume of the configured scene on the pass-filtered depth: the
+// hash scene, the fixed volume, or the shifting volume (shift, then integrate through the
+// wrap).
+static void engine_integrate(OrcEngine* e, const uint8_t* col) {
+  const OrcEngineCfg& c = e->c;
+  if (e->hs) {
+    orc_hash_scene_integrate(e->hs, e->depth.data(), col, &e->cam, &e->xf, &e->touched);
+    return;
+  }
+  if (c.voxel_shift > 0) engine_shift_volume(e);
+  int w[3];
+  engine_voxel_wrap(e, w);
+  orc_scale_depths(e->depth.data(), c.W, c.H, &e->cam);
+  orc_tsdf_integrate_wrap(e->depth.data(), col, &e->cam, &e->xf, &e->tp, e->vol.data(),
+                          c.color ? e->cvol.data() : nullptr, c.max_color_weight, &e->touched, w);
+}
+
+// NuiKinfuScene::raycastRender into the reference maps.
+static void engine_raycast(OrcEngine* e) {
+  const OrcEngineCfg& c = e->c;
+  if (e->hs) {
+    orc_hash_scene_raycast(e->hs, &e->cam, &e->xf, e->vref.data(), e->nref.data(), nullptr);
+    return;
+  }
+  int w[3];
+  engine_voxel_wrap(e, w);
+  orc_raycast_wrap(e->vol.data(), c.color ? e->cvol.data() : nullptr, &e->tp, &e->cam, &e->xf, c.W, c.H,
+                   e->vref.data(), e->nref.data(), nullptr, nullptr, w);
+}
+
 // Returns 0 on success, 1 when tracking is lost (singular ICP system).
 ORC_API int orc_engine_frame(OrcEngine* e, const uint16_t* raw, const uint8_t* bgra) {
   const OrcEngineCfg& c = e->c;
@@ -1146,16 +1375,8 @@ ORC_API int orc_engine_frame(OrcEngine* e, const uint16_t* raw, const uint8_t* b
                 c.depth_threshold, e->dl[0].data());
   orc_depth2vertex(e->dl[0].data(), W, H, &e->cam, 1, e->vl[0].data());
   const uint8_t* col = c.color ? bgra : nullptr;
-  // NuiKinfuScene::integrateVolume / raycastRender of the configured scene
-  auto integrate = [&]() {
-    if (e->hs) {
-      orc_hash_scene_integrate(e->hs, e->depth.data(), col, &e->cam, &e->xf, &e->touched);
-    } else {
-      orc_scale_depths(e->depth.data(), W, H, &e->cam);
-      orc_tsdf_integrate(e->depth.data(), col, &e->cam, &e->xf, &e->tp, e->vol.data(),
-                         c.color ? e->cvol.data() : nullptr, c.max_color_weight, &e->touched);
-    }
-  };
+  // NuiKinfuScene::integrateVolume of the configured scene
+  auto integrate = [&]() { engine_integrate(e, col); };
   const bool photometric = col && !e->cprev.empty();
   if (e->frames == 0) {
     orc_normals(e->vl[0].data(), W, H, c.depth_threshold, e->normals.data());
@@ -1182,24 +1403,36 @@ ORC_API int orc_engine_frame(OrcEngine* e, const uint16_t* raw, const uint8_t* b
                      R, t, &e->last, photometric ? &ci : nullptr);
     if (st != 0) return 1;
     orc_make_xform(R, t, &e->xf);
+    // the gate compares global translations (local + volume offset, NuiCameraPos.h:43);
+    // lastT holds the global translation of the last integration
     double rn = rel_angle(e->xf.R, e->lastR);
-    double tn = std::sqrt((double)(e->xf.t[0] - e->lastT[0]) * (e->xf.t[0] - e->lastT[0]) +
-                          (double)(e->xf.t[1] - e->lastT[1]) * (e->xf.t[1] - e->lastT[1]) +
-                          (double)(e->xf.t[2] - e->lastT[2]) * (e->xf.t[2] - e->lastT[2]));
+    float g[3];
+    engine_global_t(e, g);
+    double tn = std::sqrt((double)(g[0] - e->lastT[0]) * (g[0] - e->lastT[0]) +
+                          (double)(g[1] - e->lastT[1]) * (g[1] - e->lastT[1]) +
+                          (double)(g[2] - e->lastT[2]) * (g[2] - e->lastT[2]));
     if ((float)((rn + tn) / 2) >= c.integration_threshold) {
       integrate();
       std::memcpy(e->lastR, e->xf.R, sizeof(e->lastR));
-      std::memcpy(e->lastT, e->xf.t, sizeof(e->lastT));
+      engine_global_t(e, e->lastT);
     }
-    if (e->hs)
-      orc_hash_scene_raycast(e->hs, &e->cam, &e->xf, e->vref.data(), e->nref.data(), nullptr);
-    else
-      orc_raycast(e->vol.data(), c.color ? e->cvol.data() : nullptr, &e->tp, &e->cam, &e->xf, W, H,
-                  e->vref.data(), e->nref.data(), nullptr, nullptr);
+    engine_raycast(e);
   }
   if (photometric) std::memcpy(e->cprev.data(), col, 4 * N);  // the next frame's model colours
   e->frames += 1;
   return 0;
+}
+
+// A frame at a given camera pose: UpdateVertexBuffers, UpdateCameraTransform(R, t),
+// integrateVolume and raycastRender of the configured scene, without tracking (the
+// step-wise path of a caller that sets the pose itself).
+ORC_API void orc_engine_integrate_at(OrcEngine* e, const uint16_t* raw, const uint8_t* bgra, const float* R,
+                                     const float* t) {
+  const OrcEngineCfg& c = e->c;
+  orc_pass_filter(raw, (long)c.W * c.H, c.dmin, c.dmax, e->depth.data());
+  orc_make_xform(R, t, &e->xf);
+  engine_integrate(e, c.color ? bgra : nullptr);
+  engine_raycast(e);
 }
 
 ORC_API void orc_engine_pose(const OrcEngine* e, float* R, float* t) {
@@ -1207,6 +1440,15 @@ ORC_API void orc_engine_pose(const OrcEngine* e, float* R, float* t) {
   std::memcpy(t, e->xf.t, 3 * sizeof(float));
 }
 ORC_API const int16_t* orc_engine_volume(const OrcEngine* e) { return e->vol.data(); }
+ORC_API void orc_engine_shift_state(const OrcEngine* e, int* voff) { std::memcpy(voff, e->voff, sizeof(e->voff)); }
+// Points of the slabs that left the shifting volume: copies up to cap, returns how many
+// were found in all (more than cap were found when the cache overflowed).
+ORC_API long orc_engine_points(const OrcEngine* e, float* xyz, float* rgba, long cap) {
+  const long n = std::min(cap, (long)(e->pts_xyz.size() / 3));
+  std::memcpy(xyz, e->pts_xyz.data(), sizeof(float) * 3 * n);
+  std::memcpy(rgba, e->pts_rgba.data(), sizeof(float) * 4 * n);
+  return e->pts_n;
+}
 ORC_API OrcHash* orc_engine_hash(const OrcEngine* e) { return e->hs; }
 ORC_API const uint8_t* orc_engine_color_volume(const OrcEngine* e) {
   return e->cvol.empty() ? nullptr : e->cvol.data();

@@ -85,7 +85,8 @@ class OrcEngineCfg(C.Structure):
                 ("sigma_space2_inv_half", C.c_float), ("sigma_depth2_inv_half", C.c_float),
                 ("depth_threshold", C.c_float), ("dist_threshold", C.c_float), ("integration_threshold", C.c_float),
                 ("hash", C.c_int), ("voxel", C.c_float), ("mu", C.c_float), ("buckets", C.c_int), ("excess", C.c_int),
-                ("pool", C.c_int), ("max_w", C.c_int), ("photometric_weight", C.c_float)]
+                ("pool", C.c_int), ("max_w", C.c_int), ("photometric_weight", C.c_float),
+                ("voxel_shift", C.c_int), ("shift_basis", C.c_float * 3), ("point_cap", C.c_long)]
 
     @staticmethod
     def from_session_cfg(c):
@@ -112,6 +113,10 @@ class OrcEngineCfg(C.Structure):
         e.voxel, e.mu = c.voxel_size, c.trunc_scale
         e.buckets, e.excess, e.pool, e.max_w = c.hash_buckets, c.hash_excess, c.hash_pool_blocks, c.hash_max_weight
         e.photometric_weight = getattr(c, "photometric_weight", 0.0)
+        e.voxel_shift = getattr(c, "voxel_shift", 0)
+        for i in range(3):
+            e.shift_basis[i] = c.shift_basis[i] if hasattr(c, "shift_basis") else 0.0
+        e.point_cap = getattr(c, "shift_point_cap", 0)
         return e
 
 
@@ -138,6 +143,14 @@ def oracle():
             "orc_tsdf_init": (None, [_P, _P, C.c_long]),
             "orc_tsdf_integrate": (None, [_P, _P, _P, _P, _P, _P, _P, C.c_int, _P]),
             "orc_raycast": (None, [_P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P, _P]),
+            "orc_tsdf_integrate_wrap": (None, [_P, _P, _P, _P, _P, _P, _P, C.c_int, _P, _P]),
+            "orc_raycast_wrap": (None, [_P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P, _P, _P]),
+            "orc_raycast_wrap_mode": (None, [_P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_int]),
+            "orc_tsdf_clear_slice": (None, [_P, _P, _P, _P, _P]),
+            "orc_fetch_points": (C.c_long, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_long]),
+            "orc_engine_shift_state": (None, [_P, _P]),
+            "orc_engine_points": (C.c_long, [_P, _P, _P, C.c_long]),
+            "orc_engine_integrate_at": (None, [_P, _P, _P, _P, _P]),
             "orc_icp_rows": (None, [_P, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, C.c_float, _P, _P]),
             "orc_inverse3": (None, [_P, _P]),
             "orc_make_xform": (None, [_P, _P, _P]),
@@ -188,6 +201,11 @@ def ref():
             "ref_integrate": (None, [_P, _P, _P, _P, _P, _P, _P, C.c_uint8]),
             "ref_init_volume": (None, [_P, _P, _P]),
             "ref_raycast": (None, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int]),
+            "ref_integrate_wrap": (None, [_P, _P, _P, _P, _P, _P, _P, C.c_uint8, _P]),
+            "ref_raycast_wrap": (None, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P]),
+            "ref_clear_slice": (None, [_P, _P, _P, _P, _P]),
+            "ref_fetch_volume": (None, [_P, _P, _P, _P, _P, _P, _P]),
+            "ref_fetch_shift_volume": (None, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
             "ref_marching_cubes": (C.c_int, [_P, _P, _P, _P, _P]),
             "ref_icp_iteration": (None, [_P, _P, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_float, _P]),
             "ref_half_sample_bgra": (None, [_P, _P, C.c_int, C.c_int, C.c_uint]),
@@ -240,6 +258,26 @@ class Engine:
     def volume(self):
         ptr_ = oracle().orc_engine_volume(self.h)
         return np.ctypeslib.as_array(C.cast(ptr_, C.POINTER(C.c_int16)), shape=(self.nvox, 2)).copy()
+
+    def integrate_at(self, depth, R, t, bgra=None):
+        """A frame at the given pose without tracking: integrate (shifting first) and raycast."""
+        Rf = np.ascontiguousarray(R, np.float32).reshape(9)
+        tf = np.ascontiguousarray(t, np.float32).reshape(3)
+        oracle().orc_engine_integrate_at(self.h, p(depth), p(bgra), p(Rf), p(tf))
+
+    def shift_state(self):
+        """The shifting volume's voxel offset (m_voxel_offset)."""
+        v = np.zeros(3, np.int32)
+        oracle().orc_engine_shift_state(self.h, p(v))
+        return v
+
+    def points(self, cap=1 << 22):
+        """(xyz[n, 3], rgba[n, 4], found) of the slabs that left the shifting volume."""
+        xyz = np.zeros((cap, 3), np.float32)
+        rgba = np.zeros((cap, 4), np.float32)
+        n = oracle().orc_engine_points(self.h, p(xyz), p(rgba), cap)
+        k = min(n, cap, int(self.cfg.point_cap))
+        return xyz[:k].copy(), rgba[:k].copy(), n
 
     def refmap(self, which):
         ptr_ = oracle().orc_engine_refmap(self.h, which)
