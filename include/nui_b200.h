@@ -99,6 +99,18 @@ typedef struct {
    * of the finest level; 0 = depth only.  Needs color_volume = 1 and BGRA frames whose
    * valid pixels have alpha 255.  Colours and gradients enter in units of 1/255. */
   float photometric_weight;
+  /* shifting dense volume: the reference's eScene_ShiftingVolume (NuiKinfuOpenCLShiftScene,
+   * NuiSLAMController.cpp:55-62; NuiKinfuVolumeConfig voxel_shift / translateBasis).  On an
+   * integrating frame, every axis on which the tracked camera lies voxel_shift or more
+   * voxels from shift_basis moves the volume by voxel_shift voxels before the integration:
+   * the slab that leaves is fetched as points (fetchShiftVolumeKernel) into a device cache
+   * of shift_point_cap points and cleared, the volume's voxel offset moves forward and the
+   * session's (local) pose back.  Poses are then local to the volume: global = local +
+   * offset (nui_shift_state).  0 = fixed volume (default); dense volumes only;
+   * voxel_shift < res on every axis. */
+  int voxel_shift;
+  float shift_basis[3];
+  int shift_point_cap;        /* default 2^20 (28 MB) */
 } nui_session_cfg;
 
 typedef struct nui_ctx nui_ctx;
@@ -265,7 +277,8 @@ NUI_API nui_session* nui_server_session(nui_server* srv, int slot);
 /* Per-stage device time of the last nui_batch_tick* / nui_process_frame* call of the
  * context, when timing is enabled (CUDA events on the context stream).
  * stage: 0 preprocess, 1 pyramid + feedback maps, 2 tracking (colour gradients, ICP, gate),
- * 3 dense integration kernel, 4 brick summaries + voxel-hash allocation / integration,
+ * 3 shifting-volume shifts + dense integration kernel, 4 brick summaries + voxel-hash
+ * allocation / integration,
  * 5 raycast (dense and hash), 6 whole tick. */
 NUI_API nui_status nui_ctx_enable_timing(nui_ctx* ctx, int enable);
 NUI_API nui_status nui_ctx_stage_ms(nui_ctx* ctx, int stage, float* ms);
@@ -301,6 +314,28 @@ NUI_API nui_status nui_ctx_set_tuning(nui_ctx* ctx, const nui_tuning* t);
 NUI_API nui_status nui_ctx_autotune(nui_ctx* ctx, const nui_session_cfg* cfgs, int n,
                                     const uint16_t* const* depth_mm, const uint8_t* const* bgra, int frames,
                                     int repeats, nui_tuning* out, float* out_tick_ms);
+/* Shifting volume state (NuiKinfuOpenCLShiftScene m_voxel_offset / getVoxelOffsetSize,
+ * NuiKinfuOpenCLShiftScene.cpp:58-66): the volume's offset in voxels and metres (the
+ * camera's global translation is its pose's translation plus offset_m) and how many points
+ * the slabs that left the volume gave (more than shift_point_cap: the cache overflowed).
+ * Any pointer may be NULL. */
+NUI_API nui_status nui_shift_state(nui_session* s, int* voxel_offset, float* offset_m, uint64_t* points_found);
+/* The point cache of a shifting volume (the reference appends the same points to its
+ * NuiKinfuVertexCache, NuiKinfuOpenCLShiftScene.cpp:206-228): copies up to cap points to
+ * host xyz (3 floats each) / rgba (4 floats each) and returns in *n how many the cache
+ * holds.  Points come in no fixed order (the kernel appends them atomically, like the
+ * reference's). */
+NUI_API nui_status nui_shift_points(nui_session* s, float* xyz, float* rgba, uint64_t cap, uint64_t* n);
+NUI_API nui_status nui_shift_points_clear(nui_session* s);
+/* Point cloud of a dense volume: Volume2CLVertices of the dense scenes (fetchVolumeKernel,
+ * extract.cl:4-79, NuiKinfuOpenCLScene; fetchShiftVolumeKernel, extract.cl:82-179, over
+ * the whole buffer of a shifting volume, NuiKinfuOpenCLShiftScene.cpp:354-520): a point
+ * per voxel whose tsdf is exactly 0 and per sign change between z-neighbours, with its
+ * colour (0,0,0,1 without a colour volume).  Writes up to cap points to device d_xyz (3
+ * floats each, 4-byte aligned) / d_rgba (4 floats each, 16-byte aligned) in no fixed
+ * order and returns in *found how many exist.  Synchronous. */
+NUI_API nui_status nui_point_cloud_device(nui_session* s, float* d_xyz, float* d_rgba, uint64_t cap,
+                                          uint64_t* found);
 /* Voxels read-modify-written by the last integration of a session. */
 NUI_API nui_status nui_session_touched_voxels(nui_session* s, uint64_t* n);
 

@@ -42,6 +42,7 @@ class SessionCfg(C.Structure):
         ("voxel_size", C.c_float), ("trunc_scale", C.c_float), ("hash_buckets", C.c_int),
         ("hash_excess", C.c_int), ("hash_pool_blocks", C.c_int), ("hash_max_weight", C.c_int),
         ("photometric_weight", C.c_float),
+        ("voxel_shift", C.c_int), ("shift_basis", C.c_float * 3), ("shift_point_cap", C.c_int),
     ]
 
 
@@ -110,6 +111,10 @@ _SIGS = {
     "nui_ctx_stage_ms": (C.c_int, [_P, C.c_int, _P]),
     "nui_ctx_last_tick_kernels": (C.c_int, [_P, _P]),
     "nui_ctx_get_tuning": (C.c_int, [_P, _P]),
+    "nui_shift_state": (C.c_int, [_P, _P, _P, _P]),
+    "nui_shift_points": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
+    "nui_shift_points_clear": (C.c_int, [_P]),
+    "nui_point_cloud_device": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
     "nui_ctx_set_tuning": (C.c_int, [_P, _P]),
     "nui_ctx_autotune": (C.c_int, [_P, _P, C.c_int, _P, _P, C.c_int, C.c_int, _P, _P]),
     "nui_session_touched_voxels": (C.c_int, [_P, _P]),
@@ -340,6 +345,40 @@ class Session:
         v = C.c_uint64()
         check(lib().nui_session_touched_voxels(self.h, C.byref(v)))
         return v.value
+
+    def shift_state(self):
+        """(voxel offset int32[3], offset in metres float32[3], points found) of a shifting
+        volume; the camera's global translation is its pose's plus the offset."""
+        vo = np.zeros(3, np.int32)
+        om = np.zeros(3, np.float32)
+        n = C.c_uint64()
+        check(lib().nui_shift_state(self.h, ptr(vo), ptr(om), C.byref(n)))
+        return vo, om, n.value
+
+    def shift_points(self, cap=None):
+        """(xyz[n, 3], rgba[n, 4]) of the point cache of the slabs that left the volume."""
+        n = C.c_uint64()
+        check(lib().nui_shift_points(self.h, None, None, 0, C.byref(n)))
+        k = n.value if cap is None else min(cap, n.value)
+        xyz = np.zeros((k, 3), np.float32)
+        rgba = np.zeros((k, 4), np.float32)
+        if k:
+            check(lib().nui_shift_points(self.h, ptr(xyz), ptr(rgba), k, C.byref(n)))
+        return xyz, rgba
+
+    def clear_shift_points(self):
+        check(lib().nui_shift_points_clear(self.h))
+
+    def point_cloud(self, cap=1 << 22):
+        """Point cloud of a dense volume (fetchVolumeKernel): (xyz[n, 3], rgba[n, 4], found)."""
+        import torch
+        xyz = torch.empty((cap, 3), dtype=torch.float32, device="cuda")
+        rgba = torch.empty((cap, 4), dtype=torch.float32, device="cuda")
+        n = C.c_uint64()
+        check(lib().nui_point_cloud_device(self.h, C.c_void_p(xyz.data_ptr()), C.c_void_p(rgba.data_ptr()), cap,
+                                           C.byref(n)))
+        k = min(n.value, cap)
+        return xyz[:k].cpu().numpy(), rgba[:k].cpu().numpy(), n.value
 
     def download(self, what, level=0):
         W, H = self.W >> level, self.H >> level

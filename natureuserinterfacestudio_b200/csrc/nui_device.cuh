@@ -40,10 +40,16 @@ struct TrackState {
   int status;            // 0 ok, 3 tracking lost
   int integrate;         // integration gate of this frame
   int iterations_run;
-  float lastR[9], lastT[3];  // pose of the last integration
+  float lastR[9], lastT[3];  // pose of the last integration (global translation: local +
+                             // volume offset, NuiCameraPos.h:43)
   unsigned int block_counter;
   int dmax_bits;         // largest ray-length depth of the frame (float bits, >= 0)
   unsigned long long touched;
+  // shifting volume: voxel offset of the volume (m_voxel_offset), this frame's shift in
+  // voxels per axis (0: none), points found in the slabs that left the volume
+  int voff[3];
+  int shift[3];
+  unsigned long long points;
 };
 
 // What one session does in the current tick (host-written, read by every kernel).
@@ -85,6 +91,13 @@ struct SessionDesc {
   int max_cw;
   int zchunks;                    // integration: z chunks per column (one thread each)
   float* ztab;                    // integration: running sums shared by all columns, 2 (rz + 1)
+  // shifting volume (0: fixed): shift distance in voxels, basis translation, and the point
+  // cache of the slabs that leave the volume (pts_cap points of xyz / rgba floats)
+  int voxel_shift;
+  float shift_basis[3];
+  float* pts_xyz;
+  float* pts_rgba;
+  long long pts_cap;
   // colour tracking: weight of the photometric term (0: depth only); the previous frame's
   // colours (the model colours of the reference maps); the frame's colour pyramid (level 0
   // is bgra) and its x / y gradients per level (signed bytes)
@@ -241,6 +254,11 @@ struct Voxel<3> {  // NUI_TSDF_F16_F16: half2 (tsdf, weight)
     reinterpret_cast<__half2*>(s.vol)[i] = __floats2half2_rn(1.f, 0.f);
   }
 };
+
+// The reference's voxelWrap component of a shifting volume at voxel offset `off` on an
+// axis of r voxels (getVoxelWrap, NuiKinfuOpenCLShiftScene.cpp:44-56): voxel x of the
+// volume sits at (x + wrap) % r of the reference's buffer.
+__device__ __forceinline__ int ref_wrap(int off, int r) { return off >= 0 ? off : r - ((-off) % r); }
 
 __device__ __forceinline__ size_t vox_index(const SessionDesc& s, int x, int y, int z) {
   return (size_t)x + (size_t)s.res[0] * ((size_t)y + (size_t)s.res[1] * (size_t)z);

@@ -428,21 +428,60 @@ __device__ void fill_ztab(const SessionDesc& s, const TrackState* ts) {
   }
 }
 
-// The table for an integration the host requests directly (step-wise calls).
-__global__ void k_ztab(const SessionDesc* __restrict__ descs) {
-  const SessionDesc& s = descs[blockIdx.x];
-  if (threadIdx.x == 0 && s.kind >= 0) fill_ztab(s, s.ts);
+// NuiKinfuOpenCLShiftScene::integrateVolume -> shiftVolume (NuiKinfuOpenCLShiftScene.cpp:
+// 288-362): before a shifting volume integrates, every axis on which the camera lies
+// voxel_shift or more voxels from the basis moves the volume by voxel_shift voxels; the
+// camera's local translation moves back by the same distance and the offset forward.  The
+// frame's shift is left in ts->shift for the fetch / roll kernels that follow.
+__device__ void shift_decide(const SessionDesc& s, TrackState* ts) {
+  ts->shift[0] = ts->shift[1] = ts->shift[2] = 0;
+  const int vs = s.voxel_shift;
+  if (vs <= 0 || s.fmt < 0) return;
+  float st[3];
+  int tr[3];
+  for (int a = 0; a < 3; ++a) {
+    st[a] = ts->xf.t[a] - s.shift_basis[a];
+    const int f = (int)floorf(st[a] / s.cell[a]);
+    tr[a] = st[a] < 0.f ? max(-vs, f) : min(vs, f);
+  }
+  for (int a = 0; a < 3; ++a)
+    if (abs(tr[a]) >= vs) {
+      ts->shift[a] = tr[a];
+      ts->voff[a] += tr[a];
+      st[a] -= (float)tr[a] * s.cell[a];
+    }
+  for (int a = 0; a < 3; ++a) {
+    ts->xf.t[a] = st[a] + s.shift_basis[a];
+    ts->t[a] = ts->xf.t[a];
+  }
 }
 
-__global__ void k_track_finalize(const SessionDesc* __restrict__ descs) {
+// The table for an integration the host requests directly (step-wise calls), after the
+// shift that integration makes.
+__global__ void k_ztab(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.x];
+  if (threadIdx.x == 0 && s.kind >= 0) {
+    shift_decide(s, s.ts);
+    fill_ztab(s, s.ts);
+  }
+}
+
+// shift_now: the tick's finalize makes the shifting volume's shift of an integrating
+// frame here; the step-wise track leaves it to the integration call (k_ztab).
+__global__ void k_track_finalize(const SessionDesc* __restrict__ descs, int shift_now) {
   const SessionDesc& s = descs[blockIdx.x];
   if (threadIdx.x != 0 || s.kind < 0) return;
   TrackState* ts = s.ts;
   if (s.kind == kFirstFrame) {
     ts->integrate = ts->status == 0 ? 1 : 0;
-    if (ts->integrate) fill_ztab(s, ts);
+    ts->shift[0] = ts->shift[1] = ts->shift[2] = 0;
+    if (ts->integrate) {
+      if (shift_now) shift_decide(s, ts);
+      fill_ztab(s, ts);
+    }
     return;
   }
+  ts->shift[0] = ts->shift[1] = ts->shift[2] = 0;
   if (ts->status != 0) {  // tracking lost: keep the previous pose, skip the rest
     for (int i = 0; i < 9; ++i) ts->R[i] = ts->xf.R[i];
     for (int i = 0; i < 3; ++i) ts->t[i] = ts->xf.t[i];
@@ -467,14 +506,19 @@ __global__ void k_track_finalize(const SessionDesc* __restrict__ descs) {
     for (int k = 0; k < 3; ++k) tr += (double)ts->R[k * 3 + i] * (double)ts->lastR[k * 3 + i];
   const double cv = fmin(1.0, fmax(-1.0, (tr - 1.0) / 2.0));
   const double rn = acos(cv);
+  // translations compared globally: local + the volume's offset (0 for a fixed volume)
   double tn = 0;
-  for (int i = 0; i < 3; ++i) tn += ((double)ts->t[i] - ts->lastT[i]) * ((double)ts->t[i] - ts->lastT[i]);
+  for (int i = 0; i < 3; ++i) {
+    const float g = ts->voff[i] ? ts->t[i] + (float)ts->voff[i] * s.cell[i] : ts->t[i];
+    tn += ((double)(g - ts->lastT[i])) * ((double)(g - ts->lastT[i]));
+  }
   tn = sqrt(tn);
   ts->integrate = ((float)((rn + tn) / 2) >= s.integ_thr) ? 1 : 0;
   if (ts->integrate) {
+    if (shift_now) shift_decide(s, ts);
     fill_ztab(s, ts);
     for (int i = 0; i < 9; ++i) ts->lastR[i] = ts->R[i];
-    for (int i = 0; i < 3; ++i) ts->lastT[i] = ts->t[i];
+    for (int i = 0; i < 3; ++i) ts->lastT[i] = ts->voff[i] ? ts->t[i] + (float)ts->voff[i] * s.cell[i] : ts->t[i];
   }
 }
 

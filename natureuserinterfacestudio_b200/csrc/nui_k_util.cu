@@ -35,11 +35,13 @@ __global__ void k_export_ref(const SessionDesc* __restrict__ descs, short2* out,
   const SessionDesc& s = descs[0];
   const int rx = s.res[0], ry = s.res[1], rz = s.res[2];
   const size_t n = (size_t)rx * ry * rz;
+  // a shifting volume's voxel sits in the reference's buffer at its wrap
+  const int wx = ref_wrap(s.ts->voff[0], rx), wy = ref_wrap(s.ts->voff[1], ry), wz = ref_wrap(s.ts->voff[2], rz);
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const int x = (int)(i % rx);
     const int y = (int)((i / rx) % ry);
     const int z = (int)(i / ((size_t)rx * ry));
-    const size_t o = ((size_t)x + (size_t)y * rx) * rz + z;
+    const size_t o = ((size_t)((x + wx) % rx) + (size_t)((y + wy) % ry) * rx) * rz + (z + wz) % rz;
     if (out) {
       if (FMT == 0) {
         out[o] = reinterpret_cast<const short2*>(s.vol)[i];
@@ -76,11 +78,12 @@ __global__ void k_import_ref(const SessionDesc* __restrict__ descs, const short2
   const SessionDesc& s = descs[0];
   const int rx = s.res[0], ry = s.res[1], rz = s.res[2];
   const size_t n = (size_t)rx * ry * rz;
+  const int wx = ref_wrap(s.ts->voff[0], rx), wy = ref_wrap(s.ts->voff[1], ry), wz = ref_wrap(s.ts->voff[2], rz);
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const int x = (int)(i % rx);
     const int y = (int)((i / rx) % ry);
     const int z = (int)(i / ((size_t)rx * ry));
-    const short2 v = in[((size_t)x + (size_t)y * rx) * rz + z];
+    const short2 v = in[((size_t)((x + wx) % rx) + (size_t)((y + wy) % ry) * rx) * rz + (z + wz) % rz];
     if (FMT == 0)
       reinterpret_cast<short2*>(s.vol)[i] = v;
     else

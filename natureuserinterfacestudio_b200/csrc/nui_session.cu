@@ -31,7 +31,7 @@ __global__ void k_pyramid(const SessionDesc*, int);
 __global__ void k_feedback(const SessionDesc*);
 template <int PPT>
 __global__ void k_icp(const SessionDesc*, int, int);
-__global__ void k_track_finalize(const SessionDesc*);
+__global__ void k_track_finalize(const SessionDesc*, int);
 __global__ void k_ztab(const SessionDesc*);
 __global__ void k_color_level(const SessionDesc*, int);
 __global__ void k_color_grad(const SessionDesc*);
@@ -64,6 +64,15 @@ template <int F>
 __global__ void k_hash_raycast(const SessionDesc*, int);
 __global__ void k_hash_reset(const SessionDesc*);
 __global__ void k_hash_export_voxels(const SessionDesc*, uint8_t*);
+template <int F>
+__global__ void k_shift_fetch(const SessionDesc*, int);
+template <int F>
+__global__ void k_fetch_volume(const SessionDesc*, float*, float*, long long, unsigned long long*);
+template <typename T>
+__global__ void k_shift_roll_x(const SessionDesc*, int);
+template <typename T>
+__global__ void k_shift_roll_yz(const SessionDesc*, int, int);
+__global__ void k_shift_dirty(const SessionDesc*);
 template <int F>
 __global__ void k_export_ref(const SessionDesc*, short2*, uchar4*);
 template <int F>
@@ -104,6 +113,8 @@ struct BatchPlan {
   int hashMask;             // bit per hash sdf format
   int fmtMask;
   int colorIcp;             // some session tracks with the photometric term
+  int shiftFmtMask;         // bit per dense format of the shifting sessions
+  int shiftColor;           // some shifting session has a colour volume
   nui_tuning tune;          // the context's launch shapes
   BatchPlan() { std::memset(this, 0, sizeof(*this)); }
   bool operator<(const BatchPlan& o) const { return std::memcmp(this, &o, sizeof(BatchPlan)) < 0; }
@@ -126,6 +137,7 @@ struct nui_ctx {
   // scratch descriptor for kernel-level calls
   SessionDesc* d_kdesc = nullptr;
   TrackState* d_kts = nullptr;
+  unsigned long long* d_count = nullptr;  // counter of the point-cloud fetch
   struct Graph {
     cudaGraphExec_t exec;
     int kernels;  // kernel launches per replay
@@ -162,6 +174,8 @@ struct nui_session {
   uchar4* cprev = nullptr;        // colour tracking: the previous frame's colours and the
   uchar4* cgx[kMaxLevels] = {};   // current frame's gradients (level 0)
   uchar4* cgy[kMaxLevels] = {};
+  float* pts_xyz = nullptr;   // shifting volume: point cache of the slabs that left
+  float* pts_rgba = nullptr;
   SessionDesc* d_desc1 = nullptr;
   // voxel-block hash
   bool hash = false;
@@ -215,6 +229,14 @@ bool cfg_valid(const nui_session_cfg* c, std::string& why) {
   if (!(c->photometric_weight >= 0.f) || !(c->photometric_weight < 1e30f))
     return why = "photometric weight must be finite and >= 0", false;
   if (c->photometric_weight > 0.f && !c->color_volume) return why = "colour tracking needs color_volume = 1", false;
+  if (c->voxel_shift < 0 || c->shift_point_cap < 0) return why = "voxel shift and point cap must be >= 0", false;
+  if (c->voxel_shift > 0) {
+    if (c->volume_kind != NUI_VOLUME_DENSE) return why = "a shifting volume must be dense", false;
+    for (int i = 0; i < 3; ++i) {
+      if (c->voxel_shift >= c->res[i]) return why = "voxel shift must be below the volume resolution", false;
+      if (!(c->shift_basis[i] > -1e30f && c->shift_basis[i] < 1e30f)) return why = "shift basis must be finite", false;
+    }
+  }
   return true;
 }
 
@@ -285,6 +307,11 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
   d.occ3 = s->occ3;
   d.max_cw = c.max_color_weight;
   d.zchunks = pick_zchunks(s->cfg, s->ctx->tune.integrate_threads_log2);
+  d.voxel_shift = s->hash ? 0 : c.voxel_shift;
+  for (int i = 0; i < 3; ++i) d.shift_basis[i] = c.shift_basis[i];
+  d.pts_xyz = s->pts_xyz;
+  d.pts_rgba = s->pts_rgba;
+  d.pts_cap = s->pts_xyz ? c.shift_point_cap : 0;
   d.ts = s->ts;
   d.partials = s->partials;
   // colour tracking runs on frames that carry colour, once its buffers exist
@@ -343,6 +370,10 @@ void plan_add(BatchPlan& p, const nui_session* s) {
   p.maxBricks[c.tsdf_format] = std::max(p.maxBricks[c.tsdf_format], nb);
   const long nh = (long)((c.res[0] + 127) / 128) * ((c.res[1] + 127) / 128) * ((c.res[2] + 127) / 128);
   p.maxHyper = std::max(p.maxHyper, nh);
+  if (c.voxel_shift > 0) {
+    p.shiftFmtMask |= 1 << c.tsdf_format;
+    if (c.color_volume) p.shiftColor = 1;
+  }
 }
 
 // Elementwise maximum of two launch shapes (n stays a's).
@@ -360,6 +391,8 @@ void plan_merge(BatchPlan& a, const BatchPlan& b) {
   a.hashMask |= b.hashMask;
   a.fmtMask |= b.fmtMask;
   a.colorIcp |= b.colorIcp;
+  a.shiftFmtMask |= b.shiftFmtMask;
+  a.shiftColor |= b.shiftColor;
 }
 
 unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
@@ -427,9 +460,43 @@ void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t 
   if (p.hashMask & 2) k_hash_raycast<1><<<dim3(tiles, p.n), 128, 0, st>>>(d, tw);
 }
 
+// The shifts of the shifting volumes (after tracking, before integration): per axis, the
+// leaving slab's points, then the roll of every per-voxel array; then all bricks dirty.
+// Without a shift every launch returns at once.
+constexpr unsigned kShiftBlocks = 592;
+template <int F>
+void launch_shift_fetch(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, int axis) {
+  if (p.shiftFmtMask & (1 << F)) k_shift_fetch<F><<<dim3(kShiftBlocks, p.n), 256, 0, st>>>(d, axis);
+}
+template <typename T>
+void launch_roll(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, int axis, int which) {
+  if (axis == 0)
+    k_shift_roll_x<T><<<dim3(kShiftBlocks, p.n), 256, 0, st>>>(d, which);
+  else
+    k_shift_roll_yz<T><<<dim3(kShiftBlocks, p.n), 256, 0, st>>>(d, axis, which);
+}
+void launch_shift(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
+  if (!p.shiftFmtMask) return;
+  for (int axis = 0; axis < 3; ++axis) {
+    launch_shift_fetch<0>(p, d, st, axis);
+    launch_shift_fetch<1>(p, d, st, axis);
+    launch_shift_fetch<2>(p, d, st, axis);
+    launch_shift_fetch<3>(p, d, st, axis);
+    if (p.shiftFmtMask & 0b1001) launch_roll<uint32_t>(p, d, st, axis, 0);  // short2, half2
+    if (p.shiftFmtMask & 0b0010) launch_roll<unsigned long long>(p, d, st, axis, 0);  // float2
+    if (p.shiftFmtMask & 0b0100) {  // half plane + u8 weight plane
+      launch_roll<uint16_t>(p, d, st, axis, 0);
+      launch_roll<uint8_t>(p, d, st, axis, 1);
+    }
+    if (p.shiftColor) launch_roll<uint32_t>(p, d, st, axis, 2);
+  }
+  k_shift_dirty<<<dim3(kShiftBlocks, p.n), 256, 0, st>>>(d);
+}
+
 // Colour pyramid (if any session tracks with colour), the ICP iterations of every level,
 // the integration gate and the published pose.
-void launch_track(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, float* d_pose, int* d_status) {
+void launch_track(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, float* d_pose, int* d_status,
+                  bool tick = true) {
   const unsigned npix = cdiv((long)p.maxW * p.maxH, 256);
   if (p.colorIcp) k_color_grad<<<dim3(npix, p.n, 1), 256, 0, st>>>(d);  // finest level
   const int ppt = p.tune.icp_pixels_per_thread, per = 256 * ppt;
@@ -442,7 +509,7 @@ void launch_track(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, flo
       else k_icp<4><<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
     }
   }
-  k_track_finalize<<<p.n, 32, 0, st>>>(d);
+  k_track_finalize<<<p.n, 32, 0, st>>>(d, tick ? 1 : 0);
   k_publish<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n, d_pose, d_status);
   if (p.colorIcp) k_color_keep<<<dim3(npix, p.n), 256, 0, st>>>(d);
 }
@@ -464,6 +531,7 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
   mark(2);
   launch_track(p, d, st, d_pose, d_status);
   mark(3);
+  launch_shift(p, d, st);
   launch_integrate<0>(p, d, st);
   launch_integrate<1>(p, d, st);
   launch_integrate<2>(p, d, st);
@@ -695,6 +763,8 @@ NUI_API void nui_session_cfg_default(nui_session_cfg* c) {
   c->hash_excess = 0x30000;
   c->hash_pool_blocks = 1 << 20;
   c->hash_max_weight = 255;
+  c->voxel_shift = 0;
+  c->shift_point_cap = 1 << 20;
 }
 
 NUI_API nui_status nui_ctx_create(int device, nui_ctx** out) {
@@ -713,7 +783,8 @@ NUI_API nui_status nui_ctx_create(int device, nui_ctx** out) {
   c->stream = c->own;
   for (int i = 0; i < kStages; ++i) cudaEventCreate(&c->ev[i]);
   if (cudaMalloc(&c->d_kdesc, sizeof(SessionDesc)) != cudaSuccess ||
-      cudaMalloc(&c->d_kts, sizeof(TrackState)) != cudaSuccess) {
+      cudaMalloc(&c->d_kts, sizeof(TrackState)) != cudaSuccess ||
+      cudaMalloc(&c->d_count, sizeof(unsigned long long)) != cudaSuccess) {
     delete c;
     return fail(NUI_ERR_OOM, "context scratch");
   }
@@ -735,6 +806,7 @@ NUI_API nui_status nui_ctx_destroy(nui_ctx* c) {
   cudaFreeHost(c->h_status);
   cudaFree(c->d_kdesc);
   cudaFree(c->d_kts);
+  cudaFree(c->d_count);
   cudaStreamDestroy(c->own);
   delete c;
   return NUI_OK;
@@ -906,6 +978,7 @@ NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
   b += (size_t)((c->res[0] + 31) / 32) * ((c->res[1] + 31) / 32) * ((c->res[2] + 31) / 32);
   b += (size_t)((c->res[0] + 127) / 128) * ((c->res[1] + 127) / 128) * ((c->res[2] + 127) / 128);
   b += 2 * ((size_t)c->res[2] + 1) * sizeof(float);
+  if (c->voxel_shift > 0) b += (size_t)c->shift_point_cap * 28;
   return b;
 }
 
@@ -967,6 +1040,9 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
   }
   if (ok && c.photometric_weight > 0.f)
     ok = alloc((void**)&s->cprev, N * 4) && alloc((void**)&s->cgx[0], N * 4) && alloc((void**)&s->cgy[0], N * 4);
+  if (ok && !s->hash && c.voxel_shift > 0 && c.shift_point_cap > 0)
+    ok = alloc((void**)&s->pts_xyz, (size_t)c.shift_point_cap * 12) &&
+         alloc((void**)&s->pts_rgba, (size_t)c.shift_point_cap * 16);
   if (!ok) {
     for (void* p : s->allocs) cudaFree(p);
     delete s;
@@ -1071,6 +1147,69 @@ NUI_API nui_status nui_get_pose(nui_session* s, float* pose12) {
   return NUI_OK;
 }
 
+NUI_API nui_status nui_shift_state(nui_session* s, int* voxel_offset, float* offset_m, uint64_t* points_found) {
+  if (!s) return fail(NUI_ERR_INVALID_ARG, "null session");
+  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  TrackState t;
+  NUI_CUDA(cudaMemcpy(&t, s->ts, sizeof(t), cudaMemcpyDeviceToHost));
+  for (int a = 0; a < 3; ++a) {
+    if (voxel_offset) voxel_offset[a] = t.voff[a];
+    if (offset_m) offset_m[a] = (float)t.voff[a] * s->cell[a];
+  }
+  if (points_found) *points_found = t.points;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_shift_points(nui_session* s, float* xyz, float* rgba, uint64_t cap, uint64_t* n) {
+  if (!s || !n || (cap && (!xyz || !rgba))) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  unsigned long long found = 0;
+  NUI_CUDA(cudaMemcpy(&found, &s->ts->points, sizeof(found), cudaMemcpyDeviceToHost));
+  const uint64_t kept = s->pts_xyz ? std::min<uint64_t>(found, (uint64_t)s->cfg.shift_point_cap) : 0;
+  const uint64_t k = std::min(kept, cap);
+  if (k) {
+    NUI_CUDA(cudaMemcpy(xyz, s->pts_xyz, k * 12, cudaMemcpyDeviceToHost));
+    NUI_CUDA(cudaMemcpy(rgba, s->pts_rgba, k * 16, cudaMemcpyDeviceToHost));
+  }
+  *n = kept;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_shift_points_clear(nui_session* s) {
+  if (!s) return fail(NUI_ERR_INVALID_ARG, "null session");
+  NUI_CUDA(cudaMemsetAsync(&s->ts->points, 0, sizeof(unsigned long long), s->ctx->stream));
+  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_point_cloud_device(nui_session* s, float* d_xyz, float* d_rgba, uint64_t cap,
+                                          uint64_t* found) {
+  if (!s || !found || (cap && (!d_xyz || !d_rgba))) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  if (s->hash) return fail(NUI_ERR_INVALID_ARG, "not a dense session");
+  if (((uintptr_t)d_rgba & 15) || ((uintptr_t)d_xyz & 3)) return fail(NUI_ERR_INVALID_ARG, "misaligned buffers");
+  nui_ctx* ctx = s->ctx;
+  nui_status st = ensure_cap(ctx, 1);
+  if (st != NUI_OK) return st;
+  SessionDesc d;
+  fill_desc(s, d, kInactive, nullptr, nullptr);
+  NUI_CUDA(cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, ctx->stream));
+  unsigned long long* counter = ctx->d_count;
+  NUI_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), ctx->stream));
+  const long long c = (long long)std::min<uint64_t>(cap, (uint64_t)1 << 62);
+  switch (s->cfg.tsdf_format) {
+    case 0: k_fetch_volume<0><<<1184, 256, 0, ctx->stream>>>(s->d_desc1, d_xyz, d_rgba, c, counter); break;
+    case 1: k_fetch_volume<1><<<1184, 256, 0, ctx->stream>>>(s->d_desc1, d_xyz, d_rgba, c, counter); break;
+    case 2: k_fetch_volume<2><<<1184, 256, 0, ctx->stream>>>(s->d_desc1, d_xyz, d_rgba, c, counter); break;
+    default: k_fetch_volume<3><<<1184, 256, 0, ctx->stream>>>(s->d_desc1, d_xyz, d_rgba, c, counter); break;
+  }
+  NUI_CUDA(cudaGetLastError());
+  unsigned long long n = 0;
+  NUI_CUDA(cudaMemcpyAsync(&n, counter, sizeof(n), cudaMemcpyDeviceToHost, ctx->stream));
+  NUI_CUDA(cudaStreamSynchronize(ctx->stream));
+  *found = n;
+  return NUI_OK;
+}
+
 NUI_API nui_status nui_session_touched_voxels(nui_session* s, uint64_t* n) {
   if (!s || !n) return fail(NUI_ERR_INVALID_ARG, "null argument");
   NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
@@ -1103,9 +1242,10 @@ nui_status run_stage(nui_session* s, int what) {
     for (int l = 1; l < p.maxLevels; ++l)
       k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), 1), 256, 0, st>>>(dd, l);
   } else if (what == 1) {
-    launch_track(p, dd, st, ctx->d_pose, ctx->d_status);
+    launch_track(p, dd, st, ctx->d_pose, ctx->d_status, false);
   } else if (what == 2) {
     k_ztab<<<1, 32, 0, st>>>(dd);
+    launch_shift(p, dd, st);
     launch_integrate<0>(p, dd, st);
     launch_integrate<1>(p, dd, st);
     launch_integrate<2>(p, dd, st);

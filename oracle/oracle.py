@@ -265,6 +265,12 @@ class Engine:
         tf = np.ascontiguousarray(t, np.float32).reshape(3)
         oracle().orc_engine_integrate_at(self.h, p(depth), p(bgra), p(Rf), p(tf))
 
+    def color_volume(self):
+        ptr_ = oracle().orc_engine_color_volume(self.h)
+        if not ptr_:
+            return None
+        return np.ctypeslib.as_array(C.cast(ptr_, C.POINTER(C.c_uint8)), shape=(self.nvox, 4)).copy()
+
     def shift_state(self):
         """The shifting volume's voxel offset (m_voxel_offset)."""
         v = np.zeros(3, np.int32)
