@@ -327,15 +327,29 @@ NUI_API nui_status nui_shift_state(nui_session* s, int* voxel_offset, float* off
  * reference's). */
 NUI_API nui_status nui_shift_points(nui_session* s, float* xyz, float* rgba, uint64_t cap, uint64_t* n);
 NUI_API nui_status nui_shift_points_clear(nui_session* s);
-/* Point cloud of a dense volume: Volume2CLVertices of the dense scenes (fetchVolumeKernel,
- * extract.cl:4-79, NuiKinfuOpenCLScene; fetchShiftVolumeKernel, extract.cl:82-179, over
- * the whole buffer of a shifting volume, NuiKinfuOpenCLShiftScene.cpp:354-520): a point
- * per voxel whose tsdf is exactly 0 and per sign change between z-neighbours, with its
- * colour (0,0,0,1 without a colour volume).  Writes up to cap points to device d_xyz (3
- * floats each, 4-byte aligned) / d_rgba (4 floats each, 16-byte aligned) in no fixed
- * order and returns in *found how many exist.  Synchronous. */
+/* Point cloud of a session's scene, Volume2CLVertices of the reference's scenes.  Dense:
+ * fetchVolumeKernel (extract.cl:4-79, NuiKinfuOpenCLScene), or fetchShiftVolumeKernel
+ * (extract.cl:82-179) over the whole buffer of a shifting volume
+ * (NuiKinfuOpenCLShiftScene.cpp:354-520): a point per voxel whose tsdf is exactly 0 and per
+ * sign change between z-neighbours.  Voxel hash: fetchHashScene_kernel
+ * (KinfuHashVisualization.cl:5-52, NuiKinfuOpenCLHashScene.cpp:1066-1180) over the last
+ * frame's visible blocks: a point per weighted voxel within the truncation band.  Points
+ * carry their colour / 255 (0,0,0,1 without colour).  Writes up to cap points to device
+ * d_xyz (3 floats each, 4-byte aligned) / d_rgba (4 floats each, 16-byte aligned) in no
+ * fixed order and returns in *found how many exist.  Synchronous. */
 NUI_API nui_status nui_point_cloud_device(nui_session* s, float* d_xyz, float* d_rgba, uint64_t cap,
                                           uint64_t* found);
+/* Session snapshot / restore (checkpointing; the reference keeps no such state on disk).
+ * A snapshot holds everything a session carries from frame to frame: the volume or the
+ * hash table and voxel pool, the tracker state and pose, the reference maps of the last
+ * raycast, the colour-tracking model colours and a shifting volume's offset and point
+ * cache.  nui_session_snapshot_bytes gives its size; nui_session_snapshot copies it to
+ * host memory (waits for the session's stream); nui_session_restore loads it into a
+ * session created with the same configuration (NUI_ERR_INVALID_ARG otherwise), after
+ * which the session continues exactly as the snapshotted one would have. */
+NUI_API size_t nui_session_snapshot_bytes(nui_session* s);
+NUI_API nui_status nui_session_snapshot(nui_session* s, void* host, size_t bytes);
+NUI_API nui_status nui_session_restore(nui_session* s, const void* host, size_t bytes);
 /* Voxels read-modify-written by the last integration of a session. */
 NUI_API nui_status nui_session_touched_voxels(nui_session* s, uint64_t* n);
 

@@ -112,6 +112,9 @@ _SIGS = {
     "nui_ctx_last_tick_kernels": (C.c_int, [_P, _P]),
     "nui_ctx_get_tuning": (C.c_int, [_P, _P]),
     "nui_shift_state": (C.c_int, [_P, _P, _P, _P]),
+    "nui_session_snapshot_bytes": (C.c_size_t, [_P]),
+    "nui_session_snapshot": (C.c_int, [_P, _P, C.c_size_t]),
+    "nui_session_restore": (C.c_int, [_P, _P, C.c_size_t]),
     "nui_shift_points": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
     "nui_shift_points_clear": (C.c_int, [_P]),
     "nui_point_cloud_device": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
@@ -346,6 +349,18 @@ class Session:
         check(lib().nui_session_touched_voxels(self.h, C.byref(v)))
         return v.value
 
+    def snapshot(self):
+        """The session's state as bytes (numpy uint8) for restore() into a session of the
+        same configuration."""
+        n = lib().nui_session_snapshot_bytes(self.h)
+        buf = np.zeros(n, np.uint8)
+        check(lib().nui_session_snapshot(self.h, ptr(buf), n))
+        return buf
+
+    def restore(self, snap):
+        snap = np.ascontiguousarray(snap, np.uint8)
+        check(lib().nui_session_restore(self.h, ptr(snap), snap.size))
+
     def shift_state(self):
         """(voxel offset int32[3], offset in metres float32[3], points found) of a shifting
         volume; the camera's global translation is its pose's plus the offset."""
@@ -370,7 +385,8 @@ class Session:
         check(lib().nui_shift_points_clear(self.h))
 
     def point_cloud(self, cap=1 << 22):
-        """Point cloud of a dense volume (fetchVolumeKernel): (xyz[n, 3], rgba[n, 4], found)."""
+        """Point cloud of the scene (fetchVolumeKernel / fetchShiftVolumeKernel for dense volumes,
+        fetchHashScene_kernel for the voxel hash): (xyz[n, 3], rgba[n, 4], found)."""
         import torch
         xyz = torch.empty((cap, 3), dtype=torch.float32, device="cuda")
         rgba = torch.empty((cap, 4), dtype=torch.float32, device="cuda")

@@ -713,6 +713,41 @@ __global__ void __launch_bounds__(128, 8) k_hash_raycast(const SessionDesc* __re
   hash_finish<HF>(R, s, pid, pr, dir, stepScale, sdfv);
 }
 
+// fetchHashScene_kernel (KinfuHashVisualization.cl:5-52), launched as
+// NuiKinfuOpenCLHashScene::Volume2CLVertices does (NuiKinfuOpenCLHashScene.cpp:1066-1180):
+// a point at the centre of every weighted voxel of a visible block whose |sdf| is below
+// truncScale (compared in the int16 scale of the reference's voxels), with the voxel's
+// colour / 255 and alpha 1.  One block per visible entry, one thread per voxel; points are
+// appended atomically (no fixed order), at most cap of them.
+template <int HF>
+__global__ void __launch_bounds__(512) k_hash_fetch(const SessionDesc* __restrict__ descs, float* xyz, float* rgba,
+                                                    long long cap, unsigned long long* counter) {
+  const SessionDesc& s = descs[0];
+  const int nvis = s.hcount[2];
+  const float lim = 32767.f * s.mu;
+  const int i = threadIdx.x;
+  for (int v = blockIdx.x; v < nvis; v += gridDim.x) {
+    const int id = s.vis_ids[v];
+    if (id < 0) continue;
+    const HEntry en = load_entry(s.entries, (unsigned)id);
+    if (en.ptr < 0) continue;
+    const unsigned bi = (unsigned)en.ptr * 512u + (unsigned)i;
+    if (s.hw[bi] == 0) continue;
+    const float a = HF == 0 ? (float)abs((int)reinterpret_cast<const short*>(s.hsdf)[bi])
+                            : fabsf(HVox<1>::load(s.hsdf, bi) * 32767.f);
+    if (!(a < lim)) continue;
+    const unsigned long long k = atomicAdd(counter, 1ull);
+    if ((long long)k >= cap) continue;
+    xyz[3 * k + 2] = ((float)(en.pos[2] * 8) + ((float)(i / 64) + 0.5f)) * s.voxel;
+    xyz[3 * k + 1] = ((float)(en.pos[1] * 8) + ((float)((i % 64) / 8) + 0.5f)) * s.voxel;
+    xyz[3 * k + 0] = ((float)(en.pos[0] * 8) + ((float)((i % 64) % 8) + 0.5f)) * s.voxel;
+    const uchar4 c = s.hrgb ? s.hrgb[bi] : make_uchar4(0, 0, 0, 0);
+    reinterpret_cast<float4*>(rgba)[k] = make_float4((float)c.x / 255.f, (float)c.y / 255.f, (float)c.z / 255.f, 1.f);
+  }
+}
+
+template __global__ void k_hash_fetch<0>(const SessionDesc*, float*, float*, long long, unsigned long long*);
+template __global__ void k_hash_fetch<1>(const SessionDesc*, float*, float*, long long, unsigned long long*);
 template __global__ void k_hash_integrate<0>(const SessionDesc*);
 template __global__ void k_hash_integrate<1>(const SessionDesc*);
 template __global__ void k_hash_raycast<0>(const SessionDesc*, int);

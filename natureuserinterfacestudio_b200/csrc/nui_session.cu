@@ -68,6 +68,8 @@ template <int F>
 __global__ void k_shift_fetch(const SessionDesc*, int);
 template <int F>
 __global__ void k_fetch_volume(const SessionDesc*, float*, float*, long long, unsigned long long*);
+template <int F>
+__global__ void k_hash_fetch(const SessionDesc*, float*, float*, long long, unsigned long long*);
 template <typename T>
 __global__ void k_shift_roll_x(const SessionDesc*, int);
 template <typename T>
@@ -1147,6 +1149,106 @@ NUI_API nui_status nui_get_pose(nui_session* s, float* pose12) {
   return NUI_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Device state a session carries from frame to frame: what a snapshot holds.  Per-frame
+// scratch (depth pyramid, integration tables, hash allocation scratch, partial sums) is
+// rebuilt by the next frame and left out.
+std::vector<std::pair<void*, size_t>> state_segments(const nui_session* s) {
+  const nui_session_cfg& c = s->cfg;
+  const size_t N = (size_t)c.width * c.height;
+  std::vector<std::pair<void*, size_t>> v;
+  auto add = [&](void* p, size_t b) {
+    if (p && b) v.emplace_back(p, b);
+  };
+  add(s->ts, sizeof(TrackState));
+  add(s->vref, N * 16);
+  add(s->nref, N * 16);
+  add(s->cmap, N * 4);
+  add(s->cprev, N * 4);
+  if (s->hash) {
+    const size_t ne = (size_t)c.hash_buckets + c.hash_excess, hv = (size_t)c.hash_pool_blocks * 512;
+    add(s->entries, ne * sizeof(HEntry));
+    add(s->hsdf, hv * 2);
+    add(s->hw, hv);
+    add(s->hrgb, hv * 4);
+    add(s->alloc_list, (size_t)c.hash_pool_blocks * 4);
+    add(s->excess_list, (size_t)c.hash_excess * 4);
+    add(s->hcount, 16);
+    add(s->vis, ne);
+    add(s->vis_ids, ne * 4);
+  } else {
+    const size_t nv = (size_t)c.res[0] * c.res[1] * c.res[2];
+    add(s->vol, nv * (c.tsdf_format == NUI_TSDF_F16_U8 ? 2 : voxel_bytes(c.tsdf_format)));
+    add(s->wvol, nv);
+    add(s->cvol, nv * 4);
+    add(s->occ, (size_t)((c.res[0] + 7) / 8) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8));
+    add(s->occ2, (size_t)((c.res[0] + 31) / 32) * ((c.res[1] + 31) / 32) * ((c.res[2] + 31) / 32));
+    add(s->occ3, (size_t)((c.res[0] + 127) / 128) * ((c.res[1] + 127) / 128) * ((c.res[2] + 127) / 128));
+    add(s->pts_xyz, (size_t)c.shift_point_cap * 12);
+    add(s->pts_rgba, (size_t)c.shift_point_cap * 16);
+  }
+  return v;
+}
+
+struct SnapshotHeader {
+  char magic[8];  // "NUISNAP1"
+  uint64_t bytes;  // whole snapshot
+  nui_session_cfg cfg;
+  int64_t frames;
+};
+}  // namespace
+
+extern "C" {
+
+NUI_API size_t nui_session_snapshot_bytes(nui_session* s) {
+  if (!s) return 0;
+  size_t b = sizeof(SnapshotHeader);
+  for (auto& seg : state_segments(s)) b += seg.second;
+  return b;
+}
+
+NUI_API nui_status nui_session_snapshot(nui_session* s, void* host, size_t bytes) {
+  if (!s || !host) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  const size_t need = nui_session_snapshot_bytes(s);
+  if (bytes < need) return fail(NUI_ERR_INVALID_ARG, "snapshot buffer too small");
+  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  SnapshotHeader h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, "NUISNAP1", 8);
+  h.bytes = need;
+  h.cfg = s->cfg;
+  h.frames = s->frames;
+  std::memcpy(host, &h, sizeof(h));
+  char* p = (char*)host + sizeof(h);
+  for (auto& seg : state_segments(s)) {
+    NUI_CUDA(cudaMemcpy(p, seg.first, seg.second, cudaMemcpyDeviceToHost));
+    p += seg.second;
+  }
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_session_restore(nui_session* s, const void* host, size_t bytes) {
+  if (!s || !host) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  SnapshotHeader h;
+  if (bytes < sizeof(h)) return fail(NUI_ERR_INVALID_ARG, "not a session snapshot");
+  std::memcpy(&h, host, sizeof(h));
+  if (std::memcmp(h.magic, "NUISNAP1", 8) != 0) return fail(NUI_ERR_INVALID_ARG, "not a session snapshot");
+  if (h.bytes != nui_session_snapshot_bytes(s) || bytes < h.bytes)
+    return fail(NUI_ERR_INVALID_ARG, "snapshot size does not match the session");
+  if (std::memcmp(&h.cfg, &s->cfg, sizeof(nui_session_cfg)) != 0)
+    return fail(NUI_ERR_INVALID_ARG, "snapshot of another configuration");
+  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  const char* p = (const char*)host + sizeof(h);
+  for (auto& seg : state_segments(s)) {
+    NUI_CUDA(cudaMemcpy(seg.first, p, seg.second, cudaMemcpyHostToDevice));
+    p += seg.second;
+  }
+  s->frames = h.frames;
+  return NUI_OK;
+}
+
 NUI_API nui_status nui_shift_state(nui_session* s, int* voxel_offset, float* offset_m, uint64_t* points_found) {
   if (!s) return fail(NUI_ERR_INVALID_ARG, "null session");
   NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
@@ -1185,7 +1287,6 @@ NUI_API nui_status nui_shift_points_clear(nui_session* s) {
 NUI_API nui_status nui_point_cloud_device(nui_session* s, float* d_xyz, float* d_rgba, uint64_t cap,
                                           uint64_t* found) {
   if (!s || !found || (cap && (!d_xyz || !d_rgba))) return fail(NUI_ERR_INVALID_ARG, "null argument");
-  if (s->hash) return fail(NUI_ERR_INVALID_ARG, "not a dense session");
   if (((uintptr_t)d_rgba & 15) || ((uintptr_t)d_xyz & 3)) return fail(NUI_ERR_INVALID_ARG, "misaligned buffers");
   nui_ctx* ctx = s->ctx;
   nui_status st = ensure_cap(ctx, 1);
@@ -1196,7 +1297,12 @@ NUI_API nui_status nui_point_cloud_device(nui_session* s, float* d_xyz, float* d
   unsigned long long* counter = ctx->d_count;
   NUI_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), ctx->stream));
   const long long c = (long long)std::min<uint64_t>(cap, (uint64_t)1 << 62);
-  switch (s->cfg.tsdf_format) {
+  if (s->hash) {
+    if (s->cfg.tsdf_format == NUI_TSDF_I16)
+      k_hash_fetch<0><<<1184, 512, 0, ctx->stream>>>(s->d_desc1, d_xyz, d_rgba, c, counter);
+    else
+      k_hash_fetch<1><<<1184, 512, 0, ctx->stream>>>(s->d_desc1, d_xyz, d_rgba, c, counter);
+  } else switch (s->cfg.tsdf_format) {
     case 0: k_fetch_volume<0><<<1184, 256, 0, ctx->stream>>>(s->d_desc1, d_xyz, d_rgba, c, counter); break;
     case 1: k_fetch_volume<1><<<1184, 256, 0, ctx->stream>>>(s->d_desc1, d_xyz, d_rgba, c, counter); break;
     case 2: k_fetch_volume<2><<<1184, 256, 0, ctx->stream>>>(s->d_desc1, d_xyz, d_rgba, c, counter); break;

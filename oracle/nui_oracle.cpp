@@ -1914,6 +1914,34 @@ static inline f3 sdf_interp(f3 p1, f3 p2, float v1, float v2) {
   return p1 + (p2 - p1) * ((0.0f - v1) / (v2 - v1));
 }
 
+// fetchHashScene_kernel (KinfuHashVisualization.cl:5-52) over the visible list, as
+// NuiKinfuOpenCLHashScene::Volume2CLVertices launches it (NuiKinfuOpenCLHashScene.cpp:1066-1180):
+// a point at the centre of every weighted voxel with |sdf| < 32767 * truncScale, in visible
+// list and voxel order, with the voxel's colour / 255 (alpha 1).  Up to cap points; returns
+// how many were found.
+ORC_API long orc_hash_fetch_points(const OrcHash* h, float* xyz, float* rgba, long cap) {
+  long out = 0;
+  for (int id : h->vis_ids) {
+    const HEntry& en = h->e[id];
+    if (en.ptr < 0) continue;
+    for (int i = 0; i < 512; ++i) {
+      const long bi = (long)en.ptr * 512 + i;
+      if (!(h->w[bi] > 0 && (float)std::abs((int)h->sdf[bi]) < 32767.f * h->c.mu)) continue;
+      if (out < cap) {
+        xyz[3 * out + 2] = ((float)(en.pos[2] * 8) + ((float)(i / 64) + 0.5f)) * h->c.voxel;
+        xyz[3 * out + 1] = ((float)(en.pos[1] * 8) + ((float)((i % 64) / 8) + 0.5f)) * h->c.voxel;
+        xyz[3 * out + 0] = ((float)(en.pos[0] * 8) + ((float)((i % 64) % 8) + 0.5f)) * h->c.voxel;
+        rgba[4 * out + 0] = (float)h->rgb[3 * bi] / 255.f;
+        rgba[4 * out + 1] = (float)h->rgb[3 * bi + 1] / 255.f;
+        rgba[4 * out + 2] = (float)h->rgb[3 * bi + 2] / 255.f;
+        rgba[4 * out + 3] = 1.0f;
+      }
+      ++out;
+    }
+  }
+  return out;
+}
+
 ORC_API long orc_hash_mesh(const OrcHash* h, float* pos, float* col, long cap) {
   static const int CO[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
   static const int E[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};

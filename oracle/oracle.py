@@ -326,6 +326,7 @@ _hash_sigs = {
     "orc_hash_integrate": (None, [_P, _P, _P, _P, _P, _P]),
     "orc_hash_raycast": (None, [_P, _P, _P, _P, _P, _P, _P]),
     "orc_hash_mesh": (C.c_long, [_P, _P, _P, C.c_long]),
+    "orc_hash_fetch_points": (C.c_long, [_P, _P, _P, C.c_long]),
     "orc_hash_visible": (C.c_long, [_P, _P, C.c_long]),
     "orc_hash_entries": (_P, [_P]),
     "orc_hash_sdf": (_P, [_P]),
@@ -339,6 +340,7 @@ _ref_hash_sigs = {
     "ref_hash_frame": (None, [_P] * 15 + [C.c_float, C.c_float, C.c_int, C.c_int]),
     "ref_hash_raycast": (None, [_P, _P, _P, C.c_int, _P, _P, C.c_float, C.c_float, _P, _P, _P, _P]),
     "ref_hash_mesh": (C.c_int, [_P, _P, _P, C.c_int, C.c_float, _P, _P]),
+    "ref_hash_fetch": (C.c_int, [_P, _P, _P, C.c_int, C.c_float, C.c_float, _P, _P]),
 }
 
 
@@ -388,6 +390,13 @@ class OracleHash:
         col = np.zeros((cap, 4), np.float32)
         n = oracle().orc_hash_mesh(self.h, p(pos), p(col), cap)
         return pos[:min(n, cap)], col[:min(n, cap)], n
+
+    def fetch(self, cap=1 << 22):
+        """fetchHashScene_kernel's points: (xyz[n, 3], rgba[n, 4], found)."""
+        xyz = np.zeros((cap, 3), np.float32)
+        rgba = np.zeros((cap, 4), np.float32)
+        n = oracle().orc_hash_fetch_points(self.h, p(xyz), p(rgba), cap)
+        return xyz[:min(n, cap)], rgba[:min(n, cap)], n
 
     def visible(self):
         ids = np.zeros(self.n_entries, np.int32)
@@ -460,6 +469,14 @@ class RefHash:
         ref().ref_hash_raycast(p(self.entries), p(self.voxels), p(self.vis_ids), self.nvis.value, p(cam.flat()),
                                p(xform.flat()), self.voxel, self.mu, p(rg), p(vm), p(nm), p(cm))
         return vm, nm, cm, rg
+
+    def fetch(self):
+        cap = 5_000_000  # MAX_OUTPUT_VERTEX_SIZE
+        xyz = np.zeros((cap, 3), np.float32)
+        rgba = np.zeros((cap, 4), np.float32)
+        n = ref().ref_hash_fetch(p(self.entries), p(self.voxels), p(self.vis_ids), self.nvis.value, self.voxel,
+                                 self.mu, p(xyz), p(rgba))
+        return xyz[:n], rgba[:n], n
 
     def mesh(self):
         cap = 5_000_000 + 3  # the kernel stops at MAX_OUTPUT_VERTEX_SIZE (+2, its `>` check)

@@ -52,6 +52,13 @@ def test_hash_first_frame_bit_exact(gpu_ctx, room, color):
     assert np.array_equal(x_g, x_o)
     vis, lb, le, failed = s.hash_stats()
     assert failed == 0 and vis == v_o.size
+    # the point cloud (fetchHashScene_kernel) is the oracle's, as a set
+    xg, cg, n = s.point_cloud()
+    xo, co, no = eng.hash_scene().fetch()
+    assert n == no > 1000
+    A = np.unique(np.concatenate([xg, cg], axis=1), axis=0)
+    B = np.unique(np.concatenate([xo, co], axis=1), axis=0)
+    assert np.array_equal(A, B)
 
 
 def test_hash_tracking_sequence(gpu_ctx, orbit):

@@ -42,6 +42,9 @@ def _run(kind, W, H, frames, mesh):
         vo, no_, co, rgo = oh.raycast(cam, x, color=True)
         assert same_bits(rgr, rgo) and same_bits(vr, vo) and same_bits(nr_, no_) and np.array_equal(cr, co)
         assert (~np.isnan(vo)).mean() > 0.5
+        xr, cr_, n_r = rh.fetch()  # fetchHashScene_kernel, in the sequential order
+        xo, co_, n_o = oh.fetch()
+        assert n_r == n_o > 0 and same_bits(xr, xo) and same_bits(cr_, co_)
         if mesh:
             pr, colr, n_r = rh.mesh()
             po, colo, n_o = oh.mesh(5_000_000)
