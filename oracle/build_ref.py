@@ -46,6 +46,12 @@ UNITS = {
     "KinfuHashRaycast.cl": "launch_hash_raycast.inc",
     "KinfuHashVisualization.cl": "launch_hash_mesh.inc",
     "extract.cl": "launch_extract.inc",
+    # the global cache's kernels (the swap-in prefix-scan kernels, replaced by the host
+    # compaction of the launcher, are left out)
+    "KinfuHashSwapping.cl": ("launch_hash_swap.inc", ["reAllocateSwappedOutVoxelBlocks_kernel",
+                                                      "integrateOldIntoActiveData_kernel", "buildSwapOutList_kernel",
+                                                      "moveActiveDataToTransferBuffer_kernel",
+                                                      "cleanVoxelMemory_kernel"]),
 }
 # The reference fixes its hash table sizes at compile time (hashing_gpu_def.h:9-20:
 # 0x150000 buckets, 0x30000 excess entries, 2^20 voxel blocks = 3.2 GB of voxels).  The

@@ -27,6 +27,7 @@
 #include <cstring>
 #include <functional>
 #include <limits>
+#include <unordered_map>
 #include <vector>
 
 #include "../natureuserinterfacestudio_b200/csrc/nui_mc_tables.h"
@@ -1187,10 +1188,12 @@ struct OrcEngineCfg {
   int voxel_shift;           // > 0: the shifting dense volume (NuiKinfuVolumeConfig::voxel_shift)
   float shift_basis[3];      // NuiKinfuVolumeConfig::translateBasis
   long point_cap;            // points kept of the slabs that leave the shifting volume
+  int swapping;              // hash scene: the global cache (NuiHashingSDFConfig::m_bUseSwapping)
 };
 
 struct OrcHash;
-OrcHash* orc_hash_create_internal(int buckets, int excess, int pool, float voxel, float mu, int max_w);
+OrcHash* orc_hash_create_internal(int buckets, int excess, int pool, float voxel, float mu, int max_w,
+                                  int swapping);
 void orc_hash_destroy_internal(OrcHash* h);
 void orc_hash_scene_integrate(OrcHash* h, const float* depth, const uint8_t* bgra, const OrcCam* cam,
                               const OrcXform* m, long* touched);
@@ -1231,7 +1234,7 @@ ORC_API OrcEngine* orc_engine_create(const OrcEngineCfg* cfg) {
   }
   e->tp.trunc = std::max(c.trunc_cfg, 2.1f * std::max(e->tp.cell[0], std::max(e->tp.cell[1], e->tp.cell[2])));
   if (c.hash) {
-    e->hs = orc_hash_create_internal(c.buckets, c.excess, c.pool, c.voxel, c.mu, c.max_w);
+    e->hs = orc_hash_create_internal(c.buckets, c.excess, c.pool, c.voxel, c.mu, c.max_w, c.swapping);
   } else {
     long nvox = (long)c.res[0] * c.res[1] * c.res[2];
     e->vol.resize(2 * nvox);
@@ -1493,10 +1496,19 @@ struct OrcHashCfg {
   uint32_t mask;              // hash mask (buckets - 1 for power-of-two tables)
   float voxel, mu;            // virtualVoxelSize, truncScale
   int max_w;                  // integrationWeightMax
+  int swapping;               // NuiHashingSDFConfig::m_bUseSwapping: the global cache
+};
+
+// A voxel block kept by the global cache (NuiKinfuOpenCLHashGlobalCache m_storedVoxelBlocks).
+struct OrcStoredBlock {
+  int16_t sdf[512];
+  uint8_t w[512], rgb[512 * 3];
 };
 
 struct OrcHash {
   OrcHashCfg c;
+  std::vector<uint8_t> swap;                     // per entry swap state (0, 1, 2)
+  std::unordered_map<int, OrcStoredBlock> store;  // host copies by entry
   std::vector<HEntry> e;
   std::vector<int16_t> sdf;
   std::vector<uint8_t> w, rgb;
@@ -1523,6 +1535,8 @@ ORC_API void orc_hash_reset(OrcHash* h) {
   std::fill(h->vis.begin(), h->vis.end(), 0);
   h->vis_ids.clear();
   h->failed_allocs = 0;
+  std::fill(h->swap.begin(), h->swap.end(), 0);  // NuiKinfuOpenCLHashGlobalCache::reset
+  h->store.clear();
 }
 
 ORC_API OrcHash* orc_hash_create(const OrcHashCfg* cfg) {
@@ -1538,6 +1552,7 @@ ORC_API OrcHash* orc_hash_create(const OrcHashCfg* cfg) {
   h->alloc_type.resize(ne);
   h->vis.resize(ne);
   h->coords.resize(3 * ne);
+  h->swap.resize(ne);
   orc_hash_reset(h);
   return h;
 }
@@ -1670,7 +1685,20 @@ ORC_API long orc_hash_allocate(OrcHash* h, const float* depth, const OrcCam* cam
     const int sx = (int)(q.x * cam->fx / q.z + cam->cx + 0.5f), sy = (int)(q.y * cam->fy / q.z + cam->cy + 0.5f);
     return sx >= 0 && sx < (int)cam->W && sy >= 0 && sy < (int)cam->H;
   };
-  for (long i = 0; i < ne; ++i) {
+  if (c.swapping) {
+    // buildVisibleEnlargedList_kernel (KinfuHashScene.cl:358-385).  Its bounds are
+    // lims = (-W/8, W + W/8, -H/8, H + H/8) as unsigned numbers (:306-311): the lower bound
+    // wraps above the upper one, so checkBlockVisibilityEnlarged never passes and an entry
+    // seen only at the previous frame drops out.  Every entry visible at the start of the
+    // kernel, unless already merged (state 2), is marked for swap-in.
+    const uint32_t lx = (uint32_t)(-(int64_t)cam->W) / 8u, ux = cam->W + cam->W / 8u;
+    for (long i = 0; i < ne; ++i) {
+      const uint8_t t = h->vis[i];
+      if (t == 3 && !(lx < ux)) h->vis[i] = 0;
+      if (t > 0 && h->swap[i] != 2) h->swap[i] = 1;
+    }
+  }
+  for (long i = 0; i < ne && !c.swapping; ++i) {
     if (h->vis[i] != 3) continue;
     const HEntry& en = h->e[i];
     f3 p = mk((float)en.pos[0] * factor, (float)en.pos[1] * factor, (float)en.pos[2] * factor);
@@ -1687,8 +1715,95 @@ ORC_API long orc_hash_allocate(OrcHash* h, const float* depth, const OrcCam* cam
   h->vis_ids.clear();
   for (long i = 0; i < ne; ++i)
     if (h->vis[i] > 0) h->vis_ids.push_back((int)i);
+  if (c.swapping) {
+    // reAllocateSwappedOutVoxelBlocks_kernel (KinfuHashSwapping.cl:6-22): a visible entry
+    // whose block was swapped out takes a free block, the pops in index order
+    for (long i = 0; i < ne; ++i)
+      if (h->vis[i] > 0 && h->e[i].ptr == -1) {
+        const int vba = h->last_block--;
+        if (vba >= 0) h->e[i].ptr = h->alloc_list[vba];
+      }
+  }
   return (long)h->vis_ids.size();
 }
+
+// NuiKinfuOpenCLHashGlobalCache::integrateGlobalIntoLocal + saveToGlobalMemory
+// (NuiKinfuOpenCLHashGlobalCache.cpp:192-538), after the integration.  Lists are the
+// flagged entries in index order (the prefix sums' intended meaning), at most
+// SDF_TRANSFER_BLOCK_NUM = 4096 per operation.
+ORC_API void orc_hash_swap(OrcHash* h) {
+  const OrcHashCfg& c = h->c;
+  const long ne = (long)c.buckets + c.excess;
+  const int kTransfer = 4096;
+  // swap-in: entries marked 1 merge their stored copy (zeros if none) into the local block
+  // (integrateOldIntoActiveData_kernel, KinfuHashSwapping.cl:62-111)
+  std::vector<int> need;
+  for (long i = 0; i < ne && (int)need.size() < kTransfer; ++i)
+    if (h->swap[i] == 1) need.push_back((int)i);
+  static const OrcStoredBlock zero{};
+  for (int id : need) {
+    const int ptr = h->e[id].ptr;
+    if (ptr < 0) continue;
+    auto it = h->store.find(id);
+    const OrcStoredBlock& sb = it != h->store.end() ? it->second : zero;
+    for (int lid = 0; lid < 512; ++lid) {
+      const long bi = (long)ptr * 512 + lid;
+      const float oldF = (float)sb.sdf[lid] / 32767.0f, oldW = (float)sb.w[lid];
+      float newF = (float)h->sdf[bi] / 32767.0f;
+      const float newW = (float)h->w[bi], cw = oldW + newW;
+      newF = oldW * oldF + newW * newF;
+      newF /= cw;
+      // both weights 0: 0 / 0; the conversions of the NaN give 0 (x86 and CUDA alike)
+      h->sdf[bi] = std::isnan(newF) ? (int16_t)0 : (int16_t)(int)(newF * 32767.0f);
+      h->w[bi] = (uint8_t)std::min((int)(uint8_t)(int)cw, c.max_w);
+      for (int k = 0; k < 3; ++k) {
+        const float v = (oldW * (float)sb.rgb[3 * lid + k] + newW * (float)h->rgb[3 * bi + k]) / cw;
+        h->rgb[3 * bi + k] = std::isnan(v) ? (uint8_t)0 : (uint8_t)(int)std::min(std::max(v, 0.0f), 255.f);
+      }
+    }
+    h->swap[id] = 2;
+  }
+  // swap-out: merged entries (2) that are not visible leave for the host; their blocks are
+  // cleared and pushed back on the free list (buildSwapOutList_kernel,
+  // moveActiveDataToTransferBuffer_kernel, cleanVoxelMemory_kernel, :113-180).  Block 0 is
+  // never swapped out (the kernel tests ptr > 0).
+  std::vector<int> out;
+  for (long i = 0; i < ne && (int)out.size() < kTransfer; ++i)
+    if (h->swap[i] == 2 && h->e[i].ptr > 0 && h->vis[i] == 0) out.push_back((int)i);
+  for (int id : out) {
+    const int ptr = h->e[id].ptr;
+    OrcStoredBlock& sb = h->store[id];
+    for (int lid = 0; lid < 512; ++lid) {
+      const long bi = (long)ptr * 512 + lid;
+      sb.sdf[lid] = h->sdf[bi];
+      sb.w[lid] = h->w[bi];
+      std::memcpy(&sb.rgb[3 * lid], &h->rgb[3 * bi], 3);
+      h->sdf[bi] = 0;
+      h->w[bi] = 0;
+      std::memset(&h->rgb[3 * bi], 0, 3);
+    }
+  }
+  for (int id : out) {
+    h->swap[id] = 0;
+    const int vba = h->last_block++ ;
+    if (vba < c.pool - 1) {
+      h->alloc_list[vba + 1] = h->e[id].ptr;
+      h->e[id].ptr = -1;
+    }
+  }
+}
+
+ORC_API const uint8_t* orc_hash_swap_states(const OrcHash* h) { return h->swap.data(); }
+// The stored copy of entry id: copies it out and returns 1, or returns 0 if there is none.
+ORC_API int orc_hash_stored(const OrcHash* h, int id, int16_t* sdf, uint8_t* w, uint8_t* rgb) {
+  auto it = h->store.find(id);
+  if (it == h->store.end()) return 0;
+  std::memcpy(sdf, it->second.sdf, sizeof(it->second.sdf));
+  std::memcpy(w, it->second.w, sizeof(it->second.w));
+  std::memcpy(rgb, it->second.rgb, sizeof(it->second.rgb));
+  return 1;
+}
+ORC_API long orc_hash_stored_count(const OrcHash* h) { return (long)h->store.size(); }
 
 // A17: integrateIntoScene_kernel (KinfuHashScene.cl:387-470) over the visible list.
 ORC_API void orc_hash_integrate(OrcHash* h, const float* depth, const uint8_t* bgra, const OrcCam* cam,
@@ -2013,8 +2128,9 @@ ORC_API void orc_hash_counters(const OrcHash* h, int* last_block, int* last_exce
 
 // Engine glue for the hash scene (NuiKinfuOpenCLHashScene::integrateVolume, :533-583, and
 // raycastRender with forward rendering off, :1014-1064).
-OrcHash* orc_hash_create_internal(int buckets, int excess, int pool, float voxel, float mu, int max_w) {
-  OrcHashCfg c{buckets, excess, pool, (uint32_t)(buckets - 1), voxel, mu, max_w};
+OrcHash* orc_hash_create_internal(int buckets, int excess, int pool, float voxel, float mu, int max_w,
+                                  int swapping) {
+  OrcHashCfg c{buckets, excess, pool, (uint32_t)(buckets - 1), voxel, mu, max_w, swapping};
   return orc_hash_create(&c);
 }
 void orc_hash_destroy_internal(OrcHash* h) { orc_hash_destroy(h); }
@@ -2022,6 +2138,7 @@ void orc_hash_scene_integrate(OrcHash* h, const float* depth, const uint8_t* bgr
                               const OrcXform* m, long* touched) {
   orc_hash_allocate(h, depth, cam, m);
   orc_hash_integrate(h, depth, bgra, cam, m, touched);
+  if (h->c.swapping) orc_hash_swap(h);
 }
 void orc_hash_scene_raycast(OrcHash* h, const OrcCam* cam, const OrcXform* m, float* vmap, float* nmap,
                             uint8_t* cmap) {

@@ -86,7 +86,8 @@ class OrcEngineCfg(C.Structure):
                 ("depth_threshold", C.c_float), ("dist_threshold", C.c_float), ("integration_threshold", C.c_float),
                 ("hash", C.c_int), ("voxel", C.c_float), ("mu", C.c_float), ("buckets", C.c_int), ("excess", C.c_int),
                 ("pool", C.c_int), ("max_w", C.c_int), ("photometric_weight", C.c_float),
-                ("voxel_shift", C.c_int), ("shift_basis", C.c_float * 3), ("point_cap", C.c_long)]
+                ("voxel_shift", C.c_int), ("shift_basis", C.c_float * 3), ("point_cap", C.c_long),
+                ("swapping", C.c_int)]
 
     @staticmethod
     def from_session_cfg(c):
@@ -117,6 +118,7 @@ class OrcEngineCfg(C.Structure):
         for i in range(3):
             e.shift_basis[i] = c.shift_basis[i] if hasattr(c, "shift_basis") else 0.0
         e.point_cap = getattr(c, "shift_point_cap", 0)
+        e.swapping = getattr(c, "hash_swapping", 0)
         return e
 
 
@@ -302,7 +304,7 @@ class Engine:
         h = OracleHash.__new__(OracleHash)
         _bind(oracle(), _hash_sigs)
         c = self.cfg
-        h.cfg = OrcHashCfg(c.buckets, c.excess, c.pool, c.buckets - 1, c.voxel, c.mu, c.max_w)
+        h.cfg = OrcHashCfg(c.buckets, c.excess, c.pool, c.buckets - 1, c.voxel, c.mu, c.max_w, c.swapping)
         h.h = oracle().orc_engine_hash(self.h)
         h.n_entries = c.buckets + c.excess
         h._borrowed = True
@@ -312,7 +314,7 @@ class Engine:
 # ------------------------------------------------------------------ voxel-block hashing
 class OrcHashCfg(C.Structure):
     _fields_ = [("buckets", C.c_int), ("excess", C.c_int), ("pool", C.c_int), ("mask", C.c_uint32),
-                ("voxel", C.c_float), ("mu", C.c_float), ("max_w", C.c_int)]
+                ("voxel", C.c_float), ("mu", C.c_float), ("max_w", C.c_int), ("swapping", C.c_int)]
 
 
 HASH_ENTRY = np.dtype([("pos", np.int16, 3), ("pad", np.int16), ("ptr", np.int32), ("offset", np.uint32)])
@@ -333,6 +335,10 @@ _hash_sigs = {
     "orc_hash_weight": (_P, [_P]),
     "orc_hash_rgb": (_P, [_P]),
     "orc_hash_counters": (None, [_P, _P, _P, _P]),
+    "orc_hash_swap": (None, [_P]),
+    "orc_hash_swap_states": (_P, [_P]),
+    "orc_hash_stored": (C.c_int, [_P, C.c_int, _P, _P, _P]),
+    "orc_hash_stored_count": (C.c_long, [_P]),
 }
 _ref_hash_sigs = {
     "ref_hash_sizes": (None, [_P, _P, _P]),
@@ -341,6 +347,10 @@ _ref_hash_sigs = {
     "ref_hash_raycast": (None, [_P, _P, _P, C.c_int, _P, _P, C.c_float, C.c_float, _P, _P, _P, _P]),
     "ref_hash_mesh": (C.c_int, [_P, _P, _P, C.c_int, C.c_float, _P, _P]),
     "ref_hash_fetch": (C.c_int, [_P, _P, _P, C.c_int, C.c_float, C.c_float, _P, _P]),
+    "ref_hash_alloc_swap": (None, [_P] * 13 + [C.c_float, C.c_float, _P]),
+    "ref_hash_integrate_visible": (None, [_P, _P, _P, C.c_int, _P, _P, _P, _P, C.c_float, C.c_float, C.c_int]),
+    "ref_hash_realloc": (None, [_P, _P, _P, _P]),
+    "ref_hash_global_cache": (None, [_P, _P, _P, _P, _P, _P, C.c_int, _P, _P]),
 }
 
 
@@ -354,10 +364,11 @@ def _bind(L, sigs):
 class OracleHash:
     """The oracle's voxel-block hash scene."""
 
-    def __init__(self, buckets, excess, pool, voxel=0.005, mu=0.02, max_w=255, mask=None):
+    def __init__(self, buckets, excess, pool, voxel=0.005, mu=0.02, max_w=255, mask=None, swapping=False):
         L = oracle()
         _bind(L, _hash_sigs)
-        self.cfg = OrcHashCfg(buckets, excess, pool, (buckets - 1) if mask is None else mask, voxel, mu, max_w)
+        self.cfg = OrcHashCfg(buckets, excess, pool, (buckets - 1) if mask is None else mask, voxel, mu, max_w,
+                              1 if swapping else 0)
         self.h = L.orc_hash_create(C.byref(self.cfg))
         self.n_entries = buckets + excess
 
@@ -416,6 +427,26 @@ class OracleHash:
         rgb = np.ctypeslib.as_array(C.cast(L.orc_hash_rgb(self.h), C.POINTER(C.c_uint8)), shape=(n, 3)).copy()
         return sdf, w, rgb
 
+    def swap(self):
+        """The global cache's swap-in merge and swap-out, after an integration."""
+        oracle().orc_hash_swap(self.h)
+
+    def swap_states(self):
+        ptr_ = oracle().orc_hash_swap_states(self.h)
+        return np.ctypeslib.as_array(C.cast(ptr_, C.POINTER(C.c_uint8)), shape=(self.n_entries,)).copy()
+
+    def stored(self, entry):
+        """(sdf int16[512], w uint8[512], rgb uint8[512, 3]) kept on the host for entry, or None."""
+        sdf = np.zeros(512, np.int16)
+        w = np.zeros(512, np.uint8)
+        rgb = np.zeros((512, 3), np.uint8)
+        if not oracle().orc_hash_stored(self.h, int(entry), p(sdf), p(w), p(rgb)):
+            return None
+        return sdf, w, rgb
+
+    def stored_count(self):
+        return oracle().orc_hash_stored_count(self.h)
+
     def counters(self):
         a, b, c = C.c_int(), C.c_int(), C.c_long()
         oracle().orc_hash_counters(self.h, C.byref(a), C.byref(b), C.byref(c))
@@ -425,7 +456,7 @@ class OracleHash:
 class RefHash:
     """The reference's own hash kernels (host build, test table sizes), run sequentially."""
 
-    def __init__(self, voxel=0.005, mu=0.02, max_w=255):
+    def __init__(self, voxel=0.005, mu=0.02, max_w=255, swapping=False):
         L = ref()
         _bind(L, _ref_hash_sigs)
         b, e, pl = C.c_int(), C.c_int(), C.c_int()
@@ -443,6 +474,11 @@ class RefHash:
         self.vis_ids = np.zeros(ne, np.int32)
         self.nvis = C.c_int(0)
         self.voxel, self.mu, self.max_w = voxel, mu, max_w
+        self.swapping = swapping
+        if swapping:  # NuiKinfuOpenCLHashGlobalCache: swap states and the host store
+            self.swap_states = np.zeros(ne, np.uint8)
+            self.store = np.zeros(ne * 512, REF_VOXEL)
+            self.has_stored = np.zeros(ne, np.uint8)
         last_b, last_e = C.c_int(), C.c_int()
         L.ref_hash_reset(p(self.entries), p(self.voxels), p(self.alloc_list), p(self.excess_list), C.byref(last_b),
                          C.byref(last_e))
@@ -451,6 +487,18 @@ class RefHash:
     def frame(self, depth, bgra, cam, xform, integrate=True):
         lb = self.last[0:1]
         le = self.last[1:2]
+        if self.swapping:  # NuiKinfuOpenCLHashScene::integrateVolume with the global cache
+            L = ref()
+            L.ref_hash_alloc_swap(p(self.entries), p(self.alloc_list), p(self.excess_list), p(lb), p(le),
+                                  p(self.alloc_type), p(self.vis_type), p(self.coords), p(self.vis_ids),
+                                  C.byref(self.nvis), p(depth), p(cam.flat()), p(xform.flat()), self.voxel, self.mu,
+                                  p(self.swap_states))
+            L.ref_hash_realloc(p(self.entries), p(self.vis_type), p(self.alloc_list), p(lb))
+            L.ref_hash_integrate_visible(p(self.entries), p(self.voxels), p(self.vis_ids), self.nvis.value, p(depth),
+                                         p(bgra), p(cam.flat()), p(xform.flat()), self.voxel, self.mu, self.max_w)
+            L.ref_hash_global_cache(p(self.entries), p(self.voxels), p(self.vis_type), p(self.swap_states),
+                                    p(self.alloc_list), p(lb), self.max_w, p(self.store), p(self.has_stored))
+            return self.nvis.value
         ref().ref_hash_frame(p(self.entries), p(self.voxels), p(self.alloc_list), p(self.excess_list), p(lb), p(le),
                              p(self.alloc_type), p(self.vis_type), p(self.coords), p(self.vis_ids),
                              C.byref(self.nvis), p(depth), p(bgra), p(cam.flat()), p(xform.flat()), self.voxel,
