@@ -111,6 +111,15 @@ typedef struct {
   int voxel_shift;
   float shift_basis[3];
   int shift_point_cap;        /* default 2^20 (28 MB) */
+  /* voxel hash: the global cache (NuiHashingSDFConfig::m_bUseSwapping,
+   * NuiKinfuOpenCLHashGlobalCache).  Blocks that leave the view after being merged move to
+   * a host store and their pool blocks are freed; blocks that come back are re-allocated
+   * and merged with their stored copies, at most 4096 each way per frame.  The store is
+   * pinned host memory mapped into the device, hash_store_blocks blocks of 512 voxels
+   * (0 = one per hash entry, as the reference keeps); a full store leaves blocks in the
+   * device pool (counted by nui_hash_swap_stats). */
+  int hash_swapping;
+  int hash_store_blocks;
 } nui_session_cfg;
 
 typedef struct nui_ctx nui_ctx;
@@ -314,6 +323,15 @@ NUI_API nui_status nui_ctx_set_tuning(nui_ctx* ctx, const nui_tuning* t);
 NUI_API nui_status nui_ctx_autotune(nui_ctx* ctx, const nui_session_cfg* cfgs, int n,
                                     const uint16_t* const* depth_mm, const uint8_t* const* bgra, int frames,
                                     int repeats, nui_tuning* out, float* out_tick_ms);
+/* Hash global cache: blocks merged from the store and swapped out by the last frame,
+ * store blocks in use, and swap-outs the full store refused (all NULL-able). */
+NUI_API nui_status nui_hash_swap_stats(nui_session* s, int* swapped_in, int* swapped_out, int* store_used,
+                                       int* store_refused);
+/* The stored copy of hash entry `entry`: 512 sdf values (int16, or half for a half-sdf
+ * session), 512 weights, 512 colours (4 bytes, alpha unused; zeros without colour), in
+ * the pool's voxel order; *found = 0 if the entry has none.  Any output may be NULL. */
+NUI_API nui_status nui_hash_stored_block(nui_session* s, int entry, void* sdf, uint8_t* weight, uint8_t* rgb4,
+                                         int* found);
 /* Shifting volume state (NuiKinfuOpenCLShiftScene m_voxel_offset / getVoxelOffsetSize,
  * NuiKinfuOpenCLShiftScene.cpp:58-66): the volume's offset in voxels and metres (the
  * camera's global translation is its pose's translation plus offset_m) and how many points

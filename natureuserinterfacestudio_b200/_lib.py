@@ -43,6 +43,7 @@ class SessionCfg(C.Structure):
         ("hash_excess", C.c_int), ("hash_pool_blocks", C.c_int), ("hash_max_weight", C.c_int),
         ("photometric_weight", C.c_float),
         ("voxel_shift", C.c_int), ("shift_basis", C.c_float * 3), ("shift_point_cap", C.c_int),
+        ("hash_swapping", C.c_int), ("hash_store_blocks", C.c_int),
     ]
 
 
@@ -112,6 +113,8 @@ _SIGS = {
     "nui_ctx_last_tick_kernels": (C.c_int, [_P, _P]),
     "nui_ctx_get_tuning": (C.c_int, [_P, _P]),
     "nui_shift_state": (C.c_int, [_P, _P, _P, _P]),
+    "nui_hash_swap_stats": (C.c_int, [_P, _P, _P, _P, _P]),
+    "nui_hash_stored_block": (C.c_int, [_P, C.c_int, _P, _P, _P, _P]),
     "nui_session_snapshot_bytes": (C.c_size_t, [_P]),
     "nui_session_snapshot": (C.c_int, [_P, _P, C.c_size_t]),
     "nui_session_restore": (C.c_int, [_P, _P, C.c_size_t]),
@@ -361,6 +364,21 @@ class Session:
         snap = np.ascontiguousarray(snap, np.uint8)
         check(lib().nui_session_restore(self.h, ptr(snap), snap.size))
 
+    def hash_swap_stats(self):
+        """(swapped in, swapped out by the last frame, store blocks used, refused swap-outs)."""
+        v = [C.c_int() for _ in range(4)]
+        check(lib().nui_hash_swap_stats(self.h, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def hash_stored(self, entry):
+        """(sdf[512] raw int16 bits, weight[512], rgb[512, 4]) stored for a hash entry, or None."""
+        sdf = np.zeros(512, np.int16)
+        w = np.zeros(512, np.uint8)
+        rgb = np.zeros((512, 4), np.uint8)
+        f = C.c_int()
+        check(lib().nui_hash_stored_block(self.h, int(entry), ptr(sdf), ptr(w), ptr(rgb), C.byref(f)))
+        return (sdf, w, rgb) if f.value else None
+
     def shift_state(self):
         """(voxel offset int32[3], offset in metres float32[3], points found) of a shifting
         volume; the camera's global translation is its pose's plus the offset."""
@@ -415,10 +433,13 @@ class Session:
         return v.value, b.value, e.value, f.value
 
     def hash_download(self, what):
-        """20 entries, 21 visible list, 22 voxels (reference layout), 23 range image."""
+        """20 entries, 21 visible list, 22 voxels (reference layout), 23 range image, 24 swap
+        states (global cache)."""
         c = self.cfg
         ne = c.hash_buckets + c.hash_excess
-        if what == 20:
+        if what == 24:
+            out = np.zeros(ne, np.uint8)
+        elif what == 20:
             out = np.zeros(ne * 16, np.uint8)
         elif what == 21:
             out = np.zeros(self.hash_stats()[0], np.int32)

@@ -122,7 +122,20 @@ struct SessionDesc {
   uchar4* hrgb;                   // np * 512 colours (nullable)
   int* alloc_list;                // free-block stack
   int* excess_list;               // free excess-slot stack
-  int* hcount;                    // [0] last free block, [1] last free excess, [2] visible count, [3] failed allocations
+  int* hcount;                    // [0] last free block, [1] last free excess, [2] visible count, [3] failed
+                                  // allocations, [4] swap-in count, [5] swap-out count, [6] free-list base
+                                  // of the swap pass, [7] store blocks used, [8] store-full refusals
+  // global cache (hash swapping): per-entry swap state and store slot, the transfer lists,
+  // and the host store (pinned, mapped: kernels read and write it directly)
+  int swapping;
+  uint8_t* swap;
+  int* store_slot;
+  int* swap_in_ids;               // kTransferBlocks
+  int* swap_out_ids;              // kTransferBlocks
+  void* st_sdf;                   // st_cap * 512 (int16 or half)
+  uint8_t* st_w;                  // st_cap * 512
+  uchar4* st_rgb;                 // st_cap * 512 (nullable)
+  int st_cap;
   uint8_t* alloc_type;            // per entry
   uint8_t* vis;                   // per entry visible type
   short4* coords;                 // per entry block coordinates of a pending allocation

@@ -24,6 +24,8 @@
 
 namespace nui {
 
+constexpr int kTransferBlocks = 4096;  // SDF_TRANSFER_BLOCK_NUM (hashing_gpu_def.h:16)
+
 constexpr int kHashScanBlock = 1024;
 
 __device__ __forceinline__ unsigned hash_index(unsigned mask, int x, int y, int z) {
@@ -137,11 +139,22 @@ __global__ void __launch_bounds__(256) k_hash_walk(const SessionDesc* __restrict
   }
 }
 
+__device__ __forceinline__ int entry_ptr(const SessionDesc& s, unsigned i) {
+  return reinterpret_cast<const int*>(s.entries)[4 * i + 2];
+}
+// buildSwapOutList_kernel (KinfuHashSwapping.cl:113-124): merged (2), holding a block other
+// than block 0, not visible
+__device__ __forceinline__ bool swap_out_flag(const SessionDesc& s, unsigned i) {
+  return s.swap[i] == 2 && entry_ptr(s, i) > 0 && s.vis[i] == 0;
+}
+
 // Per 1024 entries: number of entries needing a block (type >= 1) and an excess slot
-// (type 2) (which == 0), or of visible entries (which == 1).
+// (type 2) (which == 0); of visible entries (which == 1); with the global cache, of
+// visible entries whose block was swapped out and of entries to swap in (which == 2), of
+// entries to swap out (which == 3).
 __global__ void __launch_bounds__(256) k_hash_count(const SessionDesc* __restrict__ descs, int which) {
   const SessionDesc& s = descs[blockIdx.y];
-  if (!hash_active(s)) return;
+  if (!hash_active(s) || (which >= 2 && !s.swapping)) return;
   const unsigned n = (unsigned)(s.nb + s.ne);
   const unsigned b0 = blockIdx.x * kHashScanBlock;
   if (b0 >= n) return;
@@ -151,8 +164,13 @@ __global__ void __launch_bounds__(256) k_hash_count(const SessionDesc* __restric
       const uint8_t t = s.alloc_type[i];
       a += t != 0;
       e += t == 2;
-    } else {
+    } else if (which == 1) {
       a += s.vis[i] > 0;
+    } else if (which == 2) {  // re-allocations, swap-ins
+      a += s.vis[i] > 0 && entry_ptr(s, i) == -1;
+      e += s.swap[i] == 1;
+    } else {  // swap-outs
+      a += swap_out_flag(s, i);
     }
   }
   a = __reduce_add_sync(0xffffffffu, a);
@@ -179,7 +197,7 @@ __global__ void __launch_bounds__(256) k_hash_count(const SessionDesc* __restric
 // stacks; visible -> visible count.
 __global__ void __launch_bounds__(1024) k_hash_scan(const SessionDesc* __restrict__ descs, int which) {
   const SessionDesc& s = descs[blockIdx.x];
-  if (!hash_active(s)) return;
+  if (!hash_active(s) || (which >= 2 && !s.swapping)) return;
   const int nblk = (s.nb + s.ne + kHashScanBlock - 1) / kHashScanBlock;
   __shared__ unsigned wa[32], we[32];
   __shared__ unsigned carry_a, carry_e;
@@ -230,6 +248,12 @@ __global__ void __launch_bounds__(1024) k_hash_scan(const SessionDesc* __restric
   }
   if (threadIdx.x == 0) {
     if (which == 1) s.hcount[2] = (int)carry_a;
+    if (which == 2) {  // the re-allocations pop the free list in index order (atomic_dec)
+      s.hcount[6] = s.hcount[0];
+      s.hcount[0] -= (int)carry_a;
+      s.hcount[4] = min((int)carry_e, kTransferBlocks);
+    }
+    if (which == 3) s.hcount[5] = min((int)carry_a, kTransferBlocks);
   }
 }
 
@@ -318,7 +342,12 @@ __global__ void k_hash_alloc_done(const SessionDesc* __restrict__ descs, int n) 
   s.hcount[1] -= (int)te;
 }
 
-// buildVisibleList_kernel + checkBlockVisibility (KinfuHashScene.cl:196-285)
+// buildVisibleList_kernel + checkBlockVisibility (KinfuHashScene.cl:196-285).  With the
+// global cache, buildVisibleEnlargedList_kernel (:358-385): its bounds are
+// (-W/8, W + W/8, -H/8, H + H/8) held as unsigned numbers (:306-311), so the lower bound
+// wraps above the upper one and the enlarged test never passes -- an entry seen only at the
+// previous frame drops out; every entry visible at the start, unless already merged (2),
+// is marked for swap-in.
 __device__ __forceinline__ bool point_visible(const SessionDesc& s, const DevXform& m, float3 p) {
   const float3 q = xf_inverse(m, p);
   if (isnan3(q)) return false;
@@ -331,6 +360,14 @@ __global__ void k_hash_visible(const SessionDesc* __restrict__ descs) {
   const unsigned n = (unsigned)(s.nb + s.ne);
   const DevXform& m = s.ts->xf;
   const float factor = 8.0f * s.voxel;
+  if (s.swapping) {
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+      const uint8_t t = s.vis[i];
+      if (t == 3) s.vis[i] = 0;
+      if (t > 0 && s.swap[i] != 2) s.swap[i] = 1;
+    }
+    return;
+  }
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     if (s.vis[i] != 3) continue;
     const HEntry en = load_entry(s.entries, i);
@@ -713,6 +750,178 @@ __global__ void __launch_bounds__(128, 8) k_hash_raycast(const SessionDesc* __re
   hash_finish<HF>(R, s, pid, pr, dir, stepScale, sdfv);
 }
 
+// ------------------------------------------------------------------ global cache
+// NuiKinfuOpenCLHashGlobalCache (NuiKinfuOpenCLHashGlobalCache.cpp:121-538) with its
+// kernels (KinfuHashSwapping.cl:6-180).  The reference keeps the host store in host memory
+// and moves blocks through a transfer buffer with blocking copies and host loops; here the
+// store is pinned host memory mapped into the device, and the swap kernels read and write
+// it directly over the bus, inside the tick.  Lists hold the flagged entries in index
+// order, at most kTransferBlocks (SDF_TRANSFER_BLOCK_NUM) per operation; pops and pushes of
+// the free list follow that order, as the reference's atomics do when run in order.
+
+// After the visible list: re-allocation of swapped-out visible entries
+// (reAllocateSwappedOutVoxelBlocks_kernel, :6-22) and the swap-in list.
+__global__ void __launch_bounds__(kHashScanBlock) k_hash_swap_lists(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!hash_active(s) || !s.swapping) return;
+  const unsigned n = (unsigned)(s.nb + s.ne);
+  const unsigned b = blockIdx.x;
+  if (b * kHashScanBlock >= n) return;
+  const unsigned i = b * kHashScanBlock + threadIdx.x;
+  bool fr, fi;
+  unsigned tr, ti;
+  const unsigned rr = block_rank(i, n, [&](unsigned k) { return s.vis[k] > 0 && entry_ptr(s, k) == -1; }, fr, tr);
+  const unsigned ri = block_rank(i, n, [&](unsigned k) { return s.swap[k] == 1; }, fi, ti);
+  if (fr) {
+    const int vba = s.hcount[6] - (int)(s.blk[4 * b + 2] + rr);
+    if (vba >= 0) reinterpret_cast<int*>(s.entries)[4 * i + 2] = s.alloc_list[vba];
+  }
+  if (fi) {
+    const unsigned g = s.blk[4 * b + 3] + ri;
+    if (g < (unsigned)kTransferBlocks) s.swap_in_ids[g] = (int)i;
+  }
+}
+
+// After the integration: integrateOldIntoActiveData_kernel (:62-111).  One block per listed
+// entry: its stored copy (zeros if it has none) is merged into the local block by weight.
+template <int HF>
+__global__ void __launch_bounds__(512) k_hash_swap_in(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!hash_active(s) || !s.swapping) return;
+  const int nin = s.hcount[4];
+  const int lid = threadIdx.x;
+  for (int k = blockIdx.x; k < nin; k += gridDim.x) {
+    const int id = s.swap_in_ids[k];
+    const int ptr = entry_ptr(s, (unsigned)id);
+    if (ptr < 0) continue;
+    const int slot = s.store_slot[id];
+    float oldF = 0.f, oldW = 0.f;
+    uchar4 oc = make_uchar4(0, 0, 0, 0);
+    if (slot >= 0) {
+      const size_t si = (size_t)slot * 512 + lid;
+      oldF = HVox<HF>::load(s.st_sdf, (unsigned)si);
+      oldW = (float)s.st_w[si];
+      if (s.st_rgb) oc = s.st_rgb[si];
+    }
+    const unsigned bi = (unsigned)ptr * 512u + (unsigned)lid;
+    const float newW = (float)s.hw[bi], cw = oldW + newW;
+    float newF = HVox<HF>::load(s.hsdf, bi);
+    newF = oldW * oldF + newW * newF;
+    newF /= cw;
+    // both weights 0: 0 / 0, whose conversions give 0 (as on the reference's x86 host)
+    HVox<HF>::store(s.hsdf, bi, isnan(newF) ? 0.f : newF);
+    s.hw[bi] = (uint8_t)min((int)(uint8_t)(int)cw, s.max_w);
+    if (s.hrgb) {
+      const uchar4 lc = s.hrgb[bi];
+      auto mix = [&](float o, float l) -> unsigned char {
+        const float v = (oldW * o + newW * l) / cw;
+        return isnan(v) ? (unsigned char)0 : (unsigned char)(int)fminf(fmaxf(v, 0.f), 255.f);
+      };
+      s.hrgb[bi] = make_uchar4(mix(oc.x, lc.x), mix(oc.y, lc.y), mix(oc.z, lc.z), lc.w);
+    }
+    if (lid == 0) s.swap[id] = 2;
+  }
+}
+
+// The swap-out list (buildSwapOutList_kernel, :113-124), then a store slot for every listed
+// entry that has none yet (an entry keeps its slot; a full store refuses the entry, which
+// then stays in the device pool: -1 in the list).
+__global__ void __launch_bounds__(kHashScanBlock) k_hash_swap_out_list(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!hash_active(s) || !s.swapping) return;
+  const unsigned n = (unsigned)(s.nb + s.ne);
+  const unsigned b = blockIdx.x;
+  if (b * kHashScanBlock >= n) return;
+  const unsigned i = b * kHashScanBlock + threadIdx.x;
+  bool f;
+  unsigned t;
+  const unsigned r = block_rank(i, n, [&](unsigned k) { return swap_out_flag(s, k); }, f, t);
+  if (!f) return;
+  const unsigned g = s.blk[4 * b + 2] + r;
+  if (g >= (unsigned)kTransferBlocks) return;
+  int id = (int)i;
+  if (s.store_slot[i] < 0) {
+    const int slot = atomicAdd(&s.hcount[7], 1);
+    if (slot < s.st_cap) {
+      s.store_slot[i] = slot;
+    } else {
+      atomicAdd(&s.hcount[8], 1);
+      id = -1;
+    }
+  }
+  s.swap_out_ids[g] = id;
+}
+
+// moveActiveDataToTransferBuffer_kernel (:126-153): the local block goes to the entry's
+// store slot and is cleared (sdf 0, weight 0, colour 0).
+template <int HF>
+__global__ void __launch_bounds__(512) k_hash_swap_out(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!hash_active(s) || !s.swapping) return;
+  const int nout = s.hcount[5];
+  const int lid = threadIdx.x;
+  for (int k = blockIdx.x; k < nout; k += gridDim.x) {
+    const int id = s.swap_out_ids[k];
+    if (id < 0) continue;
+    const int ptr = entry_ptr(s, (unsigned)id);
+    const unsigned bi = (unsigned)ptr * 512u + (unsigned)lid;
+    const size_t si = (size_t)s.store_slot[id] * 512 + lid;
+    if (HF == 0)
+      reinterpret_cast<short*>(s.st_sdf)[si] = reinterpret_cast<const short*>(s.hsdf)[bi];
+    else
+      reinterpret_cast<__half*>(s.st_sdf)[si] = reinterpret_cast<const __half*>(s.hsdf)[bi];
+    s.st_w[si] = s.hw[bi];
+    if (s.st_rgb) s.st_rgb[si] = s.hrgb ? s.hrgb[bi] : make_uchar4(0, 0, 0, 0);
+    HVox<HF>::store(s.hsdf, bi, 0.f);
+    s.hw[bi] = 0;
+    if (s.hrgb) s.hrgb[bi] = make_uchar4(0, 0, 0, 0);
+  }
+}
+
+// cleanVoxelMemory_kernel (:155-180): the swapped-out entries leave state 2 and push their
+// blocks on the free list (atomic_inc in list order); one block per session.
+__global__ void __launch_bounds__(1024) k_hash_swap_clean(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.x];
+  if (!hash_active(s) || !s.swapping) return;
+  __shared__ int base;
+  __shared__ unsigned wsum[32];
+  __shared__ unsigned carry;
+  if (threadIdx.x == 0) {
+    base = s.hcount[0];
+    carry = 0;
+  }
+  __syncthreads();
+  const int nout = s.hcount[5];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k0 = 0; k0 < nout; k0 += 1024) {
+    const int k = k0 + (int)threadIdx.x;
+    const int id = k < nout ? s.swap_out_ids[k] : -1;
+    const bool f = id >= 0;
+    const unsigned ballot = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) wsum[warp] = __popc(ballot);
+    __syncthreads();
+    unsigned before = carry;
+    for (int w = 0; w < warp; ++w) before += wsum[w];
+    const unsigned rank = before + __popc(ballot & ((1u << lane) - 1u));
+    if (f) {
+      s.swap[id] = 0;
+      const int vba = base + (int)rank;
+      if (vba < s.np - 1) {
+        s.alloc_list[vba + 1] = entry_ptr(s, (unsigned)id);
+        reinterpret_cast<int*>(s.entries)[4 * id + 2] = -1;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned tot = 0;
+      for (int w = 0; w < 32; ++w) tot += wsum[w];
+      carry += tot;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) s.hcount[0] = base + (int)carry;
+}
+
 // fetchHashScene_kernel (KinfuHashVisualization.cl:5-52), launched as
 // NuiKinfuOpenCLHashScene::Volume2CLVertices does (NuiKinfuOpenCLHashScene.cpp:1066-1180):
 // a point at the centre of every weighted voxel of a visible block whose |sdf| is below
@@ -746,6 +955,10 @@ __global__ void __launch_bounds__(512) k_hash_fetch(const SessionDesc* __restric
   }
 }
 
+template __global__ void k_hash_swap_in<0>(const SessionDesc*);
+template __global__ void k_hash_swap_in<1>(const SessionDesc*);
+template __global__ void k_hash_swap_out<0>(const SessionDesc*);
+template __global__ void k_hash_swap_out<1>(const SessionDesc*);
 template __global__ void k_hash_fetch<0>(const SessionDesc*, float*, float*, long long, unsigned long long*);
 template __global__ void k_hash_fetch<1>(const SessionDesc*, float*, float*, long long, unsigned long long*);
 template __global__ void k_hash_integrate<0>(const SessionDesc*);
@@ -784,11 +997,17 @@ __global__ void k_hash_reset(const SessionDesc* __restrict__ descs) {
     s.hw[i] = 0;
     if (s.hrgb) s.hrgb[i] = make_uchar4(0, 0, 0, 0);
   }
+  if (s.swapping)
+    for (size_t i = t0; i < ne; i += stride) {
+      s.swap[i] = 0;
+      s.store_slot[i] = -1;
+    }
   if (t0 == 0) {
     s.hcount[0] = s.np - 1;
     s.hcount[1] = s.ne - 1;
     s.hcount[2] = 0;
     s.hcount[3] = 0;
+    for (int k = 4; k < 9; ++k) s.hcount[k] = 0;
   }
 }
 

@@ -63,6 +63,13 @@ __global__ void k_hash_project(const SessionDesc*);
 template <int F>
 __global__ void k_hash_raycast(const SessionDesc*, int);
 __global__ void k_hash_reset(const SessionDesc*);
+__global__ void k_hash_swap_lists(const SessionDesc*);
+template <int F>
+__global__ void k_hash_swap_in(const SessionDesc*);
+__global__ void k_hash_swap_out_list(const SessionDesc*);
+template <int F>
+__global__ void k_hash_swap_out(const SessionDesc*);
+__global__ void k_hash_swap_clean(const SessionDesc*);
 __global__ void k_hash_export_voxels(const SessionDesc*, uint8_t*);
 template <int F>
 __global__ void k_shift_fetch(const SessionDesc*, int);
@@ -117,6 +124,7 @@ struct BatchPlan {
   int colorIcp;             // some session tracks with the photometric term
   int shiftFmtMask;         // bit per dense format of the shifting sessions
   int shiftColor;           // some shifting session has a colour volume
+  int hashSwap;             // some hash session swaps blocks to the host
   nui_tuning tune;          // the context's launch shapes
   BatchPlan() { std::memset(this, 0, sizeof(*this)); }
   bool operator<(const BatchPlan& o) const { return std::memcmp(this, &o, sizeof(BatchPlan)) < 0; }
@@ -195,6 +203,18 @@ struct nui_session {
   long frames = 0;
   bool color_frame = false;
   std::vector<void*> allocs;
+  std::vector<void*> host_allocs;  // pinned, mapped (the hash global cache's store)
+  // hash global cache
+  uint8_t* swap = nullptr;
+  int* store_slot = nullptr;
+  int *swap_in_ids = nullptr, *swap_out_ids = nullptr;
+  void* st_sdf = nullptr;  // device-mapped host pointers
+  uint8_t* st_w = nullptr;
+  uchar4* st_rgb = nullptr;
+  void* h_st_sdf = nullptr;  // the same memory, host pointers
+  uint8_t* h_st_w = nullptr;
+  uchar4* h_st_rgb = nullptr;
+  int st_cap = 0;
 };
 
 // ------------------------------------------------------------------ helpers
@@ -232,6 +252,8 @@ bool cfg_valid(const nui_session_cfg* c, std::string& why) {
     return why = "photometric weight must be finite and >= 0", false;
   if (c->photometric_weight > 0.f && !c->color_volume) return why = "colour tracking needs color_volume = 1", false;
   if (c->voxel_shift < 0 || c->shift_point_cap < 0) return why = "voxel shift and point cap must be >= 0", false;
+  if (c->hash_swapping && c->volume_kind != NUI_VOLUME_HASH) return why = "swapping needs a voxel-hash volume", false;
+  if (c->hash_store_blocks < 0) return why = "hash store blocks must be >= 0", false;
   if (c->voxel_shift > 0) {
     if (c->volume_kind != NUI_VOLUME_DENSE) return why = "a shifting volume must be dense", false;
     for (int i = 0; i < 3; ++i) {
@@ -342,6 +364,15 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
     d.alloc_list = s->alloc_list;
     d.excess_list = s->excess_list;
     d.hcount = s->hcount;
+    d.swapping = c.hash_swapping ? 1 : 0;
+    d.swap = s->swap;
+    d.store_slot = s->store_slot;
+    d.swap_in_ids = s->swap_in_ids;
+    d.swap_out_ids = s->swap_out_ids;
+    d.st_sdf = s->st_sdf;
+    d.st_w = s->st_w;
+    d.st_rgb = s->st_rgb;
+    d.st_cap = s->st_cap;
     d.alloc_type = s->alloc_type;
     d.vis = s->vis;
     d.coords = s->coords;
@@ -362,6 +393,7 @@ void plan_add(BatchPlan& p, const nui_session* s) {
   for (int l = 0; l < c.levels; ++l) p.maxIters[l] = std::max(p.maxIters[l], c.iterations[l]);
   if (s->hash) {
     p.hashMask |= 1 << (c.tsdf_format == NUI_TSDF_I16 ? 0 : 1);
+    if (c.hash_swapping) p.hashSwap = 1;
     p.maxHashBlk = std::max(p.maxHashBlk, ((long)c.hash_buckets + c.hash_excess + 1023) / 1024);
     return;
   }
@@ -395,6 +427,7 @@ void plan_merge(BatchPlan& a, const BatchPlan& b) {
   a.colorIcp |= b.colorIcp;
   a.shiftFmtMask |= b.shiftFmtMask;
   a.shiftColor |= b.shiftColor;
+  a.hashSwap |= b.hashSwap;
 }
 
 unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
@@ -449,8 +482,23 @@ void launch_hash_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_
   k_hash_count<<<dim3(nb, p.n), 256, 0, st>>>(d, 1);
   k_hash_scan<<<p.n, 1024, 0, st>>>(d, 1);
   k_hash_compact<<<dim3(nb, p.n), 1024, 0, st>>>(d);
+  if (p.hashSwap) {  // global cache: re-allocations and the swap-in list
+    k_hash_count<<<dim3(nb, p.n), 256, 0, st>>>(d, 2);
+    k_hash_scan<<<p.n, 1024, 0, st>>>(d, 2);
+    k_hash_swap_lists<<<dim3(nb, p.n), 1024, 0, st>>>(d);
+  }
   if (p.hashMask & 1) k_hash_integrate<0><<<dim3(1184, p.n), 512, 0, st>>>(d);
   if (p.hashMask & 2) k_hash_integrate<1><<<dim3(1184, p.n), 512, 0, st>>>(d);
+  if (p.hashSwap) {  // global cache: swap in, then swap out
+    if (p.hashMask & 1) k_hash_swap_in<0><<<dim3(1184, p.n), 512, 0, st>>>(d);
+    if (p.hashMask & 2) k_hash_swap_in<1><<<dim3(1184, p.n), 512, 0, st>>>(d);
+    k_hash_count<<<dim3(nb, p.n), 256, 0, st>>>(d, 3);
+    k_hash_scan<<<p.n, 1024, 0, st>>>(d, 3);
+    k_hash_swap_out_list<<<dim3(nb, p.n), 1024, 0, st>>>(d);
+    if (p.hashMask & 1) k_hash_swap_out<0><<<dim3(1184, p.n), 512, 0, st>>>(d);
+    if (p.hashMask & 2) k_hash_swap_out<1><<<dim3(1184, p.n), 512, 0, st>>>(d);
+    k_hash_swap_clean<<<p.n, 1024, 0, st>>>(d);
+  }
 }
 void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   if (!p.hashMask) return;
@@ -971,6 +1019,7 @@ NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
     b += ne * (16 + 1 + 1 + 8 + 8 + 4) + ((ne + 1023) / 1024) * 16 + (size_t)c->hash_pool_blocks * 4 +
          (size_t)c->hash_excess * 4 + N * 8;
     b += nv * ((c->tsdf_format == NUI_TSDF_I16 ? 2 : 2) + 1 + (c->color_volume ? 4 : 0));
+    if (c->hash_swapping) b += ne * 5 + 2 * 4096 * 4;  // the store itself is host memory
     return b;
   }
   const size_t nv = (size_t)c->res[0] * c->res[1] * c->res[2];
@@ -1012,6 +1061,19 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
     s->allocs.push_back(*p);
     return true;
   };
+  // pinned host memory mapped into the device: *h the host pointer, *d the device one
+  auto host_alloc = [&](void** h, void** d, size_t bytes) -> bool {
+    if (cudaHostAlloc(h, bytes, cudaHostAllocMapped) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    s->host_allocs.push_back(*h);
+    if (cudaHostGetDevicePointer(d, *h, 0) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    return true;
+  };
   s->hash = c.volume_kind == NUI_VOLUME_HASH;
   bool ok = alloc((void**)&s->raw, N * 2) && alloc((void**)&s->dscaled, N * 4) && alloc((void**)&s->vref, N * 16) &&
             alloc((void**)&s->nref, N * 16) && alloc((void**)&s->ts, sizeof(TrackState)) &&
@@ -1025,11 +1087,21 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
     const size_t ne = (size_t)c.hash_buckets + c.hash_excess, hv = (size_t)c.hash_pool_blocks * 512;
     ok = ok && alloc((void**)&s->entries, ne * sizeof(HEntry)) && alloc((void**)&s->hsdf, hv * 2) &&
          alloc((void**)&s->hw, hv) && alloc((void**)&s->alloc_list, (size_t)c.hash_pool_blocks * 4) &&
-         alloc((void**)&s->excess_list, (size_t)c.hash_excess * 4) && alloc((void**)&s->hcount, 16) &&
+         alloc((void**)&s->excess_list, (size_t)c.hash_excess * 4) && alloc((void**)&s->hcount, 64) &&
          alloc((void**)&s->alloc_type, ne) && alloc((void**)&s->vis, ne) && alloc((void**)&s->coords, ne * 8) &&
          alloc((void**)&s->keys, ne * 8) && alloc((void**)&s->vis_ids, ne * 4) &&
          alloc((void**)&s->blk, ((ne + 1023) / 1024) * 16) && alloc((void**)&s->range, N * 8);
     if (ok && c.color_volume) ok = alloc((void**)&s->hrgb, hv * 4) && alloc((void**)&s->bgra, N * 4) && alloc((void**)&s->cmap, N * 4);
+    if (ok && c.hash_swapping) {
+      // the global cache: swap state and store slot per entry, transfer lists, and the
+      // store in pinned host memory mapped into the device (one slot per entry by default)
+      s->st_cap = c.hash_store_blocks > 0 ? c.hash_store_blocks : (int)ne;
+      const size_t sv = (size_t)s->st_cap * 512;
+      ok = alloc((void**)&s->swap, ne) && alloc((void**)&s->store_slot, ne * 4) &&
+           alloc((void**)&s->swap_in_ids, 4096 * 4) && alloc((void**)&s->swap_out_ids, 4096 * 4) &&
+           host_alloc(&s->h_st_sdf, &s->st_sdf, sv * 2) && host_alloc((void**)&s->h_st_w, (void**)&s->st_w, sv) &&
+           (!c.color_volume || host_alloc((void**)&s->h_st_rgb, (void**)&s->st_rgb, sv * 4));
+    }
   } else {
     ok = ok && alloc((void**)&s->vol, nv * (c.tsdf_format == 2 ? 2 : voxel_bytes(c.tsdf_format)));
     if (ok && c.tsdf_format == NUI_TSDF_F16_U8) ok = alloc((void**)&s->wvol, nv);
@@ -1047,6 +1119,7 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
          alloc((void**)&s->pts_rgba, (size_t)c.shift_point_cap * 16);
   if (!ok) {
     for (void* p : s->allocs) cudaFree(p);
+    for (void* p : s->host_allocs) cudaFreeHost(p);
     delete s;
     return fail(NUI_ERR_OOM, "device allocation failed");
   }
@@ -1054,6 +1127,7 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
   nui_status st = reset_session(s);
   if (st != NUI_OK) {
     for (void* p : s->allocs) cudaFree(p);
+    for (void* p : s->host_allocs) cudaFreeHost(p);
     delete s;
     return st;
   }
@@ -1065,6 +1139,7 @@ NUI_API nui_status nui_session_destroy(nui_session* s) {
   if (!s) return NUI_OK;
   cudaStreamSynchronize(s->ctx->stream);
   for (void* p : s->allocs) cudaFree(p);
+  for (void* p : s->host_allocs) cudaFreeHost(p);
   delete s;
   return NUI_OK;
 }
@@ -1175,9 +1250,14 @@ std::vector<std::pair<void*, size_t>> state_segments(const nui_session* s) {
     add(s->hrgb, hv * 4);
     add(s->alloc_list, (size_t)c.hash_pool_blocks * 4);
     add(s->excess_list, (size_t)c.hash_excess * 4);
-    add(s->hcount, 16);
+    add(s->hcount, 64);
     add(s->vis, ne);
     add(s->vis_ids, ne * 4);
+    add(s->swap, ne);
+    add(s->store_slot, ne * 4);
+    add(s->st_sdf, (size_t)s->st_cap * 512 * 2);
+    add(s->st_w, (size_t)s->st_cap * 512);
+    add(s->st_rgb, (size_t)s->st_cap * 512 * 4);
   } else {
     const size_t nv = (size_t)c.res[0] * c.res[1] * c.res[2];
     add(s->vol, nv * (c.tsdf_format == NUI_TSDF_F16_U8 ? 2 : voxel_bytes(c.tsdf_format)));
@@ -1223,7 +1303,7 @@ NUI_API nui_status nui_session_snapshot(nui_session* s, void* host, size_t bytes
   std::memcpy(host, &h, sizeof(h));
   char* p = (char*)host + sizeof(h);
   for (auto& seg : state_segments(s)) {
-    NUI_CUDA(cudaMemcpy(p, seg.first, seg.second, cudaMemcpyDeviceToHost));
+    NUI_CUDA(cudaMemcpy(p, seg.first, seg.second, cudaMemcpyDefault));
     p += seg.second;
   }
   return NUI_OK;
@@ -1242,10 +1322,45 @@ NUI_API nui_status nui_session_restore(nui_session* s, const void* host, size_t 
   NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
   const char* p = (const char*)host + sizeof(h);
   for (auto& seg : state_segments(s)) {
-    NUI_CUDA(cudaMemcpy(seg.first, p, seg.second, cudaMemcpyHostToDevice));
+    NUI_CUDA(cudaMemcpy(seg.first, p, seg.second, cudaMemcpyDefault));
     p += seg.second;
   }
   s->frames = h.frames;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_hash_swap_stats(nui_session* s, int* swapped_in, int* swapped_out, int* store_used,
+                                       int* store_refused) {
+  if (!s || !s->hash || !s->swap) return fail(NUI_ERR_INVALID_ARG, "not a swapping hash session");
+  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  int c[9];
+  NUI_CUDA(cudaMemcpy(c, s->hcount, sizeof(c), cudaMemcpyDeviceToHost));
+  if (swapped_in) *swapped_in = c[4];
+  if (swapped_out) *swapped_out = c[5];
+  if (store_used) *store_used = std::min(c[7], s->st_cap);
+  if (store_refused) *store_refused = c[8];
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_hash_stored_block(nui_session* s, int entry, void* sdf, uint8_t* weight, uint8_t* rgb4,
+                                         int* found) {
+  if (!s || !found || !s->hash || !s->swap) return fail(NUI_ERR_INVALID_ARG, "not a swapping hash session");
+  const long ne = (long)s->cfg.hash_buckets + s->cfg.hash_excess;
+  if (entry < 0 || entry >= ne) return fail(NUI_ERR_INVALID_ARG, "entry out of range");
+  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  int slot = -1;
+  NUI_CUDA(cudaMemcpy(&slot, s->store_slot + entry, sizeof(int), cudaMemcpyDeviceToHost));
+  *found = slot >= 0;
+  if (slot < 0) return NUI_OK;
+  const size_t o = (size_t)slot * 512;
+  if (sdf) std::memcpy(sdf, (const char*)s->h_st_sdf + o * 2, 512 * 2);
+  if (weight) std::memcpy(weight, s->h_st_w + o, 512);
+  if (rgb4) {
+    if (s->h_st_rgb)
+      std::memcpy(rgb4, s->h_st_rgb + o, 512 * 4);
+    else
+      std::memset(rgb4, 0, 512 * 4);
+  }
   return NUI_OK;
 }
 
@@ -1463,6 +1578,11 @@ NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void*
       break;
     }
     case 23: src = s->range; need = N * 8; break;
+    case 24:  // the global cache's swap state per entry
+      if (!s->swap) return fail(NUI_ERR_INVALID_ARG, "not a swapping hash session");
+      src = s->swap;
+      need = (size_t)c.hash_buckets + c.hash_excess;
+      break;
     case 22: {
       if (!s->hash) return fail(NUI_ERR_INVALID_ARG, "not a hash session");
       need = (size_t)c.hash_pool_blocks * 512 * 6;

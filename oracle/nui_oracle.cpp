@@ -1804,6 +1804,14 @@ ORC_API int orc_hash_stored(const OrcHash* h, int id, int16_t* sdf, uint8_t* w, 
   return 1;
 }
 ORC_API long orc_hash_stored_count(const OrcHash* h) { return (long)h->store.size(); }
+// Entries with a stored copy, in increasing order; returns how many (up to cap written).
+ORC_API long orc_hash_stored_ids(const OrcHash* h, int* ids, long cap) {
+  std::vector<int> v;
+  for (const auto& kv : h->store) v.push_back(kv.first);
+  std::sort(v.begin(), v.end());
+  for (long i = 0; i < (long)v.size() && i < cap; ++i) ids[i] = v[i];
+  return (long)v.size();
+}
 
 // A17: integrateIntoScene_kernel (KinfuHashScene.cl:387-470) over the visible list.
 ORC_API void orc_hash_integrate(OrcHash* h, const float* depth, const uint8_t* bgra, const OrcCam* cam,

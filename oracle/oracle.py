@@ -339,6 +339,7 @@ _hash_sigs = {
     "orc_hash_swap_states": (_P, [_P]),
     "orc_hash_stored": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "orc_hash_stored_count": (C.c_long, [_P]),
+    "orc_hash_stored_ids": (C.c_long, [_P, _P, C.c_long]),
 }
 _ref_hash_sigs = {
     "ref_hash_sizes": (None, [_P, _P, _P]),
@@ -446,6 +447,11 @@ class OracleHash:
 
     def stored_count(self):
         return oracle().orc_hash_stored_count(self.h)
+
+    def stored_ids(self):
+        ids = np.zeros(self.n_entries, np.int32)
+        n = oracle().orc_hash_stored_ids(self.h, p(ids), ids.size)
+        return ids[:n].copy()
 
     def counters(self):
         a, b, c = C.c_int(), C.c_int(), C.c_long()
