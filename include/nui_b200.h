@@ -286,9 +286,10 @@ NUI_API nui_session* nui_server_session(nui_server* srv, int slot);
 /* Per-stage device time of the last nui_batch_tick* / nui_process_frame* call of the
  * context, when timing is enabled (CUDA events on the context stream).
  * stage: 0 preprocess, 1 pyramid + feedback maps, 2 tracking (colour gradients, ICP, gate),
- * 3 shifting-volume shifts + dense integration kernel, 4 brick summaries + voxel-hash
- * allocation / integration,
- * 5 raycast (dense and hash), 6 whole tick. */
+ * 3 shifting-volume shifts + dense integration kernel, 4 brick summaries (+ voxel-hash
+ * allocation / integration), 5 raycast, 6 whole tick.  When the batch holds dense and
+ * voxel-hash sessions, the hash sessions' allocation, integration and raycast run on a
+ * second stream beside stages 3-5 instead; stage 5 then ends when both are done. */
 NUI_API nui_status nui_ctx_enable_timing(nui_ctx* ctx, int enable);
 NUI_API nui_status nui_ctx_stage_ms(nui_ctx* ctx, int stage, float* ms);
 /* Kernel launches in the captured graph of the context's last graphed batch tick. */

@@ -133,6 +133,10 @@ struct BatchPlan {
 struct nui_ctx {
   int device = 0;
   cudaStream_t own = nullptr, stream = nullptr;
+  // the voxel-hash sessions' integration and raycast run beside the dense ones: a second
+  // stream forked from and joined back to `stream` within each tick (and its graph)
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   bool timing = false;
   cudaEvent_t ev[kStages] = {};
   float stage_ms[kStages] = {};
@@ -581,6 +585,20 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
   mark(2);
   launch_track(p, d, st, d_pose, d_status);
   mark(3);
+  // With dense and hash sessions in the batch, the hash sessions' allocation, integration
+  // and raycast run on the side stream, beside the dense ones: the two sets of kernels
+  // touch disjoint sessions, and the many short kernels of the hash allocation fill the
+  // gaps of the dense integration.
+  const bool fork = p.hashMask && p.fmtMask;
+  cudaStream_t hs = fork ? ctx->side : st;
+  if (fork) {
+    cudaEventRecord(ctx->fork_ev, st);
+    cudaStreamWaitEvent(hs, ctx->fork_ev, 0);
+  }
+  if (fork) {
+    launch_hash_integrate(p, d, hs);
+    launch_hash_raycast(p, d, hs);
+  }
   launch_shift(p, d, st);
   launch_integrate<0>(p, d, st);
   launch_integrate<1>(p, d, st);
@@ -588,13 +606,18 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
   launch_integrate<3>(p, d, st);
   mark(4);
   launch_summaries(p, d, st, 0);
-  launch_hash_integrate(p, d, st);
+  if (!fork) launch_hash_integrate(p, d, st);
   mark(5);
   launch_raycast<0>(p, d, st);
   launch_raycast<1>(p, d, st);
   launch_raycast<2>(p, d, st);
   launch_raycast<3>(p, d, st);
-  launch_hash_raycast(p, d, st);
+  if (fork) {
+    cudaEventRecord(ctx->join_ev, hs);
+    cudaStreamWaitEvent(st, ctx->join_ev, 0);
+  } else {
+    launch_hash_raycast(p, d, st);
+  }
   mark(6);
 }
 
@@ -832,6 +855,13 @@ NUI_API nui_status nui_ctx_create(int device, nui_ctx** out) {
   }
   c->stream = c->own;
   for (int i = 0; i < kStages; ++i) cudaEventCreate(&c->ev[i]);
+  if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return fail(NUI_ERR_DEVICE, "context streams");
+  }
   if (cudaMalloc(&c->d_kdesc, sizeof(SessionDesc)) != cudaSuccess ||
       cudaMalloc(&c->d_kts, sizeof(TrackState)) != cudaSuccess ||
       cudaMalloc(&c->d_count, sizeof(unsigned long long)) != cudaSuccess) {
@@ -858,6 +888,9 @@ NUI_API nui_status nui_ctx_destroy(nui_ctx* c) {
   cudaFree(c->d_kts);
   cudaFree(c->d_count);
   cudaStreamDestroy(c->own);
+  cudaStreamDestroy(c->side);
+  cudaEventDestroy(c->fork_ev);
+  cudaEventDestroy(c->join_ev);
   delete c;
   return NUI_OK;
 }
