@@ -135,15 +135,18 @@ struct RayVol {
     const float a = (p.x - ((float)gx + 0.5f) * c0) / c0;
     const float b = (p.y - ((float)gy + 0.5f) * c1) / c1;
     const float c = (p.z - ((float)gz + 0.5f) * c2) / c2;
+    // The eight voxels read directly: a voxel of an empty brick has weight 0 anyway, so the
+    // brick test of tsdf_at would only add work here, next to the surface.
     float t000, t001, t011, t010, t110, t111, t101, t100;
-    if (!tsdf_at(gx, gy, gz, t000)) return qnan();
-    if (!tsdf_at(gx, gy, gz + 1, t001)) return qnan();
-    if (!tsdf_at(gx + 1, gy, gz + 1, t011)) return qnan();
-    if (!tsdf_at(gx + 1, gy, gz, t010)) return qnan();
-    if (!tsdf_at(gx + 1, gy + 1, gz, t110)) return qnan();
-    if (!tsdf_at(gx + 1, gy + 1, gz + 1, t111)) return qnan();
-    if (!tsdf_at(gx, gy + 1, gz + 1, t101)) return qnan();
-    if (!tsdf_at(gx, gy + 1, gz, t100)) return qnan();
+    const unsigned i = vidx(gx, gy, gz), dy = (unsigned)rx, dz = (unsigned)rx * (unsigned)ry;
+    if (!load(i, t000)) return qnan();
+    if (!load(i + dz, t001)) return qnan();
+    if (!load(i + 1 + dz, t011)) return qnan();
+    if (!load(i + 1, t010)) return qnan();
+    if (!load(i + 1 + dy, t110)) return qnan();
+    if (!load(i + 1 + dy + dz, t111)) return qnan();
+    if (!load(i + dy + dz, t101)) return qnan();
+    if (!load(i + dy, t100)) return qnan();
     return t000 * (1 - a) * (1 - b) * (1 - c) + t001 * (1 - a) * (1 - b) * c + t010 * (1 - a) * b * (1 - c) +
            t011 * (1 - a) * b * c + t100 * a * (1 - b) * (1 - c) + t101 * a * (1 - b) * c +
            t110 * a * b * (1 - c) + t111 * a * b * c;
