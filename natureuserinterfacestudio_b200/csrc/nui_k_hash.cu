@@ -747,7 +747,27 @@ __global__ void __launch_bounds__(128, 8) k_hash_raycast(const SessionDesc* __re
   float total, totalMax, sdfv = 1.0f;
   hash_ray<HF>(s, pid, pr, total, totalMax, dir);
   hash_march<HF>(R, s, pr, total, totalMax, dir, stepScale, sdfv);
-  hash_finish<HF>(R, s, pid, pr, dir, stepScale, sdfv);
+  // the march's end point and last sdf wait in the vertex map for k_hash_finish
+  s.vref[pid] = make_float4(pr.x, pr.y, pr.z, sdfv);
+}
+
+// The surface refinement, normal and colour of every pixel after the march: a kernel of
+// its own, so that each of the two stays small in the instruction cache (the refinement's
+// many neighbourhood reads and the march's lookups do not fit it together), and the
+// refining lanes of a warp run together.
+template <int HF>
+__global__ void __launch_bounds__(256, 4) k_hash_finish(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!s.hash || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
+  const int pid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pid >= s.W * s.H) return;
+  const float4 e = s.vref[pid];
+  HashRead<HF> R{s, 0, 0, 0, -1};
+  const float stepScale = s.mu * (1.0f / s.voxel) * 0.6f;
+  float3 ps, dir;
+  float total, totalMax;
+  hash_ray<HF>(s, pid, ps, total, totalMax, dir);
+  hash_finish<HF>(R, s, pid, f3(e.x, e.y, e.z), dir, stepScale, e.w);
 }
 
 // ------------------------------------------------------------------ global cache
@@ -965,6 +985,8 @@ template __global__ void k_hash_integrate<0>(const SessionDesc*);
 template __global__ void k_hash_integrate<1>(const SessionDesc*);
 template __global__ void k_hash_raycast<0>(const SessionDesc*, int);
 template __global__ void k_hash_raycast<1>(const SessionDesc*, int);
+template __global__ void k_hash_finish<0>(const SessionDesc*);
+template __global__ void k_hash_finish<1>(const SessionDesc*);
 
 }  // namespace nui
 

@@ -62,6 +62,8 @@ __global__ void k_hash_range(const SessionDesc*);
 __global__ void k_hash_project(const SessionDesc*);
 template <int F>
 __global__ void k_hash_raycast(const SessionDesc*, int);
+template <int F>
+__global__ void k_hash_finish(const SessionDesc*);
 __global__ void k_hash_reset(const SessionDesc*);
 __global__ void k_hash_swap_lists(const SessionDesc*);
 template <int F>
@@ -512,6 +514,9 @@ void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t 
   const unsigned tiles = ray_blocks(p, tw);
   if (p.hashMask & 1) k_hash_raycast<0><<<dim3(tiles, p.n), 128, 0, st>>>(d, tw);
   if (p.hashMask & 2) k_hash_raycast<1><<<dim3(tiles, p.n), 128, 0, st>>>(d, tw);
+  const unsigned px = cdiv((long)p.maxW * p.maxH, 256);
+  if (p.hashMask & 1) k_hash_finish<0><<<dim3(px, p.n), 256, 0, st>>>(d);
+  if (p.hashMask & 2) k_hash_finish<1><<<dim3(px, p.n), 256, 0, st>>>(d);
 }
 
 // The shifts of the shifting volumes (after tracking, before integration): per axis, the
