@@ -175,6 +175,18 @@ struct RayVol {
   }
 };
 
+// Camera ray of pixel (px, py) in volume coordinates (raycast.cl:150-162): its start (the
+// camera centre), direction and the volume offset (half the x / y extent).
+__device__ __forceinline__ void ray_of(const SessionDesc& s, int px, int py, float3& start, float3& dir, float3& off) {
+  const DevXform& m = s.ts->xf;
+  off = f3(s.dim[0] / 2.0f, s.dim[1] / 2.0f, 0.f);
+  const float3 t = f3(m.t[0], m.t[1], m.t[2]);
+  start = add3(t, off);
+  float3 nx = f3(((float)px - s.cam.cx) * s.cam.fx_inv, ((float)py - s.cam.cy) * s.cam.fy_inv, 1.f);
+  nx = add3(add3(rot_rows(m.R, nx), t), off);
+  dir = normalize3(sub3(nx, start));
+}
+
 template <int FMT>
 __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__ descs, int tw) {
   const SessionDesc& s = descs[blockIdx.y];
@@ -190,19 +202,13 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
   const int py = ((int)blockIdx.x / tiles_x) * bh + (warp >> 1) * th + lane / tw;
   if (px >= W || py >= H) return;
   const int id = py * W + px;
-  const float4 nanv = make_float4(qnan(), qnan(), qnan(), 0.f);
-  float4 vout = nanv, nout = nanv;
-  uchar4 cout = make_uchar4(0, 0, 0, 0);
   const RayVol<FMT> V{s.vol, s.wvol, s.occ, s.res[0], s.res[1], s.res[2], (s.res[0] + 7) >> 3, (s.res[1] + 7) >> 3,
                       s.cell[0], s.cell[1], s.cell[2], 1.0f / s.cell[0], 1.0f / s.cell[1], 1.0f / s.cell[2]};
-  const DevXform& m = s.ts->xf;
   const float D0 = s.dim[0], D1 = s.dim[1], D2 = s.dim[2];
-  const float3 off = f3(D0 / 2.0f, D1 / 2.0f, 0.f);
-  const float3 t = f3(m.t[0], m.t[1], m.t[2]);
-  const float3 start = add3(t, off);
-  float3 nx = f3(((float)px - s.cam.cx) * s.cam.fx_inv, ((float)py - s.cam.cy) * s.cam.fy_inv, 1.f);
-  nx = add3(add3(rot_rows(m.R, nx), t), off);
-  const float3 dir = normalize3(sub3(nx, start));
+  float3 start, dir, off;
+  ray_of(s, px, py, start, dir, off);
+  bool hit = false;  // a zero crossing between the samples at tc and tc + step
+  float tc = 0.f;
   const float txmin = ((double)fabsf(dir.x) < 1e-14) ? 0.f : (((dir.x > 0 ? 0.f : D0) - start.x) / dir.x);
   const float tymin = ((double)fabsf(dir.y) < 1e-14) ? 0.f : (((dir.y > 0 ? 0.f : D1) - start.y) / dir.y);
   const float tzmin = ((double)fabsf(dir.z) < 1e-14) ? 0.f : (((dir.z > 0 ? 0.f : D2) - start.z) / dir.z);
@@ -213,7 +219,7 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
   const float tmax = fminf(fminf(txmax, tymax), tzmax);
   tmin = fmaxf(tmin, 0.f);
   if (tmin < tmax) {
-    float tc = tmin;
+    tc = tmin;
     int gx, gy, gz;
     V.voxel_of(add3(start, mul3(dir, tc)), gx, gy, gz);
     gx = max(0, min(gx, V.rx - 1));
@@ -227,7 +233,6 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
     const int hx = (V.rx + 127) >> 7, hy = (V.ry + 127) >> 7;
     const float3 idir = f3(1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z);
     bool pend = false;  // tsdf stands for a skipped sample at tc whose class (NaN or > 0) is unread
-    bool hit = false;   // a zero crossing between the samples at tc and tn = tc + step
     float tn = tc;
     while (tc < max_time) {
       float prev = tsdf;
@@ -289,31 +294,54 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
       }
       tc = tn;
     }
-    // The refinement runs after the march, so that the lanes of a warp whose rays end at
-    // different samples still refine together.
-    if (hit) {
-      const float Ftdt = V.trilinear(add3(start, mul3(dir, tn)));
-      const float Ft = isnan(Ftdt) ? Ftdt : V.trilinear(add3(start, mul3(dir, tc)));
-      if (!isnan(Ft)) {
-        const float Ts = tc - step * Ft / (Ftdt - Ft);
-        const float3 vf = add3(start, mul3(dir, Ts));
-        vout = w0(sub3(vf, off));
-        if (s.cvol) cout = s.cvol[V.vidx(gx, gy, gz)];
-        int hx, hy, hz;
-        V.voxel_of(add3(start, mul3(dir, tc)), hx, hy, hz);
-        if (hx > 1 && hy > 1 && hz > 1 && hx < V.rx - 2 && hy < V.ry - 2 && hz < V.rz - 2) {
-          float3 q, n;
-          q = vf; q.x += s.cell[0]; const float fx1 = V.trilinear(q);
-          q = vf; q.x -= s.cell[0]; const float fx2 = V.trilinear(q);
-          n.x = fx1 - fx2;
-          q = vf; q.y += s.cell[1]; const float fy1 = V.trilinear(q);
-          q = vf; q.y -= s.cell[1]; const float fy2 = V.trilinear(q);
-          n.y = fy1 - fy2;
-          q = vf; q.z += s.cell[2]; const float fz1 = V.trilinear(q);
-          q = vf; q.z -= s.cell[2]; const float fz2 = V.trilinear(q);
-          n.z = fz1 - fz2;
-          nout = w0(normalize3(n));
-        }
+  }
+  // the crossing waits in the vertex map for k_raycast_finish
+  s.vref[id] = make_float4(tc, 0.f, 0.f, hit ? 1.f : 0.f);
+}
+
+// The zero-crossing refinement, normal and colour of every pixel after the march
+// (raycast.cl:212-272): a kernel of its own, so that the march keeps fewer registers and the
+// refining lanes of a warp run together.
+template <int FMT>
+__global__ void __launch_bounds__(256) k_raycast_finish(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (s.kind != kTrackFrame || s.fmt != FMT || s.ts->status != 0) return;
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= s.W * s.H) return;
+  const float4 e = s.vref[id];
+  const float4 nanv = make_float4(qnan(), qnan(), qnan(), 0.f);
+  float4 vout = nanv, nout = nanv;
+  uchar4 cout = make_uchar4(0, 0, 0, 0);
+  if (e.w != 0.f) {
+    const RayVol<FMT> V{s.vol, s.wvol, s.occ, s.res[0], s.res[1], s.res[2], (s.res[0] + 7) >> 3, (s.res[1] + 7) >> 3,
+                        s.cell[0], s.cell[1], s.cell[2], 1.0f / s.cell[0], 1.0f / s.cell[1], 1.0f / s.cell[2]};
+    float3 start, dir, off;
+    ray_of(s, id % s.W, id / s.W, start, dir, off);
+    const float step = s.trunc * 0.8f;
+    const float tc = e.x, tn = tc + step;
+    int gx, gy, gz;
+    V.voxel_of(add3(start, mul3(dir, tn)), gx, gy, gz);
+    const float Ftdt = V.trilinear(add3(start, mul3(dir, tn)));
+    const float Ft = isnan(Ftdt) ? Ftdt : V.trilinear(add3(start, mul3(dir, tc)));
+    if (!isnan(Ft)) {
+      const float Ts = tc - step * Ft / (Ftdt - Ft);
+      const float3 vf = add3(start, mul3(dir, Ts));
+      vout = w0(sub3(vf, off));
+      if (s.cvol) cout = s.cvol[V.vidx(gx, gy, gz)];
+      int hx, hy, hz;
+      V.voxel_of(add3(start, mul3(dir, tc)), hx, hy, hz);
+      if (hx > 1 && hy > 1 && hz > 1 && hx < V.rx - 2 && hy < V.ry - 2 && hz < V.rz - 2) {
+        float3 q, n;
+        q = vf; q.x += s.cell[0]; const float fx1 = V.trilinear(q);
+        q = vf; q.x -= s.cell[0]; const float fx2 = V.trilinear(q);
+        n.x = fx1 - fx2;
+        q = vf; q.y += s.cell[1]; const float fy1 = V.trilinear(q);
+        q = vf; q.y -= s.cell[1]; const float fy2 = V.trilinear(q);
+        n.y = fy1 - fy2;
+        q = vf; q.z += s.cell[2]; const float fz1 = V.trilinear(q);
+        q = vf; q.z -= s.cell[2]; const float fz2 = V.trilinear(q);
+        n.z = fz1 - fz2;
+        nout = w0(normalize3(n));
       }
     }
   }
@@ -326,5 +354,9 @@ template __global__ void k_raycast<0>(const SessionDesc*, int);
 template __global__ void k_raycast<1>(const SessionDesc*, int);
 template __global__ void k_raycast<2>(const SessionDesc*, int);
 template __global__ void k_raycast<3>(const SessionDesc*, int);
+template __global__ void k_raycast_finish<0>(const SessionDesc*);
+template __global__ void k_raycast_finish<1>(const SessionDesc*);
+template __global__ void k_raycast_finish<2>(const SessionDesc*);
+template __global__ void k_raycast_finish<3>(const SessionDesc*);
 
 }  // namespace nui

@@ -45,6 +45,8 @@ __global__ void k_brick_summary(const SessionDesc*, int);
 __global__ void k_super_summary(const SessionDesc*, int);
 template <int F>
 __global__ void k_raycast(const SessionDesc*, int);
+template <int F>
+__global__ void k_raycast_finish(const SessionDesc*);
 __global__ void k_publish(const SessionDesc*, int, float*, int*);
 __global__ void k_tick_begin(const SessionDesc*, int);
 __global__ void k_occ_clear(const SessionDesc*);
@@ -471,6 +473,7 @@ void launch_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   if (!(p.fmtMask & (1 << F))) return;
   const int tw = p.tune.raycast_tile_width;
   k_raycast<F><<<dim3(ray_blocks(p, tw), p.n), 128, 0, st>>>(d, tw);
+  k_raycast_finish<F><<<dim3(cdiv((long)p.maxW * p.maxH, 256), p.n), 256, 0, st>>>(d);
 }
 
 void launch_hash_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
