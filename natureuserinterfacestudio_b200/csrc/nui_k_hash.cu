@@ -481,42 +481,59 @@ __global__ void k_hash_range(const SessionDesc* __restrict__ descs) {
 }
 
 // project_minmax_depths_kernel (KinfuHashRaycast.cl:4-76) with atomic min / max per pixel
-// (positive floats order like their bit patterns).
-__global__ void k_hash_project(const SessionDesc* __restrict__ descs) {
+// (positive floats order like their bit patterns).  One warp per visible block: lanes 0-7
+// project its corners, the warp reduces their bounds, and all lanes share the block's
+// pixels.  The kernel's far depth is updated as zy = max(zx, z) after each corner, which
+// leaves the depth of the last corner that projected (zx is then at most that depth).
+__global__ void __launch_bounds__(256) k_hash_project(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (!s.hash || s.kind != kTrackFrame || s.ts->status != 0) return;
   const int nvis = s.hcount[2];
   const DevXform& m = s.ts->xf;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nvis; k += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int nwarps = gridDim.x * (blockDim.x >> 5);
+  for (int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); k < nvis; k += nwarps) {
     const HEntry en = load_entry(s.entries, (unsigned)s.vis_ids[k]);
     if (en.ptr < 0) continue;
     int ulx = s.W, uly = s.H, lrx = 0, lry = 0;
-    float zx = 999999.9f, zy = 0.05f;
-    for (int corner = 0; corner < 8; ++corner) {
-      const short cx = (short)(en.pos[0] + ((corner & 1) ? 1 : 0)), cy = (short)(en.pos[1] + ((corner & 2) ? 1 : 0)),
-                  cz = (short)(en.pos[2] + ((corner & 4) ? 1 : 0));
+    float zx = 999999.9f, pz = 0.f;
+    bool valid = false;
+    if (lane < 8) {
+      const short cx = (short)(en.pos[0] + ((lane & 1) ? 1 : 0)), cy = (short)(en.pos[1] + ((lane & 2) ? 1 : 0)),
+                  cz = (short)(en.pos[2] + ((lane & 4) ? 1 : 0));
       float3 p = mul3(mul3(f3((float)cx, (float)cy, (float)cz), 8.0f), s.voxel);
       p = xf_inverse(m, p);
-      if (isnan3(p) || p.z < 1e-6) continue;
-      const float u = p.x * s.cam.fx / p.z + s.cam.cx, v = p.y * s.cam.fy / p.z + s.cam.cy;
-      ulx = min(ulx, (int)floorf(u));
-      lrx = max(lrx, (int)ceilf(u));
-      uly = min(uly, (int)floorf(v));
-      lry = max(lry, (int)ceilf(v));
-      zx = fminf(zx, p.z);
-      zy = fmaxf(zx, p.z);
+      if (!(isnan3(p) || p.z < 1e-6)) {
+        valid = true;
+        const float u = p.x * s.cam.fx / p.z + s.cam.cx, v = p.y * s.cam.fy / p.z + s.cam.cy;
+        ulx = (int)floorf(u);
+        lrx = (int)ceilf(u);
+        uly = (int)floorf(v);
+        lry = (int)ceilf(v);
+        zx = p.z;
+        pz = p.z;
+      }
     }
+    const unsigned vb = __ballot_sync(0xffffffffu, valid);
+    ulx = min(__reduce_min_sync(0xffffffffu, ulx), s.W);
+    uly = min(__reduce_min_sync(0xffffffffu, uly), s.H);
+    lrx = max(__reduce_max_sync(0xffffffffu, lrx), 0);
+    lry = max(__reduce_max_sync(0xffffffffu, lry), 0);
+    for (int off = 16; off > 0; off >>= 1) zx = fminf(zx, __shfl_xor_sync(0xffffffffu, zx, off));
+    const float last = __shfl_sync(0xffffffffu, pz, vb ? 31 - __clz(vb) : 0);
+    const float zy = vb ? last : 0.05f;
     if (ulx < 0) ulx = 0;
     if (uly < 0) uly = 0;
     if (lrx >= s.W) lrx = s.W - 1;
     if (lry >= s.H) lry = s.H - 1;
     if (zx < 0.05f) zx = 0.05f;
-    for (int by = uly; by <= lry; ++by)
-      for (int bx = ulx; bx <= lrx; ++bx) {
-        float2* r = s.range + by * s.W + bx;
-        atomicMin(reinterpret_cast<int*>(&r->x), __float_as_int(zx));
-        atomicMax(reinterpret_cast<int*>(&r->y), __float_as_int(zy));
-      }
+    const int bw = lrx - ulx + 1, bh = lry - uly + 1;
+    if (bw <= 0 || bh <= 0) continue;
+    for (int q = lane; q < bw * bh; q += 32) {
+      float2* r = s.range + (uly + q / bw) * s.W + (ulx + q % bw);
+      atomicMin(reinterpret_cast<int*>(&r->x), __float_as_int(zx));
+      atomicMax(reinterpret_cast<int*>(&r->y), __float_as_int(zy));
+    }
   }
 }
 

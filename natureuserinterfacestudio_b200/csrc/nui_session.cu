@@ -512,7 +512,7 @@ void launch_hash_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_
 void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   if (!p.hashMask) return;
   k_hash_range<<<dim3(296, p.n), 256, 0, st>>>(d);
-  k_hash_project<<<dim3(296, p.n), 128, 0, st>>>(d);
+  k_hash_project<<<dim3(296, p.n), 256, 0, st>>>(d);
   const int tw = p.tune.hash_raycast_tile_width;
   const unsigned tiles = ray_blocks(p, tw);
   if (p.hashMask & 1) k_hash_raycast<0><<<dim3(tiles, p.n), 128, 0, st>>>(d, tw);
