@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(128) k_raycast(const SessionDesc* __restrict__
 // (raycast.cl:212-272): a kernel of its own, so that the march keeps fewer registers and the
 // refining lanes of a warp run together.
 template <int FMT>
-__global__ void __launch_bounds__(256) k_raycast_finish(const SessionDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(256, 4) k_raycast_finish(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (s.kind != kTrackFrame || s.fmt != FMT || s.ts->status != 0) return;
   const int id = blockIdx.x * blockDim.x + threadIdx.x;

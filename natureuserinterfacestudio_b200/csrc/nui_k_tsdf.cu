@@ -21,7 +21,7 @@ constexpr int kZUnroll = 4;
 constexpr int kChunk = 16;  // z slices per occlusion test
 
 template <int FMT>
-__global__ void __launch_bounds__(kTsdfThreads) k_integrate(const SessionDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(kTsdfThreads, 4) k_integrate(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (s.kind < 0 || s.fmt != FMT || !s.ts->integrate) return;
   const int rx = s.res[0], ry = s.res[1], rz = s.res[2];
