@@ -16,19 +16,6 @@ namespace nui {
 
 constexpr int kIcpThreads = 256;  // pixels per thread: the template parameter PPT (tuned)
 
-__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
-  s = a + b;
-  float bb = s - a;
-  e = (a - (s - bb)) + (b - bb);
-}
-// (h1, l1) += (h2, l2)
-__device__ __forceinline__ void acc_pair(float& h1, float& l1, float h2, float l2) {
-  float s, e;
-  two_sum(h1, h2, s, e);
-  h1 = s;
-  l1 = (l1 + l2) + e;
-}
-
 // Bilinear sample with holes; taps whose linear index falls past the map read as holes.
 __device__ __forceinline__ float3 bilinear_holes(const float4* __restrict__ src, float px, float py, int W,
                                                  int N) {
@@ -274,9 +261,11 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
   if (threadIdx.x < 21) reinterpret_cast<float*>(&sp)[threadIdx.x] = reinterpret_cast<const float*>(&ts->xf)[threadIdx.x];
   __syncthreads();
 
-  float hi[kIcpTerms], lo[kIcpTerms];
+  // per-thread sums of the FP32 row products in FP64 (B200 runs FP64 adds at half the FP32
+  // rate: cheaper than a compensated FP32 pair, and as exact for these sums)
+  double acc[kIcpTerms];
 #pragma unroll
-  for (int k = 0; k < kIcpTerms; ++k) hi[k] = lo[k] = 0.f;
+  for (int k = 0; k < kIcpTerms; ++k) acc[k] = 0.0;
 
   const float4* __restrict__ V = s.vlev[level];
   const float fx = s.cam.fx, fy = s.cam.fy, cx = s.cam.cx, cy = s.cam.cy;
@@ -292,13 +281,8 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
       float c[kIcpTerms];
       if (!color_row(s, i, sR, tc, c)) continue;
 #pragma unroll
-      for (int q = 0; q < kIcpTerms - 1; ++q) {
-        float ss, e;
-        two_sum(hi[q], c[q], ss, e);
-        hi[q] = ss;
-        lo[q] += e;
-      }
-      hi[28] += 1.0f;
+      for (int q = 0; q < kIcpTerms - 1; ++q) acc[q] += (double)c[q];
+      acc[28] += 1.0;
     }
   }
   const int base = blockIdx.x * per_block;
@@ -326,42 +310,29 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
 #pragma unroll
     for (int a = 0; a < 6; ++a)
 #pragma unroll
-      for (int b = a; b < 7; ++b, ++sh) {
-        float ss, e;
-        two_sum(hi[sh], c7[a] * c7[b], ss, e);
-        hi[sh] = ss;
-        lo[sh] += e;
-      }
-    {
-      float ss, e;
-      two_sum(hi[27], c7[6] * c7[6], ss, e);
-      hi[27] = ss;
-      lo[27] += e;
-    }
-    hi[28] += 1.0f;
+      for (int b = a; b < 7; ++b, ++sh) acc[sh] += (double)(c7[a] * c7[b]);
+    acc[27] += (double)(c7[6] * c7[6]);
+    acc[28] += 1.0;
   }
 
-  // warp reduction of the (hi, lo) pairs
+  // warp, then block reduction in FP64; the block's sums leave as (hi, lo) FP32 pairs
 #pragma unroll
   for (int k = 0; k < kIcpTerms; ++k) {
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      float h2 = __shfl_down_sync(0xffffffffu, hi[k], off);
-      float l2 = __shfl_down_sync(0xffffffffu, lo[k], off);
-      acc_pair(hi[k], lo[k], h2, l2);
-    }
+    for (int off = 16; off > 0; off >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], off);
   }
   constexpr int kWarps = kIcpThreads / 32;
-  __shared__ float2 wsum[kWarps][kIcpTerms];
+  __shared__ double wsum[kWarps][kIcpTerms];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) {
 #pragma unroll
-    for (int k = 0; k < kIcpTerms; ++k) wsum[warp][k] = make_float2(hi[k], lo[k]);
+    for (int k = 0; k < kIcpTerms; ++k) wsum[warp][k] = acc[k];
   }
   __syncthreads();
   if (threadIdx.x < kIcpTerms) {
-    float H = 0.f, L = 0.f;
-    for (int wi = 0; wi < kWarps; ++wi) acc_pair(H, L, wsum[wi][threadIdx.x].x, wsum[wi][threadIdx.x].y);
+    double D = 0.0;
+    for (int wi = 0; wi < kWarps; ++wi) D += wsum[wi][threadIdx.x];
+    const float H = (float)D, L = (float)(D - (double)H);
     s.partials[(size_t)blockIdx.x * kIcpTerms + threadIdx.x] = make_float2(H, L);
   }
   __threadfence();
