@@ -29,9 +29,13 @@ __global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc
   if (ty0 >= H) return;
   constexpr int SW = kPreTX + 2 * kMaxRadius, SH = kPreTY + 2 * kMaxRadius;
   __shared__ float tile[SH][SW];
-  __shared__ float gs[2 * kMaxRadius + 1];
+  // spatial weights g[dx] * g[dy] of the taps (the products the tap loop would form)
+  __shared__ float gw[2 * kMaxRadius + 1][2 * kMaxRadius + 1];
   const int tid = threadIdx.y * kPreTX + threadIdx.x;
-  if (tid < 2 * R + 1) gs[tid] = s.gauss[tid];
+  if (tid < (2 * R + 1) * (2 * R + 1)) {
+    const int ty = tid / (2 * R + 1), tx = tid % (2 * R + 1);
+    gw[ty][tx] = s.gauss[tx] * s.gauss[ty];
+  }
   const float dmin = s.cam.dmin, dmax = s.cam.dmax;
   const int sw = kPreTX + 2 * R, sh = kPreTY + 2 * R;
   for (int i = tid; i < sw * sh; i += kPreTX * kPreTY) {
@@ -55,14 +59,13 @@ __global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc
     float sd = 0.f, swt = 0.f;
     const float thr = s.depth_thr, sig = s.sigma_depth;
     for (int dy = 0; dy <= 2 * R; ++dy) {
-      const float gy = gs[dy];
       for (int dx = 0; dx <= 2 * R; ++dx) {
         float nr = tile[threadIdx.y + dy][threadIdx.x + dx];
         if (isnan(nr)) continue;
         float diff = fabsf(c - nr);
         if (nr > 0.0f && diff < thr) {
           float d2 = diff * diff;
-          float w = gs[dx] * gy * nui_expf(-(d2 * sig));
+          float w = gw[dy][dx] * nui_expf(-(d2 * sig));
           sd += nr * w;
           swt += w;
         }

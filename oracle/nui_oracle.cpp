@@ -82,22 +82,23 @@ struct OrcTsdf {
 };
 
 // exp() used for OpenCL's exp(): x = k*ln2 + r (Cody-Waite split of ln2),
-// exp(r) by Horner evaluation of the degree-7 Taylor polynomial, times 2^k.
+// exp(r) by Horner evaluation of the degree-7 Taylor polynomial, times 2^k; the reduction
+// and the polynomial in fused multiply-adds (std::fma, exactly rounded like the device's).
 ORC_API float oracle_expf(float x) {
   if (std::isnan(x)) return x;
   if (x > 88.5f) return std::numeric_limits<float>::infinity();
   if (x < -103.5f) return 0.f;
-  float kf = std::nearbyint(x * 1.44269504088896341f);
-  float r = x - kf * 0.693145751953125f;
-  r = r - kf * 1.42860682030941723e-6f;
+  const float kf = std::nearbyint(x * 1.44269504088896341f);
+  float r = std::fma(-kf, 0.693145751953125f, x);
+  r = std::fma(-kf, 1.42860682030941723e-6f, r);
   float p = 1.98412698412698413e-4f;
-  p = p * r + 1.38888888888888889e-3f;
-  p = p * r + 8.33333333333333333e-3f;
-  p = p * r + 4.16666666666666667e-2f;
-  p = p * r + 1.66666666666666667e-1f;
-  p = p * r + 0.5f;
-  p = p * r + 1.0f;
-  p = p * r + 1.0f;
+  p = std::fma(p, r, 1.38888888888888889e-3f);
+  p = std::fma(p, r, 8.33333333333333333e-3f);
+  p = std::fma(p, r, 4.16666666666666667e-2f);
+  p = std::fma(p, r, 1.66666666666666667e-1f);
+  p = std::fma(p, r, 0.5f);
+  p = std::fma(p, r, 1.0f);
+  p = std::fma(p, r, 1.0f);
   int k = (int)kf;
   // multiply by 2^k in two exact steps so that k down to -149 stays representable
   int k1 = k / 2, k2 = k - k1;
