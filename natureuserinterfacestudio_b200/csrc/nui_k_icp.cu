@@ -297,10 +297,10 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
     const float u = pp.x * fx / pp.z + cx;
     const float vv = pp.y * fy / pp.z + cy;
     if (!(u >= 0.0f && u < fW && vv >= 0.0f && vv < fH)) continue;
+    // both maps sampled at once (their eight loads in flight together), then tested
     const float3 rn = bilinear_holes(s.nref, u, vv, RW, RN);
-    if (isnan3(rn)) continue;
     const float3 rv = bilinear_holes(s.vref, u, vv, RW, RN);
-    if (isnan3(rv)) continue;
+    if (isnan3(rn) || isnan3(rv)) continue;
     const float3 diff = sub3(rv, pv);
     const float dist = sqrtf(dot3(diff, diff));
     if (!(dist < s.dist_thr)) continue;

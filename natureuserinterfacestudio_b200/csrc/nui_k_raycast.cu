@@ -100,10 +100,10 @@ struct RayVol {
       const float2 v = __ldg(reinterpret_cast<const float2*>(vol) + i);
       f = v.x;
       return (int)v.y > 0;
-    } else if (FMT == 2) {
-      if (__ldg(wvol + i) == 0) return false;
-      f = __half2float(reinterpret_cast<const __half*>(vol)[i]);
-      return true;
+    } else if (FMT == 2) {  // both planes read at once (no load waits on the other)
+      const uint8_t w = __ldg(wvol + i);
+      f = __half2float(__ldg(reinterpret_cast<const __half*>(vol) + i));
+      return w != 0;
     } else {
       const __half2 v = reinterpret_cast<const __half2*>(vol)[i];
       f = __low2float(v);
@@ -135,18 +135,20 @@ struct RayVol {
     const float a = (p.x - ((float)gx + 0.5f) * c0) / c0;
     const float b = (p.y - ((float)gy + 0.5f) * c1) / c1;
     const float c = (p.z - ((float)gz + 0.5f) * c2) / c2;
-    // The eight voxels read directly: a voxel of an empty brick has weight 0 anyway, so the
-    // brick test of tsdf_at would only add work here, next to the surface.
+    // The eight voxels read directly, all at once (a voxel of an empty brick has weight 0
+    // anyway, so the brick test of tsdf_at would only add work here, next to the surface);
+    // any unweighted one makes the sample NaN, whichever it is.
     float t000, t001, t011, t010, t110, t111, t101, t100;
     const unsigned i = vidx(gx, gy, gz), dy = (unsigned)rx, dz = (unsigned)rx * (unsigned)ry;
-    if (!load(i, t000)) return qnan();
-    if (!load(i + dz, t001)) return qnan();
-    if (!load(i + 1 + dz, t011)) return qnan();
-    if (!load(i + 1, t010)) return qnan();
-    if (!load(i + 1 + dy, t110)) return qnan();
-    if (!load(i + 1 + dy + dz, t111)) return qnan();
-    if (!load(i + dy + dz, t101)) return qnan();
-    if (!load(i + dy, t100)) return qnan();
+    bool ok = load(i, t000);
+    ok &= load(i + dz, t001);
+    ok &= load(i + 1 + dz, t011);
+    ok &= load(i + 1, t010);
+    ok &= load(i + 1 + dy, t110);
+    ok &= load(i + 1 + dy + dz, t111);
+    ok &= load(i + dy + dz, t101);
+    ok &= load(i + dy, t100);
+    if (!ok) return qnan();
     return t000 * (1 - a) * (1 - b) * (1 - c) + t001 * (1 - a) * (1 - b) * c + t010 * (1 - a) * b * (1 - c) +
            t011 * (1 - a) * b * c + t100 * a * (1 - b) * (1 - c) + t101 * a * (1 - b) * c +
            t110 * a * b * (1 - c) + t111 * a * b * c;
