@@ -73,7 +73,7 @@ struct SessionDesc {
   const uint8_t* bgra;
   float* dscaled;                 // pass-filtered depth * ray scale (integration input)
   float* dlev[kMaxLevels];        // depth pyramid (level 0 = bilateral output)
-  float4* vlev[kMaxLevels];       // camera-space vertex pyramid
+  float4* vlev[kMaxLevels];       // camera-space vertex pyramid of the kernel-level calls (null in sessions)
   float4* vref;                   // world-space reference vertex map (W x H)
   float4* nref;                   // world-space reference normal map
   uchar4* cmap;                   // reference colour map (nullable)
@@ -176,6 +176,18 @@ __device__ __forceinline__ float3 rot_rows(const float* M, float3 v) {
 }
 __device__ __forceinline__ float qnan() { return __int_as_float(0x7fc00000); }
 
+// Camera-space vertex of pixel (x, y) of pyramid level `level` at depth d
+// (depth2vertex_kernel, transformMaps.cl:18-42, with the level's intrinsics cx / 2^l and
+// 2^l / fx as the reference's pyramid passes them); NaN where d is.  At level 0 the
+// products are the full-resolution ones (2^0 / fx and cx / 2^0 are exact), so every
+// consumer that rebuilds a vertex from the depth pyramid gets the bits the stored map had.
+__device__ __forceinline__ float3 level_vertex(const DevCam& c, int level, int x, int y, float d) {
+  const float div = (float)(1 << level);
+  const float fxi = div * c.fx_inv, fyi = div * c.fy_inv, cxl = c.cx / div, cyl = c.cy / div;
+  if (isnan(d)) return f3(qnan(), qnan(), qnan());
+  return f3(d * (((float)x - cxl) * fxi), d * (((float)y - cyl) * fyi), d * 1.0f);
+}
+
 // exp() of the bilateral filter.  Method: x = k ln2 + r with a two-constant Cody-Waite
 // split of ln2, exp(r) by Horner evaluation of the degree-7 Taylor polynomial
 // (|r| <= ln2/2, truncation error < 1e-8 relative), scaled by 2^k in two exact steps.  The
@@ -201,6 +213,25 @@ __device__ __forceinline__ float nui_expf(float x) {
   int k1 = k / 2, k2 = k - k1;
   float s1 = __int_as_float((k1 + 127) << 23), s2 = __int_as_float((k2 + 127) << 23);
   return (p * s1) * s2;
+}
+
+// nui_expf for -87 <= x <= 0, the range of every bilateral tap when the depth threshold
+// and sigma keep thr^2 * sigma <= 87: no NaN, overflow or underflow tests, and one scale by
+// 2^k, which is normal there (k >= -126).  The result is nui_expf's: p * 2^k1 is exact, so
+// nui_expf's (p * 2^k1) * 2^k2 rounds the exact product p * 2^k once, as p * 2^k does.
+__device__ __forceinline__ float nui_expf_neg(float x) {
+  const float kf = rintf(x * 1.44269504088896341f);
+  float r = __fmaf_rn(-kf, 0.693145751953125f, x);
+  r = __fmaf_rn(-kf, 1.42860682030941723e-6f, r);
+  float p = 1.98412698412698413e-4f;
+  p = __fmaf_rn(p, r, 1.38888888888888889e-3f);
+  p = __fmaf_rn(p, r, 8.33333333333333333e-3f);
+  p = __fmaf_rn(p, r, 4.16666666666666667e-2f);
+  p = __fmaf_rn(p, r, 1.66666666666666667e-1f);
+  p = __fmaf_rn(p, r, 0.5f);
+  p = __fmaf_rn(p, r, 1.0f);
+  p = __fmaf_rn(p, r, 1.0f);
+  return p * __int_as_float(((int)kf + 127) << 23);
 }
 
 // ------------------------------------------------------------------ voxel formats

@@ -1,12 +1,13 @@
 // Point-to-plane ICP, one launch per iteration, no host round trip.
 //
-// Per pixel (icp_block_kernel, icp.cl:222-292): transform the level's vertex by the running
-// estimate, project into the previous camera with full-resolution intrinsics, bilinearly
-// sample the world reference normal and vertex (icp.cl:192-220; a tap NaN -> no match), and
-// if |q - p| < distThres form the row [n x p, n | n.(q - p)].  Each thread accumulates the
-// 29 products of its pixels; blocks reduce them with warp shuffles and shared memory, all as
-// (hi, lo) two-sum pairs in FP32; the last block to finish (ticket on an atomic counter)
-// adds the per-block pairs in double in a fixed order and runs the host step of
+// Per pixel (icp_block_kernel, icp.cl:222-292): rebuild the level's vertex from its depth,
+// transform it by the running estimate, project into the previous camera with
+// full-resolution intrinsics, bilinearly sample the world reference normal and vertex
+// (icp.cl:192-220; a tap NaN -> no match), and if |q - p| < distThres form the row
+// [n x p, n | n.(q - p)].  Each thread accumulates the 29 products of its pixels in FP64;
+// blocks reduce them with warp shuffles and shared memory and store (hi, lo) FP32 pairs;
+// the last block to finish (ticket on an atomic counter) adds the per-block pairs in
+// double in a fixed order and runs the host step of
 // NuiKinfuOpenCLDepthTracker::IterativeClosestPoint (NuiKinfuOpenCLDepthTracker.cpp:324-496):
 // Levenberg-Marquardt accept/reject, FP64 determinant check and Cholesky solve, ZYX Euler
 // increment composed in FP64.  The next launch reads the updated estimate.
@@ -267,7 +268,8 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
 #pragma unroll
   for (int k = 0; k < kIcpTerms; ++k) acc[k] = 0.0;
 
-  const float4* __restrict__ V = s.vlev[level];
+  // the level's vertices are rebuilt from its depth (4 bytes a pixel read instead of 16)
+  const float* __restrict__ Dl = s.dlev[level];
   const float fx = s.cam.fx, fy = s.cam.fy, cx = s.cam.cx, cy = s.cam.cy;
   const int RW = s.W, RN = s.W * s.H;
   const float fW = (float)s.W, fH = (float)s.H;
@@ -290,8 +292,10 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
   for (int k = 0; k < PPT && (int)blockIdx.x < nblocks; ++k) {
     const int i = base + k * kIcpThreads + threadIdx.x;
     if (i >= n) break;
-    const float3 v = xyz(__ldg(V + i));
-    if (isnan3(v)) continue;
+    const float dep = __ldg(Dl + i);
+    if (isnan(dep)) continue;
+    const int py = i / w;
+    const float3 v = level_vertex(s.cam, level, i - py * w, py, dep);
     const float3 pv = add3(rot_rows(sR, v), tc);
     const float3 pp = rot_rows(sp.R_inv, sub3(pv, tp));
     const float u = pp.x * fx / pp.z + cx;

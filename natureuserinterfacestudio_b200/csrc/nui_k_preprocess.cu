@@ -19,6 +19,34 @@
 namespace nui {
 
 constexpr int kPreTX = 32, kPreTY = 16;
+constexpr int kPreSW = kPreTX + 2 * kMaxRadius, kPreSH = kPreTY + 2 * kMaxRadius, kGW = 2 * kMaxRadius + 1;
+
+// The bilateral sum of one pixel: taps in row-major window order, each weighted by its
+// spatial weight times exp(-diff^2 sigma) when it is positive and within the depth
+// threshold of the centre c (NaN taps fail both tests).  t points at the window's corner
+// in the staged tile, g at the spatial weights.  KR > 0 unrolls a window of that radius;
+// FAST takes nui_expf_neg, valid when thr^2 sigma <= 87.
+template <int KR, bool FAST>
+__device__ __forceinline__ float bilateral_px(const float* t, const float* g, int R, float c, float thr, float sig) {
+  if (KR > 0) R = KR;
+  float sd = 0.f, swt = 0.f;
+#pragma unroll
+  for (int dy = 0; dy <= 2 * R; ++dy) {
+#pragma unroll
+    for (int dx = 0; dx <= 2 * R; ++dx) {
+      const float nr = t[dy * kPreSW + dx];
+      const float diff = fabsf(c - nr);
+      if (nr > 0.0f && diff < thr) {
+        const float d2 = diff * diff;
+        const float e = FAST ? nui_expf_neg(-(d2 * sig)) : nui_expf(-(d2 * sig));
+        const float w = g[dy * kGW + dx] * e;
+        sd += nr * w;
+        swt += w;
+      }
+    }
+  }
+  return sd / swt;
+}
 
 __global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
@@ -27,10 +55,9 @@ __global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc
   const int tilesX = (W + kPreTX - 1) / kPreTX;
   const int tx0 = (blockIdx.x % tilesX) * kPreTX, ty0 = (blockIdx.x / tilesX) * kPreTY;
   if (ty0 >= H) return;
-  constexpr int SW = kPreTX + 2 * kMaxRadius, SH = kPreTY + 2 * kMaxRadius;
-  __shared__ float tile[SH][SW];
+  __shared__ float tile[kPreSH][kPreSW];
   // spatial weights g[dx] * g[dy] of the taps (the products the tap loop would form)
-  __shared__ float gw[2 * kMaxRadius + 1][2 * kMaxRadius + 1];
+  __shared__ float gw[kGW][kGW];
   const int tid = threadIdx.y * kPreTX + threadIdx.x;
   if (tid < (2 * R + 1) * (2 * R + 1)) {
     const int ty = tid / (2 * R + 1), tx = tid % (2 * R + 1);
@@ -56,30 +83,23 @@ __global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc
   const float c = tile[threadIdx.y + R][threadIdx.x + R];
   float out = qnan();
   if (!isnan(c)) {
-    float sd = 0.f, swt = 0.f;
     const float thr = s.depth_thr, sig = s.sigma_depth;
-    for (int dy = 0; dy <= 2 * R; ++dy) {
-      for (int dx = 0; dx <= 2 * R; ++dx) {
-        float nr = tile[threadIdx.y + dy][threadIdx.x + dx];
-        if (isnan(nr)) continue;
-        float diff = fabsf(c - nr);
-        if (nr > 0.0f && diff < thr) {
-          float d2 = diff * diff;
-          float w = gw[dy][dx] * nui_expf(-(d2 * sig));
-          sd += nr * w;
-          swt += w;
-        }
-      }
-    }
-    out = sd / swt;
+    // every tap's exponent lies in [-thr^2 sigma, 0] (rounding is monotone)
+    const bool fast = sig >= 0.f && thr * thr * sig <= 87.f;
+    const float* t = &tile[threadIdx.y][threadIdx.x];
+    if (fast && R == 3) out = bilateral_px<3, true>(t, &gw[0][0], R, c, thr, sig);
+    else if (fast) out = bilateral_px<0, true>(t, &gw[0][0], R, c, thr, sig);
+    else out = bilateral_px<0, false>(t, &gw[0][0], R, c, thr, sig);
   }
   const size_t i = (size_t)y * W + x;
   s.dlev[0][i] = out;
   const float xl = ((float)x - s.cam.cx) * s.cam.fx_inv;
   const float yl = ((float)y - s.cam.cy) * s.cam.fy_inv;
-  float4 v = make_float4(qnan(), qnan(), qnan(), 0.f);
-  if (!isnan(out)) v = make_float4(out * xl, out * yl, out * 1.0f, 0.f);
-  s.vlev[0][i] = v;
+  if (s.vlev[0]) {  // the kernel-level call's vertex map (sessions rebuild vertices from depth)
+    float4 v = make_float4(qnan(), qnan(), qnan(), 0.f);
+    if (!isnan(out)) v = make_float4(out * xl, out * yl, out * 1.0f, 0.f);
+    s.vlev[0][i] = v;
+  }
   // ray-length depth for integration: the pass-filtered depth, not the bilateral output
   // (NuiKinfuOpenCLScene.cpp:218 passes GetDepthBuffer())
   sc = c;
@@ -128,12 +148,16 @@ __global__ void k_pyramid(const SessionDesc* __restrict__ descs, int level) {
     }
   const float d = n > 0 ? sum / (float)n : qnan();
   s.dlev[level][idx] = d;
-  const float div = (float)(1 << level);
-  const float fxi = div * s.cam.fx_inv, fyi = div * s.cam.fy_inv;
-  const float cxl = s.cam.cx / div, cyl = s.cam.cy / div;
-  float4 v = make_float4(qnan(), qnan(), qnan(), 0.f);
-  if (!isnan(d)) v = make_float4(d * (((float)x - cxl) * fxi), d * (((float)y - cyl) * fyi), d * 1.0f, 0.f);
-  s.vlev[level][idx] = v;
+  if (s.vlev[level]) s.vlev[level][idx] = w0(level_vertex(s.cam, level, x, y, d));
+}
+
+// A level's vertex map from its depth, for downloads (sessions keep no vertex maps).
+__global__ void k_vertex_map(const SessionDesc* __restrict__ descs, int level, float4* __restrict__ out) {
+  const SessionDesc& s = descs[blockIdx.y];
+  const int W = s.W >> level, H = s.H >> level;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= W * H) return;
+  out[idx] = w0(level_vertex(s.cam, level, idx % W, idx / W, s.dlev[level][idx]));
 }
 
 // Frame-0 reference maps: simple normals from the level-0 vertex map, then both maps to
@@ -145,8 +169,12 @@ __global__ void k_feedback(const SessionDesc* __restrict__ descs) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= W * H) return;
   const int x = idx % W, y = idx / W;
+  // the level-0 vertices: the kernel-level call's map, else rebuilt from the depth
   const float4* V = s.vlev[0];
-  const float3 c = xyz(V[idx]);
+  auto vtx = [&](int j, int jx, int jy) {
+    return V ? xyz(V[j]) : level_vertex(s.cam, 0, jx, jy, s.dlev[0][j]);
+  };
+  const float3 c = vtx(idx, x, y);
   const DevXform& m = s.ts->xf;
   if (isnan3(c)) {
     s.vref[idx] = make_float4(qnan(), qnan(), qnan(), 0.f);
@@ -154,14 +182,14 @@ __global__ void k_feedback(const SessionDesc* __restrict__ descs) {
     return;
   }
   const float thr = s.depth_thr;
-  auto pick = [&](bool ok, int j) {
+  auto pick = [&](bool ok, int j, int jx, int jy) {
     if (!ok) return c;
-    float3 q = xyz(V[j]);
+    float3 q = vtx(j, jx, jy);
     if (isnan3(q) || fabsf(c.z - q.z) > thr) return c;
     return q;
   };
-  const float3 l = pick(x > 0, idx - 1), r = pick(x < W - 1, idx + 1);
-  const float3 u = pick(y > 0, idx - W), d = pick(y < H - 1, idx + W);
+  const float3 l = pick(x > 0, idx - 1, x - 1, y), r = pick(x < W - 1, idx + 1, x + 1, y);
+  const float3 u = pick(y > 0, idx - W, x, y - 1), d = pick(y < H - 1, idx + W, x, y + 1);
   const float3 n = normalize3(cross3(sub3(r, l), sub3(d, u)));
   const float3 vw = add3(rot_rows(m.R, c), f3(m.t[0], m.t[1], m.t[2]));
   s.vref[idx] = w0(vw);

@@ -29,6 +29,7 @@ namespace nui {
 __global__ void k_preprocess(const SessionDesc*);
 __global__ void k_pyramid(const SessionDesc*, int);
 __global__ void k_feedback(const SessionDesc*);
+__global__ void k_vertex_map(const SessionDesc*, int, float4*);
 template <int PPT>
 __global__ void k_icp(const SessionDesc*, int, int);
 __global__ void k_track_finalize(const SessionDesc*, int);
@@ -175,8 +176,7 @@ struct nui_session {
   uint16_t* raw = nullptr;
   uint8_t* bgra = nullptr;
   float* dscaled = nullptr;
-  float* dlev[kMaxLevels] = {};
-  float4* vlev[kMaxLevels] = {};
+  float* dlev[kMaxLevels] = {};  // depth pyramid (vertices are rebuilt from it where used)
   float4 *vref = nullptr, *nref = nullptr;
   uchar4* cmap = nullptr;
   void* vol = nullptr;
@@ -313,7 +313,6 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
     d.iters[l] = l < c.levels ? c.iterations[l] : 0;
     d.icp_min_count[l] = s->icp_min_count[l];
     d.dlev[l] = s->dlev[l];
-    d.vlev[l] = s->vlev[l];
   }
   d.integ_thr = c.integration_threshold;
   d.raw = raw;
@@ -1052,7 +1051,7 @@ NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
   if (!cfg_valid(c, why)) return 0;
   const size_t N = (size_t)c->width * c->height;
   size_t b = N * 2 + N * 4 /*bgra*/ + N * 4 /*scaled*/ + N * 16 * 2 /*ref maps*/ + N * 4 /*cmap*/;
-  for (int l = 0; l < c->levels; ++l) b += (N >> (2 * l)) * (4 + 16);
+  for (int l = 0; l < c->levels; ++l) b += (N >> (2 * l)) * 4;
   b += sizeof(TrackState) + sizeof(SessionDesc) + icp_partial_bytes(*c);
   b += (N / (kTile * kTile) + 64) * 4;
   if (c->volume_kind == NUI_VOLUME_HASH) {
@@ -1121,7 +1120,7 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
             alloc((void**)&s->partials, icp_partial_bytes(c)) &&
             alloc((void**)&s->d_desc1, sizeof(SessionDesc));
   for (int l = 0; ok && l < c.levels; ++l)
-    ok = alloc((void**)&s->dlev[l], (N >> (2 * l)) * 4) && alloc((void**)&s->vlev[l], (N >> (2 * l)) * 16);
+    ok = alloc((void**)&s->dlev[l], (N >> (2 * l)) * 4);
   const size_t ntiles = (size_t)((c.width + kTile - 1) / kTile) * ((c.height + kTile - 1) / kTile);
   if (ok) ok = alloc((void**)&s->tile_max, ntiles * sizeof(float));
   if (s->hash) {
@@ -1601,7 +1600,21 @@ NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void*
   switch (what) {
     case 0: src = s->dlev[0]; need = N * 4; break;
     case 1: src = s->dscaled; need = N * 4; break;
-    case 2: src = s->vlev[level]; need = Nl * 16; break;
+    case 2: {  // vertex map of a level, rebuilt from its depth
+      need = Nl * 16;
+      if (bytes < need) return fail(NUI_ERR_INVALID_ARG, "buffer too small");
+      void* tmp = nullptr;
+      NUI_CUDA(cudaMalloc(&tmp, need));
+      SessionDesc d;
+      fill_desc(s, d, kInactive, nullptr, nullptr);
+      cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, s->ctx->stream);
+      k_vertex_map<<<dim3(cdiv((long)Nl, 256), 1), 256, 0, s->ctx->stream>>>(s->d_desc1, level, (float4*)tmp);
+      cudaError_t e = cudaMemcpyAsync(host, tmp, need, cudaMemcpyDeviceToHost, s->ctx->stream);
+      cudaStreamSynchronize(s->ctx->stream);
+      cudaFree(tmp);
+      if (e != cudaSuccess) return fail(NUI_ERR_DEVICE, cudaGetErrorString(e));
+      return NUI_OK;
+    }
     case 3: src = s->vref; need = N * 16; break;
     case 4: src = s->nref; need = N * 16; break;
     case 6: src = s->vol; need = nv * (c.tsdf_format == 2 ? 2 : voxel_bytes(c.tsdf_format)); break;
