@@ -336,11 +336,19 @@ __device__ __forceinline__ size_t occ2_index(const SessionDesc& s, int x, int y,
 }
 // round(p / c) for a voxel coordinate, exactly as the IEEE quotient would round: the
 // product with 1/c is within 2 ulp of the quotient, so unless it lies within 4 ulp of a
-// rounding boundary (n + 0.5) both round alike; otherwise divide.
+// rounding boundary (n + 0.5) both round alike; otherwise divide.  The nearest integer of
+// the product comes from the 1.5 * 2^23 shift (adds and an integer subtract, no rounding
+// or conversion instruction; exact for |q| < 2^22, and from |q| > 2^20 on every product
+// lies within the boundary margin anyway).  Its distance |q - n| to the product is
+// min(f, 1 - f) for the fraction f = q - floor(q), so the boundary test is unchanged, and
+// away from a boundary round-to-nearest-even and round-half-away agree.
 __device__ __forceinline__ int round_div(float p, float c, float inv) {
   const float q = p * inv;
-  const float f = q - floorf(q);
-  if (fabsf(f - 0.5f) > fabsf(q) * 4.8e-7f + 1e-6f) return (int)roundf(q);
+  const float big = 12582912.f;  // 1.5 * 2^23
+  const float sh = q + big;
+  const float f = q - (sh - big);  // q - n, exact
+  if (fabsf(q) < 4194304.f && fabsf(fabsf(f) - 0.5f) > fabsf(q) * 4.8e-7f + 1e-6f)
+    return __float_as_int(sh) - 0x4B400000;
   return (int)roundf(p / c);
 }
 
