@@ -169,7 +169,7 @@ __device__ void euler_zyx(double a, double b, double g, double* R) {
 }
 
 // LM step on the reduced sums (runs on one thread of the last block).
-__device__ void icp_host_step(TrackState* ts, const double* sums, int iter, unsigned min_count) {
+__device__ __noinline__ void icp_host_step(TrackState* ts, const double* sums, int iter, unsigned min_count) {
   float err = (float)sums[27];
   const float cnt = (float)sums[28];
   err = (cnt > 0.f) ? sqrtf(err) / cnt : 3.402823466e+38f;
@@ -240,7 +240,7 @@ __device__ void icp_host_step(TrackState* ts, const double* sums, int iter, unsi
 }
 
 template <int PPT>
-__global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restrict__ descs, int level, int iter) {
+__global__ void __launch_bounds__(kIcpThreads, 2) k_icp(const SessionDesc* __restrict__ descs, int level, int iter) {
   const SessionDesc& s = descs[blockIdx.y];
   if (s.kind != kTrackFrame || level >= s.levels || iter >= s.iters[level]) return;
   TrackState* ts = s.ts;
@@ -263,7 +263,9 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
   __syncthreads();
 
   // per-thread sums of the FP32 row products in FP64 (B200 runs FP64 adds at half the FP32
-  // rate: cheaper than a compensated FP32 pair, and as exact for these sums)
+  // rate: cheaper than a compensated FP32 pair, and as exact for these sums).  A launch
+  // shape that regroups the pixels then changes the sums by FP64 rounding only, far below
+  // anything that could flip a Levenberg-Marquardt decision.
   double acc[kIcpTerms];
 #pragma unroll
   for (int k = 0; k < kIcpTerms; ++k) acc[k] = 0.0;
@@ -288,12 +290,20 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
     }
   }
   const int base = blockIdx.x * per_block;
-#pragma unroll 1
-  for (int k = 0; k < PPT && (int)blockIdx.x < nblocks; ++k) {
+  // the depths of all the thread's pixels in flight at once, consumed from the front
+  float dq[PPT];
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
     const int i = base + k * kIcpThreads + threadIdx.x;
-    if (i >= n) break;
-    const float dep = __ldg(Dl + i);
+    dq[k] = ((int)blockIdx.x < nblocks && i < n) ? __ldg(Dl + i) : qnan();
+  }
+#pragma unroll 1
+  for (int k = 0; k < PPT; ++k) {
+    const float dep = dq[0];
+#pragma unroll
+    for (int j = 0; j + 1 < PPT; ++j) dq[j] = dq[j + 1];
     if (isnan(dep)) continue;
+    const int i = base + k * kIcpThreads + threadIdx.x;
     const int py = i / w;
     const float3 v = level_vertex(s.cam, level, i - py * w, py, dep);
     const float3 pv = add3(rot_rows(sR, v), tc);
@@ -320,17 +330,15 @@ __global__ void __launch_bounds__(kIcpThreads) k_icp(const SessionDesc* __restri
   }
 
   // warp, then block reduction in FP64; the block's sums leave as (hi, lo) FP32 pairs
-#pragma unroll
-  for (int k = 0; k < kIcpTerms; ++k) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], off);
-  }
   constexpr int kWarps = kIcpThreads / 32;
   __shared__ double wsum[kWarps][kIcpTerms];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) {
 #pragma unroll
-    for (int k = 0; k < kIcpTerms; ++k) wsum[warp][k] = acc[k];
+  for (int k = 0; k < kIcpTerms; ++k) {
+    double a = acc[k];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
+    if (lane == 0) wsum[warp][k] = a;
   }
   __syncthreads();
   if (threadIdx.x < kIcpTerms) {
