@@ -69,13 +69,31 @@ __device__ __forceinline__ float3 depth_to_point(const DevCam& c, int ux, int uy
 __device__ __forceinline__ bool hash_active(const SessionDesc& s) { return s.hash && s.kind >= 0 && s.ts->integrate; }
 
 // ------------------------------------------------------------------ allocation
+// The per-entry byte flags (alloc_type, vis, swap) are scanned four at a time: the four
+// bytes from entry i (a multiple of 4) in one 32-bit word when all lie below n, else byte
+// by byte (bytes at or past n read as 0).
+__device__ __forceinline__ unsigned load4(const uint8_t* p, unsigned i, unsigned n) {
+  if (i + 4 <= n) return *reinterpret_cast<const unsigned*>(p + i);
+  unsigned w = 0;
+  for (unsigned k = 0; k < 4 && i + k < n; ++k) w |= (unsigned)p[i + k] << (8 * k);
+  return w;
+}
+
 __global__ void k_hash_prepare(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (!hash_active(s)) return;
   const unsigned n = (unsigned)(s.nb + s.ne);
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    s.alloc_type[i] = 0;
-    s.vis[i] = s.vis[i] ? 3 : 0;
+  for (unsigned i = 4 * (blockIdx.x * blockDim.x + threadIdx.x); i < n; i += 4 * gridDim.x * blockDim.x) {
+    if (i + 4 <= n) {
+      reinterpret_cast<unsigned*>(s.alloc_type)[i >> 2] = 0u;
+      unsigned* v = reinterpret_cast<unsigned*>(s.vis) + (i >> 2);
+      *v = __vcmpne4(*v, 0u) & 0x03030303u;  // visible (any type) -> 3, else 0
+    } else {
+      for (unsigned k = i; k < n; ++k) {
+        s.alloc_type[k] = 0;
+        s.vis[k] = s.vis[k] ? 3 : 0;
+      }
+    }
   }
 }
 
@@ -159,14 +177,16 @@ __global__ void __launch_bounds__(256) k_hash_count(const SessionDesc* __restric
   const unsigned b0 = blockIdx.x * kHashScanBlock;
   if (b0 >= n) return;
   unsigned a = 0, e = 0;
-  for (unsigned i = b0 + threadIdx.x; i < min(n, b0 + kHashScanBlock); i += blockDim.x) {
-    if (which == 0) {
-      const uint8_t t = s.alloc_type[i];
-      a += t != 0;
-      e += t == 2;
-    } else if (which == 1) {
-      a += s.vis[i] > 0;
-    } else if (which == 2) {  // re-allocations, swap-ins
+  if (which <= 1) {  // four flags a thread (256 threads: the 1024 entries)
+    const unsigned i = b0 + 4 * threadIdx.x;
+    if (i < n) {
+      const unsigned w = load4(which == 0 ? s.alloc_type : s.vis, i, n);
+      a = __popc(__vcmpne4(w, 0u)) >> 3;  // each set byte of the mask holds 8 bits
+      if (which == 0) e = __popc(__vcmpeq4(w, 0x02020202u)) >> 3;
+    }
+  }
+  for (unsigned i = b0 + threadIdx.x; which >= 2 && i < min(n, b0 + kHashScanBlock); i += blockDim.x) {
+    if (which == 2) {  // re-allocations, swap-ins
       a += s.vis[i] > 0 && entry_ptr(s, i) == -1;
       e += s.swap[i] == 1;
     } else {  // swap-outs
@@ -282,6 +302,7 @@ __global__ void __launch_bounds__(kHashScanBlock) k_hash_alloc(const SessionDesc
   const unsigned n = (unsigned)(s.nb + s.ne);
   const unsigned b = blockIdx.x;
   if (b * kHashScanBlock >= n) return;
+  if (s.blk[4 * b] == 0) return;  // no request among the block's entries (k_hash_count)
   const unsigned i = b * kHashScanBlock + threadIdx.x;
   bool fa, fe;
   unsigned ta, te;
@@ -368,33 +389,55 @@ __global__ void k_hash_visible(const SessionDesc* __restrict__ descs) {
     }
     return;
   }
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    if (s.vis[i] != 3) continue;
-    const HEntry en = load_entry(s.entries, i);
-    float3 p = f3((float)en.pos[0] * factor, (float)en.pos[1] * factor, (float)en.pos[2] * factor);
-    bool v = point_visible(s, m, p);
-    if (!v) { p.z += factor; v = point_visible(s, m, p); }
-    if (!v) { p.y += factor; v = point_visible(s, m, p); }
-    if (!v) { p.x += factor; v = point_visible(s, m, p); }
-    if (!v) { p.z -= factor; v = point_visible(s, m, p); }
-    if (!v) { p.y -= factor; v = point_visible(s, m, p); }
-    if (!v) { p.x -= factor; p.y += factor; v = point_visible(s, m, p); }
-    if (!v) { p.x += factor; p.y -= factor; p.z += factor; v = point_visible(s, m, p); }
-    if (!v) s.vis[i] = 0;
+  for (unsigned i4 = 4 * (blockIdx.x * blockDim.x + threadIdx.x); i4 < n; i4 += 4 * gridDim.x * blockDim.x) {
+    unsigned m3 = __vcmpeq4(load4(s.vis, i4, n), 0x03030303u);  // entries visible at the last frame
+    while (m3) {
+      const int k = (__ffs(m3) - 1) >> 3;
+      m3 &= ~(0xFFu << (8 * k));
+      const unsigned i = i4 + (unsigned)k;
+      const HEntry en = load_entry(s.entries, i);
+      float3 p = f3((float)en.pos[0] * factor, (float)en.pos[1] * factor, (float)en.pos[2] * factor);
+      bool v = point_visible(s, m, p);
+      if (!v) { p.z += factor; v = point_visible(s, m, p); }
+      if (!v) { p.y += factor; v = point_visible(s, m, p); }
+      if (!v) { p.x += factor; v = point_visible(s, m, p); }
+      if (!v) { p.z -= factor; v = point_visible(s, m, p); }
+      if (!v) { p.y -= factor; v = point_visible(s, m, p); }
+      if (!v) { p.x -= factor; p.y += factor; v = point_visible(s, m, p); }
+      if (!v) { p.x += factor; p.y -= factor; p.z += factor; v = point_visible(s, m, p); }
+      if (!v) s.vis[i] = 0;
+    }
   }
 }
 
-__global__ void __launch_bounds__(kHashScanBlock) k_hash_compact(const SessionDesc* __restrict__ descs) {
+// The visible list in index order: 256 threads a 1024-entry block, four entries each; a
+// thread's rank is the block offset (k_hash_scan) plus the visible entries of the threads
+// before it.
+__global__ void __launch_bounds__(256) k_hash_compact(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (!hash_active(s)) return;
   const unsigned n = (unsigned)(s.nb + s.ne);
   const unsigned b = blockIdx.x;
   if (b * kHashScanBlock >= n) return;
-  const unsigned i = b * kHashScanBlock + threadIdx.x;
-  bool f;
-  unsigned t;
-  const unsigned r = block_rank(i, n, [&](unsigned k) { return s.vis[k] > 0; }, f, t);
-  if (f) s.vis_ids[s.blk[4 * b + 2] + r] = (int)i;
+  if (s.blk[4 * b] == 0) return;  // no visible entry in the block
+  const unsigned i = b * kHashScanBlock + 4 * threadIdx.x;
+  const unsigned m = i < n ? __vcmpne4(load4(s.vis, i, n), 0u) : 0u;
+  const unsigned c = __popc(m) >> 3;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned incl = c;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const unsigned o = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += o;
+  }
+  __shared__ unsigned wsum[8];
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  unsigned r = s.blk[4 * b + 2] + incl - c;
+  for (int w = 0; w < warp; ++w) r += wsum[w];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if ((m >> (8 * k)) & 1u) s.vis_ids[r++] = (int)(i + k);
 }
 
 // ------------------------------------------------------------------ integration

@@ -489,7 +489,7 @@ void launch_hash_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_
   k_hash_visible<<<dim3(592, p.n), 256, 0, st>>>(d);
   k_hash_count<<<dim3(nb, p.n), 256, 0, st>>>(d, 1);
   k_hash_scan<<<p.n, 1024, 0, st>>>(d, 1);
-  k_hash_compact<<<dim3(nb, p.n), 1024, 0, st>>>(d);
+  k_hash_compact<<<dim3(nb, p.n), 256, 0, st>>>(d);
   if (p.hashSwap) {  // global cache: re-allocations and the swap-in list
     k_hash_count<<<dim3(nb, p.n), 256, 0, st>>>(d, 2);
     k_hash_scan<<<p.n, 1024, 0, st>>>(d, 2);
