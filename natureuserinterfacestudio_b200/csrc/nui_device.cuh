@@ -57,6 +57,7 @@ enum FrameKind : int { kInactive = -1, kFirstFrame = 0, kTrackFrame = 1 };
 
 struct SessionDesc {
   int kind;  // FrameKind
+  int slot;  // the session's row of the batch outputs (pose, status)
   int W, H, levels;
   DevCam cam;
   // preprocessing (NuiTrackerConfig)

@@ -295,22 +295,11 @@ __device__ __forceinline__ unsigned block_rank(unsigned i, unsigned n, Pred pred
   return before + __popc(ballot & ((1u << lane) - 1u));
 }
 
-// allocateVoxelBlocksList_kernel (KinfuHashScene.cl:138-194) with the pops in index order.
-__global__ void __launch_bounds__(kHashScanBlock) k_hash_alloc(const SessionDesc* __restrict__ descs) {
-  const SessionDesc& s = descs[blockIdx.y];
-  if (!hash_active(s)) return;
-  const unsigned n = (unsigned)(s.nb + s.ne);
-  const unsigned b = blockIdx.x;
-  if (b * kHashScanBlock >= n) return;
-  if (s.blk[4 * b] == 0) return;  // no request among the block's entries (k_hash_count)
-  const unsigned i = b * kHashScanBlock + threadIdx.x;
-  bool fa, fe;
-  unsigned ta, te;
-  const unsigned ra = block_rank(i, n, [&](unsigned k) { return s.alloc_type[k] != 0; }, fa, ta);
-  const unsigned re = block_rank(i, n, [&](unsigned k) { return s.alloc_type[k] == 2; }, fe, te);
-  if (!fa) return;
-  const int last_block = s.hcount[0], last_excess = s.hcount[1];
-  const int vba = last_block - (int)(s.blk[4 * b + 2] + ra);
+// allocateVoxelBlocksList_kernel (KinfuHashScene.cl:138-194) with the pops in index order:
+// 256 threads a 1024-entry block, four entries each; an entry's ranks among the block's
+// requests and excess requests are the counts of the threads before it (one scan of both
+// counts packed in 16-bit halves) plus those of its own lower bytes.
+__device__ __forceinline__ void alloc_one(const SessionDesc& s, unsigned i, int vba, int exl) {
   const uint8_t t = s.alloc_type[i];
   const short4 c = s.coords[i];
   s.keys[i] = 0ull;
@@ -328,7 +317,6 @@ __global__ void __launch_bounds__(kHashScanBlock) k_hash_alloc(const SessionDesc
       atomicAdd(&s.hcount[3], 1);
     }
   } else {
-    const int exl = last_excess - (int)(s.blk[4 * b + 3] + re);
     if (vba >= 0 && exl >= 0) {
       HEntry en;
       en.pos[0] = c.x;
@@ -346,6 +334,42 @@ __global__ void __launch_bounds__(kHashScanBlock) k_hash_alloc(const SessionDesc
     } else {
       atomicAdd(&s.hcount[3], 1);
     }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_hash_alloc(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!hash_active(s)) return;
+  const unsigned n = (unsigned)(s.nb + s.ne);
+  const unsigned b = blockIdx.x;
+  if (b * kHashScanBlock >= n) return;
+  if (s.blk[4 * b] == 0) return;  // no request among the block's entries (k_hash_count)
+  const unsigned i = b * kHashScanBlock + 4 * threadIdx.x;
+  const unsigned w = i < n ? load4(s.alloc_type, i, n) : 0u;
+  const unsigned ma = __vcmpne4(w, 0u), me = __vcmpeq4(w, 0x02020202u);
+  const unsigned c = (__popc(ma) >> 3) | ((__popc(me) >> 3) << 16);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned incl = c;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const unsigned o = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += o;
+  }
+  __shared__ unsigned wsum[8];
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  unsigned before = incl - c;
+  for (int q = 0; q < warp; ++q) before += wsum[q];
+  if (!ma) return;
+  const int last_block = s.hcount[0], last_excess = s.hcount[1];
+  unsigned ra = s.blk[4 * b + 2] + (before & 0xffffu), re = s.blk[4 * b + 3] + (before >> 16);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (!((ma >> (8 * k)) & 1u)) continue;
+    const bool ex = (me >> (8 * k)) & 1u;
+    alloc_one(s, i + k, last_block - (int)ra, ex ? last_excess - (int)re : 0);
+    ++ra;
+    if (ex) ++re;
   }
 }
 

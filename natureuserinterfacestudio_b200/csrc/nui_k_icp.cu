@@ -95,74 +95,113 @@ __device__ __forceinline__ bool color_row(const SessionDesc& s, int i, const flo
 }
 
 // ---------------------------------------------------------------- FP64 host step
-__device__ double det6(double* A) {
+// The 6x6 algebra of the host step runs on one thread at the end of every ICP launch, so
+// its latency is the launch's tail: every loop below is unrolled with constant indices,
+// which keeps the matrices in registers (no local-memory round trips).
+
+// Determinant by Gaussian elimination with partial pivoting (the first row holding the
+// largest |entry| of the column); destroys A.
+__device__ __forceinline__ double det6(double (&A)[6][6]) {
   double det = 1.0;
+#pragma unroll
   for (int c = 0; c < 6; ++c) {
     int piv = c;
-    for (int r = c + 1; r < 6; ++r)
-      if (fabs(A[r * 6 + c]) > fabs(A[piv * 6 + c])) piv = r;
-    if (A[piv * 6 + c] == 0.0) return 0.0;
-    if (piv != c) {
-      for (int k = 0; k < 6; ++k) {
-        double t = A[c * 6 + k];
-        A[c * 6 + k] = A[piv * 6 + k];
-        A[piv * 6 + k] = t;
+    double best = fabs(A[c][c]);
+#pragma unroll
+    for (int r = c + 1; r < 6; ++r) {
+      const double v = fabs(A[r][c]);
+      if (v > best) {
+        best = v;
+        piv = r;
       }
+    }
+    if (best == 0.0) return 0.0;
+    if (piv != c) {
+#pragma unroll
+      for (int r = c + 1; r < 6; ++r)
+        if (piv == r) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) {
+            const double t = A[c][k];
+            A[c][k] = A[r][k];
+            A[r][k] = t;
+          }
+        }
       det = -det;
     }
-    det *= A[c * 6 + c];
+    det *= A[c][c];
+#pragma unroll
     for (int r = c + 1; r < 6; ++r) {
-      double f = A[r * 6 + c] / A[c * 6 + c];
-      for (int k = c; k < 6; ++k) A[r * 6 + k] -= f * A[c * 6 + k];
+      const double f = A[r][c] / A[c][c];
+#pragma unroll
+      for (int k = c; k < 6; ++k) A[r][k] -= f * A[c][k];
     }
   }
   return det;
 }
 
-__device__ bool llt_solve6(const double* A, const double* b, double* x) {
-  double L[36];
-  for (int i = 0; i < 36; ++i) L[i] = 0.0;
+// Cholesky factorisation A = L L^T and the two triangular solves; false if a pivot is not
+// positive.
+__device__ __forceinline__ bool llt_solve6(const double (&A)[6][6], const double (&b)[6], double (&x)[6]) {
+  double L[6][6];
+#pragma unroll
   for (int j = 0; j < 6; ++j) {
-    double s = A[j * 6 + j];
-    for (int k = 0; k < j; ++k) s -= L[j * 6 + k] * L[j * 6 + k];
+    double s = A[j][j];
+#pragma unroll
+    for (int k = 0; k < j; ++k) s -= L[j][k] * L[j][k];
     if (!(s > 0.0)) return false;
-    L[j * 6 + j] = sqrt(s);
+    L[j][j] = sqrt(s);
+#pragma unroll
     for (int i = j + 1; i < 6; ++i) {
-      double t = A[i * 6 + j];
-      for (int k = 0; k < j; ++k) t -= L[i * 6 + k] * L[j * 6 + k];
-      L[i * 6 + j] = t / L[j * 6 + j];
+      double t = A[i][j];
+#pragma unroll
+      for (int k = 0; k < j; ++k) t -= L[i][k] * L[j][k];
+      L[i][j] = t / L[j][j];
     }
   }
   double y[6];
+#pragma unroll
   for (int i = 0; i < 6; ++i) {
     double t = b[i];
-    for (int k = 0; k < i; ++k) t -= L[i * 6 + k] * y[k];
-    y[i] = t / L[i * 6 + i];
+#pragma unroll
+    for (int k = 0; k < i; ++k) t -= L[i][k] * y[k];
+    y[i] = t / L[i][i];
   }
+#pragma unroll
   for (int i = 5; i >= 0; --i) {
     double t = y[i];
-    for (int k = i + 1; k < 6; ++k) t -= L[k * 6 + i] * x[k];
-    x[i] = t / L[i * 6 + i];
+#pragma unroll
+    for (int k = i + 1; k < 6; ++k) t -= L[k][i] * x[k];
+    x[i] = t / L[i][i];
   }
   return true;
 }
 
 // Rz(g) Ry(b) Rx(a) (AngleAxis composition at NuiKinfuOpenCLDepthTracker.cpp:486)
-__device__ void euler_zyx(double a, double b, double g, double* R) {
-  double ca = cos(a), sa = sin(a), cb = cos(b), sb = sin(b), cg = cos(g), sg = sin(g);
-  double Rz[9] = {cg, -sg, 0, sg, cg, 0, 0, 0, 1};
-  double Ry[9] = {cb, 0, sb, 0, 1, 0, -sb, 0, cb};
-  double Rx[9] = {1, 0, 0, 0, ca, -sa, 0, sa, ca};
+__device__ __forceinline__ void euler_zyx(double a, double b, double g, double (&R)[9]) {
+  double ca, sa, cb, sb, cg, sg;
+  sincos(a, &sa, &ca);
+  sincos(b, &sb, &cb);
+  sincos(g, &sg, &cg);
+  const double Rz[9] = {cg, -sg, 0, sg, cg, 0, 0, 0, 1};
+  const double Ry[9] = {cb, 0, sb, 0, 1, 0, -sb, 0, cb};
+  const double Rx[9] = {1, 0, 0, 0, ca, -sa, 0, sa, ca};
   double T[9];
+#pragma unroll
   for (int i = 0; i < 3; ++i)
+#pragma unroll
     for (int j = 0; j < 3; ++j) {
       double s = 0;
+#pragma unroll
       for (int k = 0; k < 3; ++k) s += Rz[i * 3 + k] * Ry[k * 3 + j];
       T[i * 3 + j] = s;
     }
+#pragma unroll
   for (int i = 0; i < 3; ++i)
+#pragma unroll
     for (int j = 0; j < 3; ++j) {
       double s = 0;
+#pragma unroll
       for (int k = 0; k < 3; ++k) s += T[i * 3 + k] * Rx[k * 3 + j];
       R[i * 3 + j] = s;
     }
@@ -198,21 +237,23 @@ __device__ __noinline__ void icp_host_step(TrackState* ts, const double* sums, i
     ts->err_old = err;
     for (int k = 0; k < 27; ++k) ts->good[k] = sums[k];
   }
-  double A[36], b[6], Ac[36];
+  double A[6][6], b[6];
+#pragma unroll
   for (int i = 0, sh = 0; i < 6; ++i) {
+#pragma unroll
     for (int j = i; j < 7; ++j, ++sh) {
-      double v = ts->good[sh] / (double)cnt;
+      const double v = ts->good[sh] / (double)cnt;
       if (j == 6)
         b[i] = v;
       else
-        A[j * 6 + i] = A[i * 6 + j] = v;
+        A[j][i] = A[i][j] = v;
     }
-    A[i * 6 + i] *= (double)(1.0f + ts->lambda);
+    A[i][i] *= (double)(1.0f + ts->lambda);
   }
-  for (int i = 0; i < 36; ++i) Ac[i] = A[i];
-  const double det = det6(Ac);
+  // a singular system (|det| < 1e-15 or NaN) or a failed factorisation loses tracking; the
+  // solve runs first because the determinant's elimination overwrites A
   double x[6];
-  if (fabs(det) < 1e-15 || isnan(det) || !llt_solve6(A, b, x)) {
+  if (!llt_solve6(A, b, x) || !(fabs(det6(A)) >= 1e-15)) {
     ts->status = 3;
     return;
   }
@@ -223,20 +264,27 @@ __device__ __noinline__ void icp_host_step(TrackState* ts, const double* sums, i
   }
   double Ri[9];
   euler_zyx(al, be, ga, Ri);
-  double tn[3], Rn[9];
+  float t0[3], R0[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) t0[i] = ts->t[i];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) R0[i] = ts->R[i];
+#pragma unroll
   for (int i = 0; i < 3; ++i) {
     double s = 0;
-    for (int k = 0; k < 3; ++k) s += Ri[k * 3 + i] * (double)ts->t[k];
-    tn[i] = s + (double)(float)x[3 + i];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s += Ri[k * 3 + i] * (double)t0[k];
+    ts->t[i] = (float)(s + (double)(float)x[3 + i]);
   }
+#pragma unroll
   for (int i = 0; i < 3; ++i)
+#pragma unroll
     for (int j = 0; j < 3; ++j) {
       double s = 0;
-      for (int k = 0; k < 3; ++k) s += Ri[k * 3 + i] * (double)ts->R[k * 3 + j];
-      Rn[i * 3 + j] = s;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) s += Ri[k * 3 + i] * (double)R0[k * 3 + j];
+      ts->R[i * 3 + j] = (float)s;
     }
-  for (int i = 0; i < 3; ++i) ts->t[i] = (float)tn[i];
-  for (int i = 0; i < 9; ++i) ts->R[i] = (float)Rn[i];
 }
 
 template <int PPT>
@@ -365,6 +413,7 @@ __global__ void __launch_bounds__(kIcpThreads, 2) k_icp(const SessionDesc* __res
       const int k = lane;  // term index handled by this lane
       double acc = 0.0;
       if (k < kIcpTerms)
+#pragma unroll 4
         for (int b = b0 + warp; b < b1; b += kWarps) {
           float2 p = __ldcg(&s.partials[(size_t)b * kIcpTerms + k]);
           acc += (double)p.x + (double)p.y;

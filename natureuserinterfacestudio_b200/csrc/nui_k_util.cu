@@ -12,12 +12,13 @@ __global__ void k_publish(const SessionDesc* __restrict__ descs, int n, float* p
   const SessionDesc& s = descs[i];
   if (s.ts == nullptr) return;
   const TrackState* ts = s.ts;
-  status[2 * i] = s.kind < 0 ? 0 : ts->status;
-  status[2 * i + 1] = ts->integrate;
-  for (int k = 0; k < 9; ++k) pose[14 * i + k] = ts->xf.R[k];
-  for (int k = 0; k < 3; ++k) pose[14 * i + 9 + k] = ts->xf.t[k];
-  pose[14 * i + 12] = ts->error;
-  pose[14 * i + 13] = ts->count;
+  const int o = s.slot;
+  status[2 * o] = s.kind < 0 ? 0 : ts->status;
+  status[2 * o + 1] = ts->integrate;
+  for (int k = 0; k < 9; ++k) pose[14 * o + k] = ts->xf.R[k];
+  for (int k = 0; k < 3; ++k) pose[14 * o + 9 + k] = ts->xf.t[k];
+  pose[14 * o + 12] = ts->error;
+  pose[14 * o + 13] = ts->count;
 }
 
 // Start of a tick: clear the per-frame counters of every active session.

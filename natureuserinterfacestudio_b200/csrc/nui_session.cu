@@ -130,6 +130,10 @@ struct BatchPlan {
   int shiftFmtMask;         // bit per dense format of the shifting sessions
   int shiftColor;           // some shifting session has a colour volume
   int hashSwap;             // some hash session swaps blocks to the host
+  // descriptor ranges: a batch table lists its non-hash slots first, so the dense kernels
+  // launch over the first n - hashTail descriptors and the hash kernels over the last
+  // n - denseHead (0, 0: both families over the whole table)
+  int hashTail, denseHead;
   nui_tuning tune;          // the context's launch shapes
   BatchPlan() { std::memset(this, 0, sizeof(*this)); }
   bool operator<(const BatchPlan& o) const { return std::memcmp(this, &o, sizeof(BatchPlan)) < 0; }
@@ -438,6 +442,7 @@ void plan_merge(BatchPlan& a, const BatchPlan& b) {
 }
 
 unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
+unsigned dense_n(const BatchPlan& p) { return (unsigned)(p.n - p.hashTail); }
 
 // ICP partial-sum slots of a session (the block count at the smallest pixels per thread,
 // twice with the photometric blocks)
@@ -450,12 +455,12 @@ size_t icp_partial_bytes(const nui_session_cfg& c) {
 template <int F>
 void launch_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   if (!(p.fmtMask & (1 << F))) return;
-  k_integrate<F><<<dim3(cdiv(p.maxIntegThreads[F], 256), p.n), 256, 0, st>>>(d);
+  k_integrate<F><<<dim3(cdiv(p.maxIntegThreads[F], 256), dense_n(p)), 256, 0, st>>>(d);
 }
 template <int F>
 void launch_summary(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, int force) {
   if (!(p.fmtMask & (1 << F))) return;
-  k_brick_summary<F><<<dim3(cdiv(p.maxBricks[F], 1024), p.n), 256, 0, st>>>(d, force);
+  k_brick_summary<F><<<dim3(cdiv(p.maxBricks[F], 1024), dense_n(p)), 256, 0, st>>>(d, force);
 }
 // Brick re-classification after integration, then the super-bricks it touched.
 void launch_summaries(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, int force) {
@@ -463,7 +468,7 @@ void launch_summaries(const BatchPlan& p, const SessionDesc* d, cudaStream_t st,
   launch_summary<1>(p, d, st, force);
   launch_summary<2>(p, d, st, force);
   launch_summary<3>(p, d, st, force);
-  if (p.fmtMask) k_super_summary<<<dim3((unsigned)p.maxHyper, p.n), 64, 0, st>>>(d, force);
+  if (p.fmtMask) k_super_summary<<<dim3((unsigned)p.maxHyper, dense_n(p)), 64, 0, st>>>(d, force);
 }
 // Blocks of the raycasts: 2 x 2 warps, each a tw x (32 / tw) pixel tile.
 unsigned ray_blocks(const BatchPlan& p, int tw) { return cdiv(p.maxW, 2 * tw) * cdiv(p.maxH, 2 * (32 / tw)); }
@@ -471,54 +476,58 @@ template <int F>
 void launch_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   if (!(p.fmtMask & (1 << F))) return;
   const int tw = p.tune.raycast_tile_width;
-  k_raycast<F><<<dim3(ray_blocks(p, tw), p.n), 128, 0, st>>>(d, tw);
-  k_raycast_finish<F><<<dim3(cdiv((long)p.maxW * p.maxH, 256), p.n), 256, 0, st>>>(d);
+  k_raycast<F><<<dim3(ray_blocks(p, tw), dense_n(p)), 128, 0, st>>>(d, tw);
+  k_raycast_finish<F><<<dim3(cdiv((long)p.maxW * p.maxH, 256), dense_n(p)), 256, 0, st>>>(d);
 }
 
-void launch_hash_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
+void launch_hash_integrate(const BatchPlan& p, const SessionDesc* d0, cudaStream_t st) {
   if (!p.hashMask) return;
+  const SessionDesc* d = d0 + p.denseHead;
+  const unsigned hn = (unsigned)(p.n - p.denseHead);
   const unsigned nb = (unsigned)p.maxHashBlk;
-  k_hash_prepare<<<dim3(592, p.n), 256, 0, st>>>(d);
+  k_hash_prepare<<<dim3(592, hn), 256, 0, st>>>(d);
   const unsigned pix = cdiv((long)p.maxW * p.maxH, 256);
-  k_hash_walk<<<dim3(pix, p.n), 256, 0, st>>>(d, 0);
-  k_hash_walk<<<dim3(pix, p.n), 256, 0, st>>>(d, 1);
-  k_hash_count<<<dim3(nb, p.n), 256, 0, st>>>(d, 0);
-  k_hash_scan<<<p.n, 1024, 0, st>>>(d, 0);
-  k_hash_alloc<<<dim3(nb, p.n), 1024, 0, st>>>(d);
-  k_hash_alloc_done<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n);
-  k_hash_visible<<<dim3(592, p.n), 256, 0, st>>>(d);
-  k_hash_count<<<dim3(nb, p.n), 256, 0, st>>>(d, 1);
-  k_hash_scan<<<p.n, 1024, 0, st>>>(d, 1);
-  k_hash_compact<<<dim3(nb, p.n), 256, 0, st>>>(d);
+  k_hash_walk<<<dim3(pix, hn), 256, 0, st>>>(d, 0);
+  k_hash_walk<<<dim3(pix, hn), 256, 0, st>>>(d, 1);
+  k_hash_count<<<dim3(nb, hn), 256, 0, st>>>(d, 0);
+  k_hash_scan<<<hn, 1024, 0, st>>>(d, 0);
+  k_hash_alloc<<<dim3(nb, hn), 256, 0, st>>>(d);
+  k_hash_alloc_done<<<cdiv(hn, 64), 64, 0, st>>>(d, (int)hn);
+  k_hash_visible<<<dim3(592, hn), 256, 0, st>>>(d);
+  k_hash_count<<<dim3(nb, hn), 256, 0, st>>>(d, 1);
+  k_hash_scan<<<hn, 1024, 0, st>>>(d, 1);
+  k_hash_compact<<<dim3(nb, hn), 256, 0, st>>>(d);
   if (p.hashSwap) {  // global cache: re-allocations and the swap-in list
-    k_hash_count<<<dim3(nb, p.n), 256, 0, st>>>(d, 2);
-    k_hash_scan<<<p.n, 1024, 0, st>>>(d, 2);
-    k_hash_swap_lists<<<dim3(nb, p.n), 1024, 0, st>>>(d);
+    k_hash_count<<<dim3(nb, hn), 256, 0, st>>>(d, 2);
+    k_hash_scan<<<hn, 1024, 0, st>>>(d, 2);
+    k_hash_swap_lists<<<dim3(nb, hn), 1024, 0, st>>>(d);
   }
-  if (p.hashMask & 1) k_hash_integrate<0><<<dim3(1184, p.n), 512, 0, st>>>(d);
-  if (p.hashMask & 2) k_hash_integrate<1><<<dim3(1184, p.n), 512, 0, st>>>(d);
+  if (p.hashMask & 1) k_hash_integrate<0><<<dim3(1184, hn), 512, 0, st>>>(d);
+  if (p.hashMask & 2) k_hash_integrate<1><<<dim3(1184, hn), 512, 0, st>>>(d);
   if (p.hashSwap) {  // global cache: swap in, then swap out
-    if (p.hashMask & 1) k_hash_swap_in<0><<<dim3(1184, p.n), 512, 0, st>>>(d);
-    if (p.hashMask & 2) k_hash_swap_in<1><<<dim3(1184, p.n), 512, 0, st>>>(d);
-    k_hash_count<<<dim3(nb, p.n), 256, 0, st>>>(d, 3);
-    k_hash_scan<<<p.n, 1024, 0, st>>>(d, 3);
-    k_hash_swap_out_list<<<dim3(nb, p.n), 1024, 0, st>>>(d);
-    if (p.hashMask & 1) k_hash_swap_out<0><<<dim3(1184, p.n), 512, 0, st>>>(d);
-    if (p.hashMask & 2) k_hash_swap_out<1><<<dim3(1184, p.n), 512, 0, st>>>(d);
-    k_hash_swap_clean<<<p.n, 1024, 0, st>>>(d);
+    if (p.hashMask & 1) k_hash_swap_in<0><<<dim3(1184, hn), 512, 0, st>>>(d);
+    if (p.hashMask & 2) k_hash_swap_in<1><<<dim3(1184, hn), 512, 0, st>>>(d);
+    k_hash_count<<<dim3(nb, hn), 256, 0, st>>>(d, 3);
+    k_hash_scan<<<hn, 1024, 0, st>>>(d, 3);
+    k_hash_swap_out_list<<<dim3(nb, hn), 1024, 0, st>>>(d);
+    if (p.hashMask & 1) k_hash_swap_out<0><<<dim3(1184, hn), 512, 0, st>>>(d);
+    if (p.hashMask & 2) k_hash_swap_out<1><<<dim3(1184, hn), 512, 0, st>>>(d);
+    k_hash_swap_clean<<<hn, 1024, 0, st>>>(d);
   }
 }
-void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
+void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d0, cudaStream_t st) {
   if (!p.hashMask) return;
-  k_hash_range<<<dim3(296, p.n), 256, 0, st>>>(d);
-  k_hash_project<<<dim3(296, p.n), 256, 0, st>>>(d);
+  const SessionDesc* d = d0 + p.denseHead;
+  const unsigned hn = (unsigned)(p.n - p.denseHead);
+  k_hash_range<<<dim3(296, hn), 256, 0, st>>>(d);
+  k_hash_project<<<dim3(296, hn), 256, 0, st>>>(d);
   const int tw = p.tune.hash_raycast_tile_width;
   const unsigned tiles = ray_blocks(p, tw);
-  if (p.hashMask & 1) k_hash_raycast<0><<<dim3(tiles, p.n), 128, 0, st>>>(d, tw);
-  if (p.hashMask & 2) k_hash_raycast<1><<<dim3(tiles, p.n), 128, 0, st>>>(d, tw);
+  if (p.hashMask & 1) k_hash_raycast<0><<<dim3(tiles, hn), 128, 0, st>>>(d, tw);
+  if (p.hashMask & 2) k_hash_raycast<1><<<dim3(tiles, hn), 128, 0, st>>>(d, tw);
   const unsigned px = cdiv((long)p.maxW * p.maxH, 256);
-  if (p.hashMask & 1) k_hash_finish<0><<<dim3(px, p.n), 256, 0, st>>>(d);
-  if (p.hashMask & 2) k_hash_finish<1><<<dim3(px, p.n), 256, 0, st>>>(d);
+  if (p.hashMask & 1) k_hash_finish<0><<<dim3(px, hn), 256, 0, st>>>(d);
+  if (p.hashMask & 2) k_hash_finish<1><<<dim3(px, hn), 256, 0, st>>>(d);
 }
 
 // The shifts of the shifting volumes (after tracking, before integration): per axis, the
@@ -527,14 +536,14 @@ void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t 
 constexpr unsigned kShiftBlocks = 592;
 template <int F>
 void launch_shift_fetch(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, int axis) {
-  if (p.shiftFmtMask & (1 << F)) k_shift_fetch<F><<<dim3(kShiftBlocks, p.n), 256, 0, st>>>(d, axis);
+  if (p.shiftFmtMask & (1 << F)) k_shift_fetch<F><<<dim3(kShiftBlocks, dense_n(p)), 256, 0, st>>>(d, axis);
 }
 template <typename T>
 void launch_roll(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, int axis, int which) {
   if (axis == 0)
-    k_shift_roll_x<T><<<dim3(kShiftBlocks, p.n), 256, 0, st>>>(d, which);
+    k_shift_roll_x<T><<<dim3(kShiftBlocks, dense_n(p)), 256, 0, st>>>(d, which);
   else
-    k_shift_roll_yz<T><<<dim3(kShiftBlocks, p.n), 256, 0, st>>>(d, axis, which);
+    k_shift_roll_yz<T><<<dim3(kShiftBlocks, dense_n(p)), 256, 0, st>>>(d, axis, which);
 }
 void launch_shift(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   if (!p.shiftFmtMask) return;
@@ -551,7 +560,7 @@ void launch_shift(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
     }
     if (p.shiftColor) launch_roll<uint32_t>(p, d, st, axis, 2);
   }
-  k_shift_dirty<<<dim3(kShiftBlocks, p.n), 256, 0, st>>>(d);
+  k_shift_dirty<<<dim3(kShiftBlocks, dense_n(p)), 256, 0, st>>>(d);
 }
 
 // Colour pyramid (if any session tracks with colour), the ICP iterations of every level,
@@ -670,17 +679,30 @@ nui_status tick_launch(nui_ctx* ctx, nui_session* const* ss, int n, const uint16
   if (st != NUI_OK) return st;
   BatchPlan p;
   p.n = n;
-  for (int i = 0; i < n; ++i) {
+  // the table lists the non-hash slots first (empty ones included), then the hash sessions,
+  // each group in slot order; a descriptor's slot is its row of the outputs
+  int nhash = 0;
+  for (int i = 0; i < n; ++i) nhash += ss[i] && ss[i]->hash;
+  for (int i = 0, jd = 0, jh = n - nhash; i < n; ++i) {
     nui_session* s = ss[i];
+    SessionDesc& dd = ctx->h_descs[s && s->hash ? jh++ : jd++];
     if (!s) {
-      std::memset(&ctx->h_descs[i], 0, sizeof(SessionDesc));
-      ctx->h_descs[i].kind = kInactive;
-      ctx->h_descs[i].fmt = -1;
+      std::memset(&dd, 0, sizeof(SessionDesc));
+      dd.kind = kInactive;
+      dd.fmt = -1;
+      dd.slot = i;
       continue;
     }
     plan_add(p, s);
     int kind = !raws[i] ? kInactive : s->frames == 0 ? kFirstFrame : kTrackFrame;
-    fill_desc(s, ctx->h_descs[i], kind, raws[i], bgras ? bgras[i] : nullptr);
+    fill_desc(s, dd, kind, raws[i], bgras ? bgras[i] : nullptr);
+    dd.slot = i;
+  }
+  // a served batch keeps one launch shape (and graph) while sessions come and go: both
+  // families then launch over the whole table
+  if (!floor) {
+    p.hashTail = nhash;
+    p.denseHead = n - nhash;
   }
   if (floor) plan_merge(p, *floor);
   p.tune = ctx->tune;

@@ -14,7 +14,7 @@ import pytest
 from natureuserinterfacestudio_b200 import _lib as L
 from oracle import oracle as O
 
-from _util import cfg_for, frames, oracle_preprocess, rot_angle, same_bits
+from _util import cfg_for, cfg_hash, frames, oracle_preprocess, rot_angle, same_bits
 
 pytestmark = pytest.mark.gpu
 
@@ -189,6 +189,30 @@ def test_batched_equals_alone(gpu_ctx):
             assert np.array_equal(poses[k], alone[k][0][i]), (i, k)
     for k in range(3):
         assert np.array_equal(ss[k].volume_ref_layout(), alone[k][1])
+
+
+def test_mixed_batch_in_any_order_equals_alone(gpu_ctx):
+    """Hash and dense sessions interleaved in a batch (the batch table lists the dense ones
+    first, each kernel family launches over its own range, results go back to the caller's
+    slots): every session's poses and reference maps equal its run alone, bit for bit."""
+    seqs = [frames(4, W=320, H=240, seed=s) for s in (3, 8, 12, 5)]
+    cfgs = [cfg_hash(), cfg_for(W=320, H=240, res=(96, 96, 96), fmt=L.TSDF_F16_U8), cfg_hash(fmt=L.TSDF_F16_U8),
+            cfg_for(W=320, H=240, res=(128, 128, 128))]
+    alone = []
+    for cfg, sq in zip(cfgs, seqs):
+        s = L.Session(gpu_ctx, cfg)
+        poses = [s.process(d)[1] for d, _, _, _ in sq]
+        alone.append((poses, s.download(3), s.download(4)))
+        s.close()
+    ss = [L.Session(gpu_ctx, c) for c in cfgs]
+    for i in range(4):
+        st, poses = gpu_ctx.batch_tick(ss, [sq[i][0] for sq in seqs])
+        assert np.all(st == 0)
+        for k in range(4):
+            assert np.array_equal(poses[k], alone[k][0][i]), (i, k)
+    for k in range(4):
+        assert same_bits(ss[k].download(3), alone[k][1]) and same_bits(ss[k].download(4), alone[k][2]), k
+        ss[k].close()
 
 
 def _volume_after(seq, cfg, n):
