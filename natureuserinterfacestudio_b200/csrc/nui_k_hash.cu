@@ -496,11 +496,16 @@ __global__ void __launch_bounds__(512) k_hash_integrate(const SessionDesc* __res
   const int lid = threadIdx.x;
   const int lx = (lid % 64) % 8, ly = (lid % 64) / 8, lz = lid / 64;
   unsigned touched = 0;
+  // the next block's list entry is loaded a block ahead, and a voxel's sdf with its weight
+  // (before the tests that may skip it), so that fewer loads wait on one another
+  int vid = blockIdx.x < (unsigned)nvis ? s.vis_ids[blockIdx.x] : 0;
   for (int k = blockIdx.x; k < nvis; k += gridDim.x) {
-    const HEntry en = load_entry(s.entries, (unsigned)s.vis_ids[k]);
+    const HEntry en = load_entry(s.entries, (unsigned)vid);
+    vid = k + (int)gridDim.x < nvis ? s.vis_ids[k + gridDim.x] : 0;
     if (en.ptr < 0) continue;
     const unsigned bid = (unsigned)en.ptr * 512u + (unsigned)lid;
     const int w = s.hw[bid];
+    const float oldF = HVox<HF>::load(s.hsdf, bid);
     if (s.max_w == w) continue;
     const float3 pm = mul3(f3((float)(en.pos[0] * 8 + lx), (float)(en.pos[1] * 8 + ly), (float)(en.pos[2] * 8 + lz)),
                            s.voxel);
@@ -514,7 +519,7 @@ __global__ void __launch_bounds__(512) k_hash_integrate(const SessionDesc* __res
     const float eta = d - pc.z;
     const float sdf = eta / s.mu;
     if (eta < -s.mu) continue;
-    const float oldF = HVox<HF>::load(s.hsdf, bid), oldW = (float)w;
+    const float oldW = (float)w;
     float newF = fminf(1.0f, sdf);
     const float newW = 1.0f, cw = oldW + newW;
     if (s.bgra && s.hrgb && eta < s.mu && fabsf(sdf) < 0.25f) {
