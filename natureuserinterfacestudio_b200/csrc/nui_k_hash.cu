@@ -8,11 +8,11 @@
 //                       entry slot, the largest (pixel, step) key that wanted it
 //   k_hash_walk(1)      the walk again: the key owner writes its block coordinates (the
 //                       block the last writer in raster order would have left)
-//   k_hash_count(0) + k_hash_scan + k_hash_alloc
+//   k_hash_flag_count(0) + k_hash_scan + k_hash_alloc
 //                       entries needing allocation, ranked in index order, pop blocks from
 //                       the free stack (and excess slots for chain appends) in that order
 //   k_hash_visible      previously visible entries (type 3): 8-corner frustum test
-//   k_hash_count(1) + k_hash_scan + k_hash_compact
+//   k_hash_flag_count(1) + k_hash_scan + k_hash_compact
 //                       visible list = entries with visible type > 0 in index order
 //   k_hash_integrate    one 512-thread block per visible entry, one voxel per thread
 //   k_hash_range + k_hash_project + k_hash_raycast
@@ -69,25 +69,54 @@ __device__ __forceinline__ float3 depth_to_point(const DevCam& c, int ux, int uy
 __device__ __forceinline__ bool hash_active(const SessionDesc& s) { return s.hash && s.kind >= 0 && s.ts->integrate; }
 
 // ------------------------------------------------------------------ allocation
-// The per-entry byte flags (alloc_type, vis, swap) are scanned four at a time: the four
-// bytes from entry i (a multiple of 4) in one 32-bit word when all lie below n, else byte
-// by byte (bytes at or past n read as 0).
-__device__ __forceinline__ unsigned load4(const uint8_t* p, unsigned i, unsigned n) {
-  if (i + 4 <= n) return *reinterpret_cast<const unsigned*>(p + i);
-  unsigned w = 0;
-  for (unsigned k = 0; k < 4 && i + k < n; ++k) w |= (unsigned)p[i + k] << (8 * k);
-  return w;
+// The per-entry byte flags (alloc_type, vis) are scanned sixteen at a time: the bytes from
+// entry i (a multiple of 16) in one 16-byte load when all lie below n, else byte by byte
+// (bytes at or past n read as 0).  A 1024-entry scan block is 64 threads.
+__device__ __forceinline__ uint4 load16(const uint8_t* p, unsigned i, unsigned n) {
+  if (i + 16 <= n) return *reinterpret_cast<const uint4*>(p + i);
+  unsigned w[4] = {0u, 0u, 0u, 0u};
+  for (unsigned k = 0; k < 16 && i + k < n; ++k) w[k >> 2] |= (unsigned)p[i + k] << (8 * (k & 3));
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+// 0xff in every byte of w equal to / different from the matching byte of v
+__device__ __forceinline__ uint4 eq16(uint4 w, unsigned v) {
+  return make_uint4(__vcmpeq4(w.x, v), __vcmpeq4(w.y, v), __vcmpeq4(w.z, v), __vcmpeq4(w.w, v));
+}
+__device__ __forceinline__ uint4 ne16(uint4 w, unsigned v) {
+  return make_uint4(__vcmpne4(w.x, v), __vcmpne4(w.y, v), __vcmpne4(w.z, v), __vcmpne4(w.w, v));
+}
+__device__ __forceinline__ unsigned count16(uint4 m) {
+  return (__popc(m.x) + __popc(m.y) + __popc(m.z) + __popc(m.w)) >> 3;
+}
+__device__ __forceinline__ bool bit16(uint4 m, int k) {
+  const unsigned w = k < 4 ? m.x : k < 8 ? m.y : k < 12 ? m.z : m.w;
+  return (w >> (8 * (k & 3))) & 1u;
+}
+// Exclusive prefix of c over the 64 threads of a scan block, in thread order.
+__device__ __forceinline__ unsigned scan64(unsigned c) {
+  const int lane = threadIdx.x & 31;
+  unsigned incl = c;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const unsigned o = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += o;
+  }
+  __shared__ unsigned w0;
+  if (threadIdx.x == 31) w0 = incl;
+  __syncthreads();
+  return incl - c + (threadIdx.x >= 32 ? w0 : 0u);
 }
 
 __global__ void k_hash_prepare(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (!hash_active(s)) return;
   const unsigned n = (unsigned)(s.nb + s.ne);
-  for (unsigned i = 4 * (blockIdx.x * blockDim.x + threadIdx.x); i < n; i += 4 * gridDim.x * blockDim.x) {
-    if (i + 4 <= n) {
-      reinterpret_cast<unsigned*>(s.alloc_type)[i >> 2] = 0u;
-      unsigned* v = reinterpret_cast<unsigned*>(s.vis) + (i >> 2);
-      *v = __vcmpne4(*v, 0u) & 0x03030303u;  // visible (any type) -> 3, else 0
+  for (unsigned i = 16 * (blockIdx.x * blockDim.x + threadIdx.x); i < n; i += 16 * gridDim.x * blockDim.x) {
+    if (i + 16 <= n) {
+      reinterpret_cast<uint4*>(s.alloc_type)[i >> 4] = make_uint4(0u, 0u, 0u, 0u);
+      uint4* v = reinterpret_cast<uint4*>(s.vis) + (i >> 4);
+      const uint4 m = ne16(*v, 0u);  // visible (any type) -> 3, else 0
+      *v = make_uint4(m.x & 0x03030303u, m.y & 0x03030303u, m.z & 0x03030303u, m.w & 0x03030303u);
     } else {
       for (unsigned k = i; k < n; ++k) {
         s.alloc_type[k] = 0;
@@ -167,25 +196,45 @@ __device__ __forceinline__ bool swap_out_flag(const SessionDesc& s, unsigned i) 
 }
 
 // Per 1024 entries: number of entries needing a block (type >= 1) and an excess slot
-// (type 2) (which == 0); of visible entries (which == 1); with the global cache, of
-// visible entries whose block was swapped out and of entries to swap in (which == 2), of
-// entries to swap out (which == 3).
+// (type 2) (which == 0); of visible entries (which == 1).  One 64-thread block per 1024
+// entries, sixteen a thread.
+__global__ void __launch_bounds__(64) k_hash_flag_count(const SessionDesc* __restrict__ descs, int which) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!hash_active(s)) return;
+  const unsigned n = (unsigned)(s.nb + s.ne);
+  const unsigned b0 = blockIdx.x * kHashScanBlock;
+  if (b0 >= n) return;
+  const unsigned i = b0 + 16 * threadIdx.x;
+  unsigned a = 0, e = 0;
+  if (i < n) {
+    const uint4 w = load16(which == 0 ? s.alloc_type : s.vis, i, n);
+    a = count16(ne16(w, 0u));
+    if (which == 0) e = count16(eq16(w, 0x02020202u));
+  }
+  a = __reduce_add_sync(0xffffffffu, a);
+  e = __reduce_add_sync(0xffffffffu, e);
+  __shared__ unsigned sa, se;
+  if (threadIdx.x == 32) {
+    sa = a;
+    se = e;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s.blk[4 * blockIdx.x] = a + sa;
+    s.blk[4 * blockIdx.x + 1] = e + se;
+  }
+}
+
+// With the global cache, per 1024 entries: number of visible entries whose block was
+// swapped out and of entries to swap in (which == 2), of entries to swap out (which == 3).
 __global__ void __launch_bounds__(256) k_hash_count(const SessionDesc* __restrict__ descs, int which) {
   const SessionDesc& s = descs[blockIdx.y];
-  if (!hash_active(s) || (which >= 2 && !s.swapping)) return;
+  if (!hash_active(s) || !s.swapping) return;
   const unsigned n = (unsigned)(s.nb + s.ne);
   const unsigned b0 = blockIdx.x * kHashScanBlock;
   if (b0 >= n) return;
   unsigned a = 0, e = 0;
-  if (which <= 1) {  // four flags a thread (256 threads: the 1024 entries)
-    const unsigned i = b0 + 4 * threadIdx.x;
-    if (i < n) {
-      const unsigned w = load4(which == 0 ? s.alloc_type : s.vis, i, n);
-      a = __popc(__vcmpne4(w, 0u)) >> 3;  // each set byte of the mask holds 8 bits
-      if (which == 0) e = __popc(__vcmpeq4(w, 0x02020202u)) >> 3;
-    }
-  }
-  for (unsigned i = b0 + threadIdx.x; which >= 2 && i < min(n, b0 + kHashScanBlock); i += blockDim.x) {
+  for (unsigned i = b0 + threadIdx.x; i < min(n, b0 + kHashScanBlock); i += blockDim.x) {
     if (which == 2) {  // re-allocations, swap-ins
       a += s.vis[i] > 0 && entry_ptr(s, i) == -1;
       e += s.swap[i] == 1;
@@ -337,36 +386,25 @@ __device__ __forceinline__ void alloc_one(const SessionDesc& s, unsigned i, int 
   }
 }
 
-__global__ void __launch_bounds__(256) k_hash_alloc(const SessionDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(64) k_hash_alloc(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (!hash_active(s)) return;
   const unsigned n = (unsigned)(s.nb + s.ne);
   const unsigned b = blockIdx.x;
   if (b * kHashScanBlock >= n) return;
-  if (s.blk[4 * b] == 0) return;  // no request among the block's entries (k_hash_count)
-  const unsigned i = b * kHashScanBlock + 4 * threadIdx.x;
-  const unsigned w = i < n ? load4(s.alloc_type, i, n) : 0u;
-  const unsigned ma = __vcmpne4(w, 0u), me = __vcmpeq4(w, 0x02020202u);
-  const unsigned c = (__popc(ma) >> 3) | ((__popc(me) >> 3) << 16);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  unsigned incl = c;
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const unsigned o = __shfl_up_sync(0xffffffffu, incl, off);
-    if (lane >= off) incl += o;
-  }
-  __shared__ unsigned wsum[8];
-  if (lane == 31) wsum[warp] = incl;
-  __syncthreads();
-  unsigned before = incl - c;
-  for (int q = 0; q < warp; ++q) before += wsum[q];
-  if (!ma) return;
+  if (s.blk[4 * b] == 0) return;  // no request among the block's entries (k_hash_flag_count)
+  const unsigned i = b * kHashScanBlock + 16 * threadIdx.x;
+  const uint4 w = i < n ? load16(s.alloc_type, i, n) : make_uint4(0u, 0u, 0u, 0u);
+  const uint4 ma = ne16(w, 0u), me = eq16(w, 0x02020202u);
+  const unsigned c = count16(ma) | (count16(me) << 16);
+  const unsigned before = scan64(c);
+  if (!count16(ma)) return;
   const int last_block = s.hcount[0], last_excess = s.hcount[1];
   unsigned ra = s.blk[4 * b + 2] + (before & 0xffffu), re = s.blk[4 * b + 3] + (before >> 16);
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (!((ma >> (8 * k)) & 1u)) continue;
-    const bool ex = (me >> (8 * k)) & 1u;
+  for (int k = 0; k < 16; ++k) {
+    if (!bit16(ma, k)) continue;
+    const bool ex = bit16(me, k);
     alloc_one(s, i + k, last_block - (int)ra, ex ? last_excess - (int)re : 0);
     ++ra;
     if (ex) ++re;
@@ -413,55 +451,46 @@ __global__ void k_hash_visible(const SessionDesc* __restrict__ descs) {
     }
     return;
   }
-  for (unsigned i4 = 4 * (blockIdx.x * blockDim.x + threadIdx.x); i4 < n; i4 += 4 * gridDim.x * blockDim.x) {
-    unsigned m3 = __vcmpeq4(load4(s.vis, i4, n), 0x03030303u);  // entries visible at the last frame
-    while (m3) {
-      const int k = (__ffs(m3) - 1) >> 3;
-      m3 &= ~(0xFFu << (8 * k));
-      const unsigned i = i4 + (unsigned)k;
-      const HEntry en = load_entry(s.entries, i);
-      float3 p = f3((float)en.pos[0] * factor, (float)en.pos[1] * factor, (float)en.pos[2] * factor);
-      bool v = point_visible(s, m, p);
-      if (!v) { p.z += factor; v = point_visible(s, m, p); }
-      if (!v) { p.y += factor; v = point_visible(s, m, p); }
-      if (!v) { p.x += factor; v = point_visible(s, m, p); }
-      if (!v) { p.z -= factor; v = point_visible(s, m, p); }
-      if (!v) { p.y -= factor; v = point_visible(s, m, p); }
-      if (!v) { p.x -= factor; p.y += factor; v = point_visible(s, m, p); }
-      if (!v) { p.x += factor; p.y -= factor; p.z += factor; v = point_visible(s, m, p); }
-      if (!v) s.vis[i] = 0;
+  for (unsigned i16 = 16 * (blockIdx.x * blockDim.x + threadIdx.x); i16 < n; i16 += 16 * gridDim.x * blockDim.x) {
+    const uint4 m16 = eq16(load16(s.vis, i16, n), 0x03030303u);  // entries visible at the last frame
+    for (int q = 0; q < 4; ++q) {
+      unsigned m3 = q == 0 ? m16.x : q == 1 ? m16.y : q == 2 ? m16.z : m16.w;
+      while (m3) {
+        const int k = (__ffs(m3) - 1) >> 3;
+        m3 &= ~(0xFFu << (8 * k));
+        const unsigned i = i16 + 4 * q + (unsigned)k;
+        const HEntry en = load_entry(s.entries, i);
+        float3 p = f3((float)en.pos[0] * factor, (float)en.pos[1] * factor, (float)en.pos[2] * factor);
+        bool v = point_visible(s, m, p);
+        if (!v) { p.z += factor; v = point_visible(s, m, p); }
+        if (!v) { p.y += factor; v = point_visible(s, m, p); }
+        if (!v) { p.x += factor; v = point_visible(s, m, p); }
+        if (!v) { p.z -= factor; v = point_visible(s, m, p); }
+        if (!v) { p.y -= factor; v = point_visible(s, m, p); }
+        if (!v) { p.x -= factor; p.y += factor; v = point_visible(s, m, p); }
+        if (!v) { p.x += factor; p.y -= factor; p.z += factor; v = point_visible(s, m, p); }
+        if (!v) s.vis[i] = 0;
+      }
     }
   }
 }
 
-// The visible list in index order: 256 threads a 1024-entry block, four entries each; a
-// thread's rank is the block offset (k_hash_scan) plus the visible entries of the threads
-// before it.
-__global__ void __launch_bounds__(256) k_hash_compact(const SessionDesc* __restrict__ descs) {
+// The visible list in index order: a 64-thread block per 1024 entries, sixteen a thread;
+// a thread's rank is the block offset (k_hash_scan) plus the visible entries of the
+// threads before it.
+__global__ void __launch_bounds__(64) k_hash_compact(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (!hash_active(s)) return;
   const unsigned n = (unsigned)(s.nb + s.ne);
   const unsigned b = blockIdx.x;
   if (b * kHashScanBlock >= n) return;
   if (s.blk[4 * b] == 0) return;  // no visible entry in the block
-  const unsigned i = b * kHashScanBlock + 4 * threadIdx.x;
-  const unsigned m = i < n ? __vcmpne4(load4(s.vis, i, n), 0u) : 0u;
-  const unsigned c = __popc(m) >> 3;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  unsigned incl = c;
+  const unsigned i = b * kHashScanBlock + 16 * threadIdx.x;
+  const uint4 m = i < n ? ne16(load16(s.vis, i, n), 0u) : make_uint4(0u, 0u, 0u, 0u);
+  unsigned r = s.blk[4 * b + 2] + scan64(count16(m));
 #pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const unsigned o = __shfl_up_sync(0xffffffffu, incl, off);
-    if (lane >= off) incl += o;
-  }
-  __shared__ unsigned wsum[8];
-  if (lane == 31) wsum[warp] = incl;
-  __syncthreads();
-  unsigned r = s.blk[4 * b + 2] + incl - c;
-  for (int w = 0; w < warp; ++w) r += wsum[w];
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-    if ((m >> (8 * k)) & 1u) s.vis_ids[r++] = (int)(i + k);
+  for (int k = 0; k < 16; ++k)
+    if (bit16(m, k)) s.vis_ids[r++] = (int)(i + k);
 }
 
 // ------------------------------------------------------------------ integration

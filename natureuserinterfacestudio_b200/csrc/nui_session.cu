@@ -54,6 +54,7 @@ __global__ void k_occ_clear(const SessionDesc*);
 __global__ void k_hash_prepare(const SessionDesc*);
 __global__ void k_hash_walk(const SessionDesc*, int);
 __global__ void k_hash_count(const SessionDesc*, int);
+__global__ void k_hash_flag_count(const SessionDesc*, int);
 __global__ void k_hash_scan(const SessionDesc*, int);
 __global__ void k_hash_alloc(const SessionDesc*);
 __global__ void k_hash_alloc_done(const SessionDesc*, int);
@@ -489,14 +490,14 @@ void launch_hash_integrate(const BatchPlan& p, const SessionDesc* d0, cudaStream
   const unsigned pix = cdiv((long)p.maxW * p.maxH, 256);
   k_hash_walk<<<dim3(pix, hn), 256, 0, st>>>(d, 0);
   k_hash_walk<<<dim3(pix, hn), 256, 0, st>>>(d, 1);
-  k_hash_count<<<dim3(nb, hn), 256, 0, st>>>(d, 0);
+  k_hash_flag_count<<<dim3(nb, hn), 64, 0, st>>>(d, 0);
   k_hash_scan<<<hn, 1024, 0, st>>>(d, 0);
-  k_hash_alloc<<<dim3(nb, hn), 256, 0, st>>>(d);
+  k_hash_alloc<<<dim3(nb, hn), 64, 0, st>>>(d);
   k_hash_alloc_done<<<cdiv(hn, 64), 64, 0, st>>>(d, (int)hn);
   k_hash_visible<<<dim3(592, hn), 256, 0, st>>>(d);
-  k_hash_count<<<dim3(nb, hn), 256, 0, st>>>(d, 1);
+  k_hash_flag_count<<<dim3(nb, hn), 64, 0, st>>>(d, 1);
   k_hash_scan<<<hn, 1024, 0, st>>>(d, 1);
-  k_hash_compact<<<dim3(nb, hn), 256, 0, st>>>(d);
+  k_hash_compact<<<dim3(nb, hn), 64, 0, st>>>(d);
   if (p.hashSwap) {  // global cache: re-allocations and the swap-in list
     k_hash_count<<<dim3(nb, hn), 256, 0, st>>>(d, 2);
     k_hash_scan<<<hn, 1024, 0, st>>>(d, 2);
