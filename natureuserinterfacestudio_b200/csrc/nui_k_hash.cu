@@ -515,9 +515,49 @@ struct HVox<1> {  // half sdf
   }
 };
 
+// One voxel of integrateIntoScene_kernel, given its entry, weight w and sdf oldF.
+template <int HF>
+__device__ __forceinline__ void integrate_voxel(const SessionDesc& s, const DevXform& m, const HEntry& en, int w,
+                                                float oldF, int lid, int lx, int ly, int lz, unsigned& touched) {
+  if (en.ptr < 0) return;
+  const unsigned bid = (unsigned)en.ptr * 512u + (unsigned)lid;
+  if (s.max_w == w) return;
+  const float3 pm = mul3(f3((float)(en.pos[0] * 8 + lx), (float)(en.pos[1] * 8 + ly), (float)(en.pos[2] * 8 + lz)),
+                         s.voxel);
+  const float3 pc = xf_inverse(m, pm);
+  if (pc.z <= 0) return;
+  const int ix = (int)(pc.x * s.cam.fx / pc.z + s.cam.cx + 0.5f), iy = (int)(pc.y * s.cam.fy / pc.z + s.cam.cy + 0.5f);
+  if (ix < 0 || ix >= s.W || iy < 0 || iy >= s.H) return;
+  const int sid = iy * s.W + ix;
+  const float d = pass_depth(s, sid);
+  if (isnan(d)) return;
+  const float eta = d - pc.z;
+  const float sdf = eta / s.mu;
+  if (eta < -s.mu) return;
+  const float oldW = (float)w;
+  float newF = fminf(1.0f, sdf);
+  const float newW = 1.0f, cw = oldW + newW;
+  if (s.bgra && s.hrgb && eta < s.mu && fabsf(sdf) < 0.25f) {
+    const uchar4 col = reinterpret_cast<const uchar4*>(s.bgra)[sid];
+    if (col.w == 255) {
+      const uchar4 vc = s.hrgb[bid];
+      const float r = (oldW * (float)vc.x + newW * (float)col.z) / cw;
+      const float g = (oldW * (float)vc.y + newW * (float)col.y) / cw;
+      const float bl = (oldW * (float)vc.z + newW * (float)col.x) / cw;
+      s.hrgb[bid] = make_uchar4((unsigned char)fminf(fmaxf(r, 0.f), 255.f), (unsigned char)fminf(fmaxf(g, 0.f), 255.f),
+                                (unsigned char)fminf(fmaxf(bl, 0.f), 255.f), 0);
+    }
+  }
+  newF = oldW * oldF + newW * newF;
+  newF /= cw;
+  HVox<HF>::store(s.hsdf, bid, newF);
+  s.hw[bid] = (uint8_t)min((int)(uint8_t)cw, s.max_w);
+  ++touched;
+}
+
 // integrateIntoScene_kernel (KinfuHashScene.cl:387-470); blocks stride over the list.
 template <int HF>
-__global__ void __launch_bounds__(512) k_hash_integrate(const SessionDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(512, 3) k_hash_integrate(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (!hash_active(s) || s.hfmt != HF) return;
   const int nvis = s.hcount[2];
@@ -525,48 +565,34 @@ __global__ void __launch_bounds__(512) k_hash_integrate(const SessionDesc* __res
   const int lid = threadIdx.x;
   const int lx = (lid % 64) % 8, ly = (lid % 64) / 8, lz = lid / 64;
   unsigned touched = 0;
-  // the next block's list entry is loaded a block ahead, and a voxel's sdf with its weight
-  // (before the tests that may skip it), so that fewer loads wait on one another
-  int vid = blockIdx.x < (unsigned)nvis ? s.vis_ids[blockIdx.x] : 0;
-  for (int k = blockIdx.x; k < nvis; k += gridDim.x) {
-    const HEntry en = load_entry(s.entries, (unsigned)vid);
-    vid = k + (int)gridDim.x < nvis ? s.vis_ids[k + gridDim.x] : 0;
-    if (en.ptr < 0) continue;
-    const unsigned bid = (unsigned)en.ptr * 512u + (unsigned)lid;
-    const int w = s.hw[bid];
-    const float oldF = HVox<HF>::load(s.hsdf, bid);
-    if (s.max_w == w) continue;
-    const float3 pm = mul3(f3((float)(en.pos[0] * 8 + lx), (float)(en.pos[1] * 8 + ly), (float)(en.pos[2] * 8 + lz)),
-                           s.voxel);
-    const float3 pc = xf_inverse(m, pm);
-    if (pc.z <= 0) continue;
-    const int ix = (int)(pc.x * s.cam.fx / pc.z + s.cam.cx + 0.5f), iy = (int)(pc.y * s.cam.fy / pc.z + s.cam.cy + 0.5f);
-    if (ix < 0 || ix >= s.W || iy < 0 || iy >= s.H) continue;
-    const int sid = iy * s.W + ix;
-    const float d = pass_depth(s, sid);
-    if (isnan(d)) continue;
-    const float eta = d - pc.z;
-    const float sdf = eta / s.mu;
-    if (eta < -s.mu) continue;
-    const float oldW = (float)w;
-    float newF = fminf(1.0f, sdf);
-    const float newW = 1.0f, cw = oldW + newW;
-    if (s.bgra && s.hrgb && eta < s.mu && fabsf(sdf) < 0.25f) {
-      const uchar4 col = reinterpret_cast<const uchar4*>(s.bgra)[sid];
-      if (col.w == 255) {
-        const uchar4 vc = s.hrgb[bid];
-        const float r = (oldW * (float)vc.x + newW * (float)col.z) / cw;
-        const float g = (oldW * (float)vc.y + newW * (float)col.y) / cw;
-        const float bl = (oldW * (float)vc.z + newW * (float)col.x) / cw;
-        s.hrgb[bid] = make_uchar4((unsigned char)fminf(fmaxf(r, 0.f), 255.f), (unsigned char)fminf(fmaxf(g, 0.f), 255.f),
-                                  (unsigned char)fminf(fmaxf(bl, 0.f), 255.f), 0);
-      }
+  // Software pipeline over the block's list positions k, k + g, k + 2g, ...: while position
+  // k is integrated, the voxel (weight and sdf) of k + g and the hash entry of k + 2g are
+  // already in flight, so only the depth read waits inside an iteration.
+  const int g = (int)gridDim.x, k0 = (int)blockIdx.x;
+  auto entry_at = [&](int k) {
+    HEntry e;
+    e.ptr = -1;
+    if (k < nvis) e = load_entry(s.entries, (unsigned)s.vis_ids[k]);
+    return e;
+  };
+  HEntry en = entry_at(k0), en1 = entry_at(k0 + g);
+  int w = 0;
+  float oldF = 0.f;
+  if (en.ptr >= 0) {
+    w = s.hw[(unsigned)en.ptr * 512u + (unsigned)lid];
+    oldF = HVox<HF>::load(s.hsdf, (unsigned)en.ptr * 512u + (unsigned)lid);
+  }
+  for (int k = k0; k < nvis; k += g) {
+    const HEntry cur = en;
+    const int cw0 = w;
+    const float cF = oldF;
+    en = en1;
+    en1 = entry_at(k + 2 * g);
+    if (en.ptr >= 0) {
+      w = s.hw[(unsigned)en.ptr * 512u + (unsigned)lid];
+      oldF = HVox<HF>::load(s.hsdf, (unsigned)en.ptr * 512u + (unsigned)lid);
     }
-    newF = oldW * oldF + newW * newF;
-    newF /= cw;
-    HVox<HF>::store(s.hsdf, bid, newF);
-    s.hw[bid] = (uint8_t)min((int)(uint8_t)cw, s.max_w);
-    ++touched;
+    integrate_voxel<HF>(s, m, cur, cw0, cF, lid, lx, ly, lz, touched);
   }
   const unsigned t = __reduce_add_sync(0xffffffffu, touched);
   if ((threadIdx.x & 31) == 0 && t) atomicAdd(&s.ts->touched, (unsigned long long)t);
