@@ -300,7 +300,7 @@ NUI_API nui_status nui_ctx_last_tick_kernels(nui_ctx* ctx, int* n);
  *   integrate_threads_log2   dense integration: each volume column is split into z chunks,
  *                            one thread each, until a session's launch has >= 2^this
  *                            threads (chunks of >= 16 slices); 14..22, default 18
- *   icp_pixels_per_thread    ICP block: 256 threads x this many pixels; 2, 4 or 8 (4)
+ *   icp_pixels_per_thread    ICP block: 256 threads x this many pixels; 2, 4, 8 or 16 (4)
  *   raycast_tile_width       dense raycast: a warp shades a tile this wide and 32 / this
  *                            high, a block 2 x 2 such tiles; 4, 8, 16 or 32 (8)
  *   hash_raycast_tile_width  the same for the voxel-hash raycast (8)

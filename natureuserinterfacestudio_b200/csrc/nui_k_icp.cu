@@ -441,6 +441,7 @@ __global__ void __launch_bounds__(kIcpThreads, 2) k_icp(const SessionDesc* __res
 template __global__ void k_icp<2>(const SessionDesc*, int, int);
 template __global__ void k_icp<4>(const SessionDesc*, int, int);
 template __global__ void k_icp<8>(const SessionDesc*, int, int);
+template __global__ void k_icp<16>(const SessionDesc*, int, int);
 
 // After the last ICP launch (or on frame 0): publish the pose, decide the integration
 // gate (NuiKinfuTrackingEngine.cpp:115-127) and reset the estimate for the next frame.

@@ -577,6 +577,7 @@ void launch_track(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, flo
     for (int it = 0; it < p.maxIters[l]; ++it) {
       if (ppt == 2) k_icp<2><<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
       else if (ppt == 8) k_icp<8><<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
+      else if (ppt == 16) k_icp<16><<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
       else k_icp<4><<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
     }
   }
@@ -955,7 +956,8 @@ NUI_API nui_status nui_ctx_last_tick_kernels(nui_ctx* c, int* n) {
 bool tuning_valid(const nui_tuning& t) {
   auto tw_ok = [](int w) { return w == 4 || w == 8 || w == 16 || w == 32; };
   return t.integrate_threads_log2 >= 14 && t.integrate_threads_log2 <= 22 &&
-         (t.icp_pixels_per_thread == 2 || t.icp_pixels_per_thread == 4 || t.icp_pixels_per_thread == 8) &&
+         (t.icp_pixels_per_thread == 2 || t.icp_pixels_per_thread == 4 || t.icp_pixels_per_thread == 8 ||
+          t.icp_pixels_per_thread == 16) &&
          tw_ok(t.raycast_tile_width) && tw_ok(t.hash_raycast_tile_width);
 }
 
@@ -1043,7 +1045,7 @@ NUI_API nui_status nui_ctx_autotune(nui_ctx* c, const nui_session_cfg* cfgs, int
     best.*field = pick;
   };
   if (dense) tune_one(&nui_tuning::integrate_threads_log2, {16, 17, 18, 19, 20}, 3);
-  tune_one(&nui_tuning::icp_pixels_per_thread, {2, 4, 8}, 2);
+  tune_one(&nui_tuning::icp_pixels_per_thread, {2, 4, 8, 16}, 2);
   if (dense) tune_one(&nui_tuning::raycast_tile_width, {4, 8, 16, 32}, 5);
   if (hash) tune_one(&nui_tuning::hash_raycast_tile_width, {4, 8, 16, 32}, 5);
   float tick_ms = 0.f;

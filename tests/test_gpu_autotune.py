@@ -53,7 +53,7 @@ def test_shapes_change_no_result_bit(gpu_ctx, mix):
 def test_icp_pixels_per_thread_regroups_sums_only(gpu_ctx, mix):
     gpu_ctx.set_tuning(L.Tuning(*DEFAULT))
     base, _ = _run(gpu_ctx, mix)
-    for ppt in (2, 8):
+    for ppt in (2, 8, 16):
         gpu_ctx.set_tuning(L.Tuning(18, ppt, 8, 8))
         p, _ = _run(gpu_ctx, mix)
         for f in range(p.shape[0]):
@@ -80,7 +80,7 @@ def test_autotune_keeps_a_valid_choice_and_frees_its_sessions(gpu_ctx, mix):
     d = t.as_dict()
     assert d == gpu_ctx.tuning().as_dict()
     assert 16 <= d["integrate_threads_log2"] <= 20
-    assert d["icp_pixels_per_thread"] in (2, 4, 8)
+    assert d["icp_pixels_per_thread"] in (2, 4, 8, 16)
     assert d["raycast_tile_width"] in (4, 8, 16, 32) and d["hash_raycast_tile_width"] in (4, 8, 16, 32)
     assert ms > 0
     assert torch.cuda.mem_get_info()[0] >= free0 - (64 << 20)
