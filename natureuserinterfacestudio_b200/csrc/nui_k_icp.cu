@@ -377,16 +377,29 @@ __global__ void __launch_bounds__(kIcpThreads, 2) k_icp(const SessionDesc* __res
     acc[28] += 1.0;
   }
 
-  // warp, then block reduction in FP64; the block's sums leave as (hi, lo) FP32 pairs
+  // warp, then block reduction in FP64; the block's sums leave as (hi, lo) FP32 pairs.
+  // The warp step is a reduce-scatter over the 32 lanes (the terms padded to 32): at each
+  // of five steps a lane keeps half of its values, sends the other half to its partner
+  // and adds what it receives, so lane k ends with the warp's sum of term k after 31
+  // exchanges instead of 29 x 5.
   constexpr int kWarps = kIcpThreads / 32;
-  __shared__ double wsum[kWarps][kIcpTerms];
+  __shared__ double wsum[kWarps][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  {
+    double v[32];
 #pragma unroll
-  for (int k = 0; k < kIcpTerms; ++k) {
-    double a = acc[k];
+    for (int k = 0; k < 32; ++k) v[k] = k < kIcpTerms ? acc[k] : 0.0;
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
-    if (lane == 0) wsum[warp][k] = a;
+    for (int half = 16; half > 0; half >>= 1) {
+      const bool upper = lane & half;
+#pragma unroll
+      for (int j = 0; j < half; ++j) {
+        const double send = upper ? v[j] : v[j + half];
+        const double keep = upper ? v[j + half] : v[j];
+        v[j] = keep + __shfl_xor_sync(0xffffffffu, send, half);
+      }
+    }
+    wsum[warp][lane] = v[0];
   }
   __syncthreads();
   if (threadIdx.x < kIcpTerms) {
