@@ -248,17 +248,28 @@ __global__ void __launch_bounds__(256) k_brick_summary(const SessionDesc* __rest
     const long b = b0 + list[k];
     const int x0 = (int)(b % bx) * 8, y0 = (int)((b / bx) % by) * 8, z0 = (int)(b / ((long)bx * by)) * 8;
     bool weighted = false, unweighted = false, nonpos = false;
-    for (int r = lane >> 3; r < 64; r += 4) {  // 64 rows (y, z) of 8 voxels; lane & 7 = x
-      const int x = x0 + (lane & 7), y = y0 + (r & 7), z = z0 + (r >> 3);
-      if (x >= s.res[0] || y >= s.res[1] || z >= s.res[2]) continue;
-      float F;
-      int W;
-      Voxel<FMT>::load(s, vox_index(s, x, y, z), F, W);
-      if (W > 0) {
-        weighted = true;
-        if (!(F > 0.f)) nonpos = true;
-      } else {
-        unweighted = true;
+    // 64 rows (y, z) of 8 voxels, lane & 7 = x: four rows' voxels loaded before any is
+    // tested
+    for (int r0 = lane >> 3; r0 < 64; r0 += 16) {
+      float F[4];
+      int W[4];
+      bool in[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = r0 + 4 * q;
+        const int x = x0 + (lane & 7), y = y0 + (r & 7), z = z0 + (r >> 3);
+        in[q] = x < s.res[0] && y < s.res[1] && z < s.res[2];
+        if (in[q]) Voxel<FMT>::load(s, vox_index(s, x, y, z), F[q], W[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (!in[q]) continue;
+        if (W[q] > 0) {
+          weighted = true;
+          if (!(F[q] > 0.f)) nonpos = true;
+        } else {
+          unweighted = true;
+        }
       }
     }
     const bool any_w = __any_sync(0xffffffffu, weighted), any_u = __any_sync(0xffffffffu, unweighted);
