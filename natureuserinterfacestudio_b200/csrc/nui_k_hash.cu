@@ -136,6 +136,11 @@ __global__ void __launch_bounds__(256) k_hash_walk(const SessionDesc* __restrict
   if (id >= W * H) return;
   const float Dp = pass_depth(s, id);
   if (isnan(Dp)) return;
+  // pass 1 only walks the rays that requested a block in pass 0 (the table does not change
+  // between the passes, so any other ray finds every block again); the flag is kept in the
+  // range image, which the raycast rewrites before it reads it
+  if (pass == 1 && s.range[id].x == 0.f) return;
+  bool requested = false;
   const int px = id % W, py = id / W;
   const DevXform& m = s.ts->xf;
   const float3 pc = depth_to_point(s.cam, px, py, Dp);
@@ -177,6 +182,7 @@ __global__ void __launch_bounds__(256) k_hash_walk(const SessionDesc* __restrict
           s.alloc_type[hi] = excess ? 2 : 1;
           s.vis[hi] = 1;
           atomicMax(&s.keys[hi], key);
+          requested = true;
         } else if (__ldcg(&s.keys[hi]) == key) {
           s.coords[hi] = make_short4(bx, by, bz, 0);
         }
@@ -184,6 +190,7 @@ __global__ void __launch_bounds__(256) k_hash_walk(const SessionDesc* __restrict
     }
     rmin = add3(rmin, rdir);
   }
+  if (pass == 0) s.range[id].x = requested ? 1.f : 0.f;
 }
 
 __device__ __forceinline__ int entry_ptr(const SessionDesc& s, unsigned i) {
