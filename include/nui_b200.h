@@ -36,7 +36,11 @@ typedef enum {
   NUI_ERR_INVALID_ARG = 1,
   NUI_ERR_OOM = 2,
   NUI_ERR_TRACKING_LOST = 3, /* singular ICP system (NuiKinfuOpenCLDepthTracker.cpp:465-472) */
-  NUI_ERR_HASH_FULL = 4,
+  NUI_ERR_HASH_FULL = 4,     /* voxel hash: a frame's allocation found the block pool or the
+                              * excess list empty (or met a corrupted excess chain) and dropped
+                              * blocks; the frame is otherwise complete (pose tracked, the
+                              * allocated blocks integrated).  The reference drops them silently
+                              * (KinfuHashScene.cl:155,171-172). */
   NUI_ERR_MESH_OVERFLOW = 5,
   NUI_ERR_TIMEOUT = 6,
   NUI_ERR_DEVICE = 7,
@@ -196,11 +200,21 @@ NUI_API nui_status nui_mesh(nui_session* s, float* pos, float* col, uint64_t cap
  * (res[1]-1)*ceil((res[0]-1)/128) <= 4095 count blocks; larger volumes are rejected with
  * NUI_ERR_INVALID_ARG.  The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call outside any
- * stream capture.  All calls share the array: two calls that overlap on the GPU (other
- * threads, other streams) race on it.  Same order, capacity and overflow rules as
- * nui_mesh; d_pos: cap*3 floats, d_col: cap*4 floats, either may be NULL. */
+ * stream capture.  The address is looked up again after nui_ctx_create on that device, so
+ * a device reset (which invalidates it, with every session) followed by a new context
+ * works.  All calls share the array: two calls that overlap on the GPU (other threads,
+ * other streams) race on it.  The kernels run on the session's context stream with no
+ * ordering against the caller's streams: the output buffers must be idle when the call is
+ * made (synchronise whatever produces or reads them first); the call synchronises its
+ * stream before it returns.  Buffers on another device are rejected.  The caller's current
+ * device is restored on return.  Same order, capacity and overflow rules as nui_mesh;
+ * d_pos: cap*3 floats, d_col: cap*4 floats, either may be NULL. */
 NUI_API nui_status nui_mesh_device_noalloc(nui_session* s, float* d_pos, float* d_col, uint64_t cap,
                                            uint64_t* nverts);
+/* Number of device and pinned-host allocations the library has made in this process (every
+ * cudaMalloc / cudaMallocHost / cudaHostAlloc it issues).  No counterpart in the
+ * reference; for tests that check an entry point allocates nothing. */
+NUI_API nui_status nui_debug_allocation_count(uint64_t* n);
 /* Marching-cubes case index of every cube, (res[0]-1)*(res[1]-1)*(res[2]-1) bytes in the
  * same (y, x, z) order; 0 for cubes skipped because a corner has no weight. */
 NUI_API nui_status nui_mesh_cases(nui_session* s, uint8_t* cases, size_t bytes, uint64_t* nverts);
@@ -423,21 +437,6 @@ NUI_API nui_status nui_camera_file_read(const char* path, float* fx_fy_cx_cy);
  * when the stored size is not width x height. */
 NUI_API nui_status nui_recording_frame(const char* dir, int index, uint16_t* depth_mm, uint8_t* bgra,
                                        float* fx_fy_cx_cy, int64_t* timestamp, uint32_t width, uint32_t height);
-
-/* ---------------------------------------------------------------- synthetic input
- * Seeded analytic scenes and trajectories standing in for recorded Kinect sessions. */
-typedef struct nui_synth_scene nui_synth_scene;
-enum { NUI_SYNTH_TABLETOP = 0, NUI_SYNTH_ROOM = 1 };
-NUI_API nui_synth_scene* nui_synth_scene_create(int kind, uint64_t seed, float extent);
-NUI_API void nui_synth_scene_destroy(nui_synth_scene* s);
-NUI_API float nui_synth_scene_sdf(const nui_synth_scene* s, float x, float y, float z);
-/* The analytic signed distance at n points (xyz: 3n floats). */
-NUI_API void nui_synth_scene_sdf_many(const nui_synth_scene* s, const float* xyz, long n, float* out);
-NUI_API void nui_synth_trajectory(int kind, uint64_t seed, int frame, float radius, float deg_per_frame,
-                                  float* R_out, float* t_out);
-NUI_API void nui_synth_render(const nui_synth_scene* s, const float* R, const float* t, int W, int H, float fx,
-                              float fy, float cx, float cy, uint64_t noise_seed, int frame, int add_noise,
-                              uint16_t* depth_mm, uint8_t* bgra);
 
 #ifdef __cplusplus
 }

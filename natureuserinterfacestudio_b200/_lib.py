@@ -9,6 +9,9 @@ import weakref
 
 import numpy as np
 
+# test and benchmark input (its own library, libnui_synth.so); re-exported for the callers
+from .synth import SYNTH_ROOM, SYNTH_TABLETOP, SynthScene  # noqa: F401
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libnui_b200.so")
 
@@ -24,7 +27,6 @@ NUI_ERR_UNSUPPORTED = 8
 
 TSDF_I16, TSDF_F32, TSDF_F16_U8, TSDF_F16_F16 = 0, 1, 2, 3
 VOLUME_DENSE, VOLUME_HASH = 0, 1
-SYNTH_TABLETOP, SYNTH_ROOM = 0, 1
 
 
 class SessionCfg(C.Structure):
@@ -90,6 +92,7 @@ _SIGS = {
     "nui_mesh": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
     "nui_mesh_cases": (C.c_int, [_P, _P, C.c_size_t, _P]),
     "nui_mesh_device_noalloc": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
+    "nui_debug_allocation_count": (C.c_int, [_P]),
     "nui_k_color_pyramid": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, _P, _P]),
     "nui_server_create": (C.c_int, [_P, C.c_size_t, C.c_int, _P]),
     "nui_server_destroy": (C.c_int, [_P]),
@@ -133,12 +136,6 @@ _SIGS = {
     "nui_camera_file_write": (C.c_int, [C.c_char_p, _P]),
     "nui_camera_file_read": (C.c_int, [C.c_char_p, _P]),
     "nui_recording_frame": (C.c_int, [C.c_char_p, C.c_int, _P, _P, _P, _P, C.c_uint32, C.c_uint32]),
-    "nui_synth_scene_create": (_P, [C.c_int, C.c_uint64, C.c_float]),
-    "nui_synth_scene_destroy": (None, [_P]),
-    "nui_synth_scene_sdf": (C.c_float, [_P, C.c_float, C.c_float, C.c_float]),
-    "nui_synth_scene_sdf_many": (None, [_P, _P, C.c_long, _P]),
-    "nui_synth_trajectory": (None, [C.c_int, C.c_uint64, C.c_int, C.c_float, C.c_float, _P, _P]),
-    "nui_synth_render": (None, [_P, _P, _P, C.c_int, C.c_int] + [C.c_float] * 4 + [C.c_uint64, C.c_int, C.c_int, _P, _P]),
 }
 
 
@@ -270,7 +267,7 @@ class Context:
         poses = np.zeros((n, 12), np.float32)
         fn = lib().nui_batch_tick_device if device else lib().nui_batch_tick
         r = fn(self.h, arr, n, d, b, ptr(st), ptr(poses))
-        if r not in (NUI_OK, NUI_ERR_TRACKING_LOST):
+        if r not in (NUI_OK, NUI_ERR_TRACKING_LOST, NUI_ERR_HASH_FULL):
             check(r)
         return st, poses
 
@@ -475,47 +472,6 @@ class Session:
         n = C.c_uint64()
         check(lib().nui_mesh_cases(self.h, ptr(out), out.nbytes, C.byref(n)))
         return out, n.value
-
-
-# ------------------------------------------------------------------ synthetic input
-class SynthScene:
-    def __init__(self, kind=SYNTH_TABLETOP, seed=1, extent=3.0):
-        self.h = lib().nui_synth_scene_create(kind, seed, extent)
-        self.kind = kind
-        self.seed = seed
-
-    def __del__(self):
-        try:
-            if self.h:
-                lib().nui_synth_scene_destroy(self.h)
-        except Exception:
-            pass
-
-    def sdf(self, x, y, z):
-        return lib().nui_synth_scene_sdf(self.h, x, y, z)
-
-    def sdf_many(self, xyz):
-        p = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
-        out = np.zeros(len(p), np.float32)
-        lib().nui_synth_scene_sdf_many(self.h, ptr(p), len(p), ptr(out))
-        return out
-
-    def pose(self, frame, radius=1.5, deg_per_frame=2.0, traj_seed=None):
-        R = np.zeros(9, np.float32)
-        t = np.zeros(3, np.float32)
-        lib().nui_synth_trajectory(self.kind, self.seed if traj_seed is None else traj_seed, frame, radius,
-                                   deg_per_frame, ptr(R), ptr(t))
-        return R.reshape(3, 3), t
-
-    def render(self, R, t, W=640, H=480, fx=525.0, fy=525.0, cx=319.5, cy=239.5, noise_seed=7, frame=0,
-               noise=True, color=False):
-        d = np.zeros((H, W), np.uint16)
-        c = np.zeros((H, W, 4), np.uint8) if color else None
-        Rf = np.ascontiguousarray(R, np.float32).reshape(9)
-        tf = np.ascontiguousarray(t, np.float32).reshape(3)
-        lib().nui_synth_render(self.h, ptr(Rf), ptr(tf), W, H, fx, fy, cx, cy, noise_seed, frame, 1 if noise else 0,
-                               ptr(d), ptr(c))
-        return d, c
 
 
 class ServerResult(C.Structure):

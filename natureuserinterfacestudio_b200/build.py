@@ -6,6 +6,10 @@ Every CUDA source is compiled with nvcc for arch=compute_100a,code=sm_100a, with
 --fmad=false (no contraction: the kernels reproduce the reference's float arithmetic
 bit for bit) and -lineinfo; host sources with the same nvcc driver.  Objects go to
 natureuserinterfacestudio_b200/_build/, the library next to this file.
+
+The synthetic-input generator of the tests and the benchmark (synth/nui_synth.cpp) is a
+separate host library, libnui_synth.so, so that generating input never loads the product
+library.
 """
 import concurrent.futures as cf
 import os
@@ -18,6 +22,8 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.normpath(os.path.join(HERE, "..", "include"))
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libnui_b200.so")
+SYNTH_SRC = os.path.join(HERE, "synth", "nui_synth.cpp")
+SYNTH_LIB = os.path.join(HERE, "libnui_synth.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp,-fvisibility=hidden",
@@ -53,7 +59,22 @@ def _compile(nvcc, src, verbose):
     return obj, r.stderr
 
 
+def build_synth():
+    """libnui_synth.so: the seeded scenes, trajectories and Kinect-like renderer."""
+    deps = [SYNTH_SRC, os.path.join(HERE, "synth", "nui_synth.h")]
+    if os.path.exists(SYNTH_LIB) and os.path.getmtime(SYNTH_LIB) >= max(os.path.getmtime(d) for d in deps):
+        return SYNTH_LIB
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-O3", "-std=c++17", "-fPIC", "-fopenmp", "-fvisibility=hidden", "-shared", SYNTH_SRC, "-o",
+           SYNTH_LIB]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("synth build failed: %s\n%s\n%s" % (" ".join(cmd), r.stdout, r.stderr))
+    return SYNTH_LIB
+
+
 def build(verbose=False):
+    build_synth()
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:

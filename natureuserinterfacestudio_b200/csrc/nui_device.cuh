@@ -55,6 +55,9 @@ struct TrackState {
 // What one session does in the current tick (host-written, read by every kernel).
 enum FrameKind : int { kInactive = -1, kFirstFrame = 0, kTrackFrame = 1 };
 
+// hcount slots read by the frame's status check (k_hash_health)
+constexpr int kHashFailed = 3, kHashChainFaults = 9, kHashFailedBefore = 10;
+
 struct SessionDesc {
   int kind;  // FrameKind
   int slot;  // the session's row of the batch outputs (pose, status)
@@ -125,7 +128,9 @@ struct SessionDesc {
   int* excess_list;               // free excess-slot stack
   int* hcount;                    // [0] last free block, [1] last free excess, [2] visible count, [3] failed
                                   // allocations, [4] swap-in count, [5] swap-out count, [6] free-list base
-                                  // of the swap pass, [7] store blocks used, [8] store-full refusals
+                                  // of the swap pass, [7] store blocks used, [8] store-full refusals,
+                                  // [9] corrupted excess chains met this frame, [10] failed
+                                  // allocations before this frame
   // global cache (hash swapping): per-entry swap state and store slot, the transfer lists,
   // and the host store (pinned, mapped: kernels read and write it directly)
   int swapping;

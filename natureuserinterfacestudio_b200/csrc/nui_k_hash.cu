@@ -163,9 +163,18 @@ __global__ void __launch_bounds__(256) k_hash_walk(const SessionDesc* __restrict
       found = true;
     }
     if (!found) {
-      bool excess = false;
+      bool excess = false, broken = false;
       if (en.ptr >= -1) {
+        // an excess chain holds at most ne entries, each link inside the excess list; a
+        // link that breaks either rule is a corrupted table: counted (the tick reports
+        // NUI_ERR_HASH_FULL) and the block is neither found nor requested
+        int links = 0;
         while (en.offset >= 1) {
+          if (en.offset > (unsigned)s.ne || ++links > s.ne) {
+            if (pass == 0) atomicAdd(&s.hcount[kHashChainFaults], 1);
+            broken = true;
+            break;
+          }
           hi = (unsigned)s.nb + en.offset - 1;
           en = load_entry(s.entries, hi);
           if (en.pos[0] == bx && en.pos[1] == by && en.pos[2] == bz && en.ptr >= -1) {
@@ -176,7 +185,7 @@ __global__ void __launch_bounds__(256) k_hash_walk(const SessionDesc* __restrict
         }
         excess = true;
       }
-      if (!found) {
+      if (!found && !broken) {
         const unsigned long long key = ((unsigned long long)(id + 1) << 16) | (unsigned long long)(i & 0xffff);
         if (pass == 0) {
           s.alloc_type[hi] = excess ? 2 : 1;
@@ -673,14 +682,19 @@ __global__ void __launch_bounds__(256) k_hash_project(const SessionDesc* __restr
 
 // Pool offset (block index * 512) of block (sx, sy, sz) or -1: the bucket, then its excess
 // chain (findVoxelBlockIndex, KinfuHashRaycast.cl:78-111).
+// The walk visits at most the bucket and ne excess entries and follows only links inside
+// the excess list: a corrupted chain ends the lookup as "missing" and is counted.
 __device__ __noinline__ int hash_block_lookup(const SessionDesc& s, short sx, short sy, short sz) {
   unsigned hi = hash_index(s.hmask, sx, sy, sz);
-  for (;;) {
+  for (int links = 0; links <= s.ne; ++links) {
     const HEntry en = load_entry(s.entries, hi);
     if (en.pos[0] == sx && en.pos[1] == sy && en.pos[2] == sz && en.ptr >= 0) return en.ptr * 512;
     if (en.offset < 1) return -1;
+    if (en.offset > (unsigned)s.ne) break;
     hi = (unsigned)s.nb + en.offset - 1;
   }
+  atomicAdd(&s.hcount[kHashChainFaults], 1);
+  return -1;
 }
 
 template <int HF>
@@ -1180,7 +1194,7 @@ __global__ void k_hash_reset(const SessionDesc* __restrict__ descs) {
     s.hcount[1] = s.ne - 1;
     s.hcount[2] = 0;
     s.hcount[3] = 0;
-    for (int k = 4; k < 9; ++k) s.hcount[k] = 0;
+    for (int k = 4; k < 16; ++k) s.hcount[k] = 0;
   }
 }
 

@@ -29,6 +29,24 @@ __global__ void k_tick_begin(const SessionDesc* __restrict__ descs, int n) {
   if (s.kind < 0 || !s.ts) return;
   s.ts->dmax_bits = 0;
   s.ts->touched = 0ull;
+  if (s.hcount) {
+    s.hcount[kHashFailedBefore] = s.hcount[kHashFailed];
+    s.hcount[kHashChainFaults] = 0;
+  }
+}
+
+// End of a tick with voxel-hash sessions: a frame whose allocation ran out of pool blocks
+// or excess slots (the reference's atomic_dec of an empty free list,
+// KinfuHashScene.cl:155,171-172, silently drops the block) or met a corrupted excess chain
+// reports NUI_ERR_HASH_FULL (4) unless tracking already failed.
+__global__ void k_hash_health(const SessionDesc* __restrict__ descs, int n, int* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !status) return;
+  const SessionDesc& s = descs[i];
+  if (s.kind < 0 || !s.ts || !s.hcount) return;
+  const int o = s.slot;
+  if (status[2 * o] != 0) return;
+  if (s.hcount[kHashFailed] > s.hcount[kHashFailedBefore] || s.hcount[kHashChainFaults] > 0) status[2 * o] = 4;
 }
 
 template <int FMT>

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <deque>
 #include <cmath>
@@ -50,6 +51,7 @@ template <int F>
 __global__ void k_raycast_finish(const SessionDesc*);
 __global__ void k_publish(const SessionDesc*, int, float*, int*);
 __global__ void k_tick_begin(const SessionDesc*, int);
+__global__ void k_hash_health(const SessionDesc*, int, int*);
 __global__ void k_occ_clear(const SessionDesc*);
 __global__ void k_hash_prepare(const SessionDesc*);
 __global__ void k_hash_walk(const SessionDesc*, int);
@@ -107,6 +109,36 @@ nui_status fail(nui_status st, const std::string& msg) {
     cudaError_t e_ = (call);                                                                \
     if (e_ != cudaSuccess) return fail(NUI_ERR_DEVICE, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
+
+// Every device or pinned-host allocation the library makes goes through these, so that
+// tests can check that an entry point allocates nothing (nui_debug_allocation_count).
+std::atomic<unsigned long long> g_allocations{0};
+cudaError_t counted_malloc(void** p, size_t bytes) {
+  g_allocations.fetch_add(1, std::memory_order_relaxed);
+  return cudaMalloc(p, bytes);
+}
+template <typename T>
+cudaError_t counted_malloc(T** p, size_t bytes) {
+  return counted_malloc(reinterpret_cast<void**>(p), bytes);
+}
+cudaError_t counted_malloc_host(void** p, size_t bytes) {
+  g_allocations.fetch_add(1, std::memory_order_relaxed);
+  return cudaMallocHost(p, bytes);
+}
+template <typename T>
+cudaError_t counted_malloc_host(T** p, size_t bytes) {
+  return counted_malloc_host(reinterpret_cast<void**>(p), bytes);
+}
+cudaError_t counted_host_alloc(void** p, size_t bytes, unsigned flags) {
+  g_allocations.fetch_add(1, std::memory_order_relaxed);
+  return cudaHostAlloc(p, bytes, flags);
+}
+template <typename T>
+cudaError_t counted_host_alloc(T** p, size_t bytes, unsigned flags) {
+  return counted_host_alloc(reinterpret_cast<void**>(p), bytes, flags);
+}
+
+void noalloc_forget(int device);  // defined with nui_mesh_device_noalloc
 
 constexpr int kStages = 7;  // 6 stage intervals and the whole tick
 constexpr int kMinIcpPpt = 2;  // smallest ICP pixels per thread: sizes the partial sums
@@ -636,6 +668,7 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
   } else {
     launch_hash_raycast(p, d, st);
   }
+  if (p.hashMask) k_hash_health<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n, d_status);
   mark(6);
 }
 
@@ -651,12 +684,12 @@ nui_status ensure_cap(nui_ctx* ctx, int n) {
   cudaFree(ctx->d_status);
   cudaFreeHost(ctx->h_pose);
   cudaFreeHost(ctx->h_status);
-  NUI_CUDA(cudaMalloc(&ctx->d_descs, sizeof(SessionDesc) * cap));
-  NUI_CUDA(cudaMallocHost(&ctx->h_descs, sizeof(SessionDesc) * cap));
-  NUI_CUDA(cudaMalloc(&ctx->d_pose, sizeof(float) * 14 * cap));
-  NUI_CUDA(cudaMalloc(&ctx->d_status, sizeof(int) * 2 * cap));
-  NUI_CUDA(cudaMallocHost(&ctx->h_pose, sizeof(float) * 14 * cap));
-  NUI_CUDA(cudaMallocHost(&ctx->h_status, sizeof(int) * 2 * cap));
+  NUI_CUDA(counted_malloc(&ctx->d_descs, sizeof(SessionDesc) * cap));
+  NUI_CUDA(counted_malloc_host(&ctx->h_descs, sizeof(SessionDesc) * cap));
+  NUI_CUDA(counted_malloc(&ctx->d_pose, sizeof(float) * 14 * cap));
+  NUI_CUDA(counted_malloc(&ctx->d_status, sizeof(int) * 2 * cap));
+  NUI_CUDA(counted_malloc_host(&ctx->h_pose, sizeof(float) * 14 * cap));
+  NUI_CUDA(counted_malloc_host(&ctx->h_status, sizeof(int) * 2 * cap));
   ctx->cap = cap;
   return NUI_OK;
 }
@@ -752,6 +785,12 @@ nui_status tick_finish(nui_ctx* ctx, nui_session* const* ss, int n, const uint16
   nui_status st = finish_timing(ctx);
   if (st != NUI_OK) return st;
   nui_status agg = NUI_OK;
+  auto note = [](nui_status r) {
+    if (r == NUI_ERR_HASH_FULL)
+      fail(r, "voxel hash: pool or excess list exhausted (or a corrupted chain); blocks dropped");
+    else if (r == NUI_ERR_TRACKING_LOST)
+      fail(r, "ICP system is singular");
+  };
   for (int i = 0; i < n; ++i) {
     nui_session* s = ss[i];
     if (!s || !raws[i]) {
@@ -759,10 +798,21 @@ nui_status tick_finish(nui_ctx* ctx, nui_session* const* ss, int n, const uint16
       continue;
     }
     int status = ctx->h_status[2 * i];
+    if (status == 4) {  // tracked and integrated, but the voxel hash dropped blocks
+      if (per) per[i] = NUI_ERR_HASH_FULL;
+      if (agg == NUI_OK) {
+        agg = NUI_ERR_HASH_FULL;
+        note(agg);
+      }
+      s->frames += 1;
+      if (poses) std::memcpy(poses + 12 * i, ctx->h_pose + 14 * i, 12 * sizeof(float));
+      continue;
+    }
     nui_status r = status == 0 ? NUI_OK : NUI_ERR_TRACKING_LOST;
     if (per) per[i] = r;
     if (r != NUI_OK) {
       agg = NUI_ERR_TRACKING_LOST;
+      note(agg);
       // the device state stays on the previous frame; clear the flag so that the next
       // frame (after nui_reset or not) starts from a clean tracker
       int zero = 0;
@@ -877,6 +927,7 @@ NUI_API nui_status nui_ctx_create(int device, nui_ctx** out) {
   NUI_CUDA(cudaGetDeviceCount(&ndev));
   if (device < 0 || device >= ndev) return fail(NUI_ERR_INVALID_ARG, "no such device");
   NUI_CUDA(cudaSetDevice(device));
+  noalloc_forget(device);
   nui_ctx* c = new nui_ctx();
   c->device = device;
   cudaError_t e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
@@ -893,9 +944,9 @@ NUI_API nui_status nui_ctx_create(int device, nui_ctx** out) {
     delete c;
     return fail(NUI_ERR_DEVICE, "context streams");
   }
-  if (cudaMalloc(&c->d_kdesc, sizeof(SessionDesc)) != cudaSuccess ||
-      cudaMalloc(&c->d_kts, sizeof(TrackState)) != cudaSuccess ||
-      cudaMalloc(&c->d_count, sizeof(unsigned long long)) != cudaSuccess) {
+  if (counted_malloc(&c->d_kdesc, sizeof(SessionDesc)) != cudaSuccess ||
+      counted_malloc(&c->d_kts, sizeof(TrackState)) != cudaSuccess ||
+      counted_malloc(&c->d_count, sizeof(unsigned long long)) != cudaSuccess) {
     delete c;
     return fail(NUI_ERR_OOM, "context scratch");
   }
@@ -1012,7 +1063,7 @@ NUI_API nui_status nui_ctx_autotune(nui_ctx* c, const nui_session_cfg* cfgs, int
     // a lost frame still ran the whole tick: it times like any other
     const nui_status r =
         nui_batch_tick(c, ss.data(), n, raws.data(), bgra ? cols.data() : nullptr, per.data(), poses.data());
-    return r == NUI_ERR_TRACKING_LOST ? NUI_OK : r;
+    return (r == NUI_ERR_TRACKING_LOST || r == NUI_ERR_HASH_FULL) ? NUI_OK : r;
   };
   nui_status st = NUI_OK;
   int f = 0;
@@ -1119,7 +1170,7 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
   const size_t N = (size_t)c.width * c.height;
   const size_t nv = (size_t)c.res[0] * c.res[1] * c.res[2];
   auto alloc = [&](void** p, size_t bytes) -> bool {
-    if (cudaMalloc(p, bytes) != cudaSuccess) {
+    if (counted_malloc(p, bytes) != cudaSuccess) {
       cudaGetLastError();
       return false;
     }
@@ -1128,7 +1179,7 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
   };
   // pinned host memory mapped into the device: *h the host pointer, *d the device one
   auto host_alloc = [&](void** h, void** d, size_t bytes) -> bool {
-    if (cudaHostAlloc(h, bytes, cudaHostAllocMapped) != cudaSuccess) {
+    if (counted_host_alloc(h, bytes, cudaHostAllocMapped) != cudaSuccess) {
       cudaGetLastError();
       return false;
     }
@@ -1602,7 +1653,15 @@ NUI_API nui_status nui_integrate(nui_session* s) {
   int one = 1;
   NUI_CUDA(cudaMemcpy(&s->ts->integrate, &one, sizeof(int), cudaMemcpyHostToDevice));
   NUI_CUDA(cudaMemset(&s->ts->touched, 0, sizeof(unsigned long long)));
-  return run_stage(s, 2);
+  if (!s->hash) return run_stage(s, 2);
+  int before[16], after[16];
+  NUI_CUDA(cudaMemcpy(before, s->hcount, sizeof(before), cudaMemcpyDeviceToHost));
+  nui_status st = run_stage(s, 2);
+  if (st != NUI_OK) return st;
+  NUI_CUDA(cudaMemcpy(after, s->hcount, sizeof(after), cudaMemcpyDeviceToHost));
+  if (after[kHashFailed] > before[kHashFailed] || after[kHashChainFaults] > before[kHashChainFaults])
+    return fail(NUI_ERR_HASH_FULL, "voxel hash: pool or excess list exhausted (or a corrupted chain); blocks dropped");
+  return NUI_OK;
 }
 
 NUI_API nui_status nui_raycast(nui_session* s) {
@@ -1629,7 +1688,7 @@ NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void*
       need = Nl * 16;
       if (bytes < need) return fail(NUI_ERR_INVALID_ARG, "buffer too small");
       void* tmp = nullptr;
-      NUI_CUDA(cudaMalloc(&tmp, need));
+      NUI_CUDA(counted_malloc(&tmp, need));
       SessionDesc d;
       fill_desc(s, d, kInactive, nullptr, nullptr);
       cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, s->ctx->stream);
@@ -1667,7 +1726,7 @@ NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void*
       need = (size_t)c.hash_pool_blocks * 512 * 6;
       if (bytes < need) return fail(NUI_ERR_INVALID_ARG, "buffer too small");
       void* tmp = nullptr;
-      NUI_CUDA(cudaMalloc(&tmp, need));
+      NUI_CUDA(counted_malloc(&tmp, need));
       SessionDesc d;
       fill_desc(s, d, kInactive, nullptr, nullptr);
       cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, s->ctx->stream);
@@ -1684,7 +1743,7 @@ NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void*
       if (bytes < need) return fail(NUI_ERR_INVALID_ARG, "buffer too small");
       if (what == 9 && !s->cvol) return fail(NUI_ERR_INVALID_ARG, "no colour volume");
       void* tmp = nullptr;
-      NUI_CUDA(cudaMalloc(&tmp, need));
+      NUI_CUDA(counted_malloc(&tmp, need));
       SessionDesc d;
       fill_desc(s, d, kInactive, nullptr, nullptr);
       cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, s->ctx->stream);
@@ -1728,7 +1787,7 @@ NUI_API nui_status nui_debug_upload_volume(nui_session* s, const int16_t* ref) {
   if (!s || !ref) return fail(NUI_ERR_INVALID_ARG, "null argument");
   const size_t nv = (size_t)s->cfg.res[0] * s->cfg.res[1] * s->cfg.res[2];
   void* tmp = nullptr;
-  NUI_CUDA(cudaMalloc(&tmp, nv * 4));
+  NUI_CUDA(counted_malloc(&tmp, nv * 4));
   SessionDesc d;
   fill_desc(s, d, kInactive, nullptr, nullptr);
   cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, s->ctx->stream);
@@ -1897,8 +1956,8 @@ nui_status nui_hash_mesh_impl(nui_session* s, float* pos, float* col, uint64_t c
   NUI_CUDA(cudaMemcpyAsync(s->d_desc1, &d, sizeof(d), cudaMemcpyHostToDevice, st));
   hash_mc_upload_tables(st, NUI_MC_TRI_PACKED);
   DevBuf cnt, off, dp, dc;
-  NUI_CUDA(cudaMalloc(&cnt.p, (size_t)nvis * 4));
-  NUI_CUDA(cudaMalloc(&off.p, ((size_t)nvis + 1) * 8));
+  NUI_CUDA(counted_malloc(&cnt.p, (size_t)nvis * 4));
+  NUI_CUDA(counted_malloc(&off.p, ((size_t)nvis + 1) * 8));
   const int hf = d.hfmt;
   if (hf == 0)
     k_hash_mesh_count<0><<<1184, 512, 0, st>>>(s->d_desc1, (unsigned*)cnt.p);
@@ -1911,8 +1970,8 @@ nui_status nui_hash_mesh_impl(nui_session* s, float* pos, float* col, uint64_t c
   *nverts = total;
   const unsigned long long k = total < cap ? total : cap;
   if (k > 0 && (pos || col)) {
-    if (pos) NUI_CUDA(cudaMalloc(&dp.p, k * 12));
-    if (col) NUI_CUDA(cudaMalloc(&dc.p, k * 16));
+    if (pos) NUI_CUDA(counted_malloc(&dp.p, k * 12));
+    if (col) NUI_CUDA(counted_malloc(&dc.p, k * 16));
     if (hf == 0)
       k_hash_mesh_emit<0><<<1184, 512, 0, st>>>(s->d_desc1, (const unsigned long long*)off.p, (float*)dp.p, (float*)dc.p, k);
     else
@@ -1957,8 +2016,8 @@ nui_status mc_prepare(nui_session* s, DevBuf& cc, DevBuf& bt, unsigned& nb, uint
   mc_upload_tables(st);
   const unsigned tilesX = cdiv(c.res[0] - 1, 128);
   nb = tilesX * (unsigned)(c.res[1] - 1);
-  NUI_CUDA(cudaMalloc(&cc.p, sizeof(unsigned) * (size_t)(c.res[0] - 1) * (c.res[1] - 1)));
-  NUI_CUDA(cudaMalloc(&bt.p, sizeof(unsigned long long) * (nb + 1)));
+  NUI_CUDA(counted_malloc(&cc.p, sizeof(unsigned) * (size_t)(c.res[0] - 1) * (c.res[1] - 1)));
+  NUI_CUDA(counted_malloc(&bt.p, sizeof(unsigned long long) * (nb + 1)));
   switch (c.tsdf_format) {
     case 0: mc_count<0>(s, nb, (unsigned*)cc.p, (unsigned long long*)bt.p, d_cases); break;
     case 1: mc_count<1>(s, nb, (unsigned*)cc.p, (unsigned long long*)bt.p, d_cases); break;
@@ -1984,8 +2043,8 @@ extern "C" NUI_API nui_status nui_mesh(nui_session* s, float* pos, float* col, u
   *nverts = total;
   const unsigned long long k = total < cap ? total : cap;
   if (k > 0 && (pos || col)) {
-    if (pos) NUI_CUDA(cudaMalloc(&dp.p, k * 3 * sizeof(float)));
-    if (col) NUI_CUDA(cudaMalloc(&dc.p, k * 4 * sizeof(float)));
+    if (pos) NUI_CUDA(counted_malloc(&dp.p, k * 3 * sizeof(float)));
+    if (col) NUI_CUDA(counted_malloc(&dc.p, k * 4 * sizeof(float)));
     switch (s->cfg.tsdf_format) {
       case 0: mc_emit<0>(s, nb, (unsigned*)cc.p, (unsigned long long*)bt.p, (float*)dp.p, (float*)dc.p, k); break;
       case 1: mc_emit<1>(s, nb, (unsigned*)cc.p, (unsigned long long*)bt.p, (float*)dp.p, (float*)dc.p, k); break;
@@ -2008,7 +2067,7 @@ extern "C" NUI_API nui_status nui_mesh_cases(nui_session* s, uint8_t* cases, siz
   const size_t need = (size_t)(c.res[0] - 1) * (c.res[1] - 1) * (c.res[2] - 1);
   if (bytes < need) return fail(NUI_ERR_INVALID_ARG, "buffer too small");
   DevBuf cc, bt, dcase;
-  NUI_CUDA(cudaMalloc(&dcase.p, need));
+  NUI_CUDA(counted_malloc(&dcase.p, need));
   unsigned nb = 0;
   unsigned long long total = 0;
   nui_status st = mc_prepare(s, cc, bt, nb, (uint8_t*)dcase.p, total);
@@ -2030,9 +2089,25 @@ constexpr int kMaxDevices = 64;
 unsigned char* g_mesh_scratch_addr[kMaxDevices] = {};
 std::mutex g_mesh_scratch_mu;
 
-// Device address of the scratch array on `device` (current); looked up on the first call.
-// Nothing in the array needs to start at zero: the count pass writes every column count and
-// every block total before the scan and the emit pass read them.
+// Restores the caller's current device when the entry point returns.
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      prev = -1;
+      cudaGetLastError();
+    }
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// Device address of the scratch array on `device` (current); looked up on the first call
+// after the library loads or after a context is created on the device (nui_ctx_create
+// forgets the cached address, so that a device reset followed by a new context looks it up
+// again).  Nothing in the array needs to start at zero: the count pass writes every column
+// count and every block total before the scan and the emit pass read them.
 nui_status noalloc_scratch(int device, unsigned char** out) {
   if (device < 0 || device >= kMaxDevices) return fail(NUI_ERR_INVALID_ARG, "device index out of range");
   std::lock_guard<std::mutex> lock(g_mesh_scratch_mu);
@@ -2045,7 +2120,19 @@ nui_status noalloc_scratch(int device, unsigned char** out) {
   *out = g_mesh_scratch_addr[device];
   return NUI_OK;
 }
+
+void noalloc_forget(int device) {
+  if (device < 0 || device >= kMaxDevices) return;
+  std::lock_guard<std::mutex> lock(g_mesh_scratch_mu);
+  g_mesh_scratch_addr[device] = nullptr;
+}
 }  // namespace
+
+extern "C" NUI_API nui_status nui_debug_allocation_count(uint64_t* n) {
+  if (!n) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  *n = g_allocations.load(std::memory_order_relaxed);
+  return NUI_OK;
+}
 
 extern "C" NUI_API nui_status nui_mesh_device_noalloc(nui_session* s, float* d_pos, float* d_col, uint64_t cap,
                                                       uint64_t* nverts) {
@@ -2056,6 +2143,7 @@ extern "C" NUI_API nui_status nui_mesh_device_noalloc(nui_session* s, float* d_p
   const unsigned nb = cdiv(c.res[0] - 1, 128) * (unsigned)(c.res[1] - 1);
   if (ncols > kNoAllocCols || (size_t)nb + 1 > kNoAllocBlocks)
     return fail(NUI_ERR_INVALID_ARG, "volume too large for the no-allocation mesh scratch");
+  DeviceGuard guard;
   NUI_CUDA(cudaSetDevice(s->ctx->device));
   for (const float* q : {(const float*)d_pos, (const float*)d_col}) {
     if (!q) continue;
@@ -2065,6 +2153,8 @@ extern "C" NUI_API nui_status nui_mesh_device_noalloc(nui_session* s, float* d_p
       cudaGetLastError();
       return fail(NUI_ERR_INVALID_ARG, "output buffers must be device memory");
     }
+    if (a.type == cudaMemoryTypeDevice && a.device != s->ctx->device)
+      return fail(NUI_ERR_INVALID_ARG, "output buffers must be on the session's device");
   }
   unsigned char* base = nullptr;
   nui_status st0 = noalloc_scratch(s->ctx->device, &base);
@@ -2161,7 +2251,7 @@ nui_status server_collect(nui_server* v) {
   std::vector<nui_status> per(n);
   std::vector<float> poses(12 * (size_t)n);
   nui_status st = tick_finish(v->ctx, v->bsess.data(), n, v->braw.data(), per.data(), poses.data());
-  if (st != NUI_OK && st != NUI_ERR_TRACKING_LOST) return st;
+  if (st != NUI_OK && st != NUI_ERR_TRACKING_LOST && st != NUI_ERR_HASH_FULL) return st;
   for (int i = 0; i < n; ++i) {
     if (!v->bsess[i] || !v->braw[i]) continue;
     nui_server_result r;
@@ -2271,8 +2361,8 @@ NUI_API nui_status nui_server_admit(nui_server* v, const nui_session_cfg* cfg, i
     server_free_slot_buffers(sl);
     bool ok = true;
     for (int b = 0; b < 2 && ok; ++b) {
-      ok = cudaMalloc(&sl.draw[b], N * 2) == cudaSuccess;
-      if (ok && col) ok = cudaMalloc(&sl.dbgra[b], N * 4) == cudaSuccess;
+      ok = counted_malloc(&sl.draw[b], N * 2) == cudaSuccess;
+      if (ok && col) ok = counted_malloc(&sl.dbgra[b], N * 4) == cudaSuccess;
     }
     if (!ok) {
       server_free_slot_buffers(sl);

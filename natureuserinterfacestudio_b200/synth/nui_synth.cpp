@@ -14,7 +14,7 @@
 #include <cstring>
 #include <vector>
 
-#include "../../include/nui_b200.h"
+#include "nui_synth.h"
 
 namespace {
 
@@ -150,7 +150,7 @@ void matmul3(const double A[9], const double B[9], double C[9]) {
 
 extern "C" {
 
-NUI_API nui_synth_scene* nui_synth_scene_create(int kind, uint64_t seed, float extent) {
+NUI_SYNTH_API nui_synth_scene* nui_synth_scene_create(int kind, uint64_t seed, float extent) {
   nui_synth_scene* s = new nui_synth_scene();
   s->kind = kind;
   s->seed = seed;
@@ -198,13 +198,13 @@ NUI_API nui_synth_scene* nui_synth_scene_create(int kind, uint64_t seed, float e
   return s;
 }
 
-NUI_API void nui_synth_scene_destroy(nui_synth_scene* s) { delete s; }
+NUI_SYNTH_API void nui_synth_scene_destroy(nui_synth_scene* s) { delete s; }
 
-NUI_API float nui_synth_scene_sdf(const nui_synth_scene* s, float x, float y, float z) {
+NUI_SYNTH_API float nui_synth_scene_sdf(const nui_synth_scene* s, float x, float y, float z) {
   return (float)scene_sdf(*s, v3(x, y, z));
 }
 
-NUI_API void nui_synth_scene_sdf_many(const nui_synth_scene* s, const float* xyz, long n, float* out) {
+NUI_SYNTH_API void nui_synth_scene_sdf_many(const nui_synth_scene* s, const float* xyz, long n, float* out) {
 #pragma omp parallel for schedule(static)
   for (long i = 0; i < n; ++i) out[i] = (float)scene_sdf(*s, v3(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
 }
@@ -213,7 +213,7 @@ NUI_API void nui_synth_scene_sdf_many(const nui_synth_scene* s, const float* xyz
 //  tabletop: orbit of radius `radius` around (0, 0, radius) starting at the origin looking
 //            down +z, deg_per_frame per frame, seeded jitter (1 mm, 0.2 deg, 1 sigma).
 //  room:     walk at 1.2 m/s (30 Hz) along a seeded smooth loop, yaw rate <= 60 deg/s.
-NUI_API void nui_synth_trajectory(int kind, uint64_t seed, int frame, float radius, float deg_per_frame,
+NUI_SYNTH_API void nui_synth_trajectory(int kind, uint64_t seed, int frame, float radius, float deg_per_frame,
                                   float* R_out, float* t_out) {
   double R[9], t[3];
   if (kind == NUI_SYNTH_TABLETOP) {
@@ -273,7 +273,7 @@ NUI_API void nui_synth_trajectory(int kind, uint64_t seed, int frame, float radi
 }
 
 // Renders one frame: uint16 depth in mm (0 = no measurement) and optional BGRA8 colour.
-NUI_API void nui_synth_render(const nui_synth_scene* s, const float* Rf, const float* tf, int W, int H, float fx,
+NUI_SYNTH_API void nui_synth_render(const nui_synth_scene* s, const float* Rf, const float* tf, int W, int H, float fx,
                               float fy, float cx, float cy, uint64_t noise_seed, int frame, int add_noise,
                               uint16_t* depth_mm, uint8_t* bgra) {
   double R[9], t[3];

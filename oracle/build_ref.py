@@ -6,7 +6,7 @@ mechanically into C++ that compiles against ref_shim/clshim.hpp, and compiled to
 with the launchers in ref_shim/launch_*.inc into one shared library.  The rewritten
 sources go to a temporary directory and are deleted after the build; only the .so is
 kept (oracle/_ref is git-ignored).  The library runs the reference kernels on the host
-cores and is used to pin the oracle restatement and as the timed reference CPU arm.
+cores and is used to pin the oracle restatement (tests/test_oracle_*pins.py).
 
 Rewrites (each purely syntactic):
   * `(float3)(a, b, c)` vector literals      -> `float3(a, b, c)`
@@ -15,7 +15,8 @@ Rewrites (each purely syntactic):
   * `__attribute__((reqd_work_group_size(..)))` and `#pragma OPENCL` lines removed
   * implicit-int declarations `const idx =` (extract.cl) -> `const int idx =`
 
-Usage:  python oracle/build_ref.py [--reference /root/reference]
+Usage:  python oracle/build_ref.py [--reference TREE]
+        (TREE defaults to $NUI_REFERENCE_TREE, else /root/reference)
 """
 import argparse
 import os
@@ -116,7 +117,7 @@ def extract(src, names):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("NUI_REFERENCE_TREE", "/root/reference"))
     ap.add_argument("--cxx", default="g++")
     args = ap.parse_args()
     kdir = os.path.join(args.reference, "src", "Kernels")

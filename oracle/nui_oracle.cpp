@@ -1374,6 +1374,7 @@ ORC_API int orc_engine_frame(OrcEngine* e, const uint16_t* raw, const uint8_t* b
   const OrcEngineCfg& c = e->c;
   const int W = c.W, H = c.H;
   const long N = (long)W * H;
+  e->touched = 0;  // voxels updated by this frame (0 when the gate skips the integration)
   orc_pass_filter(raw, N, c.dmin, c.dmax, e->depth.data());
   orc_bilateral(e->depth.data(), W, H, e->gauss.data(), c.filter_radius, c.sigma_depth2_inv_half,
                 c.depth_threshold, e->dl[0].data());

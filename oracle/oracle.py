@@ -11,7 +11,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libnui_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libnui_ref.so")
-REFERENCE_TREE = "/root/reference"
+# where the reference source tree is read from when oracle/_ref is built (NUI_REFERENCE_TREE)
+REFERENCE_TREE = os.environ.get("NUI_REFERENCE_TREE", "/root/reference")
 
 _P = C.c_void_p
 

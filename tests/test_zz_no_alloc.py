@@ -23,11 +23,20 @@ def _noalloc(s, cap, colours=True):
     pos = torch.full((max(cap, 1), 3), float("nan"), dtype=torch.float32, device="cuda")
     col = torch.full((max(cap, 1), 4), float("nan"), dtype=torch.float32, device="cuda")
     n = C.c_uint64()
-    torch.cuda.synchronize()
+    torch.cuda.synchronize()  # the output buffers must be idle when the call is made
+    before = _allocations()
     r = L.lib().nui_mesh_device_noalloc(s.h, C.c_void_p(pos.data_ptr()),
                                         C.c_void_p(col.data_ptr()) if colours else None, cap, C.byref(n))
+    # the defining property: the call makes no device or pinned-host allocation of its own
+    assert _allocations() == before
     k = min(n.value, cap)
     return r, n.value, pos[:k].cpu().numpy(), col[:k].cpu().numpy()
+
+
+def _allocations():
+    n = C.c_uint64()
+    assert L.lib().nui_debug_allocation_count(C.byref(n)) == L.NUI_OK
+    return n.value
 
 
 @pytest.fixture(scope="module")
@@ -81,3 +90,17 @@ def test_rejects_oversize_volume_and_host_buffers(gpu_ctx, sessions):
     n = C.c_uint64()
     r = L.lib().nui_mesh_device_noalloc(sessions[1].h, L.ptr(host), None, 16, C.byref(n))
     assert r == L.NUI_ERR_INVALID_ARG
+
+
+def test_rejects_buffers_of_another_device(sessions):
+    """A buffer on another GPU is refused before any launch (the kernels would otherwise
+    write another device's memory from this one)."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs a second CUDA device")
+    other = torch.zeros((16, 3), dtype=torch.float32, device="cuda:1")
+    torch.cuda.synchronize(1)
+    n = C.c_uint64(12345)
+    r = L.lib().nui_mesh_device_noalloc(sessions[1].h, C.c_void_p(other.data_ptr()), None, 16, C.byref(n))
+    assert r == L.NUI_ERR_INVALID_ARG and n.value == 12345
+    assert torch.count_nonzero(other).item() == 0
