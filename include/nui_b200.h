@@ -226,7 +226,10 @@ NUI_API nui_status nui_mesh_cases(nui_session* s, uint8_t* cases, size_t bytes, 
  *   6 raw volume storage of the session format   7 depth level `level` (f32)
  *   8 reference colour map (u8x4)        9 colour volume, reference layout (u8x4)
  *  10 model colours of colour tracking: the previous frame's (u8x4)
- *  11 / 12 x / y colour gradients of the current frame (u8x4, signed bytes; level 0) */
+ *  11 / 12 x / y colour gradients of the current frame (u8x4, signed bytes; level 0)
+ *  13 brick states (u8 per 8^3 brick, x fastest: 0 empty, 1 mixed, 2 positive, 3 awaiting
+ *     re-classification, 4 positive with unweighted voxels)
+ *  14 weight plane of NUI_TSDF_F16_U8 (u8, session layout x + rx*(y + ry*z)) */
 NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void* host, size_t bytes);
 /* Voxel-hash sessions: what = 20 entries (16 B each: short pos[3], pad, int ptr, uint
  * offset), 21 visible list (int, count = nui_hash_stats visible), 22 pool voxels in the

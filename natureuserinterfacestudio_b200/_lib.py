@@ -418,7 +418,12 @@ class Session:
                   3: ((self.H, self.W, 4), np.float32), 4: ((self.H, self.W, 4), np.float32),
                   5: ((nv, 2), np.int16), 7: ((H, W), np.float32), 8: ((self.H, self.W, 4), np.uint8),
                   9: ((nv, 4), np.uint8), 10: ((self.H, self.W, 4), np.uint8), 11: ((H, W, 4), np.uint8),
-                  12: ((H, W, 4), np.uint8)}
+                  12: ((H, W, 4), np.uint8),
+                  13: ((((self.res[0] + 7) // 8) * ((self.res[1] + 7) // 8) * ((self.res[2] + 7) // 8),), np.uint8),
+                  14: ((nv,), np.uint8)}
+        fmt = self.cfg.tsdf_format
+        shapes[6] = {TSDF_I16: ((nv, 2), np.int16), TSDF_F32: ((nv, 2), np.float32),
+                     TSDF_F16_U8: ((nv,), np.float16), TSDF_F16_F16: ((nv, 2), np.float16)}[fmt]
         shape, dt = shapes[what]
         out = np.zeros(shape, dt)
         check(lib().nui_debug_download(self.h, what, level, ptr(out), out.nbytes))

@@ -4,7 +4,8 @@
 
 Every CUDA source is compiled with nvcc for arch=compute_100a,code=sm_100a, with
 --fmad=false (no contraction: the kernels reproduce the reference's float arithmetic
-bit for bit) and -lineinfo; host sources with the same nvcc driver.  Objects go to
+bit for bit) and -lineinfo; host sources with the same nvcc driver.  The tolerance-mode
+kernels of the FP16 serving formats (*_fast.cu) are compiled with contraction on.  Objects go to
 natureuserinterfacestudio_b200/_build/, the library next to this file.
 
 The synthetic-input generator of the tests and the benchmark (synth/nui_synth.cpp) is a
@@ -48,7 +49,10 @@ def _compile(nvcc, src, verbose):
     deps.append(os.path.join(INCLUDE, "nui_b200.h"))
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj, ""
-    cmd = [nvcc] + ARCH + COMMON + ["-c", path, "-o", obj]
+    flags = COMMON
+    if src.endswith("_fast.cu"):  # tolerance-mode kernels: contraction allowed
+        flags = [f if f != "--fmad=false" else "--fmad=true" for f in COMMON]
+    cmd = [nvcc] + ARCH + flags + ["-c", path, "-o", obj]
     if src.endswith(".cpp"):
         cmd = [nvcc] + COMMON + ["-x", "c++", "-c", path, "-o", obj]
     if verbose:

@@ -41,6 +41,8 @@ __global__ void k_color_keep(const SessionDesc*);
 template <int F>
 __global__ void k_integrate(const SessionDesc*);
 template <int F>
+__global__ void k_integrate_fast(const SessionDesc*);
+template <int F>
 __global__ void k_volume_init(const SessionDesc*);
 template <int F>
 __global__ void k_brick_summary(const SessionDesc*, int);
@@ -488,6 +490,11 @@ size_t icp_partial_bytes(const nui_session_cfg& c) {
 template <int F>
 void launch_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   if (!(p.fmtMask & (1 << F))) return;
+  if (F >= NUI_TSDF_F16_U8) {  // tolerance mode: one warp per 32 x 8 x 8 tile, grid-stride
+    const long blocks = std::min<long>(cdiv(p.maxBricks[F], 4 * kFastWarps), 1024);
+    k_integrate_fast<F><<<dim3((unsigned)std::max<long>(blocks, 1), dense_n(p)), 32 * kFastWarps, 0, st>>>(d);
+    return;
+  }
   k_integrate<F><<<dim3(cdiv(p.maxIntegThreads[F], 256), dense_n(p)), 256, 0, st>>>(d);
 }
 template <int F>
@@ -1707,6 +1714,16 @@ NUI_API nui_status nui_debug_download(nui_session* s, int what, int level, void*
     case 10: src = s->cprev; need = N * 4; break;
     case 11: src = s->cgx[level]; need = Nl * 4; break;
     case 12: src = s->cgy[level]; need = Nl * 4; break;
+    case 13:  // brick states, one byte per 8^3 brick, x fastest
+      if (s->hash) return fail(NUI_ERR_INVALID_ARG, "not a dense session");
+      src = s->occ;
+      need = (size_t)((c.res[0] + 7) / 8) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8);
+      break;
+    case 14:  // the weight plane of NUI_TSDF_F16_U8
+      if (s->hash || c.tsdf_format != NUI_TSDF_F16_U8) return fail(NUI_ERR_INVALID_ARG, "no weight plane");
+      src = s->wvol;
+      need = nv;
+      break;
     case 20: src = s->entries; need = ((size_t)c.hash_buckets + c.hash_excess) * 16; break;
     case 21: {
       int cnt[4];
