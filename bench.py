@@ -121,17 +121,21 @@ def is_hash(c):
     return c.volume_kind == 1
 
 
-def render_sequences(L, nseq, nframes, seed0=100):
-    seqs = []
+def render_sequences(L, nseq, nframes, seed0=100, poses=False):
+    """nseq orbit sequences of nframes depth frames (and, with poses=True, their true
+    camera poses (R, t) in the scene frame)."""
+    seqs, gts = [], []
     for k in range(nseq):
         sc = L.SynthScene(L.SYNTH_TABLETOP, seed=seed0 + k, extent=3.0)
-        fr = []
+        fr, gt = [], []
         for i in range(nframes):
             R, t = sc.pose(i, radius=1.5, deg_per_frame=2.0)
             d, _ = sc.render(R, t, W_IMG, H_IMG, frame=i, noise_seed=seed0 * 7 + k)
             fr.append(d)
+            gt.append((np.asarray(R, np.float64), np.asarray(t, np.float64)))
         seqs.append(fr)
-    return seqs
+        gts.append(gt)
+    return (seqs, gts) if poses else seqs
 
 
 def pingpong(k, n=SEQ_FRAMES):
@@ -155,7 +159,7 @@ def run_ours(args, rank, world):
     ctx.set_stream(stream.cuda_stream)
     n = args.sessions
     nseq = min(n, args.sequences)
-    seqs = render_sequences(L, nseq, SEQ_FRAMES)
+    seqs, gts = render_sequences(L, nseq, SEQ_FRAMES, poses=True)
     dev_frames = [[torch.from_numpy(f.view(np.int16)).cuda() for f in s] for s in seqs]
     host_frames = [[torch.from_numpy(f.view(np.int16)).pin_memory() for f in s] for s in seqs]
     torch.cuda.synchronize()
@@ -211,33 +215,59 @@ def run_ours(args, rank, world):
     per_tick = [a.elapsed_time(b) for a, b in tick_ev]
     value = n * world * args.steps / (ms_total / 1e3)
 
-    # per-stage device times (un-graphed launches with stage events)
+    # per-stage device times (un-graphed launches with stage events) and the work the
+    # kernels counted in the same ticks
     ctx.enable_timing(True)
-    stage = np.zeros(7)
+    stage = np.zeros(9)
     reps = 3
-    touched = 0
+    work = {"touched": 0, "bricks": 0, "ray_reads": 0, "ray_samples": 0, "ray_hits": 0, "icp_px": 0}
     for k in range(reps):
         ctx.batch_tick(sessions, dframes(args.warmup + args.steps + k), device=True)
-        stage += np.array([ctx.stage_ms(i) for i in range(7)])
-        touched += sum(s.touched() for s, c in zip(sessions, cfgs) if not is_hash(c))
+        stage += np.array([ctx.stage_ms(i) for i in range(9)])
+        for s, c in zip(sessions, cfgs):
+            w = s.work_counters()
+            if not is_hash(c):
+                for key in ("touched", "bricks", "ray_reads", "ray_samples", "ray_hits"):
+                    work[key] += w[key]
+            work["icp_px"] += sum(it * (W_IMG >> l) * (H_IMG >> l) for l, it in enumerate(w["icp_iters"]))
     ctx.enable_timing(False)
     stage /= reps
-    touched /= reps
+    work = {k: v / reps for k, v in work.items()}
     hash_visible = [s.hash_stats()[0] for s, c in zip(sessions, cfgs) if is_hash(c)]
     for s in sessions:
         s.close()
     sessions = None
     torch.cuda.empty_cache()
 
-    # dense integration kernel: every voxel's state read and written once plus the depth
-    # image read once (N_vox * 2 * S + W * H * 4 per dense stream), S = 3 (FP16 + u8)
+    # rooflines of the dominant kernels, from the work the kernels counted:
+    #   integration (k_integrate_fast, stage 3): updated voxels read and written (3 B each
+    #     way, FP16 + u8), the voxels of re-classified bricks read once, the depth image read;
+    #   dense raycast (k_raycast_fast + k_raycast_finish_fast, stage 7): the voxels the march
+    #     read, one brick-state byte per visited sample, 64 voxels per refined crossing, and
+    #     the vertex / normal / colour maps written (12 + 12 + 4 B a pixel);
+    #   ICP (k_icp_cluster, stage 2): per pixel-iteration the depth (4 B) and one reference
+    #     vertex and normal (16 + 16 B).
     dense = [c for c in cfgs if not is_hash(c)]
-    n_vox = sum(int(np.prod(c.res)) for c in dense)
-    integ_bytes = n_vox * 2 * 3 + len(dense) * W_IMG * H_IMG * 4
-    touched_bytes = touched * 2 * 3 + len(dense) * W_IMG * H_IMG * 4
-    integ_ms = stage[3]
+    npx = W_IMG * H_IMG
     peak, peak_kind = peaks()
-    achieved = integ_bytes / (integ_ms / 1e3) / 1e9
+    kernels = [
+        ("k_integrate_fast<F16_U8>", stage[3],
+         work["touched"] * 6 + work["bricks"] * 512 * 3 + len(dense) * npx * 4),
+        ("k_raycast_fast<F16_U8>+k_raycast_finish_fast<F16_U8>", stage[7],
+         work["ray_reads"] * 3 + work["ray_samples"] + work["ray_hits"] * 64 * 3 + len(dense) * npx * 28),
+        ("k_icp_cluster", stage[2], work["icp_px"] * 36),
+    ]
+    roof = []
+    for name, ms, nbytes in kernels:
+        ach = nbytes / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+        roof.append({"kernel": name, "bound": "hbm", "achieved": round(ach, 1), "peak": peak, "peak_kind": peak_kind,
+                     "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": profile_traffic(name.split("<")[0]),
+                     "algorithmic_bytes_per_launch": int(nbytes), "launch_ms": round(float(ms), 4)})
+    top = max(roof, key=lambda r: r["launch_ms"])
+
+    # ---------------------------------------------------------------- ATE vs plain FP32
+    ate = ate_vs_plain(L, ctx, seqs, gts, args.ate_frames, args.ate_streams) if args.ate_frames > 0 else None
+    torch.cuda.empty_cache()
 
     # ---------------------------------------------------------------- e2e: serving loop
     srv = L.Server(ctx, 150 << 30, max_streams=max(64, n))
@@ -319,17 +349,15 @@ def run_ours(args, rank, world):
             "speedup_vs_plain_fp32": round(value / plain, 3) if plain else None,
             "stage_ms": {k: round(float(v), 4) for k, v in zip(
                 ["preprocess", "pyramid+feedback", "track", "integrate_dense_kernel", "summaries+hash_integrate",
-                 "raycast", "tick"], stage)},
+                 "raycast", "tick", "raycast_dense_kernels", "hash_side_stream"], stage)},
+            "work_per_tick": {k: int(v) for k, v in work.items()},
+            "ate": ate,
             "hash_visible_blocks_mean": round(float(np.mean(hash_visible)), 1) if hash_visible else None,
             "e2e": {"value": round(e2e_value, 2), "unit": "frames/s",
                     "h2d_bytes_per_step": n * W_IMG * H_IMG * 2, "d2h_bytes_per_step": n * (14 * 4 + 2 * 4)},
             "gpu_launches": kernels_per_tick * args.steps,
-            "roofline": {"kernel": "k_integrate<F16_U8>", "bound": "hbm", "achieved": round(achieved, 1),
-                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": profile_traffic("k_integrate"),
-                         "algorithmic_bytes_per_launch": int(integ_bytes), "launch_ms": round(float(integ_ms), 4),
-                         "touched_voxel_bytes_per_launch": int(touched_bytes),
-                         "touched_voxel_gbs": round(touched_bytes / (integ_ms / 1e3) / 1e9, 1)},
+            "roofline": top,
+            "roofline_kernels": roof,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "tracking_lost": lost,
@@ -438,6 +466,50 @@ def serving_sim(L, ctx, host_frames, seconds, n_target, warm=2.0, seed=11):
             "admissions_over_5ms": int(sum(a > 5 for a in admit_ms))}
 
 
+def _rel(gt, i0, i):
+    """Pose i of a sequence in the camera frame of pose i0 (trackers start at identity)."""
+    R0, t0 = gt[i0]
+    R, t = gt[i]
+    return R0.T @ R, R0.T @ (t - t0)
+
+
+def ate_vs_plain(L, ctx, seqs, gts, nframes, nstreams):
+    """The metric's accuracy condition: the first nstreams streams of the mix run nframes
+    frames (sequences replayed forth and back) in the served formats (FP16 TSDF + u8
+    weight, half-precision hash, one batched tick per frame) and in the plain path (FP32
+    dense TSDF / int16 hash, one stream at a time).  Reported per stream: the RMS distance
+    between the two trajectories' camera positions, and each one's ATE against the true
+    trajectory (RMS position error after both start at the first frame's pose)."""
+    nseq = len(seqs)
+    cfg16 = stream_cfgs(L, nstreams, L.TSDF_F16_U8, L.TSDF_F16_U8)
+    cfg32 = stream_cfgs(L, nstreams, L.TSDF_F32, L.TSDF_I16)
+    offs = [(i * 7) % 11 for i in range(nstreams)]
+    idx = [[pingpong(offs[i] + k) for k in range(nframes)] for i in range(nstreams)]
+    a = [L.Session(ctx, c) for c in cfg16]
+    b = [L.Session(ctx, c) for c in cfg32]
+    p16 = np.zeros((nstreams, nframes, 3))
+    p32 = np.zeros((nstreams, nframes, 3))
+    for k in range(nframes):
+        fr = [seqs[i % nseq][idx[i][k]] for i in range(nstreams)]
+        _, poses = ctx.batch_tick(a, fr)
+        p16[:, k] = poses[:, 9:]
+        for i in range(nstreams):
+            p32[i, k] = b[i].process(fr[i])[1][9:]
+    for s in a + b:
+        s.close()
+    out = []
+    for i in range(nstreams):
+        gt = np.array([_rel(gts[i % nseq], idx[i][0], idx[i][k])[1] for k in range(nframes)])
+        out.append({"stream": i, "kind": "hash" if is_hash(cfg16[i]) else "dense %d^3" % cfg16[i].res[0],
+                    "traj_rms_diff_mm": round(float(np.sqrt(np.mean(np.sum((p16[i] - p32[i]) ** 2, 1)))) * 1e3, 3),
+                    "ate_fp16_mm": round(float(np.sqrt(np.mean(np.sum((p16[i] - gt) ** 2, 1)))) * 1e3, 3),
+                    "ate_plain_fp32_mm": round(float(np.sqrt(np.mean(np.sum((p32[i] - gt) ** 2, 1)))) * 1e3, 3)})
+    worst = max(abs(o["ate_fp16_mm"] - o["ate_plain_fp32_mm"]) for o in out)
+    return {"frames": nframes, "streams": out, "max_abs_ate_diff_mm": round(worst, 3),
+            "max_traj_rms_diff_mm": round(max(o["traj_rms_diff_mm"] for o in out), 3),
+            "within_1mm": bool(worst <= 1.0)}
+
+
 def profile_traffic(kernel):
     """DRAM bytes per launch of `kernel` from the committed ncu summary, if present."""
     path = os.path.join(ROOT, "profiles", "traffic.txt")
@@ -509,6 +581,9 @@ def main():
     ap.add_argument("--serve-seconds", dest="serve_seconds", type=float, default=12.0)
     ap.add_argument("--no-plain", dest="plain", action="store_false")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ate-frames", dest="ate_frames", type=int, default=100,
+                    help="frames of the FP16-vs-plain-FP32 trajectory comparison (0: skip)")
+    ap.add_argument("--ate-streams", dest="ate_streams", type=int, default=8)
     ap.add_argument("--no-autotune", dest="no_autotune", action="store_true",
                     help="keep the default launch shapes instead of timing the candidates first")
     ap.add_argument("--tuning", default="",

@@ -124,6 +124,18 @@ typedef struct {
    * device pool (counted by nui_hash_swap_stats). */
   int hash_swapping;
   int hash_store_blocks;
+  /* voxel hash: how the reference maps are rendered after each frame.  0 = raycast every
+   * pixel (the reference's raycast path, NuiKinfuOpenCLHashScene::Raycast; the default
+   * here).  1 = the reference's forward rendering (ForwardRender,
+   * NuiKinfuOpenCLHashScene.cpp:991-1012, on by default in NuiSLAMController.cpp:47): the
+   * previous maps' vertices are carried to the pixels they project to, only pixels nothing
+   * lands on are raycast, and normals come from the vertex map; the reference projects the
+   * vertices with the camera-to-world transform of the pose (forwardProject_kernel,
+   * KinfuHashRaycast.cl:490), which mode 1 reproduces.  2 = forward rendering with the
+   * vertices taken into the camera (world-to-camera).  Measured on the oracle (320x240 orbit,
+   * 20 frames): ATE 4.0 mm with mode 0, 415 mm with mode 1 (tracking diverges once the
+   * camera moves), 7.9 mm with mode 2. */
+  int hash_forward_render;
 } nui_session_cfg;
 
 typedef struct nui_ctx nui_ctx;
@@ -304,9 +316,11 @@ NUI_API nui_session* nui_server_session(nui_server* srv, int slot);
  * context, when timing is enabled (CUDA events on the context stream).
  * stage: 0 preprocess, 1 pyramid + feedback maps, 2 tracking (colour gradients, ICP, gate),
  * 3 shifting-volume shifts + dense integration kernel, 4 brick summaries (+ voxel-hash
- * allocation / integration), 5 raycast, 6 whole tick.  When the batch holds dense and
- * voxel-hash sessions, the hash sessions' allocation, integration and raycast run on a
- * second stream beside stages 3-5 instead; stage 5 then ends when both are done. */
+ * allocation / integration), 5 raycast, 6 whole tick, 7 the dense raycast kernels alone,
+ * 8 the voxel-hash sessions' work on the second stream (0 when it did not run there).
+ * When the batch holds dense and voxel-hash sessions, the hash sessions' allocation,
+ * integration and raycast run on a second stream beside stages 3-5 instead; stage 5 then
+ * ends when both are done. */
 NUI_API nui_status nui_ctx_enable_timing(nui_ctx* ctx, int enable);
 NUI_API nui_status nui_ctx_stage_ms(nui_ctx* ctx, int stage, float* ms);
 /* Kernel launches in the captured graph of the context's last graphed batch tick. */
@@ -388,6 +402,12 @@ NUI_API nui_status nui_session_snapshot(nui_session* s, void* host, size_t bytes
 NUI_API nui_status nui_session_restore(nui_session* s, const void* host, size_t bytes);
 /* Voxels read-modify-written by the last integration of a session. */
 NUI_API nui_status nui_session_touched_voxels(nui_session* s, uint64_t* n);
+/* Work the kernels counted for the session's last frame, from which the algorithmic bytes of
+ * each launch follow (no counterpart in the reference): out[0] voxels updated by the
+ * integration, out[1] 8^3 bricks the tolerance-mode integration re-classified, out[2] voxel
+ * reads of the tolerance-mode dense raycast march, out[3] march samples it visited, out[4]
+ * crossings it refined, out[5..8] ICP iterations run at levels 0..3.  9 values. */
+NUI_API nui_status nui_session_work_counters(nui_session* s, uint64_t* out);
 
 /* ---------------------------------------------------------------- kernel-level calls
  * One entry point per reference kernel launch on the hot path, on device pointers,

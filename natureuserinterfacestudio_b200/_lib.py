@@ -45,7 +45,7 @@ class SessionCfg(C.Structure):
         ("hash_excess", C.c_int), ("hash_pool_blocks", C.c_int), ("hash_max_weight", C.c_int),
         ("photometric_weight", C.c_float),
         ("voxel_shift", C.c_int), ("shift_basis", C.c_float * 3), ("shift_point_cap", C.c_int),
-        ("hash_swapping", C.c_int), ("hash_store_blocks", C.c_int),
+        ("hash_swapping", C.c_int), ("hash_store_blocks", C.c_int), ("hash_forward_render", C.c_int),
     ]
 
 
@@ -127,6 +127,7 @@ _SIGS = {
     "nui_ctx_set_tuning": (C.c_int, [_P, _P]),
     "nui_ctx_autotune": (C.c_int, [_P, _P, C.c_int, _P, _P, C.c_int, C.c_int, _P, _P]),
     "nui_session_touched_voxels": (C.c_int, [_P, _P]),
+    "nui_session_work_counters": (C.c_int, [_P, _P]),
     "nui_k_preprocess": (C.c_int, [_P, _P, C.c_int, C.c_int] + [C.c_float] * 6 + [C.c_int] + [C.c_float] * 3 + [_P, _P, _P]),
     "nui_k_pyramid_level": (C.c_int, [_P, _P, C.c_int, C.c_int] + [C.c_float] * 4 + [C.c_int, C.c_float, _P, _P]),
     "nui_k_feedback_maps": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_float, _P, _P, _P]),
@@ -452,6 +453,14 @@ class Session:
         if out.size:
             check(lib().nui_debug_download(self.h, what, 0, ptr(out), out.nbytes))
         return out
+
+    def work_counters(self):
+        """Work of the last frame: updated voxels, re-classified bricks, raycast voxel reads,
+        samples visited, refined crossings, ICP iterations per level (4)."""
+        out = np.zeros(9, np.uint64)
+        check(lib().nui_session_work_counters(self.h, ptr(out)))
+        return {"touched": int(out[0]), "bricks": int(out[1]), "ray_reads": int(out[2]),
+                "ray_samples": int(out[3]), "ray_hits": int(out[4]), "icp_iters": [int(x) for x in out[5:9]]}
 
     def volume_ref_layout(self):
         """Volume as the reference stores it: short2 at ((x + y*rx)*rz + z)."""

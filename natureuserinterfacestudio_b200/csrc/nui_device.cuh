@@ -15,6 +15,7 @@ constexpr int kMaxRadius = 7;
 constexpr int kIcpTerms = 29;  // 21 JtJ + 6 Jtr + r^2 + count  (icp.cl:122-160)
 constexpr int kTile = 16;      // pixel tile of the depth bound used by integration culling
 constexpr int kFastWarps = 8;  // warps per block of the tolerance-mode integration
+constexpr int kIcpCluster = 4; // thread blocks (one cluster) per session of the ICP kernel
 
 // Camera intrinsics block (gpu_def.h:13-27).
 struct DevCam {
@@ -43,7 +44,6 @@ struct TrackState {
   int iterations_run;
   float lastR[9], lastT[3];  // pose of the last integration (global translation: local +
                              // volume offset, NuiCameraPos.h:43)
-  unsigned int block_counter;
   int dmax_bits;         // largest ray-length depth of the frame (float bits, >= 0)
   unsigned long long touched;
   // shifting volume: voxel offset of the volume (m_voxel_offset), this frame's shift in
@@ -51,6 +51,12 @@ struct TrackState {
   int voff[3];
   int shift[3];
   unsigned long long points;
+  // work of the current frame counted by the kernels (the algorithmic bytes of a launch
+  // follow from these): tolerance-mode raycast voxel reads, samples visited and refined
+  // crossings; bricks re-classified by the tolerance-mode integration; ICP iterations run
+  // per level
+  unsigned long long ray_reads, ray_samples, ray_hits, bricks;
+  unsigned int icp_iters[kMaxLevels];
 };
 
 // What one session does in the current tick (host-written, read by every kernel).
@@ -113,7 +119,6 @@ struct SessionDesc {
   uchar4* cgy[kMaxLevels];
   // tracking state and ICP scratch
   TrackState* ts;
-  float2* partials;               // per-block (hi, lo) sums, kIcpTerms per block
   // voxel-block hash (volume_kind == hash; fmt is then -1 so the dense kernels skip)
   int hash;                       // 1 for a hash session
   int hfmt;                       // 0: int16 sdf (reference), 1: half sdf
@@ -131,7 +136,16 @@ struct SessionDesc {
                                   // allocations, [4] swap-in count, [5] swap-out count, [6] free-list base
                                   // of the swap pass, [7] store blocks used, [8] store-full refusals,
                                   // [9] corrupted excess chains met this frame, [10] failed
-                                  // allocations before this frame
+                                  // allocations before this frame, [11] pixels the forward
+                                  // render casts
+  // forward rendering of the reference maps (0 off, 1 the reference's projection, 2 world to
+  // camera): per pixel the last source pixel landing on it (+1), the missing pixels listed in
+  // increasing order, per-1024-pixel-block counts then offsets, landed colours
+  int fwd;
+  int* fwd_owner;
+  int* fwd_ids;
+  unsigned* fwd_blk;
+  uchar4* fwd_col;
   // global cache (hash swapping): per-entry swap state and store slot, the transfer lists,
   // and the host store (pinned, mapped: kernels read and write it directly)
   int swapping;

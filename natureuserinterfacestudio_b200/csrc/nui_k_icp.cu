@@ -1,16 +1,18 @@
-// Point-to-plane ICP, one launch per iteration, no host round trip.
+// Point-to-plane ICP: every iteration of every level in one launch, one thread-block
+// cluster per session, no host round trip.
 //
 // Per pixel (icp_block_kernel, icp.cl:222-292): rebuild the level's vertex from its depth,
 // transform it by the running estimate, project into the previous camera with
 // full-resolution intrinsics, bilinearly sample the world reference normal and vertex
 // (icp.cl:192-220; a tap NaN -> no match), and if |q - p| < distThres form the row
 // [n x p, n | n.(q - p)].  Each thread accumulates the 29 products of its pixels in FP64;
-// blocks reduce them with warp shuffles and shared memory and store (hi, lo) FP32 pairs;
-// the last block to finish (ticket on an atomic counter) adds the per-block pairs in
-// double in a fixed order and runs the host step of
+// blocks reduce them with warp shuffles and shared memory; the cluster's first block adds
+// the blocks' sums (distributed shared memory, fixed order) and runs the host step of
 // NuiKinfuOpenCLDepthTracker::IterativeClosestPoint (NuiKinfuOpenCLDepthTracker.cpp:324-496):
 // Levenberg-Marquardt accept/reject, FP64 determinant check and Cholesky solve, ZYX Euler
-// increment composed in FP64.  The next launch reads the updated estimate.
+// increment composed in FP64.  The next iteration reads the updated estimate.
+#include <cooperative_groups.h>
+
 #include "nui_device.cuh"
 
 namespace nui {
@@ -287,63 +289,25 @@ __device__ __noinline__ void icp_host_step(TrackState* ts, const double* sums, i
     }
 }
 
+// The 29 sums of the depth rows of one block of pixels (kIcpThreads x PPT consecutive
+// pixels of the level, index `vb`), added to this thread's FP64 accumulators.  sR / tc: the
+// running estimate; sp: the previous camera pose (the reference maps' frame).
 template <int PPT>
-__global__ void __launch_bounds__(kIcpThreads, 2) k_icp(const SessionDesc* __restrict__ descs, int level, int iter) {
-  const SessionDesc& s = descs[blockIdx.y];
-  if (s.kind != kTrackFrame || level >= s.levels || iter >= s.iters[level]) return;
-  TrackState* ts = s.ts;
-  if (ts->status != 0) return;
-  if (iter > 0 && ts->level_done) return;
-  const int w = s.W >> level, h = s.H >> level, n = w * h;
-  const int per_block = kIcpThreads * PPT;
-  const int nblocks = (n + per_block - 1) / per_block;
-  // colour tracking: at the finest level, blocks past the depth ones take the photometric
-  // term over the full-size model maps
-  const bool photo = s.photo_w > 0.f && level == 0;
-  const int ncb = photo ? (s.W * s.H + per_block - 1) / per_block : 0;
-  if ((int)blockIdx.x >= nblocks + ncb) return;
-
-  __shared__ float sR[9], st[3];
-  __shared__ DevXform sp;
-  if (threadIdx.x < 9) sR[threadIdx.x] = ts->R[threadIdx.x];
-  if (threadIdx.x < 3) st[threadIdx.x] = ts->t[threadIdx.x];
-  if (threadIdx.x < 21) reinterpret_cast<float*>(&sp)[threadIdx.x] = reinterpret_cast<const float*>(&ts->xf)[threadIdx.x];
-  __syncthreads();
-
-  // per-thread sums of the FP32 row products in FP64 (B200 runs FP64 adds at half the FP32
-  // rate: cheaper than a compensated FP32 pair, and as exact for these sums).  A launch
-  // shape that regroups the pixels then changes the sums by FP64 rounding only, far below
-  // anything that could flip a Levenberg-Marquardt decision.
-  double acc[kIcpTerms];
-#pragma unroll
-  for (int k = 0; k < kIcpTerms; ++k) acc[k] = 0.0;
-
-  // the level's vertices are rebuilt from its depth (4 bytes a pixel read instead of 16)
+__device__ __forceinline__ void icp_depth_rows(const SessionDesc& s, int level, int vb, const float* sR, float3 tc,
+                                               const DevXform& sp, double (&acc)[kIcpTerms]) {
+  const int w = s.W >> level, n = w * (s.H >> level);
   const float* __restrict__ Dl = s.dlev[level];
   const float fx = s.cam.fx, fy = s.cam.fy, cx = s.cam.cx, cy = s.cam.cy;
   const int RW = s.W, RN = s.W * s.H;
   const float fW = (float)s.W, fH = (float)s.H;
-  const float3 tc = f3(st[0], st[1], st[2]), tp = f3(sp.t[0], sp.t[1], sp.t[2]);
-  if ((int)blockIdx.x >= nblocks) {
-    const int cbase = ((int)blockIdx.x - nblocks) * per_block, NM = s.W * s.H;
-#pragma unroll 1
-    for (int k = 0; k < PPT; ++k) {
-      const int i = cbase + k * kIcpThreads + threadIdx.x;
-      if (i >= NM) break;
-      float c[kIcpTerms];
-      if (!color_row(s, i, sR, tc, c)) continue;
-#pragma unroll
-      for (int q = 0; q < kIcpTerms - 1; ++q) acc[q] += (double)c[q];
-      acc[28] += 1.0;
-    }
-  }
-  const int base = blockIdx.x * per_block;
+  const float3 tp = f3(sp.t[0], sp.t[1], sp.t[2]);
+  const int base = vb * kIcpThreads * PPT;
   // the depths of all the thread's pixels in flight at once, consumed from the front
   float dq[PPT];
 #pragma unroll
   for (int k = 0; k < PPT; ++k) {
     const int i = base + k * kIcpThreads + threadIdx.x;
-    dq[k] = ((int)blockIdx.x < nblocks && i < n) ? __ldg(Dl + i) : qnan();
+    dq[k] = i < n ? __ldg(Dl + i) : qnan();
   }
 #pragma unroll 1
   for (int k = 0; k < PPT; ++k) {
@@ -376,85 +340,161 @@ __global__ void __launch_bounds__(kIcpThreads, 2) k_icp(const SessionDesc* __res
     acc[27] += (double)(c7[6] * c7[6]);
     acc[28] += 1.0;
   }
+}
 
-  // warp, then block reduction in FP64; the block's sums leave as (hi, lo) FP32 pairs.
-  // The warp step is a reduce-scatter over the 32 lanes (the terms padded to 32): at each
-  // of five steps a lane keeps half of its values, sends the other half to its partner
-  // and adds what it receives, so lane k ends with the warp's sum of term k after 31
-  // exchanges instead of 29 x 5.
-  constexpr int kWarps = kIcpThreads / 32;
-  __shared__ double wsum[kWarps][32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  {
-    double v[32];
+// The photometric rows of one block of full-resolution model points (colour tracking).
+template <int PPT>
+__device__ __forceinline__ void icp_color_rows(const SessionDesc& s, int vb, const float* sR, float3 tc,
+                                               double (&acc)[kIcpTerms]) {
+  const int cbase = vb * kIcpThreads * PPT, NM = s.W * s.H;
+#pragma unroll 1
+  for (int k = 0; k < PPT; ++k) {
+    const int i = cbase + k * kIcpThreads + threadIdx.x;
+    if (i >= NM) break;
+    float c[kIcpTerms];
+    if (!color_row(s, i, sR, tc, c)) continue;
 #pragma unroll
-    for (int k = 0; k < 32; ++k) v[k] = k < kIcpTerms ? acc[k] : 0.0;
-#pragma unroll
-    for (int half = 16; half > 0; half >>= 1) {
-      const bool upper = lane & half;
-#pragma unroll
-      for (int j = 0; j < half; ++j) {
-        const double send = upper ? v[j] : v[j + half];
-        const double keep = upper ? v[j + half] : v[j];
-        v[j] = keep + __shfl_xor_sync(0xffffffffu, send, half);
-      }
-    }
-    wsum[warp][lane] = v[0];
-  }
-  __syncthreads();
-  if (threadIdx.x < kIcpTerms) {
-    double D = 0.0;
-    for (int wi = 0; wi < kWarps; ++wi) D += wsum[wi][threadIdx.x];
-    const float H = (float)D, L = (float)(D - (double)H);
-    s.partials[(size_t)blockIdx.x * kIcpTerms + threadIdx.x] = make_float2(H, L);
-  }
-  __threadfence();
-  __shared__ unsigned int ticket;
-  __syncthreads();
-  if (threadIdx.x == 0) ticket = atomicAdd(&ts->block_counter, 1u);
-  __syncthreads();
-  if (ticket != (unsigned)(nblocks + ncb) - 1) return;
-
-  // last block: fixed-order double reduction of the per-block pairs, the depth blocks
-  // and the photometric blocks separately
-  __threadfence();
-  __shared__ double red[kWarps][32];
-  __shared__ double sums[kIcpTerms];
-  for (int part = 0; part < (photo ? 2 : 1); ++part) {
-    const int b0 = part == 0 ? 0 : nblocks, b1 = part == 0 ? nblocks : nblocks + ncb;
-    {
-      const int k = lane;  // term index handled by this lane
-      double acc = 0.0;
-      if (k < kIcpTerms)
-#pragma unroll 4
-        for (int b = b0 + warp; b < b1; b += kWarps) {
-          float2 p = __ldcg(&s.partials[(size_t)b * kIcpTerms + k]);
-          acc += (double)p.x + (double)p.y;
-        }
-      red[warp][lane] = acc;
-    }
-    __syncthreads();
-    if (threadIdx.x < kIcpTerms) {
-      double a = 0.0;
-      for (int wi = 0; wi < kWarps; ++wi) a += red[wi][threadIdx.x];
-      // the photometric normal equations and residual enter weighted; the count stays
-      // the depth count
-      if (part == 0) sums[threadIdx.x] = a;
-      else if (threadIdx.x < kIcpTerms - 1) sums[threadIdx.x] += (double)s.photo_w * a;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    icp_host_step(ts, sums, iter, s.icp_min_count[level]);
-    ts->block_counter = 0;
-    __threadfence();
+    for (int q = 0; q < kIcpTerms - 1; ++q) acc[q] += (double)c[q];
+    acc[28] += 1.0;
   }
 }
 
-template __global__ void k_icp<2>(const SessionDesc*, int, int);
-template __global__ void k_icp<4>(const SessionDesc*, int, int);
-template __global__ void k_icp<8>(const SessionDesc*, int, int);
-template __global__ void k_icp<16>(const SessionDesc*, int, int);
+// Block sum of the threads' accumulators (a reduce-scatter over the 32 lanes of a warp,
+// terms padded to 32 -- at each of five steps a lane keeps half of its values, sends the
+// other half to its partner and adds what it receives, so lane k ends with the warp's sum
+// of term k after 31 exchanges instead of 29 x 5 -- then the warps in shared memory, in a
+// fixed order).  Threads 0..28 receive term threadIdx.x; all threads must call it.
+__device__ __forceinline__ double icp_block_sum(const double (&acc)[kIcpTerms]) {
+  constexpr int kWarps = kIcpThreads / 32;
+  __shared__ double wsum[kWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double v[32];
+#pragma unroll
+  for (int k = 0; k < 32; ++k) v[k] = k < kIcpTerms ? acc[k] : 0.0;
+#pragma unroll
+  for (int half = 16; half > 0; half >>= 1) {
+    const bool upper = lane & half;
+#pragma unroll
+    for (int j = 0; j < half; ++j) {
+      const double send = upper ? v[j] : v[j + half];
+      const double keep = upper ? v[j + half] : v[j];
+      v[j] = keep + __shfl_xor_sync(0xffffffffu, send, half);
+    }
+  }
+  wsum[warp][lane] = v[0];
+  __syncthreads();
+  double D = 0.0;
+  if (threadIdx.x < kIcpTerms)
+    for (int wi = 0; wi < kWarps; ++wi) D += wsum[wi][threadIdx.x];
+  __syncthreads();  // wsum is reused by the next call
+  return D;
+}
+
+// All ICP iterations of every level of one frame, one thread-block cluster per session
+// (NuiKinfuOpenCLDepthTracker::IterativeClosestPoint, NuiKinfuOpenCLDepthTracker.cpp:240-504).
+// The kIcpCluster blocks of a cluster share the level's pixels (pixel blocks b = rank,
+// rank + kIcpCluster, ...); every iteration each block reduces its FP64 sums into its own
+// shared memory, a cluster barrier makes them visible, block 0 adds the blocks' sums in
+// rank order through distributed shared memory and runs the host step (LM accept/reject,
+// FP64 Cholesky, pose update) on one thread, and a second barrier publishes the new
+// estimate, which every block reads from block 0's shared memory.  The hardware schedules
+// a cluster's blocks together and its barriers need no polling; every block takes the same
+// exits at the same points, since each decision comes from block 0's published state.
+// One launch per tick replaces one launch per iteration, and sessions whose levels stop
+// early leave their SMs to the others.
+template <int PPT>
+__global__ void __cluster_dims__(kIcpCluster, 1, 1) __launch_bounds__(kIcpThreads, 2)
+    k_icp_cluster(const SessionDesc* __restrict__ descs) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const SessionDesc& s = descs[blockIdx.y];
+  if (s.kind != kTrackFrame) return;  // the same for every block of the cluster
+  TrackState* ts = s.ts;
+  const int rank = (int)cluster.block_rank();
+  __shared__ float sR[9], st[3];
+  __shared__ DevXform sp;
+  __shared__ double part[2][32];  // this block's depth / photometric sums
+  __shared__ float bR[9], bt[3];  // block 0: the estimate after the host step
+  __shared__ int bflags[2];       // block 0: status, level_done
+  __shared__ double sums[kIcpTerms];
+  if (threadIdx.x < 9) sR[threadIdx.x] = ts->R[threadIdx.x];
+  if (threadIdx.x < 3) st[threadIdx.x] = ts->t[threadIdx.x];
+  if (threadIdx.x < 21) reinterpret_cast<float*>(&sp)[threadIdx.x] = reinterpret_cast<const float*>(&ts->xf)[threadIdx.x];
+  const int status0 = ts->status;
+  // every block has read the initial state before block 0 writes any of it
+  cluster.sync();
+  if (status0 != 0) return;
+  for (int level = s.levels - 1; level >= 0; --level) {
+    const int n = (s.W >> level) * (s.H >> level);
+    const int per_block = kIcpThreads * PPT;
+    const int nblocks = (n + per_block - 1) / per_block;
+    const bool photo = s.photo_w > 0.f && level == 0;
+    const int ncb = photo ? (s.W * s.H + per_block - 1) / per_block : 0;
+    for (int iter = 0; iter < s.iters[level]; ++iter) {
+      const float3 tc = f3(st[0], st[1], st[2]);
+      double acc[kIcpTerms];
+#pragma unroll
+      for (int k = 0; k < kIcpTerms; ++k) acc[k] = 0.0;
+      for (int vb = rank; vb < nblocks; vb += kIcpCluster) icp_depth_rows<PPT>(s, level, vb, sR, tc, sp, acc);
+      double D = icp_block_sum(acc);
+      if (threadIdx.x < kIcpTerms) part[0][threadIdx.x] = D;
+      if (photo) {
+#pragma unroll
+        for (int k = 0; k < kIcpTerms; ++k) acc[k] = 0.0;
+        for (int vb = rank; vb < ncb; vb += kIcpCluster) icp_color_rows<PPT>(s, vb, sR, tc, acc);
+        D = icp_block_sum(acc);
+        if (threadIdx.x < kIcpTerms) part[1][threadIdx.x] = D;
+      }
+      cluster.sync();  // every block's sums are visible to block 0
+      if (rank == 0) {
+        if (threadIdx.x < kIcpTerms) {
+          // the blocks' sums in rank order; the photometric normal equations and residual
+          // enter weighted, the count stays the depth count
+          double a = 0.0, c = 0.0;
+          for (int r = 0; r < kIcpCluster; ++r) {
+            const double* pr = cluster.map_shared_rank(&part[0][0], r);
+            a += pr[threadIdx.x];
+            if (photo) c += pr[32 + threadIdx.x];
+          }
+          if (photo && threadIdx.x < kIcpTerms - 1) a += (double)s.photo_w * c;
+          sums[threadIdx.x] = a;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          ts->icp_iters[level] += 1u;
+          icp_host_step(ts, sums, iter, s.icp_min_count[level]);
+          for (int k = 0; k < 9; ++k) bR[k] = ts->R[k];
+          for (int k = 0; k < 3; ++k) bt[k] = ts->t[k];
+          bflags[0] = ts->status;
+          bflags[1] = ts->level_done;
+        }
+      }
+      cluster.sync();  // block 0's new estimate is visible to every block
+      int flags[2];
+      {
+        const float* r0 = cluster.map_shared_rank(&bR[0], 0);
+        const float* t0 = cluster.map_shared_rank(&bt[0], 0);
+        const int* f0 = cluster.map_shared_rank(&bflags[0], 0);
+        if (threadIdx.x < 9) sR[threadIdx.x] = r0[threadIdx.x];
+        if (threadIdx.x < 3) st[threadIdx.x] = t0[threadIdx.x];
+        flags[0] = f0[0];
+        flags[1] = f0[1];
+      }
+      __syncthreads();
+      if (flags[0] != 0) {  // tracking lost: every block leaves together
+        cluster.sync();     // (block 0's shared memory stays alive until all have read it)
+        return;
+      }
+      if (flags[1]) break;
+    }
+  }
+  cluster.sync();  // no block leaves while another may still read block 0's shared memory
+}
+
+template __global__ void k_icp_cluster<2>(const SessionDesc*);
+template __global__ void k_icp_cluster<4>(const SessionDesc*);
+template __global__ void k_icp_cluster<8>(const SessionDesc*);
+template __global__ void k_icp_cluster<16>(const SessionDesc*);
 
 // After the last ICP launch (or on frame 0): publish the pose, decide the integration
 // gate (NuiKinfuTrackingEngine.cpp:115-127) and reset the estimate for the next frame.

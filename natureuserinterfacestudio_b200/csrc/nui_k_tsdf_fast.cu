@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(32 * kFastWarps) k_integrate_fast(const Sessio
   const float* __restrict__ depth = s.dscaled;
   const size_t slice = (size_t)rx * ry;
   const int hx = rx / 2, hy = ry / 2;
-  unsigned int touched_total = 0;
+  unsigned int touched_total = 0, bricks = 0;
 
   for (int tile = blockIdx.x * kFastWarps + (threadIdx.x >> 5); tile < ntiles; tile += nwarps) {
     const int x0 = (tile % ntx) << 5, y0 = ((tile / ntx) % nty) << 3, z0 = (tile / (ntx * nty)) << 3;
@@ -231,11 +231,14 @@ __global__ void __launch_bounds__(32 * kFastWarps) k_integrate_fast(const Sessio
       const unsigned g = 0xffu << lane;
       const uint8_t st = (bn & g) ? kBrickMixed : !(bw & g) ? kBrickEmpty : (bu & g) ? kBrickNoNeg : kBrickPositive;
       s.occ[occ_index(s, x, y0, z0)] = st;
+      ++bricks;
     }
     if (lane == 0 && s.occ2) s.occ2[occ2_index(s, x0, y0, z0)] = kSuperDirty;
   }
   const unsigned int t = __reduce_add_sync(0xffffffffu, touched_total);
+  const unsigned int b = __reduce_add_sync(0xffffffffu, bricks);
   if (lane == 0 && t) atomicAdd(&s.ts->touched, (unsigned long long)t);
+  if (lane == 0 && b) atomicAdd(&s.ts->bricks, (unsigned long long)b);
 }
 
 template __global__ void k_integrate_fast<2>(const SessionDesc*);

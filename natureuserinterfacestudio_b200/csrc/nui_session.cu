@@ -32,7 +32,7 @@ __global__ void k_pyramid(const SessionDesc*, int);
 __global__ void k_feedback(const SessionDesc*);
 __global__ void k_vertex_map(const SessionDesc*, int, float4*);
 template <int PPT>
-__global__ void k_icp(const SessionDesc*, int, int);
+__global__ void k_icp_cluster(const SessionDesc*);
 __global__ void k_track_finalize(const SessionDesc*, int);
 __global__ void k_ztab(const SessionDesc*);
 __global__ void k_color_level(const SessionDesc*, int);
@@ -51,6 +51,10 @@ template <int F>
 __global__ void k_raycast(const SessionDesc*, int);
 template <int F>
 __global__ void k_raycast_finish(const SessionDesc*);
+template <int F>
+__global__ void k_raycast_fast(const SessionDesc*, int);
+template <int F>
+__global__ void k_raycast_finish_fast(const SessionDesc*);
 __global__ void k_publish(const SessionDesc*, int, float*, int*);
 __global__ void k_tick_begin(const SessionDesc*, int);
 __global__ void k_hash_health(const SessionDesc*, int, int*);
@@ -142,8 +146,10 @@ cudaError_t counted_host_alloc(T** p, size_t bytes, unsigned flags) {
 
 void noalloc_forget(int device);  // defined with nui_mesh_device_noalloc
 
-constexpr int kStages = 7;  // 6 stage intervals and the whole tick
-constexpr int kMinIcpPpt = 2;  // smallest ICP pixels per thread: sizes the partial sums
+// stage intervals: 0-5 consecutive stages, 6 the whole tick, 7 the dense raycast kernels,
+// 8 the voxel-hash work on the side stream; kEvents events mark them
+constexpr int kStages = 9;
+constexpr int kEvents = 11;
 constexpr size_t kMaxGraphs = 64;  // captured tick graphs kept per context
 }  // namespace
 
@@ -182,7 +188,8 @@ struct nui_ctx {
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   bool timing = false;
-  cudaEvent_t ev[kStages] = {};
+  bool side_timed = false;  // the last timed tick ran voxel-hash work on the side stream
+  cudaEvent_t ev[kEvents] = {};
   float stage_ms[kStages] = {};
   // batch table (device + pinned staging) and per-session outputs (status + pose)
   int cap = 0;
@@ -227,7 +234,6 @@ struct nui_session {
   uint8_t* occ3 = nullptr;
   float* tile_max = nullptr;
   TrackState* ts = nullptr;
-  float2* partials = nullptr;
   uchar4* cprev = nullptr;        // colour tracking: the previous frame's colours and the
   uchar4* cgx[kMaxLevels] = {};   // current frame's gradients (level 0)
   uchar4* cgy[kMaxLevels] = {};
@@ -246,6 +252,9 @@ struct nui_session {
   unsigned long long* keys = nullptr;
   unsigned* blk = nullptr;
   float2* range = nullptr;  // one-entry table for the per-session path
+  int *fwd_owner = nullptr, *fwd_ids = nullptr;  // forward rendering scratch
+  unsigned* fwd_blk = nullptr;
+  uchar4* fwd_col = nullptr;
 
   long frames = 0;
   bool color_frame = false;
@@ -301,6 +310,9 @@ bool cfg_valid(const nui_session_cfg* c, std::string& why) {
   if (c->voxel_shift < 0 || c->shift_point_cap < 0) return why = "voxel shift and point cap must be >= 0", false;
   if (c->hash_swapping && c->volume_kind != NUI_VOLUME_HASH) return why = "swapping needs a voxel-hash volume", false;
   if (c->hash_store_blocks < 0) return why = "hash store blocks must be >= 0", false;
+  if (c->hash_forward_render < 0 || c->hash_forward_render > 2) return why = "hash forward render must be 0, 1 or 2", false;
+  if (c->hash_forward_render && c->volume_kind != NUI_VOLUME_HASH)
+    return why = "forward rendering needs a voxel-hash volume", false;
   if (c->voxel_shift > 0) {
     if (c->volume_kind != NUI_VOLUME_DENSE) return why = "a shifting volume must be dense", false;
     for (int i = 0; i < 3; ++i) {
@@ -383,7 +395,6 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
   d.pts_rgba = s->pts_rgba;
   d.pts_cap = s->pts_xyz ? c.shift_point_cap : 0;
   d.ts = s->ts;
-  d.partials = s->partials;
   // colour tracking runs on frames that carry colour, once its buffers exist
   d.photo_w = (bgra && s->cgx[0] && s->cprev) ? s->cfg.photometric_weight : 0.f;
   d.cprev = s->cprev;
@@ -426,6 +437,11 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
     d.vis_ids = s->vis_ids;
     d.blk = s->blk;
     d.range = s->range;
+    d.fwd = c.hash_forward_render;
+    d.fwd_owner = s->fwd_owner;
+    d.fwd_ids = s->fwd_ids;
+    d.fwd_blk = s->fwd_blk;
+    d.fwd_col = s->fwd_col;
   }
 }
 
@@ -479,12 +495,6 @@ void plan_merge(BatchPlan& a, const BatchPlan& b) {
 unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
 unsigned dense_n(const BatchPlan& p) { return (unsigned)(p.n - p.hashTail); }
 
-// ICP partial-sum slots of a session (the block count at the smallest pixels per thread,
-// twice with the photometric blocks)
-size_t icp_partial_bytes(const nui_session_cfg& c) {
-  const size_t N = (size_t)c.width * c.height, per = 256 * kMinIcpPpt;
-  return ((N + per - 1) / per) * kIcpTerms * sizeof(float2) * (c.photometric_weight > 0.f ? 2 : 1);
-}
 
 
 template <int F>
@@ -516,6 +526,11 @@ template <int F>
 void launch_raycast(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   if (!(p.fmtMask & (1 << F))) return;
   const int tw = p.tune.raycast_tile_width;
+  if (F >= NUI_TSDF_F16_U8) {  // tolerance mode
+    k_raycast_fast<F><<<dim3(ray_blocks(p, tw), dense_n(p)), 128, 0, st>>>(d, tw);
+    k_raycast_finish_fast<F><<<dim3(cdiv((long)p.maxW * p.maxH, 256), dense_n(p)), 256, 0, st>>>(d);
+    return;
+  }
   k_raycast<F><<<dim3(ray_blocks(p, tw), dense_n(p)), 128, 0, st>>>(d, tw);
   k_raycast_finish<F><<<dim3(cdiv((long)p.maxW * p.maxH, 256), dense_n(p)), 256, 0, st>>>(d);
 }
@@ -609,17 +624,14 @@ void launch_track(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, flo
                   bool tick = true) {
   const unsigned npix = cdiv((long)p.maxW * p.maxH, 256);
   if (p.colorIcp) k_color_grad<<<dim3(npix, p.n, 1), 256, 0, st>>>(d);  // finest level
-  const int ppt = p.tune.icp_pixels_per_thread, per = 256 * ppt;
-  for (int l = p.maxLevels - 1; l >= 0; --l) {
-    const unsigned nb = cdiv((long)(p.maxW >> l) * (p.maxH >> l), per) +
-                        (l == 0 && p.colorIcp ? cdiv((long)p.maxW * p.maxH, per) : 0);
-    for (int it = 0; it < p.maxIters[l]; ++it) {
-      if (ppt == 2) k_icp<2><<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
-      else if (ppt == 8) k_icp<8><<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
-      else if (ppt == 16) k_icp<16><<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
-      else k_icp<4><<<dim3(nb, p.n), 256, 0, st>>>(d, l, it);
-    }
-  }
+  // every level and iteration of every session in one launch: a cluster of kIcpCluster
+  // blocks per session
+  const int ppt = p.tune.icp_pixels_per_thread;
+  const dim3 grid(kIcpCluster, p.n);
+  if (ppt == 2) k_icp_cluster<2><<<grid, 256, 0, st>>>(d);
+  else if (ppt == 8) k_icp_cluster<8><<<grid, 256, 0, st>>>(d);
+  else if (ppt == 16) k_icp_cluster<16><<<grid, 256, 0, st>>>(d);
+  else k_icp_cluster<4><<<grid, 256, 0, st>>>(d);
   k_track_finalize<<<p.n, 32, 0, st>>>(d, tick ? 1 : 0);
   k_publish<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n, d_pose, d_status);
   if (p.colorIcp) k_color_keep<<<dim3(npix, p.n), 256, 0, st>>>(d);
@@ -652,9 +664,12 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
     cudaEventRecord(ctx->fork_ev, st);
     cudaStreamWaitEvent(hs, ctx->fork_ev, 0);
   }
+  if (ev) ctx->side_timed = fork;
   if (fork) {
+    if (ev) cudaEventRecord(ctx->ev[9], hs);
     launch_hash_integrate(p, d, hs);
     launch_hash_raycast(p, d, hs);
+    if (ev) cudaEventRecord(ctx->ev[10], hs);
   }
   launch_shift(p, d, st);
   launch_integrate<0>(p, d, st);
@@ -665,10 +680,12 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
   launch_summaries(p, d, st, 0);
   if (!fork) launch_hash_integrate(p, d, st);
   mark(5);
+  mark(7);
   launch_raycast<0>(p, d, st);
   launch_raycast<1>(p, d, st);
   launch_raycast<2>(p, d, st);
   launch_raycast<3>(p, d, st);
+  mark(8);
   if (fork) {
     cudaEventRecord(ctx->join_ev, hs);
     cudaStreamWaitEvent(st, ctx->join_ev, 0);
@@ -703,9 +720,13 @@ nui_status ensure_cap(nui_ctx* ctx, int n) {
 
 nui_status finish_timing(nui_ctx* ctx) {
   if (!ctx->timing) return NUI_OK;
-  NUI_CUDA(cudaEventSynchronize(ctx->ev[kStages - 1]));
-  for (int i = 0; i < kStages - 1; ++i) cudaEventElapsedTime(&ctx->stage_ms[i], ctx->ev[i], ctx->ev[i + 1]);
-  cudaEventElapsedTime(&ctx->stage_ms[kStages - 1], ctx->ev[0], ctx->ev[kStages - 1]);
+  NUI_CUDA(cudaEventSynchronize(ctx->ev[6]));
+  for (int i = 0; i < 6; ++i) cudaEventElapsedTime(&ctx->stage_ms[i], ctx->ev[i], ctx->ev[i + 1]);
+  cudaEventElapsedTime(&ctx->stage_ms[6], ctx->ev[0], ctx->ev[6]);
+  if (cudaEventElapsedTime(&ctx->stage_ms[7], ctx->ev[7], ctx->ev[8]) != cudaSuccess) ctx->stage_ms[7] = 0.f;
+  if (!ctx->side_timed || cudaEventElapsedTime(&ctx->stage_ms[8], ctx->ev[9], ctx->ev[10]) != cudaSuccess)
+    ctx->stage_ms[8] = 0.f;
+  cudaGetLastError();
   return NUI_OK;
 }
 
@@ -943,7 +964,7 @@ NUI_API nui_status nui_ctx_create(int device, nui_ctx** out) {
     return fail(NUI_ERR_DEVICE, cudaGetErrorString(e));
   }
   c->stream = c->own;
-  for (int i = 0; i < kStages; ++i) cudaEventCreate(&c->ev[i]);
+  for (int i = 0; i < kEvents; ++i) cudaEventCreate(&c->ev[i]);
   if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess) {
@@ -966,7 +987,7 @@ NUI_API nui_status nui_ctx_destroy(nui_ctx* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
-  for (int i = 0; i < kStages; ++i) cudaEventDestroy(c->ev[i]);
+  for (int i = 0; i < kEvents; ++i) cudaEventDestroy(c->ev[i]);
   cudaFree(c->d_descs);
   cudaFreeHost(c->h_descs);
   cudaFree(c->d_pose);
@@ -1080,7 +1101,7 @@ NUI_API nui_status nui_ctx_autotune(nui_ctx* c, const nui_session_cfg* cfgs, int
     for (int r = 0; r < repeats && st == NUI_OK; ++r) {
       st = tick(f++);
       t.push_back(c->stage_ms[stage]);
-      w.push_back(c->stage_ms[kStages - 1]);
+      w.push_back(c->stage_ms[6]);
     }
     if (st != NUI_OK) return 0.f;
     std::sort(t.begin(), t.end());
@@ -1109,7 +1130,7 @@ NUI_API nui_status nui_ctx_autotune(nui_ctx* c, const nui_session_cfg* cfgs, int
   float tick_ms = 0.f;
   if (st == NUI_OK) {
     c->tune = best;
-    measure(kStages - 1, &tick_ms);
+    measure(6, &tick_ms);
   }
   const std::string why = g_err;
   c->timing = timing;
@@ -1135,7 +1156,7 @@ NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
   const size_t N = (size_t)c->width * c->height;
   size_t b = N * 2 + N * 4 /*bgra*/ + N * 4 /*scaled*/ + N * 16 * 2 /*ref maps*/ + N * 4 /*cmap*/;
   for (int l = 0; l < c->levels; ++l) b += (N >> (2 * l)) * 4;
-  b += sizeof(TrackState) + sizeof(SessionDesc) + icp_partial_bytes(*c);
+  b += sizeof(TrackState) + sizeof(SessionDesc);
   b += (N / (kTile * kTile) + 64) * 4;
   if (c->volume_kind == NUI_VOLUME_HASH) {
     const size_t ne = (size_t)c->hash_buckets + c->hash_excess, nv = (size_t)c->hash_pool_blocks * 512;
@@ -1143,6 +1164,7 @@ NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
          (size_t)c->hash_excess * 4 + N * 8;
     b += nv * ((c->tsdf_format == NUI_TSDF_I16 ? 2 : 2) + 1 + (c->color_volume ? 4 : 0));
     if (c->hash_swapping) b += ne * 5 + 2 * 4096 * 4;  // the store itself is host memory
+    if (c->hash_forward_render) b += N * (4 + 4 + (c->color_volume ? 4 : 0)) + ((N + 1023) / 1024 + 1) * 4;
     return b;
   }
   const size_t nv = (size_t)c->res[0] * c->res[1] * c->res[2];
@@ -1200,7 +1222,6 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
   s->hash = c.volume_kind == NUI_VOLUME_HASH;
   bool ok = alloc((void**)&s->raw, N * 2) && alloc((void**)&s->dscaled, N * 4) && alloc((void**)&s->vref, N * 16) &&
             alloc((void**)&s->nref, N * 16) && alloc((void**)&s->ts, sizeof(TrackState)) &&
-            alloc((void**)&s->partials, icp_partial_bytes(c)) &&
             alloc((void**)&s->d_desc1, sizeof(SessionDesc));
   for (int l = 0; ok && l < c.levels; ++l)
     ok = alloc((void**)&s->dlev[l], (N >> (2 * l)) * 4);
@@ -1215,6 +1236,10 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
          alloc((void**)&s->keys, ne * 8) && alloc((void**)&s->vis_ids, ne * 4) &&
          alloc((void**)&s->blk, ((ne + 1023) / 1024) * 16) && alloc((void**)&s->range, N * 8);
     if (ok && c.color_volume) ok = alloc((void**)&s->hrgb, hv * 4) && alloc((void**)&s->bgra, N * 4) && alloc((void**)&s->cmap, N * 4);
+    if (ok && c.hash_forward_render)
+      ok = alloc((void**)&s->fwd_owner, N * 4) && alloc((void**)&s->fwd_ids, N * 4) &&
+           alloc((void**)&s->fwd_blk, ((N + 1023) / 1024 + 1) * 4) &&
+           (!c.color_volume || alloc((void**)&s->fwd_col, N * 4));
     if (ok && c.hash_swapping) {
       // the global cache: swap state and store slot per entry, transfer lists, and the
       // store in pinned host memory mapped into the device (one slot per entry by default)
@@ -1551,6 +1576,20 @@ NUI_API nui_status nui_point_cloud_device(nui_session* s, float* d_xyz, float* d
   NUI_CUDA(cudaMemcpyAsync(&n, counter, sizeof(n), cudaMemcpyDeviceToHost, ctx->stream));
   NUI_CUDA(cudaStreamSynchronize(ctx->stream));
   *found = n;
+  return NUI_OK;
+}
+
+NUI_API nui_status nui_session_work_counters(nui_session* s, uint64_t* out) {
+  if (!s || !out) return fail(NUI_ERR_INVALID_ARG, "null argument");
+  NUI_CUDA(cudaStreamSynchronize(s->ctx->stream));
+  TrackState t;
+  NUI_CUDA(cudaMemcpy(&t, s->ts, sizeof(t), cudaMemcpyDeviceToHost));
+  out[0] = t.touched;
+  out[1] = t.bricks;
+  out[2] = t.ray_reads;
+  out[3] = t.ray_samples;
+  out[4] = t.ray_hits;
+  for (int l = 0; l < kMaxLevels; ++l) out[5 + l] = t.icp_iters[l];
   return NUI_OK;
 }
 

@@ -1190,6 +1190,7 @@ struct OrcEngineCfg {
   float shift_basis[3];      // NuiKinfuVolumeConfig::translateBasis
   long point_cap;            // points kept of the slabs that leave the shifting volume
   int swapping;              // hash scene: the global cache (NuiHashingSDFConfig::m_bUseSwapping)
+  int forward_render;        // hash scene: ForwardRender instead of the full raycast (m_bUseForwardRender)
 };
 
 struct OrcHash;
@@ -1357,10 +1358,19 @@ static void engine_integrate(OrcEngine* e, const uint8_t* col) {
 }
 
 // NuiKinfuScene::raycastRender into the reference maps.
+ORC_API long orc_hash_forward_render(OrcHash* h, const OrcCam* cam, const OrcXform* m, const float* vprev,
+                                     const uint8_t* cprev, float* vmap, float* nmap, uint8_t* cmap, float* range_out,
+                                     uint8_t* missing_out, int mode);
 static void engine_raycast(OrcEngine* e) {
   const OrcEngineCfg& c = e->c;
   if (e->hs) {
-    orc_hash_scene_raycast(e->hs, &e->cam, &e->xf, e->vref.data(), e->nref.data(), nullptr);
+    if (c.forward_render) {  // from the previous maps (a copy: the render rewrites vref)
+      const std::vector<float> vprev = e->vref;
+      orc_hash_forward_render(e->hs, &e->cam, &e->xf, vprev.data(), nullptr, e->vref.data(), e->nref.data(), nullptr,
+                              nullptr, nullptr, c.forward_render);
+    } else {
+      orc_hash_scene_raycast(e->hs, &e->cam, &e->xf, e->vref.data(), e->nref.data(), nullptr);
+    }
     return;
   }
   int w[3];
@@ -1873,12 +1883,13 @@ static float hash_read_sdf(const OrcHash* h, int x, int y, int z) {
   return bi < 0 ? 1.0f : (float)h->sdf[bi] / 32767.0f;
 }
 
-ORC_API void orc_hash_raycast(OrcHash* h, const OrcCam* cam, const OrcXform* m, float* vmap, float* nmap,
-                              uint8_t* cmap, float* range_out) {
+// CreateExpectedDepths (project_minmax_depths_kernel, KinfuHashRaycast.cl:4-76) over the
+// visible list: per pixel (min, max) camera depth of the visible blocks that cover it.
+static void hash_expected_range(const OrcHash* h, const OrcCam* cam, const OrcXform* m, std::vector<float>& rg) {
   const OrcHashCfg& c = h->c;
   const int W = (int)cam->W, H = (int)cam->H;
   const long N = (long)W * H;
-  std::vector<float> rg(2 * N);
+  rg.assign(2 * N, 0.f);
   for (long i = 0; i < N; ++i) {
     rg[2 * i] = 999999.9f;
     rg[2 * i + 1] = 0.05f;
@@ -1914,12 +1925,18 @@ ORC_API void orc_hash_raycast(OrcHash* h, const OrcCam* cam, const OrcXform* m, 
         rg[2 * li + 1] = std::fmax(rg[2 * li + 1], zy);
       }
   }
-  if (range_out) std::memcpy(range_out, rg.data(), sizeof(float) * 2 * N);
+}
+
+// castRay (KinfuHashRaycast.cl:155-452) of pixel (px, py) over its expected range: writes the
+// world vertex (and, when nmap is given, the normal) and the colour of the pixel.
+static void hash_cast_ray(const OrcHash* h, const OrcCam* cam, const OrcXform* m, const float* rg, int px, int py,
+                          float* vmap, float* nmap, uint8_t* cmap) {
+  const OrcHashCfg& c = h->c;
+  const int W = (int)cam->W;
   const float oov = 1.0f / c.voxel;
   const float stepScale = c.mu * oov * 0.6f;
-#pragma omp parallel for schedule(dynamic, 4)
-  for (int py = 0; py < H; ++py)
-    for (int px = 0; px < W; ++px) {
+  {
+    {
       const long pid = (long)py * W + px;
       f3 ps = depth_to_point(cam, px, py, rg[2 * pid]);
       float total = length3(ps) * oov;
@@ -2027,6 +2044,85 @@ ORC_API void orc_hash_raycast(OrcHash* h, const OrcCam* cam, const OrcXform* m, 
       if (nmap) st3(nmap, pid, nout);
       if (cmap) std::memcpy(cmap + 4 * pid, col, 4);
     }
+  }
+}
+
+// A18, forward rendering off (NuiKinfuOpenCLHashScene::Raycast, :659-736): every pixel.
+ORC_API void orc_hash_raycast(OrcHash* h, const OrcCam* cam, const OrcXform* m, float* vmap, float* nmap,
+                              uint8_t* cmap, float* range_out) {
+  const int W = (int)cam->W, H = (int)cam->H;
+  std::vector<float> rg;
+  hash_expected_range(h, cam, m, rg);
+  if (range_out) std::memcpy(range_out, rg.data(), sizeof(float) * 2 * (size_t)W * H);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int py = 0; py < H; ++py)
+    for (int px = 0; px < W; ++px) hash_cast_ray(h, cam, m, rg.data(), px, py, vmap, nmap, cmap);
+}
+
+// A18 with forward rendering on, the reference's default for the hash scene
+// (NuiSLAMController.cpp:47; NuiKinfuOpenCLHashScene::ForwardRender, :991-1012):
+//  1. forwardProject_kernel (KinfuHashRaycast.cl:473-506): every valid vertex p of the
+//     previous maps goes to pixel trunc(screen(transform(p) * voxel) + 0.5) -- transform is
+//     the camera-to-world transform of the current pose, applied here to a world point, as
+//     the reference writes it -- when that lies inside the image (a value in (-1, 0) truncates
+//     to 0, as the reference's float-to-uint conversion does); it carries its vertex and
+//     colour there.  Several vertices may land on one pixel: the last in raster order wins
+//     (the reference's unordered stores; its in-place colour copy is read from the previous
+//     colours here);
+//  2. findMissingPoints_kernel (:508-528): a pixel is missing when nothing landed on it and
+//     its expected range is not empty; other pixels take what landed (NaN if nothing);
+//  3. genericRaycastMissingPoints_kernel (:530-559): castRay without normals for every
+//     missing pixel, which a prefix-sum compaction lists in increasing order (the
+//     reference's compaction sizes its scan down to a power of two and loses the first
+//     index; every missing pixel is cast here);
+//  4. Vertex2Normal (:940-983): estimate_normals_simple_kernel over the new vertices, depth
+//     threshold 0.3 m.
+// vprev / cprev: the previous world vertex map (3 floats a pixel) and colours (nullable);
+// missing_out (nullable): 1 for the pixels that were cast.  Returns the missing count.
+ORC_API long orc_hash_forward_render(OrcHash* h, const OrcCam* cam, const OrcXform* m, const float* vprev,
+                                     const uint8_t* cprev, float* vmap, float* nmap, uint8_t* cmap, float* range_out,
+                                     uint8_t* missing_out, int mode) {
+  const OrcHashCfg& c = h->c;
+  const int W = (int)cam->W, H = (int)cam->H;
+  const long N = (long)W * H;
+  std::vector<float> rg;
+  hash_expected_range(h, cam, m, rg);
+  if (range_out) std::memcpy(range_out, rg.data(), sizeof(float) * 2 * N);
+  std::vector<long> owner(N, -1);
+  for (long i = 0; i < N; ++i) {
+    const f3 p = ld3(vprev, i);
+    if (isnan3(p)) continue;
+    // mode 1: the reference's expression; mode 2: the world point taken into the camera
+    const f3 q = mode == 2 ? xf_inverse(m, p) : xf_apply(m, p) * c.voxel;
+    const float u = q.x * cam->fx / q.z + cam->cx + 0.5f, v = q.y * cam->fy / q.z + cam->cy + 0.5f;
+    if (!(u > -1.0f && v > -1.0f)) continue;
+    const float tu = std::trunc(u), tv = std::trunc(v);
+    if (!(tu < (float)W && tv < (float)H)) continue;
+    owner[(long)tv * W + (long)tu] = i;
+  }
+  std::vector<uint8_t> missing(N, 0);
+  long nmiss = 0;
+  for (long t = 0; t < N; ++t) {
+    const long o = owner[t];
+    const bool empty_range = !(rg[2 * t] < rg[2 * t + 1]);
+    if (o < 0 && !empty_range) {
+      missing[t] = 1;
+      ++nmiss;
+      continue;
+    }
+    st3(vmap, t, o >= 0 ? ld3(vprev, o) : mk(QNAN, QNAN, QNAN));
+    if (cmap) {
+      if (o >= 0 && cprev) std::memcpy(cmap + 4 * t, cprev + 4 * o, 4);
+      else std::memset(cmap + 4 * t, 0, 4);
+    }
+  }
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int py = 0; py < H; ++py)
+    for (int px = 0; px < W; ++px)
+      if (missing[(long)py * W + px]) hash_cast_ray(h, cam, m, rg.data(), px, py, vmap, nullptr, cmap);
+  orc_normals(vmap, W, H, 0.3f, nmap);
+  if (missing_out) std::memcpy(missing_out, missing.data(), N);
+  return nmiss;
 }
 
 // A19: meshHashScene_kernel (KinfuHashVisualization.cl:88-271) over the visible list, in

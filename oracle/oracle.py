@@ -88,7 +88,7 @@ class OrcEngineCfg(C.Structure):
                 ("hash", C.c_int), ("voxel", C.c_float), ("mu", C.c_float), ("buckets", C.c_int), ("excess", C.c_int),
                 ("pool", C.c_int), ("max_w", C.c_int), ("photometric_weight", C.c_float),
                 ("voxel_shift", C.c_int), ("shift_basis", C.c_float * 3), ("point_cap", C.c_long),
-                ("swapping", C.c_int)]
+                ("swapping", C.c_int), ("forward_render", C.c_int)]
 
     @staticmethod
     def from_session_cfg(c):
@@ -119,6 +119,7 @@ class OrcEngineCfg(C.Structure):
         for i in range(3):
             e.shift_basis[i] = c.shift_basis[i] if hasattr(c, "shift_basis") else 0.0
         e.point_cap = getattr(c, "shift_point_cap", 0)
+        e.forward_render = getattr(c, "hash_forward_render", 0)
         e.swapping = getattr(c, "hash_swapping", 0)
         return e
 
@@ -328,6 +329,7 @@ _hash_sigs = {
     "orc_hash_allocate": (C.c_long, [_P, _P, _P, _P]),
     "orc_hash_integrate": (None, [_P, _P, _P, _P, _P, _P]),
     "orc_hash_raycast": (None, [_P, _P, _P, _P, _P, _P, _P]),
+    "orc_hash_forward_render": (C.c_long, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_int]),
     "orc_hash_mesh": (C.c_long, [_P, _P, _P, C.c_long]),
     "orc_hash_fetch_points": (C.c_long, [_P, _P, _P, C.c_long]),
     "orc_hash_visible": (C.c_long, [_P, _P, C.c_long]),
@@ -347,6 +349,7 @@ _ref_hash_sigs = {
     "ref_hash_reset": (None, [_P, _P, _P, _P, _P, _P]),
     "ref_hash_frame": (None, [_P] * 15 + [C.c_float, C.c_float, C.c_int, C.c_int]),
     "ref_hash_raycast": (None, [_P, _P, _P, C.c_int, _P, _P, C.c_float, C.c_float, _P, _P, _P, _P]),
+    "ref_hash_forward_render": (C.c_int, [_P, _P, _P, C.c_int, _P, _P, C.c_float, C.c_float, _P, _P, _P, _P, _P]),
     "ref_hash_mesh": (C.c_int, [_P, _P, _P, C.c_int, C.c_float, _P, _P]),
     "ref_hash_fetch": (C.c_int, [_P, _P, _P, C.c_int, C.c_float, C.c_float, _P, _P]),
     "ref_hash_alloc_swap": (None, [_P] * 13 + [C.c_float, C.c_float, _P]),
@@ -397,6 +400,21 @@ class OracleHash:
         rg = np.zeros(N * 2, np.float32)
         oracle().orc_hash_raycast(self.h, C.byref(cam), C.byref(xform), p(vm), p(nm), p(cm), p(rg))
         return vm, nm, cm, rg
+
+    def forward_render(self, cam, xform, vprev, cprev=None, color=False, mode=1):
+        """ForwardRender of the hash scene from the previous world vertex map (N x 3 floats) and
+        colours (N x 4 bytes): (vmap, nmap, cmap, range, missing flags, missing count)."""
+        N = cam.W * cam.H
+        vm = np.zeros(N * 3, np.float32)
+        nm = np.zeros(N * 3, np.float32)
+        cm = np.zeros(N * 4, np.uint8) if color else None
+        rg = np.zeros(N * 2, np.float32)
+        miss = np.zeros(N, np.uint8)
+        vp = np.ascontiguousarray(vprev, np.float32).reshape(-1)
+        cp = None if cprev is None else np.ascontiguousarray(cprev, np.uint8).reshape(-1)
+        n = oracle().orc_hash_forward_render(self.h, C.byref(cam), C.byref(xform), p(vp), p(cp), p(vm), p(nm), p(cm),
+                                             p(rg), p(miss), mode)
+        return vm, nm, cm, rg, miss, n
 
     def mesh(self, cap):
         pos = np.zeros((cap, 3), np.float32)
@@ -524,6 +542,20 @@ class RefHash:
         ref().ref_hash_raycast(p(self.entries), p(self.voxels), p(self.vis_ids), self.nvis.value, p(cam.flat()),
                                p(xform.flat()), self.voxel, self.mu, p(rg), p(vm), p(nm), p(cm))
         return vm, nm, cm, rg
+
+    def forward_render(self, cam, xform, vprev, cprev):
+        """The reference's ForwardRender kernels up to the normals (see the launcher):
+        (vmap, cmap, range, flags, count); vprev / cprev are copied, not modified."""
+        N = cam.W * cam.H
+        vm = np.ascontiguousarray(vprev, np.float32).reshape(-1).copy()
+        nm = np.zeros(N * 3, np.float32)
+        cm = np.ascontiguousarray(cprev, np.uint8).reshape(-1).copy()
+        rg = np.zeros(N * 2, np.float32)
+        fl = np.zeros(N, np.uint8)
+        n = ref().ref_hash_forward_render(p(self.entries), p(self.voxels), p(self.vis_ids), self.nvis.value,
+                                          p(cam.flat()), p(xform.flat()), self.voxel, self.mu, p(rg), p(vm), p(nm),
+                                          p(cm), p(fl))
+        return vm, cm, rg, fl, n
 
     def fetch(self):
         cap = 5_000_000  # MAX_OUTPUT_VERTEX_SIZE

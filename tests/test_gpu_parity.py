@@ -161,6 +161,44 @@ def test_raycast_bit_exact_on_given_volume(gpu_ctx, seq):
     assert same_bits(s.download(4)[..., :3].reshape(-1), nm)
 
 
+@pytest.mark.parametrize("fmt", [L.TSDF_F16_U8, L.TSDF_F16_F16])
+def test_fp16_raycast_within_tolerance_of_oracle(gpu_ctx, seq, fmt):
+    """Tolerance-mode raycast of the FP16 formats (direct sample parameters, arithmetic
+    empty-space jumps) on the oracle's volume at the oracle's pose: the same pixels hit the
+    surface (all but 0.1 %), and where both do, the surface points agree within 0.5 mm at
+    the 0.999 quantile and the normals within 0.05 rad at the 0.99 quantile."""
+    res = (128, 128, 128)
+    eng = O.Engine(cfg_for(res=res))
+    for d, _, _, _ in seq[:3]:
+        assert eng.frame(d)
+    s = L.Session(gpu_ctx, cfg_for(res=res, fmt=fmt))
+    s.upload_volume(eng.volume())
+    R, t = eng.pose()
+    s.set_pose(R, t)
+    s.raycast()
+    tp = eng.tsdf
+    cam = O.OrcCam.make(640, 480, 525.0, 525.0, 319.5, 239.5)
+    x = O.make_xform(R, t)
+    N = 640 * 480
+    vm, nm = np.zeros(N * 3, np.float32), np.zeros(N * 3, np.float32)
+    O.oracle().orc_raycast(O.p(eng.volume()), None, C.byref(tp), C.byref(cam), C.byref(x), 640, 480, O.p(vm),
+                           O.p(nm), None, None)
+    vg, ng = s.download(3)[..., :3].reshape(-1, 3), s.download(4)[..., :3].reshape(-1, 3)
+    vo, no = vm.reshape(-1, 3), nm.reshape(-1, 3)
+    hg, ho = ~np.isnan(vg[:, 0]), ~np.isnan(vo[:, 0])
+    assert ho.mean() > 0.5
+    assert np.mean(hg != ho) <= 1e-3, float(np.mean(hg != ho))
+    both = hg & ho
+    dist = np.linalg.norm(vg[both] - vo[both], axis=1)
+    assert np.quantile(dist, 0.999) <= 5e-4, float(np.quantile(dist, 0.999))
+    nb = both & ~np.isnan(ng[:, 0]) & ~np.isnan(no[:, 0])
+    cosang = np.clip(np.sum(ng[nb] * no[nb], axis=1), -1, 1)
+    assert np.quantile(np.arccos(cosang), 0.99) <= 0.05
+    w = s.work_counters()
+    assert w["ray_hits"] >= int(hg.sum()) and w["ray_reads"] > 0 and w["ray_samples"] >= w["ray_hits"]
+    s.close()
+
+
 def test_tracking_sequence_against_oracle(gpu_ctx, seq):
     cfg = cfg_for(res=(128, 128, 128))
     s = L.Session(gpu_ctx, cfg)
