@@ -107,10 +107,12 @@ def stream_cfg(L, i, fmt_dense, fmt_hash):
         dim = 3.0 if r == 256 else 4.0
         return L.default_cfg(res=(r, r, r), dim=(dim, dim, dim), tsdf_format=fmt_dense, trunc_dist=0.03,
                              iterations=[10, 5, 4, 0], integration_threshold=0.0)
+    # voxel-hash streams are RGB-D: colour volume and colour ICP (photometric weight 0.1)
     pool = HASH_POOLS[(i // 5 * 2 + i % 5 - 3) % len(HASH_POOLS)]
     return L.default_cfg(volume_kind=L.VOLUME_HASH, tsdf_format=fmt_hash, voxel_size=0.005, trunc_scale=0.02,
                          hash_buckets=1 << 20, hash_excess=1 << 16, hash_pool_blocks=pool,
-                         iterations=[10, 5, 4, 0], integration_threshold=0.0, depth_min=0.4)
+                         iterations=[10, 5, 4, 0], integration_threshold=0.0, depth_min=0.4,
+                         color_volume=1, photometric_weight=0.1)
 
 
 def stream_cfgs(L, n, fmt_dense, fmt_hash):
@@ -121,17 +123,17 @@ def is_hash(c):
     return c.volume_kind == 1
 
 
-def render_sequences(L, nseq, nframes, seed0=100, poses=False):
-    """nseq orbit sequences of nframes depth frames (and, with poses=True, their true
-    camera poses (R, t) in the scene frame)."""
+def render_sequences(L, nseq, nframes, seed0=100, poses=False, color=False):
+    """nseq orbit sequences of nframes depth frames (with color=True, (depth, BGRA) pairs;
+    with poses=True also their true camera poses (R, t) in the scene frame)."""
     seqs, gts = [], []
     for k in range(nseq):
         sc = L.SynthScene(L.SYNTH_TABLETOP, seed=seed0 + k, extent=3.0)
         fr, gt = [], []
         for i in range(nframes):
             R, t = sc.pose(i, radius=1.5, deg_per_frame=2.0)
-            d, _ = sc.render(R, t, W_IMG, H_IMG, frame=i, noise_seed=seed0 * 7 + k)
-            fr.append(d)
+            d, c = sc.render(R, t, W_IMG, H_IMG, frame=i, noise_seed=seed0 * 7 + k, color=color)
+            fr.append((d, np.ascontiguousarray(c)) if color else d)
             gt.append((np.asarray(R, np.float64), np.asarray(t, np.float64)))
         seqs.append(fr)
         gts.append(gt)
@@ -159,9 +161,11 @@ def run_ours(args, rank, world):
     ctx.set_stream(stream.cuda_stream)
     n = args.sessions
     nseq = min(n, args.sequences)
-    seqs, gts = render_sequences(L, nseq, SEQ_FRAMES, poses=True)
-    dev_frames = [[torch.from_numpy(f.view(np.int16)).cuda() for f in s] for s in seqs]
-    host_frames = [[torch.from_numpy(f.view(np.int16)).pin_memory() for f in s] for s in seqs]
+    seqs, gts = render_sequences(L, nseq, SEQ_FRAMES, poses=True, color=True)
+    dev_frames = [[torch.from_numpy(d.view(np.int16)).cuda() for d, _ in s] for s in seqs]
+    dev_colors = [[torch.from_numpy(c).cuda() for _, c in s] for s in seqs]
+    host_frames = [[torch.from_numpy(d.view(np.int16)).pin_memory() for d, _ in s] for s in seqs]
+    host_colors = [[torch.from_numpy(c).pin_memory() for _, c in s] for s in seqs]
     torch.cuda.synchronize()
     offs = [(i * 7) % 11 for i in range(n)]  # streams sharing a sequence start at different frames
     cfgs = stream_cfgs(L, n, L.TSDF_F16_U8, L.TSDF_F16_U8)
@@ -170,8 +174,15 @@ def run_ours(args, rank, world):
     def dframes(step):
         return [dev_frames[i % nseq][pingpong(offs[i] + step)].data_ptr() for i in range(n)]
 
+    def dcolors(step):  # BGRA for the RGB-D (voxel-hash) streams
+        return [dev_colors[i % nseq][pingpong(offs[i] + step)].data_ptr() if is_hash(cfgs[i]) else None
+                for i in range(n)]
+
     def hframe(i, step):
         return host_frames[i % nseq][pingpong(offs[i] + step)].numpy()
+
+    def hcolor(i, step):
+        return host_colors[i % nseq][pingpong(offs[i] + step)].numpy() if is_hash(cfgs[i]) else None
 
     # ---------------------------------------------------------------- launch shapes
     tuning, tune_s = None, 0.0
@@ -180,7 +191,8 @@ def run_ours(args, rank, world):
         tuning = ctx.tuning().as_dict()
     elif not args.no_autotune:
         t0 = time.perf_counter()
-        t, _ = ctx.autotune(cfgs, [[hframe(i, k) for k in range(4)] for i in range(n)], repeats=5)
+        t, _ = ctx.autotune(cfgs, [[hframe(i, k) for k in range(4)] for i in range(n)], repeats=5,
+                            bgras=[[hcolor(i, k) for k in range(4)] for i in range(n)])
         tune_s = time.perf_counter() - t0
         tuning = t.as_dict()
         torch.cuda.empty_cache()
@@ -189,7 +201,7 @@ def run_ours(args, rank, world):
     sessions = [L.Session(ctx, c) for c in cfgs]
     with ClockSampler(dev) as clk:
         for w in range(args.warmup):
-            ctx.batch_tick(sessions, dframes(w), device=True)
+            ctx.batch_tick(sessions, dframes(w), dcolors(w), device=True)
         if world > 1:
             import torch.distributed as dist
             dist.barrier()
@@ -203,7 +215,7 @@ def run_ours(args, rank, world):
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            st, _ = ctx.batch_tick(sessions, dframes(args.warmup + k), device=True)
+            st, _ = ctx.batch_tick(sessions, dframes(args.warmup + k), dcolors(args.warmup + k), device=True)
             b.record(stream)
             tick_ev.append((a, b))
             lost += int(np.sum(st != 0))
@@ -222,7 +234,8 @@ def run_ours(args, rank, world):
     reps = 3
     work = {"touched": 0, "bricks": 0, "ray_reads": 0, "ray_samples": 0, "ray_hits": 0, "icp_px": 0}
     for k in range(reps):
-        ctx.batch_tick(sessions, dframes(args.warmup + args.steps + k), device=True)
+        ctx.batch_tick(sessions, dframes(args.warmup + args.steps + k), dcolors(args.warmup + args.steps + k),
+                       device=True)
         stage += np.array([ctx.stage_ms(i) for i in range(9)])
         for s, c in zip(sessions, cfgs):
             w = s.work_counters()
@@ -265,6 +278,13 @@ def run_ours(args, rank, world):
                      "algorithmic_bytes_per_launch": int(nbytes), "launch_ms": round(float(ms), 4)})
     top = max(roof, key=lambda r: r["launch_ms"])
 
+    # ---------------------------------------------------------------- batched mixed sizes
+    mixed = mixed_batch(L, ctx, torch, args.steps, args.warmup) if args.mixed else None
+    torch.cuda.empty_cache()
+    if tuning is not None:  # the mixed batch autotuned the context for itself
+        ctx.set_tuning(L.Tuning(*[tuning[k] for k in ("integrate_threads_log2", "icp_pixels_per_thread",
+                                                       "raycast_tile_width", "hash_raycast_tile_width")]))
+
     # ---------------------------------------------------------------- ATE vs plain FP32
     ate = ate_vs_plain(L, ctx, seqs, gts, args.ate_frames, args.ate_streams) if args.ate_frames > 0 else None
     torch.cuda.empty_cache()
@@ -275,7 +295,7 @@ def run_ours(args, rank, world):
     assert all(s is not None for s in slots), "the 64 streams must fit the budget"
     for w in range(args.warmup):
         for i, sl in enumerate(slots):
-            srv.submit(sl, hframe(i, w), tag=w)
+            srv.submit(sl, hframe(i, w), hcolor(i, w), tag=w)
         srv.step()
     srv.drain()
     srv.poll()
@@ -284,7 +304,7 @@ def run_ours(args, rank, world):
     lat = []
     for k in range(args.steps):
         for i, sl in enumerate(slots):
-            srv.submit(sl, hframe(i, args.warmup + k), tag=args.warmup + k)
+            srv.submit(sl, hframe(i, args.warmup + k), hcolor(i, args.warmup + k), tag=args.warmup + k)
         srv.step()
         lat += [r.t_done - r.t_submit for r in srv.poll()]
     srv.drain()
@@ -297,7 +317,7 @@ def run_ours(args, rank, world):
     torch.cuda.empty_cache()
 
     # ---------------------------------------------------------------- serving simulation
-    sim = serving_sim(L, ctx, host_frames, args.serve_seconds, n) if args.serve_seconds > 0 else None
+    sim = serving_sim(L, ctx, host_frames, host_colors, args.serve_seconds, n) if args.serve_seconds > 0 else None
     torch.cuda.empty_cache()
 
     # ---------------------------------------------------------------- plain FP32 path
@@ -305,18 +325,18 @@ def run_ours(args, rank, world):
     if args.plain:
         plain_sessions = [L.Session(ctx, c) for c in stream_cfgs(L, n, L.TSDF_F32, L.TSDF_I16)]
         for w in range(args.warmup):
-            fr = dframes(w)
+            fr, co = dframes(w), dcolors(w)
             for i, s in enumerate(plain_sessions):
-                s.process_device(fr[i])
+                s.process_device(fr[i], co[i])
         torch.cuda.synchronize()
         p0 = torch.cuda.Event(enable_timing=True)
         p1 = torch.cuda.Event(enable_timing=True)
         psteps = max(2, min(args.steps, 10))
         p0.record(stream)
         for k in range(psteps):
-            fr = dframes(args.warmup + k)
+            fr, co = dframes(args.warmup + k), dcolors(args.warmup + k)
             for i, s in enumerate(plain_sessions):
-                s.process_device(fr[i])
+                s.process_device(fr[i], co[i])
         p1.record(stream)
         torch.cuda.synchronize()
         pms = max_over_ranks(p0.elapsed_time(p1), world)
@@ -336,7 +356,8 @@ def run_ours(args, rank, world):
             "config": {"workload": "serving-%dx640x480-dense%d-hash%d" % (n, n - n_hash, n_hash),
                        "streams_per_gpu": n,
                        "dense": "FP16 TSDF + u8 weight, %s^3 round robin" % "/".join(map(str, VOLUMES)),
-                       "hash": "5 mm voxels, 2^20 buckets, pools 2^19/2^20/2^21 blocks, half sdf + u8 weight",
+                       "hash": "RGB-D: 5 mm voxels, 2^20 buckets, pools 2^19/2^20/2^21 blocks, half sdf + u8 weight + "
+                               "RGB, colour ICP (photometric weight 0.1)",
                        "icp_iterations": [10, 5, 4], "l2": "inputs larger than L2 (volumes ~60 GB per GPU)",
                        "graph": "one CUDA graph per tick",
                        "tuning": tuning, "autotune_s": round(tune_s, 2)},
@@ -352,9 +373,11 @@ def run_ours(args, rank, world):
                  "raycast", "tick", "raycast_dense_kernels", "hash_side_stream"], stage)},
             "work_per_tick": {k: int(v) for k, v in work.items()},
             "ate": ate,
+            "batched_mixed": mixed,
             "hash_visible_blocks_mean": round(float(np.mean(hash_visible)), 1) if hash_visible else None,
             "e2e": {"value": round(e2e_value, 2), "unit": "frames/s",
-                    "h2d_bytes_per_step": n * W_IMG * H_IMG * 2, "d2h_bytes_per_step": n * (14 * 4 + 2 * 4)},
+                    "h2d_bytes_per_step": n * W_IMG * H_IMG * 2 + n_hash * W_IMG * H_IMG * 4,
+                    "d2h_bytes_per_step": n * (14 * 4 + 2 * 4)},
             "gpu_launches": kernels_per_tick * args.steps,
             "roofline": top,
             "roofline_kernels": roof,
@@ -366,7 +389,7 @@ def run_ours(args, rank, world):
     return 0
 
 
-def serving_sim(L, ctx, host_frames, seconds, n_target, warm=2.0, seed=11):
+def serving_sim(L, ctx, host_frames, host_colors, seconds, n_target, warm=2.0, seed=11):
     """Real-time run of the serving loop.  Streams arrive as a Poisson process whose rate
     keeps n_target streams live at steady state (Little's law with a mean life of 300
     frames at 30 Hz), send frames every 1/30 s +- 3 ms, and are admitted under a 150 GB
@@ -431,8 +454,10 @@ def serving_sim(L, ctx, host_frames, seconds, n_target, warm=2.0, seed=11):
             waiting.pop(0)
         for st in live.values():
             while st["sent"] < st["life"] and st["next"] <= now:
-                fr = host_frames[st["seq"]][pingpong(st["off"] + st["sent"])].numpy()
-                srv.submit(st["slot"], fr, tag=st["sent"], t_submit=st["next"])
+                fi = pingpong(st["off"] + st["sent"])
+                fr = host_frames[st["seq"]][fi].numpy()
+                co = host_colors[st["seq"]][fi].numpy() if is_hash(st["cfg"]) else None
+                srv.submit(st["slot"], fr, co, tag=st["sent"], t_submit=st["next"])
                 st["sent"] += 1
                 st["next"] += 1 / 30.0 + rng.uniform(-0.003, 0.003)
         s0 = time.perf_counter()
@@ -466,6 +491,74 @@ def serving_sim(L, ctx, host_frames, seconds, n_target, warm=2.0, seed=11):
             "admissions_over_5ms": int(sum(a > 5 for a in admit_ms))}
 
 
+def mixed_batch(L, ctx, torch, steps, warmup, seed=4):
+    """The batched configuration: 32 independent sessions, one frame each per tick, all in
+    one graphed tick; volumes drawn from {128^3, 256^3, 384^3, 512^3} as dense FP16 TSDF +
+    u8 weight or voxel hash at 5-10 mm, images from {320x240, 640x480}, each session on its
+    own seeded scene and orbit; launch shapes from the autotuner.  Reports frames/s and the
+    tick's p50 / p99 (frames already on the device; inputs larger than L2)."""
+    rng = np.random.default_rng(seed)
+    nsess, nfr = 32, 12
+    cfgs, frames_d = [], []
+    for i in range(nsess):
+        W, H = (320, 240) if rng.random() < 0.5 else (640, 480)
+        f = 525.0 * W / 640.0
+        common = dict(width=W, height=H, fx=f, fy=f, cx=(W - 1) / 2.0, cy=(H - 1) / 2.0, iterations=[10, 5, 4, 0],
+                      integration_threshold=0.0)
+        if rng.random() < 0.6:
+            r = int(rng.choice([128, 256, 384, 512]))
+            dim = 3.0 if r <= 256 else 4.0
+            c = L.default_cfg(res=(r, r, r), dim=(dim, dim, dim), tsdf_format=L.TSDF_F16_U8, trunc_dist=0.03, **common)
+        else:
+            vox = float(rng.uniform(0.005, 0.010))
+            c = L.default_cfg(volume_kind=L.VOLUME_HASH, tsdf_format=L.TSDF_F16_U8, voxel_size=vox,
+                              trunc_scale=4 * vox, hash_buckets=1 << 20, hash_excess=1 << 16,
+                              hash_pool_blocks=1 << 19, depth_min=0.4, **common)
+        cfgs.append(c)
+        sc = L.SynthScene(L.SYNTH_TABLETOP, seed=1000 + i, extent=3.0)
+        fr = []
+        for k in range(nfr):
+            R, t = sc.pose(k, radius=1.5, deg_per_frame=2.0, traj_seed=2000 + i)
+            d, _ = sc.render(R, t, W, H, fx=f, fy=f, cx=(W - 1) / 2.0, cy=(H - 1) / 2.0, frame=k, noise_seed=3000 + i)
+            fr.append(d)
+        frames_d.append(fr)
+    dev = [[torch.from_numpy(d.view(np.int16)).cuda() for d in fr] for fr in frames_d]
+    t0 = time.perf_counter()
+    tune, _ = ctx.autotune(cfgs, [fr[:4] for fr in frames_d], repeats=3)
+    tune_s = time.perf_counter() - t0
+    sessions = [L.Session(ctx, c) for c in cfgs]
+    stream = torch.cuda.current_stream()
+
+    def fptr(k):
+        return [dev[i][pingpong(k, nfr)].data_ptr() for i in range(nsess)]
+    for k in range(warmup):
+        ctx.batch_tick(sessions, fptr(k), device=True)
+    torch.cuda.synchronize()
+    ticks = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    lost = 0
+    for k in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        st, _ = ctx.batch_tick(sessions, fptr(warmup + k), device=True)
+        b.record(stream)
+        ticks.append((a, b))
+        lost += int(np.sum(st != 0))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    per = np.array([a.elapsed_time(b) for a, b in ticks])
+    kinds = {"dense": sum(not is_hash(c) for c in cfgs), "hash": sum(is_hash(c) for c in cfgs),
+             "640x480": sum(c.width == 640 for c in cfgs)}
+    for s_ in sessions:
+        s_.close()
+    return {"workload": "batched-32-mixed", "sessions": nsess, "mix": kinds, "steps": steps,
+            "frames_per_s": round(nsess * steps / (ms / 1e3), 1), "tick_ms_p50": round(float(np.percentile(per, 50)), 3),
+            "tick_ms_p99": round(float(np.percentile(per, 99)), 3), "tracking_lost": lost,
+            "kernels_per_tick": ctx.last_tick_kernels(), "tuning": tune.as_dict(), "autotune_s": round(tune_s, 2)}
+
+
 def _rel(gt, i0, i):
     """Pose i of a sequence in the camera frame of pose i0 (trackers start at identity)."""
     R0, t0 = gt[i0]
@@ -490,11 +583,12 @@ def ate_vs_plain(L, ctx, seqs, gts, nframes, nstreams):
     p16 = np.zeros((nstreams, nframes, 3))
     p32 = np.zeros((nstreams, nframes, 3))
     for k in range(nframes):
-        fr = [seqs[i % nseq][idx[i][k]] for i in range(nstreams)]
-        _, poses = ctx.batch_tick(a, fr)
+        fr = [seqs[i % nseq][idx[i][k]][0] for i in range(nstreams)]
+        co = [seqs[i % nseq][idx[i][k]][1] if is_hash(cfg16[i]) else None for i in range(nstreams)]
+        _, poses = ctx.batch_tick(a, fr, co)
         p16[:, k] = poses[:, 9:]
         for i in range(nstreams):
-            p32[i, k] = b[i].process(fr[i])[1][9:]
+            p32[i, k] = b[i].process(fr[i], co[i])[1][9:]
     for s in a + b:
         s.close()
     out = []
@@ -584,6 +678,8 @@ def main():
     ap.add_argument("--ate-frames", dest="ate_frames", type=int, default=100,
                     help="frames of the FP16-vs-plain-FP32 trajectory comparison (0: skip)")
     ap.add_argument("--ate-streams", dest="ate_streams", type=int, default=8)
+    ap.add_argument("--no-mixed", dest="mixed", action="store_false",
+                    help="skip the batched run of 32 sessions of mixed volume and image sizes")
     ap.add_argument("--no-autotune", dest="no_autotune", action="store_true",
                     help="keep the default launch shapes instead of timing the candidates first")
     ap.add_argument("--tuning", default="",

@@ -245,10 +245,10 @@ class Context:
         keep = [np.ascontiguousarray(x) for q in seqs for x in q]
         d = (C.c_void_p * (n * frames))(*[x.ctypes.data for x in keep])
         b = None
-        if bgras is not None:
-            keepc = [np.ascontiguousarray(x) for q in bgras for x in q]
-            keep += keepc
-            b = (C.c_void_p * (n * frames))(*[x.ctypes.data for x in keepc])
+        if bgras is not None:  # None entries: sessions without colour frames
+            keepc = [None if x is None else np.ascontiguousarray(x) for q in bgras for x in q]
+            keep += [x for x in keepc if x is not None]
+            b = (C.c_void_p * (n * frames))(*[None if x is None else x.ctypes.data for x in keepc])
         t, ms = Tuning(), C.c_float()
         check(lib().nui_ctx_autotune(self.h, cf, n, d, b, frames, repeats, C.byref(t), C.byref(ms)))
         return t, ms.value

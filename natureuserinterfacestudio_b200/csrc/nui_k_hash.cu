@@ -619,8 +619,10 @@ __global__ void k_hash_range(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (!s.hash || s.kind != kTrackFrame || s.ts->status != 0) return;
   const int n = s.W * s.H;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     s.range[i] = make_float2(999999.9f, 0.05f);
+    if (s.fwd) s.fwd_owner[i] = 0;
+  }
 }
 
 // project_minmax_depths_kernel (KinfuHashRaycast.cl:4-76) with atomic min / max per pixel
@@ -821,7 +823,7 @@ __device__ __forceinline__ void hash_ray(const SessionDesc& s, int pid, float3& 
 
 // The surface refinement, normal and colour of castRay / raycast_kernel
 // (KinfuHashRaycast.cl:233-471) and the map writes of pixel pid.
-template <int HF>
+template <int HF, bool NORMALS = true>
 __device__ __forceinline__ void hash_finish(HashRead<HF>& R, const SessionDesc& s, int pid, float3 pr,
                                             const float3 dir, const float stepScale, float sdfv) {
   float stepLen;
@@ -858,6 +860,11 @@ __device__ __forceinline__ void hash_finish(HashRead<HF>& R, const SessionDesc& 
     stepLen = sdfv * stepScale;
     pr = add3(pr, mul3(dir, stepLen));
     vout = w0(mul3(pr, s.voxel));
+    if (!NORMALS) {  // the forward render casts without normals (genericRaycastMissingPoints_kernel)
+      s.vref[pid] = vout;
+      if (s.cmap) s.cmap[pid] = col;
+      return;
+    }
     float p1, p2, v1;
     auto nr = [&](int dx, int dy, int dz) { return R.hood_sdf(h, ix + dx, iy + dy, iz + dz); };
     float3 g;
@@ -888,14 +895,14 @@ __device__ __forceinline__ void hash_finish(HashRead<HF>& R, const SessionDesc& 
     nout = w0(normalize3(g));
   }
   s.vref[pid] = vout;
-  s.nref[pid] = nout;
+  if (NORMALS) s.nref[pid] = nout;
   if (s.cmap) s.cmap[pid] = col;
 }
 
 template <int HF>
 __global__ void __launch_bounds__(128, 8) k_hash_raycast(const SessionDesc* __restrict__ descs, int tw) {
   const SessionDesc& s = descs[blockIdx.y];
-  if (!s.hash || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
+  if (!s.hash || s.fwd || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
   // each warp shades a tw x (32 / tw) pixel tile, a block 2 x 2 of them (neighbouring rays
   // march alike; tw is tuned)
   const int th = 32 / tw, bw = 2 * tw, bh = 2 * th;
@@ -923,7 +930,7 @@ __global__ void __launch_bounds__(128, 8) k_hash_raycast(const SessionDesc* __re
 template <int HF>
 __global__ void __launch_bounds__(256, 4) k_hash_finish(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
-  if (!s.hash || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
+  if (!s.hash || s.fwd || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
   const int pid = blockIdx.x * blockDim.x + threadIdx.x;
   if (pid >= s.W * s.H) return;
   const float4 e = s.vref[pid];
@@ -934,6 +941,182 @@ __global__ void __launch_bounds__(256, 4) k_hash_finish(const SessionDesc* __res
   hash_ray<HF>(s, pid, ps, total, totalMax, dir);
   hash_finish<HF>(R, s, pid, f3(e.x, e.y, e.z), dir, stepScale, e.w);
 }
+
+// ------------------------------------------------------------------ forward rendering
+// ForwardRender of the hash scene (NuiKinfuOpenCLHashScene.cpp:991-1012; forwardProject_kernel,
+// findMissingPoints_kernel, genericRaycastMissingPoints_kernel, KinfuHashRaycast.cl:473-559,
+// then estimate_normals_simple_kernel, normalEstimation.cl:770-822).  The previous reference
+// maps' vertices land on the pixels they project to; only pixels nothing lands on whose
+// expected range is not empty are raycast, listed in increasing order by a scan; normals are
+// recomputed from the new vertex map.  Where several vertices land on one pixel the last in
+// raster order wins (an atomic max of the source index: the reference's unordered stores
+// made deterministic); colours are read from the previous map, not from the map being
+// written (the reference copies them within one buffer).
+
+// Where each previous vertex lands (mode 1: the reference's transform(p) * voxel; mode 2:
+// the world point taken into the camera).  A coordinate in (-1, 0) truncates to pixel 0, as
+// the reference's float-to-uint conversion does.
+__global__ void __launch_bounds__(256) k_fwd_project(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!s.hash || !s.fwd || s.kind != kTrackFrame || s.ts->status != 0) return;
+  const int W = s.W, H = s.H, n = W * H;
+  const DevXform& m = s.ts->xf;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float3 p = xyz(s.vref[i]);
+    if (isnan3(p)) continue;
+    const float3 q = s.fwd == 2 ? xf_inverse(m, p) : mul3(xf_apply(m, p), s.voxel);
+    const float u = q.x * s.cam.fx / q.z + s.cam.cx + 0.5f, v = q.y * s.cam.fy / q.z + s.cam.cy + 0.5f;
+    if (!(u > -1.0f && v > -1.0f)) continue;
+    const float tu = truncf(u), tv = truncf(v);
+    if (!(tu < (float)W && tv < (float)H)) continue;
+    atomicMax(s.fwd_owner + (int)tv * W + (int)tu, i + 1);
+  }
+}
+
+__device__ __forceinline__ bool fwd_missing(const SessionDesc& s, int t, float landed_x) {
+  const float2 mm = s.range[t];
+  return isnan(landed_x) && mm.x < mm.y;
+}
+
+// Per pixel (1024 a block): the landed vertex (into nref, kept there until the commit) and
+// colour, and the block's count of missing pixels.
+__global__ void __launch_bounds__(1024) k_fwd_fill(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!s.hash || !s.fwd || s.kind != kTrackFrame || s.ts->status != 0) return;
+  const int n = s.W * s.H;
+  if ((int)blockIdx.x * 1024 >= n) return;
+  const int t = blockIdx.x * 1024 + threadIdx.x;
+  bool miss = false;
+  if (t < n) {
+    const int o = s.fwd_owner[t];
+    const float4 v = o > 0 ? s.vref[o - 1] : make_float4(qnan(), qnan(), qnan(), 0.f);
+    s.nref[t] = v;
+    if (s.cmap) s.fwd_col[t] = o > 0 ? s.cmap[o - 1] : make_uchar4(0, 0, 0, 0);
+    miss = fwd_missing(s, t, v.x);
+  }
+  const int c = __syncthreads_count(miss);
+  if (threadIdx.x == 0) s.fwd_blk[blockIdx.x] = (unsigned)c;
+}
+
+// Exclusive scan of the per-block counts (one block per session); the total goes to hcount[11].
+__global__ void __launch_bounds__(1024) k_fwd_scan(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!s.hash || !s.fwd || s.kind != kTrackFrame || s.ts->status != 0) return;
+  const int nb = (s.W * s.H + 1023) / 1024;  // <= 1024 (images up to 1M pixels)
+  __shared__ unsigned wsum[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned c = (int)threadIdx.x < nb ? s.fwd_blk[threadIdx.x] : 0u;
+  unsigned incl = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    unsigned w = wsum[lane], wi = w;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    wsum[lane] = wi - w;
+  }
+  __syncthreads();
+  const unsigned excl = wsum[warp] + incl - c;
+  if ((int)threadIdx.x < nb) s.fwd_blk[threadIdx.x] = excl;
+  if ((int)threadIdx.x == nb - 1) s.hcount[11] = (int)(excl + c);
+}
+
+// The new maps: landed vertices and colours (NaN / 0 where nothing landed), and the missing
+// pixels listed in increasing order.
+__global__ void __launch_bounds__(1024) k_fwd_commit(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!s.hash || !s.fwd || s.kind != kTrackFrame || s.ts->status != 0) return;
+  const int n = s.W * s.H;
+  if ((int)blockIdx.x * 1024 >= n) return;
+  const int t = blockIdx.x * 1024 + threadIdx.x;
+  bool miss = false;
+  if (t < n) {
+    const float4 v = s.nref[t];
+    s.vref[t] = v;
+    if (s.cmap) s.cmap[t] = s.fwd_col[t];
+    miss = fwd_missing(s, t, v.x);
+  }
+  __shared__ unsigned wsum[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned b = __ballot_sync(0xffffffffu, miss);
+  if (lane == 0) wsum[warp] = __popc(b);
+  __syncthreads();
+  unsigned before = 0;
+  for (int w = 0; w < warp; ++w) before += wsum[w];
+  if (miss) s.fwd_ids[s.fwd_blk[blockIdx.x] + before + __popc(b & ((1u << lane) - 1u))] = t;
+}
+
+// castRay of the listed pixels (genericRaycastMissingPoints_kernel): the march, its end
+// waiting in nref for the refinement.
+template <int HF>
+__global__ void __launch_bounds__(128, 8) k_fwd_raycast(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!s.hash || !s.fwd || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= s.hcount[11]) return;
+  const int pid = s.fwd_ids[k];
+  HashRead<HF> R{s, 0, 0, 0, -1};
+  const float stepScale = s.mu * (1.0f / s.voxel) * 0.6f;
+  float3 pr, dir;
+  float total, totalMax, sdfv = 1.0f;
+  hash_ray<HF>(s, pid, pr, total, totalMax, dir);
+  hash_march<HF>(R, s, pr, total, totalMax, dir, stepScale, sdfv);
+  s.nref[pid] = make_float4(pr.x, pr.y, pr.z, sdfv);
+}
+
+// The refinement and colour of the listed pixels (no normals: they follow from the map).
+template <int HF>
+__global__ void __launch_bounds__(256, 4) k_fwd_finish(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!s.hash || !s.fwd || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= s.hcount[11]) return;
+  const int pid = s.fwd_ids[k];
+  const float4 e = s.nref[pid];
+  HashRead<HF> R{s, 0, 0, 0, -1};
+  const float stepScale = s.mu * (1.0f / s.voxel) * 0.6f;
+  float3 ps, dir;
+  float total, totalMax;
+  hash_ray<HF>(s, pid, ps, total, totalMax, dir);
+  hash_finish<HF, false>(R, s, pid, f3(e.x, e.y, e.z), dir, stepScale, e.w);
+}
+
+// Vertex2Normal (NuiKinfuOpenCLHashScene.cpp:940-983): estimate_normals_simple_kernel over the
+// new world vertex map, depth threshold 0.3 m.
+__global__ void __launch_bounds__(256) k_fwd_normals(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (!s.hash || !s.fwd || s.kind != kTrackFrame || s.ts->status != 0) return;
+  const int W = s.W, H = s.H;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W * H) return;
+  const int x = i % W, y = i / W;
+  const float thr = 0.3f;
+  const float3 c = xyz(s.vref[i]);
+  if (isnan3(c)) {
+    s.nref[i] = make_float4(qnan(), qnan(), qnan(), 0.f);
+    return;
+  }
+  auto pick = [&](bool ok, int j) {
+    if (!ok) return c;
+    const float3 q = xyz(s.vref[j]);
+    if (isnan3(q) || fabsf(c.z - q.z) > thr) return c;
+    return q;
+  };
+  const float3 l = pick(x > 0, i - 1), r = pick(x < W - 1, i + 1);
+  const float3 u = pick(y > 0, i - W), d = pick(y < H - 1, i + W);
+  s.nref[i] = w0(normalize3(cross3(sub3(r, l), sub3(d, u))));
+}
+
+template __global__ void k_fwd_raycast<0>(const SessionDesc*);
+template __global__ void k_fwd_raycast<1>(const SessionDesc*);
+template __global__ void k_fwd_finish<0>(const SessionDesc*);
+template __global__ void k_fwd_finish<1>(const SessionDesc*);
 
 // ------------------------------------------------------------------ global cache
 // NuiKinfuOpenCLHashGlobalCache (NuiKinfuOpenCLHashGlobalCache.cpp:121-538) with its

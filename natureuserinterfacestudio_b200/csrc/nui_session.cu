@@ -76,6 +76,15 @@ template <int F>
 __global__ void k_hash_raycast(const SessionDesc*, int);
 template <int F>
 __global__ void k_hash_finish(const SessionDesc*);
+__global__ void k_fwd_project(const SessionDesc*);
+__global__ void k_fwd_fill(const SessionDesc*);
+__global__ void k_fwd_scan(const SessionDesc*);
+__global__ void k_fwd_commit(const SessionDesc*);
+template <int F>
+__global__ void k_fwd_raycast(const SessionDesc*);
+template <int F>
+__global__ void k_fwd_finish(const SessionDesc*);
+__global__ void k_fwd_normals(const SessionDesc*);
 __global__ void k_hash_reset(const SessionDesc*);
 __global__ void k_hash_swap_lists(const SessionDesc*);
 template <int F>
@@ -135,6 +144,13 @@ template <typename T>
 cudaError_t counted_malloc_host(T** p, size_t bytes) {
   return counted_malloc_host(reinterpret_cast<void**>(p), bytes);
 }
+// Session state comes from the context's memory pool in stream order: allocation and free
+// are queued on the context stream and never synchronise the device (a served stream can
+// join or leave while a tick runs).
+cudaError_t counted_pool_alloc(void** p, size_t bytes, cudaMemPool_t pool, cudaStream_t st) {
+  g_allocations.fetch_add(1, std::memory_order_relaxed);
+  return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
 cudaError_t counted_host_alloc(void** p, size_t bytes, unsigned flags) {
   g_allocations.fetch_add(1, std::memory_order_relaxed);
   return cudaHostAlloc(p, bytes, flags);
@@ -171,6 +187,7 @@ struct BatchPlan {
   int shiftFmtMask;         // bit per dense format of the shifting sessions
   int shiftColor;           // some shifting session has a colour volume
   int hashSwap;             // some hash session swaps blocks to the host
+  int hashFwd, hashPlain;   // some hash session renders forward / raycasts every pixel
   // descriptor ranges: a batch table lists its non-hash slots first, so the dense kernels
   // launch over the first n - hashTail descriptors and the hash kernels over the last
   // n - denseHead (0, 0: both families over the whole table)
@@ -210,6 +227,7 @@ struct nui_ctx {
   std::map<BatchPlan, Graph> graphs;
   int last_kernels = 0;  // kernels of the last graphed tick
   nui_tuning tune = {18, 4, 8, 8};
+  cudaMemPool_t pool = nullptr;  // session state (stream-ordered; freed memory stays here)
 };
 
 struct nui_session {
@@ -313,6 +331,8 @@ bool cfg_valid(const nui_session_cfg* c, std::string& why) {
   if (c->hash_forward_render < 0 || c->hash_forward_render > 2) return why = "hash forward render must be 0, 1 or 2", false;
   if (c->hash_forward_render && c->volume_kind != NUI_VOLUME_HASH)
     return why = "forward rendering needs a voxel-hash volume", false;
+  if (c->hash_forward_render && (long)c->width * c->height > 1024L * 1024L)
+    return why = "forward rendering: images up to 2^20 pixels", false;
   if (c->voxel_shift > 0) {
     if (c->volume_kind != NUI_VOLUME_DENSE) return why = "a shifting volume must be dense", false;
     for (int i = 0; i < 3; ++i) {
@@ -456,6 +476,7 @@ void plan_add(BatchPlan& p, const nui_session* s) {
   if (s->hash) {
     p.hashMask |= 1 << (c.tsdf_format == NUI_TSDF_I16 ? 0 : 1);
     if (c.hash_swapping) p.hashSwap = 1;
+    (c.hash_forward_render ? p.hashFwd : p.hashPlain) = 1;
     p.maxHashBlk = std::max(p.maxHashBlk, ((long)c.hash_buckets + c.hash_excess + 1023) / 1024);
     return;
   }
@@ -576,11 +597,24 @@ void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d0, cudaStream_t
   const unsigned hn = (unsigned)(p.n - p.denseHead);
   k_hash_range<<<dim3(296, hn), 256, 0, st>>>(d);
   k_hash_project<<<dim3(296, hn), 256, 0, st>>>(d);
+  const unsigned px = cdiv((long)p.maxW * p.maxH, 256);
+  if (p.hashFwd) {  // forward rendering: land the previous vertices, cast the missing pixels
+    const unsigned px1k = cdiv((long)p.maxW * p.maxH, 1024), pl = cdiv((long)p.maxW * p.maxH, 128);
+    k_fwd_project<<<dim3(296, hn), 256, 0, st>>>(d);
+    k_fwd_fill<<<dim3(px1k, hn), 1024, 0, st>>>(d);
+    k_fwd_scan<<<dim3(1, hn), 1024, 0, st>>>(d);
+    k_fwd_commit<<<dim3(px1k, hn), 1024, 0, st>>>(d);
+    if (p.hashMask & 1) k_fwd_raycast<0><<<dim3(pl, hn), 128, 0, st>>>(d);
+    if (p.hashMask & 2) k_fwd_raycast<1><<<dim3(pl, hn), 128, 0, st>>>(d);
+    if (p.hashMask & 1) k_fwd_finish<0><<<dim3(px, hn), 256, 0, st>>>(d);
+    if (p.hashMask & 2) k_fwd_finish<1><<<dim3(px, hn), 256, 0, st>>>(d);
+    k_fwd_normals<<<dim3(px, hn), 256, 0, st>>>(d);
+  }
+  if (!p.hashPlain) return;
   const int tw = p.tune.hash_raycast_tile_width;
   const unsigned tiles = ray_blocks(p, tw);
   if (p.hashMask & 1) k_hash_raycast<0><<<dim3(tiles, hn), 128, 0, st>>>(d, tw);
   if (p.hashMask & 2) k_hash_raycast<1><<<dim3(tiles, hn), 128, 0, st>>>(d, tw);
-  const unsigned px = cdiv((long)p.maxW * p.maxH, 256);
   if (p.hashMask & 1) k_hash_finish<0><<<dim3(px, hn), 256, 0, st>>>(d);
   if (p.hashMask & 2) k_hash_finish<1><<<dim3(px, hn), 256, 0, st>>>(d);
 }
@@ -978,6 +1012,17 @@ NUI_API nui_status nui_ctx_create(int device, nui_ctx** out) {
     delete c;
     return fail(NUI_ERR_OOM, "context scratch");
   }
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  if (cudaMemPoolCreate(&c->pool, &props) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return fail(NUI_ERR_DEVICE, "context memory pool");
+  }
+  uint64_t keep = ~0ull;  // freed session memory stays in the pool for the next session
+  cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
   *out = c;
   return NUI_OK;
 }
@@ -1001,6 +1046,10 @@ NUI_API nui_status nui_ctx_destroy(nui_ctx* c) {
   cudaStreamDestroy(c->side);
   cudaEventDestroy(c->fork_ev);
   cudaEventDestroy(c->join_ev);
+  if (c->pool) {
+    cudaDeviceSynchronize();
+    cudaMemPoolDestroy(c->pool);
+  }
   delete c;
   return NUI_OK;
 }
@@ -1178,7 +1227,21 @@ NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
   return b;
 }
 
-NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, nui_session** out) {
+}  // extern "C"
+
+namespace {
+// Frees a session's memory in stream order (sync: wait for its stream first).
+void session_free(nui_session* s, bool sync) {
+  cudaStream_t st = s->ctx->stream;
+  if (sync) cudaStreamSynchronize(st);
+  for (void* p : s->allocs) cudaFreeAsync(p, st);
+  for (void* p : s->host_allocs) cudaFreeHost(p);
+  delete s;
+}
+
+// sync = false: the allocation and the reset are queued on the context stream and the call
+// returns at once (the serving loop admits streams this way while a tick runs).
+nui_status session_create(nui_ctx* ctx, const nui_session_cfg* cfg, nui_session** out, bool sync) {
   std::string why;
   if (!ctx || !out) return fail(NUI_ERR_INVALID_ARG, "null argument");
   if (!cfg_valid(cfg, why)) return fail(NUI_ERR_INVALID_ARG, why);
@@ -1199,7 +1262,7 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
   const size_t N = (size_t)c.width * c.height;
   const size_t nv = (size_t)c.res[0] * c.res[1] * c.res[2];
   auto alloc = [&](void** p, size_t bytes) -> bool {
-    if (counted_malloc(p, bytes) != cudaSuccess) {
+    if (counted_pool_alloc(p, bytes, ctx->pool, ctx->stream) != cudaSuccess) {
       cudaGetLastError();
       return false;
     }
@@ -1266,29 +1329,28 @@ NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, 
     ok = alloc((void**)&s->pts_xyz, (size_t)c.shift_point_cap * 12) &&
          alloc((void**)&s->pts_rgba, (size_t)c.shift_point_cap * 16);
   if (!ok) {
-    for (void* p : s->allocs) cudaFree(p);
-    for (void* p : s->host_allocs) cudaFreeHost(p);
-    delete s;
+    session_free(s, true);
     return fail(NUI_ERR_OOM, "device allocation failed");
   }
   cudaMemsetAsync(s->ts, 0, sizeof(TrackState), ctx->stream);
-  nui_status st = reset_session(s);
+  nui_status st = reset_session(s, sync);
   if (st != NUI_OK) {
-    for (void* p : s->allocs) cudaFree(p);
-    for (void* p : s->host_allocs) cudaFreeHost(p);
-    delete s;
+    session_free(s, true);
     return st;
   }
   *out = s;
   return NUI_OK;
 }
+}  // namespace
+
+extern "C" {
+NUI_API nui_status nui_session_create(nui_ctx* ctx, const nui_session_cfg* cfg, nui_session** out) {
+  return session_create(ctx, cfg, out, true);
+}
 
 NUI_API nui_status nui_session_destroy(nui_session* s) {
   if (!s) return NUI_OK;
-  cudaStreamSynchronize(s->ctx->stream);
-  for (void* p : s->allocs) cudaFree(p);
-  for (void* p : s->host_allocs) cudaFreeHost(p);
-  delete s;
+  session_free(s, true);
   return NUI_OK;
 }
 
@@ -2399,13 +2461,15 @@ NUI_API nui_status nui_server_admit(nui_server* v, const nui_session_cfg* cfg, i
       if (st != NUI_OK) return st;
     }
   if (!s) {
+    // pooled sessions of other configurations make room; frees and the new session's
+    // allocation and reset are queued on the context stream behind the tick in flight
     while (v->used + need > v->budget && !v->pool.empty()) {
-      nui_session_destroy(v->pool.front().s);
+      session_free(v->pool.front().s, false);
       v->used -= v->pool.front().bytes;
       v->pool.erase(v->pool.begin());
     }
     if (v->used + need > v->budget) return fail(NUI_ERR_OOM, "stream does not fit in the HBM budget");
-    nui_status st = nui_session_create(v->ctx, cfg, &s);
+    nui_status st = session_create(v->ctx, cfg, &s, false);
     if (st != NUI_OK) return st;
     v->used += need;
   }
@@ -2449,6 +2513,9 @@ NUI_API nui_status nui_server_reserve(nui_server* v, const nui_session_cfg* cfg,
     if (st != NUI_OK) return st;
     v->used += need;
     v->pool.push_back(nui_server::Pooled{s, need});
+    // the tick's launch shape covers the reserved kinds from now on, so that their streams
+    // join without a new graph capture
+    plan_add(v->floor, s);
   }
   return NUI_OK;
 }

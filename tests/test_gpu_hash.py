@@ -110,3 +110,69 @@ def test_hash_half_format_tracks_like_int16(gpu_ctx, orbit):
         assert np.max(np.abs(p1[9:] - p2[9:])) < 4e-3, i
     ate = [float(np.sqrt(np.mean(err[k]))) for k in (0, 1)]
     assert ate[1] <= ate[0] + 1e-3, ate
+
+
+@pytest.mark.parametrize("mode,color", [(1, False), (2, True)])
+def test_hash_forward_render_at_given_poses_bit_exact(gpu_ctx, mode, color):
+    """Forward rendering of the hash scene (hash_forward_render 1: the reference's projection,
+    2: world to camera) at the true poses of a turning camera: after every frame the vertex
+    and normal maps, the range image and (with colour) the colours of the rendered pixels
+    equal the oracle's forward render, itself pinned to the reference's kernels."""
+    from _util import oracle_preprocess
+    W, H = 320, 240
+    cfg = cfg_hash(W=W, H=H, color=color)
+    cfg.hash_forward_render = mode
+    seq = frames(5, W=W, H=H, seed=5, kind=L.SYNTH_ROOM, deg=2.0, color=color)
+    gt = relative_gt(seq)
+    s = L.Session(gpu_ctx, cfg)
+    oh = O.OracleHash(cfg.hash_buckets, cfg.hash_excess, cfg.hash_pool_blocks, voxel=cfg.voxel_size,
+                      mu=cfg.trunc_scale, max_w=cfg.hash_max_weight)
+    cam = O.OrcCam.make(W, H, cfg.fx, cfg.fy, cfg.cx, cfg.cy, cfg.depth_min, cfg.depth_max)
+    cast = 0
+    try:
+        for k, ((raw, bgra, _, _), (R, t)) in enumerate(zip(seq, gt)):
+            bgra = np.ascontiguousarray(bgra) if color else None
+            x = O.make_xform(R, t)
+            d = np.zeros(W * H, np.float32)
+            O.oracle().orc_pass_filter(O.p(raw.reshape(-1)), W * H, cfg.depth_min, cfg.depth_max, O.p(d))
+            s.upload(raw, bgra)
+            s.set_pose(R, t)
+            if k == 0:  # the first frame's maps come from its depth (UpdateBuffers)
+                s.feedback_update()
+                s.integrate()
+                oh.allocate(d, cam, x)
+                oh.integrate(d, bgra.reshape(-1) if color else None, cam, x)
+                continue
+            vprev = s.download(3)[..., :3].reshape(-1).copy()
+            cprev = s.download(8).reshape(-1).copy() if color else None
+            oh.allocate(d, cam, x)
+            oh.integrate(d, bgra.reshape(-1) if color else None, cam, x)
+            vo, no, co, rgo, miss, n = oh.forward_render(cam, x, vprev, cprev, color=color, mode=mode)
+            s.integrate()
+            s.raycast()
+            assert same_bits(s.hash_download(23).reshape(-1), rgo), k
+            vg = s.download(3)[..., :3].reshape(-1)
+            assert same_bits(vg, vo), k
+            assert same_bits(s.download(4)[..., :3].reshape(-1), no), k
+            if color:
+                ok = ~np.isnan(vo.reshape(-1, 3)[:, 0])
+                assert np.array_equal(s.download(8).reshape(-1, 4)[ok], co.reshape(-1, 4)[ok]), k
+            cast += int(n)
+        assert cast > 0
+    finally:
+        s.close()
+
+
+def test_hash_forward_render_tracks_through_the_tick(gpu_ctx, orbit):
+    """Through the batched tick, a session with the world-to-camera forward render tracks the
+    orbit like the oracle engine with the same setting (poses within 1e-4)."""
+    cfg = cfg_hash()
+    cfg.hash_forward_render = 2
+    s = L.Session(gpu_ctx, cfg)
+    eng = O.Engine(cfg)
+    for i, (d, _, _, _) in enumerate(orbit):
+        ok, pose = s.process(d)
+        assert ok and eng.frame(d), i
+        Ro, to = eng.pose()
+        assert rot_angle(pose[:9].reshape(3, 3), Ro) < 1e-4 and np.max(np.abs(pose[9:] - to)) < 1e-4, i
+    s.close()
