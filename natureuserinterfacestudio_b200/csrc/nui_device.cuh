@@ -101,6 +101,7 @@ struct SessionDesc {
   uint8_t* occ3;                  // per 128^3 region state (kSuper*, over its super-bricks)
   int max_cw;
   int zchunks;                    // integration: z chunks per column (one thread each)
+  uint8_t* fast_tiles;            // tolerance-mode integration: 32 x 8 x 8 tiles kept by the cull
   float* ztab;                    // integration: running sums shared by all columns, 2 (rz + 1)
   // shifting volume (0: fixed): shift distance in voxels, basis translation, and the point
   // cache of the slabs that leave the volume (pts_cap points of xyz / rgba floats)

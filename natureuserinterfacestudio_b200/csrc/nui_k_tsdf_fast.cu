@@ -10,15 +10,15 @@
 // with contraction on.
 //
 // Work decomposition (HBM-bound by design): the volume is cut into tiles of 32 (x) x 8 (y)
-// x 8 (z) voxels, one warp per tile, lane = x, so every row a warp touches is one
-// contiguous 64 B run of the tsdf plane and 32 B of the weight plane.  A warp first culls
-// its tile with eight lanes projecting the tile's corners: tiles entirely behind the
-// camera, projecting outside the image, or farther from the camera than the largest ray
-// depth of the pixel tiles they project to plus the truncation are skipped without a
-// memory access.  Surviving tiles run two passes over their 64 rows: the update (only
-// updated voxels are read and written), then -- for the 8^3 bricks of the tile that had
-// an update -- the brick classification that the exact path leaves to k_brick_summary
-// (every voxel of such a brick read once; the voxels just written come back from L2).
+// x 8 (z) voxels.  k_integrate_cull tests every tile on one thread: tiles entirely behind
+// the camera, projecting outside the image, or farther from the camera than the largest
+// ray depth of the pixel tiles they project to plus the truncation are dropped without a
+// memory access.  k_integrate_fast then runs the kept tiles, one warp per tile, lane = x,
+// so every row a warp touches is one contiguous 64 B run of the tsdf plane and 32 B of the
+// weight plane: the update pass over the tile's 64 rows (only updated voxels are read and
+// written), then -- for the 8^3 bricks of the tile that had an update -- the brick
+// classification that the exact path leaves to k_brick_summary (every voxel of such a
+// brick read once; the voxels just written come back from L2).
 #include "nui_device.cuh"
 
 namespace nui {
@@ -35,6 +35,84 @@ __device__ __forceinline__ void fast_load(const SessionDesc& s, size_t i, float&
   }
 }
 
+// Tile culling, one thread per tile: a tile can hold an updated voxel only if part of it
+// is in front of the camera, projects into the image, and is no farther from the camera
+// than the largest ray depth of the pixel tiles it projects to plus the truncation.  The
+// corners' camera coordinates follow from one corner and the tile's three edge vectors.
+template <int FMT>
+__global__ void __launch_bounds__(256) k_integrate_cull(const SessionDesc* __restrict__ descs) {
+  const SessionDesc& s = descs[blockIdx.y];
+  if (s.kind < 0 || s.fmt != FMT || !s.ts->integrate) return;
+  const int rx = s.res[0], ry = s.res[1], rz = s.res[2];
+  const int ntx = (rx + 31) >> 5, nty = (ry + 7) >> 3, ntz = (rz + 7) >> 3;
+  const int tile = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tile >= ntx * nty * ntz) return;
+  const DevXform& m = s.ts->xf;
+  const float* Ri = m.R_inv;
+  const float c0 = s.cell[0], c1 = s.cell[1], c2 = s.cell[2];
+  const int x0 = (tile % ntx) << 5, y0 = ((tile / ntx) % nty) << 3, z0 = (tile / (ntx * nty)) << 3;
+  const int xn = min(32, rx - x0), yn = min(8, ry - y0), zn = min(8, rz - z0);
+  const float gx = ((float)(x0 - rx / 2) + 0.5f) * c0 - m.t[0];
+  const float gy = ((float)(y0 - ry / 2) + 0.5f) * c1 - m.t[1];
+  const float gz = ((float)z0 + 0.5f) * c2 - m.t[2];
+  const float ex = (float)(xn - 1) * c0, ey = (float)(yn - 1) * c1, ez = (float)(zn - 1) * c2;
+  const float3 v0 = f3(Ri[0] * gx + Ri[1] * gy + Ri[2] * gz, Ri[3] * gx + Ri[4] * gy + Ri[5] * gz,
+                       Ri[6] * gx + Ri[7] * gy + Ri[8] * gz);
+  const float3 dx = f3(Ri[0] * ex, Ri[3] * ex, Ri[6] * ex), dy = f3(Ri[1] * ey, Ri[4] * ey, Ri[7] * ey),
+               dz = f3(Ri[2] * ez, Ri[5] * ez, Ri[8] * ez);
+  const float fx = s.cam.fx, fy = s.cam.fy, ccx = s.cam.cx, ccy = s.cam.cy;
+  const float fW = (float)s.W, fH = (float)s.H;
+  float u0 = 3.4e38f, u1 = -3.4e38f, w0 = 3.4e38f, w1 = -3.4e38f;
+  int front = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    float3 v = v0;
+    if (k & 1) v = add3(v, dx);
+    if (k & 2) v = add3(v, dy);
+    if (k & 4) v = add3(v, dz);
+    if (v.z > 1e-6f) {
+      ++front;
+      const float iz = __fdividef(1.f, v.z);
+      const float u = fx * v.x * iz + ccx, w = fy * v.y * iz + ccy;
+      u0 = fminf(u0, u);
+      u1 = fmaxf(u1, u);
+      w0 = fminf(w0, w);
+      w1 = fmaxf(w1, w);
+    }
+  }
+  bool keep = front > 0;
+  if (keep) {
+    if (front < 8) {  // straddles the camera plane: the footprint is unbounded
+      u0 = 0.f, u1 = fW - 1.f, w0 = 0.f, w1 = fH - 1.f;
+    } else {
+      u0 = fmaxf(u0 - 1.f, 0.f), u1 = fminf(u1 + 1.f, fW - 1.f);
+      w0 = fmaxf(w0 - 1.f, 0.f), w1 = fminf(w1 + 1.f, fH - 1.f);
+    }
+    keep = u0 <= u1 && w0 <= w1;
+  }
+  if (keep) {
+    // largest ray depth over the pixel tiles of the footprint (the frame's largest when the
+    // footprint spans more than 64 of them); 0 = no valid depth there
+    const int ptx = (s.W + kTile - 1) / kTile;
+    const int a0 = (int)u0 / kTile, a1 = (int)u1 / kTile, b0 = (int)w0 / kTile, b1 = (int)w1 / kTile;
+    float mx = 0.f;
+    if ((a1 - a0 + 1) * (b1 - b0 + 1) <= 64) {
+      for (int b = b0; b <= b1; ++b)
+        for (int a = a0; a <= a1; ++a) mx = fmaxf(mx, __ldg(s.tile_max + b * ptx + a));
+    } else {
+      mx = __int_as_float(s.ts->dmax_bits);
+    }
+    // nearest distance from the camera to the tile's box of voxel centres
+    const float bx = fmaxf(fmaxf(gx, -(gx + ex)), 0.f), by = fmaxf(fmaxf(gy, -(gy + ey)), 0.f),
+                bz = fmaxf(fmaxf(gz, -(gz + ez)), 0.f);
+    const float dmin = sqrtf(bx * bx + by * by + bz * bz);
+    keep = mx > 0.f && !(dmin > mx + s.trunc + 1e-3f * (1.f + dmin));
+  }
+  s.fast_tiles[tile] = keep ? 1 : 0;
+}
+
+// The tiles the cull kept: a warp reads the flags of 32 consecutive tiles and runs the ones
+// that are set, one after the other.
 template <int FMT>
 __global__ void __launch_bounds__(32 * kFastWarps) k_integrate_fast(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
@@ -52,81 +130,19 @@ __global__ void __launch_bounds__(32 * kFastWarps) k_integrate_fast(const Sessio
   const float c0 = s.cell[0], c1 = s.cell[1], c2 = s.cell[2];
   const float fx = s.cam.fx, fy = s.cam.fy, ccx = s.cam.cx, ccy = s.cam.cy;
   const int W = s.W, H = s.H;
-  const float fW = (float)W, fH = (float)H;
   const float trunc = s.trunc, tinv = 1.f / trunc;
-  const float dmax = __int_as_float(s.ts->dmax_bits);
-  const int ptx = (W + kTile - 1) / kTile;
   const float* __restrict__ depth = s.dscaled;
   const size_t slice = (size_t)rx * ry;
   const int hx = rx / 2, hy = ry / 2;
   unsigned int touched_total = 0, bricks = 0;
 
-  for (int tile = blockIdx.x * kFastWarps + (threadIdx.x >> 5); tile < ntiles; tile += nwarps) {
+  for (int g32 = (blockIdx.x * kFastWarps + (threadIdx.x >> 5)) * 32; g32 < ntiles; g32 += nwarps * 32) {
+   unsigned todo = __ballot_sync(0xffffffffu, g32 + lane < ntiles && s.fast_tiles[g32 + lane] != 0);
+   while (todo) {
+    const int tile = g32 + __ffs(todo) - 1;
+    todo &= todo - 1u;
     const int x0 = (tile % ntx) << 5, y0 = ((tile / ntx) % nty) << 3, z0 = (tile / (ntx * nty)) << 3;
     const int xn = min(32, rx - x0), yn = min(8, ry - y0), zn = min(8, rz - z0);
-    // ---- cull: the tile's corner voxel centres, relative to the camera, in camera space
-    bool skip;
-    {
-      const int cx = x0 + ((lane & 1) ? xn - 1 : 0), cy = y0 + ((lane & 2) ? yn - 1 : 0),
-                cz = z0 + ((lane & 4) ? zn - 1 : 0);
-      const float gx = ((float)(cx - hx) + 0.5f) * c0 - t0;
-      const float gy = ((float)(cy - hy) + 0.5f) * c1 - t1;
-      const float gz = ((float)cz + 0.5f) * c2 - t2;
-      const float vx = Ri[0] * gx + Ri[1] * gy + Ri[2] * gz;
-      const float vy = Ri[3] * gx + Ri[4] * gy + Ri[5] * gz;
-      const float vz = Ri[6] * gx + Ri[7] * gy + Ri[8] * gz;
-      const bool corner = lane < 8;
-      const unsigned front = __ballot_sync(0xffffffffu, corner && vz > 1e-6f) & 0xffu;
-      float u0 = 0.f, u1 = fW - 1.f, w0 = 0.f, w1 = fH - 1.f;
-      if (front == 0u) {
-        skip = true;  // the whole tile is behind the camera
-      } else {
-        if (front == 0xffu) {  // in front: the projections' bounding box bounds the tile's
-          const float iz = __fdividef(1.f, vz);
-          float ua = corner ? fx * vx * iz + ccx : 3.4e38f, ub = corner ? ua : -3.4e38f;
-          float va = corner ? fy * vy * iz + ccy : 3.4e38f, vb = corner ? va : -3.4e38f;
-#pragma unroll
-          for (int o = 1; o < 8; o <<= 1) {
-            ua = fminf(ua, __shfl_xor_sync(0xffffffffu, ua, o));
-            ub = fmaxf(ub, __shfl_xor_sync(0xffffffffu, ub, o));
-            va = fminf(va, __shfl_xor_sync(0xffffffffu, va, o));
-            vb = fmaxf(vb, __shfl_xor_sync(0xffffffffu, vb, o));
-          }
-          ua = __shfl_sync(0xffffffffu, ua, 0);
-          ub = __shfl_sync(0xffffffffu, ub, 0);
-          va = __shfl_sync(0xffffffffu, va, 0);
-          vb = __shfl_sync(0xffffffffu, vb, 0);
-          u0 = fmaxf(ua - 1.f, 0.f);
-          u1 = fminf(ub + 1.f, fW - 1.f);
-          w0 = fmaxf(va - 1.f, 0.f);
-          w1 = fminf(vb + 1.f, fH - 1.f);
-        }
-        skip = !(u0 <= u1 && w0 <= w1);
-        if (!skip) {
-          // largest ray depth over the pixel tiles of the footprint (the frame's largest
-          // when the footprint spans more than 64 of them); 0 = no valid depth there
-          const int a0 = (int)u0 / kTile, a1 = (int)u1 / kTile, b0 = (int)w0 / kTile, b1 = (int)w1 / kTile;
-          const int na = a1 - a0 + 1, nt = na * (b1 - b0 + 1);
-          float mx = 0.f;
-          if (nt <= 64) {
-            for (int k = lane; k < nt; k += 32) mx = fmaxf(mx, __ldg(s.tile_max + (b0 + k / na) * ptx + a0 + k % na));
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-          } else {
-            mx = dmax;
-          }
-          // nearest distance from the camera to the tile's box of voxel centres
-          const float bx0 = ((float)(x0 - hx) + 0.5f) * c0 - t0, bx1 = bx0 + (float)(xn - 1) * c0;
-          const float by0 = ((float)(y0 - hy) + 0.5f) * c1 - t1, by1 = by0 + (float)(yn - 1) * c1;
-          const float bz0 = ((float)z0 + 0.5f) * c2 - t2, bz1 = bz0 + (float)(zn - 1) * c2;
-          const float dx = fmaxf(fmaxf(bx0, -bx1), 0.f), dy = fmaxf(fmaxf(by0, -by1), 0.f),
-                      dz = fmaxf(fmaxf(bz0, -bz1), 0.f);
-          const float dmin = sqrtf(dx * dx + dy * dy + dz * dz);
-          skip = !(mx > 0.f) || dmin > mx + trunc + 1e-3f * (1.f + dmin);
-        }
-      }
-    }
-    if (skip) continue;
 
     // ---- update pass: rows (y, z) of the tile, four at a time, lane = x
     const int x = x0 + lane;
@@ -234,6 +250,7 @@ __global__ void __launch_bounds__(32 * kFastWarps) k_integrate_fast(const Sessio
       ++bricks;
     }
     if (lane == 0 && s.occ2) s.occ2[occ2_index(s, x0, y0, z0)] = kSuperDirty;
+   }
   }
   const unsigned int t = __reduce_add_sync(0xffffffffu, touched_total);
   const unsigned int b = __reduce_add_sync(0xffffffffu, bricks);
@@ -241,6 +258,8 @@ __global__ void __launch_bounds__(32 * kFastWarps) k_integrate_fast(const Sessio
   if (lane == 0 && b) atomicAdd(&s.ts->bricks, (unsigned long long)b);
 }
 
+template __global__ void k_integrate_cull<2>(const SessionDesc*);
+template __global__ void k_integrate_cull<3>(const SessionDesc*);
 template __global__ void k_integrate_fast<2>(const SessionDesc*);
 template __global__ void k_integrate_fast<3>(const SessionDesc*);
 

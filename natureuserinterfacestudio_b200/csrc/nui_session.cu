@@ -43,6 +43,8 @@ __global__ void k_integrate(const SessionDesc*);
 template <int F>
 __global__ void k_integrate_fast(const SessionDesc*);
 template <int F>
+__global__ void k_integrate_cull(const SessionDesc*);
+template <int F>
 __global__ void k_volume_init(const SessionDesc*);
 template <int F>
 __global__ void k_brick_summary(const SessionDesc*, int);
@@ -249,6 +251,7 @@ struct nui_session {
   uint8_t* occ = nullptr;
   uint8_t* occ2 = nullptr;
   float* ztab = nullptr;
+  uint8_t* fast_tiles = nullptr;
   uint8_t* occ3 = nullptr;
   float* tile_max = nullptr;
   TrackState* ts = nullptr;
@@ -406,6 +409,7 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
   d.occ = s->occ;
   d.occ2 = s->occ2;
   d.ztab = s->ztab;
+  d.fast_tiles = s->fast_tiles;
   d.occ3 = s->occ3;
   d.max_cw = c.max_color_weight;
   d.zchunks = pick_zchunks(s->cfg, s->ctx->tune.integrate_threads_log2);
@@ -521,8 +525,10 @@ unsigned dense_n(const BatchPlan& p) { return (unsigned)(p.n - p.hashTail); }
 template <int F>
 void launch_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   if (!(p.fmtMask & (1 << F))) return;
-  if (F >= NUI_TSDF_F16_U8) {  // tolerance mode: one warp per 32 x 8 x 8 tile, grid-stride
-    const long blocks = std::min<long>(cdiv(p.maxBricks[F], 4 * kFastWarps), 1024);
+  if (F >= NUI_TSDF_F16_U8) {  // tolerance mode: cull the 32 x 8 x 8 tiles, then a warp per kept tile
+    const long tiles = p.maxBricks[F] / 4 + 1;  // >= the tiles of any session of the format
+    k_integrate_cull<F><<<dim3(cdiv(tiles, 256), dense_n(p)), 256, 0, st>>>(d);
+    const long blocks = std::min<long>(cdiv(tiles, 32 * kFastWarps), 1024);
     k_integrate_fast<F><<<dim3((unsigned)std::max<long>(blocks, 1), dense_n(p)), 32 * kFastWarps, 0, st>>>(d);
     return;
   }
@@ -1218,6 +1224,8 @@ NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
   }
   const size_t nv = (size_t)c->res[0] * c->res[1] * c->res[2];
   b += nv * voxel_bytes(c->tsdf_format);
+  if (c->tsdf_format >= NUI_TSDF_F16_U8)  // tolerance-mode tile flags
+    b += (size_t)((c->res[0] + 31) / 32) * ((c->res[1] + 7) / 8) * ((c->res[2] + 7) / 8);
   if (c->color_volume) b += nv * 4;
   b += (size_t)((c->res[0] + 7) / 8) * ((c->res[1] + 7) / 8) * ((c->res[2] + 7) / 8);
   b += (size_t)((c->res[0] + 31) / 32) * ((c->res[1] + 31) / 32) * ((c->res[2] + 31) / 32);
@@ -1316,6 +1324,8 @@ nui_status session_create(nui_ctx* ctx, const nui_session_cfg* cfg, nui_session*
   } else {
     ok = ok && alloc((void**)&s->vol, nv * (c.tsdf_format == 2 ? 2 : voxel_bytes(c.tsdf_format)));
     if (ok && c.tsdf_format == NUI_TSDF_F16_U8) ok = alloc((void**)&s->wvol, nv);
+    if (ok && c.tsdf_format >= NUI_TSDF_F16_U8)
+      ok = alloc((void**)&s->fast_tiles, (size_t)((c.res[0] + 31) / 32) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8));
     const size_t nbricks = (size_t)((c.res[0] + 7) / 8) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8);
     const size_t nsuper = (size_t)((c.res[0] + 31) / 32) * ((c.res[1] + 31) / 32) * ((c.res[2] + 31) / 32);
     const size_t nhyper = (size_t)((c.res[0] + 127) / 128) * ((c.res[1] + 127) / 128) * ((c.res[2] + 127) / 128);
