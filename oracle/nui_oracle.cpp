@@ -985,9 +985,29 @@ struct OrcColorIcp {
 // photometric normal equations of orc_color_rows times the weight to the point-to-plane
 // ones, and the weighted |diff|^2 sum to the residual sum; the accept/reject count stays
 // the depth count.
+// The 29 sums of one iteration at level lv for the estimate (R, t); user: the caller's state.
+typedef void (*OrcIcpRowsFn)(void* user, int lv, const float* R, const float* t, double* sums29);
+static int icp_host_loop(const float* const* vlevels, const int* iters, int levels, const float* vref,
+                         const float* nref, const OrcCam* cam, const OrcXform* prev, float dist_thr, float* R,
+                         float* t, OrcIcpStats* stats, const OrcColorIcp* col, OrcIcpRowsFn rows_fn, void* user);
+
 ORC_API int orc_icp(const float* const* vlevels, const int* iters, int levels, const float* vref,
                     const float* nref, const OrcCam* cam, const OrcXform* prev, float dist_thr,
                     float* R, float* t, OrcIcpStats* stats, const OrcColorIcp* col) {
+  return icp_host_loop(vlevels, iters, levels, vref, nref, cam, prev, dist_thr, R, t, stats, col, nullptr, nullptr);
+}
+
+// The same host loop with the per-iteration sums supplied by the caller (for example the
+// reference's own icp_block_kernel + compute_sums run on the host).
+ORC_API int orc_icp_with_rows(const int* iters, int levels, const OrcCam* cam, float* R, float* t,
+                              OrcIcpStats* stats, OrcIcpRowsFn rows_fn, void* user) {
+  return icp_host_loop(nullptr, iters, levels, nullptr, nullptr, cam, nullptr, 0.f, R, t, stats, nullptr, rows_fn,
+                       user);
+}
+
+static int icp_host_loop(const float* const* vlevels, const int* iters, int levels, const float* vref,
+                         const float* nref, const OrcCam* cam, const OrcXform* prev, float dist_thr, float* R,
+                         float* t, OrcIcpStats* stats, const OrcColorIcp* col, OrcIcpRowsFn rows_fn, void* user) {
   size_t gsize = (size_t)cam->W * cam->H;  // kernelGlobalSize[0]; stale across levels
   float Rc[9], tc[3];
   std::memcpy(Rc, R, sizeof(Rc));
@@ -1005,7 +1025,10 @@ ORC_API int orc_icp(const float* const* vlevels, const int* iters, int levels, c
     const int w = (int)cam->W >> lv, h = (int)cam->H >> lv;
     for (int it = 0; it < iters[lv]; ++it) {
       double sums[29];
-      orc_icp_rows(vlevels[lv], w, h, vref, nref, cam, Rc, tc, prev, dist_thr, nullptr, sums);
+      if (rows_fn)
+        rows_fn(user, lv, Rc, tc, sums);
+      else
+        orc_icp_rows(vlevels[lv], w, h, vref, nref, cam, Rc, tc, prev, dist_thr, nullptr, sums);
       if (col && col->weight > 0.f && lv == 0) {
         double sc[29];
         orc_color_rows(col->mv, col->mc, cam, 0, col->pyr, col->gx, col->gy, Rc, tc, 0, nullptr, sc);
