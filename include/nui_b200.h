@@ -50,7 +50,11 @@ typedef enum {
 /* TSDF storage formats of the dense volume.
  * NUI_TSDF_I16 is the reference's short2 (tsdf * 32766 truncated, int16 weight;
  * tsdfVolume.cl:31-190 with utils.cl:69-79).  The others store the same running average
- * without the 16-bit quantisation. */
+ * without the 16-bit quantisation.  I16 and F32 sessions reproduce the reference's float
+ * arithmetic bit for bit; the FP16 formats (the serving formats, for dense volumes and, as
+ * half-precision sdf, voxel hashes) run tolerance-mode kernels for the bilateral filter,
+ * dense integration and dense raycast: results agree with the reference within 1e-3
+ * truncation units (TSDF) and 0.5 mm (raycast depth), not bit for bit. */
 typedef enum {
   NUI_TSDF_I16 = 0,     /* 4 B/voxel: int16 tsdf, int16 weight                 */
   NUI_TSDF_F32 = 1,     /* 8 B/voxel: float tsdf, float weight                 */

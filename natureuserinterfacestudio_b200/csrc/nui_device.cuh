@@ -91,6 +91,7 @@ struct SessionDesc {
   float* tile_max;                // per 16x16 pixel tile: largest ray-length depth (0 = none)
   // dense volume
   int fmt;                        // nui_tsdf_format
+  int tol;                        // an FP16 serving format: the tolerance-mode kernels apply
   int res[3];
   float dim[3], cell[3], trunc;
   void* vol;                      // format storage, x-fastest: x + rx*(y + ry*z)

@@ -48,6 +48,28 @@ __device__ __forceinline__ float bilateral_px(const float* t, const float* g, in
   return sd / swt;
 }
 
+// Tolerance mode (sessions in an FP16 serving format): the same taps and weights with the
+// hardware exponential (__expf) and fused multiply-adds; the filtered depth differs from the
+// reference's by the exponential's few-ulp error.
+__device__ __forceinline__ float bilateral_px_tol(const float* t, const float* g, float c, float thr, float sig) {
+  constexpr int R = 3;
+  float sd = 0.f, swt = 0.f;
+#pragma unroll
+  for (int dy = 0; dy <= 2 * R; ++dy) {
+#pragma unroll
+    for (int dx = 0; dx <= 2 * R; ++dx) {
+      const float nr = t[dy * kPreSW + dx];
+      const float diff = fabsf(c - nr);
+      if (nr > 0.0f && diff < thr) {
+        const float w = g[dy * kGW + dx] * __expf(-(diff * diff) * sig);
+        sd = __fmaf_rn(nr, w, sd);
+        swt += w;
+      }
+    }
+  }
+  return __fdividef(sd, swt);
+}
+
 __global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (s.kind < 0) return;
@@ -87,7 +109,8 @@ __global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc
     // every tap's exponent lies in [-thr^2 sigma, 0] (rounding is monotone)
     const bool fast = sig >= 0.f && thr * thr * sig <= 87.f;
     const float* t = &tile[threadIdx.y][threadIdx.x];
-    if (fast && R == 3) out = bilateral_px<3, true>(t, &gw[0][0], R, c, thr, sig);
+    if (s.tol && R == 3) out = bilateral_px_tol(t, &gw[0][0], c, thr, sig);
+    else if (fast && R == 3) out = bilateral_px<3, true>(t, &gw[0][0], R, c, thr, sig);
     else if (fast) out = bilateral_px<0, true>(t, &gw[0][0], R, c, thr, sig);
     else out = bilateral_px<0, false>(t, &gw[0][0], R, c, thr, sig);
   }

@@ -409,6 +409,7 @@ void fill_desc(const nui_session* s, SessionDesc& d, int kind, const uint16_t* r
   d.occ = s->occ;
   d.occ2 = s->occ2;
   d.ztab = s->ztab;
+  d.tol = c.tsdf_format >= NUI_TSDF_F16_U8 ? 1 : 0;
   d.fast_tiles = s->fast_tiles;
   d.occ3 = s->occ3;
   d.max_cw = c.max_color_weight;
