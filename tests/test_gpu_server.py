@@ -80,3 +80,55 @@ def test_admission_follows_the_budget(gpu_ctx):
     srv.release(a)
     assert srv.admit(cfg) is not None
     srv.close()
+
+
+def test_admission_that_evicts_a_pooled_session(gpu_ctx):
+    """A released stream's session stays pooled; a stream of another configuration that
+    needs its budget evicts it.  The eviction and the new session's allocation and reset are
+    queued on the stream behind another stream's tick in flight (stream-ordered memory, no
+    device synchronisation), and both live streams' results equal their runs alone."""
+    c1 = cfg_for(res=(128, 128, 128))
+    c2 = cfg_for(W=320, H=240, res=(96, 96, 160), fmt=L.TSDF_F16_U8)
+    s1, s2 = frames(8, W=640, H=480, seed=3), frames(5, W=320, H=240, seed=8)
+    expect = {}
+    for key, cfg, seq in (("c", c1, s1), ("b", c2, s2)):
+        alone = L.Session(gpu_ctx, cfg)
+        expect[key] = [alone.process(d)[1] for d, _, _, _ in seq]
+        alone.close()
+    need = [L.lib().nui_session_device_bytes(C.byref(c)) + c.width * c.height * 12 for c in (c1, c2)]
+    assert need[0] >= need[1] // 2
+    srv = L.Server(gpu_ctx, 2 * need[0] + need[1] // 2, max_streams=4)
+    a, c = srv.admit(c1), srv.admit(c1)
+    assert a is not None and c is not None
+    got = {"b": {}, "c": {}}
+    slots = {c: "c"}
+
+    def collect():
+        for r in srv.poll():
+            if r.slot in slots:
+                assert r.status == L.NUI_OK
+                got[slots[r.slot]][r.tag] = np.array(r.pose)
+    for i in range(3):  # both streams run; a leaves, its session is pooled
+        srv.submit(a, s1[i][0], tag=i)
+        srv.submit(c, s1[i][0], tag=i)
+        srv.step()
+        collect()
+    srv.release(a)
+    collect()
+    srv.submit(c, s1[3][0], tag=3)
+    srv.step()  # c's tick is in flight
+    b = srv.admit(c2)  # evicts a's pooled session
+    assert b is not None
+    slots[b] = "b"
+    for i in range(5):
+        srv.submit(b, s2[i][0], tag=i)
+        if 4 + i < len(s1):
+            srv.submit(c, s1[4 + i][0], tag=4 + i)
+        srv.step()
+        collect()
+    srv.drain()
+    collect()
+    for key in ("b", "c"):
+        for i, p in enumerate(expect[key]):
+            assert np.array_equal(got[key][i], p), (key, i)
+    srv.close()
