@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(256) k_integrate_cull(const SessionDesc* __res
 // The tiles the cull kept: a warp reads the flags of 32 consecutive tiles and runs the ones
 // that are set, one after the other.
 template <int FMT>
-__global__ void __launch_bounds__(32 * kFastWarps) k_integrate_fast(const SessionDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(32 * kFastWarps, 2) k_integrate_fast(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (s.kind < 0 || s.fmt != FMT || !s.ts->integrate) return;
   const int rx = s.res[0], ry = s.res[1], rz = s.res[2];
@@ -144,77 +144,82 @@ __global__ void __launch_bounds__(32 * kFastWarps) k_integrate_fast(const Sessio
     const int x0 = (tile % ntx) << 5, y0 = ((tile / ntx) % nty) << 3, z0 = (tile / (ntx * nty)) << 3;
     const int xn = min(32, rx - x0), yn = min(8, ry - y0), zn = min(8, rz - z0);
 
-    // ---- update pass: rows (y, z) of the tile, four at a time, lane = x
+    // ---- update pass: one z slice of the tile (8 rows, lane = x) at a time; the rows'
+    // projections first, then their 8 depth loads, then the 8 voxel loads of the rows that
+    // update, so that each phase has 8 independent loads in flight
     const int x = x0 + lane;
     const bool xin = lane < xn;
     const float gx = ((float)(x - hx) + 0.5f) * c0 - t0;
-    const float ax = Ri[0] * gx, ay = Ri[3] * gx, az = Ri[6] * gx;
+    const float gy0 = ((float)(y0 - hy) + 0.5f) * c1 - t1;
+    const float3 ey = f3(Ri[1] * c1, Ri[4] * c1, Ri[7] * c1);  // camera step of one y row
     const float gx2 = gx * gx;
     unsigned int touched = 0;  // voxels this lane updated in the tile
 #pragma unroll 1
-    for (int r0 = 0; r0 < 64; r0 += 4) {
-      float sdf[4];
-      int pix[4];
-      bool ok[4];
+    for (int zz = 0; zz < zn; ++zz) {
+      const float gz = ((float)(z0 + zz) + 0.5f) * c2 - t2;
+      float3 v = f3(Ri[0] * gx + Ri[1] * gy0 + Ri[2] * gz, Ri[3] * gx + Ri[4] * gy0 + Ri[5] * gz,
+                    Ri[6] * gx + Ri[7] * gy0 + Ri[8] * gz);
+      int pix[8];
+      unsigned in = 0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int r = r0 + q, yy = r & 7, zz = r >> 3;
-        ok[q] = false;
-        pix[q] = 0;
-        sdf[q] = 0.f;
-        if (!xin || yy >= yn || zz >= zn) continue;
-        const float gy = ((float)(y0 + yy - hy) + 0.5f) * c1 - t1;
-        const float gz = ((float)(z0 + zz) + 0.5f) * c2 - t2;
-        const float vz = az + Ri[7] * gy + Ri[8] * gz;
-        if (!(vz > 0.f)) continue;
-        const float iz = __fdividef(1.f, vz);
-        const float vx = ax + Ri[1] * gy + Ri[2] * gz;
-        const float vy = ay + Ri[4] * gy + Ri[5] * gz;
-        const int px = __float2int_rn(fx * vx * iz + ccx), py = __float2int_rn(fy * vy * iz + ccy);
-        if (px < 0 || py < 0 || px >= W || py >= H) continue;
-        const float r2 = gx2 + gy * gy + gz * gz;
-        const float Dp = __ldg(depth + py * W + px);
-        const float sd = Dp - r2 * rsqrtf(r2);
-        if (!(sd >= -trunc)) continue;  // also false for a NaN depth
-        ok[q] = true;
-        sdf[q] = sd;
-        pix[q] = py * W + px;
+      for (int yy = 0; yy < 8; ++yy) {
+        pix[yy] = 0;
+        if (xin && yy < yn && v.z > 0.f) {
+          const float iz = __fdividef(1.f, v.z);
+          const int px = __float2int_rn(fx * v.x * iz + ccx), py = __float2int_rn(fy * v.y * iz + ccy);
+          if (px >= 0 && py >= 0 && px < W && py < H) {
+            pix[yy] = py * W + px;
+            in |= 1u << yy;
+          }
+        }
+        v = add3(v, ey);
       }
-      size_t idx[4];
-      float F[4];
-      int Wt[4];
+      float sdf[8];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int r = r0 + q;
-        idx[q] = (size_t)x + (size_t)rx * (size_t)(y0 + (r & 7)) + slice * (size_t)(z0 + (r >> 3));
-        if (ok[q]) fast_load<FMT>(s, idx[q], F[q], Wt[q]);
+      for (int yy = 0; yy < 8; ++yy) sdf[yy] = (in >> yy) & 1u ? __ldg(depth + pix[yy]) : 0.f;
+      unsigned ok = 0;
+      const float gz2 = gz * gz;
+#pragma unroll
+      for (int yy = 0; yy < 8; ++yy) {
+        const float gy = gy0 + (float)yy * c1;
+        const float r2 = gx2 + gy * gy + gz2;
+        const float sd = sdf[yy] - r2 * rsqrtf(r2);
+        sdf[yy] = sd;
+        if (((in >> yy) & 1u) && sd >= -trunc) ok |= 1u << yy;  // false for a NaN depth
       }
+      const size_t zbase = (size_t)x + (size_t)rx * (size_t)y0 + slice * (size_t)(z0 + zz);
+      float F[8];
+      int Wt[8];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (!ok[q]) continue;
-        const float tsdf = fminf(1.0f, sdf[q] * tinv);
-        const float tn = __fdividef(F[q] * (float)Wt[q] + tsdf, (float)(Wt[q] + 1));
-        const int wn = min(Wt[q] + 1, 128);
+      for (int yy = 0; yy < 8; ++yy)
+        if ((ok >> yy) & 1u) fast_load<FMT>(s, zbase + (size_t)rx * yy, F[yy], Wt[yy]);
+#pragma unroll
+      for (int yy = 0; yy < 8; ++yy) {
+        if (!((ok >> yy) & 1u)) continue;
+        const size_t vi = zbase + (size_t)rx * yy;
+        const float tsdf = fminf(1.0f, sdf[yy] * tinv);
+        const float tn = __fdividef(F[yy] * (float)Wt[yy] + tsdf, (float)(Wt[yy] + 1));
+        const int wn = min(Wt[yy] + 1, 128);
         if (FMT == 2) {
-          reinterpret_cast<__half*>(s.vol)[idx[q]] = __float2half_rn(tn);
-          s.wvol[idx[q]] = (uint8_t)wn;
+          reinterpret_cast<__half*>(s.vol)[vi] = __float2half_rn(tn);
+          s.wvol[vi] = (uint8_t)wn;
         } else {
-          reinterpret_cast<__half2*>(s.vol)[idx[q]] = __floats2half2_rn(tn, (float)wn);
+          reinterpret_cast<__half2*>(s.vol)[vi] = __floats2half2_rn(tn, (float)wn);
         }
         touched += 1u;
-        if (s.cvol && s.bgra && fabsf(sdf[q]) < trunc) {
-          const uchar4 nc = reinterpret_cast<const uchar4*>(s.bgra)[pix[q]];
+        if (s.cvol && s.bgra && fabsf(sdf[yy]) < trunc) {
+          const uchar4 nc = reinterpret_cast<const uchar4*>(s.bgra)[pix[yy]];
           if (nc.w != 0) {
             // the reference's arithmetic exactly (no product to contract, IEEE division):
             // colours agree bit for bit wherever the same voxels are updated
-            const uchar4 vc = s.cvol[idx[q]];
+            const uchar4 vc = s.cvol[vi];
             const float den = (float)vc.w + 1.f;
             uchar4 o;
             o.x = (unsigned char)fminf(fmaxf(((float)(vc.x * vc.w) + (float)nc.x) / den, 0.f), 255.f);
             o.y = (unsigned char)fminf(fmaxf(((float)(vc.y * vc.w) + (float)nc.y) / den, 0.f), 255.f);
             o.z = (unsigned char)fminf(fmaxf(((float)(vc.z * vc.w) + (float)nc.z) / den, 0.f), 255.f);
             o.w = min((unsigned char)s.max_cw, (unsigned char)(vc.w + 1));
-            s.cvol[idx[q]] = o;
+            s.cvol[vi] = o;
           }
         }
       }
@@ -226,7 +231,7 @@ __global__ void __launch_bounds__(32 * kFastWarps) k_integrate_fast(const Sessio
     const bool mine = (upd >> (lane & ~7)) & 0xffu;
     bool weighted = false, unweighted = false, nonpos = false;
     if (mine && xin) {
-#pragma unroll 4
+#pragma unroll 8
       for (int r = 0; r < 64; ++r) {
         const int yy = r & 7, zz = r >> 3;
         if (yy >= yn || zz >= zn) continue;
