@@ -196,6 +196,7 @@ def run_ours(args, rank, world):
         tune_s = time.perf_counter() - t0
         tuning = t.as_dict()
         torch.cuda.empty_cache()
+    ctx.trim()
 
     # ---------------------------------------------------------------- value: device frames
     sessions = [L.Session(ctx, c) for c in cfgs]
@@ -251,6 +252,7 @@ def run_ours(args, rank, world):
         s.close()
     sessions = None
     torch.cuda.empty_cache()
+    ctx.trim()
 
     # rooflines of the dominant kernels, from the work the kernels counted:
     #   integration (k_integrate_fast, stage 3): updated voxels read and written (3 B each
@@ -281,6 +283,7 @@ def run_ours(args, rank, world):
     # ---------------------------------------------------------------- batched mixed sizes
     mixed = mixed_batch(L, ctx, torch, args.steps, args.warmup) if args.mixed else None
     torch.cuda.empty_cache()
+    ctx.trim()
     if tuning is not None:  # the mixed batch autotuned the context for itself
         ctx.set_tuning(L.Tuning(*[tuning[k] for k in ("integrate_threads_log2", "icp_pixels_per_thread",
                                                        "raycast_tile_width", "hash_raycast_tile_width")]))
@@ -288,6 +291,7 @@ def run_ours(args, rank, world):
     # ---------------------------------------------------------------- ATE vs plain FP32
     ate = ate_vs_plain(L, ctx, seqs, gts, args.ate_frames, args.ate_streams) if args.ate_frames > 0 else None
     torch.cuda.empty_cache()
+    ctx.trim()
 
     # ---------------------------------------------------------------- e2e: serving loop
     srv = L.Server(ctx, 150 << 30, max_streams=max(64, n))
@@ -315,10 +319,12 @@ def run_ours(args, rank, world):
     e2e_lat = np.array(lat) * 1e3
     srv.close()
     torch.cuda.empty_cache()
+    ctx.trim()
 
     # ---------------------------------------------------------------- serving simulation
     sim = serving_sim(L, ctx, host_frames, host_colors, args.serve_seconds, n) if args.serve_seconds > 0 else None
     torch.cuda.empty_cache()
+    ctx.trim()
 
     # ---------------------------------------------------------------- plain FP32 path
     plain = None

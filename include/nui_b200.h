@@ -160,6 +160,11 @@ NUI_API nui_status nui_ctx_create(int device, nui_ctx** out);
 NUI_API nui_status nui_ctx_destroy(nui_ctx* ctx);
 NUI_API nui_status nui_ctx_set_stream(nui_ctx* ctx, void* cuda_stream);
 NUI_API nui_status nui_ctx_synchronize(nui_ctx* ctx);
+/* Session memory comes from a memory pool of the context, allocated and freed in stream
+ * order (a destroyed session's memory stays in the pool for the next session, and serving
+ * admissions never synchronise the device).  nui_ctx_trim waits for the context's stream and
+ * returns the pool's unused memory to the device. */
+NUI_API nui_status nui_ctx_trim(nui_ctx* ctx);
 
 /* ---------------------------------------------------------------- sessions
  * A session holds one RGB-D stream's device state: frame pyramids, reference maps,

@@ -76,6 +76,7 @@ _SIGS = {
     "nui_ctx_destroy": (C.c_int, [_P]),
     "nui_ctx_set_stream": (C.c_int, [_P, _P]),
     "nui_ctx_synchronize": (C.c_int, [_P]),
+    "nui_ctx_trim": (C.c_int, [_P]),
     "nui_session_device_bytes": (C.c_size_t, [_P]),
     "nui_session_create": (C.c_int, [_P, _P, _P]),
     "nui_session_destroy": (C.c_int, [_P]),
@@ -188,6 +189,10 @@ class Context:
         check(lib().nui_ctx_create(device, C.byref(h)))
         self.h = h
         self._sessions = weakref.WeakSet()
+
+    def trim(self):
+        """Returns the context's unused session memory to the device."""
+        check(lib().nui_ctx_trim(self.h))
 
     def close(self):
         """Destroys the context; sessions still open on it are closed first (a session

@@ -1070,6 +1070,13 @@ NUI_API nui_status nui_ctx_set_stream(nui_ctx* c, void* stream) {
   return NUI_OK;
 }
 
+NUI_API nui_status nui_ctx_trim(nui_ctx* c) {
+  if (!c) return fail(NUI_ERR_INVALID_ARG, "null context");
+  NUI_CUDA(cudaStreamSynchronize(c->stream));
+  NUI_CUDA(cudaMemPoolTrimTo(c->pool, 0));
+  return NUI_OK;
+}
+
 NUI_API nui_status nui_ctx_synchronize(nui_ctx* c) {
   if (!c) return fail(NUI_ERR_INVALID_ARG, "null context");
   NUI_CUDA(cudaStreamSynchronize(c->stream));
@@ -2441,6 +2448,7 @@ NUI_API nui_status nui_server_destroy(nui_server* v) {
     server_free_slot_buffers(sl);
   }
   for (auto& p : v->pool) nui_session_destroy(p.s);
+  nui_ctx_trim(v->ctx);  // the served sessions' memory goes back to the device
   cudaStreamDestroy(v->up);
   cudaEventDestroy(v->ev_t0);
   cudaEventDestroy(v->ev_up);
