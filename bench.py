@@ -285,8 +285,7 @@ def run_ours(args, rank, world):
     torch.cuda.empty_cache()
     ctx.trim()
     if tuning is not None:  # the mixed batch autotuned the context for itself
-        ctx.set_tuning(L.Tuning(*[tuning[k] for k in ("integrate_threads_log2", "icp_pixels_per_thread",
-                                                       "raycast_tile_width", "hash_raycast_tile_width")]))
+        ctx.set_tuning(L.Tuning(**tuning))
 
     # ---------------------------------------------------------------- ATE vs plain FP32
     ate = ate_vs_plain(L, ctx, seqs, gts, args.ate_frames, args.ate_streams) if args.ate_frames > 0 else None
@@ -706,7 +705,7 @@ def main():
                     help="keep the default launch shapes instead of timing the candidates first")
     ap.add_argument("--tuning", default="",
                     help="launch shapes to use instead of autotuning: integration threads log2, ICP pixels "
-                         "per thread, dense and hash ray tile widths (e.g. 16,8,8,4)")
+                         "per thread, dense and hash ray tile widths, ICP blocks per session (e.g. 16,8,8,4,8)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))

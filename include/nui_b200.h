@@ -335,12 +335,14 @@ NUI_API nui_status nui_ctx_stage_ms(nui_ctx* ctx, int stage, float* ms);
 /* Kernel launches in the captured graph of the context's last graphed batch tick. */
 NUI_API nui_status nui_ctx_last_tick_kernels(nui_ctx* ctx, int* n);
 /* Launch shapes of a context's tick, chosen by nui_ctx_autotune (or set by hand).  No
- * choice changes a result bit except the ICP pixels per thread, which regroups the float
- * partial sums of the normal equations (poses agree to the rounding of those sums).
+ * choice changes a result bit except the two ICP shapes, which regroup the FP64 partial
+ * sums of the normal equations (poses agree to the rounding of those sums).
  *   integrate_threads_log2   dense integration: each volume column is split into z chunks,
  *                            one thread each, until a session's launch has >= 2^this
  *                            threads (chunks of >= 16 slices); 14..22, default 18
  *   icp_pixels_per_thread    ICP block: 256 threads x this many pixels; 2, 4, 8 or 16 (4)
+ *   icp_cluster_blocks       ICP: thread blocks of the cluster that tracks one session;
+ *                            2, 4, 8 or 16 (8; 16 is a non-portable cluster size)
  *   raycast_tile_width       dense raycast: a warp shades a tile this wide and 32 / this
  *                            high, a block 2 x 2 such tiles; 4, 8, 16 or 32 (8)
  *   hash_raycast_tile_width  the same for the voxel-hash raycast (8)
@@ -350,6 +352,7 @@ typedef struct nui_tuning {
   int icp_pixels_per_thread;
   int raycast_tile_width;
   int hash_raycast_tile_width;
+  int icp_cluster_blocks;
 } nui_tuning;
 NUI_API nui_status nui_ctx_get_tuning(nui_ctx* ctx, nui_tuning* out);
 NUI_API nui_status nui_ctx_set_tuning(nui_ctx* ctx, const nui_tuning* t);

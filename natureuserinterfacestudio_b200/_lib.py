@@ -53,8 +53,14 @@ class Tuning(C.Structure):
     """Launch shapes of a context's tick (nui_tuning)."""
     _fields_ = [
         ("integrate_threads_log2", C.c_int), ("icp_pixels_per_thread", C.c_int),
-        ("raycast_tile_width", C.c_int), ("hash_raycast_tile_width", C.c_int),
+        ("raycast_tile_width", C.c_int), ("hash_raycast_tile_width", C.c_int), ("icp_cluster_blocks", C.c_int),
     ]
+
+    def __init__(self, *args, **kw):
+        # the ICP cluster size defaults to the library's default when left out
+        super().__init__(*args, **kw)
+        if len(args) < 5 and "icp_cluster_blocks" not in kw:
+            self.icp_cluster_blocks = 8
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

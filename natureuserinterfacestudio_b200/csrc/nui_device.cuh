@@ -15,7 +15,6 @@ constexpr int kMaxRadius = 7;
 constexpr int kIcpTerms = 29;  // 21 JtJ + 6 Jtr + r^2 + count  (icp.cl:122-160)
 constexpr int kTile = 16;      // pixel tile of the depth bound used by integration culling
 constexpr int kFastWarps = 8;  // warps per block of the tolerance-mode integration
-constexpr int kIcpCluster = 4; // thread blocks (one cluster) per session of the ICP kernel
 
 // Camera intrinsics block (gpu_def.h:13-27).
 struct DevCam {

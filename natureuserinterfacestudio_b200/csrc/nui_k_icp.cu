@@ -392,8 +392,9 @@ __device__ __forceinline__ double icp_block_sum(const double (&acc)[kIcpTerms]) 
 
 // All ICP iterations of every level of one frame, one thread-block cluster per session
 // (NuiKinfuOpenCLDepthTracker::IterativeClosestPoint, NuiKinfuOpenCLDepthTracker.cpp:240-504).
-// The kIcpCluster blocks of a cluster share the level's pixels (pixel blocks b = rank,
-// rank + kIcpCluster, ...); every iteration each block reduces its FP64 sums into its own
+// The C blocks of a cluster (C = 2, 4, 8 or 16, a launch attribute: the ICP tuning's
+// blocks per session) share the level's pixels (pixel blocks b = rank, rank + C, ...);
+// every iteration each block reduces its FP64 sums into its own
 // shared memory, a cluster barrier makes them visible, block 0 adds the blocks' sums in
 // rank order through distributed shared memory and runs the host step (LM accept/reject,
 // FP64 Cholesky, pose update) on one thread, and a second barrier publishes the new
@@ -403,14 +404,14 @@ __device__ __forceinline__ double icp_block_sum(const double (&acc)[kIcpTerms]) 
 // One launch per tick replaces one launch per iteration, and sessions whose levels stop
 // early leave their SMs to the others.
 template <int PPT>
-__global__ void __cluster_dims__(kIcpCluster, 1, 1) __launch_bounds__(kIcpThreads, 2)
+__global__ void __launch_bounds__(kIcpThreads, 2)
     k_icp_cluster(const SessionDesc* __restrict__ descs) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   const SessionDesc& s = descs[blockIdx.y];
   if (s.kind != kTrackFrame) return;  // the same for every block of the cluster
   TrackState* ts = s.ts;
-  const int rank = (int)cluster.block_rank();
+  const int rank = (int)cluster.block_rank(), C = (int)cluster.num_blocks();
   __shared__ float sR[9], st[3];
   __shared__ DevXform sp;
   __shared__ double part[2][32];  // this block's depth / photometric sums
@@ -435,13 +436,13 @@ __global__ void __cluster_dims__(kIcpCluster, 1, 1) __launch_bounds__(kIcpThread
       double acc[kIcpTerms];
 #pragma unroll
       for (int k = 0; k < kIcpTerms; ++k) acc[k] = 0.0;
-      for (int vb = rank; vb < nblocks; vb += kIcpCluster) icp_depth_rows<PPT>(s, level, vb, sR, tc, sp, acc);
+      for (int vb = rank; vb < nblocks; vb += C) icp_depth_rows<PPT>(s, level, vb, sR, tc, sp, acc);
       double D = icp_block_sum(acc);
       if (threadIdx.x < kIcpTerms) part[0][threadIdx.x] = D;
       if (photo) {
 #pragma unroll
         for (int k = 0; k < kIcpTerms; ++k) acc[k] = 0.0;
-        for (int vb = rank; vb < ncb; vb += kIcpCluster) icp_color_rows<PPT>(s, vb, sR, tc, acc);
+        for (int vb = rank; vb < ncb; vb += C) icp_color_rows<PPT>(s, vb, sR, tc, acc);
         D = icp_block_sum(acc);
         if (threadIdx.x < kIcpTerms) part[1][threadIdx.x] = D;
       }
@@ -451,7 +452,7 @@ __global__ void __cluster_dims__(kIcpCluster, 1, 1) __launch_bounds__(kIcpThread
           // the blocks' sums in rank order; the photometric normal equations and residual
           // enter weighted, the count stays the depth count
           double a = 0.0, c = 0.0;
-          for (int r = 0; r < kIcpCluster; ++r) {
+          for (int r = 0; r < C; ++r) {
             const double* pr = cluster.map_shared_rank(&part[0][0], r);
             a += pr[threadIdx.x];
             if (photo) c += pr[32 + threadIdx.x];

@@ -166,7 +166,9 @@ __global__ void __launch_bounds__(32 * kFastWarps, 2) k_integrate_fast(const Ses
         pix[yy] = 0;
         if (xin && yy < yn && v.z > 0.f) {
           const float iz = __fdividef(1.f, v.z);
-          const int px = __float2int_rn(fx * v.x * iz + ccx), py = __float2int_rn(fy * v.y * iz + ccy);
+          // round half away from zero, as OpenCL's round(): ties are frequent (pixel centres
+          // and voxel centres sit on rational grids), and half-to-even would split them
+          const int px = (int)roundf(fx * v.x * iz + ccx), py = (int)roundf(fy * v.y * iz + ccy);
           if (px >= 0 && py >= 0 && px < W && py < H) {
             pix[yy] = py * W + px;
             in |= 1u << yy;

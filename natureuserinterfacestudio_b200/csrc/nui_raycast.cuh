@@ -48,9 +48,9 @@ struct RayVol {
   }
   __device__ __forceinline__ void voxel_of(float3 p, int& gx, int& gy, int& gz) const {
     if (FAST) {
-      gx = __float2int_rn(p.x * i0);
-      gy = __float2int_rn(p.y * i1);
-      gz = __float2int_rn(p.z * i2);
+      gx = (int)roundf(p.x * i0);  // half away from zero, as OpenCL's round()
+      gy = (int)roundf(p.y * i1);
+      gz = (int)roundf(p.z * i2);
     } else {
       gx = round_div(p.x, c0, i0);
       gy = round_div(p.y, c1, i1);

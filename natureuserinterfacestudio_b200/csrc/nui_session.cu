@@ -228,7 +228,7 @@ struct nui_ctx {
   };
   std::map<BatchPlan, Graph> graphs;
   int last_kernels = 0;  // kernels of the last graphed tick
-  nui_tuning tune = {18, 4, 8, 8};
+  nui_tuning tune = {18, 4, 8, 8, 8};
   cudaMemPool_t pool = nullptr;  // session state (stream-ordered; freed memory stays here)
 };
 
@@ -659,20 +659,46 @@ void launch_shift(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
   k_shift_dirty<<<dim3(kShiftBlocks, dense_n(p)), 256, 0, st>>>(d);
 }
 
+// The ICP kernel over n sessions, one cluster of cl blocks each (cl = 16 is beyond the
+// portable cluster size and needs the kernel's opt-in, given once per kernel).
+void launch_icp_cluster(void (*kern)(const SessionDesc*), const SessionDesc* d, int n, int cl, cudaStream_t st) {
+  if (cl == 16) {
+    static std::mutex mu;
+    static std::vector<const void*> opted;
+    std::lock_guard<std::mutex> lock(mu);
+    if (std::find(opted.begin(), opted.end(), (const void*)kern) == opted.end()) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      opted.push_back((const void*)kern);
+    }
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cl, n);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cl;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, d);
+}
+
 // Colour pyramid (if any session tracks with colour), the ICP iterations of every level,
 // the integration gate and the published pose.
 void launch_track(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, float* d_pose, int* d_status,
                   bool tick = true) {
   const unsigned npix = cdiv((long)p.maxW * p.maxH, 256);
   if (p.colorIcp) k_color_grad<<<dim3(npix, p.n, 1), 256, 0, st>>>(d);  // finest level
-  // every level and iteration of every session in one launch: a cluster of kIcpCluster
-  // blocks per session
+  // every level and iteration of every session in one launch: a cluster of
+  // icp_cluster_blocks blocks per session
   const int ppt = p.tune.icp_pixels_per_thread;
-  const dim3 grid(kIcpCluster, p.n);
-  if (ppt == 2) k_icp_cluster<2><<<grid, 256, 0, st>>>(d);
-  else if (ppt == 8) k_icp_cluster<8><<<grid, 256, 0, st>>>(d);
-  else if (ppt == 16) k_icp_cluster<16><<<grid, 256, 0, st>>>(d);
-  else k_icp_cluster<4><<<grid, 256, 0, st>>>(d);
+  if (ppt == 2) launch_icp_cluster(k_icp_cluster<2>, d, p.n, p.tune.icp_cluster_blocks, st);
+  else if (ppt == 8) launch_icp_cluster(k_icp_cluster<8>, d, p.n, p.tune.icp_cluster_blocks, st);
+  else if (ppt == 16) launch_icp_cluster(k_icp_cluster<16>, d, p.n, p.tune.icp_cluster_blocks, st);
+  else launch_icp_cluster(k_icp_cluster<4>, d, p.n, p.tune.icp_cluster_blocks, st);
   k_track_finalize<<<p.n, 32, 0, st>>>(d, tick ? 1 : 0);
   k_publish<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n, d_pose, d_status);
   if (p.colorIcp) k_color_keep<<<dim3(npix, p.n), 256, 0, st>>>(d);
@@ -1100,6 +1126,8 @@ bool tuning_valid(const nui_tuning& t) {
   return t.integrate_threads_log2 >= 14 && t.integrate_threads_log2 <= 22 &&
          (t.icp_pixels_per_thread == 2 || t.icp_pixels_per_thread == 4 || t.icp_pixels_per_thread == 8 ||
           t.icp_pixels_per_thread == 16) &&
+         (t.icp_cluster_blocks == 2 || t.icp_cluster_blocks == 4 || t.icp_cluster_blocks == 8 ||
+          t.icp_cluster_blocks == 16) &&
          tw_ok(t.raycast_tile_width) && tw_ok(t.hash_raycast_tile_width);
 }
 
@@ -1187,6 +1215,7 @@ NUI_API nui_status nui_ctx_autotune(nui_ctx* c, const nui_session_cfg* cfgs, int
     best.*field = pick;
   };
   if (dense) tune_one(&nui_tuning::integrate_threads_log2, {16, 17, 18, 19, 20}, 3);
+  tune_one(&nui_tuning::icp_cluster_blocks, {4, 8, 16}, 2);
   tune_one(&nui_tuning::icp_pixels_per_thread, {2, 4, 8, 16}, 2);
   if (dense) tune_one(&nui_tuning::raycast_tile_width, {4, 8, 16, 32}, 5);
   if (hash) tune_one(&nui_tuning::hash_raycast_tile_width, {4, 8, 16, 32}, 5);

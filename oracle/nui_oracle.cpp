@@ -353,6 +353,9 @@ struct RcVol {
   // the reference's trilinear neighbour addressing (buffer strides from the wrapped first
   // voxel), for pinning only; false: each neighbour wrapped on its own
   bool strides = false;
+  // TSDF values stored as floats (the FP16 serving formats, widened), one per voxel, in place
+  // of the int16 values / 32766; the weights stay those of v.  nullptr: the int16 values
+  const float* values = nullptr;
   long idx(int x, int y, int z) const {
     return ((long)((y + w[1]) % ry) * rx + (x + w[0]) % rx) * rz + (z + w[2]) % rz;
   }
@@ -370,7 +373,7 @@ inline void voxel_of(f3 p, const float* cell, int& gx, int& gy, int& gz) {
 inline bool tsdf_at(const RcVol& V, long idx, float& f) {
   if (idx < 0 || idx >= (long)V.rx * V.ry * V.rz) return false;  // strides past the buffer
   int16_t a = V.v[2 * idx], w = V.v[2 * idx + 1];
-  f = (float)a / 32766.f;
+  f = V.values ? V.values[idx] : (float)a / 32766.f;
   return w > 0;
 }
 float trilinear(f3 p, const RcVol& V) {
@@ -408,11 +411,12 @@ float trilinear(f3 p, const RcVol& V) {
 // from the wrapped first voxel (raycast.cl:62-108), so that a read straddling the wrap seam
 // takes voxels of the next buffer row as the reference does; used to pin the rest of this
 // function against the reference.  0: each neighbour is the voxel's true neighbour.
-ORC_API void orc_raycast_wrap_mode(const int16_t* vol, const uint8_t* cvol, const OrcTsdf* p, const OrcCam* cam,
-                                   const OrcXform* m, int W, int H, float* vmap, float* nmap, uint8_t* cmap,
-                                   long* steps_out, const int* wrap, int ref_strides) {
+namespace {
+void raycast_impl(const int16_t* vol, const float* values, const uint8_t* cvol, const OrcTsdf* p, const OrcCam* cam,
+                  const OrcXform* m, int W, int H, float* vmap, float* nmap, uint8_t* cmap, long* steps_out,
+                  const int* wrap, int ref_strides) {
   RcVol V{vol, (int)p->res[0], (int)p->res[1], (int)p->res[2], {p->cell[0], p->cell[1], p->cell[2]},
-          {wrap ? wrap[0] : 0, wrap ? wrap[1] : 0, wrap ? wrap[2] : 0}, ref_strides != 0};
+          {wrap ? wrap[0] : 0, wrap ? wrap[1] : 0, wrap ? wrap[2] : 0}, ref_strides != 0, values};
   const f3 off = mk(p->dim[0] / 2.0f, p->dim[1] / 2.0f, 0.f);
   const f3 r0 = mk(m->R[0], m->R[1], m->R[2]), r1 = mk(m->R[3], m->R[4], m->R[5]),
            r2 = mk(m->R[6], m->R[7], m->R[8]), t = mk(m->t[0], m->t[1], m->t[2]);
@@ -488,6 +492,21 @@ ORC_API void orc_raycast_wrap_mode(const int16_t* vol, const uint8_t* cvol, cons
       }
     }
   if (steps_out) *steps_out = steps_total;
+}
+}  // namespace
+
+ORC_API void orc_raycast_wrap_mode(const int16_t* vol, const uint8_t* cvol, const OrcTsdf* p, const OrcCam* cam,
+                                   const OrcXform* m, int W, int H, float* vmap, float* nmap, uint8_t* cmap,
+                                   long* steps_out, const int* wrap, int ref_strides) {
+  raycast_impl(vol, nullptr, cvol, p, cam, m, W, H, vmap, nmap, cmap, steps_out, wrap, ref_strides);
+}
+
+// The same raycast over TSDF values given as floats (one per voxel, reference layout) with
+// the weights of vol: the reference's march and refinement applied to the values a
+// half-precision volume stores.
+ORC_API void orc_raycast_values(const int16_t* vol, const float* values, const OrcTsdf* p, const OrcCam* cam,
+                                const OrcXform* m, int W, int H, float* vmap, float* nmap) {
+  raycast_impl(vol, values, nullptr, p, cam, m, W, H, vmap, nmap, nullptr, nullptr, nullptr, 0);
 }
 
 ORC_API void orc_raycast_wrap(const int16_t* vol, const uint8_t* cvol, const OrcTsdf* p, const OrcCam* cam,

@@ -150,6 +150,7 @@ def oracle():
             "orc_tsdf_integrate_wrap": (None, [_P, _P, _P, _P, _P, _P, _P, C.c_int, _P, _P]),
             "orc_raycast_wrap": (None, [_P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P, _P, _P]),
             "orc_raycast_wrap_mode": (None, [_P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_int]),
+            "orc_raycast_values": (None, [_P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P]),
             "orc_tsdf_clear_slice": (None, [_P, _P, _P, _P, _P]),
             "orc_fetch_points": (C.c_long, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_long]),
             "orc_engine_shift_state": (None, [_P, _P]),

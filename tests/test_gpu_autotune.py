@@ -12,7 +12,7 @@ from _util import cfg_for, cfg_hash, frames, rot_angle, same_bits
 
 pytestmark = pytest.mark.gpu
 
-DEFAULT = (18, 4, 8, 8)
+DEFAULT = (18, 4, 8, 8, 8)
 
 
 @pytest.fixture(scope="module")
@@ -50,23 +50,26 @@ def test_shapes_change_no_result_bit(gpu_ctx, mix):
     gpu_ctx.set_tuning(L.Tuning(*DEFAULT))
 
 
-def test_icp_pixels_per_thread_regroups_sums_only(gpu_ctx, mix):
+def test_icp_shapes_regroup_sums_only(gpu_ctx, mix):
+    """Pixels per thread and blocks per session (cluster sizes 2 .. 16, 16 being the
+    non-portable size) change only the grouping of the FP64 partial sums."""
     gpu_ctx.set_tuning(L.Tuning(*DEFAULT))
     base, _ = _run(gpu_ctx, mix)
-    for ppt in (2, 8, 16):
-        gpu_ctx.set_tuning(L.Tuning(18, ppt, 8, 8))
+    for ppt, cl in ((2, 8), (8, 8), (16, 8), (4, 2), (4, 4), (8, 16)):
+        gpu_ctx.set_tuning(L.Tuning(18, ppt, 8, 8, cl))
         p, _ = _run(gpu_ctx, mix)
         for f in range(p.shape[0]):
             for i in range(p.shape[1]):
                 a, b = p[f, i], base[f, i]
-                assert rot_angle(a[:9].reshape(3, 3), b[:9].reshape(3, 3)) < 1e-5, (ppt, f, i)
-                assert np.max(np.abs(a[9:] - b[9:])) < 1e-5, (ppt, f, i)
+                assert rot_angle(a[:9].reshape(3, 3), b[:9].reshape(3, 3)) < 1e-5, (ppt, cl, f, i)
+                assert np.max(np.abs(a[9:] - b[9:])) < 1e-5, (ppt, cl, f, i)
     gpu_ctx.set_tuning(L.Tuning(*DEFAULT))
 
 
 def test_out_of_range_tuning_is_rejected(gpu_ctx):
     before = gpu_ctx.tuning().as_dict()
-    for bad in [L.Tuning(13, 4, 8, 8), L.Tuning(18, 3, 8, 8), L.Tuning(18, 4, 12, 8), L.Tuning(18, 4, 8, 64)]:
+    for bad in [L.Tuning(13, 4, 8, 8), L.Tuning(18, 3, 8, 8), L.Tuning(18, 4, 12, 8), L.Tuning(18, 4, 8, 64),
+                L.Tuning(18, 4, 8, 8, 3), L.Tuning(18, 4, 8, 8, 32)]:
         with pytest.raises(L.NuiError):
             gpu_ctx.set_tuning(bad)
     assert gpu_ctx.tuning().as_dict() == before
@@ -80,7 +83,7 @@ def test_autotune_keeps_a_valid_choice_and_frees_its_sessions(gpu_ctx, mix):
     d = t.as_dict()
     assert d == gpu_ctx.tuning().as_dict()
     assert 16 <= d["integrate_threads_log2"] <= 20
-    assert d["icp_pixels_per_thread"] in (2, 4, 8, 16)
+    assert d["icp_pixels_per_thread"] in (2, 4, 8, 16) and d["icp_cluster_blocks"] in (4, 8, 16)
     assert d["raycast_tile_width"] in (4, 8, 16, 32) and d["hash_raycast_tile_width"] in (4, 8, 16, 32)
     assert ms > 0
     assert torch.cuda.mem_get_info()[0] >= free0 - (64 << 20)
