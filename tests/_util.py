@@ -96,3 +96,33 @@ def relative_gt(seq):
     for _, _, R, t in seq:
         out.append((R0.T @ np.asarray(R, np.float64), R0.T @ (np.asarray(t, np.float64) - t0)))
     return out
+
+
+def integration_near_ties(cfg, tp, R, t, scaled, eps_px=1e-4, eps_m=1e-5):
+    """Voxels (reference layout, flattened) whose integration decision is a near tie at pose
+    (R, t): the exact (FP64) projection lies within eps_px of a rounding boundary (a half
+    pixel) in u or v, or the signed distance within eps_m of -trunc.  There any float
+    evaluation -- the reference's running sums or a direct one -- may take the other side,
+    i.e. the neighbouring pixel's depth or the other update decision.  scaled: the
+    frame's ray-length depth (oracle_preprocess(...)["scaled"])."""
+    rx, ry, rz = (int(v) for v in tp.res)
+    cell = [float(np.float32(c)) for c in tp.cell[:3]]
+    Ri = np.asarray(R, np.float64).T
+    t = np.asarray(t, np.float64)
+    x = (np.arange(rx) - rx // 2 + 0.5) * cell[0] - t[0]
+    y = (np.arange(ry) - ry // 2 + 0.5) * cell[1] - t[1]
+    z = (np.arange(rz) + 0.5) * cell[2] - t[2]
+    gy, gx, gz = np.meshgrid(y, x, z, indexing="ij")  # reference layout: (x + y rx) rz + z
+    vx = Ri[0, 0] * gx + Ri[0, 1] * gy + Ri[0, 2] * gz
+    vy = Ri[1, 0] * gx + Ri[1, 1] * gy + Ri[1, 2] * gz
+    vz = Ri[2, 0] * gx + Ri[2, 1] * gy + Ri[2, 2] * gz
+    with np.errstate(divide="ignore", invalid="ignore"):
+        qx, qy = vx * cfg.fx / vz + cfg.cx, vy * cfg.fy / vz + cfg.cy
+        tie = (np.abs(qx - np.floor(qx) - 0.5) < eps_px) | (np.abs(qy - np.floor(qy) - 0.5) < eps_px)
+        px, py = np.trunc(qx + np.copysign(0.5, qx)), np.trunc(qy + np.copysign(0.5, qy))
+        W, H = cfg.width, cfg.height
+        ok = (vz > 0) & (px >= 0) & (py >= 0) & (px < W) & (py < H)
+        D = np.where(ok, scaled[np.where(ok, py, 0).astype(np.int64), np.where(ok, px, 0).astype(np.int64)], np.nan)
+        sd = D - np.sqrt(gx * gx + gy * gy + gz * gz)
+        tie |= np.abs(sd + float(tp.trunc)) < eps_m
+    return (tie & (vz > 0)).reshape(-1)

@@ -14,7 +14,7 @@ import pytest
 from natureuserinterfacestudio_b200 import _lib as L
 from oracle import oracle as O
 
-from _util import cfg_for, cfg_hash, frames, oracle_preprocess, rot_angle, same_bits
+from _util import cfg_for, cfg_hash, frames, integration_near_ties, oracle_preprocess, rot_angle, same_bits
 
 pytestmark = pytest.mark.gpu
 
@@ -92,27 +92,39 @@ def test_integration_over_frames_bit_exact(gpu_ctx, seq):
 @pytest.mark.parametrize("res", [(192, 160, 176), (100, 90, 70)])
 def test_fp16_integration_within_tolerance_of_oracle(gpu_ctx, seq, fmt, res):
     """The FP16 serving formats integrate in tolerance mode (direct voxel positions,
-    contraction, approximate reciprocals): at the oracle's poses, after every frame, the
-    same voxels are updated (counts within 1e-4), weights agree on all but 1e-4 of the
-    voxels, and TSDF values agree within 1e-3 truncation units at the 0.9999 quantile of
-    the voxels weighted in both (half precision rounds to 2.4e-4 near 1).  The odd
-    resolution leaves partial 32 x 8 x 8 tiles at the volume's faces."""
+    contraction, approximate reciprocals, round-half-away projections) at the oracle's poses.
+    After every frame, wherever the GPU and the oracle disagree -- a weight, or a TSDF value by
+    more than 1e-3 truncation units -- the voxel's decision was a near tie in some frame so far:
+    its exact (FP64) projection within 3e-3 px of a half pixel, or its signed distance within
+    10 um of -trunc.  There the reference's running z sums (errors of ~1e-4 px after ~200
+    slices) and the direct evaluation may pick neighbouring pixels; a neighbouring depth at
+    ~2 m is ~4 mm away, far beyond 1e-3 truncation units, so such voxels are told apart from
+    errors by their geometry, not by a bound on the difference.  The updated-voxel counts
+    differ by at most the frame's near ties.  Everywhere else the two agree to 1e-3 (half
+    precision rounds to 2.4e-4 near 1); the FP64 comparison (test_gpu_fp64_errors) bounds the
+    format's error quantiles.  The odd resolution leaves partial 32 x 8 x 8 tiles at the
+    volume's faces, and its 3 cm cells make exact ties frequent at the first pose."""
     cfg = cfg_for(res=res, fmt=fmt)
     eng = O.Engine(cfg_for(res=res))
     s = L.Session(gpu_ctx, cfg)
+    amb = np.zeros(res[0] * res[1] * res[2], bool)
     for i, (d, _, _, _) in enumerate(seq):
         assert eng.frame(d), i
         R, t = eng.pose()
         s.upload(d)
         s.set_pose(R, t)
         s.integrate()
+        scaled = oracle_preprocess(d, cfg)["scaled"]
+        now = integration_near_ties(cfg, eng.tsdf, R, t, scaled, eps_px=3e-3)
+        amb |= now
         g, o = s.touched(), eng.touched()
-        assert o > 0 and abs(g - o) <= 1e-4 * o, (i, g, o)
+        assert o > 0 and abs(g - o) <= int(now.sum()), (i, g, o)
         vg, vo = s.volume_ref_layout().astype(np.float64), eng.volume().astype(np.float64)
-        assert np.mean(vg[:, 1] != vo[:, 1]) <= 1e-4, i
+        wdiff = vg[:, 1] != vo[:, 1]
         both = (vg[:, 1] > 0) & (vo[:, 1] > 0)
-        diff = np.abs(vg[both, 0] - vo[both, 0]) / 32766.0
-        assert np.quantile(diff, 0.9999) <= 1e-3, (i, float(np.quantile(diff, 0.9999)))
+        fdiff = both & (np.abs(vg[:, 0] - vo[:, 0]) / 32766.0 > 1e-3)
+        bad = wdiff | fdiff
+        assert not np.any(bad & ~amb), (i, int(np.sum(bad & ~amb)), int(np.sum(bad)))
         # the brick classification fused into the tolerance-mode kernel: every brick's
         # state is what its voxels say (k_brick_summary's rule)
         assert np.array_equal(s.download(13), _brick_states(s, res)), i
@@ -203,8 +215,13 @@ def test_fp16_raycast_within_tolerance_of_oracle(gpu_ctx, seq, fmt):
     dist = np.where(np.isfinite(dist), dist, np.inf)  # a degenerate refinement (0 / 0) in either
     q99, far = float(np.quantile(dist, 0.99)), float(np.mean(dist > 5e-4))
     assert q99 <= 5e-4 and far <= 0.015, (q99, far)
+    # normals: a zero vector where the central differences cancel (the reference keeps it,
+    # about 1 % of the hits here); the zero masks agree, and elsewhere the directions
     nb = both & ~np.isnan(ng[:, 0]) & ~np.isnan(no[:, 0])
-    cosang = np.clip(np.sum(ng[nb] * no[nb], axis=1), -1, 1)
+    zg, zo = np.all(ng[nb] == 0, axis=1), np.all(no[nb] == 0, axis=1)
+    assert np.mean(zg != zo) <= 1e-3, float(np.mean(zg != zo))
+    nz = ~zg & ~zo
+    cosang = np.clip(np.sum(ng[nb][nz] * no[nb][nz], axis=1), -1, 1)
     assert np.quantile(np.arccos(cosang), 0.99) <= 0.05
     w = s.work_counters()
     assert w["ray_hits"] >= int(hg.sum()) and w["ray_reads"] > 0 and w["ray_samples"] >= w["ray_hits"]
