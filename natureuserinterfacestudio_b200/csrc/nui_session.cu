@@ -2389,7 +2389,7 @@ struct nui_server {
   nui_ctx* ctx = nullptr;
   size_t budget = 0, used = 0;  // live and pooled sessions
   cudaStream_t up = nullptr;
-  cudaEvent_t ev_t0 = nullptr, ev_up = nullptr, ev_done = nullptr;
+  cudaEvent_t ev_t0 = nullptr, ev_up = nullptr, ev_done = nullptr, ev_order = nullptr;
   std::chrono::steady_clock::time_point t0;
   std::vector<Slot> slots;
   std::vector<Pooled> pool;
@@ -2431,10 +2431,18 @@ nui_status server_collect(nui_server* v) {
   return NUI_OK;
 }
 
-void server_free_slot_buffers(nui_server::Slot& sl) {
+// A slot's frame buffers come from the context's pool in the order of the upload stream:
+// they are freed there behind the batch in flight (which may still read them) and the
+// new ones allocated there before the first upload into them, so that neither waits for
+// the device.
+void server_free_slot_buffers(nui_server* v, nui_server::Slot& sl) {
+  if (sl.draw[0] || sl.dbgra[0]) {
+    cudaEventRecord(v->ev_order, v->ctx->stream);
+    cudaStreamWaitEvent(v->up, v->ev_order, 0);
+  }
   for (int b = 0; b < 2; ++b) {
-    cudaFree(sl.draw[b]);
-    cudaFree(sl.dbgra[b]);
+    if (sl.draw[b]) cudaFreeAsync(sl.draw[b], v->up);
+    if (sl.dbgra[b]) cudaFreeAsync(sl.dbgra[b], v->up);
     sl.draw[b] = nullptr;
     sl.dbgra[b] = nullptr;
   }
@@ -2455,9 +2463,26 @@ NUI_API nui_status nui_server_create(nui_ctx* ctx, size_t budget, int max_stream
   v->floor.n = max_streams;
   if (cudaStreamCreateWithFlags(&v->up, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&v->ev_t0) != cudaSuccess || cudaEventCreateWithFlags(&v->ev_up, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreate(&v->ev_done) != cudaSuccess) {
+      cudaEventCreate(&v->ev_done) != cudaSuccess ||
+      cudaEventCreateWithFlags(&v->ev_order, cudaEventDisableTiming) != cudaSuccess) {
     delete v;
     return fail(NUI_ERR_DEVICE, "stream / event creation failed");
+  }
+  // The budget is taken into the context's pool now (one allocation, freed at once: the
+  // pool keeps the memory, its release threshold being unbounded), so that admissions
+  // sub-allocate from memory the pool holds instead of mapping new memory while ticks run.
+  // A budget above what the device has free is taken as far as it goes.
+  {
+    size_t free_b = 0, total_b = 0;
+    NUI_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t margin = (size_t)2 << 30;
+    const size_t take = std::min(budget, free_b > margin ? free_b - margin : 0);
+    void* p = nullptr;
+    if (take > 0 && counted_pool_alloc(&p, take, ctx->pool, ctx->stream) == cudaSuccess) {
+      cudaFreeAsync(p, ctx->stream);
+    } else {
+      cudaGetLastError();
+    }
   }
   // the server clock: host time of a recorded event, so device completion times map onto it
   NUI_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -2474,14 +2499,16 @@ NUI_API nui_status nui_server_destroy(nui_server* v) {
   cudaStreamSynchronize(v->up);
   for (auto& sl : v->slots) {
     if (sl.s) nui_session_destroy(sl.s);
-    server_free_slot_buffers(sl);
+    server_free_slot_buffers(v, sl);
   }
+  cudaStreamSynchronize(v->up);
   for (auto& p : v->pool) nui_session_destroy(p.s);
   nui_ctx_trim(v->ctx);  // the served sessions' memory goes back to the device
   cudaStreamDestroy(v->up);
   cudaEventDestroy(v->ev_t0);
   cudaEventDestroy(v->ev_up);
   cudaEventDestroy(v->ev_done);
+  cudaEventDestroy(v->ev_order);
   delete v;
   return NUI_OK;
 }
@@ -2525,15 +2552,15 @@ NUI_API nui_status nui_server_admit(nui_server* v, const nui_session_cfg* cfg, i
   const size_t N = (size_t)cfg->width * cfg->height;
   const bool col = s->cmap != nullptr;
   if (sl.cap_px < N || (col && !sl.cap_bgra)) {
-    cudaStreamSynchronize(v->up);
-    server_free_slot_buffers(sl);
+    server_free_slot_buffers(v, sl);
     bool ok = true;
     for (int b = 0; b < 2 && ok; ++b) {
-      ok = counted_malloc(&sl.draw[b], N * 2) == cudaSuccess;
-      if (ok && col) ok = counted_malloc(&sl.dbgra[b], N * 4) == cudaSuccess;
+      ok = counted_pool_alloc((void**)&sl.draw[b], N * 2, v->ctx->pool, v->up) == cudaSuccess;
+      if (ok && col) ok = counted_pool_alloc((void**)&sl.dbgra[b], N * 4, v->ctx->pool, v->up) == cudaSuccess;
     }
     if (!ok) {
-      server_free_slot_buffers(sl);
+      cudaGetLastError();
+      server_free_slot_buffers(v, sl);
       v->pool.push_back(nui_server::Pooled{s, bytes});
       return fail(NUI_ERR_OOM, "device allocation failed");
     }
