@@ -56,6 +56,9 @@ struct TrackState {
   // per level
   unsigned long long ray_reads, ray_samples, ray_hits, bricks;
   unsigned int icp_iters[kMaxLevels];
+  // tolerance-mode integration: tiles listed by the cull; blocks of the integration done
+  // (both zero between integrations)
+  unsigned int fast_count, fast_done;
 };
 
 // What one session does in the current tick (host-written, read by every kernel).
@@ -101,7 +104,7 @@ struct SessionDesc {
   uint8_t* occ3;                  // per 128^3 region state (kSuper*, over its super-bricks)
   int max_cw;
   int zchunks;                    // integration: z chunks per column (one thread each)
-  uint8_t* fast_tiles;            // tolerance-mode integration: 32 x 8 x 8 tiles kept by the cull
+  unsigned* fast_tiles;           // tolerance-mode integration: 32 x 8 x 8 tiles kept by the cull (list)
   float* ztab;                    // integration: running sums shared by all columns, 2 (rz + 1)
   // shifting volume (0: fixed): shift distance in voxels, basis translation, and the point
   // cache of the slabs that leave the volume (pts_cap points of xyz / rgba floats)
@@ -364,6 +367,12 @@ __device__ __forceinline__ size_t occ2_index(const SessionDesc& s, int x, int y,
 // lies within the boundary margin anyway).  Its distance |q - n| to the product is
 // min(f, 1 - f) for the fraction f = q - floor(q), so the boundary test is unchanged, and
 // away from a boundary round-to-nearest-even and round-half-away agree.
+// Tolerance-mode rounding to the nearest integer: floor(q + 0.5).  At exact ties it rounds
+// up, which is OpenCL's round() (half away from zero) for every q > -0.5; it differs from
+// round() only within one ulp below a tie (where q + 0.5 itself rounds up) and at q = -0.5,
+// both near ties that the tolerance admits.  Two instructions, no branch.
+__device__ __forceinline__ int round_half_up(float q) { return __float2int_rd(q + 0.5f); }
+
 __device__ __forceinline__ int round_div(float p, float c, float inv) {
   const float q = p * inv;
   const float big = 12582912.f;  // 1.5 * 2^23

@@ -13,7 +13,10 @@
 // x 8 (z) voxels.  k_integrate_cull tests every tile on one thread: tiles entirely behind
 // the camera, projecting outside the image, or farther from the camera than the largest
 // ray depth of the pixel tiles they project to plus the truncation are dropped without a
-// memory access.  k_integrate_fast then runs the kept tiles, one warp per tile, lane = x,
+// memory access; the kept ones are appended to the session's tile list.  k_integrate_fast
+// then runs the listed tiles, dealt round robin to all its warps (the kept tiles cluster
+// in the frustum, so a fixed tile-to-warp map would leave most warps idle), one warp per
+// tile, lane = x,
 // so every row a warp touches is one contiguous 64 B run of the tsdf plane and 32 B of the
 // weight plane: the update pass over the tile's 64 rows (only updated voxels are read and
 // written), then -- for the 8^3 bricks of the tile that had an update -- the brick
@@ -108,7 +111,13 @@ __global__ void __launch_bounds__(256) k_integrate_cull(const SessionDesc* __res
     const float dmin = sqrtf(bx * bx + by * by + bz * bz);
     keep = mx > 0.f && !(dmin > mx + s.trunc + 1e-3f * (1.f + dmin));
   }
-  s.fast_tiles[tile] = keep ? 1 : 0;
+  // append the kept tile to the session's list (one atomic per warp)
+  const unsigned act = __activemask(), kept = __ballot_sync(act, keep);
+  const int lane = threadIdx.x & 31;
+  unsigned base = 0;
+  if (kept && lane == __ffs(act) - 1) base = atomicAdd(&s.ts->fast_count, (unsigned)__popc(kept));
+  base = __shfl_sync(act, base, __ffs(act) - 1);
+  if (keep) s.fast_tiles[base + __popc(kept & ((1u << lane) - 1u))] = (unsigned)tile;
 }
 
 // The tiles the cull kept: a warp reads the flags of 32 consecutive tiles and runs the ones
@@ -136,11 +145,9 @@ __global__ void __launch_bounds__(32 * kFastWarps, 2) k_integrate_fast(const Ses
   const int hx = rx / 2, hy = ry / 2;
   unsigned int touched_total = 0, bricks = 0;
 
-  for (int g32 = (blockIdx.x * kFastWarps + (threadIdx.x >> 5)) * 32; g32 < ntiles; g32 += nwarps * 32) {
-   unsigned todo = __ballot_sync(0xffffffffu, g32 + lane < ntiles && s.fast_tiles[g32 + lane] != 0);
-   while (todo) {
-    const int tile = g32 + __ffs(todo) - 1;
-    todo &= todo - 1u;
+  const unsigned count = *(volatile const unsigned*)&s.ts->fast_count;
+  for (unsigned li = blockIdx.x * kFastWarps + (threadIdx.x >> 5); li < count; li += (unsigned)nwarps) {
+    const int tile = (int)__ldg(s.fast_tiles + li);
     const int x0 = (tile % ntx) << 5, y0 = ((tile / ntx) % nty) << 3, z0 = (tile / (ntx * nty)) << 3;
     const int xn = min(32, rx - x0), yn = min(8, ry - y0), zn = min(8, rz - z0);
 
@@ -166,9 +173,9 @@ __global__ void __launch_bounds__(32 * kFastWarps, 2) k_integrate_fast(const Ses
         pix[yy] = 0;
         if (xin && yy < yn && v.z > 0.f) {
           const float iz = __fdividef(1.f, v.z);
-          // round half away from zero, as OpenCL's round(): ties are frequent (pixel centres
-          // and voxel centres sit on rational grids), and half-to-even would split them
-          const int px = (int)roundf(fx * v.x * iz + ccx), py = (int)roundf(fy * v.y * iz + ccy);
+          // exact ties round up, as OpenCL's round(): they are frequent (pixel centres and
+          // voxel centres sit on rational grids), and half-to-even would split them
+          const int px = round_half_up(fx * v.x * iz + ccx), py = round_half_up(fy * v.y * iz + ccy);
           if (px >= 0 && py >= 0 && px < W && py < H) {
             pix[yy] = py * W + px;
             in |= 1u << yy;
@@ -257,12 +264,18 @@ __global__ void __launch_bounds__(32 * kFastWarps, 2) k_integrate_fast(const Ses
       ++bricks;
     }
     if (lane == 0 && s.occ2) s.occ2[occ2_index(s, x0, y0, z0)] = kSuperDirty;
-   }
   }
   const unsigned int t = __reduce_add_sync(0xffffffffu, touched_total);
   const unsigned int b = __reduce_add_sync(0xffffffffu, bricks);
   if (lane == 0 && t) atomicAdd(&s.ts->touched, (unsigned long long)t);
   if (lane == 0 && b) atomicAdd(&s.ts->bricks, (unsigned long long)b);
+  // the session's last block to finish empties the list for the next integration (every
+  // block has read the count by then)
+  __syncthreads();
+  if (threadIdx.x == 0 && atomicAdd(&s.ts->fast_done, 1u) == gridDim.x - 1) {
+    s.ts->fast_count = 0u;
+    s.ts->fast_done = 0u;
+  }
 }
 
 template __global__ void k_integrate_cull<2>(const SessionDesc*);

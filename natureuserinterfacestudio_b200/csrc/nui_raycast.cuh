@@ -48,9 +48,9 @@ struct RayVol {
   }
   __device__ __forceinline__ void voxel_of(float3 p, int& gx, int& gy, int& gz) const {
     if (FAST) {
-      gx = (int)roundf(p.x * i0);  // half away from zero, as OpenCL's round()
-      gy = (int)roundf(p.y * i1);
-      gz = (int)roundf(p.z * i2);
+      gx = round_half_up(p.x * i0);  // exact ties up, as OpenCL's round()
+      gy = round_half_up(p.y * i1);
+      gz = round_half_up(p.z * i2);
     } else {
       gx = round_div(p.x, c0, i0);
       gy = round_div(p.y, c1, i1);

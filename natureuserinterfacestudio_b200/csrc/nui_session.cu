@@ -251,7 +251,7 @@ struct nui_session {
   uint8_t* occ = nullptr;
   uint8_t* occ2 = nullptr;
   float* ztab = nullptr;
-  uint8_t* fast_tiles = nullptr;
+  unsigned* fast_tiles = nullptr;
   uint8_t* occ3 = nullptr;
   float* tile_max = nullptr;
   TrackState* ts = nullptr;
@@ -1261,8 +1261,8 @@ NUI_API size_t nui_session_device_bytes(const nui_session_cfg* c) {
   }
   const size_t nv = (size_t)c->res[0] * c->res[1] * c->res[2];
   b += nv * voxel_bytes(c->tsdf_format);
-  if (c->tsdf_format >= NUI_TSDF_F16_U8)  // tolerance-mode tile flags
-    b += (size_t)((c->res[0] + 31) / 32) * ((c->res[1] + 7) / 8) * ((c->res[2] + 7) / 8);
+  if (c->tsdf_format >= NUI_TSDF_F16_U8)  // tolerance-mode tile list
+    b += (size_t)((c->res[0] + 31) / 32) * ((c->res[1] + 7) / 8) * ((c->res[2] + 7) / 8) * 4;
   if (c->color_volume) b += nv * 4;
   b += (size_t)((c->res[0] + 7) / 8) * ((c->res[1] + 7) / 8) * ((c->res[2] + 7) / 8);
   b += (size_t)((c->res[0] + 31) / 32) * ((c->res[1] + 31) / 32) * ((c->res[2] + 31) / 32);
@@ -1362,7 +1362,7 @@ nui_status session_create(nui_ctx* ctx, const nui_session_cfg* cfg, nui_session*
     ok = ok && alloc((void**)&s->vol, nv * (c.tsdf_format == 2 ? 2 : voxel_bytes(c.tsdf_format)));
     if (ok && c.tsdf_format == NUI_TSDF_F16_U8) ok = alloc((void**)&s->wvol, nv);
     if (ok && c.tsdf_format >= NUI_TSDF_F16_U8)
-      ok = alloc((void**)&s->fast_tiles, (size_t)((c.res[0] + 31) / 32) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8));
+      ok = alloc((void**)&s->fast_tiles, (size_t)((c.res[0] + 31) / 32) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8) * 4);
     const size_t nbricks = (size_t)((c.res[0] + 7) / 8) * ((c.res[1] + 7) / 8) * ((c.res[2] + 7) / 8);
     const size_t nsuper = (size_t)((c.res[0] + 31) / 32) * ((c.res[1] + 31) / 32) * ((c.res[2] + 31) / 32);
     const size_t nhyper = (size_t)((c.res[0] + 127) / 128) * ((c.res[1] + 127) / 128) * ((c.res[2] + 127) / 128);
