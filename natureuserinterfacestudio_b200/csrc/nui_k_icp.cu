@@ -5,9 +5,8 @@
 // transform it by the running estimate, project into the previous camera with
 // full-resolution intrinsics, bilinearly sample the world reference normal and vertex
 // (icp.cl:192-220; a tap NaN -> no match), and if |q - p| < distThres form the row
-// [n x p, n | n.(q - p)].  The 29 products of a warp's 32 pixels are summed in FP32 by a
-// shuffle reduce-scatter and added to one FP64 running sum per lane (lane k: term k);
-// blocks add their warps' sums in shared memory; the cluster's first block adds
+// [n x p, n | n.(q - p)].  Each thread accumulates the 29 products of its pixels in FP64;
+// blocks reduce them with warp shuffles and shared memory; the cluster's first block adds
 // the blocks' sums (distributed shared memory, fixed order) and runs the host step of
 // NuiKinfuOpenCLDepthTracker::IterativeClosestPoint (NuiKinfuOpenCLDepthTracker.cpp:324-496):
 // Levenberg-Marquardt accept/reject, FP64 determinant check and Cholesky solve, ZYX Euler
@@ -210,8 +209,36 @@ __device__ __forceinline__ void euler_zyx(double a, double b, double g, double (
     }
 }
 
-// LM step on the reduced sums (runs on one thread of the last block).
-__device__ __noinline__ void icp_host_step(TrackState* ts, const double* sums, int iter, unsigned min_count) {
+// The tracker state the host step reads and writes: kept in block 0's shared memory for
+// the whole ICP kernel (so that the single thread's step makes no global-memory round
+// trips), copied in at the start and back at the end.
+struct IcpLm {
+  float R[9], t[3], Rg[9], tg[3];
+  double good[27];
+  float lambda, err_old, error, count;
+  int level_done, status, iterations_run;
+  unsigned icp_iters[kMaxLevels];
+};
+
+// Copies the fields (d <- s); T, U: TrackState or IcpLm.
+template <class T, class U>
+__device__ __forceinline__ void lm_copy(T* d, const U* s) {
+  for (int k = 0; k < 9; ++k) d->R[k] = s->R[k], d->Rg[k] = s->Rg[k];
+  for (int k = 0; k < 3; ++k) d->t[k] = s->t[k], d->tg[k] = s->tg[k];
+  for (int k = 0; k < 27; ++k) d->good[k] = s->good[k];
+  d->lambda = s->lambda;
+  d->err_old = s->err_old;
+  d->error = s->error;
+  d->count = s->count;
+  d->level_done = s->level_done;
+  d->status = s->status;
+  d->iterations_run = s->iterations_run;
+  for (int k = 0; k < kMaxLevels; ++k) d->icp_iters[k] = s->icp_iters[k];
+}
+
+// LM step on the reduced sums (runs on one thread of the cluster's first block).
+template <class St>
+__device__ __noinline__ void icp_host_step(St* ts, const double* sums, int iter, unsigned min_count) {
   float err = (float)sums[27];
   const float cnt = (float)sums[28];
   err = (cnt > 0.f) ? sqrtf(err) / cnt : 3.402823466e+38f;
@@ -290,34 +317,12 @@ __device__ __noinline__ void icp_host_step(TrackState* ts, const double* sums, i
     }
 }
 
-// Warp sum of the 29 row products of the lanes' pixels, reduce-scattered: at each of five
-// steps a lane keeps half of its values, sends the other half to its partner and adds what
-// it receives, so that after 31 exchanges lane k holds the warp's float sum of term k
-// (terms padded to 32).  The lane adds it to its own FP64 running sum: one FP64 accumulator
-// per lane instead of 29 per thread, which keeps the kernel's registers low enough for
-// twice the resident warps.
-__device__ __forceinline__ void warp_rows_add(float (&v)[32], double& acc) {
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int half = 16; half > 0; half >>= 1) {
-    const bool upper = lane & half;
-#pragma unroll
-    for (int j = 0; j < half; ++j) {
-      const float send = upper ? v[j] : v[j + half];
-      const float keep = upper ? v[j + half] : v[j];
-      v[j] = keep + __shfl_xor_sync(0xffffffffu, send, half);
-    }
-  }
-  acc += (double)v[0];
-}
-
-// The depth rows of one block of pixels (kIcpThreads x PPT consecutive pixels of the
-// level, index `vb`), added to the lanes' FP64 sums (lane k: term k).  sR / tc: the running
-// estimate; sp: the previous camera pose (the reference maps' frame).  Every lane takes
-// part in each step's exchange; a pixel without a match contributes zeros.
+// The 29 sums of the depth rows of one block of pixels (kIcpThreads x PPT consecutive
+// pixels of the level, index `vb`), added to this thread's FP64 accumulators.  sR / tc: the
+// running estimate; sp: the previous camera pose (the reference maps' frame).
 template <int PPT>
 __device__ __forceinline__ void icp_depth_rows(const SessionDesc& s, int level, int vb, const float* sR, float3 tc,
-                                               const DevXform& sp, double& acc) {
+                                               const DevXform& sp, double (&acc)[kIcpTerms]) {
   const int w = s.W >> level, n = w * (s.H >> level);
   const float* __restrict__ Dl = s.dlev[level];
   const float fx = s.cam.fx, fy = s.cam.fy, cx = s.cam.cx, cy = s.cam.cy;
@@ -337,73 +342,74 @@ __device__ __forceinline__ void icp_depth_rows(const SessionDesc& s, int level, 
     const float dep = dq[0];
 #pragma unroll
     for (int j = 0; j + 1 < PPT; ++j) dq[j] = dq[j + 1];
-    // the warp's pixels of this step all lie past the level's end: nothing to add
-    if (base + k * kIcpThreads + (int)(threadIdx.x & ~31u) >= n) break;
-    float c7[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    bool ok = !isnan(dep);
-    if (ok) {
-      const int i = base + k * kIcpThreads + threadIdx.x;
-      const int py = i / w;
-      const float3 v = level_vertex(s.cam, level, i - py * w, py, dep);
-      const float3 pv = add3(rot_rows(sR, v), tc);
-      const float3 pp = rot_rows(sp.R_inv, sub3(pv, tp));
-      const float u = pp.x * fx / pp.z + cx;
-      const float vv = pp.y * fy / pp.z + cy;
-      ok = u >= 0.0f && u < fW && vv >= 0.0f && vv < fH;
-      if (ok) {
-        // both maps sampled at once (their eight loads in flight together), then tested
-        const float3 rn = bilinear_holes(s.nref, u, vv, RW, RN);
-        const float3 rv = bilinear_holes(s.vref, u, vv, RW, RN);
-        ok = !isnan3(rn) && !isnan3(rv);
-        if (ok) {
-          const float3 diff = sub3(rv, pv);
-          const float dist = sqrtf(dot3(diff, diff));
-          ok = dist < s.dist_thr;
-          const float3 r0 = cross3(rn, pv);
-          c7[0] = r0.x, c7[1] = r0.y, c7[2] = r0.z, c7[3] = rn.x, c7[4] = rn.y, c7[5] = rn.z;
-          c7[6] = dot3(rn, diff);
-        }
-      }
-    }
-    float v[32];
+    if (isnan(dep)) continue;
+    const int i = base + k * kIcpThreads + threadIdx.x;
+    const int py = i / w;
+    const float3 v = level_vertex(s.cam, level, i - py * w, py, dep);
+    const float3 pv = add3(rot_rows(sR, v), tc);
+    const float3 pp = rot_rows(sp.R_inv, sub3(pv, tp));
+    const float u = pp.x * fx / pp.z + cx;
+    const float vv = pp.y * fy / pp.z + cy;
+    if (!(u >= 0.0f && u < fW && vv >= 0.0f && vv < fH)) continue;
+    // both maps sampled at once (their eight loads in flight together), then tested
+    const float3 rn = bilinear_holes(s.nref, u, vv, RW, RN);
+    const float3 rv = bilinear_holes(s.vref, u, vv, RW, RN);
+    if (isnan3(rn) || isnan3(rv)) continue;
+    const float3 diff = sub3(rv, pv);
+    const float dist = sqrtf(dot3(diff, diff));
+    if (!(dist < s.dist_thr)) continue;
+    const float3 r0 = cross3(rn, pv);
+    const float c7[7] = {r0.x, r0.y, r0.z, rn.x, rn.y, rn.z, dot3(rn, diff)};
     int sh = 0;
 #pragma unroll
     for (int a = 0; a < 6; ++a)
 #pragma unroll
-      for (int b = a; b < 7; ++b, ++sh) v[sh] = ok ? c7[a] * c7[b] : 0.f;
-    v[27] = ok ? c7[6] * c7[6] : 0.f;
-    v[28] = ok ? 1.f : 0.f;
-    v[29] = v[30] = v[31] = 0.f;
-    warp_rows_add(v, acc);
+      for (int b = a; b < 7; ++b, ++sh) acc[sh] += (double)(c7[a] * c7[b]);
+    acc[27] += (double)(c7[6] * c7[6]);
+    acc[28] += 1.0;
   }
 }
 
 // The photometric rows of one block of full-resolution model points (colour tracking).
 template <int PPT>
 __device__ __forceinline__ void icp_color_rows(const SessionDesc& s, int vb, const float* sR, float3 tc,
-                                               double& acc) {
+                                               double (&acc)[kIcpTerms]) {
   const int cbase = vb * kIcpThreads * PPT, NM = s.W * s.H;
 #pragma unroll 1
   for (int k = 0; k < PPT; ++k) {
-    if (cbase + k * kIcpThreads + (int)(threadIdx.x & ~31u) >= NM) break;
     const int i = cbase + k * kIcpThreads + threadIdx.x;
-    float v[32];
-    if (!(i < NM && color_row(s, i, sR, tc, v))) {
+    if (i >= NM) break;
+    float c[kIcpTerms];
+    if (!color_row(s, i, sR, tc, c)) continue;
 #pragma unroll
-      for (int q = 0; q < kIcpTerms; ++q) v[q] = 0.f;
-    }
-    v[29] = v[30] = v[31] = 0.f;
-    warp_rows_add(v, acc);
+    for (int q = 0; q < kIcpTerms - 1; ++q) acc[q] += (double)c[q];
+    acc[28] += 1.0;
   }
 }
 
-// Block sum of the lanes' FP64 sums (warp w, lane k: term k) in a fixed order of warps.
-// Threads 0..28 receive term threadIdx.x; all threads must call it.
-__device__ __forceinline__ double icp_block_sum(double acc) {
+// Block sum of the threads' accumulators (a reduce-scatter over the 32 lanes of a warp,
+// terms padded to 32 -- at each of five steps a lane keeps half of its values, sends the
+// other half to its partner and adds what it receives, so lane k ends with the warp's sum
+// of term k after 31 exchanges instead of 29 x 5 -- then the warps in shared memory, in a
+// fixed order).  Threads 0..28 receive term threadIdx.x; all threads must call it.
+__device__ __forceinline__ double icp_block_sum(const double (&acc)[kIcpTerms]) {
   constexpr int kWarps = kIcpThreads / 32;
   __shared__ double wsum[kWarps][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  wsum[warp][lane] = acc;
+  double v[32];
+#pragma unroll
+  for (int k = 0; k < 32; ++k) v[k] = k < kIcpTerms ? acc[k] : 0.0;
+#pragma unroll
+  for (int half = 16; half > 0; half >>= 1) {
+    const bool upper = lane & half;
+#pragma unroll
+    for (int j = 0; j < half; ++j) {
+      const double send = upper ? v[j] : v[j + half];
+      const double keep = upper ? v[j + half] : v[j];
+      v[j] = keep + __shfl_xor_sync(0xffffffffu, send, half);
+    }
+  }
+  wsum[warp][lane] = v[0];
   __syncthreads();
   double D = 0.0;
   if (threadIdx.x < kIcpTerms)
@@ -426,7 +432,7 @@ __device__ __forceinline__ double icp_block_sum(double acc) {
 // One launch per tick replaces one launch per iteration, and sessions whose levels stop
 // early leave their SMs to the others.
 template <int PPT>
-__global__ void __launch_bounds__(kIcpThreads, 3)
+__global__ void __launch_bounds__(kIcpThreads, 2)
     k_icp_cluster(const SessionDesc* __restrict__ descs) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
@@ -440,10 +446,12 @@ __global__ void __launch_bounds__(kIcpThreads, 3)
   __shared__ float bR[9], bt[3];  // block 0: the estimate after the host step
   __shared__ int bflags[2];       // block 0: status, level_done
   __shared__ double sums[kIcpTerms];
+  __shared__ IcpLm lm;  // block 0: the tracker state during the kernel
   if (threadIdx.x < 9) sR[threadIdx.x] = ts->R[threadIdx.x];
   if (threadIdx.x < 3) st[threadIdx.x] = ts->t[threadIdx.x];
   if (threadIdx.x < 21) reinterpret_cast<float*>(&sp)[threadIdx.x] = reinterpret_cast<const float*>(&ts->xf)[threadIdx.x];
   const int status0 = ts->status;
+  if (rank == 0 && threadIdx.x == 0) lm_copy(&lm, ts);
   // every block has read the initial state before block 0 writes any of it
   cluster.sync();
   if (status0 != 0) return;
@@ -455,12 +463,15 @@ __global__ void __launch_bounds__(kIcpThreads, 3)
     const int ncb = photo ? (s.W * s.H + per_block - 1) / per_block : 0;
     for (int iter = 0; iter < s.iters[level]; ++iter) {
       const float3 tc = f3(st[0], st[1], st[2]);
-      double acc = 0.0;
+      double acc[kIcpTerms];
+#pragma unroll
+      for (int k = 0; k < kIcpTerms; ++k) acc[k] = 0.0;
       for (int vb = rank; vb < nblocks; vb += C) icp_depth_rows<PPT>(s, level, vb, sR, tc, sp, acc);
       double D = icp_block_sum(acc);
       if (threadIdx.x < kIcpTerms) part[0][threadIdx.x] = D;
       if (photo) {
-        acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < kIcpTerms; ++k) acc[k] = 0.0;
         for (int vb = rank; vb < ncb; vb += C) icp_color_rows<PPT>(s, vb, sR, tc, acc);
         D = icp_block_sum(acc);
         if (threadIdx.x < kIcpTerms) part[1][threadIdx.x] = D;
@@ -481,12 +492,12 @@ __global__ void __launch_bounds__(kIcpThreads, 3)
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-          ts->icp_iters[level] += 1u;
-          icp_host_step(ts, sums, iter, s.icp_min_count[level]);
-          for (int k = 0; k < 9; ++k) bR[k] = ts->R[k];
-          for (int k = 0; k < 3; ++k) bt[k] = ts->t[k];
-          bflags[0] = ts->status;
-          bflags[1] = ts->level_done;
+          lm.icp_iters[level] += 1u;
+          icp_host_step(&lm, sums, iter, s.icp_min_count[level]);
+          for (int k = 0; k < 9; ++k) bR[k] = lm.R[k];
+          for (int k = 0; k < 3; ++k) bt[k] = lm.t[k];
+          bflags[0] = lm.status;
+          bflags[1] = lm.level_done;
         }
       }
       cluster.sync();  // block 0's new estimate is visible to every block
@@ -502,12 +513,14 @@ __global__ void __launch_bounds__(kIcpThreads, 3)
       }
       __syncthreads();
       if (flags[0] != 0) {  // tracking lost: every block leaves together
+        if (rank == 0 && threadIdx.x == 0) lm_copy(ts, &lm);
         cluster.sync();     // (block 0's shared memory stays alive until all have read it)
         return;
       }
       if (flags[1]) break;
     }
   }
+  if (rank == 0 && threadIdx.x == 0) lm_copy(ts, &lm);
   cluster.sync();  // no block leaves while another may still read block 0's shared memory
 }
 

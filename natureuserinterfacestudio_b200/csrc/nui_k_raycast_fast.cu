@@ -165,8 +165,11 @@ __global__ void __launch_bounds__(256, 4) k_raycast_finish_fast(const SessionDes
       const float tc = fmaf((float)kc, step, e.x), tn = fmaf((float)(kc + 1), step, e.x);
       int gx, gy, gz;
       V.voxel_of(add3(start, mul3(dir, tn)), gx, gy, gz);
-      const float Ftdt = V.trilinear(add3(start, mul3(dir, tn)));
-      const float Ft = isnan(Ftdt) ? Ftdt : V.trilinear(add3(start, mul3(dir, tc)));
+      // both samples read together (the reference skips the second when the first is NaN;
+      // the result is the same)
+      const float Ftdt = V.trilinear_inl(add3(start, mul3(dir, tn)));
+      const float Ftc = V.trilinear_inl(add3(start, mul3(dir, tc)));
+      const float Ft = isnan(Ftdt) ? Ftdt : Ftc;
       if (!isnan(Ft)) {
         const float Ts = tc - step * __fdividef(Ft, Ftdt - Ft);
         const float3 vf = add3(start, mul3(dir, Ts));
@@ -176,15 +179,16 @@ __global__ void __launch_bounds__(256, 4) k_raycast_finish_fast(const SessionDes
         int hx, hy, hz;
         V.voxel_of(add3(start, mul3(dir, tc)), hx, hy, hz);
         if (hx > 1 && hy > 1 && hz > 1 && hx < V.rx - 2 && hy < V.ry - 2 && hz < V.rz - 2) {
-          float3 q, n;
-          q = vf; q.x += s.cell[0]; const float fx1 = V.trilinear(q);
-          q = vf; q.x -= s.cell[0]; const float fx2 = V.trilinear(q);
+          // the six samples in two groups of three, each group's 24 voxel reads in flight
+          float3 n;
+          const float fx1 = V.trilinear_inl(f3(vf.x + s.cell[0], vf.y, vf.z));
+          const float fy1 = V.trilinear_inl(f3(vf.x, vf.y + s.cell[1], vf.z));
+          const float fz1 = V.trilinear_inl(f3(vf.x, vf.y, vf.z + s.cell[2]));
+          const float fx2 = V.trilinear_inl(f3(vf.x - s.cell[0], vf.y, vf.z));
+          const float fy2 = V.trilinear_inl(f3(vf.x, vf.y - s.cell[1], vf.z));
+          const float fz2 = V.trilinear_inl(f3(vf.x, vf.y, vf.z - s.cell[2]));
           n.x = fx1 - fx2;
-          q = vf; q.y += s.cell[1]; const float fy1 = V.trilinear(q);
-          q = vf; q.y -= s.cell[1]; const float fy2 = V.trilinear(q);
           n.y = fy1 - fy2;
-          q = vf; q.z += s.cell[2]; const float fz1 = V.trilinear(q);
-          q = vf; q.z -= s.cell[2]; const float fz2 = V.trilinear(q);
           n.z = fz1 - fz2;
           nout = w0(normalize3(n));
         }

@@ -57,9 +57,12 @@ struct RayVol {
       gz = round_div(p.z, c2, i2);
     }
   }
-  // Out of line: called at eight places of the hit refinement, whose inlined copies
+  // Out of line: called at eight places of the exact hit refinement, whose inlined copies
   // overflow the instruction cache.
-  __device__ __noinline__ float trilinear(float3 p) const {
+  __device__ __noinline__ float trilinear(float3 p) const { return trilinear_inl(p); }
+  // Inlined form: the tolerance-mode refinement evaluates several samples in one
+  // expression, so that their voxel loads are in flight together.
+  __device__ __forceinline__ float trilinear_inl(float3 p) const {
     int gx, gy, gz;
     voxel_of(p, gx, gy, gz);
     if (gx <= 0 || gx >= rx - 1) return qnan();
