@@ -5,7 +5,8 @@
 // transform it by the running estimate, project into the previous camera with
 // full-resolution intrinsics, bilinearly sample the world reference normal and vertex
 // (icp.cl:192-220; a tap NaN -> no match), and if |q - p| < distThres form the row
-// [n x p, n | n.(q - p)].  Each thread accumulates the 29 products of its pixels in FP64;
+// [n x p, n | n.(q - p)].  Each thread accumulates the 29 products of its pixels in FP64
+// (exact products of the FP32 row values, fused multiply-adds);
 // blocks reduce them with warp shuffles and shared memory; the cluster's first block adds
 // the blocks' sums (distributed shared memory, fixed order) and runs the host step of
 // NuiKinfuOpenCLDepthTracker::IterativeClosestPoint (NuiKinfuOpenCLDepthTracker.cpp:324-496):
@@ -179,12 +180,10 @@ __device__ __forceinline__ bool llt_solve6(const double (&A)[6][6], const double
   return true;
 }
 
-// Rz(g) Ry(b) Rx(a) (AngleAxis composition at NuiKinfuOpenCLDepthTracker.cpp:486)
-__device__ __forceinline__ void euler_zyx(double a, double b, double g, double (&R)[9]) {
-  double ca, sa, cb, sb, cg, sg;
-  sincos(a, &sa, &ca);
-  sincos(b, &sb, &cb);
-  sincos(g, &sg, &cg);
+// Rz(g) Ry(b) Rx(a) (AngleAxis composition at NuiKinfuOpenCLDepthTracker.cpp:486), from
+// the angles' sines and cosines
+__device__ __forceinline__ void euler_zyx(double sa, double ca, double sb, double cb, double sg, double cg,
+                                          double (&R)[9]) {
   const double Rz[9] = {cg, -sg, 0, sg, cg, 0, 0, 0, 1};
   const double Ry[9] = {cb, 0, sb, 0, 1, 0, -sb, 0, cb};
   const double Rx[9] = {1, 0, 0, 0, ca, -sa, 0, sa, ca};
@@ -236,85 +235,138 @@ __device__ __forceinline__ void lm_copy(T* d, const U* s) {
   for (int k = 0; k < kMaxLevels; ++k) d->icp_iters[k] = s->icp_iters[k];
 }
 
-// LM step on the reduced sums (runs on one thread of the cluster's first block).
-template <class St>
-__device__ __noinline__ void icp_host_step(St* ts, const double* sums, int iter, unsigned min_count) {
-  float err = (float)sums[27];
-  const float cnt = (float)sums[28];
-  err = (cnt > 0.f) ? sqrtf(err) / cnt : 3.402823466e+38f;
-  ts->error = err;
-  ts->count = cnt;
-  ts->iterations_run += 1;
-  if (iter == 0) {  // level start: lambda = 1, Rgood = Rcurr, errorOld = 1e20
-    ts->lambda = 1.0f;
-    for (int i = 0; i < 9; ++i) ts->Rg[i] = ts->R[i];
-    for (int i = 0; i < 3; ++i) ts->tg[i] = ts->t[i];
-    ts->err_old = 1e20f;
-    ts->level_done = 0;
-  }
-  if (cnt < (float)min_count || err > ts->err_old) {
-    ts->lambda *= 10.0f;
-    for (int i = 0; i < 9; ++i) ts->R[i] = ts->Rg[i];
-    for (int i = 0; i < 3; ++i) ts->t[i] = ts->tg[i];
-    if (iter == 0) {
-      ts->level_done = 1;
-      return;
+// The LM step on the reduced sums (NuiKinfuOpenCLDepthTracker.cpp:324-496), spread over
+// the threads of the cluster's first block in phases separated by block barriers: the
+// bookkeeping on one thread, the 27 normalised sums on 27 threads, the Cholesky solve and
+// the determinant on two threads of different warps at once, the increments' sines and
+// cosines on three threads, the composition on one.  Every value comes from the same FP64
+// operations in the same order as a one-thread step; only their latencies overlap (one
+// thread took ~8 us per iteration, while the cluster's other blocks waited).  All threads
+// of the block call it.
+struct IcpStepScratch {
+  double A[6][6], b[6], x[6], det, sc[6];
+  float cnt;
+  int go, solved;
+};
+__device__ __noinline__ void icp_host_step(IcpLm* ts, IcpStepScratch& w, const double* sums, int iter,
+                                              unsigned min_count) {
+  const int tid = threadIdx.x;
+  if (tid == 0) {  // bookkeeping: error, LM accept / reject
+    float err = (float)sums[27];
+    const float cnt = (float)sums[28];
+    err = (cnt > 0.f) ? sqrtf(err) / cnt : 3.402823466e+38f;
+    ts->error = err;
+    ts->count = cnt;
+    ts->iterations_run += 1;
+    w.cnt = cnt;
+    w.go = 1;
+    if (iter == 0) {  // level start: lambda = 1, Rgood = Rcurr, errorOld = 1e20
+      ts->lambda = 1.0f;
+      for (int i = 0; i < 9; ++i) ts->Rg[i] = ts->R[i];
+      for (int i = 0; i < 3; ++i) ts->tg[i] = ts->t[i];
+      ts->err_old = 1e20f;
+      ts->level_done = 0;
     }
-  } else {
-    ts->lambda /= 10.0f;
-    for (int i = 0; i < 9; ++i) ts->Rg[i] = ts->R[i];
-    for (int i = 0; i < 3; ++i) ts->tg[i] = ts->t[i];
-    ts->err_old = err;
-    for (int k = 0; k < 27; ++k) ts->good[k] = sums[k];
-  }
-  double A[6][6], b[6];
-#pragma unroll
-  for (int i = 0, sh = 0; i < 6; ++i) {
-#pragma unroll
-    for (int j = i; j < 7; ++j, ++sh) {
-      const double v = ts->good[sh] / (double)cnt;
-      if (j == 6)
-        b[i] = v;
-      else
-        A[j][i] = A[i][j] = v;
+    if (cnt < (float)min_count || err > ts->err_old) {
+      ts->lambda *= 10.0f;
+      for (int i = 0; i < 9; ++i) ts->R[i] = ts->Rg[i];
+      for (int i = 0; i < 3; ++i) ts->t[i] = ts->tg[i];
+      if (iter == 0) {
+        ts->level_done = 1;
+        w.go = 0;
+      }
+    } else {
+      ts->lambda /= 10.0f;
+      for (int i = 0; i < 9; ++i) ts->Rg[i] = ts->R[i];
+      for (int i = 0; i < 3; ++i) ts->tg[i] = ts->t[i];
+      ts->err_old = err;
+      for (int k = 0; k < 27; ++k) ts->good[k] = sums[k];
     }
-    A[i][i] *= (double)(1.0f + ts->lambda);
   }
+  __syncthreads();
+  if (!w.go) return;
+  if (tid < 27) {  // sum sh = (i, j) of the upper triangle of [J|r] by rows, over the count
+    int i = 0, j = tid;
+    while (j >= 7 - i) j -= 7 - i, ++i;
+    j += i;
+    double v = ts->good[tid] / (double)w.cnt;
+    if (j == 6) {
+      w.b[i] = v;
+    } else {
+      if (i == j) v *= (double)(1.0f + ts->lambda);
+      w.A[i][j] = v;
+      w.A[j][i] = v;
+    }
+  }
+  __syncthreads();
   // a singular system (|det| < 1e-15 or NaN) or a failed factorisation loses tracking; the
-  // solve runs first because the determinant's elimination overwrites A
-  double x[6];
-  if (!llt_solve6(A, b, x) || !(fabs(det6(A)) >= 1e-15)) {
-    ts->status = 3;
-    return;
+  // determinant's elimination works on a copy
+  if (tid == 0) {
+    double A[6][6], b[6], x[6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      b[r] = w.b[r];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) A[r][c] = w.A[r][c];
+    }
+    w.solved = llt_solve6(A, b, x) ? 1 : 0;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) w.x[r] = x[r];
+  } else if (tid == 32) {
+    double A[6][6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) A[r][c] = w.A[r][c];
+    w.det = det6(A);
   }
-  const float al = (float)x[0], be = (float)x[1], ga = (float)x[2];
-  if (al * al + be * be + ga * ga < 1e-6f) {
-    ts->level_done = 1;
-    return;
+  __syncthreads();
+  if (tid == 0) {
+    if (!w.solved || !(fabs(w.det) >= 1e-15)) {
+      ts->status = 3;
+      w.go = 0;
+    } else {
+      const float al = (float)w.x[0], be = (float)w.x[1], ga = (float)w.x[2];
+      if (al * al + be * be + ga * ga < 1e-6f) {
+        ts->level_done = 1;
+        w.go = 0;
+      }
+    }
   }
-  double Ri[9];
-  euler_zyx(al, be, ga, Ri);
-  float t0[3], R0[9];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) t0[i] = ts->t[i];
-#pragma unroll
-  for (int i = 0; i < 9; ++i) R0[i] = ts->R[i];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    double s = 0;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) s += Ri[k * 3 + i] * (double)t0[k];
-    ts->t[i] = (float)(s + (double)(float)x[3 + i]);
+  __syncthreads();
+  if (!w.go) return;
+  if (tid < 3) {  // sin and cos of the increment's angles (alpha, beta, gamma)
+    double sn, cs;
+    sincos((double)(float)w.x[tid], &sn, &cs);
+    w.sc[2 * tid] = sn;
+    w.sc[2 * tid + 1] = cs;
   }
+  __syncthreads();
+  if (tid == 0) {
+    double Ri[9];
+    euler_zyx(w.sc[0], w.sc[1], w.sc[2], w.sc[3], w.sc[4], w.sc[5], Ri);
+    float t0[3], R0[9];
 #pragma unroll
-  for (int i = 0; i < 3; ++i)
+    for (int i = 0; i < 3; ++i) t0[i] = ts->t[i];
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
+    for (int i = 0; i < 9; ++i) R0[i] = ts->R[i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
       double s = 0;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) s += Ri[k * 3 + i] * (double)R0[k * 3 + j];
-      ts->R[i * 3 + j] = (float)s;
+      for (int k = 0; k < 3; ++k) s += Ri[k * 3 + i] * (double)t0[k];
+      ts->t[i] = (float)(s + (double)(float)w.x[3 + i]);
     }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        double s = 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s += Ri[k * 3 + i] * (double)R0[k * 3 + j];
+        ts->R[i * 3 + j] = (float)s;
+      }
+  }
 }
 
 // The 29 sums of the depth rows of one block of pixels (kIcpThreads x PPT consecutive
@@ -359,13 +411,16 @@ __device__ __forceinline__ void icp_depth_rows(const SessionDesc& s, int level, 
     const float dist = sqrtf(dot3(diff, diff));
     if (!(dist < s.dist_thr)) continue;
     const float3 r0 = cross3(rn, pv);
-    const float c7[7] = {r0.x, r0.y, r0.z, rn.x, rn.y, rn.z, dot3(rn, diff)};
+    // the row's seven FP32 values widened once; each product is exact in FP64 and enters
+    // its sum with one rounding (fused multiply-add)
+    const double c7[7] = {(double)r0.x, (double)r0.y, (double)r0.z, (double)rn.x, (double)rn.y, (double)rn.z,
+                          (double)dot3(rn, diff)};
     int sh = 0;
 #pragma unroll
     for (int a = 0; a < 6; ++a)
 #pragma unroll
-      for (int b = a; b < 7; ++b, ++sh) acc[sh] += (double)(c7[a] * c7[b]);
-    acc[27] += (double)(c7[6] * c7[6]);
+      for (int b = a; b < 7; ++b, ++sh) acc[sh] = fma(c7[a], c7[b], acc[sh]);
+    acc[27] = fma(c7[6], c7[6], acc[27]);
     acc[28] += 1.0;
   }
 }
@@ -447,6 +502,7 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
   __shared__ int bflags[2];       // block 0: status, level_done
   __shared__ double sums[kIcpTerms];
   __shared__ IcpLm lm;  // block 0: the tracker state during the kernel
+  __shared__ IcpStepScratch hw;  // block 0: the LM step's intermediate values
   if (threadIdx.x < 9) sR[threadIdx.x] = ts->R[threadIdx.x];
   if (threadIdx.x < 3) st[threadIdx.x] = ts->t[threadIdx.x];
   if (threadIdx.x < 21) reinterpret_cast<float*>(&sp)[threadIdx.x] = reinterpret_cast<const float*>(&ts->xf)[threadIdx.x];
@@ -491,9 +547,10 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
           sums[threadIdx.x] = a;
         }
         __syncthreads();
+        if (threadIdx.x == 0) lm.icp_iters[level] += 1u;
+        icp_host_step(&lm, hw, sums, iter, s.icp_min_count[level]);
+        __syncthreads();
         if (threadIdx.x == 0) {
-          lm.icp_iters[level] += 1u;
-          icp_host_step(&lm, sums, iter, s.icp_min_count[level]);
           for (int k = 0; k < 9; ++k) bR[k] = lm.R[k];
           for (int k = 0; k < 3; ++k) bt[k] = lm.t[k];
           bflags[0] = lm.status;

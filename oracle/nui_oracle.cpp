@@ -621,7 +621,9 @@ ORC_API long orc_fetch_points(const int16_t* vol, const uint8_t* cvol, const Orc
 
 // ---------------------------------------------------------------------------------
 // A7  icp_block_kernel + compute_sums (icp.cl:222-326): per-pixel rows, summed here in
-// double.  `vcur` is the level's vertex map (w x h), `vref`/`nref` the full-size world
+// double, each product of the row's float values taken exactly (a double fused
+// multiply-add) -- the reference rounds the products to float and sums in float; the
+// sums agree within its float rounding.  `vcur` is the level's vertex map (w x h), `vref`/`nref` the full-size world
 // reference maps (cam->W x cam->H), Rc/tc the current estimate (row-major), prev the
 // previous camera transform.  sums[0..26] = upper triangle of [J|r]^T[J|r] by rows,
 // sums[27] = sum r^2, sums[28] = count.
@@ -683,6 +685,13 @@ ORC_API void orc_icp_rows(const float* vcur, int w, int h, const float* vref, co
                   for (int b = a; b < 7; ++b) cr[s++] = c7[a] * c7[b];
                 cr[s++] = c7[6] * c7[6];
                 cr[s++] = 1.0f;
+                // the sums take each product exactly (FP64 fused multiply-add of the FP32
+                // row values), not the FP32-rounded rows above
+                s = 0;
+                for (int a = 0; a < 6; ++a)
+                  for (int b = a; b < 7; ++b, ++s) acc[s] = std::fma((double)c7[a], (double)c7[b], acc[s]);
+                acc[27] = std::fma((double)c7[6], (double)c7[6], acc[27]);
+                acc[28] += 1.0;
                 ok = true;
               }
             }
@@ -693,8 +702,6 @@ ORC_API void orc_icp_rows(const float* vcur, int w, int h, const float* vref, co
         for (int k = 0; k < 29; ++k) cr[k] = 0.f;
       if (rows)
         for (int k = 0; k < 29; ++k) rows[29 * i + k] = cr[k];
-      if (ok)
-        for (int k = 0; k < 29; ++k) acc[k] += (double)cr[k];
     }
   }
   for (int k = 0; k < 29; ++k) {
