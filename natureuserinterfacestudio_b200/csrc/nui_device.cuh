@@ -59,9 +59,6 @@ struct TrackState {
   // tolerance-mode integration: tiles listed by the cull; blocks of the integration done
   // (both zero between integrations)
   unsigned int fast_count, fast_done;
-  // voxel-hash raycast: ray indices handed out; blocks of the march done (both zero
-  // between raycasts)
-  unsigned int hray_next, hray_done;
 };
 
 // What one session does in the current tick (host-written, read by every kernel).

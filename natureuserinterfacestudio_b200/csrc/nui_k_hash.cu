@@ -899,108 +899,28 @@ __device__ __forceinline__ void hash_finish(HashRead<HF>& R, const SessionDesc& 
   if (s.cmap) s.cmap[pid] = col;
 }
 
-// Ray index r -> pixel: indices run through tiles of tw x (32 / tw) pixels in raster order
-// of the tiles, 32 indices a tile (neighbouring rays march alike); -1 past the image.
-__device__ __forceinline__ int hash_ray_pixel(const SessionDesc& s, unsigned r, int tw) {
-  const int th = 32 / tw, tiles_x = (s.W + tw - 1) / tw;
-  const int t = (int)(r >> 5), q = (int)(r & 31u);
-  const int px = (t % tiles_x) * tw + q % tw, py = (t / tiles_x) * th + q / tw;
-  return (px < s.W && py < s.H) ? py * s.W + px : -1;
-}
-
-// The march with lanes that refill: the rays of a frame march very different distances
-// (8-voxel steps through unallocated blocks, max(sdf * 2.4, 1) inside allocated ones), so a
-// warp that marched 32 fixed rays ran at a third of its lanes.  Here a lane whose ray ends
-// takes the session's next ray index (one atomic per warp and round) and every round
-// advances each lane's ray by one step of castRay; the warps of a session leave when its
-// rays are handed out and done.  Each ray's arithmetic is castRay's, step for step, so the
-// results are those of one thread per pixel.  The session's last block to finish resets the
-// ray counter for the next frame.
 template <int HF>
 __global__ void __launch_bounds__(128, 8) k_hash_raycast(const SessionDesc* __restrict__ descs, int tw) {
   const SessionDesc& s = descs[blockIdx.y];
   if (!s.hash || s.fwd || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
-  const int th = 32 / tw;
-  const unsigned nidx = (unsigned)(((s.W + tw - 1) / tw) * ((s.H + th - 1) / th)) * 32u;
-  const int lane = threadIdx.x & 31;
-  const float stepScale = s.mu * (1.0f / s.voxel) * 0.6f;
+  // each warp shades a tw x (32 / tw) pixel tile, a block 2 x 2 of them (neighbouring rays
+  // march alike; tw is tuned)
+  const int th = 32 / tw, bw = 2 * tw, bh = 2 * th;
+  const int tiles_x = (s.W + bw - 1) / bw;
+  if ((int)blockIdx.x >= tiles_x * ((s.H + bh - 1) / bh)) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int px = ((int)blockIdx.x % tiles_x) * bw + (warp & 1) * tw + lane % tw;
+  const int py = ((int)blockIdx.x / tiles_x) * bh + (warp >> 1) * th + lane / tw;
+  if (px >= s.W || py >= s.H) return;
+  const int pid = py * s.W + px;
   HashRead<HF> R{s, 0, 0, 0, -1};
-  int pid = -1;
-  bool drained = false;
-  float3 pr = f3(0.f, 0.f, 0.f), dir = f3(0.f, 0.f, 0.f);
-  float total = 0.f, totalMax = 0.f, sdfv = 1.0f;
-  for (;;) {
-    // lanes without a ray take the next indices, in lane order
-    const unsigned need = __ballot_sync(0xffffffffu, pid < 0 && !drained);
-    if (need) {
-      const int leader = __ffs(need) - 1;
-      unsigned base = 0;
-      if (lane == leader) base = atomicAdd(&s.ts->hray_next, (unsigned)__popc(need));
-      base = __shfl_sync(0xffffffffu, base, leader);
-      if ((need >> lane) & 1u) {
-        const unsigned r = base + (unsigned)__popc(need & ((1u << lane) - 1u));
-        if (r >= nidx) {
-          drained = true;
-        } else {
-          const int p = hash_ray_pixel(s, r, tw);  // -1: past the image, ask again
-          if (p >= 0) {
-            pid = p;
-            sdfv = 1.0f;
-            hash_ray<HF>(s, pid, pr, total, totalMax, dir);
-          }
-        }
-      }
-    }
-    if (!__any_sync(0xffffffffu, pid >= 0 || !drained)) break;
-    if (pid < 0) continue;
-    // one step of castRay's march (hash_march's loop body)
-    bool done = !(total < totalMax);
-    if (!done) {
-      const int vx = (int)roundf(pr.x), vy = (int)roundf(pr.y), vz = (int)roundf(pr.z);
-      const int bi = R.find(vx, vy, vz);
-      float stepLen;
-      if (bi < 0) {
-        sdfv = 1.0f;
-        stepLen = 8.0f;
-      } else {
-        sdfv = HVox<HF>::load(s.hsdf, (unsigned)bi);
-        if (sdfv <= 0.1f && sdfv >= -0.5f) {
-          const int ix = (int)floorf(pr.x), iy = (int)floorf(pr.y), iz = (int)floorf(pr.z);
-          const float3 cf = f3(pr.x - (float)ix, pr.y - (float)iy, pr.z - (float)iz);
-          typename HashRead<HF>::Hood h;
-          R.template hood<0, 1>(h, ix, iy, iz);
-          float v1 = R.hood_sdf(h, ix, iy, iz), v2 = R.hood_sdf(h, ix + 1, iy, iz);
-          float r1 = (1.0f - cf.x) * v1 + cf.x * v2;
-          v1 = R.hood_sdf(h, ix, iy + 1, iz);
-          v2 = R.hood_sdf(h, ix + 1, iy + 1, iz);
-          r1 = (1.0f - cf.y) * r1 + cf.y * ((1.0f - cf.x) * v1 + cf.x * v2);
-          v1 = R.hood_sdf(h, ix, iy, iz + 1);
-          v2 = R.hood_sdf(h, ix + 1, iy, iz + 1);
-          float r2 = (1.0f - cf.x) * v1 + cf.x * v2;
-          v1 = R.hood_sdf(h, ix, iy + 1, iz + 1);
-          v2 = R.hood_sdf(h, ix + 1, iy + 1, iz + 1);
-          r2 = (1.0f - cf.y) * r2 + cf.y * ((1.0f - cf.x) * v1 + cf.x * v2);
-          sdfv = (1.0f - cf.z) * r1 + cf.z * r2;
-        }
-        stepLen = fmaxf(sdfv * stepScale, 1.0f);
-      }
-      if (sdfv <= 0.0f) {
-        done = true;
-      } else {
-        pr = add3(pr, mul3(dir, stepLen));
-        total += stepLen;
-      }
-    }
-    if (done) {  // the march's end point and last sdf wait in the vertex map for k_hash_finish
-      s.vref[pid] = make_float4(pr.x, pr.y, pr.z, sdfv);
-      pid = -1;
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0 && atomicAdd(&s.ts->hray_done, 1u) == gridDim.x - 1) {
-    s.ts->hray_next = 0u;
-    s.ts->hray_done = 0u;
-  }
+  const float stepScale = s.mu * (1.0f / s.voxel) * 0.6f;
+  float3 pr, dir;
+  float total, totalMax, sdfv = 1.0f;
+  hash_ray<HF>(s, pid, pr, total, totalMax, dir);
+  hash_march<HF>(R, s, pr, total, totalMax, dir, stepScale, sdfv);
+  // the march's end point and last sdf wait in the vertex map for k_hash_finish
+  s.vref[pid] = make_float4(pr.x, pr.y, pr.z, sdfv);
 }
 
 // The surface refinement, normal and colour of every pixel after the march: a kernel of

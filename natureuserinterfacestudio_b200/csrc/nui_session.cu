@@ -619,9 +619,7 @@ void launch_hash_raycast(const BatchPlan& p, const SessionDesc* d0, cudaStream_t
   }
   if (!p.hashPlain) return;
   const int tw = p.tune.hash_raycast_tile_width;
-  // the march's warps refill their lanes from the session's rays: enough blocks per
-  // session to fill the SMs about twice over between all hash sessions
-  const unsigned tiles = std::min(ray_blocks(p, tw), std::max(16u, 2368u / hn));
+  const unsigned tiles = ray_blocks(p, tw);
   if (p.hashMask & 1) k_hash_raycast<0><<<dim3(tiles, hn), 128, 0, st>>>(d, tw);
   if (p.hashMask & 2) k_hash_raycast<1><<<dim3(tiles, hn), 128, 0, st>>>(d, tw);
   if (p.hashMask & 1) k_hash_finish<0><<<dim3(px, hn), 256, 0, st>>>(d);
