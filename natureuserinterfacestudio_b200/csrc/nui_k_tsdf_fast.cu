@@ -9,34 +9,20 @@
 // the int16 and FP32 formats keep the exact kernel (nui_k_tsdf.cu).  This file is compiled
 // with contraction on.
 //
-// Work decomposition (HBM-bound by design): the volume is cut into tiles of 32 (x) x 8 (y)
-// x 8 (z) voxels.  k_integrate_cull tests every tile on one thread: tiles entirely behind
-// the camera, projecting outside the image, or farther from the camera than the largest
-// ray depth of the pixel tiles they project to plus the truncation are dropped without a
-// memory access; the kept ones are appended to the session's tile list.  k_integrate_fast
-// then runs the listed tiles, dealt round robin to all its warps (the kept tiles cluster
-// in the frustum, so a fixed tile-to-warp map would leave most warps idle), one warp per
-// tile, lane = x,
-// so every row a warp touches is one contiguous 64 B run of the tsdf plane and 32 B of the
-// weight plane: the update pass over the tile's 64 rows (only updated voxels are read and
-// written), then -- for the 8^3 bricks of the tile that had an update -- the brick
-// classification that the exact path leaves to k_brick_summary (every voxel of such a
-// brick read once; the voxels just written come back from L2).
+// Work decomposition: the volume is cut into tiles of 32 (x) x 8 (y) x 8 (z) voxels.
+// k_integrate_cull tests every tile on one thread: tiles entirely behind the camera,
+// projecting outside the image, or farther from the camera than the largest ray depth of
+// the pixel tiles they project to plus the truncation are dropped without a memory access;
+// the kept ones are appended to the session's tile list.  k_integrate_fast deals the listed
+// tiles round robin to its warps (the kept tiles cluster in the frustum, so a fixed
+// tile-to-warp map would leave most warps idle), lane = x: a tile's depth pixels and voxel
+// rows are brought into the warp's shared memory by asynchronous copies, all 64 rows at
+// once, then updated from there (only updated voxels are written back), and the 8^3 bricks
+// of the tile that had an update are re-classified from the same shared copy -- the brick
+// summary the exact path leaves to k_brick_summary.
 #include "nui_device.cuh"
 
 namespace nui {
-
-template <int FMT>
-__device__ __forceinline__ void fast_load(const SessionDesc& s, size_t i, float& F, int& W) {
-  if (FMT == 2) {
-    F = __half2float(reinterpret_cast<const __half*>(s.vol)[i]);
-    W = s.wvol[i];
-  } else {
-    const __half2 v = reinterpret_cast<const __half2*>(s.vol)[i];
-    F = __low2float(v);
-    W = (int)__high2float(v);
-  }
-}
 
 // Tile culling, one thread per tile: a tile can hold an updated voxel only if part of it
 // is in front of the camera, projects into the image, and is no farther from the camera
@@ -120,17 +106,64 @@ __global__ void __launch_bounds__(256) k_integrate_cull(const SessionDesc* __res
   if (keep) s.fast_tiles[base + __popc(kept & ((1u << lane) - 1u))] = (unsigned)tile;
 }
 
-// The tiles the cull kept: a warp reads the flags of 32 consecutive tiles and runs the ones
-// that are set, one after the other.
+// Asynchronous copies global -> shared (cp.async): the data lands in shared memory without
+// passing through registers, so a lane can have a whole tile's requests in flight.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+               "l"(gmem));
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+               "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Shared memory of one warp (kFastWarpSmem bytes): the depth each voxel of the tile
+// projects to (NaN: none), and the tile's voxels (64 rows of 32).
 template <int FMT>
-__global__ void __launch_bounds__(32 * kFastWarps, 2) k_integrate_fast(const SessionDesc* __restrict__ descs) {
+struct FastTileSmem {
+  float* dep;  // [64][32]
+  __half* fh;  // F16_U8: [64][32] tsdf
+  uint8_t* wb; // F16_U8: [64][32] weight
+  __half2* f2; // F16_F16: [64][32] (tsdf, weight)
+  __device__ explicit FastTileSmem(unsigned char* base) {
+    dep = reinterpret_cast<float*>(base);
+    fh = reinterpret_cast<__half*>(base + 64 * 32 * 4);
+    wb = base + 64 * 32 * 4 + 64 * 32 * 2;
+    f2 = reinterpret_cast<__half2*>(base + 64 * 32 * 4);
+  }
+  __device__ __forceinline__ void get(int i, float& F, int& W) const {
+    if (FMT == 2) {
+      F = __half2float(fh[i]);
+      W = wb[i];
+    } else {
+      const __half2 v = f2[i];
+      F = __low2float(v);
+      W = (int)__high2float(v);
+    }
+  }
+};
+
+// The tiles the cull listed, dealt round robin to the warps.  Per tile, in three phases:
+//  1. every row of the tile is requested at once: each lane projects its voxel and copies
+//     the depth pixel it lands on into shared memory (NaN when it lands on none), and the
+//     row's voxels are copied as 16-byte pieces (4 + 2 lanes for FP16 + u8, 8 for FP16 +
+//     FP16) -- 64 rows of requests in flight, one round trip for the tile;
+//  2. the update from shared memory: sd = depth - |voxel - camera|, the running average,
+//     stores of the updated voxels (and their new values into the shared copy);
+//  3. the 8^3 bricks of the tile that had an update are re-classified from the shared copy.
+// Rows that are not whole (a tile past the volume's x end) or not 16-byte aligned (x sizes
+// not a multiple of 16) are loaded lane by lane instead.
+template <int FMT>
+__global__ void __launch_bounds__(32 * kFastWarps, 3) k_integrate_fast(const SessionDesc* __restrict__ descs) {
+  extern __shared__ __align__(16) unsigned char fast_smem[];
   const SessionDesc& s = descs[blockIdx.y];
   if (s.kind < 0 || s.fmt != FMT || !s.ts->integrate) return;
   const int rx = s.res[0], ry = s.res[1], rz = s.res[2];
-  const int ntx = (rx + 31) >> 5, nty = (ry + 7) >> 3, ntz = (rz + 7) >> 3;
-  const int ntiles = ntx * nty * ntz;
+  const int ntx = (rx + 31) >> 5, nty = (ry + 7) >> 3;
   const int lane = threadIdx.x & 31;
   const int nwarps = gridDim.x * kFastWarps;
+  const FastTileSmem<FMT> sm(fast_smem + (threadIdx.x >> 5) * kFastWarpSmem);
   const DevXform& m = s.ts->xf;
   float Ri[9];
 #pragma unroll
@@ -143,6 +176,8 @@ __global__ void __launch_bounds__(32 * kFastWarps, 2) k_integrate_fast(const Ses
   const float* __restrict__ depth = s.dscaled;
   const size_t slice = (size_t)rx * ry;
   const int hx = rx / 2, hy = ry / 2;
+  // whole rows start 16-byte aligned in every plane when the x size is a multiple of 16
+  const bool aligned = (rx & 15) == 0 && ((reinterpret_cast<uintptr_t>(s.vol) | reinterpret_cast<uintptr_t>(s.wvol)) & 15) == 0;
   unsigned int touched_total = 0, bricks = 0;
 
   const unsigned count = *(volatile const unsigned*)&s.ts->fast_count;
@@ -150,110 +185,141 @@ __global__ void __launch_bounds__(32 * kFastWarps, 2) k_integrate_fast(const Ses
     const int tile = (int)__ldg(s.fast_tiles + li);
     const int x0 = (tile % ntx) << 5, y0 = ((tile / ntx) % nty) << 3, z0 = (tile / (ntx * nty)) << 3;
     const int xn = min(32, rx - x0), yn = min(8, ry - y0), zn = min(8, rz - z0);
-
-    // ---- update pass: one z slice of the tile (8 rows, lane = x) at a time; the rows'
-    // projections first, then their 8 depth loads, then the 8 voxel loads of the rows that
-    // update, so that each phase has 8 independent loads in flight
     const int x = x0 + lane;
     const bool xin = lane < xn;
+    const bool whole = aligned && xn == 32;
     const float gx = ((float)(x - hx) + 0.5f) * c0 - t0;
     const float gy0 = ((float)(y0 - hy) + 0.5f) * c1 - t1;
     const float3 ey = f3(Ri[1] * c1, Ri[4] * c1, Ri[7] * c1);  // camera step of one y row
-    const float gx2 = gx * gx;
-    unsigned int touched = 0;  // voxels this lane updated in the tile
+
+    // ---- 1. requests: depth pixels and voxel rows of the whole tile
+    __syncwarp();  // the previous tile's shared copy is no longer read
 #pragma unroll 1
     for (int zz = 0; zz < zn; ++zz) {
       const float gz = ((float)(z0 + zz) + 0.5f) * c2 - t2;
       float3 v = f3(Ri[0] * gx + Ri[1] * gy0 + Ri[2] * gz, Ri[3] * gx + Ri[4] * gy0 + Ri[5] * gz,
                     Ri[6] * gx + Ri[7] * gy0 + Ri[8] * gz);
-      int pix[8];
-      unsigned in = 0;
-#pragma unroll
-      for (int yy = 0; yy < 8; ++yy) {
-        pix[yy] = 0;
-        if (xin && yy < yn && v.z > 0.f) {
+      const size_t zbase = (size_t)x0 + (size_t)rx * (size_t)y0 + slice * (size_t)(z0 + zz);
+#pragma unroll 2
+      for (int yy = 0; yy < yn; ++yy) {
+        const int r = zz * 8 + yy;
+        float* dslot = sm.dep + r * 32 + lane;
+        bool got = false;
+        if (xin && v.z > 0.f) {
           const float iz = __fdividef(1.f, v.z);
           // exact ties round up, as OpenCL's round(): they are frequent (pixel centres and
           // voxel centres sit on rational grids), and half-to-even would split them
           const int px = round_half_up(fx * v.x * iz + ccx), py = round_half_up(fy * v.y * iz + ccy);
           if (px >= 0 && py >= 0 && px < W && py < H) {
-            pix[yy] = py * W + px;
-            in |= 1u << yy;
+            cp_async4(dslot, depth + py * W + px);
+            got = true;
+          }
+        }
+        if (!got) *dslot = __int_as_float(0x7fffffff);
+        const size_t rb = zbase + (size_t)rx * yy;  // the row's first voxel
+        if (whole) {
+          if (FMT == 2) {
+            if (lane < 4) cp_async16(sm.fh + r * 32 + lane * 8, reinterpret_cast<const __half*>(s.vol) + rb + lane * 8);
+            else if (lane < 6) cp_async16(sm.wb + r * 32 + (lane - 4) * 16, s.wvol + rb + (lane - 4) * 16);
+          } else {
+            if (lane < 8) cp_async16(sm.f2 + r * 32 + lane * 4, reinterpret_cast<const __half2*>(s.vol) + rb + lane * 4);
+          }
+        } else if (xin) {
+          if (FMT == 2) {
+            sm.fh[r * 32 + lane] = reinterpret_cast<const __half*>(s.vol)[rb + lane];
+            sm.wb[r * 32 + lane] = s.wvol[rb + lane];
+          } else {
+            sm.f2[r * 32 + lane] = reinterpret_cast<const __half2*>(s.vol)[rb + lane];
           }
         }
         v = add3(v, ey);
       }
-      float sdf[8];
-#pragma unroll
-      for (int yy = 0; yy < 8; ++yy) sdf[yy] = (in >> yy) & 1u ? __ldg(depth + pix[yy]) : 0.f;
-      unsigned ok = 0;
-      const float gz2 = gz * gz;
-#pragma unroll
-      for (int yy = 0; yy < 8; ++yy) {
-        const float gy = gy0 + (float)yy * c1;
-        const float r2 = gx2 + gy * gy + gz2;
-        const float sd = sdf[yy] - r2 * rsqrtf(r2);
-        sdf[yy] = sd;
-        if (((in >> yy) & 1u) && sd >= -trunc) ok |= 1u << yy;  // false for a NaN depth
-      }
-      const size_t zbase = (size_t)x + (size_t)rx * (size_t)y0 + slice * (size_t)(z0 + zz);
-      float F[8];
-      int Wt[8];
-#pragma unroll
-      for (int yy = 0; yy < 8; ++yy)
-        if ((ok >> yy) & 1u) fast_load<FMT>(s, zbase + (size_t)rx * yy, F[yy], Wt[yy]);
-#pragma unroll
-      for (int yy = 0; yy < 8; ++yy) {
-        if (!((ok >> yy) & 1u)) continue;
-        const size_t vi = zbase + (size_t)rx * yy;
-        const float tsdf = fminf(1.0f, sdf[yy] * tinv);
-        const float tn = __fdividef(F[yy] * (float)Wt[yy] + tsdf, (float)(Wt[yy] + 1));
-        const int wn = min(Wt[yy] + 1, 128);
-        if (FMT == 2) {
-          reinterpret_cast<__half*>(s.vol)[vi] = __float2half_rn(tn);
-          s.wvol[vi] = (uint8_t)wn;
-        } else {
-          reinterpret_cast<__half2*>(s.vol)[vi] = __floats2half2_rn(tn, (float)wn);
-        }
-        touched += 1u;
-        if (s.cvol && s.bgra && fabsf(sdf[yy]) < trunc) {
-          const uchar4 nc = reinterpret_cast<const uchar4*>(s.bgra)[pix[yy]];
-          if (nc.w != 0) {
-            // the reference's arithmetic exactly (no product to contract, IEEE division):
-            // colours agree bit for bit wherever the same voxels are updated
-            const uchar4 vc = s.cvol[vi];
-            const float den = (float)vc.w + 1.f;
-            uchar4 o;
-            o.x = (unsigned char)fminf(fmaxf(((float)(vc.x * vc.w) + (float)nc.x) / den, 0.f), 255.f);
-            o.y = (unsigned char)fminf(fmaxf(((float)(vc.y * vc.w) + (float)nc.y) / den, 0.f), 255.f);
-            o.z = (unsigned char)fminf(fmaxf(((float)(vc.z * vc.w) + (float)nc.z) / den, 0.f), 255.f);
-            o.w = min((unsigned char)s.max_cw, (unsigned char)(vc.w + 1));
-            s.cvol[vi] = o;
+    }
+    cp_async_wait_all();
+    __syncwarp();
+
+    // ---- 2. the update, from shared memory
+    unsigned int touched = 0;  // voxels this lane updated in the tile
+    const float gx2 = gx * gx;
+    if (xin) {
+#pragma unroll 1
+      for (int zz = 0; zz < zn; ++zz) {
+        const float gz = ((float)(z0 + zz) + 0.5f) * c2 - t2;
+        const float gz2 = gz * gz;
+        const size_t zbase = (size_t)x + (size_t)rx * (size_t)y0 + slice * (size_t)(z0 + zz);
+#pragma unroll 2
+        for (int yy = 0; yy < yn; ++yy) {
+          const int r = zz * 8 + yy, i = r * 32 + lane;
+          const float gy = gy0 + (float)yy * c1;
+          const float r2 = gx2 + gy * gy + gz2;
+          const float sd = sm.dep[i] - r2 * rsqrtf(r2);
+          if (!(sd >= -trunc)) continue;  // also a voxel without a depth (NaN)
+          float F;
+          int Wt;
+          sm.get(i, F, Wt);
+          const size_t vi = zbase + (size_t)rx * yy;
+          const float tsdf = fminf(1.0f, sd * tinv);
+          const float tn = __fdividef(F * (float)Wt + tsdf, (float)(Wt + 1));
+          const int wn = min(Wt + 1, 128);
+          if (FMT == 2) {
+            const __half h = __float2half_rn(tn);
+            reinterpret_cast<__half*>(s.vol)[vi] = h;
+            s.wvol[vi] = (uint8_t)wn;
+            sm.fh[i] = h;
+            sm.wb[i] = (uint8_t)wn;
+          } else {
+            const __half2 h = __floats2half2_rn(tn, (float)wn);
+            reinterpret_cast<__half2*>(s.vol)[vi] = h;
+            sm.f2[i] = h;
+          }
+          touched += 1u;
+          if (s.cvol && s.bgra && fabsf(sd) < trunc) {
+            // the voxel's pixel again, by the same operations as in the request phase
+            float3 v = f3(Ri[0] * gx + Ri[1] * gy0 + Ri[2] * gz, Ri[3] * gx + Ri[4] * gy0 + Ri[5] * gz,
+                          Ri[6] * gx + Ri[7] * gy0 + Ri[8] * gz);
+            for (int k = 0; k < yy; ++k) v = add3(v, ey);
+            const float iz = __fdividef(1.f, v.z);
+            const int px = round_half_up(fx * v.x * iz + ccx), py = round_half_up(fy * v.y * iz + ccy);
+            const bool inimg = px >= 0 && py >= 0 && px < W && py < H;  // (a contraction may differ)
+            const uchar4 nc = inimg ? reinterpret_cast<const uchar4*>(s.bgra)[py * W + px] : make_uchar4(0, 0, 0, 0);
+            if (nc.w != 0) {
+              // the reference's arithmetic exactly (no product to contract, IEEE division):
+              // colours agree bit for bit wherever the same voxels are updated
+              const uchar4 vc = s.cvol[vi];
+              const float den = (float)vc.w + 1.f;
+              uchar4 o;
+              o.x = (unsigned char)fminf(fmaxf(((float)(vc.x * vc.w) + (float)nc.x) / den, 0.f), 255.f);
+              o.y = (unsigned char)fminf(fmaxf(((float)(vc.y * vc.w) + (float)nc.y) / den, 0.f), 255.f);
+              o.z = (unsigned char)fminf(fmaxf(((float)(vc.z * vc.w) + (float)nc.z) / den, 0.f), 255.f);
+              o.w = min((unsigned char)s.max_cw, (unsigned char)(vc.w + 1));
+              s.cvol[vi] = o;
+            }
           }
         }
       }
     }
     touched_total += touched;
-    // ---- classification of the bricks (lanes 8b .. 8b+7) that had an update
+    // ---- 3. classification of the bricks (lanes 8b .. 8b+7) that had an update, from the
+    // shared copy (which holds the values just written)
     const unsigned upd = __ballot_sync(0xffffffffu, touched != 0u);
     if (upd == 0u || !s.occ) continue;
     const bool mine = (upd >> (lane & ~7)) & 0xffu;
     bool weighted = false, unweighted = false, nonpos = false;
     if (mine && xin) {
-#pragma unroll 8
-      for (int r = 0; r < 64; ++r) {
-        const int yy = r & 7, zz = r >> 3;
-        if (yy >= yn || zz >= zn) continue;
-        float F;
-        int Wt;
-        fast_load<FMT>(s, (size_t)x + (size_t)rx * (size_t)(y0 + yy) + slice * (size_t)(z0 + zz), F, Wt);
-        if (Wt > 0) {
-          weighted = true;
-          if (!(F > 0.f)) nonpos = true;
-        } else {
-          unweighted = true;
+#pragma unroll 1
+      for (int zz = 0; zz < zn; ++zz)
+#pragma unroll 4
+        for (int yy = 0; yy < yn; ++yy) {
+          float F;
+          int Wt;
+          sm.get((zz * 8 + yy) * 32 + lane, F, Wt);
+          if (Wt > 0) {
+            weighted = true;
+            if (!(F > 0.f)) nonpos = true;
+          } else {
+            unweighted = true;
+          }
         }
-      }
     }
     const unsigned bw = __ballot_sync(0xffffffffu, weighted), bu = __ballot_sync(0xffffffffu, unweighted),
                    bn = __ballot_sync(0xffffffffu, nonpos);

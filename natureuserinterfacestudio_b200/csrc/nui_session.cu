@@ -530,7 +530,10 @@ void launch_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st)
     const long tiles = p.maxBricks[F] / 4 + 1;  // >= the tiles of any session of the format
     k_integrate_cull<F><<<dim3(cdiv(tiles, 256), dense_n(p)), 256, 0, st>>>(d);
     const long blocks = std::min<long>(cdiv(tiles, 32 * kFastWarps), 1024);
-    k_integrate_fast<F><<<dim3((unsigned)std::max<long>(blocks, 1), dense_n(p)), 32 * kFastWarps, 0, st>>>(d);
+    const int smem = kFastWarps * kFastWarpSmem;
+    static std::once_flag opt_in;  // more than 48 KB of dynamic shared memory a block
+    std::call_once(opt_in, [&] { cudaFuncSetAttribute(k_integrate_fast<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); });
+    k_integrate_fast<F><<<dim3((unsigned)std::max<long>(blocks, 1), dense_n(p)), 32 * kFastWarps, smem, st>>>(d);
     return;
   }
   k_integrate<F><<<dim3(cdiv(p.maxIntegThreads[F], 256), dense_n(p)), 256, 0, st>>>(d);
