@@ -233,7 +233,7 @@ def run_ours(args, rank, world):
     ctx.enable_timing(True)
     stage = np.zeros(9)
     reps = 3
-    work = {"touched": 0, "bricks": 0, "ray_reads": 0, "ray_samples": 0, "ray_hits": 0, "icp_px": 0}
+    work = {"touched": 0, "bricks": 0, "ray_reads": 0, "ray_samples": 0, "ray_hits": 0, "icp_px": 0, "tiles": 0}
     for k in range(reps):
         ctx.batch_tick(sessions, dframes(args.warmup + args.steps + k), dcolors(args.warmup + args.steps + k),
                        device=True)
@@ -241,7 +241,7 @@ def run_ours(args, rank, world):
         for s, c in zip(sessions, cfgs):
             w = s.work_counters()
             if not is_hash(c):
-                for key in ("touched", "bricks", "ray_reads", "ray_samples", "ray_hits"):
+                for key in ("touched", "bricks", "ray_reads", "ray_samples", "ray_hits", "tiles"):
                     work[key] += w[key]
             work["icp_px"] += sum(it * (W_IMG >> l) * (H_IMG >> l) for l, it in enumerate(w["icp_iters"]))
     ctx.enable_timing(False)

@@ -418,7 +418,8 @@ NUI_API nui_status nui_session_touched_voxels(nui_session* s, uint64_t* n);
  * each launch follow (no counterpart in the reference): out[0] voxels updated by the
  * integration, out[1] 8^3 bricks the tolerance-mode integration re-classified, out[2] voxel
  * reads of the tolerance-mode dense raycast march, out[3] march samples it visited, out[4]
- * crossings it refined, out[5..8] ICP iterations run at levels 0..3.  9 values. */
+ * crossings it refined, out[5..8] ICP iterations run at levels 0..3, out[9] 32 x 8 x 8 voxel
+ * tiles the tolerance-mode integration ran (those its cull kept).  10 values. */
 NUI_API nui_status nui_session_work_counters(nui_session* s, uint64_t* out);
 
 /* ---------------------------------------------------------------- kernel-level calls

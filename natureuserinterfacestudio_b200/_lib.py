@@ -467,11 +467,12 @@ class Session:
 
     def work_counters(self):
         """Work of the last frame: updated voxels, re-classified bricks, raycast voxel reads,
-        samples visited, refined crossings, ICP iterations per level (4)."""
-        out = np.zeros(9, np.uint64)
+        samples visited, refined crossings, ICP iterations per level (4), integration tiles run."""
+        out = np.zeros(10, np.uint64)
         check(lib().nui_session_work_counters(self.h, ptr(out)))
         return {"touched": int(out[0]), "bricks": int(out[1]), "ray_reads": int(out[2]),
-                "ray_samples": int(out[3]), "ray_hits": int(out[4]), "icp_iters": [int(x) for x in out[5:9]]}
+                "ray_samples": int(out[3]), "ray_hits": int(out[4]), "icp_iters": [int(x) for x in out[5:9]],
+                "tiles": int(out[9])}
 
     def volume_ref_layout(self):
         """Volume as the reference stores it: short2 at ((x + y*rx)*rz + z)."""

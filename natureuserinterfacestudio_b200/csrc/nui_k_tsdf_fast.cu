@@ -339,6 +339,7 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) k_integrate_fast(const Ses
   // block has read the count by then)
   __syncthreads();
   if (threadIdx.x == 0 && atomicAdd(&s.ts->fast_done, 1u) == gridDim.x - 1) {
+    s.ts->tiles += count;
     s.ts->fast_count = 0u;
     s.ts->fast_done = 0u;
   }

@@ -29,7 +29,7 @@ __global__ void k_tick_begin(const SessionDesc* __restrict__ descs, int n) {
   if (s.kind < 0 || !s.ts) return;
   s.ts->dmax_bits = 0;
   s.ts->touched = 0ull;
-  s.ts->ray_reads = s.ts->ray_samples = s.ts->ray_hits = s.ts->bricks = 0ull;
+  s.ts->ray_reads = s.ts->ray_samples = s.ts->ray_hits = s.ts->bricks = s.ts->tiles = 0ull;
   for (int l = 0; l < kMaxLevels; ++l) s.ts->icp_iters[l] = 0u;
   if (s.hcount) {
     s.hcount[kHashFailedBefore] = s.hcount[kHashFailed];

@@ -663,21 +663,23 @@ void launch_shift(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
 }
 
 // The ICP kernel over n sessions, one cluster of cl blocks each (cl = 16 is beyond the
-// portable cluster size and needs the kernel's opt-in, given once per kernel).
+// portable cluster size and needs the kernel's opt-in, given once per kernel, as does its
+// 64 KB of dynamic shared memory).
 void launch_icp_cluster(void (*kern)(const SessionDesc*), const SessionDesc* d, int n, int cl, cudaStream_t st) {
-  if (cl == 16) {
+  {
     static std::mutex mu;
     static std::vector<const void*> opted;
     std::lock_guard<std::mutex> lock(mu);
     if (std::find(opted.begin(), opted.end(), (const void*)kern) == opted.end()) {
       cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kIcpStageBytes);
       opted.push_back((const void*)kern);
     }
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cl, n);
   cfg.blockDim = dim3(256);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = kIcpStageBytes;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -1702,6 +1704,7 @@ NUI_API nui_status nui_session_work_counters(nui_session* s, uint64_t* out) {
   out[3] = t.ray_samples;
   out[4] = t.ray_hits;
   for (int l = 0; l < kMaxLevels; ++l) out[5 + l] = t.icp_iters[l];
+  out[9] = t.tiles;
   return NUI_OK;
 }
 
