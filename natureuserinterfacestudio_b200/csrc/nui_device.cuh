@@ -14,7 +14,6 @@ constexpr int kMaxLevels = 4;
 constexpr int kMaxRadius = 7;
 constexpr int kIcpTerms = 29;  // 21 JtJ + 6 Jtr + r^2 + count  (icp.cl:122-160)
 constexpr int kTile = 16;      // pixel tile of the depth bound used by integration culling
-constexpr int kIcpStageBytes = 256 * 16 * 16;  // ICP: dynamic shared memory a block (texel staging)
 constexpr int kFastWarps = 4;  // warps per block of the tolerance-mode integration
 constexpr int kFastWarpSmem = 64 * 32 * 4 + 64 * 32 * 4;  // its shared memory per warp (bytes)
 

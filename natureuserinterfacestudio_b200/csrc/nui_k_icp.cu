@@ -369,35 +369,12 @@ __device__ __noinline__ void icp_host_step(IcpLm* ts, IcpStepScratch& w, const d
   }
 }
 
-// Asynchronous 16-byte copy global -> shared (cp.async, no registers held).
-__device__ __forceinline__ void icp_cp16(void* smem, const void* gmem) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
-               "l"(gmem));
-}
-
-// Bilinear sample with holes from four staged texels (a, b: row iy; c, d: row iy + 1),
-// bilinear_holes' arithmetic.
-__device__ __forceinline__ float3 bilinear_staged(const float4* t, float dx, float dy) {
-  const float3 a = xyz(t[0]), b = xyz(t[1]), c = xyz(t[2]), d = xyz(t[3]);
-  if (isnan3(a) || isnan3(b) || isnan3(c) || isnan3(d)) return f3(qnan(), qnan(), qnan());
-  const float ex = 1.0f - dx, ey = 1.0f - dy;
-  float3 r;
-  r.x = a.x * ex * ey + b.x * dx * ey + c.x * ex * dy + d.x * dx * dy;
-  r.y = a.y * ex * ey + b.y * dx * ey + c.y * ex * dy + d.y * dx * dy;
-  r.z = a.z * ex * ey + b.z * dx * ey + c.z * ex * dy + d.z * dx * dy;
-  return r;
-}
-
 // The 29 sums of the depth rows of one block of pixels (kIcpThreads x PPT consecutive
 // pixels of the level, index `vb`), added to this thread's FP64 accumulators.  sR / tc: the
-// running estimate; sp: the previous camera pose (the reference maps' frame).  The pixels
-// go two at a time: both are projected and their 2 x 8 reference-map texels copied into the
-// thread's own slots of shared memory (`stage`, 16 texels) by asynchronous copies, then both
-// rows are formed from there -- sixteen gathers in flight a thread without holding them in
-// registers.
+// running estimate; sp: the previous camera pose (the reference maps' frame).
 template <int PPT>
 __device__ __forceinline__ void icp_depth_rows(const SessionDesc& s, int level, int vb, const float* sR, float3 tc,
-                                               const DevXform& sp, float4* stage, double (&acc)[kIcpTerms]) {
+                                               const DevXform& sp, double (&acc)[kIcpTerms]) {
   const int w = s.W >> level, n = w * (s.H >> level);
   const float* __restrict__ Dl = s.dlev[level];
   const float fx = s.cam.fx, fy = s.cam.fy, cx = s.cam.cx, cy = s.cam.cy;
@@ -405,70 +382,46 @@ __device__ __forceinline__ void icp_depth_rows(const SessionDesc& s, int level, 
   const float fW = (float)s.W, fH = (float)s.H;
   const float3 tp = f3(sp.t[0], sp.t[1], sp.t[2]);
   const int base = vb * kIcpThreads * PPT;
-  // the depths of all the thread's pixels in flight at once
+  // the depths of all the thread's pixels in flight at once, consumed from the front
   float dq[PPT];
 #pragma unroll
   for (int k = 0; k < PPT; ++k) {
     const int i = base + k * kIcpThreads + threadIdx.x;
     dq[k] = i < n ? __ldg(Dl + i) : qnan();
   }
+#pragma unroll 1
+  for (int k = 0; k < PPT; ++k) {
+    const float dep = dq[0];
 #pragma unroll
-  for (int k0 = 0; k0 < PPT; k0 += 2) {
-    float3 pv[2];
-    float du[2], dv[2];
-    bool ok[2];
+    for (int j = 0; j + 1 < PPT; ++j) dq[j] = dq[j + 1];
+    if (isnan(dep)) continue;
+    const int i = base + k * kIcpThreads + threadIdx.x;
+    const int py = i / w;
+    const float3 v = level_vertex(s.cam, level, i - py * w, py, dep);
+    const float3 pv = add3(rot_rows(sR, v), tc);
+    const float3 pp = rot_rows(sp.R_inv, sub3(pv, tp));
+    const float u = pp.x * fx / pp.z + cx;
+    const float vv = pp.y * fy / pp.z + cy;
+    if (!(u >= 0.0f && u < fW && vv >= 0.0f && vv < fH)) continue;
+    // both maps sampled at once (their eight loads in flight together), then tested
+    const float3 rn = bilinear_holes(s.nref, u, vv, RW, RN);
+    const float3 rv = bilinear_holes(s.vref, u, vv, RW, RN);
+    if (isnan3(rn) || isnan3(rv)) continue;
+    const float3 diff = sub3(rv, pv);
+    const float dist = sqrtf(dot3(diff, diff));
+    if (!(dist < s.dist_thr)) continue;
+    const float3 r0 = cross3(rn, pv);
+    // the row's seven FP32 values widened once; each product is exact in FP64 and enters
+    // its sum with one rounding (fused multiply-add)
+    const double c7[7] = {(double)r0.x, (double)r0.y, (double)r0.z, (double)rn.x, (double)rn.y, (double)rn.z,
+                          (double)dot3(rn, diff)};
+    int sh = 0;
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      ok[j] = false;
-      const int k = k0 + j;
-      if (k >= PPT || isnan(dq[k])) continue;
-      const int i = base + k * kIcpThreads + threadIdx.x;
-      const int py = i / w;
-      const float3 v = level_vertex(s.cam, level, i - py * w, py, dq[k]);
-      pv[j] = add3(rot_rows(sR, v), tc);
-      const float3 pp = rot_rows(sp.R_inv, sub3(pv[j], tp));
-      const float u = pp.x * fx / pp.z + cx;
-      const float vv = pp.y * fy / pp.z + cy;
-      if (!(u >= 0.0f && u < fW && vv >= 0.0f && vv < fH)) continue;
-      const int ix = (int)floorf(u), iy = (int)floorf(vv);
-      du[j] = u - (float)ix;
-      dv[j] = vv - (float)iy;
-      const int ia = ix + iy * RW;
-      if (ia + RW + 1 >= RN) continue;  // a tap past the map: a hole (bilinear_holes)
-      ok[j] = true;
-      float4* t = stage + 8 * j;
-      icp_cp16(t + 0, s.nref + ia);
-      icp_cp16(t + 1, s.nref + ia + 1);
-      icp_cp16(t + 2, s.nref + ia + RW);
-      icp_cp16(t + 3, s.nref + ia + RW + 1);
-      icp_cp16(t + 4, s.vref + ia);
-      icp_cp16(t + 5, s.vref + ia + 1);
-      icp_cp16(t + 6, s.vref + ia + RW);
-      icp_cp16(t + 7, s.vref + ia + RW + 1);
-    }
-    asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's own copies
+    for (int a = 0; a < 6; ++a)
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      if (!ok[j]) continue;
-      const float3 rn = bilinear_staged(stage + 8 * j, du[j], dv[j]);
-      const float3 rv = bilinear_staged(stage + 8 * j + 4, du[j], dv[j]);
-      if (isnan3(rn) || isnan3(rv)) continue;
-      const float3 diff = sub3(rv, pv[j]);
-      const float dist = sqrtf(dot3(diff, diff));
-      if (!(dist < s.dist_thr)) continue;
-      const float3 r0 = cross3(rn, pv[j]);
-      // the row's seven FP32 values widened once; each product is exact in FP64 and enters
-      // its sum with one rounding (fused multiply-add)
-      const double c7[7] = {(double)r0.x, (double)r0.y, (double)r0.z, (double)rn.x, (double)rn.y, (double)rn.z,
-                            (double)dot3(rn, diff)};
-      int sh = 0;
-#pragma unroll
-      for (int a = 0; a < 6; ++a)
-#pragma unroll
-        for (int b = a; b < 7; ++b, ++sh) acc[sh] = fma(c7[a], c7[b], acc[sh]);
-      acc[27] = fma(c7[6], c7[6], acc[27]);
-      acc[28] += 1.0;
-    }
+      for (int b = a; b < 7; ++b, ++sh) acc[sh] = fma(c7[a], c7[b], acc[sh]);
+    acc[27] = fma(c7[6], c7[6], acc[27]);
+    acc[28] += 1.0;
   }
 }
 
@@ -550,8 +503,6 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
   __shared__ double sums[kIcpTerms];
   __shared__ IcpLm lm;  // block 0: the tracker state during the kernel
   __shared__ IcpStepScratch hw;  // block 0: the LM step's intermediate values
-  extern __shared__ float4 icp_stage[];  // kIcpStageBytes: 16 texels a thread
-  float4* stage = icp_stage + threadIdx.x * 16;
   if (threadIdx.x < 9) sR[threadIdx.x] = ts->R[threadIdx.x];
   if (threadIdx.x < 3) st[threadIdx.x] = ts->t[threadIdx.x];
   if (threadIdx.x < 21) reinterpret_cast<float*>(&sp)[threadIdx.x] = reinterpret_cast<const float*>(&ts->xf)[threadIdx.x];
@@ -571,7 +522,7 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
       double acc[kIcpTerms];
 #pragma unroll
       for (int k = 0; k < kIcpTerms; ++k) acc[k] = 0.0;
-      for (int vb = rank; vb < nblocks; vb += C) icp_depth_rows<PPT>(s, level, vb, sR, tc, sp, stage, acc);
+      for (int vb = rank; vb < nblocks; vb += C) icp_depth_rows<PPT>(s, level, vb, sR, tc, sp, acc);
       double D = icp_block_sum(acc);
       if (threadIdx.x < kIcpTerms) part[0][threadIdx.x] = D;
       if (photo) {

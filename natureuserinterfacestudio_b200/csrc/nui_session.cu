@@ -663,8 +663,7 @@ void launch_shift(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
 }
 
 // The ICP kernel over n sessions, one cluster of cl blocks each (cl = 16 is beyond the
-// portable cluster size and needs the kernel's opt-in, given once per kernel, as does its
-// 64 KB of dynamic shared memory).
+// portable cluster size and needs the kernel's opt-in, given once per kernel).
 void launch_icp_cluster(void (*kern)(const SessionDesc*), const SessionDesc* d, int n, int cl, cudaStream_t st) {
   {
     static std::mutex mu;
@@ -672,14 +671,13 @@ void launch_icp_cluster(void (*kern)(const SessionDesc*), const SessionDesc* d, 
     std::lock_guard<std::mutex> lock(mu);
     if (std::find(opted.begin(), opted.end(), (const void*)kern) == opted.end()) {
       cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kIcpStageBytes);
       opted.push_back((const void*)kern);
     }
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cl, n);
   cfg.blockDim = dim3(256);
-  cfg.dynamicSmemBytes = kIcpStageBytes;
+  cfg.dynamicSmemBytes = 0;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
