@@ -192,8 +192,26 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) k_integrate_fast(const Ses
     const float gy0 = ((float)(y0 - hy) + 0.5f) * c1 - t1;
     const float3 ey = f3(Ri[1] * c1, Ri[4] * c1, Ri[7] * c1);  // camera step of one y row
 
-    // ---- 1. requests: depth pixels and voxel rows of the whole tile
+    // ---- 1. requests: voxel rows and depth pixels of the whole tile
     __syncwarp();  // the previous tile's shared copy is no longer read
+    if (whole) {
+      // the rows' 16-byte pieces dealt over the lanes (FP16 + u8: 4 tsdf + 2 weight pieces
+      // a row; FP16 + FP16: 8 pieces), no lane idle and no branch per row
+      constexpr int kPieces = FMT == 2 ? 6 : 8;
+      const int nrow = zn * 8;  // rows of slices past the volume's y end are skipped below
+      for (int j = lane; j < nrow * kPieces; j += 32) {
+        const int r = j / kPieces, piece = j - r * kPieces, yy = r & 7, zz = r >> 3;
+        if (yy >= yn) continue;
+        const size_t rb = (size_t)x0 + (size_t)rx * (size_t)(y0 + yy) + slice * (size_t)(z0 + zz);
+        if (FMT == 2) {
+          if (piece < 4) cp_async16(sm.fh + r * 32 + piece * 8, reinterpret_cast<const __half*>(s.vol) + rb + piece * 8);
+          else cp_async16(sm.wb + r * 32 + (piece - 4) * 16, s.wvol + rb + (piece - 4) * 16);
+        } else {
+          cp_async16(sm.f2 + r * 32 + piece * 4, reinterpret_cast<const __half2*>(s.vol) + rb + piece * 4);
+        }
+      }
+    }
+    const unsigned dep_s = (unsigned)__cvta_generic_to_shared(sm.dep + lane);  // this lane's column
 #pragma unroll 1
     for (int zz = 0; zz < zn; ++zz) {
       const float gz = ((float)(z0 + zz) + 0.5f) * c2 - t2;
@@ -203,7 +221,6 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) k_integrate_fast(const Ses
 #pragma unroll 2
       for (int yy = 0; yy < yn; ++yy) {
         const int r = zz * 8 + yy;
-        float* dslot = sm.dep + r * 32 + lane;
         bool got = false;
         if (xin && v.z > 0.f) {
           const float iz = __fdividef(1.f, v.z);
@@ -211,20 +228,14 @@ __global__ void __launch_bounds__(32 * kFastWarps, 3) k_integrate_fast(const Ses
           // voxel centres sit on rational grids), and half-to-even would split them
           const int px = round_half_up(fx * v.x * iz + ccx), py = round_half_up(fy * v.y * iz + ccy);
           if (px >= 0 && py >= 0 && px < W && py < H) {
-            cp_async4(dslot, depth + py * W + px);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dep_s + (unsigned)r * 128u),
+                         "l"(depth + py * W + px));
             got = true;
           }
         }
-        if (!got) *dslot = __int_as_float(0x7fffffff);
-        const size_t rb = zbase + (size_t)rx * yy;  // the row's first voxel
-        if (whole) {
-          if (FMT == 2) {
-            if (lane < 4) cp_async16(sm.fh + r * 32 + lane * 8, reinterpret_cast<const __half*>(s.vol) + rb + lane * 8);
-            else if (lane < 6) cp_async16(sm.wb + r * 32 + (lane - 4) * 16, s.wvol + rb + (lane - 4) * 16);
-          } else {
-            if (lane < 8) cp_async16(sm.f2 + r * 32 + lane * 4, reinterpret_cast<const __half2*>(s.vol) + rb + lane * 4);
-          }
-        } else if (xin) {
+        if (!got) sm.dep[r * 32 + lane] = __int_as_float(0x7fffffff);
+        if (!whole && xin) {
+          const size_t rb = zbase + (size_t)rx * yy;  // the row's first voxel
           if (FMT == 2) {
             sm.fh[r * 32 + lane] = reinterpret_cast<const __half*>(s.vol)[rb + lane];
             sm.wb[r * 32 + lane] = s.wvol[rb + lane];
