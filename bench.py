@@ -233,7 +233,8 @@ def run_ours(args, rank, world):
     ctx.enable_timing(True)
     stage = np.zeros(9)
     reps = 3
-    work = {"touched": 0, "bricks": 0, "ray_reads": 0, "ray_samples": 0, "ray_hits": 0, "icp_px": 0, "tiles": 0}
+    work = {"touched": 0, "bricks": 0, "ray_reads": 0, "ray_samples": 0, "ray_hits": 0, "icp_px": 0, "icp_px_dense": 0,
+            "tiles": 0}
     for k in range(reps):
         ctx.batch_tick(sessions, dframes(args.warmup + args.steps + k), dcolors(args.warmup + args.steps + k),
                        device=True)
@@ -243,7 +244,10 @@ def run_ours(args, rank, world):
             if not is_hash(c):
                 for key in ("touched", "bricks", "ray_reads", "ray_samples", "ray_hits", "tiles"):
                     work[key] += w[key]
-            work["icp_px"] += sum(it * (W_IMG >> l) * (H_IMG >> l) for l, it in enumerate(w["icp_iters"]))
+            px = sum(it * (W_IMG >> l) * (H_IMG >> l) for l, it in enumerate(w["icp_iters"]))
+            work["icp_px"] += px
+            if not is_hash(c):
+                work["icp_px_dense"] += px
     ctx.enable_timing(False)
     stage /= reps
     work = {k: v / reps for k, v in work.items()}
@@ -260,8 +264,9 @@ def run_ours(args, rank, world):
     #   dense raycast (k_raycast_fast + k_raycast_finish_fast, stage 7): the voxels the march
     #     read, one brick-state byte per visited sample, 64 voxels per refined crossing, and
     #     the vertex / normal / colour maps written (12 + 12 + 4 B a pixel);
-    #   ICP (k_icp_cluster, stage 2): per pixel-iteration the depth (4 B) and one reference
-    #     vertex and normal (16 + 16 B).
+    #   ICP (k_icp_cluster over the dense sessions, stage 2 -- the hash sessions' tracking runs
+    #     on the second stream): per pixel-iteration the depth (4 B) and one reference vertex
+    #     and normal (16 + 16 B).
     dense = [c for c in cfgs if not is_hash(c)]
     npx = W_IMG * H_IMG
     peak, peak_kind = peaks()
@@ -270,7 +275,7 @@ def run_ours(args, rank, world):
          work["touched"] * 6 + work["bricks"] * 512 * 3 + len(dense) * npx * 4),
         ("k_raycast_fast<F16_U8>+k_raycast_finish_fast<F16_U8>", stage[7],
          work["ray_reads"] * 3 + work["ray_samples"] + work["ray_hits"] * 64 * 3 + len(dense) * npx * 28),
-        ("k_icp_cluster", stage[2], work["icp_px"] * 36),
+        ("k_icp_cluster", stage[2], work["icp_px_dense"] * 36),
     ]
     roof = []
     for name, ms, nbytes in kernels:
@@ -582,35 +587,62 @@ def ate_vs_plain(L, ctx, seqs, gts, nframes, nstreams):
     weight, half-precision hash, one batched tick per frame) and in the plain path (FP32
     dense TSDF / int16 hash, one stream at a time).  Reported per stream: the RMS distance
     between the two trajectories' camera positions, and each one's ATE against the true
-    trajectory (RMS position error after both start at the first frame's pose)."""
+    trajectory (RMS position error after both start at the first frame's pose).  The plain
+    path also runs a second time with other ICP launch shapes (8-block clusters, 8 pixels a
+    thread), which change nothing but the FP64 rounding of the ICP sums: the spread between
+    the two plain runs is how far rounding alone moves a trajectory of that stream."""
     nseq = len(seqs)
     cfg16 = stream_cfgs(L, nstreams, L.TSDF_F16_U8, L.TSDF_F16_U8)
     cfg32 = stream_cfgs(L, nstreams, L.TSDF_F32, L.TSDF_I16)
     offs = [(i * 7) % 11 for i in range(nstreams)]
     idx = [[pingpong(offs[i] + k) for k in range(nframes)] for i in range(nstreams)]
+    tune0 = ctx.tuning().as_dict()
+
+    def frames(k):
+        fr = [seqs[i % nseq][idx[i][k]][0] for i in range(nstreams)]
+        co = [seqs[i % nseq][idx[i][k]][1] if is_hash(cfg16[i]) else None for i in range(nstreams)]
+        return fr, co
+
     a = [L.Session(ctx, c) for c in cfg16]
     b = [L.Session(ctx, c) for c in cfg32]
     p16 = np.zeros((nstreams, nframes, 3))
     p32 = np.zeros((nstreams, nframes, 3))
     for k in range(nframes):
-        fr = [seqs[i % nseq][idx[i][k]][0] for i in range(nstreams)]
-        co = [seqs[i % nseq][idx[i][k]][1] if is_hash(cfg16[i]) else None for i in range(nstreams)]
+        fr, co = frames(k)
         _, poses = ctx.batch_tick(a, fr, co)
         p16[:, k] = poses[:, 9:]
         for i in range(nstreams):
             p32[i, k] = b[i].process(fr[i], co[i])[1][9:]
     for s in a + b:
         s.close()
+    # the plain path again with other ICP launch shapes
+    ctx.set_tuning(L.Tuning(**dict(tune0, icp_cluster_blocks=8, icp_pixels_per_thread=8)))
+    b = [L.Session(ctx, c) for c in cfg32]
+    p32b = np.zeros((nstreams, nframes, 3))
+    for k in range(nframes):
+        fr, co = frames(k)
+        for i in range(nstreams):
+            p32b[i, k] = b[i].process(fr[i], co[i])[1][9:]
+    for s in b:
+        s.close()
+    ctx.set_tuning(L.Tuning(**tune0))
+
+    def rms(x):
+        return round(float(np.sqrt(np.mean(np.sum(x ** 2, 1)))) * 1e3, 3)
+
     out = []
     for i in range(nstreams):
         gt = np.array([_rel(gts[i % nseq], idx[i][0], idx[i][k])[1] for k in range(nframes)])
         out.append({"stream": i, "kind": "hash" if is_hash(cfg16[i]) else "dense %d^3" % cfg16[i].res[0],
-                    "traj_rms_diff_mm": round(float(np.sqrt(np.mean(np.sum((p16[i] - p32[i]) ** 2, 1)))) * 1e3, 3),
-                    "ate_fp16_mm": round(float(np.sqrt(np.mean(np.sum((p16[i] - gt) ** 2, 1)))) * 1e3, 3),
-                    "ate_plain_fp32_mm": round(float(np.sqrt(np.mean(np.sum((p32[i] - gt) ** 2, 1)))) * 1e3, 3)})
+                    "traj_rms_diff_mm": rms(p16[i] - p32[i]), "ate_fp16_mm": rms(p16[i] - gt),
+                    "ate_plain_fp32_mm": rms(p32[i] - gt), "ate_plain_reshaped_mm": rms(p32b[i] - gt),
+                    "plain_vs_reshaped_traj_rms_diff_mm": rms(p32[i] - p32b[i])})
     worst = max(abs(o["ate_fp16_mm"] - o["ate_plain_fp32_mm"]) for o in out)
+    floor = max(abs(o["ate_plain_reshaped_mm"] - o["ate_plain_fp32_mm"]) for o in out)
     return {"frames": nframes, "streams": out, "max_abs_ate_diff_mm": round(worst, 3),
             "max_traj_rms_diff_mm": round(max(o["traj_rms_diff_mm"] for o in out), 3),
+            "max_abs_ate_diff_plain_vs_reshaped_mm": round(floor, 3),
+            "streams_within_1mm": int(sum(abs(o["ate_fp16_mm"] - o["ate_plain_fp32_mm"]) <= 1.0 for o in out)),
             "within_1mm": bool(worst <= 1.0)}
 
 

@@ -327,9 +327,11 @@ NUI_API nui_session* nui_server_session(nui_server* srv, int slot);
  * 3 shifting-volume shifts + dense integration kernel, 4 brick summaries (+ voxel-hash
  * allocation / integration), 5 raycast, 6 whole tick, 7 the dense raycast kernels alone,
  * 8 the voxel-hash sessions' work on the second stream (0 when it did not run there).
- * When the batch holds dense and voxel-hash sessions, the hash sessions' allocation,
- * integration and raycast run on a second stream beside stages 3-5 instead; stage 5 then
- * ends when both are done. */
+ * When the batch holds dense and voxel-hash sessions, the hash sessions' tracking,
+ * allocation, integration and raycast run on a second stream beside stages 2-5 instead
+ * (stage 2 then times the dense sessions' tracking, stage 8 all of the hash sessions'
+ * work, tracking included; in a served batch, whose table mixes the two families, the
+ * tracking of both stays in stage 2); stage 5 ends when both streams are done. */
 NUI_API nui_status nui_ctx_enable_timing(nui_ctx* ctx, int enable);
 NUI_API nui_status nui_ctx_stage_ms(nui_ctx* ctx, int stage, float* ms);
 /* Kernel launches in the captured graph of the context's last graphed batch tick. */

@@ -690,21 +690,22 @@ void launch_icp_cluster(void (*kern)(const SessionDesc*), const SessionDesc* d, 
 }
 
 // Colour pyramid (if any session tracks with colour), the ICP iterations of every level,
-// the integration gate and the published pose.
-void launch_track(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, float* d_pose, int* d_status,
+// the integration gate and the published pose, for the n descriptors at d.
+void launch_track(const BatchPlan& p, const SessionDesc* d, int n, cudaStream_t st, float* d_pose, int* d_status,
                   bool tick = true) {
+  if (n <= 0) return;
   const unsigned npix = cdiv((long)p.maxW * p.maxH, 256);
-  if (p.colorIcp) k_color_grad<<<dim3(npix, p.n, 1), 256, 0, st>>>(d);  // finest level
+  if (p.colorIcp) k_color_grad<<<dim3(npix, n, 1), 256, 0, st>>>(d);  // finest level
   // every level and iteration of every session in one launch: a cluster of
   // icp_cluster_blocks blocks per session
   const int ppt = p.tune.icp_pixels_per_thread;
-  if (ppt == 2) launch_icp_cluster(k_icp_cluster<2>, d, p.n, p.tune.icp_cluster_blocks, st);
-  else if (ppt == 8) launch_icp_cluster(k_icp_cluster<8>, d, p.n, p.tune.icp_cluster_blocks, st);
-  else if (ppt == 16) launch_icp_cluster(k_icp_cluster<16>, d, p.n, p.tune.icp_cluster_blocks, st);
-  else launch_icp_cluster(k_icp_cluster<4>, d, p.n, p.tune.icp_cluster_blocks, st);
-  k_track_finalize<<<p.n, 32, 0, st>>>(d, tick ? 1 : 0);
-  k_publish<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n, d_pose, d_status);
-  if (p.colorIcp) k_color_keep<<<dim3(npix, p.n), 256, 0, st>>>(d);
+  if (ppt == 2) launch_icp_cluster(k_icp_cluster<2>, d, n, p.tune.icp_cluster_blocks, st);
+  else if (ppt == 8) launch_icp_cluster(k_icp_cluster<8>, d, n, p.tune.icp_cluster_blocks, st);
+  else if (ppt == 16) launch_icp_cluster(k_icp_cluster<16>, d, n, p.tune.icp_cluster_blocks, st);
+  else launch_icp_cluster(k_icp_cluster<4>, d, n, p.tune.icp_cluster_blocks, st);
+  k_track_finalize<<<n, 32, 0, st>>>(d, tick ? 1 : 0);
+  k_publish<<<cdiv(n, 64), 64, 0, st>>>(d, n, d_pose, d_status);
+  if (p.colorIcp) k_color_keep<<<dim3(npix, n), 256, 0, st>>>(d);
 }
 
 // The launch schedule of one tick.  ev: optional stage events (timing only).
@@ -722,21 +723,32 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
     k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), p.n), 256, 0, st>>>(d, l);
   k_feedback<<<dim3(cdiv((long)p.maxW * p.maxH, 256), p.n), 256, 0, st>>>(d);
   mark(2);
-  launch_track(p, d, st, d_pose, d_status);
-  mark(3);
-  // With dense and hash sessions in the batch, the hash sessions' allocation, integration
-  // and raycast run on the side stream, beside the dense ones: the two sets of kernels
-  // touch disjoint sessions, and the many short kernels of the hash allocation fill the
-  // gaps of the dense integration.
+  // With dense and hash sessions in the batch, the hash sessions' tracking, allocation,
+  // integration and raycast run on the side stream, beside the dense ones: the two sets of
+  // kernels touch disjoint sessions, the dense integration starts as soon as the dense
+  // sessions are tracked (instead of after the longer colour-tracked hash sessions), and
+  // the many short kernels of the hash allocation fill the gaps of the dense integration.
+  // A served batch, whose descriptor table mixes the two families, tracks them together.
   const bool fork = p.hashMask && p.fmtMask;
+  const bool split = fork && p.hashTail > 0 && p.denseHead > 0;
   cudaStream_t hs = fork ? ctx->side : st;
-  if (fork) {
+  if (split) {
+    cudaEventRecord(ctx->fork_ev, st);
+    cudaStreamWaitEvent(hs, ctx->fork_ev, 0);
+    if (ev) cudaEventRecord(ctx->ev[9], hs);
+    launch_track(p, d + p.denseHead, p.n - p.denseHead, hs, d_pose, d_status);
+    launch_track(p, d, p.denseHead, st, d_pose, d_status);
+  } else {
+    launch_track(p, d, p.n, st, d_pose, d_status);
+  }
+  mark(3);
+  if (fork && !split) {
     cudaEventRecord(ctx->fork_ev, st);
     cudaStreamWaitEvent(hs, ctx->fork_ev, 0);
   }
   if (ev) ctx->side_timed = fork;
   if (fork) {
-    if (ev) cudaEventRecord(ctx->ev[9], hs);
+    if (ev && !split) cudaEventRecord(ctx->ev[9], hs);
     launch_hash_integrate(p, d, hs);
     launch_hash_raycast(p, d, hs);
     if (ev) cudaEventRecord(ctx->ev[10], hs);
@@ -1738,7 +1750,7 @@ nui_status run_stage(nui_session* s, int what) {
     for (int l = 1; l < p.maxLevels; ++l)
       k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), 1), 256, 0, st>>>(dd, l);
   } else if (what == 1) {
-    launch_track(p, dd, st, ctx->d_pose, ctx->d_status, false);
+    launch_track(p, dd, p.n, st, ctx->d_pose, ctx->d_status, false);
   } else if (what == 2) {
     k_ztab<<<1, 32, 0, st>>>(dd);
     launch_shift(p, dd, st);
