@@ -1230,10 +1230,12 @@ NUI_API nui_status nui_ctx_autotune(nui_ctx* c, const nui_session_cfg* cfgs, int
     best.*field = pick;
   };
   if (dense) tune_one(&nui_tuning::integrate_threads_log2, {16, 17, 18, 19, 20}, 3);
-  tune_one(&nui_tuning::icp_cluster_blocks, {4, 8, 16}, 2);
-  tune_one(&nui_tuning::icp_pixels_per_thread, {2, 4, 8, 16}, 2);
-  if (dense) tune_one(&nui_tuning::raycast_tile_width, {4, 8, 16, 32}, 5);
-  if (hash) tune_one(&nui_tuning::hash_raycast_tile_width, {4, 8, 16, 32}, 5);
+  // the ICP shapes and ray tiles by the whole tick: with dense and hash sessions the hash
+  // sessions' tracking and raycast run on the second stream, beside stages 2-5
+  tune_one(&nui_tuning::icp_cluster_blocks, {4, 8, 16}, 6);
+  tune_one(&nui_tuning::icp_pixels_per_thread, {2, 4, 8, 16}, 6);
+  if (dense) tune_one(&nui_tuning::raycast_tile_width, {4, 8, 16, 32}, 6);
+  if (hash) tune_one(&nui_tuning::hash_raycast_tile_width, {4, 8, 16, 32}, 6);
   float tick_ms = 0.f;
   if (st == NUI_OK) {
     c->tune = best;
