@@ -1047,11 +1047,7 @@ NUI_API nui_status nui_ctx_create(int device, nui_ctx** out) {
   }
   c->stream = c->own;
   for (int i = 0; i < kEvents; ++i) cudaEventCreate(&c->ev[i]);
-  // the second stream carries the voxel-hash sessions' chain of short dependent kernels,
-  // the tick's longest path: its kernels get the SMs first, the dense ones fill the rest
-  int prio_lo = 0, prio_hi = 0;
-  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
-  if (cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+  if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
