@@ -699,18 +699,50 @@ __device__ __noinline__ int hash_block_lookup(const SessionDesc& s, short sx, sh
   return -1;
 }
 
+// A warp's shared cache of block lookups: 64 direct-mapped 64-bit entries in shared memory,
+// each the block's coordinates (14 bits an axis, offset by 8192; 16383 marks an empty
+// entry) above its pool block index + 1 (22 bits; 0: not allocated).  The rays of a warp
+// shade neighbouring pixels and walk largely the same blocks, so a lane finds most lookups
+// another lane made.  An entry is written and read whole, so any lane sees a consistent
+// (key, value) pair; the table does not change during the raycast.
+constexpr int kWarpCache = 64;
+__device__ __forceinline__ void warp_cache_clear(unsigned long long* wc) {
+  const int lane = threadIdx.x & 31;
+  wc[lane] = ~0ull;
+  wc[lane + 32] = ~0ull;
+  __syncwarp();
+}
+
 template <int HF>
 struct HashRead {
   const SessionDesc& s;
   short cbx, cby, cbz;
   int cptr;  // cached block (findVoxelBlockIndex's cache; transparent to results)
+  volatile unsigned long long* wc;  // the warp's shared lookup cache, or nullptr
   // Pool offset (block index * 512) of block (bx, by, bz), or -1 if it is not allocated.
   // The lookup itself is out of line: it is called from many places of the raycast, and
   // inlined copies of its chain walk overflow the instruction cache.
   __device__ __forceinline__ int block(int bx, int by, int bz) {
     const short sx = (short)bx, sy = (short)by, sz = (short)bz;
     if (cptr >= 0 && sx == cbx && sy == cby && sz == cbz) return cptr;
-    const int p = hash_block_lookup(s, sx, sy, sz);
+    const bool cacheable = wc && sx > -8192 && sx < 8191 && sy > -8192 && sy < 8191 && sz > -8192 && sz < 8191;
+    unsigned long long key = 0;
+    int slot = 0;
+    int p;
+    if (cacheable) {
+      key = ((unsigned long long)(sx + 8192) << 28) | ((unsigned long long)(sy + 8192) << 14) |
+            (unsigned long long)(sz + 8192);
+      slot = (int)(hash_index(kWarpCache - 1, sx, sy, sz));
+      const unsigned long long e = wc[slot];
+      if ((e >> 22) == key) {
+        p = (int)(e & 0x3fffffull) - 1;
+        p = p < 0 ? -1 : p * 512;
+        if (p >= 0) cbx = sx, cby = sy, cbz = sz, cptr = p;
+        return p;
+      }
+    }
+    p = hash_block_lookup(s, sx, sy, sz);
+    if (cacheable) wc[slot] = (key << 22) | (unsigned long long)(p < 0 ? 0 : p / 512 + 1);
     if (p >= 0) {
       cbx = sx;
       cby = sy;
@@ -909,11 +941,13 @@ __global__ void __launch_bounds__(128, 8) k_hash_raycast(const SessionDesc* __re
   const int tiles_x = (s.W + bw - 1) / bw;
   if ((int)blockIdx.x >= tiles_x * ((s.H + bh - 1) / bh)) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ unsigned long long wcache[4][kWarpCache];
+  warp_cache_clear(wcache[warp]);
   const int px = ((int)blockIdx.x % tiles_x) * bw + (warp & 1) * tw + lane % tw;
   const int py = ((int)blockIdx.x / tiles_x) * bh + (warp >> 1) * th + lane / tw;
   if (px >= s.W || py >= s.H) return;
   const int pid = py * s.W + px;
-  HashRead<HF> R{s, 0, 0, 0, -1};
+  HashRead<HF> R{s, 0, 0, 0, -1, wcache[warp]};
   const float stepScale = s.mu * (1.0f / s.voxel) * 0.6f;
   float3 pr, dir;
   float total, totalMax, sdfv = 1.0f;
@@ -931,10 +965,12 @@ template <int HF>
 __global__ void __launch_bounds__(256, 4) k_hash_finish(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (!s.hash || s.fwd || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
+  __shared__ unsigned long long wcache[8][kWarpCache];
+  warp_cache_clear(wcache[threadIdx.x >> 5]);
   const int pid = blockIdx.x * blockDim.x + threadIdx.x;
   if (pid >= s.W * s.H) return;
   const float4 e = s.vref[pid];
-  HashRead<HF> R{s, 0, 0, 0, -1};
+  HashRead<HF> R{s, 0, 0, 0, -1, wcache[threadIdx.x >> 5]};
   const float stepScale = s.mu * (1.0f / s.voxel) * 0.6f;
   float3 ps, dir;
   float total, totalMax;
