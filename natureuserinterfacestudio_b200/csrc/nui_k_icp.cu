@@ -49,10 +49,10 @@ __device__ __forceinline__ float3 bilinear_holes(const float4* __restrict__ src,
 // for the rotations and -R^T e_k for the translations (the depth ICP's update
 // R <- Rinc^-1 R, t <- Rinc^-1 t + tinc).  Colours count with alpha 255.  c receives the
 // upper triangle of [D | -diff]^T [D | -diff] by rows (21 + 6), |diff|^2 and 1.
-__device__ __forceinline__ bool color_row(const SessionDesc& s, const float4 mv, const uchar4 mc, const float* R,
-                                          const float3 t, float* c) {
-  const float3 m = xyz(mv);
+__device__ __forceinline__ bool color_row(const SessionDesc& s, int i, const float* R, const float3 t, float* c) {
+  const float3 m = xyz(__ldg(s.vref + i));
   if (isnan3(m)) return false;
+  const uchar4 mc = __ldg(s.cprev + i);
   if (mc.w != 255) return false;
   const float3 d = sub3(m, t);
   const float3 c0 = f3(R[0], R[3], R[6]), c1 = f3(R[1], R[4], R[7]), c2 = f3(R[2], R[5], R[8]);
@@ -425,36 +425,20 @@ __device__ __forceinline__ void icp_depth_rows(const SessionDesc& s, int level, 
   }
 }
 
-// The photometric rows of one block of full-resolution model points (colour tracking): the
-// model points and their colours of four of the thread's pixels are loaded first, in flight
-// together, then each point's gathers follow.
+// The photometric rows of one block of full-resolution model points (colour tracking).
 template <int PPT>
 __device__ __forceinline__ void icp_color_rows(const SessionDesc& s, int vb, const float* sR, float3 tc,
                                                double (&acc)[kIcpTerms]) {
-  constexpr int G = PPT < 4 ? PPT : 4;
   const int cbase = vb * kIcpThreads * PPT, NM = s.W * s.H;
 #pragma unroll 1
-  for (int k0 = 0; k0 < PPT; k0 += G) {
-    float4 mq[G];
-    uchar4 cq[G];
+  for (int k = 0; k < PPT; ++k) {
+    const int i = cbase + k * kIcpThreads + threadIdx.x;
+    if (i >= NM) break;
+    float c[kIcpTerms];
+    if (!color_row(s, i, sR, tc, c)) continue;
 #pragma unroll
-    for (int k = 0; k < G; ++k) {
-      const int i = cbase + (k0 + k) * kIcpThreads + threadIdx.x;
-      mq[k] = make_float4(qnan(), qnan(), qnan(), 0.f);
-      cq[k] = make_uchar4(0, 0, 0, 0);
-      if (i < NM) {
-        mq[k] = __ldg(s.vref + i);
-        cq[k] = __ldg(s.cprev + i);
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < G; ++k) {
-      float c[kIcpTerms];
-      if (!color_row(s, mq[k], cq[k], sR, tc, c)) continue;
-#pragma unroll
-      for (int q = 0; q < kIcpTerms - 1; ++q) acc[q] += (double)c[q];
-      acc[28] += 1.0;
-    }
+    for (int q = 0; q < kIcpTerms - 1; ++q) acc[q] += (double)c[q];
+    acc[28] += 1.0;
   }
 }
 
