@@ -965,12 +965,10 @@ template <int HF>
 __global__ void __launch_bounds__(256, 4) k_hash_finish(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (!s.hash || s.fwd || s.hfmt != HF || s.kind != kTrackFrame || s.ts->status != 0) return;
-  __shared__ unsigned long long wcache[8][kWarpCache];
-  warp_cache_clear(wcache[threadIdx.x >> 5]);
   const int pid = blockIdx.x * blockDim.x + threadIdx.x;
   if (pid >= s.W * s.H) return;
   const float4 e = s.vref[pid];
-  HashRead<HF> R{s, 0, 0, 0, -1, wcache[threadIdx.x >> 5]};
+  HashRead<HF> R{s, 0, 0, 0, -1};  // (a warp-shared lookup cache made this kernel slower)
   const float stepScale = s.mu * (1.0f / s.voxel) * 0.6f;
   float3 ps, dir;
   float total, totalMax;
