@@ -71,7 +71,8 @@ __global__ void __launch_bounds__(128) k_raycast_fast(const SessionDesc* __restr
         const int kn = kc + 1;
         const float tn = fmaf((float)kn, step, t0);
         V.voxel_of(add3(start, mul3(dir, tn)), gx, gy, gz);
-        if (!(gx >= 0 && gy >= 0 && gz >= 0 && gx < V.rx && gy < V.ry && gz < V.rz)) break;
+        // inside the volume on all three axes (one unsigned compare an axis)
+        if (!((unsigned)gx < (unsigned)V.rx && (unsigned)gy < (unsigned)V.ry && (unsigned)gz < (unsigned)V.rz)) break;
         ++visited;
         const uint8_t st = V.occ ? __ldg(V.occ + V.bidx(gx, gy, gz)) : (uint8_t)kBrickMixed;
         if (st == kBrickEmpty) {
@@ -82,7 +83,9 @@ __global__ void __launch_bounds__(128) k_raycast_fast(const SessionDesc* __restr
           tsdf = V.load(V.vidx(gx, gy, gz), f) ? f : qnan();
           ++reads;
         }
-        if ((st == kBrickEmpty || st == kBrickPositive || st == kBrickNoNeg) && (!(prev < 0.f) || isnan(tsdf))) {
+        // empty, positive or no-negative (states 0, 2, 4): a region the march may cross
+        const bool crossable = (0x15u >> st) & 1u;
+        if (crossable && (!(prev < 0.f) || isnan(tsdf))) {
           int S = 128;
           bool uniform;
           const uint8_t s3 = __ldg(s.occ3 + (gx >> 7) + hx * ((gy >> 7) + hy * (gz >> 7)));
