@@ -705,6 +705,166 @@ def cpu_baseline(args, seconds=12.0):
                       % (frames, cores)}
 
 
+def _ate(poses, gt, idx0=0):
+    """RMS position error (mm) of a trajectory against the true one, both from frame idx0."""
+    err = [np.asarray(p, np.float64) - _rel(gt, idx0, k)[1] for k, p in enumerate(poses)]
+    return round(float(np.sqrt(np.mean(np.sum(np.square(err), 1)))) * 1e3, 3)
+
+
+STAGE_NAMES = ("preprocess", "pyramid+feedback", "track", "integrate", "summaries", "raycast", "tick")
+
+
+def _run_stream(L, ctx, cfg, frames, colors, gt, mesh_every=0, mesh_cap=1 << 22, skip=3):
+    """One stream frame by frame through the public per-frame call (host frames), with the
+    per-stage device times of each frame; meshes every mesh_every frames.  Stage times and
+    frames/s are taken over the frames after the first `skip`."""
+    import torch
+    s = L.Session(ctx, cfg)
+    ctx.enable_timing(True)
+    st, poses, mesh_ms, verts, lost = [], [], [], [], 0
+    for k in range(len(frames)):
+        ok, p = s.process(frames[k], colors[k] if colors is not None else None)
+        lost += 0 if ok else 1
+        if k >= skip:
+            st.append([ctx.stage_ms(i) for i in range(7)])
+        poses.append(p[9:12].copy())
+        if mesh_every and (k + 1) % mesh_every == 0:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _, _, n = s.mesh(mesh_cap)
+            torch.cuda.synchronize()
+            mesh_ms.append((time.perf_counter() - t0) * 1e3)
+            verts.append(int(n))
+    ctx.enable_timing(False)
+    hs = s.hash_stats() if cfg.volume_kind == 1 else None
+    s.close()
+    st = np.array(st)
+    med = np.median(st, 0)
+    out = {"frames": len(frames), "tracking_lost": lost, "frames_per_s": round(1e3 / float(med[6]), 1),
+           "stage_ms_median": {n: round(float(v), 4) for n, v in zip(STAGE_NAMES, med)},
+           "ate_mm": _ate(poses, gt)}
+    if mesh_every:
+        out["mesh_ms"] = [round(x, 2) for x in mesh_ms]
+        out["mesh_vertices"] = verts
+    if hs is not None:
+        out["hash_visible_blocks_last"] = int(hs[0])
+    return out, np.array(poses)
+
+
+def _render(L, kind, seed, n, color, W=W_IMG, H=H_IMG, radius=1.5, deg=2.0, extent=3.0):
+    sc = L.SynthScene(kind, seed=seed, extent=extent)
+    fr, co, gt = [], [], []
+    for k in range(n):
+        R, t = sc.pose(k, radius=radius, deg_per_frame=deg)
+        d, c = sc.render(R, t, W, H, frame=k, noise_seed=seed * 7 + 1, color=color)
+        fr.append(d)
+        co.append(np.ascontiguousarray(c) if color else None)
+        gt.append((np.asarray(R, np.float64), np.asarray(t, np.float64)))
+    return fr, (co if color else None), gt
+
+
+def _cpu_stages(frames, cfg_ns, nframes):
+    """The reference's kernels compiled for the host (oracle/_ref), per stage, on the first
+    nframes tracked frames of a sequence: ms per frame of preprocessing, ICP, integration and
+    raycast (all host threads)."""
+    from oracle.ref_engine import RefEngine
+    eng = RefEngine(cfg_ns)
+    spent = {"preprocess": 0.0, "icp": 0.0, "integrate": 0.0, "raycast": 0.0}
+    pre, integ, ray = eng._preprocess, eng._integrate, eng._raycast
+
+    def timed(name, f):
+        def g(*a):
+            t0 = time.perf_counter()
+            r = f(*a)
+            spent[name] += time.perf_counter() - t0
+            return r
+        return g
+    eng._preprocess, eng._integrate, eng._raycast = timed("preprocess", pre), timed("integrate", integ), \
+        timed("raycast", ray)
+    eng.frame(frames[0])
+    for k in spent:
+        spent[k] = 0.0
+    t0 = time.perf_counter()
+    for k in range(1, nframes + 1):
+        eng.frame(frames[k])
+    total = time.perf_counter() - t0
+    spent["icp"] = total - spent["preprocess"] - spent["integrate"] - spent["raycast"]
+    return {"frames": nframes, "threads": os.cpu_count(), "frames_per_s": round(nframes / total, 3),
+            "stage_ms": {k: round(v / nframes * 1e3, 1) for k, v in spent.items()},
+            "format": "int16 (the reference's short2 volume)"}
+
+
+def run_configs(args):
+    """The workload's other configurations, each through the public per-frame or batched
+    call on one GPU (synthetic scenes rendered first, not timed):
+      1. dense 256^3 FP32 TSDF + weight over 3 m, 100 frames, ICP 10/5/4, marching cubes at
+         the end; the reference's kernels on the host cores beside it, per stage;
+      2. dense 512^3 over 4 m with colour ICP (photometric weight 0.1), FP32 against FP16 +
+         u8, 100 frames;
+      3. voxel hashing at 5 mm (2^20 buckets, 2^21-block pool), room-scale scene walked at
+         1.2 m/s, colour ICP, raycast every frame, marching cubes every 100 frames;
+      4. 32 batched sessions of mixed volume and image sizes (as in the main line).
+    Prints one JSON line."""
+    import types
+
+    import torch
+    from natureuserinterfacestudio_b200 import _lib as L
+    torch.cuda.set_device(0)
+    ctx = L.Context(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    out = {}
+    # 1. plain dense 256^3
+    fr, _, gt = _render(L, L.SYNTH_TABLETOP, 11, args.config_frames, False)
+    cfg = L.default_cfg(res=(256, 256, 256), dim=(3.0, 3.0, 3.0), tsdf_format=L.TSDF_F32, trunc_dist=0.046875,
+                        iterations=[10, 5, 4, 0], integration_threshold=0.0)
+    r1, _ = _run_stream(L, ctx, cfg, fr, None, gt, mesh_every=len(fr))
+    cpu_cfg = types.SimpleNamespace(width=W_IMG, height=H_IMG, fx=FOCAL, fy=FOCAL, cx=(W_IMG - 1) / 2.0,
+                                    cy=(H_IMG - 1) / 2.0, depth_min=0.5, depth_max=4.5, res=(256, 256, 256),
+                                    dim=(3.0, 3.0, 3.0), trunc_dist=0.046875, filter_radius=3,
+                                    sigma_space2_inv_half=0.08, sigma_depth2_inv_half=50.0, depth_threshold=0.3,
+                                    dist_threshold=0.1, levels=3, iterations=[10, 5, 4, 0])
+    r1["cpu_reference"] = _cpu_stages(fr, cpu_cfg, args.config_cpu_frames)
+    out["1_dense_256_fp32"] = r1
+    # 2. dense 512^3 with colour ICP, FP32 and FP16 + u8
+    fr, co, gt = _render(L, L.SYNTH_TABLETOP, 12, args.config_frames, True, extent=3.0)
+    res2 = {}
+    poses2 = {}
+    for name, fmt in (("fp32", L.TSDF_F32), ("fp16_u8", L.TSDF_F16_U8)):
+        cfg = L.default_cfg(res=(512, 512, 512), dim=(4.0, 4.0, 4.0), tsdf_format=fmt, trunc_dist=0.03,
+                            iterations=[10, 5, 4, 0], integration_threshold=0.0, color_volume=1,
+                            photometric_weight=0.1)
+        res2[name], poses2[name] = _run_stream(L, ctx, cfg, fr, co, gt)
+    res2["traj_rms_diff_mm"] = round(float(np.sqrt(np.mean(np.sum((poses2["fp32"] - poses2["fp16_u8"]) ** 2, 1))))
+                                     * 1e3, 3)
+    out["2_dense_512_color_fp32_vs_fp16"] = res2
+    torch.cuda.empty_cache()
+    ctx.trim()
+    # 3. room-scale voxel hashing
+    sc = L.SynthScene(L.SYNTH_ROOM, seed=13)
+    fr, co, gt = [], [], []
+    for k in range(args.room_frames):
+        R, t = sc.pose(k)
+        d, c = sc.render(R, t, W_IMG, H_IMG, frame=k, noise_seed=91, color=True)
+        fr.append(d)
+        co.append(np.ascontiguousarray(c))
+        gt.append((np.asarray(R, np.float64), np.asarray(t, np.float64)))
+    cfg = L.default_cfg(volume_kind=L.VOLUME_HASH, tsdf_format=L.TSDF_F16_U8, voxel_size=0.005, trunc_scale=0.02,
+                        hash_buckets=1 << 20, hash_excess=1 << 16, hash_pool_blocks=1 << 21,
+                        iterations=[10, 5, 4, 0], integration_threshold=0.0, depth_min=0.4, color_volume=1,
+                        photometric_weight=0.1)
+    out["3_hash_room_5mm"], _ = _run_stream(L, ctx, cfg, fr, co, gt, mesh_every=100, mesh_cap=1 << 24)
+    out["3_hash_room_5mm"]["walk"] = "1.2 m/s at 30 Hz, %d frames" % args.room_frames
+    torch.cuda.empty_cache()
+    ctx.trim()
+    # 4. batched mixed sizes
+    out["4_batched_32_mixed"] = mixed_batch(L, ctx, torch, args.steps, args.warmup)
+    print(json.dumps({"impl": "ours", "configs": out, "n_gpus": 1, "data": "synthetic: seeded analytic scenes, "
+                      "Kinect noise model", "dtype": "f32 / f16"}))
+    return 0
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -740,11 +900,19 @@ def main():
                     help="skip the batched run of 32 sessions of mixed volume and image sizes")
     ap.add_argument("--no-autotune", dest="no_autotune", action="store_true",
                     help="keep the default launch shapes instead of timing the candidates first")
+    ap.add_argument("--configs", action="store_true",
+                    help="measure the other configurations (dense 256^3 with the reference's kernels on the host, "
+                         "512^3 colour FP32 vs FP16, room-scale hash, batched) instead of the serving line")
+    ap.add_argument("--config-frames", dest="config_frames", type=int, default=100)
+    ap.add_argument("--config-cpu-frames", dest="config_cpu_frames", type=int, default=4)
+    ap.add_argument("--room-frames", dest="room_frames", type=int, default=300)
     ap.add_argument("--tuning", default="",
                     help="launch shapes to use instead of autotuning: integration threads log2, ICP pixels "
                          "per thread, dense and hash ray tile widths, ICP blocks per session (e.g. 16,8,8,4,8)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.configs:
+        return run_configs(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if world > 1 and args.impl == "ours":
