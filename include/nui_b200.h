@@ -363,7 +363,7 @@ NUI_API nui_status nui_ctx_set_tuning(nui_ctx* ctx, const nui_tuning* t);
  * + f], host u16; bgra likewise or NULL), then times every candidate of each parameter in
  * turn (coordinate descent: integration, ICP, dense raycast, hash raycast; parameters no
  * session uses are skipped) as the median device time over `repeats` ticks of the
- * integration stage (integration) or of the whole tick (the others),
+ * integration stage (integration) or of the whole graphed tick (the others),
  * keeps the fastest in the context, frees the scratch sessions and reports the choice
  * (out) and the whole-tick median with it (out_tick_ms, nullable).  Takes the context's
  * stream for the whole call. */
