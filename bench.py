@@ -191,8 +191,8 @@ def run_ours(args, rank, world):
         tuning = ctx.tuning().as_dict()
     elif not args.no_autotune:
         t0 = time.perf_counter()
-        t, _ = ctx.autotune(cfgs, [[hframe(i, k) for k in range(4)] for i in range(n)], repeats=5,
-                            bgras=[[hcolor(i, k) for k in range(4)] for i in range(n)])
+        t, _ = ctx.autotune(cfgs, [[hframe(i, k) for k in range(8)] for i in range(n)], repeats=5,
+                            bgras=[[hcolor(i, k) for k in range(8)] for i in range(n)])
         tune_s = time.perf_counter() - t0
         tuning = t.as_dict()
         torch.cuda.empty_cache()
@@ -722,8 +722,13 @@ def _run_stream(L, ctx, cfg, frames, colors, gt, mesh_every=0, mesh_cap=1 << 22,
     s = L.Session(ctx, cfg)
     ctx.enable_timing(True)
     st, poses, mesh_ms, verts, lost = [], [], [], [], 0
+    error = None
     for k in range(len(frames)):
-        ok, p = s.process(frames[k], colors[k] if colors is not None else None)
+        try:
+            ok, p = s.process(frames[k], colors[k] if colors is not None else None)
+        except L.NuiError as e:  # e.g. a full hash pool: the stream stops there
+            error = {"frame": k, "status": e.status, "message": str(e)}
+            break
         lost += 0 if ok else 1
         if k >= skip:
             st.append([ctx.stage_ms(i) for i in range(7)])
@@ -740,7 +745,7 @@ def _run_stream(L, ctx, cfg, frames, colors, gt, mesh_every=0, mesh_cap=1 << 22,
     s.close()
     st = np.array(st)
     med = np.median(st, 0)
-    out = {"frames": len(frames), "tracking_lost": lost, "frames_per_s": round(1e3 / float(med[6]), 1),
+    out = {"frames": len(poses), "tracking_lost": lost, "frames_per_s": round(1e3 / float(med[6]), 1),
            "stage_ms_median": {n: round(float(v), 4) for n, v in zip(STAGE_NAMES, med)},
            "ate_mm": _ate(poses, gt)}
     if mesh_every:
@@ -748,6 +753,8 @@ def _run_stream(L, ctx, cfg, frames, colors, gt, mesh_every=0, mesh_cap=1 << 22,
         out["mesh_vertices"] = verts
     if hs is not None:
         out["hash_visible_blocks_last"] = int(hs[0])
+    if error is not None:
+        out["error"] = error
     return out, np.array(poses)
 
 
@@ -851,7 +858,7 @@ def run_configs(args):
         co.append(np.ascontiguousarray(c))
         gt.append((np.asarray(R, np.float64), np.asarray(t, np.float64)))
     cfg = L.default_cfg(volume_kind=L.VOLUME_HASH, tsdf_format=L.TSDF_F16_U8, voxel_size=0.005, trunc_scale=0.02,
-                        hash_buckets=1 << 20, hash_excess=1 << 16, hash_pool_blocks=1 << 21,
+                        hash_buckets=1 << 20, hash_excess=1 << 20, hash_pool_blocks=1 << 21,
                         iterations=[10, 5, 4, 0], integration_threshold=0.0, depth_min=0.4, color_volume=1,
                         photometric_weight=0.1)
     out["3_hash_room_5mm"], _ = _run_stream(L, ctx, cfg, fr, co, gt, mesh_every=100, mesh_cap=1 << 24)

@@ -344,7 +344,7 @@ NUI_API nui_status nui_ctx_last_tick_kernels(nui_ctx* ctx, int* n);
  *                            threads (chunks of >= 16 slices); 14..22, default 18
  *   icp_pixels_per_thread    ICP block: 256 threads x this many pixels; 2, 4, 8 or 16 (4)
  *   icp_cluster_blocks       ICP: thread blocks of the cluster that tracks one session;
- *                            2, 4, 8 or 16 (8; 16 is a non-portable cluster size)
+ *                            2, 4, 8 or 16 (16, a non-portable cluster size)
  *   raycast_tile_width       dense raycast: a warp shades a tile this wide and 32 / this
  *                            high, a block 2 x 2 such tiles; 4, 8, 16 or 32 (8)
  *   hash_raycast_tile_width  the same for the voxel-hash raycast (8)
@@ -363,7 +363,8 @@ NUI_API nui_status nui_ctx_set_tuning(nui_ctx* ctx, const nui_tuning* t);
  * + f], host u16; bgra likewise or NULL), then times every candidate of each parameter in
  * turn (coordinate descent: integration, ICP, dense raycast, hash raycast; parameters no
  * session uses are skipped) as the median device time over `repeats` ticks of the
- * integration stage (integration) or of the whole graphed tick (the others),
+ * integration stage (integration) or of the whole graphed tick (the others); a setting
+ * keeps its current value unless a candidate is at least 2 % faster,
  * keeps the fastest in the context, frees the scratch sessions and reports the choice
  * (out) and the whole-tick median with it (out_tick_ms, nullable).  Takes the context's
  * stream for the whole call. */

@@ -228,7 +228,7 @@ struct nui_ctx {
   };
   std::map<BatchPlan, Graph> graphs;
   int last_kernels = 0;  // kernels of the last graphed tick
-  nui_tuning tune = {18, 4, 8, 8, 8};
+  nui_tuning tune = {18, 4, 8, 8, 16};
   cudaMemPool_t pool = nullptr;  // session state (stream-ordered; freed memory stays here)
 };
 
@@ -1238,22 +1238,28 @@ NUI_API nui_status nui_ctx_autotune(nui_ctx* c, const nui_session_cfg* cfgs, int
   };
   nui_tuning best = c->tune;
   // one parameter at a time: its stage's median over `repeats` ticks
+  // The current value is timed first and stays unless a candidate beats it by 2 %: tick
+  // times wander by a few per cent between otherwise equal runs, and a noise-driven switch
+  // away from the default shape cost more than it ever gained.
   auto tune_one = [&](int nui_tuning::*field, std::initializer_list<int> cands, int stage) {
-    float best_ms = 0.f;
-    int pick = best.*field;
+    const int cur = best.*field;
+    c->tune = best;
+    float best_ms = measure(stage, nullptr), cur_ms = best_ms;
+    int pick = cur;
     for (int v : cands) {
       if (st != NUI_OK) return;
+      if (v == cur) continue;
       c->tune = best;
       c->tune.*field = v;
       const float ms = measure(stage, nullptr);
-      if (st == NUI_OK && (best_ms == 0.f || ms < best_ms)) best_ms = ms, pick = v;
+      if (st == NUI_OK && ms < best_ms && ms < 0.98f * cur_ms) best_ms = ms, pick = v;
     }
     best.*field = pick;
   };
   if (dense) tune_one(&nui_tuning::integrate_threads_log2, {16, 17, 18, 19, 20}, 3);
   // the ICP shapes and ray tiles by the whole tick: with dense and hash sessions the hash
   // sessions' tracking and raycast run on the second stream, beside stages 2-5
-  tune_one(&nui_tuning::icp_cluster_blocks, {4, 8, 16}, 6);
+  tune_one(&nui_tuning::icp_cluster_blocks, {8, 16}, 6);
   tune_one(&nui_tuning::icp_pixels_per_thread, {2, 4, 8, 16}, 6);
   if (dense) tune_one(&nui_tuning::raycast_tile_width, {4, 8, 16, 32}, 6);
   if (hash) tune_one(&nui_tuning::hash_raycast_tile_width, {4, 8, 16, 32}, 6);
