@@ -492,6 +492,15 @@ class Session:
         k = min(n.value, cap)
         return pos[:k], col[:k], n.value
 
+    def mesh_into(self, pos):
+        """Marching cubes into a caller's (cap, 3) float32 array (no colours); the vertex count
+        (more than cap: the mesh was cut)."""
+        n = C.c_uint64()
+        r = lib().nui_mesh(self.h, ptr(pos), None, pos.shape[0], C.byref(n))
+        if r not in (NUI_OK, NUI_ERR_MESH_OVERFLOW):
+            check(r)
+        return n.value
+
     def mesh_cases(self):
         rx, ry, rz = self.res
         out = np.zeros((ry - 1) * (rx - 1) * (rz - 1), np.uint8)
