@@ -78,11 +78,20 @@ __global__ void __launch_bounds__(256) k_color_grad(const SessionDesc* __restric
                             grad_byte(sob_x(s31.z, s11.z, s32.z, s12.z, s33.z, s13.z)), 255);
 }
 
+// Four pixels a thread (16-byte copies when both buffers allow them).
 __global__ void __launch_bounds__(256) k_color_keep(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (s.kind < 0 || !(s.photo_w > 0.f) || !s.bgra || !s.cprev) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < s.W * s.H) s.cprev[i] = __ldg(reinterpret_cast<const uchar4*>(s.bgra) + i);
+  const int n = s.W * s.H;
+  const int i = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= n) return;
+  const uchar4* src = reinterpret_cast<const uchar4*>(s.bgra);
+  const bool vec = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(s.cprev)) & 15) == 0;
+  if (vec && i + 3 < n) {
+    reinterpret_cast<uint4*>(s.cprev)[i / 4] = __ldg(reinterpret_cast<const uint4*>(src) + i / 4);
+  } else {
+    for (int k = i; k < min(i + 4, n); ++k) s.cprev[k] = __ldg(src + k);
+  }
 }
 
 }  // namespace nui

@@ -185,7 +185,7 @@ struct BatchPlan {
   long maxHashBlk;          // scan blocks of 1024 entries
   int hashMask;             // bit per hash sdf format
   int fmtMask;
-  int colorIcp;             // some session tracks with the photometric term
+  int colorIcp;             // some dense (bit 0) / hash (bit 1) session tracks with the photometric term
   int shiftFmtMask;         // bit per dense format of the shifting sessions
   int shiftColor;           // some shifting session has a colour volume
   int hashSwap;             // some hash session swaps blocks to the host
@@ -476,7 +476,7 @@ void plan_add(BatchPlan& p, const nui_session* s) {
   p.maxW = std::max(p.maxW, c.width);
   p.maxH = std::max(p.maxH, c.height);
   p.maxLevels = std::max(p.maxLevels, c.levels);
-  if (c.photometric_weight > 0.f) p.colorIcp = 1;
+  if (c.photometric_weight > 0.f) p.colorIcp |= s->hash ? 2 : 1;
   for (int l = 0; l < c.levels; ++l) p.maxIters[l] = std::max(p.maxIters[l], c.iterations[l]);
   if (s->hash) {
     p.hashMask |= 1 << (c.tsdf_format == NUI_TSDF_I16 ? 0 : 1);
@@ -692,10 +692,10 @@ void launch_icp_cluster(void (*kern)(const SessionDesc*), const SessionDesc* d, 
 // Colour pyramid (if any session tracks with colour), the ICP iterations of every level,
 // the integration gate and the published pose, for the n descriptors at d.
 void launch_track(const BatchPlan& p, const SessionDesc* d, int n, cudaStream_t st, float* d_pose, int* d_status,
-                  bool tick = true) {
+                  bool color, bool tick = true) {
   if (n <= 0) return;
   const unsigned npix = cdiv((long)p.maxW * p.maxH, 256);
-  if (p.colorIcp) k_color_grad<<<dim3(npix, n, 1), 256, 0, st>>>(d);  // finest level
+  if (color) k_color_grad<<<dim3(npix, n, 1), 256, 0, st>>>(d);  // finest level
   // every level and iteration of every session in one launch: a cluster of
   // icp_cluster_blocks blocks per session
   const int ppt = p.tune.icp_pixels_per_thread;
@@ -705,7 +705,7 @@ void launch_track(const BatchPlan& p, const SessionDesc* d, int n, cudaStream_t 
   else launch_icp_cluster(k_icp_cluster<4>, d, n, p.tune.icp_cluster_blocks, st);
   k_track_finalize<<<n, 32, 0, st>>>(d, tick ? 1 : 0);
   k_publish<<<cdiv(n, 64), 64, 0, st>>>(d, n, d_pose, d_status);
-  if (p.colorIcp) k_color_keep<<<dim3(npix, n), 256, 0, st>>>(d);
+  if (color) k_color_keep<<<dim3(cdiv(((long)p.maxW * p.maxH + 3) / 4, 256), n), 256, 0, st>>>(d);
 }
 
 // The launch schedule of one tick.  ev: optional stage events (timing only).
@@ -736,10 +736,10 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
     cudaEventRecord(ctx->fork_ev, st);
     cudaStreamWaitEvent(hs, ctx->fork_ev, 0);
     if (ev) cudaEventRecord(ctx->ev[9], hs);
-    launch_track(p, d + p.denseHead, p.n - p.denseHead, hs, d_pose, d_status);
-    launch_track(p, d, p.denseHead, st, d_pose, d_status);
+    launch_track(p, d + p.denseHead, p.n - p.denseHead, hs, d_pose, d_status, (p.colorIcp & 2) != 0);
+    launch_track(p, d, p.denseHead, st, d_pose, d_status, (p.colorIcp & 1) != 0);
   } else {
-    launch_track(p, d, p.n, st, d_pose, d_status);
+    launch_track(p, d, p.n, st, d_pose, d_status, p.colorIcp != 0);
   }
   mark(3);
   if (fork && !split) {
@@ -1781,7 +1781,7 @@ nui_status run_stage(nui_session* s, int what) {
     for (int l = 1; l < p.maxLevels; ++l)
       k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), 1), 256, 0, st>>>(dd, l);
   } else if (what == 1) {
-    launch_track(p, dd, p.n, st, ctx->d_pose, ctx->d_status, false);
+    launch_track(p, dd, p.n, st, ctx->d_pose, ctx->d_status, p.colorIcp != 0, false);
   } else if (what == 2) {
     k_ztab<<<1, 32, 0, st>>>(dd);
     launch_shift(p, dd, st);
@@ -1799,7 +1799,7 @@ nui_status run_stage(nui_session* s, int what) {
     launch_hash_raycast(p, dd, st);
   } else if (what == 4) {
     k_feedback<<<dim3(cdiv((long)p.maxW * p.maxH, 256), 1), 256, 0, st>>>(dd);
-    if (p.colorIcp) k_color_keep<<<dim3(cdiv((long)p.maxW * p.maxH, 256), 1), 256, 0, st>>>(dd);
+    if (p.colorIcp) k_color_keep<<<dim3(cdiv(((long)p.maxW * p.maxH + 3) / 4, 256), 1), 256, 0, st>>>(dd);
   }
   NUI_CUDA(cudaGetLastError());
   NUI_CUDA(cudaStreamSynchronize(st));
