@@ -100,52 +100,6 @@ struct RayVol {
            t011 * (1 - a) * b * c + t100 * a * (1 - b) * (1 - c) + t101 * a * (1 - b) * c +
            t110 * a * b * (1 - c) + t111 * a * b * c;
   }
-  // Tolerance mode: the central-difference normal at vf from its six samples vf +- cell
-  // along each axis (raycast.cl:253-268), read as one neighbourhood.  In exact arithmetic
-  // a sample one cell away has vf's trilinear base shifted by one voxel and the same
-  // fractions, so the six samples need the 32 voxels of a cross around vf's base (four
-  // along the axis of the pair, two across) instead of 6 x 8 separate reads; each sample
-  // keeps trilinear()'s bounds test (on its rounded voxel) and its weights.
-  __device__ __forceinline__ float3 normal_fast(float3 vf) const {
-    int gx, gy, gz;
-    voxel_of(vf, gx, gy, gz);
-    const float vx = ((float)gx + 0.5f) * c0, vy = ((float)gy + 0.5f) * c1, vz = ((float)gz + 0.5f) * c2;
-    const int bx = (vf.x < vx) ? gx - 1 : gx, by = (vf.y < vy) ? gy - 1 : gy, bz = (vf.z < vz) ? gz - 1 : gz;
-    const float a = vf.x * i0 - ((float)bx + 0.5f), b = vf.y * i1 - ((float)by + 0.5f),
-                c = vf.z * i2 - ((float)bz + 0.5f);
-    // v[z + 1][y + 1][x + 1] at offsets -1..2 from the base; only the cross is read
-    float v[4][4][4];
-#pragma unroll
-    for (int dz = -1; dz <= 2; ++dz)
-#pragma unroll
-      for (int dy = -1; dy <= 2; ++dy)
-#pragma unroll
-        for (int dx = -1; dx <= 2; ++dx) {
-          const int out = (dx < 0 || dx > 1) + (dy < 0 || dy > 1) + (dz < 0 || dz > 1);
-          if (out > 1) continue;
-          const int x = bx + dx, y = by + dy, z = bz + dz;
-          float f = qnan();
-          if ((unsigned)x < (unsigned)rx && (unsigned)y < (unsigned)ry && (unsigned)z < (unsigned)rz) {
-            float w;
-            f = load(vidx(x, y, z), w) ? w : qnan();
-          }
-          v[dz + 1][dy + 1][dx + 1] = f;
-        }
-    // trilinear() of the sample whose base is offset by (ox, oy, oz), its rounded voxel by
-    // the same offset from (gx, gy, gz)
-    auto tri = [&](int ox, int oy, int oz) -> float {
-      const int rx_ = gx + ox, ry_ = gy + oy, rz_ = gz + oz;
-      if (rx_ <= 0 || rx_ >= rx - 1 || ry_ <= 0 || ry_ >= ry - 1 || rz_ <= 0 || rz_ >= rz - 1) return qnan();
-      const int X = ox + 1, Y = oy + 1, Z = oz + 1;
-      const float t000 = v[Z][Y][X], t001 = v[Z + 1][Y][X], t011 = v[Z + 1][Y][X + 1], t010 = v[Z][Y][X + 1],
-                  t110 = v[Z][Y + 1][X + 1], t111 = v[Z + 1][Y + 1][X + 1], t101 = v[Z + 1][Y + 1][X],
-                  t100 = v[Z][Y + 1][X];
-      return t000 * (1 - a) * (1 - b) * (1 - c) + t001 * (1 - a) * (1 - b) * c + t010 * (1 - a) * b * (1 - c) +
-             t011 * (1 - a) * b * c + t100 * a * (1 - b) * (1 - c) + t101 * a * (1 - b) * c +
-             t110 * a * b * (1 - c) + t111 * a * b * c;
-    };
-    return f3(tri(1, 0, 0) - tri(-1, 0, 0), tri(0, 1, 0) - tri(0, -1, 0), tri(0, 0, 1) - tri(0, 0, -1));
-  }
   // Largest ray parameter up to which a sample stays (by 1% of a voxel) inside the
   // p-box of the aligned region of S^3 voxels (S a power of two) holding (gx, gy, gz),
   // clipped to the volume; samples with parameter below it map to voxels of that region.
