@@ -172,6 +172,13 @@ struct SessionDesc {
   float2* range;                  // expected range image
 };
 
+// Session families of a launch that covers the whole batch table: 0 every session, 1 the
+// dense (non-hash) ones, 2 the voxel-hash ones.
+constexpr int kFamAll = 0, kFamDense = 1, kFamHash = 2;
+__device__ __forceinline__ bool in_family(const SessionDesc& s, int fam) {
+  return fam == kFamAll || (fam == kFamHash) == (s.hash != 0);
+}
+
 // Hash entry (NuiKinfuHashEntry, hashing_gpu_def.h:49-63): 16 bytes.
 struct __align__(16) HEntry {
   short pos[3];

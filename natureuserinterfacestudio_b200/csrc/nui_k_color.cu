@@ -49,10 +49,10 @@ __global__ void __launch_bounds__(256) k_color_level(const SessionDesc* __restri
 
 __device__ __forceinline__ unsigned char grad_byte(float v) { return (unsigned char)(int)v; }
 
-__global__ void __launch_bounds__(256) k_color_grad(const SessionDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(256) k_color_grad(const SessionDesc* __restrict__ descs, int fam) {
   const SessionDesc& s = descs[blockIdx.y];
   const int l = blockIdx.z;
-  if (s.kind != kTrackFrame || !(s.photo_w > 0.f) || !s.bgra || l >= s.levels || !s.cgx[l]) return;
+  if (s.kind != kTrackFrame || !in_family(s, fam) || !(s.photo_w > 0.f) || !s.bgra || l >= s.levels || !s.cgx[l]) return;
   const int W = s.W >> l, H = s.H >> l;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= W * H) return;
@@ -79,9 +79,9 @@ __global__ void __launch_bounds__(256) k_color_grad(const SessionDesc* __restric
 }
 
 // Four pixels a thread (16-byte copies when both buffers allow them).
-__global__ void __launch_bounds__(256) k_color_keep(const SessionDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(256) k_color_keep(const SessionDesc* __restrict__ descs, int fam) {
   const SessionDesc& s = descs[blockIdx.y];
-  if (s.kind < 0 || !(s.photo_w > 0.f) || !s.bgra || !s.cprev) return;
+  if (s.kind < 0 || !in_family(s, fam) || !(s.photo_w > 0.f) || !s.bgra || !s.cprev) return;
   const int n = s.W * s.H;
   const int i = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
   if (i >= n) return;

@@ -488,11 +488,11 @@ __device__ __forceinline__ double icp_block_sum(const double (&acc)[kIcpTerms]) 
 // early leave their SMs to the others.
 template <int PPT>
 __global__ void __launch_bounds__(kIcpThreads, 2)
-    k_icp_cluster(const SessionDesc* __restrict__ descs) {
+    k_icp_cluster(const SessionDesc* __restrict__ descs, int fam) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   const SessionDesc& s = descs[blockIdx.y];
-  if (s.kind != kTrackFrame) return;  // the same for every block of the cluster
+  if (s.kind != kTrackFrame || !in_family(s, fam)) return;  // the same for every block of the cluster
   TrackState* ts = s.ts;
   const int rank = (int)cluster.block_rank(), C = (int)cluster.num_blocks();
   __shared__ float sR[9], st[3];
@@ -581,10 +581,10 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
   cluster.sync();  // no block leaves while another may still read block 0's shared memory
 }
 
-template __global__ void k_icp_cluster<2>(const SessionDesc*);
-template __global__ void k_icp_cluster<4>(const SessionDesc*);
-template __global__ void k_icp_cluster<8>(const SessionDesc*);
-template __global__ void k_icp_cluster<16>(const SessionDesc*);
+template __global__ void k_icp_cluster<2>(const SessionDesc*, int);
+template __global__ void k_icp_cluster<4>(const SessionDesc*, int);
+template __global__ void k_icp_cluster<8>(const SessionDesc*, int);
+template __global__ void k_icp_cluster<16>(const SessionDesc*, int);
 
 // After the last ICP launch (or on frame 0): publish the pose, decide the integration
 // gate (NuiKinfuTrackingEngine.cpp:115-127) and reset the estimate for the next frame.
@@ -644,9 +644,9 @@ __global__ void k_ztab(const SessionDesc* __restrict__ descs) {
 
 // shift_now: the tick's finalize makes the shifting volume's shift of an integrating
 // frame here; the step-wise track leaves it to the integration call (k_ztab).
-__global__ void k_track_finalize(const SessionDesc* __restrict__ descs, int shift_now) {
+__global__ void k_track_finalize(const SessionDesc* __restrict__ descs, int shift_now, int fam) {
   const SessionDesc& s = descs[blockIdx.x];
-  if (threadIdx.x != 0 || s.kind < 0) return;
+  if (threadIdx.x != 0 || s.kind < 0 || !in_family(s, fam)) return;
   TrackState* ts = s.ts;
   if (s.kind == kFirstFrame) {
     ts->integrate = ts->status == 0 ? 1 : 0;

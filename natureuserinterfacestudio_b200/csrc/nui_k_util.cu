@@ -6,11 +6,11 @@ namespace nui {
 
 // One thread per session: status, gate and pose of this tick into a packed array that
 // the host reads back with one copy.
-__global__ void k_publish(const SessionDesc* __restrict__ descs, int n, float* pose, int* status) {
+__global__ void k_publish(const SessionDesc* __restrict__ descs, int n, float* pose, int* status, int fam) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !pose || !status) return;
   const SessionDesc& s = descs[i];
-  if (s.ts == nullptr) return;
+  if (s.ts == nullptr || !in_family(s, fam)) return;
   const TrackState* ts = s.ts;
   const int o = s.slot;
   status[2 * o] = s.kind < 0 ? 0 : ts->status;

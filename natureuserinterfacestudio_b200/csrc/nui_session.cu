@@ -32,12 +32,12 @@ __global__ void k_pyramid(const SessionDesc*, int);
 __global__ void k_feedback(const SessionDesc*);
 __global__ void k_vertex_map(const SessionDesc*, int, float4*);
 template <int PPT>
-__global__ void k_icp_cluster(const SessionDesc*);
-__global__ void k_track_finalize(const SessionDesc*, int);
+__global__ void k_icp_cluster(const SessionDesc*, int);
+__global__ void k_track_finalize(const SessionDesc*, int, int);
 __global__ void k_ztab(const SessionDesc*);
 __global__ void k_color_level(const SessionDesc*, int);
-__global__ void k_color_grad(const SessionDesc*);
-__global__ void k_color_keep(const SessionDesc*);
+__global__ void k_color_grad(const SessionDesc*, int);
+__global__ void k_color_keep(const SessionDesc*, int);
 template <int F>
 __global__ void k_integrate(const SessionDesc*);
 template <int F>
@@ -57,7 +57,7 @@ template <int F>
 __global__ void k_raycast_fast(const SessionDesc*, int);
 template <int F>
 __global__ void k_raycast_finish_fast(const SessionDesc*);
-__global__ void k_publish(const SessionDesc*, int, float*, int*);
+__global__ void k_publish(const SessionDesc*, int, float*, int*, int);
 __global__ void k_tick_begin(const SessionDesc*, int);
 __global__ void k_hash_health(const SessionDesc*, int, int*);
 __global__ void k_occ_clear(const SessionDesc*);
@@ -664,7 +664,8 @@ void launch_shift(const BatchPlan& p, const SessionDesc* d, cudaStream_t st) {
 
 // The ICP kernel over n sessions, one cluster of cl blocks each (cl = 16 is beyond the
 // portable cluster size and needs the kernel's opt-in, given once per kernel).
-void launch_icp_cluster(void (*kern)(const SessionDesc*), const SessionDesc* d, int n, int cl, cudaStream_t st) {
+void launch_icp_cluster(void (*kern)(const SessionDesc*, int), const SessionDesc* d, int n, int cl, int fam,
+                        cudaStream_t st) {
   {
     static std::mutex mu;
     static std::vector<const void*> opted;
@@ -686,26 +687,28 @@ void launch_icp_cluster(void (*kern)(const SessionDesc*), const SessionDesc* d, 
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, kern, d);
+  cudaLaunchKernelEx(&cfg, kern, d, fam);
 }
 
 // Colour pyramid (if any session tracks with colour), the ICP iterations of every level,
-// the integration gate and the published pose, for the n descriptors at d.
+// the integration gate and the published pose, for the sessions of family fam among the n
+// descriptors at d.
 void launch_track(const BatchPlan& p, const SessionDesc* d, int n, cudaStream_t st, float* d_pose, int* d_status,
-                  bool color, bool tick = true) {
+                  bool color, int fam = kFamAll, bool tick = true) {
   if (n <= 0) return;
   const unsigned npix = cdiv((long)p.maxW * p.maxH, 256);
-  if (color) k_color_grad<<<dim3(npix, n, 1), 256, 0, st>>>(d);  // finest level
+  if (color) k_color_grad<<<dim3(npix, n, 1), 256, 0, st>>>(d, fam);  // finest level
   // every level and iteration of every session in one launch: a cluster of
   // icp_cluster_blocks blocks per session
   const int ppt = p.tune.icp_pixels_per_thread;
-  if (ppt == 2) launch_icp_cluster(k_icp_cluster<2>, d, n, p.tune.icp_cluster_blocks, st);
-  else if (ppt == 8) launch_icp_cluster(k_icp_cluster<8>, d, n, p.tune.icp_cluster_blocks, st);
-  else if (ppt == 16) launch_icp_cluster(k_icp_cluster<16>, d, n, p.tune.icp_cluster_blocks, st);
-  else launch_icp_cluster(k_icp_cluster<4>, d, n, p.tune.icp_cluster_blocks, st);
-  k_track_finalize<<<n, 32, 0, st>>>(d, tick ? 1 : 0);
-  k_publish<<<cdiv(n, 64), 64, 0, st>>>(d, n, d_pose, d_status);
-  if (color) k_color_keep<<<dim3(cdiv(((long)p.maxW * p.maxH + 3) / 4, 256), n), 256, 0, st>>>(d);
+  const int cl = p.tune.icp_cluster_blocks;
+  if (ppt == 2) launch_icp_cluster(k_icp_cluster<2>, d, n, cl, fam, st);
+  else if (ppt == 8) launch_icp_cluster(k_icp_cluster<8>, d, n, cl, fam, st);
+  else if (ppt == 16) launch_icp_cluster(k_icp_cluster<16>, d, n, cl, fam, st);
+  else launch_icp_cluster(k_icp_cluster<4>, d, n, cl, fam, st);
+  k_track_finalize<<<n, 32, 0, st>>>(d, tick ? 1 : 0, fam);
+  k_publish<<<cdiv(n, 64), 64, 0, st>>>(d, n, d_pose, d_status, fam);
+  if (color) k_color_keep<<<dim3(cdiv(((long)p.maxW * p.maxH + 3) / 4, 256), n), 256, 0, st>>>(d, fam);
 }
 
 // The launch schedule of one tick.  ev: optional stage events (timing only).
@@ -728,27 +731,28 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
   // kernels touch disjoint sessions, the dense integration starts as soon as the dense
   // sessions are tracked (instead of after the longer colour-tracked hash sessions), and
   // the many short kernels of the hash allocation fill the gaps of the dense integration.
-  // A served batch, whose descriptor table mixes the two families, tracks them together.
+  // A served batch, whose table keeps one launch shape while streams of either family come
+  // and go, launches both trackings over the whole table, each skipping the other family.
   const bool fork = p.hashMask && p.fmtMask;
-  const bool split = fork && p.hashTail > 0 && p.denseHead > 0;
+  const bool ranged = p.hashTail > 0 && p.denseHead > 0;
   cudaStream_t hs = fork ? ctx->side : st;
-  if (split) {
+  if (fork) {
     cudaEventRecord(ctx->fork_ev, st);
     cudaStreamWaitEvent(hs, ctx->fork_ev, 0);
     if (ev) cudaEventRecord(ctx->ev[9], hs);
-    launch_track(p, d + p.denseHead, p.n - p.denseHead, hs, d_pose, d_status, (p.colorIcp & 2) != 0);
-    launch_track(p, d, p.denseHead, st, d_pose, d_status, (p.colorIcp & 1) != 0);
+    if (ranged) {
+      launch_track(p, d + p.denseHead, p.n - p.denseHead, hs, d_pose, d_status, (p.colorIcp & 2) != 0);
+      launch_track(p, d, p.denseHead, st, d_pose, d_status, (p.colorIcp & 1) != 0);
+    } else {
+      launch_track(p, d, p.n, hs, d_pose, d_status, (p.colorIcp & 2) != 0, kFamHash);
+      launch_track(p, d, p.n, st, d_pose, d_status, (p.colorIcp & 1) != 0, kFamDense);
+    }
   } else {
     launch_track(p, d, p.n, st, d_pose, d_status, p.colorIcp != 0);
   }
   mark(3);
-  if (fork && !split) {
-    cudaEventRecord(ctx->fork_ev, st);
-    cudaStreamWaitEvent(hs, ctx->fork_ev, 0);
-  }
   if (ev) ctx->side_timed = fork;
   if (fork) {
-    if (ev && !split) cudaEventRecord(ctx->ev[9], hs);
     launch_hash_integrate(p, d, hs);
     launch_hash_raycast(p, d, hs);
     if (ev) cudaEventRecord(ctx->ev[10], hs);
@@ -1781,7 +1785,7 @@ nui_status run_stage(nui_session* s, int what) {
     for (int l = 1; l < p.maxLevels; ++l)
       k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), 1), 256, 0, st>>>(dd, l);
   } else if (what == 1) {
-    launch_track(p, dd, p.n, st, ctx->d_pose, ctx->d_status, p.colorIcp != 0, false);
+    launch_track(p, dd, p.n, st, ctx->d_pose, ctx->d_status, p.colorIcp != 0, kFamAll, false);
   } else if (what == 2) {
     k_ztab<<<1, 32, 0, st>>>(dd);
     launch_shift(p, dd, st);
@@ -1799,7 +1803,7 @@ nui_status run_stage(nui_session* s, int what) {
     launch_hash_raycast(p, dd, st);
   } else if (what == 4) {
     k_feedback<<<dim3(cdiv((long)p.maxW * p.maxH, 256), 1), 256, 0, st>>>(dd);
-    if (p.colorIcp) k_color_keep<<<dim3(cdiv(((long)p.maxW * p.maxH + 3) / 4, 256), 1), 256, 0, st>>>(dd);
+    if (p.colorIcp) k_color_keep<<<dim3(cdiv(((long)p.maxW * p.maxH + 3) / 4, 256), 1), 256, 0, st>>>(dd, kFamAll);
   }
   NUI_CUDA(cudaGetLastError());
   NUI_CUDA(cudaStreamSynchronize(st));
@@ -2100,7 +2104,7 @@ NUI_API nui_status nui_k_color_pyramid(nui_ctx* ctx, const uint8_t* d_bgra, int 
   NUI_CUDA(cudaMemcpyAsync(ctx->d_kdesc, &d, sizeof(d), cudaMemcpyHostToDevice, ctx->stream));
   for (int l = 1; l < levels; ++l)
     k_color_level<<<dim3(cdiv((long)(W >> l) * (H >> l), 256), 1), 256, 0, ctx->stream>>>(ctx->d_kdesc, l);
-  k_color_grad<<<dim3(cdiv((long)W * H, 256), 1, levels), 256, 0, ctx->stream>>>(ctx->d_kdesc);
+  k_color_grad<<<dim3(cdiv((long)W * H, 256), 1, levels), 256, 0, ctx->stream>>>(ctx->d_kdesc, kFamAll);
   NUI_CUDA(cudaGetLastError());
   NUI_CUDA(cudaStreamSynchronize(ctx->stream));
   return NUI_OK;
