@@ -21,12 +21,15 @@ __global__ void k_publish(const SessionDesc* __restrict__ descs, int n, float* p
   pose[14 * o + 13] = ts->count;
 }
 
-// Start of a tick: clear the per-frame counters of every active session.
+// Start of a tick: clear the per-frame counters of every active session, and the flag of a
+// frame that lost tracking (the state stayed on the frame before it; this frame starts
+// from a clean tracker even when it was launched before the loss was read back).
 __global__ void k_tick_begin(const SessionDesc* __restrict__ descs, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const SessionDesc& s = descs[i];
   if (s.kind < 0 || !s.ts) return;
+  s.ts->status = 0;
   s.ts->dmax_bits = 0;
   s.ts->touched = 0ull;
   s.ts->ray_reads = s.ts->ray_samples = s.ts->ray_hits = s.ts->bricks = s.ts->tiles = 0ull;

@@ -210,14 +210,19 @@ struct nui_ctx {
   bool side_timed = false;  // the last timed tick ran voxel-hash work on the side stream
   cudaEvent_t ev[kEvents] = {};
   float stage_ms[kStages] = {};
-  // batch table (device + pinned staging) and per-session outputs (status + pose)
+  // batch table (device + pinned staging) and per-session outputs (status + pose).  The
+  // host sides come in two halves used by alternate ticks (`par`), so that a tick can be
+  // launched while the previous one's results are still to be read; ev_tick[par] is
+  // recorded behind the last tick that used half par.
   int cap = 0;
   SessionDesc* d_descs = nullptr;
-  SessionDesc* h_descs = nullptr;
+  SessionDesc* h_descs = nullptr;  // 2 * cap
   float* d_pose = nullptr;  // cap * 14: R(9) t(3) err count
   int* d_status = nullptr;  // cap * 2: status, integrate
-  float* h_pose = nullptr;
-  int* h_status = nullptr;
+  float* h_pose = nullptr;  // 2 * cap * 14
+  int* h_status = nullptr;  // 2 * cap * 2
+  int par = 0;              // the half the next tick uses
+  cudaEvent_t ev_tick[2] = {nullptr, nullptr};
   // scratch descriptor for kernel-level calls
   SessionDesc* d_kdesc = nullptr;
   TrackState* d_kts = nullptr;
@@ -788,18 +793,27 @@ nui_status ensure_cap(nui_ctx* ctx, int n) {
   cudaStreamSynchronize(ctx->stream);
   for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second.exec);
   ctx->graphs.clear();
+  float* old_pose = ctx->h_pose;  // results of a tick not yet read move to the new arrays
+  int* old_status = ctx->h_status;
+  const int old_cap = ctx->cap;
   cudaFree(ctx->d_descs);
   cudaFreeHost(ctx->h_descs);
   cudaFree(ctx->d_pose);
   cudaFree(ctx->d_status);
-  cudaFreeHost(ctx->h_pose);
-  cudaFreeHost(ctx->h_status);
+  ctx->h_pose = nullptr;
+  ctx->h_status = nullptr;
   NUI_CUDA(counted_malloc(&ctx->d_descs, sizeof(SessionDesc) * cap));
-  NUI_CUDA(counted_malloc_host(&ctx->h_descs, sizeof(SessionDesc) * cap));
+  NUI_CUDA(counted_malloc_host(&ctx->h_descs, sizeof(SessionDesc) * 2 * cap));
   NUI_CUDA(counted_malloc(&ctx->d_pose, sizeof(float) * 14 * cap));
   NUI_CUDA(counted_malloc(&ctx->d_status, sizeof(int) * 2 * cap));
-  NUI_CUDA(counted_malloc_host(&ctx->h_pose, sizeof(float) * 14 * cap));
-  NUI_CUDA(counted_malloc_host(&ctx->h_status, sizeof(int) * 2 * cap));
+  NUI_CUDA(counted_malloc_host(&ctx->h_pose, sizeof(float) * 2 * 14 * cap));
+  NUI_CUDA(counted_malloc_host(&ctx->h_status, sizeof(int) * 2 * 2 * cap));
+  for (int h = 0; h < 2 && old_pose; ++h) {
+    std::memcpy(ctx->h_pose + (size_t)h * 14 * cap, old_pose + (size_t)h * 14 * old_cap, sizeof(float) * 14 * old_cap);
+    std::memcpy(ctx->h_status + (size_t)h * 2 * cap, old_status + (size_t)h * 2 * old_cap, sizeof(int) * 2 * old_cap);
+  }
+  cudaFreeHost(old_pose);
+  cudaFreeHost(old_status);
   ctx->cap = cap;
   return NUI_OK;
 }
@@ -823,9 +837,14 @@ nui_status finish_timing(nui_ctx* ctx) {
 // (nullable) is merged into the launch shape, so that a caller can keep one shape -- and
 // its graph -- while sessions come and go.
 nui_status tick_launch(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t* const* raws,
-                       const uint8_t* const* bgras, bool use_graph, const BatchPlan* floor) {
+                       const uint8_t* const* bgras, bool use_graph, const BatchPlan* floor, int* par_out) {
   nui_status st = ensure_cap(ctx, n);
   if (st != NUI_OK) return st;
+  // this tick's half of the host staging: the tick before last used it, and its table copy
+  // and result copies are complete once its event is
+  const int par = ctx->par;
+  NUI_CUDA(cudaEventSynchronize(ctx->ev_tick[par]));
+  SessionDesc* const hd = ctx->h_descs + (size_t)par * ctx->cap;
   BatchPlan p;
   p.n = n;
   // the table lists the non-hash slots first (empty ones included), then the hash sessions,
@@ -834,7 +853,7 @@ nui_status tick_launch(nui_ctx* ctx, nui_session* const* ss, int n, const uint16
   for (int i = 0; i < n; ++i) nhash += ss[i] && ss[i]->hash;
   for (int i = 0, jd = 0, jh = n - nhash; i < n; ++i) {
     nui_session* s = ss[i];
-    SessionDesc& dd = ctx->h_descs[s && s->hash ? jh++ : jd++];
+    SessionDesc& dd = hd[s && s->hash ? jh++ : jd++];
     if (!s) {
       std::memset(&dd, 0, sizeof(SessionDesc));
       dd.kind = kInactive;
@@ -855,7 +874,7 @@ nui_status tick_launch(nui_ctx* ctx, nui_session* const* ss, int n, const uint16
   }
   if (floor) plan_merge(p, *floor);
   p.tune = ctx->tune;
-  NUI_CUDA(cudaMemcpyAsync(ctx->d_descs, ctx->h_descs, sizeof(SessionDesc) * n, cudaMemcpyHostToDevice, ctx->stream));
+  NUI_CUDA(cudaMemcpyAsync(ctx->d_descs, hd, sizeof(SessionDesc) * n, cudaMemcpyHostToDevice, ctx->stream));
   if (use_graph && !ctx->timing) {
     auto it = ctx->graphs.find(p);
     if (it == ctx->graphs.end()) {
@@ -887,17 +906,28 @@ nui_status tick_launch(nui_ctx* ctx, nui_session* const* ss, int n, const uint16
     enqueue_tick(ctx, p, ctx->d_descs, ctx->d_pose, ctx->d_status, ctx->timing);
     NUI_CUDA(cudaGetLastError());
   }
-  NUI_CUDA(cudaMemcpyAsync(ctx->h_pose, ctx->d_pose, sizeof(float) * 14 * n, cudaMemcpyDeviceToHost, ctx->stream));
-  NUI_CUDA(cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int) * 2 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  NUI_CUDA(cudaMemcpyAsync(ctx->h_pose + (size_t)par * 14 * ctx->cap, ctx->d_pose, sizeof(float) * 14 * n,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  NUI_CUDA(cudaMemcpyAsync(ctx->h_status + (size_t)par * 2 * ctx->cap, ctx->d_status, sizeof(int) * 2 * n,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  NUI_CUDA(cudaEventRecord(ctx->ev_tick[par], ctx->stream));
+  ctx->par = par ^ 1;
+  if (par_out) *par_out = par;
+  // a session's frame count advances when its frame is launched (a lost frame takes it
+  // back when its result is read), so that the next tick can be launched before then
+  for (int i = 0; i < n; ++i)
+    if (ss[i] && raws[i]) ss[i]->frames += 1;
   return NUI_OK;
 }
 
-// Waits for the launched tick and takes its per-session results.
+// Waits for the tick launched with staging half par and takes its per-session results.
 nui_status tick_finish(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t* const* raws, nui_status* per,
-                       float* poses) {
-  NUI_CUDA(cudaStreamSynchronize(ctx->stream));
+                       float* poses, int par) {
+  NUI_CUDA(cudaEventSynchronize(ctx->ev_tick[par]));
   nui_status st = finish_timing(ctx);
   if (st != NUI_OK) return st;
+  const float* h_pose = ctx->h_pose + (size_t)par * 14 * ctx->cap;
+  const int* h_status = ctx->h_status + (size_t)par * 2 * ctx->cap;
   nui_status agg = NUI_OK;
   auto note = [](nui_status r) {
     if (r == NUI_ERR_HASH_FULL)
@@ -911,15 +941,14 @@ nui_status tick_finish(nui_ctx* ctx, nui_session* const* ss, int n, const uint16
       if (per) per[i] = NUI_OK;
       continue;
     }
-    int status = ctx->h_status[2 * i];
+    int status = h_status[2 * i];
     if (status == 4) {  // tracked and integrated, but the voxel hash dropped blocks
       if (per) per[i] = NUI_ERR_HASH_FULL;
       if (agg == NUI_OK) {
         agg = NUI_ERR_HASH_FULL;
         note(agg);
       }
-      s->frames += 1;
-      if (poses) std::memcpy(poses + 12 * i, ctx->h_pose + 14 * i, 12 * sizeof(float));
+      if (poses) std::memcpy(poses + 12 * i, h_pose + 14 * i, 12 * sizeof(float));
       continue;
     }
     nui_status r = status == 0 ? NUI_OK : NUI_ERR_TRACKING_LOST;
@@ -927,23 +956,23 @@ nui_status tick_finish(nui_ctx* ctx, nui_session* const* ss, int n, const uint16
     if (r != NUI_OK) {
       agg = NUI_ERR_TRACKING_LOST;
       note(agg);
-      // the device state stays on the previous frame; clear the flag so that the next
-      // frame (after nui_reset or not) starts from a clean tracker
-      int zero = 0;
-      cudaMemcpy(&s->ts->status, &zero, sizeof(int), cudaMemcpyHostToDevice);
-    } else {
-      s->frames += 1;
+      // the device state stays on the previous frame, which the frame count follows; the
+      // flag is cleared in stream order (every tick also clears it when it starts), so
+      // that the next frame (after nui_reset or not) starts from a clean tracker
+      s->frames -= 1;
+      NUI_CUDA(cudaMemsetAsync(&s->ts->status, 0, sizeof(int), ctx->stream));
     }
-    if (poses) std::memcpy(poses + 12 * i, ctx->h_pose + 14 * i, 12 * sizeof(float));
+    if (poses) std::memcpy(poses + 12 * i, h_pose + 14 * i, 12 * sizeof(float));
   }
   return agg;
 }
 
 nui_status run_tick(nui_ctx* ctx, nui_session* const* ss, int n, const uint16_t* const* raws,
                     const uint8_t* const* bgras, bool use_graph, nui_status* per, float* poses) {
-  nui_status st = tick_launch(ctx, ss, n, raws, bgras, use_graph, nullptr);
+  int par = 0;
+  nui_status st = tick_launch(ctx, ss, n, raws, bgras, use_graph, nullptr, &par);
   if (st != NUI_OK) return st;
-  return tick_finish(ctx, ss, n, raws, per, poses);
+  return tick_finish(ctx, ss, n, raws, per, poses, par);
 }
 
 nui_status upload_frame(nui_session* s, const uint16_t* depth, const uint8_t* bgra) {
@@ -1052,6 +1081,8 @@ NUI_API nui_status nui_ctx_create(int device, nui_ctx** out) {
   c->stream = c->own;
   for (int i = 0; i < kEvents; ++i) cudaEventCreate(&c->ev[i]);
   if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_tick[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_tick[1], cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
@@ -1098,6 +1129,8 @@ NUI_API nui_status nui_ctx_destroy(nui_ctx* c) {
   cudaStreamDestroy(c->side);
   cudaEventDestroy(c->fork_ev);
   cudaEventDestroy(c->join_ev);
+  cudaEventDestroy(c->ev_tick[0]);
+  cudaEventDestroy(c->ev_tick[1]);
   if (c->pool) {
     cudaDeviceSynchronize();
     cudaMemPoolDestroy(c->pool);
@@ -2440,13 +2473,16 @@ struct nui_server {
   nui_ctx* ctx = nullptr;
   size_t budget = 0, used = 0;  // live and pooled sessions
   cudaStream_t up = nullptr;
-  cudaEvent_t ev_t0 = nullptr, ev_up = nullptr, ev_done = nullptr, ev_order = nullptr;
+  cudaEvent_t ev_t0 = nullptr, ev_up = nullptr, ev_order = nullptr;
+  cudaEvent_t ev_done[2] = {nullptr, nullptr};  // behind the tick of each host staging half
   std::chrono::steady_clock::time_point t0;
   std::vector<Slot> slots;
   std::vector<Pooled> pool;
   BatchPlan floor;
-  // the batch in flight: every slot, with its session and frame (or none)
+  // the batch in flight: every slot, with its session and frame (or none), and the
+  // context's staging half it was launched with
   bool inflight = false;
+  int bpar = 0;
   std::vector<nui_session*> bsess;
   std::vector<const uint16_t*> braw;
   std::vector<const uint8_t*> bbgra;
@@ -2459,14 +2495,14 @@ namespace {
 nui_status server_collect(nui_server* v) {
   if (!v->inflight) return NUI_OK;
   v->inflight = false;
-  NUI_CUDA(cudaEventSynchronize(v->ev_done));
+  NUI_CUDA(cudaEventSynchronize(v->ev_done[v->bpar]));
   float ms = 0.f;
-  NUI_CUDA(cudaEventElapsedTime(&ms, v->ev_t0, v->ev_done));
+  NUI_CUDA(cudaEventElapsedTime(&ms, v->ev_t0, v->ev_done[v->bpar]));
   const double t_done = ms * 1e-3;
   const int n = (int)v->bsess.size();
   std::vector<nui_status> per(n);
   std::vector<float> poses(12 * (size_t)n);
-  nui_status st = tick_finish(v->ctx, v->bsess.data(), n, v->braw.data(), per.data(), poses.data());
+  nui_status st = tick_finish(v->ctx, v->bsess.data(), n, v->braw.data(), per.data(), poses.data(), v->bpar);
   if (st != NUI_OK && st != NUI_ERR_TRACKING_LOST && st != NUI_ERR_HASH_FULL) return st;
   for (int i = 0; i < n; ++i) {
     if (!v->bsess[i] || !v->braw[i]) continue;
@@ -2514,7 +2550,7 @@ NUI_API nui_status nui_server_create(nui_ctx* ctx, size_t budget, int max_stream
   v->floor.n = max_streams;
   if (cudaStreamCreateWithFlags(&v->up, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&v->ev_t0) != cudaSuccess || cudaEventCreateWithFlags(&v->ev_up, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreate(&v->ev_done) != cudaSuccess ||
+      cudaEventCreate(&v->ev_done[0]) != cudaSuccess || cudaEventCreate(&v->ev_done[1]) != cudaSuccess ||
       cudaEventCreateWithFlags(&v->ev_order, cudaEventDisableTiming) != cudaSuccess) {
     delete v;
     return fail(NUI_ERR_DEVICE, "stream / event creation failed");
@@ -2558,7 +2594,8 @@ NUI_API nui_status nui_server_destroy(nui_server* v) {
   cudaStreamDestroy(v->up);
   cudaEventDestroy(v->ev_t0);
   cudaEventDestroy(v->ev_up);
-  cudaEventDestroy(v->ev_done);
+  cudaEventDestroy(v->ev_done[0]);
+  cudaEventDestroy(v->ev_done[1]);
   cudaEventDestroy(v->ev_order);
   delete v;
   return NUI_OK;
@@ -2697,21 +2734,26 @@ NUI_API nui_status nui_server_step(nui_server* v, int* launched) {
     ++count;
   }
   NUI_CUDA(cudaEventRecord(v->ev_up, v->up));
-  // collect the batch in flight while these uploads run
-  nui_status st = server_collect(v);
-  if (st != NUI_OK) return st;
   if (launched) *launched = count;
-  if (count == 0) return NUI_OK;
+  if (count == 0) return server_collect(v);
+  // the new batch is queued behind the one in flight before that one is waited for, so
+  // that the device goes from one tick to the next without waiting for the host
   NUI_CUDA(cudaStreamWaitEvent(v->ctx->stream, v->ev_up, 0));
-  st = tick_launch(v->ctx, nsess.data(), ns, nraw.data(), nbgra.data(), true, &v->floor);
-  if (st != NUI_OK) return st;
-  NUI_CUDA(cudaEventRecord(v->ev_done, v->ctx->stream));
+  int par = 0;
+  nui_status st = tick_launch(v->ctx, nsess.data(), ns, nraw.data(), nbgra.data(), true, &v->floor, &par);
+  if (st != NUI_OK) {
+    server_collect(v);
+    return st;
+  }
+  NUI_CUDA(cudaEventRecord(v->ev_done[par], v->ctx->stream));
+  st = server_collect(v);  // the batch launched by the previous step
   v->bsess.swap(nsess);
   v->braw.swap(nraw);
   v->bbgra.swap(nbgra);
   v->bframe.swap(nframe);
+  v->bpar = par;
   v->inflight = true;
-  return NUI_OK;
+  return st;
 }
 
 NUI_API nui_status nui_server_drain(nui_server* v) {
