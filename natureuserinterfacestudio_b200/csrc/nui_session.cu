@@ -866,9 +866,11 @@ nui_status tick_launch(nui_ctx* ctx, nui_session* const* ss, int n, const uint16
     fill_desc(s, dd, kind, raws[i], bgras ? bgras[i] : nullptr);
     dd.slot = i;
   }
-  // a served batch keeps one launch shape (and graph) while sessions come and go: both
-  // families then launch over the whole table
-  if (!floor) {
+  // the dense kernels launch over the rows before the hash sessions and the hash kernels
+  // over theirs.  A served batch keeps its launch shape while streams come and go, but the
+  // split follows the count of hash streams (a graph per count; empty slots sit among the
+  // dense rows); with one family absent both launch over the whole table.
+  if (!floor || (nhash > 0 && nhash < n)) {
     p.hashTail = nhash;
     p.denseHead = n - nhash;
   }
