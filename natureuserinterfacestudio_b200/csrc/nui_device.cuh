@@ -14,6 +14,7 @@ constexpr int kMaxLevels = 4;
 constexpr int kMaxRadius = 7;
 constexpr int kIcpTerms = 29;  // 21 JtJ + 6 Jtr + r^2 + count  (icp.cl:122-160)
 constexpr int kTile = 16;      // pixel tile of the depth bound used by integration culling
+constexpr int kPreBlockX = 32, kPreBlockY = 8;  // k_preprocess block: 32 x 16 pixels, two a thread
 constexpr int kFastWarps = 4;  // warps per block of the tolerance-mode integration
 constexpr int kFastWarpSmem = 64 * 32 * 4 + 64 * 32 * 4;  // its shared memory per warp (bytes)
 

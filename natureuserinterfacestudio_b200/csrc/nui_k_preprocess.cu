@@ -3,8 +3,9 @@
 //  k_preprocess   depth_passing_filter_kernel (filters.cl:9-23) + bilateral_filter_depth_kernel
 //                 (bilateralFilter.cl:68-119) + depth2vertex_kernel at level 0
 //                 (transformMaps.cl:18-42) + scaleDepthsKernel (tsdfVolume.cl:8-29), fused.
-//                 One block per 32x16 output tile; the pass-filtered depth of the tile and
-//                 its radius-r halo is staged in shared memory once and read 49 times.
+//                 One block per 32x16 output tile, two vertically adjacent pixels a thread;
+//                 the pass-filtered depth of the tile and its radius-r halo is staged in
+//                 shared memory once.
 //                 Also writes the largest ray-length depth of each 16x16 tile (integration
 //                 uses it to skip voxels that are behind every surface they can project to).
 //  k_pyramid      half_sample_kernel (transformMaps.cl:44-88) + depth2vertex_kernel for one
@@ -18,7 +19,7 @@
 
 namespace nui {
 
-constexpr int kPreTX = 32, kPreTY = 16;
+constexpr int kPreTX = kPreBlockX, kPreTY = 2 * kPreBlockY;
 constexpr int kPreSW = kPreTX + 2 * kMaxRadius, kPreSH = kPreTY + 2 * kMaxRadius, kGW = 2 * kMaxRadius + 1;
 
 // The bilateral sum of one pixel: taps in row-major window order, each weighted by its
@@ -48,29 +49,50 @@ __device__ __forceinline__ float bilateral_px(const float* t, const float* g, in
   return sd / swt;
 }
 
-// Tolerance mode (sessions in an FP16 serving format): the same taps and weights with the
-// hardware exponential (__expf) and fused multiply-adds; the filtered depth differs from the
-// reference's by the exponential's few-ulp error.
-__device__ __forceinline__ float bilateral_px_tol(const float* t, const float* g, float c, float thr, float sig) {
-  constexpr int R = 3;
-  float sd = 0.f, swt = 0.f;
+// Tolerance mode (sessions in an FP16 serving format), radius 3: the same taps for two
+// vertically adjacent pixels (centres c0, c1; t points at pixel 0's window corner, pixel 1's
+// window starts one row lower), the eight staged rows read once for both.  A tap's weight
+// g exp(-diff^2 sigma) is taken as one hardware base-2 exponential of
+// log2(g) + diff^2 (-sigma log2(e)) (lg: log2 of the spatial weights, nk = -sigma log2(e)),
+// with fused multiply-adds; the filtered depth differs from the reference's by a few ulps
+// of the weights.
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ void bilateral_px2_tol(const float* t, const float* lg, float c0, float c1, float thr,
+                                                  float nk, float& out0, float& out1) {
+  constexpr int R = 3, G = 2 * R + 1;
+  float sd0 = 0.f, sw0 = 0.f, sd1 = 0.f, sw1 = 0.f;
 #pragma unroll
-  for (int dy = 0; dy <= 2 * R; ++dy) {
+  for (int r = 0; r <= G; ++r) {
 #pragma unroll
-    for (int dx = 0; dx <= 2 * R; ++dx) {
-      const float nr = t[dy * kPreSW + dx];
-      const float diff = fabsf(c - nr);
-      if (nr > 0.0f && diff < thr) {
-        const float w = g[dy * kGW + dx] * __expf(-(diff * diff) * sig);
-        sd = __fmaf_rn(nr, w, sd);
-        swt += w;
+    for (int dx = 0; dx < G; ++dx) {
+      const float nr = t[r * kPreSW + dx];
+      if (r < G) {
+        const float diff = c0 - nr;
+        if (nr > 0.0f && fabsf(diff) < thr) {
+          const float w = ex2_approx(__fmaf_rn(diff * diff, nk, lg[r * kGW + dx]));
+          sd0 = __fmaf_rn(nr, w, sd0);
+          sw0 += w;
+        }
+      }
+      if (r > 0) {
+        const float diff = c1 - nr;
+        if (nr > 0.0f && fabsf(diff) < thr) {
+          const float w = ex2_approx(__fmaf_rn(diff * diff, nk, lg[(r - 1) * kGW + dx]));
+          sd1 = __fmaf_rn(nr, w, sd1);
+          sw1 += w;
+        }
       }
     }
   }
-  return __fdividef(sd, swt);
+  out0 = __fdividef(sd0, sw0);
+  out1 = __fdividef(sd1, sw1);
 }
 
-__global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(kPreBlockX* kPreBlockY) k_preprocess(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (s.kind < 0) return;
   const int W = s.W, H = s.H, R = s.radius;
@@ -78,16 +100,19 @@ __global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc
   const int tx0 = (blockIdx.x % tilesX) * kPreTX, ty0 = (blockIdx.x / tilesX) * kPreTY;
   if (ty0 >= H) return;
   __shared__ float tile[kPreSH][kPreSW];
-  // spatial weights g[dx] * g[dy] of the taps (the products the tap loop would form)
-  __shared__ float gw[kGW][kGW];
-  const int tid = threadIdx.y * kPreTX + threadIdx.x;
+  // spatial weights g[dx] * g[dy] of the taps (the products the tap loop would form), and
+  // their base-2 logarithms for the tolerance-mode weights
+  __shared__ float gw[kGW][kGW], lgw[kGW][kGW];
+  const int tid = threadIdx.y * kPreBlockX + threadIdx.x;
   if (tid < (2 * R + 1) * (2 * R + 1)) {
     const int ty = tid / (2 * R + 1), tx = tid % (2 * R + 1);
-    gw[ty][tx] = s.gauss[tx] * s.gauss[ty];
+    const float g = s.gauss[tx] * s.gauss[ty];
+    gw[ty][tx] = g;
+    lgw[ty][tx] = log2f(g);
   }
   const float dmin = s.cam.dmin, dmax = s.cam.dmax;
   const int sw = kPreTX + 2 * R, sh = kPreTY + 2 * R;
-  for (int i = tid; i < sw * sh; i += kPreTX * kPreTY) {
+  for (int i = tid; i < sw * sh; i += kPreBlockX * kPreBlockY) {
     int ly = i / sw, lx = i - ly * sw;
     int gx = tx0 - R + lx, gy = ty0 - R + ly;
     float d = qnan();
@@ -98,47 +123,62 @@ __global__ void __launch_bounds__(kPreTX* kPreTY) k_preprocess(const SessionDesc
     tile[ly][lx] = d;
   }
   __syncthreads();
-  const int x = tx0 + threadIdx.x, y = ty0 + threadIdx.y;
-  const bool inside = x < W && y < H;
-  float sc = qnan();
-  if (inside) {
-  const float c = tile[threadIdx.y + R][threadIdx.x + R];
-  float out = qnan();
-  if (!isnan(c)) {
-    const float thr = s.depth_thr, sig = s.sigma_depth;
+  const int ly0 = 2 * threadIdx.y;  // this thread's rows of the tile: ly0, ly0 + 1
+  const int x = tx0 + threadIdx.x;
+  float cs[2], outs[2];
+  for (int k = 0; k < 2; ++k) {
+    cs[k] = tile[ly0 + k + R][threadIdx.x + R];
+    outs[k] = qnan();
+  }
+  const float thr = s.depth_thr, sig = s.sigma_depth;
+  if (s.tol && R == 3) {
+    if (!isnan(cs[0]) || !isnan(cs[1])) {
+      bilateral_px2_tol(&tile[ly0][threadIdx.x], &lgw[0][0], cs[0], cs[1], thr, -sig * 1.44269504088896341f,
+                        outs[0], outs[1]);
+      for (int k = 0; k < 2; ++k)
+        if (isnan(cs[k])) outs[k] = qnan();
+    }
+  } else {
     // every tap's exponent lies in [-thr^2 sigma, 0] (rounding is monotone)
     const bool fast = sig >= 0.f && thr * thr * sig <= 87.f;
-    const float* t = &tile[threadIdx.y][threadIdx.x];
-    if (s.tol && R == 3) out = bilateral_px_tol(t, &gw[0][0], c, thr, sig);
-    else if (fast && R == 3) out = bilateral_px<3, true>(t, &gw[0][0], R, c, thr, sig);
-    else if (fast) out = bilateral_px<0, true>(t, &gw[0][0], R, c, thr, sig);
-    else out = bilateral_px<0, false>(t, &gw[0][0], R, c, thr, sig);
+    for (int k = 0; k < 2; ++k) {
+      if (isnan(cs[k])) continue;
+      const float* t = &tile[ly0 + k][threadIdx.x];
+      if (fast && R == 3) outs[k] = bilateral_px<3, true>(t, &gw[0][0], R, cs[k], thr, sig);
+      else if (fast) outs[k] = bilateral_px<0, true>(t, &gw[0][0], R, cs[k], thr, sig);
+      else outs[k] = bilateral_px<0, false>(t, &gw[0][0], R, cs[k], thr, sig);
+    }
   }
-  const size_t i = (size_t)y * W + x;
-  s.dlev[0][i] = out;
-  const float xl = ((float)x - s.cam.cx) * s.cam.fx_inv;
-  const float yl = ((float)y - s.cam.cy) * s.cam.fy_inv;
-  if (s.vlev[0]) {  // the kernel-level call's vertex map (sessions rebuild vertices from depth)
-    float4 v = make_float4(qnan(), qnan(), qnan(), 0.f);
-    if (!isnan(out)) v = make_float4(out * xl, out * yl, out * 1.0f, 0.f);
-    s.vlev[0][i] = v;
-  }
-  // ray-length depth for integration: the pass-filtered depth, not the bilateral output
-  // (NuiKinfuOpenCLScene.cpp:218 passes GetDepthBuffer())
-  sc = c;
-  if (!isnan(c)) sc = c * sqrtf(xl * xl + yl * yl + 1.f);
-  s.dscaled[i] = sc;
+  float m = 0.f;  // largest ray-length depth of this thread's two pixels
+  for (int k = 0; k < 2; ++k) {
+    const int y = ty0 + ly0 + k;
+    if (x >= W || y >= H) continue;
+    const float c = cs[k], out = outs[k];
+    const size_t i = (size_t)y * W + x;
+    s.dlev[0][i] = out;
+    const float xl = ((float)x - s.cam.cx) * s.cam.fx_inv;
+    const float yl = ((float)y - s.cam.cy) * s.cam.fy_inv;
+    if (s.vlev[0]) {  // the kernel-level call's vertex map (sessions rebuild vertices from depth)
+      float4 v = make_float4(qnan(), qnan(), qnan(), 0.f);
+      if (!isnan(out)) v = make_float4(out * xl, out * yl, out * 1.0f, 0.f);
+      s.vlev[0][i] = v;
+    }
+    // ray-length depth for integration: the pass-filtered depth, not the bilateral output
+    // (NuiKinfuOpenCLScene.cpp:218 passes GetDepthBuffer())
+    float sc = c;
+    if (!isnan(c)) sc = c * sqrtf(xl * xl + yl * yl + 1.f);
+    s.dscaled[i] = sc;
+    if (!isnan(sc)) m = fmaxf(m, sc);
   }
   // largest ray-length depth of each 16x16 tile (lanes 0-15 / 16-31 of a row are two
   // tiles) and of the frame: the bounds integration culls with
-  float m = isnan(sc) ? 0.f : sc;
   for (int off = 8; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
-  __shared__ float rowmax[kPreTY][2];
+  __shared__ float rowmax[kPreBlockY][2];
   if ((threadIdx.x & 15) == 0) rowmax[threadIdx.y][threadIdx.x >> 4] = m;
   __syncthreads();
   if (threadIdx.y == 0 && threadIdx.x < 2) {
     float t = 0.f;
-    for (int r = 0; r < kPreTY; ++r) t = fmaxf(t, rowmax[r][threadIdx.x]);
+    for (int r = 0; r < kPreBlockY; ++r) t = fmaxf(t, rowmax[r][threadIdx.x]);
     const int tcol = tx0 / kTile + threadIdx.x, trow = ty0 / kTile;
     const int ntx = (W + kTile - 1) / kTile;
     if (s.tile_max && tcol < ntx) s.tile_max[trow * ntx + tcol] = t;

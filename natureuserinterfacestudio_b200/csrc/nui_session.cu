@@ -725,7 +725,7 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
   mark(0);
   k_tick_begin<<<cdiv(p.n, 64), 64, 0, st>>>(d, p.n);
   const unsigned tiles = cdiv(p.maxW, 32) * cdiv(p.maxH, 16);
-  k_preprocess<<<dim3(tiles, p.n), dim3(32, 16), 0, st>>>(d);
+  k_preprocess<<<dim3(tiles, p.n), dim3(kPreBlockX, kPreBlockY), 0, st>>>(d);
   mark(1);
   for (int l = 1; l < p.maxLevels; ++l)
     k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), p.n), 256, 0, st>>>(d, l);
@@ -1816,7 +1816,7 @@ nui_status run_stage(nui_session* s, int what) {
   const SessionDesc* dd = s->d_desc1;
   if (what == 0) {
     k_tick_begin<<<1, 64, 0, st>>>(dd, 1);
-    k_preprocess<<<dim3(cdiv(p.maxW, 32) * cdiv(p.maxH, 16), 1), dim3(32, 16), 0, st>>>(dd);
+    k_preprocess<<<dim3(cdiv(p.maxW, 32) * cdiv(p.maxH, 16), 1), dim3(kPreBlockX, kPreBlockY), 0, st>>>(dd);
     for (int l = 1; l < p.maxLevels; ++l)
       k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), 1), 256, 0, st>>>(dd, l);
   } else if (what == 1) {
@@ -2086,7 +2086,7 @@ NUI_API nui_status nui_k_preprocess(nui_ctx* ctx, const uint16_t* d_raw, int W, 
   d.vlev[0] = (float4*)d_vertex4;
   d.dscaled = d_scaled;
   NUI_CUDA(cudaMemcpyAsync(ctx->d_kdesc, &d, sizeof(d), cudaMemcpyHostToDevice, ctx->stream));
-  k_preprocess<<<dim3(cdiv(W, 32) * cdiv(H, 16), 1), dim3(32, 16), 0, ctx->stream>>>(ctx->d_kdesc);
+  k_preprocess<<<dim3(cdiv(W, 32) * cdiv(H, 16), 1), dim3(kPreBlockX, kPreBlockY), 0, ctx->stream>>>(ctx->d_kdesc);
   NUI_CUDA(cudaGetLastError());
   NUI_CUDA(cudaStreamSynchronize(ctx->stream));
   return NUI_OK;
