@@ -674,10 +674,13 @@ __global__ void __launch_bounds__(256) k_hash_project(const SessionDesc* __restr
     if (zx < 0.05f) zx = 0.05f;
     const int bw = lrx - ulx + 1, bh = lry - uly + 1;
     if (bw <= 0 || bh <= 0) continue;
+    // an atomic that cannot lower the pixel's near bound or raise its far bound is skipped:
+    // the bounds only move one way, so a stale read costs an atomic, never a result
     for (int q = lane; q < bw * bh; q += 32) {
       float2* r = s.range + (uly + q / bw) * s.W + (ulx + q % bw);
-      atomicMin(reinterpret_cast<int*>(&r->x), __float_as_int(zx));
-      atomicMax(reinterpret_cast<int*>(&r->y), __float_as_int(zy));
+      const float2 cur = __ldcg(r);
+      if (__float_as_int(zx) < __float_as_int(cur.x)) atomicMin(reinterpret_cast<int*>(&r->x), __float_as_int(zx));
+      if (__float_as_int(zy) > __float_as_int(cur.y)) atomicMax(reinterpret_cast<int*>(&r->y), __float_as_int(zy));
     }
   }
 }

@@ -92,7 +92,7 @@ __device__ __forceinline__ void bilateral_px2_tol(const float* t, const float* l
   out1 = __fdividef(sd1, sw1);
 }
 
-__global__ void __launch_bounds__(kPreBlockX* kPreBlockY) k_preprocess(const SessionDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(kPreBlockX* kPreBlockY, 4) k_preprocess(const SessionDesc* __restrict__ descs) {
   const SessionDesc& s = descs[blockIdx.y];
   if (s.kind < 0) return;
   const int W = s.W, H = s.H, R = s.radius;

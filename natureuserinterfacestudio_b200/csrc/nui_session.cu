@@ -194,6 +194,7 @@ struct BatchPlan {
   // launch over the first n - hashTail descriptors and the hash kernels over the last
   // n - denseHead (0, 0: both families over the whole table)
   int hashTail, denseHead;
+  int anyFirst;             // some session of the batch has its first frame (frame-0 maps)
   nui_tuning tune;          // the context's launch shapes
   BatchPlan() { std::memset(this, 0, sizeof(*this)); }
   bool operator<(const BatchPlan& o) const { return std::memcmp(this, &o, sizeof(BatchPlan)) < 0; }
@@ -546,6 +547,9 @@ void launch_integrate(const BatchPlan& p, const SessionDesc* d, cudaStream_t st)
 template <int F>
 void launch_summary(const BatchPlan& p, const SessionDesc* d, cudaStream_t st, int force) {
   if (!(p.fmtMask & (1 << F))) return;
+  // the tolerance-mode integration re-classifies the bricks it updates itself: bricks of
+  // those formats are left dirty only by a shift (or an import, which forces the pass)
+  if (F >= NUI_TSDF_F16_U8 && !force && !(p.shiftFmtMask & (1 << F))) return;
   k_brick_summary<F><<<dim3(cdiv(p.maxBricks[F], 1024), dense_n(p)), 256, 0, st>>>(d, force);
 }
 // Brick re-classification after integration, then the super-bricks it touched.
@@ -729,7 +733,7 @@ void enqueue_tick(nui_ctx* ctx, const BatchPlan& p, const SessionDesc* d, float*
   mark(1);
   for (int l = 1; l < p.maxLevels; ++l)
     k_pyramid<<<dim3(cdiv((long)(p.maxW >> l) * (p.maxH >> l), 256), p.n), 256, 0, st>>>(d, l);
-  k_feedback<<<dim3(cdiv((long)p.maxW * p.maxH, 256), p.n), 256, 0, st>>>(d);
+  if (p.anyFirst) k_feedback<<<dim3(cdiv((long)p.maxW * p.maxH, 256), p.n), 256, 0, st>>>(d);
   mark(2);
   // With dense and hash sessions in the batch, the hash sessions' tracking, allocation,
   // integration and raycast run on the side stream, beside the dense ones: the two sets of
@@ -863,6 +867,7 @@ nui_status tick_launch(nui_ctx* ctx, nui_session* const* ss, int n, const uint16
     }
     plan_add(p, s);
     int kind = !raws[i] ? kInactive : s->frames == 0 ? kFirstFrame : kTrackFrame;
+    if (kind == kFirstFrame) p.anyFirst = 1;
     fill_desc(s, dd, kind, raws[i], bgras ? bgras[i] : nullptr);
     dd.slot = i;
   }
