@@ -293,7 +293,9 @@ NUI_API nui_status nui_batch_tick_device(nui_ctx* ctx, nui_session* const* sessi
  *            stream needs its budget.
  * Streams join and leave between steps; the batch keeps every live stream (streams without
  * a queued frame sit the tick out), so its captured graph changes only when streams join
- * or leave.  One server per context; not thread-safe. */
+ * or leave.  One server per context; not thread-safe.  Between a step and the next step
+ * (or drain) a tick of the server is in flight: the context runs no other tick
+ * (nui_batch_tick*, nui_process_frame*) until nui_server_drain has returned. */
 typedef struct nui_server nui_server;
 typedef struct {
   int slot;
