@@ -531,7 +531,11 @@ struct HVox<1> {  // half sdf
   }
 };
 
-// One voxel of integrateIntoScene_kernel, given its entry, weight w and sdf oldF.
+// One voxel of integrateIntoScene_kernel, given its entry, weight w and sdf oldF.  The
+// reference's int16 format (HF 0) repeats its arithmetic operation for operation; the half
+// format (HF 1, a serving format judged by tolerance) takes the same steps with fused
+// multiply-adds and approximate reciprocals, which can move a voxel across a pixel's
+// rounding edge or change its value by a few ulps, well inside the half quantum.
 template <int HF>
 __device__ __forceinline__ void integrate_voxel(const SessionDesc& s, const DevXform& m, const HEntry& en, int w,
                                                 float oldF, int lid, int lx, int ly, int lz, unsigned& touched) {
@@ -540,15 +544,29 @@ __device__ __forceinline__ void integrate_voxel(const SessionDesc& s, const DevX
   if (s.max_w == w) return;
   const float3 pm = mul3(f3((float)(en.pos[0] * 8 + lx), (float)(en.pos[1] * 8 + ly), (float)(en.pos[2] * 8 + lz)),
                          s.voxel);
-  const float3 pc = xf_inverse(m, pm);
-  if (pc.z <= 0) return;
-  const int ix = (int)(pc.x * s.cam.fx / pc.z + s.cam.cx + 0.5f), iy = (int)(pc.y * s.cam.fy / pc.z + s.cam.cy + 0.5f);
+  float3 pc;
+  int ix, iy;
+  if (HF == 0) {
+    pc = xf_inverse(m, pm);
+    if (pc.z <= 0) return;
+    ix = (int)(pc.x * s.cam.fx / pc.z + s.cam.cx + 0.5f);
+    iy = (int)(pc.y * s.cam.fy / pc.z + s.cam.cy + 0.5f);
+  } else {
+    const float dx = pm.x - m.t[0], dy = pm.y - m.t[1], dz = pm.z - m.t[2];
+    const float* Ri = m.R_inv;
+    pc = f3(__fmaf_rn(Ri[0], dx, __fmaf_rn(Ri[1], dy, Ri[2] * dz)), __fmaf_rn(Ri[3], dx, __fmaf_rn(Ri[4], dy, Ri[5] * dz)),
+            __fmaf_rn(Ri[6], dx, __fmaf_rn(Ri[7], dy, Ri[8] * dz)));
+    if (pc.z <= 0) return;
+    const float iz = __fdividef(1.0f, pc.z);
+    ix = (int)__fmaf_rn(pc.x * s.cam.fx, iz, s.cam.cx + 0.5f);
+    iy = (int)__fmaf_rn(pc.y * s.cam.fy, iz, s.cam.cy + 0.5f);
+  }
   if (ix < 0 || ix >= s.W || iy < 0 || iy >= s.H) return;
   const int sid = iy * s.W + ix;
   const float d = pass_depth(s, sid);
   if (isnan(d)) return;
   const float eta = d - pc.z;
-  const float sdf = eta / s.mu;
+  const float sdf = HF == 0 ? eta / s.mu : eta * __fdividef(1.0f, s.mu);
   if (eta < -s.mu) return;
   const float oldW = (float)w;
   float newF = fminf(1.0f, sdf);
@@ -557,15 +575,27 @@ __device__ __forceinline__ void integrate_voxel(const SessionDesc& s, const DevX
     const uchar4 col = reinterpret_cast<const uchar4*>(s.bgra)[sid];
     if (col.w == 255) {
       const uchar4 vc = s.hrgb[bid];
-      const float r = (oldW * (float)vc.x + newW * (float)col.z) / cw;
-      const float g = (oldW * (float)vc.y + newW * (float)col.y) / cw;
-      const float bl = (oldW * (float)vc.z + newW * (float)col.x) / cw;
+      float r, g, bl;
+      if (HF == 0) {
+        r = (oldW * (float)vc.x + newW * (float)col.z) / cw;
+        g = (oldW * (float)vc.y + newW * (float)col.y) / cw;
+        bl = (oldW * (float)vc.z + newW * (float)col.x) / cw;
+      } else {
+        const float icw = __fdividef(1.0f, cw);
+        r = __fmaf_rn(oldW, (float)vc.x, (float)col.z) * icw;
+        g = __fmaf_rn(oldW, (float)vc.y, (float)col.y) * icw;
+        bl = __fmaf_rn(oldW, (float)vc.z, (float)col.x) * icw;
+      }
       s.hrgb[bid] = make_uchar4((unsigned char)fminf(fmaxf(r, 0.f), 255.f), (unsigned char)fminf(fmaxf(g, 0.f), 255.f),
                                 (unsigned char)fminf(fmaxf(bl, 0.f), 255.f), 0);
     }
   }
-  newF = oldW * oldF + newW * newF;
-  newF /= cw;
+  if (HF == 0) {
+    newF = oldW * oldF + newW * newF;
+    newF /= cw;
+  } else {
+    newF = __fdividef(__fmaf_rn(oldW, oldF, newF), cw);
+  }
   HVox<HF>::store(s.hsdf, bid, newF);
   s.hw[bid] = (uint8_t)min((int)(uint8_t)cw, s.max_w);
   ++touched;

@@ -97,6 +97,46 @@ def test_hash_serving_table_sizes_bit_exact(gpu_ctx):
     _hash_given_poses(gpu_ctx, cfg, seq, mesh_at=(2,), color=False)
 
 
+def test_hash_half_format_given_poses_within_tolerance(gpu_ctx):
+    """The half-sdf pool of the serving mix (tolerance-mode voxel update) at given poses
+    against the oracle's int16 pool: the same table (entries and visible list) bit for bit,
+    and over the voxels either side has updated, sdf within 1e-3 truncation units at the
+    0.999 quantile (the half quantum is at most 4.9e-4 there), weights equal on all but 1e-3
+    of them and colours within one level on all but 1e-3."""
+    cfg = cfg_hash(fmt=L.TSDF_F16_U8, color=True)
+    seq = frames(5, W=320, H=240, seed=5, kind=L.SYNTH_ROOM, deg=3.0, color=True)
+    W, H = cfg.width, cfg.height
+    s = L.Session(gpu_ctx, cfg)
+    oh = O.OracleHash(cfg.hash_buckets, cfg.hash_excess, cfg.hash_pool_blocks, voxel=cfg.voxel_size,
+                      mu=cfg.trunc_scale, max_w=cfg.hash_max_weight)
+    cam = O.OrcCam.make(W, H, cfg.fx, cfg.fy, cfg.cx, cfg.cy, cfg.depth_min, cfg.depth_max)
+    try:
+        for k, ((raw, bgra, _, _), (R, t)) in enumerate(zip(seq, relative_gt(seq))):
+            bgra = np.ascontiguousarray(bgra)
+            x = O.make_xform(R, t)
+            d = _pass_depth(raw, cfg)
+            oh.allocate(d, cam, x)
+            oh.integrate(d, bgra.reshape(-1), cam, x)
+            oh.raycast(cam, x, color=True)
+            s.upload(raw, bgra)
+            s.set_pose(R, t)
+            s.integrate()
+            s.raycast()
+            assert np.array_equal(s.hash_download(21), oh.visible()), k
+            assert np.array_equal(s.hash_download(20), oh.entries().view(np.uint8)), k
+            g = s.hash_download(22).view(O.REF_VOXEL)
+            o = _oracle_voxels(oh).view(O.REF_VOXEL)
+            upd = (g["w"] > 0) | (o["w"] > 0)
+            assert upd.sum() > 10000, k
+            dsdf = np.abs(g["sdf"][upd].astype(np.int64) - o["sdf"][upd]) / 32767.0
+            assert np.quantile(dsdf, 0.999) <= 1e-3, (k, float(np.quantile(dsdf, 0.999)))
+            assert np.mean(g["w"][upd] != o["w"][upd]) <= 1e-3, k
+            dc = np.abs(g["rgb"][upd].astype(np.int64) - o["rgb"][upd]).max(axis=1)
+            assert np.mean(dc > 1) <= 1e-3, k
+    finally:
+        s.close()
+
+
 def test_dense_256_config_poses_over_32_frames(gpu_ctx):
     """256^3 over 3 m, truncation 46.875 mm, ICP 10/5/4, 640x480 with sensor noise."""
     cfg = cfg_for(res=(256, 256, 256), dim=3.0, trunc=0.046875, iters=(10, 5, 4))
