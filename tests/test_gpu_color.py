@@ -80,6 +80,26 @@ def test_hash_color_tracking_against_oracle(gpu_ctx):
         assert rot_angle(pose[:9].reshape(3, 3), Ro) < 1e-4 and np.max(np.abs(pose[9:] - to)) < 1e-4, i
 
 
+def test_hash_half_color_tracking_close_to_oracle(gpu_ctx):
+    """The served voxel-hash streams' configuration -- half-sdf pool, colour ICP in
+    tolerance mode (one reciprocal of the depth per photometric row) -- stays frame by frame
+    within 4 mrad / 4 mm of the oracle tracking the reference's int16 pool."""
+    seq = frames(6, W=320, H=240, seed=3, color=True)
+    cfg = cfg_hash(color=True, fmt=L.TSDF_F16_U8)
+    cfg.photometric_weight = 0.1
+    ocfg = cfg_hash(color=True)
+    ocfg.photometric_weight = 0.1
+    s = L.Session(gpu_ctx, cfg)
+    eng = O.Engine(ocfg)
+    for i, (d, c, _, _) in enumerate(seq):
+        c = np.ascontiguousarray(c)
+        ok, pose = s.process(d, c)
+        assert ok and eng.frame(d, c), i
+        Ro, to = eng.pose()
+        assert rot_angle(pose[:9].reshape(3, 3), Ro) < 4e-3 and np.max(np.abs(pose[9:] - to)) < 4e-3, i
+    s.close()
+
+
 def test_color_tracking_fp16_ate_within_1mm_of_fp32(gpu_ctx):
     seq = frames(16, W=640, H=480, seed=4, color=True)
     ate = {}
