@@ -513,7 +513,10 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
   if (status0 != 0) return;
   for (int level = s.levels - 1; level >= 0; --level) {
     const int n = (s.W >> level) * (s.H >> level);
-    const int per_block = kIcpThreads * PPT;
+    // the coarser levels in blocks of one pixel a thread: their few pixel blocks would
+    // otherwise fall unevenly on the cluster's blocks (19 blocks of 1024 pixels for 16 at
+    // 160 x 120), and a pass waits for its slowest block
+    const int per_block = kIcpThreads * (level == 0 ? PPT : 1);
     const int nblocks = (n + per_block - 1) / per_block;
     const bool photo = s.photo_w > 0.f && level == 0;
     const int ncb = photo ? (s.W * s.H + per_block - 1) / per_block : 0;
@@ -522,7 +525,11 @@ __global__ void __launch_bounds__(kIcpThreads, 2)
       double acc[kIcpTerms];
 #pragma unroll
       for (int k = 0; k < kIcpTerms; ++k) acc[k] = 0.0;
-      for (int vb = rank; vb < nblocks; vb += C) icp_depth_rows<PPT>(s, level, vb, sR, tc, sp, acc);
+      if (level == 0) {
+        for (int vb = rank; vb < nblocks; vb += C) icp_depth_rows<PPT>(s, level, vb, sR, tc, sp, acc);
+      } else {
+        for (int vb = rank; vb < nblocks; vb += C) icp_depth_rows<1>(s, level, vb, sR, tc, sp, acc);
+      }
       double D = icp_block_sum(acc);
       if (threadIdx.x < kIcpTerms) part[0][threadIdx.x] = D;
       if (photo) {
