@@ -346,7 +346,8 @@ NUI_API nui_status nui_ctx_last_tick_kernels(nui_ctx* ctx, int* n);
  *                            threads (chunks of >= 16 slices); 14..22, default 18
  *   icp_pixels_per_thread    ICP block: 256 threads x this many pixels; 2, 4, 8 or 16 (4)
  *   icp_cluster_blocks       ICP: thread blocks of the cluster that tracks one session;
- *                            2, 4, 8 or 16 (16, a non-portable cluster size)
+ *                            2..16 (12: six SMs at two blocks an SM, so that three
+ *                            clusters fill an 18-SM GPC; above 8 a non-portable size)
  *   raycast_tile_width       dense raycast: a warp shades a tile this wide and 32 / this
  *                            high, a block 2 x 2 such tiles; 4, 8, 16 or 32 (8)
  *   hash_raycast_tile_width  the same for the voxel-hash raycast (8)

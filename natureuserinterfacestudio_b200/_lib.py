@@ -60,7 +60,7 @@ class Tuning(C.Structure):
         # the ICP cluster size defaults to the library's default when left out
         super().__init__(*args, **kw)
         if len(args) < 5 and "icp_cluster_blocks" not in kw:
-            self.icp_cluster_blocks = 16
+            self.icp_cluster_blocks = 12
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

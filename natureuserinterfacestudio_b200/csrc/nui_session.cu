@@ -234,7 +234,7 @@ struct nui_ctx {
   };
   std::map<BatchPlan, Graph> graphs;
   int last_kernels = 0;  // kernels of the last graphed tick
-  nui_tuning tune = {18, 4, 8, 8, 16};
+  nui_tuning tune = {18, 4, 8, 8, 12};
   cudaMemPool_t pool = nullptr;  // session state (stream-ordered; freed memory stays here)
 };
 
@@ -1185,8 +1185,7 @@ bool tuning_valid(const nui_tuning& t) {
   return t.integrate_threads_log2 >= 14 && t.integrate_threads_log2 <= 22 &&
          (t.icp_pixels_per_thread == 2 || t.icp_pixels_per_thread == 4 || t.icp_pixels_per_thread == 8 ||
           t.icp_pixels_per_thread == 16) &&
-         (t.icp_cluster_blocks == 2 || t.icp_cluster_blocks == 4 || t.icp_cluster_blocks == 8 ||
-          t.icp_cluster_blocks == 16) &&
+         (t.icp_cluster_blocks >= 2 && t.icp_cluster_blocks <= 16) &&
          tw_ok(t.raycast_tile_width) && tw_ok(t.hash_raycast_tile_width);
 }
 
@@ -1303,7 +1302,7 @@ NUI_API nui_status nui_ctx_autotune(nui_ctx* c, const nui_session_cfg* cfgs, int
   if (dense) tune_one(&nui_tuning::integrate_threads_log2, {16, 17, 18, 19, 20}, 3);
   // the ICP shapes and ray tiles by the whole tick: with dense and hash sessions the hash
   // sessions' tracking and raycast run on the second stream, beside stages 2-5
-  tune_one(&nui_tuning::icp_cluster_blocks, {8, 16}, 6);
+  tune_one(&nui_tuning::icp_cluster_blocks, {8, 12, 16}, 6);
   tune_one(&nui_tuning::icp_pixels_per_thread, {2, 4, 8, 16}, 6);
   if (dense) tune_one(&nui_tuning::raycast_tile_width, {4, 8, 16, 32}, 6);
   if (hash) tune_one(&nui_tuning::hash_raycast_tile_width, {4, 8, 16, 32}, 6);

@@ -12,7 +12,7 @@ from _util import cfg_for, cfg_hash, frames, rot_angle, same_bits
 
 pytestmark = pytest.mark.gpu
 
-DEFAULT = (18, 4, 8, 8, 16)
+DEFAULT = (18, 4, 8, 8, 12)
 
 
 @pytest.fixture(scope="module")
@@ -55,7 +55,7 @@ def test_icp_shapes_regroup_sums_only(gpu_ctx, mix):
     non-portable size) change only the grouping of the FP64 partial sums."""
     gpu_ctx.set_tuning(L.Tuning(*DEFAULT))
     base, _ = _run(gpu_ctx, mix)
-    for ppt, cl in ((2, 16), (8, 16), (16, 16), (4, 2), (4, 4), (8, 8)):
+    for ppt, cl in ((2, 16), (8, 16), (16, 16), (4, 2), (4, 4), (8, 8), (4, 10), (4, 16)):
         gpu_ctx.set_tuning(L.Tuning(18, ppt, 8, 8, cl))
         p, _ = _run(gpu_ctx, mix)
         for f in range(p.shape[0]):
@@ -69,7 +69,7 @@ def test_icp_shapes_regroup_sums_only(gpu_ctx, mix):
 def test_out_of_range_tuning_is_rejected(gpu_ctx):
     before = gpu_ctx.tuning().as_dict()
     for bad in [L.Tuning(13, 4, 8, 8), L.Tuning(18, 3, 8, 8), L.Tuning(18, 4, 12, 8), L.Tuning(18, 4, 8, 64),
-                L.Tuning(18, 4, 8, 8, 3), L.Tuning(18, 4, 8, 8, 32)]:
+                L.Tuning(18, 4, 8, 8, 1), L.Tuning(18, 4, 8, 8, 17), L.Tuning(18, 4, 8, 8, 32)]:
         with pytest.raises(L.NuiError):
             gpu_ctx.set_tuning(bad)
     assert gpu_ctx.tuning().as_dict() == before
@@ -83,7 +83,7 @@ def test_autotune_keeps_a_valid_choice_and_frees_its_sessions(gpu_ctx, mix):
     d = t.as_dict()
     assert d == gpu_ctx.tuning().as_dict()
     assert 16 <= d["integrate_threads_log2"] <= 20
-    assert d["icp_pixels_per_thread"] in (2, 4, 8, 16) and d["icp_cluster_blocks"] in (8, 16)
+    assert d["icp_pixels_per_thread"] in (2, 4, 8, 16) and d["icp_cluster_blocks"] in (8, 12, 16)
     assert d["raycast_tile_width"] in (4, 8, 16, 32) and d["hash_raycast_tile_width"] in (4, 8, 16, 32)
     assert ms > 0
     assert torch.cuda.mem_get_info()[0] >= free0 - (64 << 20)
