@@ -5,6 +5,8 @@ results depend only on given poses, so that every comparison runs unconditionall
   colour, expected range) and the block mesh, bit for bit, after every frame; once with a
   small table whose excess chains are long, once at 640x480 with 2^20 buckets and a 2^19-block
   pool (the serving configuration's table sizes).
+- The half-sdf pool of the served streams at given poses: the table bit for bit, voxels and
+  raycast maps within tolerance of the oracle's int16 pool.
 - Dense 256^3 over 3 m (truncation 46.875 mm, ICP 10/5/4): per-frame pose within 1e-4 rad and
   0.1 mm of the oracle over 32 tracked frames.
 - Dense 512^3 over 4 m at given poses: the int16 volume and the raycast maps bit for bit.
@@ -102,7 +104,9 @@ def test_hash_half_format_given_poses_within_tolerance(gpu_ctx):
     against the oracle's int16 pool: the same table (entries and visible list) bit for bit,
     and over the voxels either side has updated, sdf within 1e-3 truncation units at the
     0.999 quantile (the half quantum is at most 4.9e-4 there), weights equal on all but 1e-3
-    of them and colours within one level on all but 1e-3."""
+    of them and colours within one level on all but 1e-3.  The raycast of the half pool
+    against the oracle's: hit masks agree on all but 1 % of the pixels, and where both hit
+    the surface points agree within 0.5 mm at the 0.99 quantile."""
     cfg = cfg_hash(fmt=L.TSDF_F16_U8, color=True)
     seq = frames(5, W=320, H=240, seed=5, kind=L.SYNTH_ROOM, deg=3.0, color=True)
     W, H = cfg.width, cfg.height
@@ -117,7 +121,7 @@ def test_hash_half_format_given_poses_within_tolerance(gpu_ctx):
             d = _pass_depth(raw, cfg)
             oh.allocate(d, cam, x)
             oh.integrate(d, bgra.reshape(-1), cam, x)
-            oh.raycast(cam, x, color=True)
+            vm, _, _, _ = oh.raycast(cam, x, color=True)
             s.upload(raw, bgra)
             s.set_pose(R, t)
             s.integrate()
@@ -133,6 +137,14 @@ def test_hash_half_format_given_poses_within_tolerance(gpu_ctx):
             assert np.mean(g["w"][upd] != o["w"][upd]) <= 1e-3, k
             dc = np.abs(g["rgb"][upd].astype(np.int64) - o["rgb"][upd]).max(axis=1)
             assert np.mean(dc > 1) <= 1e-3, k
+            gv = s.download(3)[..., :3].reshape(-1, 3).astype(np.float64)
+            ov = vm.reshape(-1, 3).astype(np.float64)
+            hg, ho = ~np.isnan(gv[:, 0]), ~np.isnan(ov[:, 0])
+            assert ho.mean() > 0.3, k
+            assert np.mean(hg != ho) <= 0.01, (k, float(np.mean(hg != ho)))
+            both = hg & ho
+            dist = np.linalg.norm(gv[both] - ov[both], axis=1)
+            assert np.quantile(dist, 0.99) <= 5e-4, (k, float(np.quantile(dist, 0.99)), float(dist.max()))
     finally:
         s.close()
 
