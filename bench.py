@@ -258,7 +258,7 @@ def run_ours(args, rank, world):
     torch.cuda.empty_cache()
     ctx.trim()
 
-    # rooflines of the dominant kernels, from the work the kernels counted (DESIGN.md §3):
+    # rooflines of the dominant kernels, from the work the kernels counted:
     #   integration (k_integrate_fast, stage 3): updated voxels read and written (3 B each
     #     way, FP16 + u8), the voxels of re-classified bricks read once, the depth image read;
     #   dense raycast (k_raycast_fast + k_raycast_finish_fast, stage 7): the voxels the march

@@ -533,7 +533,7 @@ struct HVox<1> {  // half sdf
 
 // One voxel of integrateIntoScene_kernel, given its entry, weight w and sdf oldF.  The
 // reference's int16 format (HF 0) repeats its arithmetic operation for operation; the half
-// format (HF 1, a serving format judged by tolerance) takes the same steps with fused
+// format (HF 1, a serving format checked against tolerances) takes the same steps with fused
 // multiply-adds and approximate reciprocals, which can move a voxel across a pixel's
 // rounding edge or change its value by a few ulps, well inside the half quantum.
 template <int HF>

@@ -48,12 +48,12 @@ def _place_rank(rank, world, port, out):
         GB = 1 << 30
         pl = Placement([10 * GB, 10 * GB]) if rank == 0 else None
         got, waited = [], []
-        # round 1: six streams of 3 GB -> three per GPU, alternating; the seventh waits
+        # first placement: six streams of 3 GB -> three per GPU, alternating; the seventh waits
         arrivals = [(i, 3 * GB) for i in range(7)]
         mine, waiting = place_round(pl, arrivals, [], rank, world)
         got.append(mine)
         waited.append(waiting)
-        # round 2: stream 0 leaves; the waiting stream takes its place
+        # second placement: stream 0 leaves; the waiting stream takes its place
         mine, waiting = place_round(pl, [(6, 3 * GB)], [0], rank, world)
         got.append(mine)
         waited.append(waiting)
